@@ -1,0 +1,168 @@
+"""CPU tests: the oracle against the reference-generated golden fixtures and the reference's
+known-answer properties (no GPU)."""
+
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+
+from oracle import assemble as oa
+from oracle import element as oe
+from oracle import mesh as om
+from oracle import pcg as op
+
+CASES = [(2, 2, 2), (3, 2, 4), (4, 4, 4)]
+
+
+@pytest.mark.parametrize("nx,ny,nz", CASES)
+def test_mesh_matches_reference(golden, nx, ny, nz):
+    tag = f"{nx}x{ny}x{nz}"
+    pts, tets = om.equi_distant_box(nx, ny, nz)
+    assert np.array_equal(pts, golden[f"{tag}/points"])
+    assert np.array_equal(tets, golden[f"{tag}/tets"])
+
+
+@pytest.mark.parametrize("nx,ny,nz", CASES)
+def test_p2_numbering_matches_reference(golden, nx, ny, nz):
+    tag = f"{nx}x{ny}x{nz}"
+    pts, cells = om.promote_p2(golden[f"{tag}/jittered"], golden[f"{tag}/tets"])
+    assert np.array_equal(cells, golden[f"{tag}/p2_cells"])
+    assert np.array_equal(pts, golden[f"{tag}/p2_points"])
+
+
+@pytest.mark.parametrize("nx,ny,nz", CASES)
+@pytest.mark.parametrize("order", [1, 2])
+def test_compress_plan_matches_reference(golden, nx, ny, nz, order):
+    tag = f"{nx}x{ny}x{nz}"
+    cells = golden[f"{tag}/tets"] if order == 1 else golden[f"{tag}/p2_cells"]
+    idx, inverse, nse = oa.compress_plan(cells)
+    assert nse == int(golden[f"{tag}/p{order}_nse"])
+    assert np.array_equal(idx, golden[f"{tag}/p{order}_idx"])
+    assert np.array_equal(inverse, golden[f"{tag}/p{order}_inverse"])
+    n = int(cells.max()) + 1
+    indptr, indices, slot = oa.csr_pattern_fast(cells, n)
+    ip2, ind2 = oa.plan_to_csr(idx, n)
+    assert np.array_equal(indptr, ip2) and np.array_equal(indices, ind2)
+    assert np.array_equal(slot, inverse)
+
+
+@pytest.mark.parametrize("nx,ny,nz", CASES)
+@pytest.mark.parametrize("order", [1, 2])
+def test_boundary_nodes_match_reference(golden, nx, ny, nz, order):
+    tag = f"{nx}x{ny}x{nz}"
+    cells = golden[f"{tag}/tets"] if order == 1 else golden[f"{tag}/p2_cells"]
+    assert np.array_equal(om.boundary_nodes(cells, order), golden[f"{tag}/p{order}_boundary"])
+
+
+def test_sizes_of_the_configs():
+    """Appendix sizes: n, boundary DOFs and nse at P1 8^3 / P2 4^3 follow the closed formulas."""
+    for nh in (3, 8):
+        pts, tets = om.equi_distant_box(nh, nh, nh)
+        E = 3 * nh * (nh + 1) ** 2 + 3 * nh**2 * (nh + 1) + nh**3
+        n = (nh + 1) ** 3
+        _, _, nse = oa.compress_plan(tets)
+        assert nse == n + 2 * E
+        assert om.boundary_nodes(tets, 1).size == 6 * nh * nh + 2
+        p2p, p2c = om.promote_p2(pts, tets)
+        assert p2p.shape[0] == n + E
+        assert om.boundary_nodes(p2c, 2).size == 6 * (2 * nh) ** 2 + 2
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_closed_form_equals_quadrature(order):
+    pts, tets = om.equi_distant_box(3, 3, 3)
+    pts = om.jitter_interior(pts, 3, 3, 3, seed=5)
+    X = pts[tets]
+    K1, F1 = oe.element_matrices(X, order)
+    K2, F2 = oe.element_matrices_quadrature(X, order)
+    assert np.abs(K1 - K2).max() <= 1e-12 * np.abs(K1).max()
+    assert np.abs(F1 - F2).max() <= 1e-12 * np.abs(F1).max()
+    # symmetric, rows sum to zero (constants are in the kernel), partition of unity on the load
+    assert np.abs(K1 - K1.transpose(0, 2, 1)).max() <= 1e-13 * np.abs(K1).max()
+    assert np.abs(K1.sum(axis=2)).max() <= 1e-12 * np.abs(K1).max()
+    vol = np.abs(np.linalg.det(np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], -1))) / 6
+    assert np.allclose(F1.sum(axis=1), vol, rtol=1e-13)
+
+
+def _solve_direct(system):
+    return spla.spsolve(system.csr().tocsc(), system.b)
+
+
+def test_p1_recovers_linear_field():
+    """Port of tests/test_fem_3d.py:76-89: u = 1 + 2x + 3y + 4z is reproduced exactly by P1."""
+    n = 4
+    pts, tets = om.equi_distant_box(n, n, n)
+    pts = om.jitter_interior(pts, n, n, n, seed=3)
+    bnd = om.boundary_nodes(tets, 1)
+    g = 1 + 2 * pts[:, 0] + 3 * pts[:, 1] + 4 * pts[:, 2]
+    s = oa.assemble(pts, tets, 1, bnd, np.ones(len(tets)), f=0.0, g=g)
+    u = _solve_direct(s)
+    assert np.abs(u - g).max() < 1e-9
+
+
+def test_p2_reproduces_quadratic_exactly():
+    """Port of tests/test_fem_native_lagrange.py:377-395 (P2 patch test, f = -12)."""
+    n = 3
+    pts, tets = om.equi_distant_box(n, n, n)
+    pts = om.jitter_interior(pts, n, n, n, seed=4)
+    p2p, p2c = om.promote_p2(pts, tets)
+    bnd = om.boundary_nodes(p2c, 2)
+    x, y, z = p2p.T
+    exact = x**2 + 2 * y**2 + 3 * z**2 + x * y
+    s = oa.assemble(p2p, p2c, 2, bnd, np.ones(len(tets)), f=-12.0, g=exact)
+    u = _solve_direct(s)
+    assert np.abs(u - exact).max() < 1e-9
+
+
+def test_p0_linearity_and_support():
+    """Port of tests/test_topology_optimisation.py:210-237 on the free block."""
+    n = 3
+    pts, tets = om.equi_distant_box(n, n, n)
+    bnd = om.boundary_nodes(tets, 1)
+    T = len(tets)
+    full = oa.assemble(pts, tets, 1, bnd, np.ones(T)).csr().toarray()
+    free = np.setdiff1d(np.arange(full.shape[0]), bnd)
+    acc = np.zeros((free.size, free.size))
+    for j in range(T):
+        acc += oa.assemble(pts, tets, 1, bnd, np.eye(T)[j]).csr().toarray()[np.ix_(free, free)]
+    assert np.abs(acc - full[np.ix_(free, free)]).max() <= 1e-12
+    j = 40
+    kj = oa.assemble(pts, tets, 1, bnd, np.eye(T)[j]).csr().toarray()
+    cell = set(tets[j].tolist())
+    off = [i for i in range(kj.shape[0]) if i not in cell and i not in set(bnd.tolist())]
+    assert np.abs(kj[np.ix_(off, off)]).max() == 0.0
+
+
+def test_dirichlet_rows_are_identity_and_zeros_kept():
+    n = 3
+    pts, tets = om.equi_distant_box(n, n, n)
+    bnd = om.boundary_nodes(tets, 1)
+    s = oa.assemble(pts, tets, 1, bnd, np.exp(om.logk_field(len(tets), 1)))
+    _, _, nse = oa.compress_plan(tets)
+    assert s.data.size == nse  # explicit zeros stay stored (parametric route)
+    A = s.csr().toarray()
+    assert np.array_equal(A[bnd][:, bnd], np.eye(bnd.size))
+    assert np.abs(A[bnd]).sum() == bnd.size and np.abs(A[:, bnd]).sum() == bnd.size
+    assert np.allclose(A, A.T, atol=0, rtol=0) or np.abs(A - A.T).max() < 1e-15
+    assert oa.compact(s).nnz < nse
+
+
+def test_pcg_matches_direct_and_jacobi_guard():
+    n = 6
+    pts, tets = om.equi_distant_box(n, n, n)
+    pts = om.jitter_interior(pts, n, n, n, seed=0)
+    bnd = om.boundary_nodes(tets, 1)
+    s = oa.assemble(pts, tets, 1, bnd, np.exp(om.logk_field(len(tets), 1000)))
+    A = s.csr()
+    d = oa.matrix_diagonal(s)
+    x, it, hist = op.pcg(A, s.b, oa.jacobi_inverse(d), tol=1e-8)
+    xd = _solve_direct(s)
+    assert it > 5 and hist[-1] <= 1e-16 * np.dot(s.b, s.b)
+    assert np.abs(x - xd).max() <= 1e-7 * np.abs(xd).max()
+    assert op.residual_check(A, s.b, x) < 1e-7
+    assert np.array_equal(oa.jacobi_inverse(np.array([0.0, 2.0, 1e-31])), np.array([1.0, 0.5, 1.0]))
+
+
+def test_pcg_zero_rhs_takes_no_iteration():
+    A = np.eye(3)
+    x, it, _ = op.pcg(A, np.zeros(3), np.ones(3))
+    assert it == 0 and np.all(x == 0)
