@@ -1,0 +1,469 @@
+#!/usr/bin/env python
+"""Benchmark: P1 128^3 Kuhn-tet Poisson, FP64 assembly + Jacobi-PCG to 1e-8, DOF/s on B200.
+
+One step = assemble the CSR operator for one of 20 seeded log-conductivity fields, build the Jacobi
+inverse, run PCG from x0 = 0 to the 1e-8 relative stop rule and evaluate the eager residual guard
+(one more SpMV), with the mesh, plan and k fields resident in HBM. ``value`` = DOFs / step time
+(all ranks' DOFs over the max-over-ranks time). Variants (mixed precision, matrix-free), the SpMV
+roofline, the end-to-end number through the public ``jno_b200`` API with host buffers, SM clocks
+and a CPU baseline (the numpy/scipy oracle on a bounded sample) ride on the same JSON line.
+
+``--impl reference`` times the oracle (the CPU restatement of jNO's path; jNO itself cannot be
+imported on this image) on the same workload instead.
+"""
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "assemble+CG DOF/s at 1e-8 rel err, mixed vs FP64 (1 B200); SpMV HBM GB/s"
+N_FIELDS = 20
+FIELD_SEED0 = 1000
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=128, help="hexes per cube side")
+    ap.add_argument("--order", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
+    return ap.parse_args()
+
+
+def workload_desc(n, order, T, ndof, nnz):
+    return (f"P{order} {n}^3 Kuhn tets ({T:,} tets, {ndof:,} DOF, {nnz:,} CSR nnz), jittered +-0.1h, "
+            f"k=exp(N(0,0.5^2)) per tet, u=0 on the boundary, FP64 assembly to CSR + Jacobi-PCG to 1e-8, "
+            f"{N_FIELDS} seeded k fields")
+
+
+def make_mesh(n):
+    from jno_b200.domain import box_points_tets, jitter_interior
+
+    pts, tets = box_points_tets(n, n, n)
+    return jitter_interior(pts, n, n, n, seed=0), tets
+
+
+def logk_fields(T, count=N_FIELDS):
+    return [np.random.default_rng(FIELD_SEED0 + i).normal(0.0, 0.5, T) for i in range(count)]
+
+
+# ------------------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.rows = []
+        self.proc = None
+        self.dev = device_index
+
+    def start(self):
+        try:
+            ident = self._ident()
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={ident}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _ident(self):
+        import torch
+
+        try:
+            return "GPU-" + str(torch.cuda.get_device_properties(self.dev).uuid)
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            return vis.split(",")[self.dev] if vis else str(self.dev)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], [], set()
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+                for nm, v in zip(names, r[4:8]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------ CPU oracle
+class CpuOracle:
+    """The oracle pipeline on the CPU: pattern and boundary set as setup, then timed samples."""
+
+    def __init__(self, n):
+        from oracle import assemble as oa
+        from oracle import mesh as om
+
+        self.oa = oa
+        self.n_h = n
+        self.pf, self.cf, self.tets, self.p1 = om.kuhn_cube(n, order=1, seed=0)
+        self.ndof = self.pf.shape[0]
+        self.indptr, self.indices, self.slot = oa.csr_pattern_fast(self.cf, self.ndof)
+        self.bnd = om.boundary_nodes(self.cf, 1)
+        self.fields = logk_fields(len(self.tets), 2)
+
+    def assemble_full(self, logk):
+        return self.oa.assemble(self.pf, self.cf, 1, self.bnd, np.exp(logk), plan=(self.indptr, self.indices,
+                                                                                   self.slot))
+
+    def sample(self, logk, iters_total, slab_fraction=8, cg_iters=20, system=None):
+        """Time 1/slab_fraction of the element assembly and cg_iters PCG iterations; extrapolate."""
+        from oracle import element as oe
+        from oracle import pcg as op
+
+        T = len(self.tets)
+        m = T // slab_fraction
+        t0 = time.perf_counter()
+        K, F = oe.element_matrices(self.p1[self.tets[:m]], 1)
+        Ke = np.exp(logk[:m])[:, None, None] * K
+        np.bincount(self.slot[: m * 16], weights=Ke.reshape(-1), minlength=self.indices.size)
+        np.bincount(self.cf[:m].reshape(-1), weights=F.reshape(-1), minlength=self.ndof)
+        t_asm = (time.perf_counter() - t0) * slab_fraction
+        if system is None:
+            system = self.assemble_full(logk)
+        A = system.csr()
+        t0 = time.perf_counter()
+        inv = self.oa.jacobi_inverse(self.oa.matrix_diagonal(system))
+        t_jac = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        op.pcg(A, system.b, inv, tol=1e-8, maxiter=cg_iters)
+        t_cg = time.perf_counter() - t0
+        t_total = t_asm + t_jac + t_cg / cg_iters * iters_total
+        desc = (f"oracle (numpy/scipy, FP64, 1 thread) on P1 {self.n_h}^3: element assembly of 1/{slab_fraction} "
+                f"of the tets x{slab_fraction}, Jacobi, {cg_iters} PCG iterations x {iters_total}/{cg_iters} "
+                f"(iterations of the full solve)")
+        return self.ndof / t_total, t_total, desc
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cpu = CpuOracle(args.n)
+    sys_full = cpu.assemble_full(cpu.fields[0])
+    from oracle import pcg as op
+
+    A = sys_full.csr()
+    x, iters, _ = op.pcg(A, sys_full.b, cpu.oa.jacobi_inverse(cpu.oa.matrix_diagonal(sys_full)), tol=1e-8)
+    vals, totals = [], []
+    desc = ""
+    for i in range(args.warmup + args.steps):
+        v, t, desc = cpu.sample(cpu.fields[0], iters, system=sys_full)
+        if i >= args.warmup:
+            vals.append(v)
+            totals.append(t)
+    value = cpu.ndof / float(np.mean(totals))
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(totals)) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded jittered Kuhn cube, lognormal P0 k)",
+        "config": {"workload": workload_desc(args.n, 1, len(cpu.tets), cpu.ndof, cpu.indices.size),
+                   "iterations": iters, "parallelism": "cpu, 1 thread"},
+        "cpu_baseline": {"value": value, "unit": "DOF/s", "cores": 1, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": "DOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "jNO (JAX) cannot be imported on this image; the oracle port stands in for its CPU path",
+    }
+    print(json.dumps(out), flush=True)
+
+
+# ------------------------------------------------------------------------------------------ ours
+def roofline_traffic():
+    """DRAM bytes per SpMV launch from the committed ncu summary, if one exists."""
+    path = os.path.join(ROOT, "profiles", "csr_spmv_p1_128.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    import jno_b200 as jno
+    from jno_b200 import _lib
+    from jno_b200.plan import FemPlan
+
+    lib = _lib.load()
+    pts, tets = make_mesh(args.n)
+    t0 = time.perf_counter()
+    plan = FemPlan(pts, tets, args.order)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    T, ndof, nnz = plan.ntet, plan.n, plan.nnz
+    fields_h = logk_fields(T)
+    fields = [torch.as_tensor(f, device=dev) for f in fields_h]
+    vals = torch.empty(nnz, dtype=torch.float64, device=dev)
+    b = torch.empty(ndof, dtype=torch.float64, device=dev)
+    inv = torch.empty(ndof, dtype=torch.float64, device=dev)
+    x = torch.empty(ndof, dtype=torch.float64, device=dev)
+    iters_seen = []
+    rel_seen = []
+    phase = {"asm": [], "solve": []}
+
+    def step(i, record=False):
+        lk = fields[(i + rank) % N_FIELDS]
+        if record:
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record()
+        plan.assemble(lk, vals=vals, b=b)
+        plan.jacobi(vals, out=inv)
+        if record:
+            e1.record()
+        x.zero_()
+        _, it, rel, st = plan.pcg(vals, b, x, inv, tol=1e-8)
+        if record:
+            e2.record()
+            phase["pending"] = (e0, e1, e2)
+        iters_seen.append(it)
+        rel_seen.append(rel)
+        if st != 0 or rel > 1e-4:
+            raise RuntimeError(f"solve failed: status {st}, relres {rel}")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, steps, warmup):
+        for i in range(warmup):
+            fn(i)
+        barrier()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for i in range(steps):
+            fn(warmup + i)
+        end.record()
+        barrier()
+        ms = start.elapsed_time(end)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = t.item()
+        return ms
+
+    # ---- headline: FP64 CSR
+    for i in range(args.warmup):
+        step(i)
+    iters_seen.clear()
+    rel_seen.clear()
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = lib.femk_kernel_launches()
+    barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for i in range(args.steps):
+        step(args.warmup + i)
+    end.record()
+    barrier()
+    launches = lib.femk_kernel_launches() - launches0
+    clk = clocks.stop()
+    ms_total = start.elapsed_time(end)
+    if world > 1:
+        t = torch.tensor([ms_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = t.item()
+    ms_step = ms_total / args.steps
+    value = world * ndof / (ms_step / 1e3)
+    iters_mean = float(np.mean(iters_seen))
+
+    # phase split (separate short run with events between phases)
+    asm_ms, solve_ms = [], []
+    for i in range(3):
+        step(i, record=True)
+        e0, e1, e2 = phase.pop("pending")
+        torch.cuda.synchronize()
+        asm_ms.append(e0.elapsed_time(e1))
+        solve_ms.append(e1.elapsed_time(e2))
+
+    # ---- dominant kernel: CSR SpMV (same kernel template as the CG step), CUDA events
+    xr = torch.randn(ndof, dtype=torch.float64, device=dev)
+    yr = torch.empty_like(xr)
+    for _ in range(5):
+        plan.spmv(vals, xr, yr)
+    torch.cuda.synchronize()
+    reps = 50
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(reps):
+        plan.spmv(vals, xr, yr)
+    s1.record()
+    torch.cuda.synchronize()
+    spmv_ms = s0.elapsed_time(s1) / reps
+    spmv_bytes = 12 * nnz + 20 * ndof + 4
+    peak = 6547.5
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak_src = "fallback"
+    if os.path.exists(peaks_path):
+        try:
+            peak = float(json.load(open(peaks_path))["hbm_gbs"])
+            peak_src = "measured"
+        except Exception:
+            pass
+    achieved = spmv_bytes / (spmv_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": roofline_traffic(), "kernel": "k_csr (FP64 CSR SpMV, 16 lanes/row)",
+                "bytes_per_launch": spmv_bytes, "ms_per_launch": spmv_ms, "peak_source": peak_src}
+
+    variants = {}
+    if not args.no_variants:
+        # FP64 tight reference solution for error reporting
+        plan.assemble(fields[0], vals=vals, b=b)
+        plan.jacobi(vals, out=inv)
+        x_ref = torch.zeros_like(x)
+        plan.pcg(vals, b, x_ref, inv, tol=1e-12, relres=False)
+        ref_norm = torch.linalg.norm(x_ref).item()
+        # mixed precision, reliable updates
+        mixed_info = {}
+
+        def mstep(i):
+            lk = fields[i % N_FIELDS]
+            plan.assemble(lk, vals=vals, b=b)
+            plan.jacobi(vals, out=inv)
+            x.zero_()
+            _, inner, outer, rel, st = plan.pcg_mixed(vals, b, inv, x, tol=1e-8)
+            mixed_info.setdefault("inner", []).append(inner)
+            mixed_info.setdefault("outer", []).append(outer)
+            mixed_info.setdefault("rel", []).append(rel)
+
+        vsteps = min(args.steps, N_FIELDS)
+        ms = timed(mstep, vsteps, 2) / vsteps
+        mstep(N_FIELDS * 10)  # field 0 again for the error check
+        err = (torch.linalg.norm(x - x_ref).item() / ref_norm)
+        variants["mixed_fp32_fp64_reliable"] = {
+            "value": world * ndof / (ms / 1e3), "unit": "DOF/s", "ms_per_step": ms,
+            "speedup_vs_fp64": ms_step / ms, "inner_iters": float(np.mean(mixed_info["inner"])),
+            "fp64_updates": float(np.mean(mixed_info["outer"])), "max_relres": float(np.max(mixed_info["rel"])),
+            "err_vs_fp64_tight": err}
+        # matrix-free FP64
+        mf_info = {}
+
+        def fstep(i):
+            lk = fields[i % N_FIELDS]
+            plan.assemble(lk, vals=None, b=b)
+            plan.jacobi_matfree(lk, out=inv)
+            x.zero_()
+            _, it, rel, st = plan.pcg_matfree(lk, b, x, inv, tol=1e-8)
+            mf_info.setdefault("it", []).append(it)
+
+        fsteps = min(args.steps, 5)
+        ms_f = timed(fstep, fsteps, 1) / fsteps
+        variants["matrix_free_fp64"] = {"value": world * ndof / (ms_f / 1e3), "unit": "DOF/s", "ms_per_step": ms_f,
+                                        "iters": float(np.mean(mf_info["it"]))}
+        variants["spmv_csr_fp64"] = {"GB/s": achieved, "frac_of_peak": achieved / peak, "ms": spmv_ms}
+
+    # ---- end to end through the public API with host buffers
+    d = jno.domain.from_mesh(pts, tets)
+    u, v = d.fem_symbols(order=args.order)
+    _r, s = d.fem_symbols(space="P0", names=("r", "s"))
+    xi, yi, zi = d.variable("interior")
+    xb, yb, zb = d.variable("boundary")
+    ui, vi = u.bind(x=xi, y=yi, z=zi), v.bind(x=xi, y=yi, z=zi)
+    logk_sym = jno.np.parameter(s, name="logk")
+    fem = jno.fem([jno.np.exp(logk_sym) * (ui.x * vi.x + ui.y * vi.y + ui.z * vi.z) - 1.0 * vi, u(xb, yb, zb) - 0.0])
+    system = fem.operator
+    solver = jno.solve.cg(tol=1e-8)
+    host_fields = [torch.as_tensor(f).pin_memory() for f in fields_h]
+    out_host = torch.empty(ndof, dtype=torch.float64).pin_memory()
+
+    def estep(i):
+        lk = host_fields[(i + rank) % N_FIELDS].to(dev, non_blocking=True)
+        A, bb = system.evaluate({"logk": lk})
+        xs = solver(A, bb, M=jno.precond.jacobi())
+        out_host.copy_(xs, non_blocking=True)
+
+    esteps = min(args.steps, N_FIELDS)
+    ms_e = timed(estep, esteps, 2) / esteps
+    e2e = {"value": world * ndof / (ms_e / 1e3), "unit": "DOF/s", "h2d_bytes_per_step": 8 * T,
+           "d2h_bytes_per_step": 8 * ndof, "ms_per_step": ms_e,
+           "path": "jno_b200.fem(...).operator.evaluate({'logk'}) + jno_b200.solve.cg(tol=1e-8)(A, b, M=jacobi())"}
+
+    cpu_baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = CpuOracle(args.n)
+        v_cpu, t_cpu, desc = cpu.sample(fields_h[0], int(round(iters_mean)))
+        cpu_baseline = {"value": v_cpu, "unit": "DOF/s", "cores": 1, "kind": "port", "sample": desc,
+                        "host_cpus": os.cpu_count()}
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded jittered Kuhn cube, lognormal P0 k)",
+            "config": {"workload": workload_desc(args.n, args.order, T, ndof, nnz), "order": args.order,
+                       "n_hex_side": args.n, "ntet": T, "dofs": ndof, "nnz": nnz, "tol": 1e-8,
+                       "iterations_mean": iters_mean, "max_relres": float(np.max(rel_seen)),
+                       "assemble_ms": float(np.mean(asm_ms)), "solve_ms": float(np.mean(solve_ms)),
+                       "plan_setup_s": setup_s,
+                       "l2": "inputs larger than L2 (381 MB CSR stream per SpMV vs 126 MB L2)",
+                       "parallelism": f"replicas x{world} (independent problems per GPU, no collective)"},
+            "variants": variants, "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clk,
+        }
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

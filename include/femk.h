@@ -1,0 +1,174 @@
+/*
+ * femk.h -- C ABI of the B200 (sm_100a) P1/P2 tetrahedral FEM assembly + Jacobi-PCG kernels.
+ *
+ * This is the drop-in boundary for jNO's hot path: parametric element assembly of
+ * -div(k grad u) = f on Lagrange P1/P2 tetrahedra into the compress-plan CSR pattern, the Jacobi
+ * preconditioner, and jax-cg-semantics preconditioned CG. Every entry point takes plain pointers
+ * and sizes, returns an int status (FEMK_OK == 0) and never throws; the message of the last
+ * failure on the calling thread is femk_last_error_string().
+ *
+ * Memory: arrays named *_dev are caller-owned DEVICE pointers on the plan's device; arrays named
+ * *_host are host pointers. A plan owns its pattern arrays and its solver workspace and is
+ * released with femk_plan_destroy. `stream` is a cudaStream_t passed as void* (NULL = default).
+ * One plan may be used by one stream at a time.
+ */
+#ifndef FEMK_H
+#define FEMK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FEMK_OK 0
+#define FEMK_EINVAL 1        /* bad argument (null pointer, size, out-of-range index) */
+#define FEMK_ECUDA 2         /* a CUDA runtime call failed */
+#define FEMK_ENOMEM 3        /* device allocation failed */
+#define FEMK_NOT_CONVERGED 4 /* iteration cap reached above tolerance (solution still written) */
+#define FEMK_NONFINITE 5     /* NaN/Inf met in a reduction */
+#define FEMK_TIMEOUT 6       /* a bounded device-side wait gave up */
+#define FEMK_EBOUNDS 7       /* an index check inside a kernel failed */
+#define FEMK_BREAKDOWN 8     /* <p, A p> <= 0: operator not SPD */
+
+/* coefficient modes for femk_assemble: k_e = coef_scale * g(param_e) */
+#define FEMK_COEF_EXP 0      /* g = exp  : jno.np.exp(logk) * ...  (P0 log-conductivity) */
+#define FEMK_COEF_LINEAR 1   /* g = id   : rho * ...               (P0 linear parameter) */
+#define FEMK_COEF_CONST 2    /* g = 1    : param ignored (may be NULL) */
+
+/* precision modes for femk_pcg_mixed */
+#define FEMK_MIXED_RELIABLE 0 /* FP32 inner CG with FP64 reliable updates (no restart) */
+#define FEMK_MIXED_RESTART 1  /* classic iterative refinement: restart FP32 CG per outer step */
+
+typedef struct femk_plan femk_plan;
+
+typedef struct femk_plan_info {
+  int32_t order;      /* 1 or 2 */
+  int32_t ndof_local; /* 4 or 10 */
+  int64_t ntet;       /* elements */
+  int64_t nvert;      /* P1 vertices */
+  int64_t n;          /* DOFs (rows) */
+  int64_t nnz;        /* stored entries of the canonical CSR (= compress-plan nse) */
+  int64_t n_dirichlet;
+  int32_t cols16;     /* 1 when every column fits an int16 offset from its row (compact inner format) */
+  int32_t device;
+} femk_plan_info;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int femk_version(void);
+
+/* Number of CUDA kernels this library has launched in this process (all devices, all threads). */
+int64_t femk_kernel_launches(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* femk_last_error_string(void);
+
+/*
+ * Build the assembly plan on the current device.
+ *   xyz_dev   f64[nvert*3]  P1 vertex coordinates (x, y, z per vertex)
+ *   tets_dev  i32[ntet*4]   P1 connectivity
+ *   order     1 or 2        (P2 adds edge-midpoint DOFs numbered in first-encounter order)
+ *   dirichlet_mask_dev  u8[n] or NULL: NULL = every node on a boundary facet (a facet owned by
+ *             exactly one tet). For order 2 the DOF count n is only known after the build, so a
+ *             P2 mask must come from a previous plan's export of the same mesh.
+ * Replaces: jno/utils/solver/fem_native.py:218-288 (_get_mesh), fem_utils.py:1979-2044
+ * (_promote_to_degree), fem_native.py:2264-2298 + fem_utils.py:4009-4057 (pattern hoist +
+ * compress_plan), fem_native.py:2563-2636 (_boundary_node_ids) / jno/_fem.py:2695.
+ */
+int femk_plan_create(const double* xyz_dev, int64_t nvert, const int32_t* tets_dev, int64_t ntet,
+                     int order, const uint8_t* dirichlet_mask_dev, void* stream, femk_plan** out);
+
+int femk_plan_destroy(femk_plan* plan);
+
+int femk_plan_get_info(const femk_plan* plan, femk_plan_info* out);
+
+/*
+ * Copy plan arrays into caller buffers (device pointers; each may be NULL to skip):
+ *   indptr i32[n+1], indices i32[nnz]  canonical CSR (compress_plan(...)[0], fem_utils.py:4049-4053)
+ *   slot   i32[ntet*nd*nd]             element -> CSR slot in (c, a, b) order (compress_plan inverse)
+ *   cells  i32[ntet*nd]                global DOF per (cell, local dof) (fem_native.py:908-913)
+ *   points f64[n*3]                    DOF coordinates (P2 midpoints = 0.5*xa + 0.5*xb)
+ *   dirichlet_mask u8[n], diag_slot i32[n]
+ */
+int femk_plan_export(const femk_plan* plan, int32_t* indptr_dev, int32_t* indices_dev,
+                     int32_t* slot_dev, int32_t* cells_dev, double* points_dev,
+                     uint8_t* dirichlet_mask_dev, int32_t* diag_slot_dev, void* stream);
+
+/*
+ * Parametric assembly of  k_e * grad u . grad v - f v  with symmetric Dirichlet u = g.
+ *   param_dev f64[ntet] (per-element P0 value, see FEMK_COEF_*), coef_scale multiplies k_e,
+ *   f       constant source, g_dev f64[n] Dirichlet values or NULL (= 0),
+ *   vals_dev f64[nnz] (canonical CSR values, explicit zeros kept) or NULL to assemble the load only
+ *   (matrix-free use), b_dev f64[n].
+ * Dirichlet rows/columns are zero, the diagonal 1, b[d] = g[d], and b -= A e carries g into the
+ * free rows. Replaces: FemLinearSystem.evaluate (jno/trace/__init__.py:3612-3615) ->
+ * _assemble_at (jno/utils/solver/fem_native.py:3311-3316): jacobian + residual + segment_sum +
+ * _apply_dirichlet_symmetric (fem_1d.py:667-686).
+ */
+int femk_assemble(const femk_plan* plan, const double* param_dev, int coef_mode, double coef_scale,
+                  double f, const double* g_dev, double* vals_dev, double* b_dev, void* stream);
+
+/* Unit-coefficient element matrices K_hat f64[ntet*nd*nd] and loads F_hat f64[ntet*nd]
+ * (either may be NULL). Replaces the per-cell jacfwd of fem_native.py:2333-2334 for k = 1. */
+int femk_element_matrices(const femk_plan* plan, double* khat_dev, double* fhat_dev, void* stream);
+
+/* inv_diag[i] = 1 / where(|A_ii| > 1e-30, A_ii, 1).
+ * Replaces matrix_diagonal (jno/utils/solver/linear.py:88-94) + _Jacobi.materialize (jno/precond.py:106-111). */
+int femk_jacobi(const femk_plan* plan, const double* vals_dev, double* inv_diag_dev, void* stream);
+
+/* Jacobi inverse diagonal of the matrix-free operator (same values as femk_jacobi on the
+ * assembled matrix, summed per element instead of read from the CSR diagonal slot). */
+int femk_jacobi_matfree(const femk_plan* plan, const double* param_dev, int coef_mode, double coef_scale,
+                        double* inv_diag_dev, void* stream);
+
+/* y = A x with the canonical CSR (FP64). Replaces LinearOperator.mv (solver_api.py:137-148). */
+int femk_spmv(const femk_plan* plan, const double* vals_dev, const double* x_dev, double* y_dev,
+              void* stream);
+
+/* y = A x without an assembled matrix: per-element K_e x_e from coordinates and k_e. */
+int femk_spmv_matfree(const femk_plan* plan, const double* param_dev, int coef_mode,
+                      double coef_scale, const double* x_dev, double* y_dev, void* stream);
+
+/*
+ * Jacobi-preconditioned CG with jax.scipy.sparse.linalg.cg semantics (jNO: jno.solve.cg,
+ * jno/solve.py:191-206). x_dev holds x0 on entry (zeros for jax's default) and the solution on
+ * exit. inv_diag_dev may be NULL (no preconditioner). Stops when <r, r> <= max(tol^2 <b,b>, atol^2)
+ * (<r, z> without a preconditioner) or after maxiter iterations. iters_out / relres_out may be
+ * NULL; relres is ||b - A x|| / (||b|| + 1e-30) of the returned x (the eager guard of
+ * solver_api.py:224-240). matfree_param_dev != NULL selects the matrix-free operator (vals_dev
+ * is then ignored and may be NULL; inv_diag_dev must come from an assembled diagonal).
+ */
+int femk_pcg(const femk_plan* plan, const double* vals_dev, const double* b_dev, double* x_dev,
+             const double* inv_diag_dev, double tol, double atol, int32_t maxiter, int32_t* iters_out,
+             double* relres_out, void* stream);
+
+int femk_pcg_matfree(const femk_plan* plan, const double* param_dev, int coef_mode, double coef_scale,
+                     const double* b_dev, double* x_dev, const double* inv_diag_dev, double tol,
+                     double atol, int32_t maxiter, int32_t* iters_out, double* relres_out, void* stream);
+
+/*
+ * Mixed precision: inner CG on FP32 values and vectors, FP64 outer residual b - A x with the FP64
+ * values and an FP64 solution. Converges to the same stopping rule as femk_pcg (on the true FP64
+ * residual). mode = FEMK_MIXED_*. inner_iters_out counts FP32 iterations, outer_out FP64
+ * residual evaluations. No reference counterpart (jNO runs x64 throughout).
+ */
+int femk_pcg_mixed(const femk_plan* plan, const double* vals_dev, const double* b_dev, double* x_dev,
+                   const double* inv_diag_dev, double tol, double atol, int32_t maxiter, int mode,
+                   int32_t* inner_iters_out, int32_t* outer_out, double* relres_out, void* stream);
+
+/*
+ * Adjoint contraction: grad[c] = -k_c * (m o lam)_e^T K_hat_e (m o u)_e, m = 1 - dirichlet mask,
+ * k_c = coef_scale * exp(param_c) (FEMK_COEF_EXP) or coef_scale (FEMK_COEF_LINEAR: d/dparam).
+ * Replaces jax.grad through custom_linear_solve + segment_sum + jacfwd (no jNO function).
+ */
+int femk_adjoint_grad(const femk_plan* plan, const double* param_dev, int coef_mode, double coef_scale,
+                      const double* u_dev, const double* lam_dev, double* grad_dev, void* stream);
+
+/* Lumped mass m_i = sum over elements of integral(phi_i) (= the unit-source load before Dirichlet). */
+int femk_lumped_mass(const femk_plan* plan, double* mass_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FEMK_H */

@@ -1,0 +1,202 @@
+// Fused parametric assembly: element geometry -> local stiffness -> scatter-add through the
+// element -> CSR slot map -> symmetric Dirichlet elimination -> RHS, in one pass over elements.
+//
+// Replaces FemLinearSystem.evaluate (jno/trace/__init__.py:3612-3615) -> _assemble_at
+// (jno/utils/solver/fem_native.py:3311-3316): per-cell jacfwd (fem_native.py:2333-2334) +
+// segment_sum through the compress plan (fem_native.py:2318-2329) + _apply_dirichlet_symmetric
+// (jno/utils/solver/fem_1d.py:667-686) + the residual's -1*v load (fem_native.py:2137-2181).
+//
+// Dirichlet semantics of the parametric route: entries in a Dirichlet row or column are stored as
+// explicit zeros (they are never added), the diagonal slot of a Dirichlet row holds exactly 1
+// (masked 0 + the appended unit triplet), b[d] = g[d], and free rows receive b -= A e.
+#include "femk_element.cuh"
+#include "femk_internal.cuh"
+
+namespace femk {
+namespace {
+
+constexpr int kThreads = 128;
+
+template <int ND>
+__global__ void __launch_bounds__(kThreads) k_assemble(const double* __restrict__ xyz, const int32_t* __restrict__ cells,
+                                                       int64_t ntet, const int32_t* __restrict__ slot,
+                                                       const uint8_t* __restrict__ dmask, const double* __restrict__ param,
+                                                       int mode, double scale, double f, const double* __restrict__ g,
+                                                       double* __restrict__ vals, double* __restrict__ b) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t dof[ND];
+#pragma unroll
+    for (int a = 0; a < ND; ++a) dof[a] = __ldg(cells + c * ND + a);
+    TetGeom T;
+    tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
+    double VG[4][4];
+    gram(T, VG);
+    const double k = coef_of(param, mode, scale, c);
+    bool dir[ND];
+#pragma unroll
+    for (int a = 0; a < ND; ++a) dir[a] = __ldg(dmask + dof[a]) != 0;
+    const int32_t* srow = slot + c * ND * ND;
+#pragma unroll
+    for (int a = 0; a < ND; ++a) {
+      if (dir[a]) continue;
+      double rhs = f * fhat<ND>(T.vol, a);
+#pragma unroll
+      for (int bb = 0; bb < ND; ++bb) {
+        const double kab = k * khat<ND>(VG, a, bb);
+        if (dir[bb]) {
+          if (g) rhs -= kab * __ldg(g + dof[bb]);
+        } else if (vals) {
+          atomicAdd(vals + __ldg(srow + a * ND + bb), kab);
+        }
+      }
+      atomicAdd(b + dof[a], rhs);
+    }
+  }
+}
+
+__global__ void k_dirichlet_rows(const int32_t* __restrict__ dlist, int64_t nd, const int32_t* __restrict__ diag,
+                                 const double* __restrict__ g, double* __restrict__ vals, double* __restrict__ b) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nd; t += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t d = dlist[t];
+    if (vals) vals[diag[d]] = 1.0;
+    b[d] = g ? g[d] : 0.0;
+  }
+}
+
+template <int ND>
+__global__ void k_element_matrices(const double* __restrict__ xyz, const int32_t* __restrict__ cells, int64_t ntet,
+                                   double* __restrict__ khat_out, double* __restrict__ fhat_out) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
+    TetGeom T;
+    tet_geometry(xyz, cells[c * ND], cells[c * ND + 1], cells[c * ND + 2], cells[c * ND + 3], T);
+    double VG[4][4];
+    gram(T, VG);
+    if (khat_out) {
+#pragma unroll
+      for (int a = 0; a < ND; ++a)
+#pragma unroll
+        for (int bb = 0; bb < ND; ++bb) khat_out[(c * ND + a) * ND + bb] = khat<ND>(VG, a, bb);
+    }
+    if (fhat_out) {
+#pragma unroll
+      for (int a = 0; a < ND; ++a) fhat_out[c * ND + a] = fhat<ND>(T.vol, a);
+    }
+  }
+}
+
+// Lumped mass: m_i = sum_e integral(phi_i) over every element (no Dirichlet masking).
+template <int ND>
+__global__ void k_lumped_mass(const double* __restrict__ xyz, const int32_t* __restrict__ cells, int64_t ntet,
+                              double* __restrict__ m) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t dof[ND];
+#pragma unroll
+    for (int a = 0; a < ND; ++a) dof[a] = cells[c * ND + a];
+    TetGeom T;
+    tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
+#pragma unroll
+    for (int a = 0; a < ND; ++a) atomicAdd(m + dof[a], fhat<ND>(T.vol, a));
+  }
+}
+
+// grad[c] = -k'_c (m o lam)_e^T K_hat_e (m o u)_e ; k'_c = dk/dparam_c
+template <int ND>
+__global__ void k_adjoint(const double* __restrict__ xyz, const int32_t* __restrict__ cells, int64_t ntet,
+                          const uint8_t* __restrict__ dmask, const double* __restrict__ param, int mode, double scale,
+                          const double* __restrict__ u, const double* __restrict__ lam, double* __restrict__ grad) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t dof[ND];
+    double ue[ND], le[ND];
+#pragma unroll
+    for (int a = 0; a < ND; ++a) {
+      dof[a] = __ldg(cells + c * ND + a);
+      const bool d = __ldg(dmask + dof[a]) != 0;
+      ue[a] = d ? 0.0 : __ldg(u + dof[a]);
+      le[a] = d ? 0.0 : __ldg(lam + dof[a]);
+    }
+    TetGeom T;
+    tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
+    double VG[4][4];
+    gram(T, VG);
+    double acc = 0.0;
+#pragma unroll
+    for (int a = 0; a < ND; ++a) {
+      double row = 0.0;
+#pragma unroll
+      for (int bb = 0; bb < ND; ++bb) row += khat<ND>(VG, a, bb) * ue[bb];
+      acc += le[a] * row;
+    }
+    const double dk = mode == 0 ? scale * exp(__ldg(param + c)) : scale;
+    grad[c] = -dk * acc;
+  }
+}
+
+}  // namespace
+}  // namespace femk
+
+using namespace femk;
+
+extern "C" int femk_assemble(const femk_plan* p, const double* param, int mode, double scale, double f,
+                             const double* g, double* vals, double* b, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && b, "femk_assemble: NULL plan/b");
+  FEMK_CHECK_ARG(mode >= 0 && mode <= 2, "femk_assemble: unknown coef_mode");
+  FEMK_CHECK_ARG(mode == 2 || param, "femk_assemble: param is NULL");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (vals) FEMK_CUDA_TRY(cudaMemsetAsync(vals, 0, sizeof(double) * p->nnz, s));
+  FEMK_CUDA_TRY(cudaMemsetAsync(b, 0, sizeof(double) * p->n, s));
+  const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);
+  if (p->nd == 4)
+    k_assemble<4><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->slot, p->dmask, param, mode, scale, f, g, vals, b);
+  else
+    k_assemble<10><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->slot, p->dmask, param, mode, scale, f, g, vals, b);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  if (p->n_dir > 0) {
+    k_dirichlet_rows<<<::femk::counted_launch() + blocks_for(p->n_dir, 256, 65535), 256, 0, s>>>(p->dlist, p->n_dir, p->diag, g, vals, b);
+    FEMK_CUDA_TRY(cudaGetLastError());
+  }
+  return FEMK_OK;
+}
+
+extern "C" int femk_element_matrices(const femk_plan* p, double* khat_out, double* fhat_out, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p, "femk_element_matrices: NULL plan");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);
+  if (p->nd == 4)
+    k_element_matrices<4><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, khat_out, fhat_out);
+  else
+    k_element_matrices<10><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, khat_out, fhat_out);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}
+
+extern "C" int femk_lumped_mass(const femk_plan* p, double* mass, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && mass, "femk_lumped_mass: NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  FEMK_CUDA_TRY(cudaMemsetAsync(mass, 0, sizeof(double) * p->n, s));
+  const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);
+  if (p->nd == 4)
+    k_lumped_mass<4><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, mass);
+  else
+    k_lumped_mass<10><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, mass);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}
+
+extern "C" int femk_adjoint_grad(const femk_plan* p, const double* param, int mode, double scale, const double* u,
+                                 const double* lam, double* grad, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && u && lam && grad, "femk_adjoint_grad: NULL argument");
+  FEMK_CHECK_ARG(mode == 0 || mode == 1, "femk_adjoint_grad: coef_mode must be EXP or LINEAR");
+  FEMK_CHECK_ARG(mode == 1 || param, "femk_adjoint_grad: param is NULL");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);
+  if (p->nd == 4)
+    k_adjoint<4><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param, mode, scale, u, lam, grad);
+  else
+    k_adjoint<10><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param, mode, scale, u, lam, grad);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}

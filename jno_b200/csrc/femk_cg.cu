@@ -1,0 +1,612 @@
+// CSR / matrix-free SpMV and the Jacobi-PCG loop with jax.scipy.sparse.linalg.cg semantics.
+//
+// Per iteration three kernels run on the caller's stream, all steered by a device-resident
+// CgState (no host round trip per iteration):
+//   1. q = A p fused with <p, q>              -> alpha = gamma / <p, q>
+//   2. x += alpha p; r -= alpha q; z = D^-1 r fused with <r, z>, <r, r>  -> stop test, beta
+//   3. p = z + beta p
+// Dot products finish in the last block to arrive (fixed grid, fixed order: deterministic).
+// Once the stop test holds every later kernel returns at entry, so the host enqueues iterations
+// in chunks and only looks at the done flag of the previous chunk while the next one runs.
+//
+// Replaces jno.solve.cg (jno/solve.py:191-206) -> jax.scipy.sparse.linalg.cg (jax 0.10.1) with
+// M = jno.precond.jacobi() (jno/precond.py:106-111) and LinearOperator.mv (solver_api.py:137-148).
+#include <algorithm>
+#include <cmath>
+
+#include "femk_element.cuh"
+#include "femk_internal.cuh"
+
+namespace femk {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kChunk = 16;  // iterations enqueued between looks at the done flag
+
+// ---------------------------------------------------------------------------------------------
+// reductions: per-block partials + last-block finish
+// ---------------------------------------------------------------------------------------------
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* partials) {
+  __shared__ double red[NV][kThreads / 32];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) red[j][threadIdx.x >> 5] = v[j];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      double t = 0.0;
+      for (int w = 0; w < kThreads / 32; ++w) t += red[j][w];
+      partials[(int64_t)blockIdx.x * NV + j] = t;
+    }
+  }
+}
+
+// Returns true in every thread of the last block to finish; `out` then holds the grid totals.
+template <int NV>
+__device__ __forceinline__ bool grid_finish(double* partials, uint32_t* ticket, double (&out)[NV]) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t t = atomicAdd(ticket, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  double v[NV];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) v[j] = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += kThreads) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] += __ldcg(partials + (int64_t)b * NV + j);
+  }
+  __shared__ double red[NV][kThreads / 32];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) red[j][threadIdx.x >> 5] = v[j];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double t = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) t += red[j][w];
+    out[j] = t;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+  return true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// CSR row sum: L lanes per row, rows of a warp processed together (shuffles stay converged)
+// ---------------------------------------------------------------------------------------------
+template <int L>
+__device__ __forceinline__ double csr_row(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                                          const double* __restrict__ vals, const double* __restrict__ x, int64_t row,
+                                          bool valid, int sub) {
+  double s = 0.0;
+  if (valid) {
+    const int32_t beg = __ldg(indptr + row), end = __ldg(indptr + row + 1);
+    for (int32_t k = beg + sub; k < end; k += L) s += __ldcs(vals + k) * __ldg(x + __ldcs(indices + k));
+  }
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+enum SpmvMode { kPlain = 0, kCgStep = 1, kInit = 2, kResid = 3 };
+
+// One kernel for every CSR-SpMV use of the solver:
+//  kPlain : y = A x
+//  kCgStep: q = A p, <p, q>                     (finish: alpha)
+//  kInit  : r = b - A x, z = D^-1 r, p = z, <r,z>, <r,r>, <b,b>   (finish: gamma, rr, atol2, done)
+//  kResid : w = b - A x, <w,w>, <b,b>           (finish: stored in st->pq / st->bb)
+template <int L, int MODE>
+__global__ void __launch_bounds__(kThreads) k_csr(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                                                 const double* __restrict__ vals, int64_t n, const double* __restrict__ x,
+                                                 double* __restrict__ y, const double* __restrict__ b,
+                                                 const double* __restrict__ dinv, double* __restrict__ z,
+                                                 double* __restrict__ pout, double* __restrict__ partials, CgState* st,
+                                                 double tol2, double atol2) {
+  constexpr int NV = MODE == kPlain ? 1 : (MODE == kCgStep ? 1 : (MODE == kInit ? 3 : 2));
+  if (MODE == kCgStep && st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane % L;
+  const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
+  constexpr int RPW = 32 / L;  // rows per warp step
+  double acc[NV];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+  for (int64_t base = warp * RPW; base < n; base += nwarps * RPW) {
+    const int64_t row = base + lane / L;
+    const bool valid = row < n;
+    const double s = csr_row<L>(indptr, indices, vals, x, row, valid, sub);
+    if (valid && sub == 0) {
+      if (MODE == kPlain) {
+        y[row] = s;
+      } else if (MODE == kCgStep) {
+        y[row] = s;
+        acc[0] += __ldg(x + row) * s;
+      } else if (MODE == kInit) {
+        const double bi = b[row];
+        const double ri = bi - s;
+        const double zi = dinv ? dinv[row] * ri : ri;
+        y[row] = ri;
+        z[row] = zi;
+        pout[row] = zi;
+        acc[0] += ri * zi;
+        acc[1] += ri * ri;
+        acc[2] += bi * bi;
+      } else {
+        const double bi = b[row];
+        const double wi = bi - s;
+        acc[0] += wi * wi;
+        acc[1] += bi * bi;
+      }
+    }
+  }
+  if (MODE == kPlain) return;
+  block_reduce_store<NV>(acc, partials);
+  double tot[NV];
+  if (!grid_finish<NV>(partials, &st->ticket, tot)) return;
+  if (threadIdx.x != 0) return;
+  if (MODE == kCgStep) {
+    st->pq = tot[0];
+    st->alpha = st->gamma / tot[0];
+    if (!isfinite(tot[0])) {
+      st->status = FEMK_NONFINITE;
+      st->done = 1;
+    } else if (!(tot[0] > 0.0)) {
+      st->status = FEMK_BREAKDOWN;
+      st->done = 1;
+    }
+  } else if (MODE == kInit) {
+    st->gamma = tot[0];
+    st->rr = tot[1];
+    st->bb = tot[2];
+    st->atol2 = fmax(tol2 * tot[2], atol2);
+    st->iter = 0;
+    st->status = isfinite(tot[0]) && isfinite(tot[1]) ? FEMK_OK : FEMK_NONFINITE;
+    const double rs = st->precond ? tot[1] : tot[0];
+    st->done = (!(rs > st->atol2) || st->maxiter <= 0 || st->status != FEMK_OK) ? 1 : 0;
+    st->rr_since = tot[1];
+  } else {
+    st->pq = tot[0];
+    st->bb = tot[1];
+  }
+}
+
+// x += alpha p; r -= alpha q; z = D^-1 r; <r, z>, <r, r>; stop test; beta
+__global__ void __launch_bounds__(kThreads) k_update(int64_t n, double* __restrict__ x, double* __restrict__ r,
+                                                    double* __restrict__ z, const double* __restrict__ p,
+                                                    const double* __restrict__ q, const double* __restrict__ dinv,
+                                                    double* __restrict__ partials, CgState* st) {
+  if (st->done) return;
+  const double alpha = st->alpha;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+    const double pi = p[i];
+    x[i] = x[i] + alpha * pi;
+    const double ri = r[i] - alpha * q[i];
+    const double zi = dinv ? dinv[i] * ri : ri;
+    r[i] = ri;
+    z[i] = zi;
+    acc[0] += ri * zi;
+    acc[1] += ri * ri;
+  }
+  block_reduce_store<2>(acc, partials);
+  double tot[2];
+  if (!grid_finish<2>(partials, &st->ticket, tot)) return;
+  if (threadIdx.x != 0) return;
+  const double gamma_new = tot[0];
+  st->beta = gamma_new / st->gamma;
+  st->gamma = gamma_new;
+  st->rr = tot[1];
+  st->iter += 1;
+  const double rs = st->precond ? tot[1] : gamma_new;
+  if (!isfinite(gamma_new) || !isfinite(tot[1])) {
+    st->status = FEMK_NONFINITE;
+    st->done = 1;
+  } else if (!(rs > st->atol2) || st->iter >= st->maxiter) {
+    st->done = 1;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_pupdate(int64_t n, double* __restrict__ p, const double* __restrict__ z,
+                                                     const CgState* st) {
+  if (st->done) return;
+  const double beta = st->beta;
+  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads)
+    p[i] = z[i] + beta * p[i];
+}
+
+// ---------------------------------------------------------------------------------------------
+// matrix-free operator: y = A x, A the Dirichlet-eliminated stiffness, recomputed per element
+// ---------------------------------------------------------------------------------------------
+template <int ND>
+__global__ void __launch_bounds__(128) k_matfree(const double* __restrict__ xyz, const int32_t* __restrict__ cells,
+                                                 int64_t ntet, const uint8_t* __restrict__ dmask,
+                                                 const double* __restrict__ param, int mode, double scale,
+                                                 const double* __restrict__ x, double* __restrict__ y,
+                                                 const CgState* st) {
+  if (st && st->done) return;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t dof[ND];
+    double xe[ND];
+    bool dir[ND];
+#pragma unroll
+    for (int a = 0; a < ND; ++a) {
+      dof[a] = __ldg(cells + c * ND + a);
+      dir[a] = __ldg(dmask + dof[a]) != 0;
+      xe[a] = dir[a] ? 0.0 : __ldg(x + dof[a]);
+    }
+    TetGeom T;
+    tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
+    double VG[4][4];
+    gram(T, VG);
+    const double k = coef_of(param, mode, scale, c);
+#pragma unroll
+    for (int a = 0; a < ND; ++a) {
+      if (dir[a]) continue;
+      double s = 0.0;
+#pragma unroll
+      for (int b = 0; b < ND; ++b) s += khat<ND>(VG, a, b) * xe[b];
+      atomicAdd(y + dof[a], k * s);
+    }
+  }
+}
+
+__global__ void k_dirichlet_identity(const int32_t* __restrict__ dlist, int64_t nd, const double* __restrict__ x,
+                                     double* __restrict__ y, const CgState* st) {
+  if (st && st->done) return;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nd; t += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t d = dlist[t];
+    y[d] = x[d];
+  }
+}
+
+template <int ND>
+__global__ void k_matfree_diag(const double* __restrict__ xyz, const int32_t* __restrict__ cells, int64_t ntet,
+                               const uint8_t* __restrict__ dmask, const double* __restrict__ param, int mode,
+                               double scale, double* __restrict__ d) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t dof[ND];
+#pragma unroll
+    for (int a = 0; a < ND; ++a) dof[a] = __ldg(cells + c * ND + a);
+    TetGeom T;
+    tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
+    double VG[4][4];
+    gram(T, VG);
+    const double k = coef_of(param, mode, scale, c);
+#pragma unroll
+    for (int a = 0; a < ND; ++a)
+      if (!__ldg(dmask + dof[a])) atomicAdd(d + dof[a], k * khat<ND>(VG, a, a));
+  }
+}
+
+// The rest of a CG step for the matrix-free operator: <p, q> (q already holds A p)
+__global__ void __launch_bounds__(kThreads) k_dot_pq(int64_t n, const double* __restrict__ p, const double* __restrict__ q,
+                                                    double* __restrict__ partials, CgState* st) {
+  if (st->done) return;
+  double acc[1] = {0.0};
+  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads)
+    acc[0] += p[i] * q[i];
+  block_reduce_store<1>(acc, partials);
+  double tot[1];
+  if (!grid_finish<1>(partials, &st->ticket, tot)) return;
+  if (threadIdx.x != 0) return;
+  st->pq = tot[0];
+  st->alpha = st->gamma / tot[0];
+  if (!isfinite(tot[0])) {
+    st->status = FEMK_NONFINITE;
+    st->done = 1;
+  } else if (!(tot[0] > 0.0)) {
+    st->status = FEMK_BREAKDOWN;
+    st->done = 1;
+  }
+}
+
+// r = b - y (y = A x), z = D^-1 r, p = z and the init dots (matrix-free init)
+__global__ void __launch_bounds__(kThreads) k_init_from_ax(int64_t n, const double* __restrict__ b,
+                                                          const double* __restrict__ ax, const double* __restrict__ dinv,
+                                                          double* __restrict__ r, double* __restrict__ z,
+                                                          double* __restrict__ p, double* __restrict__ partials,
+                                                          CgState* st, double tol2, double atol2) {
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+    const double bi = b[i];
+    const double ri = bi - ax[i];
+    const double zi = dinv ? dinv[i] * ri : ri;
+    r[i] = ri;
+    z[i] = zi;
+    p[i] = zi;
+    acc[0] += ri * zi;
+    acc[1] += ri * ri;
+    acc[2] += bi * bi;
+  }
+  block_reduce_store<3>(acc, partials);
+  double tot[3];
+  if (!grid_finish<3>(partials, &st->ticket, tot)) return;
+  if (threadIdx.x != 0) return;
+  st->gamma = tot[0];
+  st->rr = tot[1];
+  st->bb = tot[2];
+  st->atol2 = fmax(tol2 * tot[2], atol2);
+  st->iter = 0;
+  st->status = isfinite(tot[0]) && isfinite(tot[1]) ? FEMK_OK : FEMK_NONFINITE;
+  const double rs = st->precond ? tot[1] : tot[0];
+  st->done = (!(rs > st->atol2) || st->maxiter <= 0 || st->status != FEMK_OK) ? 1 : 0;
+}
+
+__global__ void __launch_bounds__(kThreads) k_resid_from_ax(int64_t n, const double* __restrict__ b,
+                                                           const double* __restrict__ ax, double* __restrict__ partials,
+                                                           CgState* st) {
+  double acc[2] = {0.0, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+    const double bi = b[i];
+    const double w = bi - ax[i];
+    acc[0] += w * w;
+    acc[1] += bi * bi;
+  }
+  block_reduce_store<2>(acc, partials);
+  double tot[2];
+  if (!grid_finish<2>(partials, &st->ticket, tot)) return;
+  if (threadIdx.x != 0) return;
+  st->pq = tot[0];
+  st->bb = tot[1];
+}
+
+__global__ void k_jacobi(const int32_t* __restrict__ diag, const double* __restrict__ vals, int64_t n,
+                         double* __restrict__ inv) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double d = vals[diag[i]];
+    inv[i] = 1.0 / (fabs(d) > 1e-30 ? d : 1.0);
+  }
+}
+
+__global__ void k_invert_diag(double* __restrict__ d, int64_t n, const uint8_t* __restrict__ dmask) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double v = dmask[i] ? 1.0 : d[i];
+    d[i] = 1.0 / (fabs(v) > 1e-30 ? v : 1.0);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------------
+int lanes_for(const femk_plan* p) {
+  const double avg = p->n > 0 ? (double)p->nnz / (double)p->n : 1.0;
+  if (avg <= 5.0) return 4;
+  if (avg <= 10.0) return 8;
+  if (avg <= 20.0) return 16;
+  return 32;
+}
+
+int spmv_grid(const femk_plan* p) { return p->n_sm * (2048 / kThreads); }
+
+template <int MODE>
+int launch_csr(const femk_plan* p, const double* vals, const double* x, double* y, const double* b, const double* dinv,
+               double* z, double* pout, CgState* st, double tol2, double atol2, cudaStream_t s) {
+  const int grid = spmv_grid(p);
+  switch (lanes_for(p)) {
+    case 4:
+      k_csr<4, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+      break;
+    case 8:
+      k_csr<8, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+      break;
+    case 16:
+      k_csr<16, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+      break;
+    default:
+      k_csr<32, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+  }
+  FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}
+
+struct MatFree {
+  const double* param;
+  int mode;
+  double scale;
+};
+
+__global__ void k_zero(double* __restrict__ y, int64_t n, const CgState* st) {
+  if (st && st->done) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = 0.0;
+}
+
+// y = A x for the matrix-free operator; with st != NULL every launch is a no-op once st->done.
+int launch_matfree(const femk_plan* p, const MatFree& m, const double* x, double* y, cudaStream_t s,
+                   const CgState* st = nullptr) {
+  k_zero<<<::femk::counted_launch() + p->n_sm * 8, 256, 0, s>>>(y, p->n, st);
+  const int grid = blocks_for(p->ntet, 128, p->n_sm * 16);
+  if (p->nd == 4)
+    k_matfree<4><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, m.param, m.mode, m.scale, x, y, st);
+  else
+    k_matfree<10><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, m.param, m.mode, m.scale, x, y, st);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  if (p->n_dir > 0) {
+    k_dirichlet_identity<<<::femk::counted_launch() + blocks_for(p->n_dir, 256, 65535), 256, 0, s>>>(p->dlist, p->n_dir, x, y, st);
+    FEMK_CUDA_TRY(cudaGetLastError());
+  }
+  return FEMK_OK;
+}
+
+int pcg_run(const femk_plan* p, const double* vals, const MatFree* mf, const double* b, double* x, const double* dinv,
+            double tol, double atol, int32_t maxiter, int32_t* iters_out, double* relres_out, cudaStream_t s) {
+  FEMK_TRY(ensure_workspace(const_cast<femk_plan*>(p)));
+  const int64_t n = p->n;
+  double* r = p->work;
+  double* z = r + n;
+  double* pv = z + n;
+  double* q = pv + n;
+  CgState* st = p->state;
+  CgState init{};
+  init.maxiter = maxiter;
+  init.precond = dinv ? 1 : 0;
+  FEMK_CUDA_TRY(cudaMemcpyAsync(st, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
+  const double tol2 = tol * tol, atol2 = atol * atol;
+  const int vgrid = p->n_sm * (2048 / kThreads);
+  if (mf) {
+    FEMK_TRY(launch_matfree(p, *mf, x, q, s));
+    k_init_from_ax<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, b, q, dinv, r, z, pv, p->partials, st, tol2, atol2);
+  } else {
+    FEMK_TRY(launch_csr<kInit>(p, vals, x, r, b, dinv, z, pv, st, tol2, atol2, s));
+  }
+  FEMK_CUDA_TRY(cudaGetLastError());
+  cudaEvent_t ev[2];
+  FEMK_CUDA_TRY(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  FEMK_CUDA_TRY(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+  CgState* hs = p->state_host;
+  int status = FEMK_OK;
+  int64_t enq = 0;  // iterations enqueued
+  int chunk_id = 0;
+  bool have_prev = false;
+  while (true) {
+    // enqueue one chunk
+    const int64_t todo = std::min<int64_t>(kChunk, (int64_t)maxiter - enq);
+    for (int64_t it = 0; it < todo; ++it) {
+      if (mf) {
+        FEMK_TRY(launch_matfree(p, *mf, pv, q, s, st));
+        k_dot_pq<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, pv, q, p->partials, st);
+      } else {
+        FEMK_TRY(launch_csr<kCgStep>(p, vals, pv, q, nullptr, nullptr, nullptr, nullptr, st, 0.0, 0.0, s));
+      }
+      k_update<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, x, r, z, pv, q, dinv, p->partials, st);
+      k_pupdate<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, pv, z, st);
+    }
+    FEMK_CUDA_TRY(cudaGetLastError());
+    enq += todo;
+    CgState* slot_h = hs + (chunk_id & 1);
+    FEMK_CUDA_TRY(cudaMemcpyAsync(slot_h, st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+    FEMK_CUDA_TRY(cudaEventRecord(ev[chunk_id & 1], s));
+    // look at the previous chunk's flag while this one runs
+    if (have_prev) {
+      FEMK_CUDA_TRY(cudaEventSynchronize(ev[(chunk_id - 1) & 1]));
+      if (hs[(chunk_id - 1) & 1].done) break;
+    }
+    have_prev = true;
+    if (enq >= maxiter) break;
+    ++chunk_id;
+  }
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  CgState fin{};
+  FEMK_CUDA_TRY(cudaMemcpy(&fin, st, sizeof(CgState), cudaMemcpyDeviceToHost));
+  // the final chunk may have ended exactly at maxiter without the flag being observed: fin is exact
+  if (iters_out) *iters_out = fin.iter;
+  if (fin.status != FEMK_OK) status = fin.status;
+  if (relres_out) {
+    if (mf) {
+      FEMK_TRY(launch_matfree(p, *mf, x, q, s));
+      k_resid_from_ax<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, b, q, p->partials, st);
+    } else {
+      FEMK_TRY(launch_csr<kResid>(p, vals, x, nullptr, b, nullptr, nullptr, nullptr, st, 0.0, 0.0, s));
+    }
+    FEMK_CUDA_TRY(cudaMemcpyAsync(hs, st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+    FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+    *relres_out = std::sqrt(hs->pq) / (std::sqrt(hs->bb) + 1e-30);
+  }
+  if (status == FEMK_OK) {
+    const double rs = fin.precond ? fin.rr : fin.gamma;
+    if (rs > fin.atol2) {
+      set_error("femk_pcg: iteration cap reached above tolerance");
+      status = FEMK_NOT_CONVERGED;
+    }
+  } else if (status == FEMK_BREAKDOWN) {
+    set_error("femk_pcg: <p, A p> <= 0 (operator not symmetric positive definite)");
+  } else if (status == FEMK_NONFINITE) {
+    set_error("femk_pcg: non-finite value in a CG reduction");
+  }
+  return status;
+}
+
+}  // namespace
+
+int ensure_workspace(femk_plan* p) {
+  if (p->work) return FEMK_OK;
+  FEMK_CUDA_TRY(cudaMalloc(&p->work, sizeof(double) * 4 * (p->n + 1)));
+  FEMK_CUDA_TRY(cudaMalloc(&p->partials, sizeof(double) * 4 * (int64_t)p->n_sm * 64));
+  FEMK_CUDA_TRY(cudaMalloc(&p->state, sizeof(CgState)));
+  FEMK_CUDA_TRY(cudaMemset(p->state, 0, sizeof(CgState)));
+  FEMK_CUDA_TRY(cudaMallocHost(&p->state_host, 2 * sizeof(CgState)));
+  return FEMK_OK;
+}
+
+int spmv_csr(const femk_plan* p, const double* vals, const double* x, double* y, cudaStream_t s) {
+  return launch_csr<kPlain>(p, vals, x, y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.0, 0.0, s);
+}
+
+}  // namespace femk
+
+using namespace femk;
+
+extern "C" int femk_jacobi(const femk_plan* p, const double* vals, double* inv, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && vals && inv, "femk_jacobi: NULL argument");
+  k_jacobi<<<::femk::counted_launch() + blocks_for(p->n, 256, p->n_sm * 8), 256, 0, (cudaStream_t)stream>>>(p->diag, vals, p->n, inv);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}
+
+extern "C" int femk_spmv(const femk_plan* p, const double* vals, const double* x, double* y, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && vals && x && y, "femk_spmv: NULL argument");
+  return spmv_csr(p, vals, x, y, (cudaStream_t)stream);
+}
+
+extern "C" int femk_spmv_matfree(const femk_plan* p, const double* param, int mode, double scale, const double* x,
+                                 double* y, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && x && y, "femk_spmv_matfree: NULL argument");
+  FEMK_CHECK_ARG(mode >= 0 && mode <= 2 && (mode == 2 || param), "femk_spmv_matfree: bad coefficient");
+  MatFree m{param, mode, scale};
+  return launch_matfree(p, m, x, y, (cudaStream_t)stream);
+}
+
+extern "C" int femk_jacobi_matfree(const femk_plan* p, const double* param, int mode, double scale, double* inv,
+                                   void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && inv, "femk_jacobi_matfree: NULL argument");
+  FEMK_CHECK_ARG(mode >= 0 && mode <= 2 && (mode == 2 || param), "femk_jacobi_matfree: bad coefficient");
+  cudaStream_t s = (cudaStream_t)stream;
+  FEMK_CUDA_TRY(cudaMemsetAsync(inv, 0, sizeof(double) * p->n, s));
+  const int grid = blocks_for(p->ntet, 128, p->n_sm * 16);
+  if (p->nd == 4)
+    k_matfree_diag<4><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param, mode, scale, inv);
+  else
+    k_matfree_diag<10><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param, mode, scale, inv);
+  k_invert_diag<<<::femk::counted_launch() + blocks_for(p->n, 256, p->n_sm * 8), 256, 0, s>>>(inv, p->n, p->dmask);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}
+
+extern "C" int femk_pcg(const femk_plan* p, const double* vals, const double* b, double* x, const double* dinv,
+                        double tol, double atol, int32_t maxiter, int32_t* iters_out, double* relres_out,
+                        void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && vals && b && x, "femk_pcg: NULL argument");
+  FEMK_CHECK_ARG(tol >= 0.0 && atol >= 0.0, "femk_pcg: negative tolerance");
+  return pcg_run(p, vals, nullptr, b, x, dinv, tol, atol, maxiter, iters_out, relres_out, (cudaStream_t)stream);
+}
+
+extern "C" int femk_pcg_matfree(const femk_plan* p, const double* param, int mode, double scale, const double* b,
+                                double* x, const double* dinv, double tol, double atol, int32_t maxiter,
+                                int32_t* iters_out, double* relres_out, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && b && x, "femk_pcg_matfree: NULL argument");
+  FEMK_CHECK_ARG(mode >= 0 && mode <= 2 && (mode == 2 || param), "femk_pcg_matfree: bad coefficient");
+  MatFree m{param, mode, scale};
+  return pcg_run(p, nullptr, &m, b, x, dinv, tol, atol, maxiter, iters_out, relres_out, (cudaStream_t)stream);
+}

@@ -1,0 +1,124 @@
+// Internal declarations shared by the femk translation units (sm_100a only).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/femk.h"
+
+#define FEMK_VERSION 10000
+
+namespace femk {
+
+void set_error(const std::string& msg);
+void clear_error();
+
+// Every kernel launch of the library is written `k<<<counted_launch() + grid, ...>>>`: the call adds
+// one to a process-wide counter (read by femk_kernel_launches) and returns 0.
+int counted_launch();
+
+// Return FEMK_ECUDA with a message if a CUDA runtime call failed.
+#define FEMK_CUDA_TRY(expr)                                                              \
+  do {                                                                                   \
+    cudaError_t _e = (expr);                                                             \
+    if (_e != cudaSuccess) {                                                             \
+      ::femk::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));           \
+      return _e == cudaErrorMemoryAllocation ? FEMK_ENOMEM : FEMK_ECUDA;                \
+    }                                                                                    \
+  } while (0)
+
+#define FEMK_CHECK_ARG(cond, msg)           \
+  do {                                      \
+    if (!(cond)) {                          \
+      ::femk::set_error(msg);               \
+      return FEMK_EINVAL;                   \
+    }                                       \
+  } while (0)
+
+#define FEMK_TRY(expr)          \
+  do {                          \
+    int _s = (expr);            \
+    if (_s != FEMK_OK) return _s; \
+  } while (0)
+
+// Device-side solver scalars of one CG run. Lives in plan-owned device memory.
+struct CgState {
+  double gamma;     // <r, z>
+  double rr;        // <r, r>
+  double pq;        // <p, A p>
+  double alpha, beta;
+  double atol2;     // max(tol^2 <b, b>, atol^2)
+  double bb;        // <b, b>
+  int32_t iter;     // iterations taken
+  int32_t maxiter;
+  int32_t done;     // 1 once the stop test holds (or on failure)
+  int32_t status;   // FEMK_OK / FEMK_BREAKDOWN / FEMK_NONFINITE
+  uint32_t ticket;  // last-block-done counter of the reduction in flight
+  int32_t precond;  // 1 when inv_diag is used in the stop test (rs = <r, r>), 0: rs = gamma
+  // mixed precision bookkeeping
+  double rr_since;  // rr at the last reliable update
+  int32_t inner;    // FP32 iterations
+  int32_t outer;    // FP64 residual evaluations
+};
+
+}  // namespace femk
+
+struct femk_plan {
+  int device = 0;
+  int order = 1, nd = 4;
+  int64_t ntet = 0, nvert = 0, n = 0, nnz = 0, n_dir = 0;
+  // pattern (plan-owned device memory)
+  double* xyz = nullptr;        // f64[nvert*3] P1 vertex coordinates
+  double* points = nullptr;     // f64[n*3] DOF coordinates
+  int32_t* cells = nullptr;     // i32[ntet*nd]
+  int32_t* indptr = nullptr;    // i32[n+1]
+  int32_t* indices = nullptr;   // i32[nnz]
+  int32_t* slot = nullptr;      // i32[ntet*nd*nd]
+  int32_t* diag = nullptr;      // i32[n]
+  uint8_t* dmask = nullptr;     // u8[n]
+  int32_t* dlist = nullptr;     // i32[n_dir] ascending
+  int32_t* inc_ptr = nullptr;   // i32[n+1] DOF -> element incidence
+  int32_t* inc_elem = nullptr;  // i32[ntet*nd]
+  int16_t* cols16 = nullptr;    // i16[nnz] col - row, when every entry fits
+  int max_row = 0;              // longest CSR row
+  // solver workspace (allocated on first use)
+  double* work = nullptr;       // 4*n doubles: r, z, p, q
+  double* partials = nullptr;   // reduction partials
+  femk::CgState* state = nullptr;
+  femk::CgState* state_host = nullptr;  // pinned mirror
+  float* work32 = nullptr;      // FP32 inner vectors (mixed precision)
+  float* vals32 = nullptr;      // FP32 copy of the values (mixed precision)
+  double* work64b = nullptr;    // FP64 extra vectors for mixed precision (x_base, r64)
+  int n_sm = 148;
+};
+
+namespace femk {
+
+// grid-size helpers
+inline int blocks_for(int64_t n, int threads, int cap = 1 << 30) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (int)b;
+}
+
+// Exclusive scan of int64 values: out[0..n] with out[n] = total. Works in place only when
+// in != out is false-safe (it is not: pass distinct buffers).
+int scan_exclusive_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
+
+int ensure_workspace(femk_plan* p);
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace femk

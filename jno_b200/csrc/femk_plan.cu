@@ -1,0 +1,552 @@
+// Plan build on the device: P2 numbering, DOF -> element incidence, the compress-plan CSR
+// pattern, the element -> slot map, diagonal slots and the boundary-facet Dirichlet set.
+//
+// Reference behaviour reproduced (pinned by the oracle tests):
+//  * P2 DOFs: vertices keep ids 0..nv-1, edge midpoints are numbered in first-encounter order over
+//    (cell, local dof), local edge order (2,3),(1,3),(1,2),(0,3),(0,2),(0,1)
+//    (jno/utils/solver/fem_utils.py:1979-2044, jno/utils/solver/fem_topology.py:44).
+//  * Pattern: the unique (row, col) pairs of all element dofs, rows ascending, columns ascending
+//    within a row (compress_plan, fem_utils.py:4049-4057); slot[c, a, b] is the plan's inverse.
+//  * Dirichlet: every node on a facet owned by exactly one tet (jno/_fem.py:2695).
+//
+// Everything here is integer work: one thread (or warp) per element/row, no sorting library.
+#include <climits>
+
+#include "femk_internal.cuh"
+
+namespace femk {
+namespace {
+
+__constant__ int c_edge[6][2] = {{2, 3}, {1, 3}, {1, 2}, {0, 3}, {0, 2}, {0, 1}};
+__constant__ int c_face[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+// local edge index of the vertex pair (i, j); -1 on the diagonal
+__constant__ int c_edge_of[4][4] = {{-1, 5, 4, 3}, {5, -1, 2, 1}, {4, 2, -1, 0}, {3, 1, 0, -1}};
+
+constexpr int kThreads = 256;
+
+__global__ void k_count(const int32_t* __restrict__ cells, int64_t m, int64_t n,
+                        unsigned long long* __restrict__ cnt, int* __restrict__ err) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = cells[t];
+    if (v < 0 || v >= n) {
+      atomicOr(err, 1);
+      continue;
+    }
+    atomicAdd(&cnt[v], 1ull);
+  }
+}
+
+__global__ void k_to_i32(const int64_t* __restrict__ in, int64_t n, int32_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (int32_t)in[i];
+}
+
+template <int ND>
+__global__ void k_fill(const int32_t* __restrict__ cells, int64_t ntet, const int32_t* __restrict__ ptr,
+                       int32_t* __restrict__ cursor, int32_t* __restrict__ inc) {
+  const int64_t m = ntet * ND;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = cells[t];
+    const int32_t pos = atomicAdd(&cursor[v], 1);
+    inc[ptr[v] + pos] = (int32_t)(t / ND);
+  }
+}
+
+// Sort each incidence list ascending (lists are short: the element valence of a node).
+__global__ void k_sort_lists(const int32_t* __restrict__ ptr, int64_t n, int32_t* __restrict__ inc) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t b = ptr[v], e = ptr[v + 1];
+    for (int32_t i = b + 1; i < e; ++i) {
+      const int32_t key = inc[i];
+      int32_t j = i - 1;
+      while (j >= b && inc[j] > key) {
+        inc[j + 1] = inc[j];
+        --j;
+      }
+      inc[j + 1] = key;
+    }
+  }
+}
+
+// For every (cell, local edge): the raw index c'*6+e' of the first cell containing the same edge.
+__global__ void k_edge_first(const int32_t* __restrict__ tets, int64_t ntet, const int32_t* __restrict__ vptr,
+                             const int32_t* __restrict__ vinc, int32_t* __restrict__ first_raw,
+                             int64_t* __restrict__ is_first, int* __restrict__ err) {
+  const int64_t m = ntet * 6;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = r / 6;
+    const int e = (int)(r % 6);
+    const int32_t a = tets[c * 4 + c_edge[e][0]], b = tets[c * 4 + c_edge[e][1]];
+    const int32_t u = min(a, b), w = max(a, b);
+    int64_t found = -1;
+    for (int32_t j = vptr[u]; j < vptr[u + 1] && found < 0; ++j) {
+      const int32_t c2 = vinc[j];
+      int iu = -1, iw = -1;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int32_t t = tets[(int64_t)c2 * 4 + q];
+        if (t == u) iu = q;
+        if (t == w) iw = q;
+      }
+      if (iw >= 0 && iu >= 0) found = (int64_t)c2 * 6 + c_edge_of[iu][iw];
+    }
+    if (found < 0) {
+      atomicOr(err, 2);
+      found = r;
+    }
+    first_raw[r] = (int32_t)found;
+    is_first[r] = found == r ? 1 : 0;
+  }
+}
+
+__global__ void k_p2_cells(const int32_t* __restrict__ tets, int64_t ntet, int64_t nvert,
+                           const int32_t* __restrict__ first_raw, const int64_t* __restrict__ rank,
+                           const double* __restrict__ xyz, int32_t* __restrict__ cells, double* __restrict__ points) {
+  const int64_t m = ntet * 6;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = r / 6;
+    const int e = (int)(r % 6);
+    const int64_t fr = first_raw[r];
+    const int64_t id = nvert + rank[fr];
+    cells[c * 10 + 4 + e] = (int32_t)id;
+    if (e < 4) cells[c * 10 + e] = tets[c * 4 + e];
+    if (fr == r) {
+      const int32_t a = tets[c * 4 + c_edge[e][0]], b = tets[c * 4 + c_edge[e][1]];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) points[id * 3 + k] = 0.5 * xyz[(int64_t)a * 3 + k] + 0.5 * xyz[(int64_t)b * 3 + k];
+    }
+  }
+}
+
+__device__ __forceinline__ int warp_min_i32(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Row pattern by repeated warp-wide minimum extraction over the candidate dofs of a row's
+// incident elements: no sort, deterministic, each row's columns ascending.
+template <int ND>
+__global__ void k_row_pattern(const int32_t* __restrict__ cells, const int32_t* __restrict__ inc_ptr,
+                              const int32_t* __restrict__ inc, int64_t n, const int64_t* __restrict__ rowptr,
+                              int64_t* __restrict__ rowlen, int32_t* __restrict__ cols, int* __restrict__ max_len) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = warp; row < n; row += nwarps) {
+    const int32_t beg = inc_ptr[row];
+    const int32_t m = (inc_ptr[row + 1] - beg) * ND;
+    int prev = -1;
+    int32_t count = 0;
+    const int64_t out = cols ? rowptr[row] : 0;
+    while (true) {
+      int best = INT_MAX;
+      for (int32_t idx = lane; idx < m; idx += 32) {
+        const int32_t c = inc[beg + idx / ND];
+        const int v = cells[(int64_t)c * ND + idx % ND];
+        if (v > prev && v < best) best = v;
+      }
+      best = warp_min_i32(best);
+      if (best == INT_MAX) break;
+      if (cols && lane == 0) cols[out + count] = best;
+      ++count;
+      prev = best;
+    }
+    if (lane == 0) {
+      rowlen[row] = count;
+      atomicMax(max_len, count);
+    }
+  }
+}
+
+__device__ __forceinline__ int32_t find_col(const int32_t* __restrict__ cols, int32_t lo, int32_t hi, int32_t key) {
+  while (lo < hi) {
+    const int32_t mid = (lo + hi) >> 1;
+    if (cols[mid] < key)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+template <int ND>
+__global__ void k_slot_map(const int32_t* __restrict__ cells, int64_t ntet, const int32_t* __restrict__ indptr,
+                           const int32_t* __restrict__ indices, int32_t* __restrict__ slot, int* __restrict__ err) {
+  const int64_t m = ntet * ND;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = t / ND;
+    const int32_t row = cells[t];
+    const int32_t lo = indptr[row], hi = indptr[row + 1];
+#pragma unroll
+    for (int b = 0; b < ND; ++b) {
+      const int32_t col = cells[c * ND + b];
+      const int32_t pos = find_col(indices, lo, hi, col);
+      if (pos >= hi || indices[pos] != col) atomicOr(err, 4);
+      slot[t * ND + b] = pos;
+    }
+  }
+}
+
+__global__ void k_diag_slot(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices, int64_t n,
+                            int32_t* __restrict__ diag, int* __restrict__ err) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t lo = indptr[i], hi = indptr[i + 1];
+    const int32_t pos = find_col(indices, lo, hi, (int32_t)i);
+    if (pos >= hi || indices[pos] != i) atomicOr(err, 8);
+    diag[i] = pos;
+  }
+}
+
+// A facet is on the boundary when no other tet has all three of its vertices.
+template <int ND>
+__global__ void k_boundary(const int32_t* __restrict__ cells, int64_t ntet, const int32_t* __restrict__ vptr,
+                           const int32_t* __restrict__ vinc, uint8_t* __restrict__ mask) {
+  const int64_t m = ntet * 4;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = t / 4;
+    const int f = (int)(t % 4);
+    int32_t v0 = cells[c * ND + c_face[f][0]], v1 = cells[c * ND + c_face[f][1]], v2 = cells[c * ND + c_face[f][2]];
+    const int32_t lo = min(v0, min(v1, v2));
+    bool shared = false;
+    for (int32_t j = vptr[lo]; j < vptr[lo + 1] && !shared; ++j) {
+      const int32_t c2 = vinc[j];
+      if (c2 == c) continue;
+      int hit = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int32_t w = cells[(int64_t)c2 * ND + q];
+        hit += (w == v0) + (w == v1) + (w == v2);
+      }
+      shared = hit == 3;
+    }
+    if (shared) continue;
+    mask[v0] = 1;
+    mask[v1] = 1;
+    mask[v2] = 1;
+    if (ND == 10) {
+#pragma unroll
+      for (int e = 0; e < 6; ++e) {
+        const int a = c_edge[e][0], b = c_edge[e][1];
+        const bool ina = a == c_face[f][0] || a == c_face[f][1] || a == c_face[f][2];
+        const bool inb = b == c_face[f][0] || b == c_face[f][1] || b == c_face[f][2];
+        if (ina && inb) mask[cells[c * ND + 4 + e]] = 1;
+      }
+    }
+  }
+}
+
+__global__ void k_mask_to_i64(const uint8_t* __restrict__ mask, int64_t n, int64_t* __restrict__ flag) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    flag[i] = mask[i] ? 1 : 0;
+}
+
+__global__ void k_compact(const uint8_t* __restrict__ mask, const int64_t* __restrict__ pos, int64_t n,
+                          int32_t* __restrict__ list) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (mask[i]) list[pos[i]] = (int32_t)i;
+}
+
+__global__ void k_cols16(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices, int64_t n,
+                         int16_t* __restrict__ c16, int* __restrict__ bad) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    for (int32_t k = indptr[i]; k < indptr[i + 1]; ++k) {
+      const int64_t d = (int64_t)indices[k] - i;
+      if (d < -32768 || d > 32767) {
+        atomicOr(bad, 1);
+        c16[k] = 0;
+      } else {
+        c16[k] = (int16_t)d;
+      }
+    }
+  }
+}
+
+__global__ void k_copy_xyz(const double* __restrict__ xyz, int64_t m, double* __restrict__ a,
+                           double* __restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+    const double v = xyz[i];
+    a[i] = v;
+    if (b) b[i] = v;
+  }
+}
+
+template <typename T>
+int dev_alloc(T** p, int64_t count, cudaStream_t s) {
+  if (count <= 0) count = 1;
+  FEMK_CUDA_TRY(cudaMalloc((void**)p, sizeof(T) * count));
+  (void)s;
+  return FEMK_OK;
+}
+
+struct Temp {
+  void* p = nullptr;
+  ~Temp() {
+    if (p) cudaFree(p);
+  }
+};
+
+int read_err(int* d_err, cudaStream_t s, int* h) {
+  FEMK_CUDA_TRY(cudaMemcpyAsync(h, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  return FEMK_OK;
+}
+
+// incidence of `cells` (nd per element) over n dofs into plan-owned ptr/inc arrays
+template <int ND>
+int build_incidence(const int32_t* cells, int64_t ntet, int64_t n, int32_t** ptr_out, int32_t** inc_out,
+                    int* d_err, cudaStream_t s) {
+  Temp cnt, scan, cur;
+  FEMK_CUDA_TRY(cudaMalloc(&cnt.p, sizeof(int64_t) * (n + 1)));
+  FEMK_CUDA_TRY(cudaMalloc(&scan.p, sizeof(int64_t) * (n + 1)));
+  FEMK_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, sizeof(int64_t) * (n + 1), s));
+  const int64_t m = ntet * ND;
+  k_count<<<::femk::counted_launch() + blocks_for(m, kThreads, 65535 * 4), kThreads, 0, s>>>(cells, m, n, (unsigned long long*)cnt.p, d_err);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  FEMK_TRY(scan_exclusive_i64((const int64_t*)cnt.p, (int64_t*)scan.p, n, s));
+  FEMK_TRY(dev_alloc(ptr_out, n + 1, s));
+  FEMK_TRY(dev_alloc(inc_out, m, s));
+  k_to_i32<<<::femk::counted_launch() + blocks_for(n + 1, kThreads, 65535 * 4), kThreads, 0, s>>>((const int64_t*)scan.p, n + 1, *ptr_out);
+  FEMK_CUDA_TRY(cudaMalloc(&cur.p, sizeof(int32_t) * (n + 1)));
+  FEMK_CUDA_TRY(cudaMemsetAsync(cur.p, 0, sizeof(int32_t) * (n + 1), s));
+  k_fill<ND><<<::femk::counted_launch() + blocks_for(m, kThreads, 65535 * 4), kThreads, 0, s>>>(cells, ntet, *ptr_out, (int32_t*)cur.p, *inc_out);
+  k_sort_lists<<<::femk::counted_launch() + blocks_for(n, 128, 65535 * 4), 128, 0, s>>>(*ptr_out, n, *inc_out);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));  // temporaries are freed on return
+  return FEMK_OK;
+}
+
+template <int ND>
+int build_pattern(femk_plan* p, int* d_err, int* h_err, cudaStream_t s) {
+  const int64_t n = p->n;
+  Temp rowlen, rowptr, dmax;
+  FEMK_CUDA_TRY(cudaMalloc(&rowlen.p, sizeof(int64_t) * (n + 1)));
+  FEMK_CUDA_TRY(cudaMalloc(&rowptr.p, sizeof(int64_t) * (n + 1)));
+  FEMK_CUDA_TRY(cudaMalloc(&dmax.p, sizeof(int)));
+  FEMK_CUDA_TRY(cudaMemsetAsync(dmax.p, 0, sizeof(int), s));
+  const int warps_blocks = blocks_for(n * 32, kThreads, p->n_sm * 64);
+  k_row_pattern<ND><<<::femk::counted_launch() + warps_blocks, kThreads, 0, s>>>(p->cells, p->inc_ptr, p->inc_elem, n, nullptr,
+                                                      (int64_t*)rowlen.p, nullptr, (int*)dmax.p);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  FEMK_TRY(scan_exclusive_i64((const int64_t*)rowlen.p, (int64_t*)rowptr.p, n, s));
+  int64_t nnz = 0;
+  FEMK_CUDA_TRY(cudaMemcpyAsync(&nnz, (int64_t*)rowptr.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaMemcpyAsync(&p->max_row, dmax.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  if (nnz >= INT32_MAX) {
+    set_error("femk_plan_create: the CSR pattern has >= 2^31 entries; int32 indptr cannot hold it");
+    return FEMK_EINVAL;
+  }
+  p->nnz = nnz;
+  FEMK_TRY(dev_alloc(&p->indptr, n + 1, s));
+  FEMK_TRY(dev_alloc(&p->indices, nnz, s));
+  k_to_i32<<<::femk::counted_launch() + blocks_for(n + 1, kThreads, 65535 * 4), kThreads, 0, s>>>((const int64_t*)rowptr.p, n + 1, p->indptr);
+  k_row_pattern<ND><<<::femk::counted_launch() + warps_blocks, kThreads, 0, s>>>(p->cells, p->inc_ptr, p->inc_elem, n, (const int64_t*)rowptr.p,
+                                                      (int64_t*)rowlen.p, p->indices, (int*)dmax.p);
+  FEMK_TRY(dev_alloc(&p->slot, p->ntet * ND * ND, s));
+  k_slot_map<ND><<<::femk::counted_launch() + blocks_for(p->ntet * ND, kThreads, 65535 * 4), kThreads, 0, s>>>(p->cells, p->ntet, p->indptr,
+                                                                                    p->indices, p->slot, d_err);
+  FEMK_TRY(dev_alloc(&p->diag, n, s));
+  k_diag_slot<<<::femk::counted_launch() + blocks_for(n, kThreads, 65535 * 4), kThreads, 0, s>>>(p->indptr, p->indices, n, p->diag, d_err);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  FEMK_TRY(read_err(d_err, s, h_err));
+  if (*h_err) {
+    set_error("femk_plan_create: slot map or diagonal lookup failed (corrupt connectivity?)");
+    return FEMK_EBOUNDS;
+  }
+  // compact int16 column offsets for the FP32 inner solve
+  int* d_bad = nullptr;
+  FEMK_CUDA_TRY(cudaMalloc(&d_bad, sizeof(int)));
+  Temp bad;
+  bad.p = d_bad;
+  FEMK_CUDA_TRY(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
+  FEMK_TRY(dev_alloc(&p->cols16, nnz, s));
+  k_cols16<<<::femk::counted_launch() + blocks_for(n, kThreads, 65535 * 4), kThreads, 0, s>>>(p->indptr, p->indices, n, p->cols16, d_bad);
+  int hbad = 0;
+  FEMK_TRY(read_err(d_bad, s, &hbad));
+  if (hbad) {
+    cudaFree(p->cols16);
+    p->cols16 = nullptr;
+  }
+  return FEMK_OK;
+}
+
+int build_dirichlet(femk_plan* p, const uint8_t* user_mask, const int32_t* vptr, const int32_t* vinc, cudaStream_t s) {
+  const int64_t n = p->n;
+  FEMK_TRY(dev_alloc(&p->dmask, n, s));
+  if (user_mask) {
+    FEMK_CUDA_TRY(cudaMemcpyAsync(p->dmask, user_mask, n, cudaMemcpyDeviceToDevice, s));
+  } else {
+    FEMK_CUDA_TRY(cudaMemsetAsync(p->dmask, 0, n, s));
+    if (p->nd == 4)
+      k_boundary<4><<<::femk::counted_launch() + blocks_for(p->ntet * 4, kThreads, 65535 * 4), kThreads, 0, s>>>(p->cells, p->ntet, vptr, vinc, p->dmask);
+    else
+      k_boundary<10><<<::femk::counted_launch() + blocks_for(p->ntet * 4, kThreads, 65535 * 4), kThreads, 0, s>>>(p->cells, p->ntet, vptr, vinc, p->dmask);
+    FEMK_CUDA_TRY(cudaGetLastError());
+  }
+  Temp flag, pos;
+  FEMK_CUDA_TRY(cudaMalloc(&flag.p, sizeof(int64_t) * (n + 1)));
+  FEMK_CUDA_TRY(cudaMalloc(&pos.p, sizeof(int64_t) * (n + 1)));
+  k_mask_to_i64<<<::femk::counted_launch() + blocks_for(n, kThreads, 65535 * 4), kThreads, 0, s>>>(p->dmask, n, (int64_t*)flag.p);
+  FEMK_TRY(scan_exclusive_i64((const int64_t*)flag.p, (int64_t*)pos.p, n, s));
+  int64_t nd = 0;
+  FEMK_CUDA_TRY(cudaMemcpyAsync(&nd, (int64_t*)pos.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  p->n_dir = nd;
+  FEMK_TRY(dev_alloc(&p->dlist, nd, s));
+  k_compact<<<::femk::counted_launch() + blocks_for(n, kThreads, 65535 * 4), kThreads, 0, s>>>(p->dmask, (const int64_t*)pos.p, n, p->dlist);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  return FEMK_OK;
+}
+
+int create_impl(femk_plan* p, const double* xyz, const int32_t* tets, const uint8_t* mask, cudaStream_t s) {
+  int* d_err = nullptr;
+  FEMK_CUDA_TRY(cudaMalloc(&d_err, sizeof(int)));
+  Temp err_guard;
+  err_guard.p = d_err;
+  FEMK_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), s));
+  int h_err = 0;
+
+  FEMK_TRY(dev_alloc(&p->xyz, p->nvert * 3, s));
+  // vertex incidence (P1 connectivity): used by P2 numbering and by the boundary test
+  int32_t* vptr = nullptr;
+  int32_t* vinc = nullptr;
+  FEMK_TRY(build_incidence<4>(tets, p->ntet, p->nvert, &vptr, &vinc, d_err, s));
+  FEMK_TRY(read_err(d_err, s, &h_err));
+  if (h_err) {
+    cudaFree(vptr);
+    cudaFree(vinc);
+    set_error("femk_plan_create: a tet references a vertex outside [0, nvert)");
+    return FEMK_EINVAL;
+  }
+  if (p->order == 1) {
+    p->n = p->nvert;
+    FEMK_TRY(dev_alloc(&p->cells, p->ntet * 4, s));
+    FEMK_CUDA_TRY(cudaMemcpyAsync(p->cells, tets, sizeof(int32_t) * p->ntet * 4, cudaMemcpyDeviceToDevice, s));
+    FEMK_TRY(dev_alloc(&p->points, p->n * 3, s));
+    k_copy_xyz<<<::femk::counted_launch() + blocks_for(p->nvert * 3, kThreads, 65535 * 4), kThreads, 0, s>>>(xyz, p->nvert * 3, p->xyz, p->points);
+    p->inc_ptr = vptr;
+    p->inc_elem = vinc;
+  } else {
+    k_copy_xyz<<<::femk::counted_launch() + blocks_for(p->nvert * 3, kThreads, 65535 * 4), kThreads, 0, s>>>(xyz, p->nvert * 3, p->xyz, nullptr);
+    const int64_t m = p->ntet * 6;
+    Temp first, isf, rank;
+    FEMK_CUDA_TRY(cudaMalloc(&first.p, sizeof(int32_t) * m));
+    FEMK_CUDA_TRY(cudaMalloc(&isf.p, sizeof(int64_t) * (m + 1)));
+    FEMK_CUDA_TRY(cudaMalloc(&rank.p, sizeof(int64_t) * (m + 1)));
+    k_edge_first<<<::femk::counted_launch() + blocks_for(m, kThreads, 65535 * 4), kThreads, 0, s>>>(tets, p->ntet, vptr, vinc, (int32_t*)first.p,
+                                                                         (int64_t*)isf.p, d_err);
+    FEMK_CUDA_TRY(cudaGetLastError());
+    FEMK_TRY(scan_exclusive_i64((const int64_t*)isf.p, (int64_t*)rank.p, m, s));
+    int64_t nedge = 0;
+    FEMK_CUDA_TRY(cudaMemcpyAsync(&nedge, (int64_t*)rank.p + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+    p->n = p->nvert + nedge;
+    if (p->n >= INT32_MAX) {
+      cudaFree(vptr);
+      cudaFree(vinc);
+      set_error("femk_plan_create: too many DOFs for int32 indices");
+      return FEMK_EINVAL;
+    }
+    FEMK_TRY(dev_alloc(&p->cells, p->ntet * 10, s));
+    FEMK_TRY(dev_alloc(&p->points, p->n * 3, s));
+    FEMK_CUDA_TRY(cudaMemcpyAsync(p->points, xyz, sizeof(double) * p->nvert * 3, cudaMemcpyDeviceToDevice, s));
+    k_p2_cells<<<::femk::counted_launch() + blocks_for(m, kThreads, 65535 * 4), kThreads, 0, s>>>(tets, p->ntet, p->nvert, (const int32_t*)first.p,
+                                                                       (const int64_t*)rank.p, xyz, p->cells, p->points);
+    FEMK_CUDA_TRY(cudaGetLastError());
+    FEMK_TRY(build_incidence<10>(p->cells, p->ntet, p->n, &p->inc_ptr, &p->inc_elem, d_err, s));
+  }
+  FEMK_TRY(read_err(d_err, s, &h_err));
+  if (h_err) {
+    if (vptr != p->inc_ptr) {
+      cudaFree(vptr);
+      cudaFree(vinc);
+    }
+    set_error("femk_plan_create: inconsistent connectivity (edge lookup failed)");
+    return FEMK_EINVAL;
+  }
+  int st = p->nd == 4 ? build_pattern<4>(p, d_err, &h_err, s) : build_pattern<10>(p, d_err, &h_err, s);
+  if (st == FEMK_OK) st = build_dirichlet(p, mask, vptr, vinc, s);
+  if (vptr != p->inc_ptr) {
+    cudaFree(vptr);
+    cudaFree(vinc);
+  }
+  return st;
+}
+
+}  // namespace
+}  // namespace femk
+
+extern "C" int femk_plan_destroy(femk_plan* p) {
+  if (!p) return FEMK_OK;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(p->device);
+  void* ptrs[] = {p->xyz,   p->points,  p->cells,    p->indptr,  p->indices, p->slot,   p->diag,
+                  p->dmask, p->dlist,   p->inc_ptr,  p->inc_elem, p->cols16, p->work,   p->partials,
+                  p->state, p->work32,  p->vals32,   p->work64b};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  if (p->state_host) cudaFreeHost(p->state_host);
+  cudaSetDevice(cur);
+  delete p;
+  return FEMK_OK;
+}
+
+extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int32_t* tets_dev, int64_t ntet,
+                                int order, const uint8_t* dirichlet_mask_dev, void* stream, femk_plan** out) {
+  femk::clear_error();
+  FEMK_CHECK_ARG(out != nullptr, "femk_plan_create: out is NULL");
+  *out = nullptr;
+  FEMK_CHECK_ARG(xyz_dev && tets_dev, "femk_plan_create: xyz/tets is NULL");
+  FEMK_CHECK_ARG(order == 1 || order == 2, "femk_plan_create: order must be 1 or 2");
+  FEMK_CHECK_ARG(nvert >= 4 && ntet >= 1, "femk_plan_create: empty mesh");
+  FEMK_CHECK_ARG(ntet * (order == 1 ? 16 : 100) < INT32_MAX, "femk_plan_create: mesh too large for int32 slot map");
+  FEMK_CHECK_ARG(nvert < INT32_MAX, "femk_plan_create: too many vertices");
+  cudaStream_t s = (cudaStream_t)stream;
+  femk_plan* p = new femk_plan();
+  cudaGetDevice(&p->device);
+  cudaDeviceGetAttribute(&p->n_sm, cudaDevAttrMultiProcessorCount, p->device);
+  p->order = order;
+  p->nd = order == 1 ? 4 : 10;
+  p->nvert = nvert;
+  p->ntet = ntet;
+  const int st = femk::create_impl(p, xyz_dev, tets_dev, dirichlet_mask_dev, s);
+  if (st != FEMK_OK) {
+    femk_plan_destroy(p);
+    return st;
+  }
+  *out = p;
+  return FEMK_OK;
+}
+
+extern "C" int femk_plan_get_info(const femk_plan* p, femk_plan_info* out) {
+  FEMK_CHECK_ARG(p && out, "femk_plan_get_info: NULL argument");
+  out->order = p->order;
+  out->ndof_local = p->nd;
+  out->ntet = p->ntet;
+  out->nvert = p->nvert;
+  out->n = p->n;
+  out->nnz = p->nnz;
+  out->n_dirichlet = p->n_dir;
+  out->cols16 = p->cols16 ? 1 : 0;
+  out->device = p->device;
+  return FEMK_OK;
+}
+
+extern "C" int femk_plan_export(const femk_plan* p, int32_t* indptr, int32_t* indices, int32_t* slot, int32_t* cells,
+                                double* points, uint8_t* dmask, int32_t* diag, void* stream) {
+  femk::clear_error();
+  FEMK_CHECK_ARG(p, "femk_plan_export: plan is NULL");
+  cudaStream_t s = (cudaStream_t)stream;
+  const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+  if (indptr) FEMK_CUDA_TRY(cudaMemcpyAsync(indptr, p->indptr, sizeof(int32_t) * (p->n + 1), k, s));
+  if (indices) FEMK_CUDA_TRY(cudaMemcpyAsync(indices, p->indices, sizeof(int32_t) * p->nnz, k, s));
+  if (slot) FEMK_CUDA_TRY(cudaMemcpyAsync(slot, p->slot, sizeof(int32_t) * p->ntet * p->nd * p->nd, k, s));
+  if (cells) FEMK_CUDA_TRY(cudaMemcpyAsync(cells, p->cells, sizeof(int32_t) * p->ntet * p->nd, k, s));
+  if (points) FEMK_CUDA_TRY(cudaMemcpyAsync(points, p->points, sizeof(double) * p->n * 3, k, s));
+  if (dmask) FEMK_CUDA_TRY(cudaMemcpyAsync(dmask, p->dmask, p->n, k, s));
+  if (diag) FEMK_CUDA_TRY(cudaMemcpyAsync(diag, p->diag, sizeof(int32_t) * p->n, k, s));
+  return FEMK_OK;
+}

@@ -1,0 +1,108 @@
+"""Mesh front end: the structured Kuhn box and a ``jno.domain``-shaped holder (host, numpy).
+
+``equi_distant_box`` follows ``Geometries.equi_distant_box(..., cell="tetra")``
+(jno/domain/geometries.py:203-300): lattice points in C order ``idx = (i(ny+1) + j)(nz+1) + k`` and
+six Kuhn tets per voxel in (i, j, k, kuhn) order, corner bits ``(c>>2, c>>1, c)``. It returns a
+``constructor(geo) -> (mesh, 3, ds)`` like the reference; ``domain(constructor)`` builds the mesh.
+"""
+
+import numpy as np
+
+KUHN = ((0, 4, 6, 7), (0, 4, 5, 7), (0, 2, 6, 7), (0, 2, 3, 7), (0, 1, 5, 7), (0, 1, 3, 7))
+
+
+class Mesh:
+    """Minimal mesh record: ``points`` f64[nv, 3] and ``tets`` i64[T, 4]."""
+
+    def __init__(self, points, tets):
+        self.points = np.asarray(points, dtype=np.float64)
+        self.tets = np.asarray(tets, dtype=np.int64)
+        self.cells_dict = {"tetra": self.tets}
+
+
+def box_points_tets(nx, ny, nz, x_range=(0.0, 1.0), y_range=(0.0, 1.0), z_range=(0.0, 1.0)):
+    X = np.linspace(x_range[0], x_range[1], nx + 1)
+    Y = np.linspace(y_range[0], y_range[1], ny + 1)
+    Z = np.linspace(z_range[0], z_range[1], nz + 1)
+    xx, yy, zz = np.meshgrid(X, Y, Z, indexing="ij")
+    points = np.column_stack([xx.ravel(), yy.ravel(), zz.ravel()])
+    ny1, nz1 = ny + 1, nz + 1
+    I, J, K = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    I, J, K = I.ravel(), J.ravel(), K.ravel()
+    corner = np.stack(
+        [((I + ((c >> 2) & 1)) * ny1 + (J + ((c >> 1) & 1))) * nz1 + (K + (c & 1)) for c in range(8)], axis=1
+    )
+    tets = corner[:, np.asarray(KUHN)].reshape(-1, 4).astype(np.int64)
+    return points, tets
+
+
+def equi_distant_box(x_range=(0, 1), y_range=(0, 1), z_range=(0, 1), nx=8, ny=8, nz=8, cell="tetra"):
+    """Structured Kuhn-tet box constructor (the reference's ``equi_distant_box`` contract)."""
+    if cell != "tetra":
+        raise NotImplementedError("only cell='tetra' is on the B200 path (hexahedra are out of scope)")
+
+    def constructor(geo=None):
+        pts, tets = box_points_tets(nx, ny, nz, x_range, y_range, z_range)
+        ds = min((x_range[1] - x_range[0]) / nx, (y_range[1] - y_range[0]) / ny, (z_range[1] - z_range[0]) / nz)
+        return Mesh(pts, tets), 3, ds
+
+    constructor.lattice = (nx, ny, nz, x_range, y_range, z_range)
+    return constructor
+
+
+def jitter_interior(points, nx, ny, nz, seed, amp=0.1, x_range=(0.0, 1.0), y_range=(0.0, 1.0), z_range=(0.0, 1.0)):
+    """Synthetic workload input: move every interior lattice vertex by U(-amp h, amp h) per axis.
+
+    ``np.random.default_rng(seed).uniform(-amp, amp, (n_interior, 3)) * h`` in node-id order.
+    """
+    pts = np.array(points, dtype=np.float64, copy=True)
+    i, j, k = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+    inner = ((i > 0) & (i < nx) & (j > 0) & (j < ny) & (k > 0) & (k < nz)).ravel()
+    h = np.array([(x_range[1] - x_range[0]) / nx, (y_range[1] - y_range[0]) / ny, (z_range[1] - z_range[0]) / nz])
+    rng = np.random.default_rng(seed)
+    pts[inner] += rng.uniform(-amp, amp, size=(int(inner.sum()), 3)) * h[None, :]
+    return pts
+
+
+class domain:
+    """``jno.domain(constructor)``: holds the built mesh and hands out FEM symbols."""
+
+    def __init__(self, constructor, jitter=None, seed=0):
+        mesh, dim, ds = constructor(None)
+        if dim != 3:
+            raise NotImplementedError("only 3-D tetrahedral meshes are on the B200 path")
+        self.built_mesh = mesh
+        self.dimension = dim
+        self.ds = ds
+        if jitter:
+            nx, ny, nz, xr, yr, zr = constructor.lattice
+            mesh.points = jitter_interior(mesh.points, nx, ny, nz, seed, jitter, xr, yr, zr)
+
+    @classmethod
+    def from_mesh(cls, points, tets):
+        obj = cls.__new__(cls)
+        obj.built_mesh = Mesh(points, tets)
+        obj.dimension = 3
+        obj.ds = None
+        return obj
+
+    def _cells_p1(self):
+        return self.built_mesh.tets
+
+    def fem_symbols(self, names=("u", "v"), order=1, space=None, value_shape=None):
+        from .trace import FieldSymbol
+
+        if value_shape not in (None, (), 1):
+            raise NotImplementedError("vector-valued fields are outside the B200 scalar Poisson path")
+        if space == "P0":
+            return (FieldSymbol(names[0], "trial", self, 0, "P0"), FieldSymbol(names[1], "test", self, 0, "P0"))
+        if order not in (1, 2):
+            raise NotImplementedError("only Lagrange P1/P2 are on the B200 path")
+        return (FieldSymbol(names[0], "trial", self, order), FieldSymbol(names[1], "test", self, order))
+
+    def variable(self, region, split=True):
+        from .trace import Coordinate
+
+        if region not in ("interior", "boundary"):
+            raise NotImplementedError(f"region {region!r}: only 'interior' and 'boundary' are on the B200 path")
+        return tuple(Coordinate(region, a) for a in range(3))

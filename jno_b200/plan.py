@@ -1,0 +1,193 @@
+"""Device-resident assembly plan and the CSR operator it produces (host side of the C ABI).
+
+A :class:`FemPlan` owns one ``femk_plan``: the P1/P2 DOF numbering, the compress-plan CSR
+pattern, the element -> slot map, the Dirichlet set and the solver workspace, all in HBM. Every
+method launches CUDA kernels through ``libfemk.so`` on the current torch stream; inputs and outputs
+are CUDA tensors. Nothing here computes on the CPU.
+"""
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+def _device_tensor(a, dtype):
+    if isinstance(a, torch.Tensor):
+        t = a.to(device="cuda", dtype=dtype)
+    else:
+        t = torch.as_tensor(np.ascontiguousarray(a)).to(device="cuda", dtype=dtype)
+    return t.contiguous()
+
+
+class FemPlan:
+    """P1/P2 tetrahedral assembly plan on the current CUDA device.
+
+    ``points`` f64[nv, 3] and ``tets`` int[T, 4] describe the P1 mesh; ``order`` 2 adds the edge
+    midpoint DOFs in the reference's first-encounter numbering. ``dirichlet_mask`` (bool/uint8 per
+    DOF) overrides the default Dirichlet set (every node on a boundary facet).
+    """
+
+    def __init__(self, points, tets, order=1, dirichlet_mask=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("jno_b200 needs a CUDA device (B200, sm_100a); there is no CPU path")
+        lib = _lib.load()
+        self._lib = lib
+        xyz = _device_tensor(points, torch.float64)
+        cells = _device_tensor(tets, torch.int32)
+        if xyz.ndim != 2 or xyz.shape[1] != 3 or cells.ndim != 2 or cells.shape[1] != 4:
+            raise ValueError("points must be [nv, 3] and tets [T, 4]")
+        mask = None if dirichlet_mask is None else _device_tensor(dirichlet_mask, torch.uint8)
+        handle = ctypes.c_void_p()
+        _lib.check(
+            lib.femk_plan_create(
+                _lib.ptr(xyz), xyz.shape[0], _lib.ptr(cells), cells.shape[0], int(order), _lib.ptr(mask),
+                _lib.stream_handle(), ctypes.byref(handle),
+            )
+        )
+        self._h = handle
+        info = _lib.PlanInfo()
+        _lib.check(lib.femk_plan_get_info(self._h, ctypes.byref(info)))
+        self.order = info.order
+        self.nd = info.ndof_local
+        self.ntet = info.ntet
+        self.nvert = info.nvert
+        self.n = info.n
+        self.nnz = info.nnz
+        self.n_dirichlet = info.n_dirichlet
+        self.cols16 = bool(info.cols16)
+        self.device = torch.device("cuda", info.device)
+        self._pattern = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self._lib.femk_plan_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---------------------------------------------------------------- pattern export
+    def pattern(self):
+        """(indptr i32[n+1], indices i32[nnz]) of the canonical CSR, cached on the device."""
+        if self._pattern is None:
+            indptr = torch.empty(self.n + 1, dtype=torch.int32, device=self.device)
+            indices = torch.empty(self.nnz, dtype=torch.int32, device=self.device)
+            _lib.check(self._lib.femk_plan_export(self._h, _lib.ptr(indptr), _lib.ptr(indices), None, None, None,
+                                                  None, None, _lib.stream_handle()))
+            self._pattern = (indptr, indices)
+        return self._pattern
+
+    def export(self):
+        """Every plan array as CUDA tensors (dict)."""
+        d = self.device
+        out = {
+            "slot": torch.empty(self.ntet * self.nd * self.nd, dtype=torch.int32, device=d),
+            "cells": torch.empty(self.ntet * self.nd, dtype=torch.int32, device=d),
+            "points": torch.empty(self.n * 3, dtype=torch.float64, device=d),
+            "dirichlet_mask": torch.empty(self.n, dtype=torch.uint8, device=d),
+            "diag_slot": torch.empty(self.n, dtype=torch.int32, device=d),
+        }
+        indptr, indices = self.pattern()
+        _lib.check(self._lib.femk_plan_export(
+            self._h, None, None, _lib.ptr(out["slot"]), _lib.ptr(out["cells"]), _lib.ptr(out["points"]),
+            _lib.ptr(out["dirichlet_mask"]), _lib.ptr(out["diag_slot"]), _lib.stream_handle()))
+        out["indptr"], out["indices"] = indptr, indices
+        out["slot"] = out["slot"].view(self.ntet, self.nd, self.nd)
+        out["cells"] = out["cells"].view(self.ntet, self.nd)
+        out["points"] = out["points"].view(self.n, 3)
+        return out
+
+    # ---------------------------------------------------------------- kernels
+    def assemble(self, param=None, mode=_lib.COEF_EXP, scale=1.0, f=1.0, g=None, vals=None, b=None):
+        """(vals f64[nnz], b f64[n]) of ``k_e grad u . grad v - f v`` with Dirichlet ``u = g``."""
+        if mode != _lib.COEF_CONST:
+            param = _device_tensor(param, torch.float64)
+            if param.numel() != self.ntet:
+                raise ValueError(f"a P0 parameter needs {self.ntet} values, got {param.numel()}")
+        g = None if g is None else _device_tensor(g, torch.float64)
+        vals = torch.empty(self.nnz, dtype=torch.float64, device=self.device) if vals is None else vals
+        b = torch.empty(self.n, dtype=torch.float64, device=self.device) if b is None else b
+        _lib.check(self._lib.femk_assemble(self._h, _lib.ptr(param), int(mode), float(scale), float(f), _lib.ptr(g),
+                                           _lib.ptr(vals), _lib.ptr(b), _lib.stream_handle()))
+        return vals, b
+
+    def element_matrices(self):
+        khat = torch.empty(self.ntet, self.nd, self.nd, dtype=torch.float64, device=self.device)
+        fhat = torch.empty(self.ntet, self.nd, dtype=torch.float64, device=self.device)
+        _lib.check(self._lib.femk_element_matrices(self._h, _lib.ptr(khat), _lib.ptr(fhat), _lib.stream_handle()))
+        return khat, fhat
+
+    def lumped_mass(self):
+        m = torch.empty(self.n, dtype=torch.float64, device=self.device)
+        _lib.check(self._lib.femk_lumped_mass(self._h, _lib.ptr(m), _lib.stream_handle()))
+        return m
+
+    def jacobi(self, vals, out=None):
+        out = torch.empty(self.n, dtype=torch.float64, device=self.device) if out is None else out
+        _lib.check(self._lib.femk_jacobi(self._h, _lib.ptr(vals), _lib.ptr(out), _lib.stream_handle()))
+        return out
+
+    def jacobi_matfree(self, param=None, mode=_lib.COEF_EXP, scale=1.0, out=None):
+        out = torch.empty(self.n, dtype=torch.float64, device=self.device) if out is None else out
+        _lib.check(self._lib.femk_jacobi_matfree(self._h, _lib.ptr(param), int(mode), float(scale), _lib.ptr(out),
+                                                 _lib.stream_handle()))
+        return out
+
+    def spmv(self, vals, x, out=None):
+        out = torch.empty(self.n, dtype=torch.float64, device=self.device) if out is None else out
+        _lib.check(self._lib.femk_spmv(self._h, _lib.ptr(vals), _lib.ptr(x), _lib.ptr(out), _lib.stream_handle()))
+        return out
+
+    def spmv_matfree(self, param, x, mode=_lib.COEF_EXP, scale=1.0, out=None):
+        out = torch.empty(self.n, dtype=torch.float64, device=self.device) if out is None else out
+        _lib.check(self._lib.femk_spmv_matfree(self._h, _lib.ptr(param), int(mode), float(scale), _lib.ptr(x),
+                                               _lib.ptr(out), _lib.stream_handle()))
+        return out
+
+    def pcg(self, vals, b, x=None, inv_diag=None, tol=1e-8, atol=0.0, maxiter=20_000, relres=True):
+        """Jacobi-PCG (jax cg semantics). Returns (x, iterations, relres, status)."""
+        x = torch.zeros(self.n, dtype=torch.float64, device=self.device) if x is None else x
+        it = ctypes.c_int32(0)
+        rr = ctypes.c_double(float("nan"))
+        st = self._lib.femk_pcg(self._h, _lib.ptr(vals), _lib.ptr(b), _lib.ptr(x), _lib.ptr(inv_diag), float(tol),
+                                float(atol), int(maxiter), ctypes.byref(it), ctypes.byref(rr) if relres else None,
+                                _lib.stream_handle())
+        _lib.check(st, allow=(_lib.FEMK_NOT_CONVERGED,))
+        return x, it.value, rr.value, st
+
+    def pcg_matfree(self, param, b, x=None, inv_diag=None, mode=_lib.COEF_EXP, scale=1.0, tol=1e-8, atol=0.0,
+                    maxiter=20_000, relres=True):
+        x = torch.zeros(self.n, dtype=torch.float64, device=self.device) if x is None else x
+        it = ctypes.c_int32(0)
+        rr = ctypes.c_double(float("nan"))
+        st = self._lib.femk_pcg_matfree(self._h, _lib.ptr(param), int(mode), float(scale), _lib.ptr(b), _lib.ptr(x),
+                                        _lib.ptr(inv_diag), float(tol), float(atol), int(maxiter), ctypes.byref(it),
+                                        ctypes.byref(rr) if relres else None, _lib.stream_handle())
+        _lib.check(st, allow=(_lib.FEMK_NOT_CONVERGED,))
+        return x, it.value, rr.value, st
+
+    def pcg_mixed(self, vals, b, inv_diag, x=None, tol=1e-8, atol=0.0, maxiter=20_000, mode=_lib.MIXED_RELIABLE):
+        """FP32-inner / FP64-refined PCG. Returns (x, inner iterations, outer updates, relres, status)."""
+        x = torch.zeros(self.n, dtype=torch.float64, device=self.device) if x is None else x
+        inner = ctypes.c_int32(0)
+        outer = ctypes.c_int32(0)
+        rr = ctypes.c_double(float("nan"))
+        st = self._lib.femk_pcg_mixed(self._h, _lib.ptr(vals), _lib.ptr(b), _lib.ptr(x), _lib.ptr(inv_diag),
+                                      float(tol), float(atol), int(maxiter), int(mode), ctypes.byref(inner),
+                                      ctypes.byref(outer), ctypes.byref(rr), _lib.stream_handle())
+        _lib.check(st, allow=(_lib.FEMK_NOT_CONVERGED,))
+        return x, inner.value, outer.value, rr.value, st
+
+    def adjoint_grad(self, param, u, lam, mode=_lib.COEF_EXP, scale=1.0, out=None):
+        out = torch.empty(self.ntet, dtype=torch.float64, device=self.device) if out is None else out
+        _lib.check(self._lib.femk_adjoint_grad(self._h, _lib.ptr(param), int(mode), float(scale), _lib.ptr(u),
+                                               _lib.ptr(lam), _lib.ptr(out), _lib.stream_handle()))
+        return out

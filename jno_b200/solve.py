@@ -1,0 +1,102 @@
+"""``jno.solve.cg`` on the B200 kernels (jno/solve.py:191-206, jno/utils/solver/solver_api.py:243-301).
+
+``cg(tol=1e-8, atol=0.0, maxiter=20_000)`` returns a :class:`LinearSolver` called as
+``solver(A, b, *, M=None, x0=None) -> x``. The iteration is ``jax.scipy.sparse.linalg.cg``'s
+(jax 0.10.1): x0 = 0 by default, stop when <r, r> <= max(tol^2 <b, b>, atol^2) with a
+preconditioner (<r, z> without one) or at maxiter. After the solve the eager residual guard of
+``_maybe_residual_check`` (solver_api.py:224-240) raises ``RuntimeError`` when
+``||b - A x|| / (||b|| + 1e-30) > 1e-4``.
+
+Extensions with no reference counterpart: ``precision="mixed"`` (FP32 inner CG with FP64 reliable
+updates, ``refine="reliable"`` or classic restarted refinement ``refine="restart"``) and matrix-free
+operators (:class:`~jno_b200.sparse.MatrixFreeOperator`).
+"""
+
+import math
+
+import torch
+
+from . import _lib
+from .precond import JacobiApplier, PrecondContext
+from .sparse import CsrMatrix, MatrixFreeOperator, _as_cuda
+
+
+class LinearOperator:
+    """Wrapper kept for signature parity with ``jno.solve.LinearOperator``; holds a device operator."""
+
+    def __init__(self, A):
+        self.A = A.A if isinstance(A, LinearOperator) else A
+
+    def mv(self, v):
+        return self.A @ v
+
+    __matmul__ = mv
+
+    def diag(self):
+        return self.A.diag()
+
+
+class SolveInfo:
+    def __init__(self, iterations, relres, status, outer=None):
+        self.iterations, self.relres, self.status, self.outer = iterations, relres, status, outer
+
+    def __repr__(self):
+        return f"SolveInfo(iterations={self.iterations}, relres={self.relres:.3e}, outer={self.outer})"
+
+
+class LinearSolver:
+    def __init__(self, tol, atol, maxiter, precision="fp64", refine="reliable", name="cg"):
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        if refine not in ("reliable", "restart"):
+            raise ValueError("refine must be 'reliable' or 'restart'")
+        self.tol, self.atol = float(tol), float(atol)
+        self.maxiter = 20_000 if maxiter is None else int(maxiter)
+        self.precision, self.refine, self.name = precision, refine, name
+        self.direct = False
+        self.key = (type(self), name, (self.tol, self.atol, self.maxiter, precision, refine))
+        self.last_info = None
+
+    def __eq__(self, other):
+        return isinstance(other, LinearSolver) and other.key == self.key
+
+    def __hash__(self):
+        return hash(self.key)
+
+    def __call__(self, A, b, *, M=None, x0=None):
+        op = A.A if isinstance(A, LinearOperator) else A
+        if not isinstance(op, (CsrMatrix, MatrixFreeOperator)):
+            raise TypeError("the B200 CG takes an assembled CsrMatrix or a MatrixFreeOperator")
+        plan = op.plan
+        b = _as_cuda(b, plan.device).reshape(-1)
+        if M is not None and hasattr(M, "materialize"):
+            M = M.materialize(PrecondContext(op))
+        if M is not None and not isinstance(M, JacobiApplier):
+            raise TypeError("the fused CG kernels apply the Jacobi preconditioner only (jno_b200.precond.jacobi())")
+        inv = None if M is None else M.inv_diag
+        x = torch.zeros_like(b) if x0 is None else _as_cuda(x0, plan.device).reshape(-1).clone()
+        if self.precision == "mixed":
+            if not isinstance(op, CsrMatrix) or inv is None:
+                raise ValueError("precision='mixed' needs an assembled CsrMatrix and M=jacobi()")
+            mode = _lib.MIXED_RELIABLE if self.refine == "reliable" else _lib.MIXED_RESTART
+            x, inner, outer, rel, st = plan.pcg_mixed(op.data, b, inv, x, self.tol, self.atol, self.maxiter, mode)
+            self.last_info = SolveInfo(inner, rel, st, outer)
+        elif isinstance(op, MatrixFreeOperator):
+            x, it, rel, st = plan.pcg_matfree(op.param, b, x, inv, op.mode, op.scale, self.tol, self.atol,
+                                              self.maxiter)
+            self.last_info = SolveInfo(it, rel, st)
+        else:
+            x, it, rel, st = plan.pcg(op.data, b, x, inv, self.tol, self.atol, self.maxiter)
+            self.last_info = SolveInfo(it, rel, st)
+        rel = self.last_info.relres
+        if not math.isfinite(rel) or rel > 1e-4:
+            raise RuntimeError(
+                f"jno.solve.{self.name} did not solve the system (relative residual {rel:.1e}); the problem may be "
+                "singular/ill-posed or need a preconditioner. Try jno.solve.lu(), a precond= spec, or your own solve_fn."
+            )
+        return x
+
+
+def cg(*, tol=1e-8, atol=0.0, maxiter=20_000, precision="fp64", refine="reliable"):
+    """Jacobi-preconditionable CG on the B200 kernels (``jax.scipy.sparse.linalg.cg`` semantics)."""
+    return LinearSolver(tol, atol, maxiter, precision, refine)

@@ -1,0 +1,257 @@
+"""A small symbolic front end that recognises the weak forms of the B200 path.
+
+It mirrors the reference's DSL surface for this path only (``d.fem_symbols``, ``u.bind``, ``ui.x``,
+``jno.np.exp``, ``jno.np.parameter``, ``u(xb, yb, zb) - g``; jno/trace/__init__.py,
+jno/architectures/models.py:58-142) and classifies a form into the kernel arguments:
+
+    coef * (ui.x*vi.x + ui.y*vi.y + ui.z*vi.z) - f * vi,   coef in {c, c*p, c*exp(p)}, p a P0 parameter
+
+Anything else raises ``NotImplementedError``: other physics is outside this path.
+"""
+
+import numbers
+
+import numpy as np
+
+
+class Expr:
+    def __add__(self, o):
+        return Add(self, _wrap(o))
+
+    def __radd__(self, o):
+        return Add(_wrap(o), self)
+
+    def __sub__(self, o):
+        return Add(self, Mul(Const(-1.0), _wrap(o)))
+
+    def __rsub__(self, o):
+        return Add(_wrap(o), Mul(Const(-1.0), self))
+
+    def __mul__(self, o):
+        return Mul(self, _wrap(o))
+
+    def __rmul__(self, o):
+        return Mul(_wrap(o), self)
+
+    def __neg__(self):
+        return Mul(Const(-1.0), self)
+
+    def __pow__(self, k):
+        if not isinstance(k, numbers.Integral) or k < 1:
+            raise NotImplementedError("only positive integer powers")
+        out = self
+        for _ in range(k - 1):
+            out = Mul(out, self)
+        return out
+
+
+def _wrap(o):
+    if isinstance(o, Expr):
+        return o
+    if isinstance(o, numbers.Number):
+        return Const(float(o))
+    raise TypeError(f"cannot use {type(o).__name__} in a weak form")
+
+
+class Const(Expr):
+    def __init__(self, v):
+        self.v = float(v)
+
+
+class Add(Expr):
+    def __init__(self, a, b):
+        self.a, self.b = a, b
+
+
+class Mul(Expr):
+    def __init__(self, a, b):
+        self.a, self.b = a, b
+
+
+class Exp(Expr):
+    def __init__(self, a):
+        self.a = a
+
+
+class Coordinate(Expr):
+    def __init__(self, region, axis):
+        self.region, self.axis = region, axis
+
+
+class FieldSymbol(Expr):
+    """A trial/test symbol (``role``) of a Lagrange field or a P0 symbol (space='P0')."""
+
+    def __init__(self, name, role, domain, order, space="P"):
+        self.name, self.role, self.domain, self.order, self.space = name, role, domain, order, space
+
+    def bind(self, **coords):
+        return Bound(self)
+
+    def __call__(self, *coords):
+        regions = {getattr(c, "region", None) for c in coords}
+        if regions != {"boundary"}:
+            raise NotImplementedError("Dirichlet conditions are supported on the whole 'boundary' only")
+        return TraceOn(self, "boundary")
+
+
+class Bound(Expr):
+    def __init__(self, sym):
+        self.sym = sym
+
+    @property
+    def x(self):
+        return Deriv(self.sym, 0)
+
+    @property
+    def y(self):
+        return Deriv(self.sym, 1)
+
+    @property
+    def z(self):
+        return Deriv(self.sym, 2)
+
+
+class Deriv(Expr):
+    def __init__(self, sym, axis):
+        self.sym, self.axis = sym, axis
+
+
+class TraceOn(Expr):
+    def __init__(self, sym, region):
+        self.sym, self.region = sym, region
+
+
+class Param(Expr):
+    """``jno.np.parameter(<P0 symbol>, name=...)``: one value per element (models.py:92-107)."""
+
+    def __init__(self, sym, name):
+        self.sym, self.name = sym, name
+
+
+def parameter(sym, name="param", **_):
+    if not isinstance(sym, FieldSymbol) or sym.space != "P0":
+        raise NotImplementedError("only P0 (per-element) field parameters are on the B200 path")
+    return Param(sym, name)
+
+
+def exp(a):
+    a = _wrap(a)
+    if isinstance(a, Const):
+        return Const(float(np.exp(a.v)))
+    return Exp(a)
+
+
+# ------------------------------------------------------------------------------ classification
+def _monomials(e):
+    """Expand into a list of (scalar, [factors])."""
+    if isinstance(e, Const):
+        return [(e.v, [])]
+    if isinstance(e, Add):
+        return _monomials(e.a) + _monomials(e.b)
+    if isinstance(e, Mul):
+        out = []
+        for ca, fa in _monomials(e.a):
+            for cb, fb in _monomials(e.b):
+                out.append((ca * cb, fa + fb))
+        return out
+    return [(1.0, [e])]
+
+
+def _coef_key(factors):
+    """Coefficient factors -> ('const',) | ('linear', name) | ('exp', name)."""
+    params = [f for f in factors if isinstance(f, Param)]
+    exps = [f for f in factors if isinstance(f, Exp)]
+    other = [f for f in factors if not isinstance(f, (Param, Exp))]
+    if other:
+        raise NotImplementedError("a spatially varying coefficient is outside the B200 path (P0 parameters only)")
+    if not params and not exps:
+        return ("const",)
+    if len(params) == 1 and not exps:
+        return ("linear", params[0].name)
+    if len(exps) == 1 and not params and isinstance(exps[0].a, Param):
+        return ("exp", exps[0].a.name)
+    raise NotImplementedError("only c, c*p and c*exp(p) coefficients are on the B200 path")
+
+
+class WeakForm:
+    """Classified volume form: k_e = scale * g(param_e), source f, field order."""
+
+    def __init__(self, order, mode, scale, param, f, domain):
+        self.order, self.mode, self.scale, self.param, self.f, self.domain = order, mode, scale, param, f, domain
+
+
+def classify_volume(expr):
+    stiff = {}  # axis -> (scale, key)
+    source = 0.0
+    order = None
+    domain = None
+    for c, factors in _monomials(expr):
+        ders = [f for f in factors if isinstance(f, Deriv)]
+        vals = [f for f in factors if isinstance(f, Bound)]
+        rest = [f for f in factors if not isinstance(f, (Deriv, Bound))]
+        if len(ders) == 2 and not vals:
+            roles = {d.sym.role for d in ders}
+            if roles != {"trial", "test"} or ders[0].axis != ders[1].axis:
+                raise NotImplementedError("only grad u . grad v stiffness terms are on the B200 path")
+            ax = ders[0].axis
+            if ax in stiff:
+                raise NotImplementedError("repeated stiffness component")
+            stiff[ax] = (c, _coef_key(rest))
+            order = ders[0].sym.order
+            domain = ders[0].sym.domain
+        elif len(vals) == 1 and not ders and vals[0].sym.role == "test":
+            if rest:
+                raise NotImplementedError("only a constant source f is on the B200 path")
+            source += -c
+        elif not ders and not vals:
+            continue
+        else:
+            raise NotImplementedError("this term is outside the B200 path (-div(k grad u) = f only)")
+    if sorted(stiff) != [0, 1, 2]:
+        raise NotImplementedError("the form needs ui.x*vi.x + ui.y*vi.y + ui.z*vi.z")
+    scales = {s for s, _ in stiff.values()}
+    keys = {k for _, k in stiff.values()}
+    if len(scales) != 1 or len(keys) != 1:
+        raise NotImplementedError("an anisotropic coefficient is outside the B200 path")
+    scale, key = scales.pop(), keys.pop()
+    from . import _lib
+
+    mode = {"const": _lib.COEF_CONST, "linear": _lib.COEF_LINEAR, "exp": _lib.COEF_EXP}[key[0]]
+    return WeakForm(order, mode, scale, key[1] if len(key) > 1 else None, source, domain)
+
+
+def evaluate_on(expr, pts):
+    """Evaluate a Dirichlet value expression (constants and boundary coordinates) at points f64[m, 3]."""
+    if isinstance(expr, Const):
+        return np.full(pts.shape[0], expr.v)
+    if isinstance(expr, Coordinate):
+        return pts[:, expr.axis].copy()
+    if isinstance(expr, Add):
+        return evaluate_on(expr.a, pts) + evaluate_on(expr.b, pts)
+    if isinstance(expr, Mul):
+        return evaluate_on(expr.a, pts) * evaluate_on(expr.b, pts)
+    if isinstance(expr, Exp):
+        return np.exp(evaluate_on(expr.a, pts))
+    raise NotImplementedError("Dirichlet values may use constants and boundary coordinates only")
+
+
+def classify_dirichlet(expr):
+    """``u(boundary) - g`` -> (symbol, g expression)."""
+    traces, rest = [], []
+    for c, factors in _monomials(expr):
+        tr = [f for f in factors if isinstance(f, TraceOn)]
+        if tr:
+            if len(tr) != 1 or len(factors) != 1 or c != 1.0:
+                raise NotImplementedError("Dirichlet terms must read u(boundary) - g")
+            traces.append(tr[0])
+        else:
+            prod = Const(-c)
+            for f in factors:
+                prod = Mul(prod, f)
+            rest.append(prod)
+    if len(traces) != 1:
+        raise NotImplementedError("exactly one u(boundary) per Dirichlet term")
+    g = Const(0.0)
+    for r in rest:
+        g = Add(g, r)
+    return traces[0].sym, g

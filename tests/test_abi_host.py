@@ -1,0 +1,103 @@
+"""CPU tests: the C-ABI library loads and exports every declared symbol; host-side logic of the
+jno-shaped surface (form classification, argument checks). No kernel is launched."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "femk.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(femk_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    from jno_b200 import _lib
+
+    lib = _lib.load()
+    names = _declared()
+    assert len(names) >= 15
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
+    assert lib.femk_version() >= 10000
+    assert isinstance(lib.femk_last_error_string(), bytes)
+
+
+def test_null_arguments_are_rejected_without_a_gpu():
+    from jno_b200 import _lib
+
+    lib = _lib.load()
+    out = ctypes.c_void_p()
+    st = lib.femk_plan_create(None, 8, None, 1, 1, None, None, ctypes.byref(out))
+    assert st == _lib.FEMK_EINVAL
+    assert b"NULL" in lib.femk_last_error_string()
+    st = lib.femk_plan_create(None, 8, None, 1, 3, None, None, ctypes.byref(out))
+    assert st == _lib.FEMK_EINVAL
+    assert lib.femk_assemble(None, None, 0, 1.0, 1.0, None, None, None, None) == _lib.FEMK_EINVAL
+    assert lib.femk_pcg(None, None, None, None, None, 1e-8, 0.0, 10, None, None, None) == _lib.FEMK_EINVAL
+    assert lib.femk_plan_destroy(None) == _lib.FEMK_OK
+
+
+def _recipe():
+    import jno_b200 as jno
+
+    d = jno.domain(jno.domain.equi_distant_box(nx=2, ny=2, nz=2))
+    u, v = d.fem_symbols()
+    _r, s = d.fem_symbols(space="P0", names=("r", "s"))
+    xi, yi, zi = d.variable("interior", split=True)
+    xb, yb, zb = d.variable("boundary", split=True)
+    ui, vi = u.bind(x=xi, y=yi, z=zi), v.bind(x=xi, y=yi, z=zi)
+    return jno, d, u, v, s, ui, vi, (xb, yb, zb)
+
+
+def test_form_classification():
+    from jno_b200 import _lib
+    from jno_b200.trace import classify_dirichlet, classify_volume, evaluate_on
+
+    jno, d, u, v, s, ui, vi, xb = _recipe()
+    logk = jno.np.parameter(s, name="logk")
+    f = classify_volume(jno.np.exp(logk) * (ui.x * vi.x + ui.y * vi.y + ui.z * vi.z) - 1.0 * vi)
+    assert (f.mode, f.scale, f.param, f.f, f.order) == (_lib.COEF_EXP, 1.0, "logk", 1.0, 1)
+    f = classify_volume(2.0 * logk * (ui.x * vi.x + ui.y * vi.y + ui.z * vi.z) + 3.0 * vi)
+    assert (f.mode, f.scale, f.f) == (_lib.COEF_LINEAR, 2.0, -3.0)
+    f = classify_volume(ui.x * vi.x + ui.y * vi.y + ui.z * vi.z)
+    assert (f.mode, f.f) == (_lib.COEF_CONST, 0.0)
+    sym, g = classify_dirichlet(u(*xb) - (1.0 + 2.0 * xb[0]))
+    pts = np.array([[0.5, 0.0, 0.0], [1.0, 1.0, 1.0]])
+    assert np.allclose(evaluate_on(g, pts), [2.0, 3.0])
+    with pytest.raises(NotImplementedError):
+        classify_volume(ui.x * vi.y + ui.y * vi.x + ui.z * vi.z)
+    with pytest.raises(NotImplementedError):
+        classify_volume(ui.x * vi.x + ui.y * vi.y)
+    with pytest.raises(NotImplementedError):
+        classify_volume(logk * (ui.x * vi.x) + ui.y * vi.y + ui.z * vi.z)
+    with pytest.raises(NotImplementedError):
+        jno.np.parameter(u, name="nodal")
+
+
+def test_product_has_no_cpu_fallback():
+    """Without a CUDA device the product refuses to run instead of computing on the CPU."""
+    import torch
+
+    from jno_b200.plan import FemPlan
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(RuntimeError, match="CUDA device"):
+        FemPlan(np.zeros((4, 3)), np.array([[0, 1, 2, 3]]), 1)
+
+
+def test_product_never_imports_the_oracle():
+    pkg = os.path.join(ROOT, "jno_b200")
+    for dirpath, _, files in os.walk(pkg):
+        for fn in files:
+            if fn.endswith((".py", ".cu", ".cuh")):
+                src = open(os.path.join(dirpath, fn)).read()
+                assert "import oracle" not in src and "from oracle" not in src, fn

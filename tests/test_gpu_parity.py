@@ -1,0 +1,273 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle on the same seeded inputs.
+
+Bars: integer/index outputs bit-exact; FP64 matrix values and loads within 1e-12 of the oracle
+relative to the largest entry; solves to the 1e-8 stop rule with the solution within 1e-7 of the
+oracle's; adjoint gradient within 1e-8 of the oracle's adjoint and 1e-6 of central differences.
+"""
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from oracle import adjoint as oadj  # noqa: E402
+from oracle import assemble as oa  # noqa: E402
+from oracle import element as oe  # noqa: E402
+from oracle import mesh as om  # noqa: E402
+from oracle import pcg as op  # noqa: E402
+
+VAL_TOL = 1e-12
+
+
+def _plan(points, tets, order):
+    from jno_b200.plan import FemPlan
+
+    return FemPlan(points, tets, order)
+
+
+def _mesh(n, order, seed=0):
+    return om.kuhn_cube(n, order=order, seed=seed)
+
+
+def _oracle_system(pf, cf, order, logk, f=1.0, g=None):
+    bnd = om.boundary_nodes(cf, order)
+    return oa.assemble(pf, cf, order, bnd, np.exp(logk), f=f, g=g), bnd
+
+
+@pytest.mark.parametrize("n,order", [(2, 1), (4, 1), (8, 1), (2, 2), (4, 2), (6, 2)])
+def test_plan_matches_oracle_bit_exact(n, order):
+    pf, cf, tets, p1 = _mesh(n, order)
+    plan = _plan(p1, tets, order)
+    ex = plan.export()
+    idx, inverse, nse = oa.compress_plan(cf)
+    indptr, indices = oa.plan_to_csr(idx, pf.shape[0])
+    assert plan.n == pf.shape[0] and plan.nnz == nse
+    assert np.array_equal(ex["cells"].cpu().numpy(), cf)
+    assert np.array_equal(ex["indptr"].cpu().numpy(), indptr)
+    assert np.array_equal(ex["indices"].cpu().numpy(), indices)
+    assert np.array_equal(ex["slot"].cpu().numpy().reshape(-1), inverse)
+    assert np.array_equal(ex["points"].cpu().numpy(), pf)
+    bnd = om.boundary_nodes(cf, order)
+    assert np.array_equal(np.flatnonzero(ex["dirichlet_mask"].cpu().numpy()), bnd)
+    rows = np.repeat(np.arange(plan.n), np.diff(indptr))
+    assert np.array_equal(ex["diag_slot"].cpu().numpy(), np.flatnonzero(rows == indices))
+
+
+def test_plan_golden_reference_fixture(golden):
+    """The device plan reproduces the reference-generated fixture directly (4x4x4, P1 and P2)."""
+    tag = "4x4x4"
+    plan1 = _plan(golden[f"{tag}/jittered"], golden[f"{tag}/tets"], 1)
+    ex = plan1.export()
+    idx = golden[f"{tag}/p1_idx"]
+    assert np.array_equal(ex["indices"].cpu().numpy(), idx[:, 1])
+    assert np.array_equal(ex["slot"].cpu().numpy().reshape(-1), golden[f"{tag}/p1_inverse"])
+    plan2 = _plan(golden[f"{tag}/jittered"], golden[f"{tag}/tets"], 2)
+    ex2 = plan2.export()
+    assert np.array_equal(ex2["cells"].cpu().numpy(), golden[f"{tag}/p2_cells"])
+    assert np.array_equal(ex2["points"].cpu().numpy(), golden[f"{tag}/p2_points"])
+    assert np.array_equal(ex2["slot"].cpu().numpy().reshape(-1), golden[f"{tag}/p2_inverse"])
+    assert np.array_equal(np.flatnonzero(ex2["dirichlet_mask"].cpu().numpy()), golden[f"{tag}/p2_boundary"])
+
+
+@pytest.mark.parametrize("n,order", [(3, 1), (8, 1), (16, 1), (3, 2), (6, 2)])
+def test_assembly_matches_oracle(n, order):
+    pf, cf, tets, p1 = _mesh(n, order, seed=1)
+    logk = om.logk_field(len(tets), 1000)
+    plan = _plan(p1, tets, order)
+    vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
+    s, _ = _oracle_system(pf, cf, order, logk)
+    v = vals.cpu().numpy()
+    assert np.abs(v - s.data).max() <= VAL_TOL * np.abs(s.data).max()
+    assert np.abs(b.cpu().numpy() - s.b).max() <= VAL_TOL * np.abs(s.b).max()
+    # Dirichlet entries are explicit zeros, diagonal exactly 1
+    assert np.array_equal(v == 0.0, s.data == 0.0)
+    kh, fh = plan.element_matrices()
+    K, F = oe.element_matrices(p1[tets], order)
+    assert np.abs(kh.cpu().numpy() - K).max() <= VAL_TOL * np.abs(K).max()
+    assert np.abs(fh.cpu().numpy() - F).max() <= VAL_TOL * np.abs(F).max()
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_inhomogeneous_dirichlet_patch(order):
+    """P1 reproduces a linear field, P2 a quadratic one (tests/test_fem_3d.py:76-89,
+    tests/test_fem_native_lagrange.py:377-395), through the CUDA assembly and CG."""
+    n = 4
+    pf, cf, tets, p1 = _mesh(n, order, seed=3)
+    x, y, z = pf.T
+    if order == 1:
+        exact, f = 1 + 2 * x + 3 * y + 4 * z, 0.0
+    else:
+        exact, f = x**2 + 2 * y**2 + 3 * z**2 + x * y, -12.0
+    plan = _plan(p1, tets, order)
+    g = torch.as_tensor(exact, device="cuda")
+    vals, b = plan.assemble(None, mode=2, scale=1.0, f=f, g=g)
+    s, _ = _oracle_system(pf, cf, order, np.zeros(len(tets)), f=f, g=exact)
+    assert np.abs(vals.cpu().numpy() - s.data).max() <= VAL_TOL * np.abs(s.data).max()
+    assert np.abs(b.cpu().numpy() - s.b).max() <= 1e-11 * np.abs(s.b).max()
+    inv = plan.jacobi(vals)
+    u, it, rel, st = plan.pcg(vals, b, inv_diag=inv, tol=1e-13)
+    assert np.abs(u.cpu().numpy() - exact).max() < 1e-9
+
+
+@pytest.mark.parametrize("n,order", [(8, 1), (24, 1), (4, 2), (8, 2)])
+def test_pcg_matches_oracle(n, order):
+    pf, cf, tets, p1 = _mesh(n, order)
+    logk = om.logk_field(len(tets), 1000)
+    plan = _plan(p1, tets, order)
+    vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
+    inv = plan.jacobi(vals)
+    u, it, rel, st = plan.pcg(vals, b, inv_diag=inv, tol=1e-8)
+    s, _ = _oracle_system(pf, cf, order, logk)
+    A = s.csr()
+    xo, ito, hist = op.pcg(A, s.b, oa.jacobi_inverse(oa.matrix_diagonal(s)), tol=1e-8)
+    assert st == 0
+    assert abs(it - ito) <= 1, (it, ito)
+    uu = u.cpu().numpy()
+    assert np.linalg.norm(uu - xo) <= 1e-7 * np.linalg.norm(xo)
+    assert rel <= 2e-8 and abs(rel - op.residual_check(A, s.b, uu)) <= 1e-12
+    # inverse diagonal matches the reference's materialize
+    assert np.abs(inv.cpu().numpy() - oa.jacobi_inverse(oa.matrix_diagonal(s))).max() <= 1e-12 * np.abs(
+        oa.jacobi_inverse(oa.matrix_diagonal(s))).max()
+
+
+def test_spmv_and_matrix_free_match():
+    for n, order in ((8, 1), (4, 2)):
+        pf, cf, tets, p1 = _mesh(n, order, seed=2)
+        logk = om.logk_field(len(tets), 7)
+        plan = _plan(p1, tets, order)
+        lk = torch.as_tensor(logk, device="cuda")
+        vals, b = plan.assemble(lk)
+        xv = torch.as_tensor(np.random.default_rng(0).standard_normal(plan.n), device="cuda")
+        y1 = plan.spmv(vals, xv).cpu().numpy()
+        s, _ = _oracle_system(pf, cf, order, logk)
+        yo = s.csr() @ xv.cpu().numpy()
+        assert np.abs(y1 - yo).max() <= 1e-12 * np.abs(yo).max()
+        y2 = plan.spmv_matfree(lk, xv).cpu().numpy()
+        assert np.abs(y2 - yo).max() <= 1e-12 * np.abs(yo).max()
+        inv = plan.jacobi(vals)
+        inv_mf = plan.jacobi_matfree(lk)
+        assert np.abs(inv.cpu().numpy() - inv_mf.cpu().numpy()).max() <= 1e-12 * inv.abs().max().item()
+        u1, it1, _, _ = plan.pcg(vals, b, inv_diag=inv)
+        u2, it2, rel2, _ = plan.pcg_matfree(lk, b, inv_diag=inv_mf)
+        assert abs(it1 - it2) <= 1 and rel2 <= 2e-8
+        assert torch.linalg.norm(u1 - u2) <= 1e-7 * torch.linalg.norm(u1)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_mixed_precision_reaches_fp64_accuracy(mode):
+    pf, cf, tets, p1 = _mesh(16, 1)
+    logk = om.logk_field(len(tets), 1001)
+    plan = _plan(p1, tets, 1)
+    vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
+    inv = plan.jacobi(vals)
+    u64, it64, rel64, _ = plan.pcg(vals, b, inv_diag=inv, tol=1e-12)
+    u, inner, outer, rel, st = plan.pcg_mixed(vals, b, inv, tol=1e-8, mode=mode)
+    assert st == 0 and rel <= 1e-8 and outer >= 2
+    # true FP64 residual of the returned x
+    r = b - plan.spmv(vals, u)
+    assert (torch.linalg.norm(r) / torch.linalg.norm(b)).item() <= 1e-8
+    assert (torch.linalg.norm(u - u64) / torch.linalg.norm(u64)).item() <= 1e-7
+
+
+def test_adjoint_gradient_matches_oracle_and_fd():
+    n = 6
+    pf, cf, tets, p1 = _mesh(n, 1)
+    logk = om.logk_field(len(tets), 1002)
+    ustar_logk = om.logk_field(len(tets), 2000)
+    bnd = om.boundary_nodes(cf, 1)
+    ustar, _, _ = oadj.solve(pf, cf, 1, bnd, ustar_logk)
+    mass = oadj.lumped_mass(pf, cf, 1)
+    J_o, g_o = oadj.gradient(pf, cf, 1, bnd, logk, ustar, mass)
+
+    from jno_b200.autograd import solve_p0
+
+    plan = _plan(p1, tets, 1)
+    m = plan.lumped_mass()
+    assert np.abs(m.cpu().numpy() - mass).max() <= 1e-13 * mass.max()
+    us = torch.as_tensor(ustar, device="cuda")
+    lk = torch.as_tensor(logk, device="cuda").requires_grad_(True)
+    u = solve_p0(plan, lk, tol=1e-13)
+    J = 0.5 * torch.sum(m * (u - us) ** 2)
+    J.backward()
+    g = lk.grad.cpu().numpy()
+    assert abs(J.item() - J_o) <= 1e-10 * abs(J_o)
+    assert np.abs(g - g_o).max() <= 1e-8 * np.abs(g_o).max()
+
+    def Jof(v):
+        with torch.no_grad():
+            uu = solve_p0(plan, torch.as_tensor(v, device="cuda"), tol=1e-14)
+            return (0.5 * torch.sum(m * (uu - us) ** 2)).item()
+
+    rng = np.random.default_rng(5)
+    for c in rng.choice(len(tets), 8, replace=False):
+        e = np.zeros(len(tets))
+        e[c] = 1e-6
+        fd = (Jof(logk + e) - Jof(logk - e)) / 2e-6
+        assert abs(fd - g[c]) <= 1e-6 * np.abs(g).max() + 1e-6 * abs(g[c])
+
+
+def test_status_paths_do_not_fault():
+    pf, cf, tets, p1 = _mesh(4, 1)
+    plan = _plan(p1, tets, 1)
+    lk = torch.zeros(len(tets), dtype=torch.float64, device="cuda")
+    vals, b = plan.assemble(lk)
+    inv = plan.jacobi(vals)
+    # iteration cap -> NOT_CONVERGED status, x written
+    u, it, rel, st = plan.pcg(vals, b, inv_diag=inv, maxiter=1)
+    assert st == 4 and it == 1 and rel > 1e-8
+    # zero right-hand side -> no iteration
+    u, it, rel, st = plan.pcg(vals, torch.zeros_like(b), inv_diag=inv)
+    assert it == 0 and st == 0 and torch.all(u == 0)
+    # negative definite operator -> breakdown reported, no fault
+    from jno_b200._lib import FemkError
+
+    vneg, bneg = plan.assemble(-torch.ones(len(tets), dtype=torch.float64, device="cuda"), mode=1)
+    with pytest.raises(FemkError):
+        plan.pcg(vneg, bneg, inv_diag=None)
+    # out-of-range connectivity is rejected before any indexed access
+    bad = tets.copy()
+    bad[3, 2] = 10**6
+    with pytest.raises(FemkError):
+        _plan(p1, bad, 1)
+    # the guard of _maybe_residual_check raises on a non-solution
+    import jno_b200 as jno
+    from jno_b200.sparse import CsrMatrix
+
+    A = CsrMatrix(plan, vals)
+    with pytest.raises(RuntimeError, match="did not solve"):
+        jno.solve.cg(maxiter=1)(A, b, M=jno.precond.jacobi())
+
+
+def test_jno_surface_end_to_end():
+    """The reference recipe (tests/test_topology_optimisation.py:176-195 shape) on the B200 path."""
+    import jno_b200 as jno
+
+    n = 8
+    d = jno.domain(jno.domain.equi_distant_box(nx=n, ny=n, nz=n), jitter=0.1, seed=0)
+    u, v = d.fem_symbols()
+    _r, s = d.fem_symbols(space="P0", names=("r", "s"))
+    xi, yi, zi = d.variable("interior", split=True)
+    xb, yb, zb = d.variable("boundary", split=True)
+    ui, vi = u.bind(x=xi, y=yi, z=zi), v.bind(x=xi, y=yi, z=zi)
+    logk = jno.np.parameter(s, name="logk")
+    fem = jno.fem([jno.np.exp(logk) * (ui.x * vi.x + ui.y * vi.y + ui.z * vi.z) - 1.0 * vi, u(xb, yb, zb) - 0.0])
+    assert fem.problem is None and fem.dofs == (n + 1) ** 3
+    lk = om.logk_field(6 * n**3, 1000)
+    A, b = fem.operator.evaluate({"logk": lk})
+    x = jno.solve.cg(tol=1e-8)(A, b, M=jno.precond.jacobi())
+    pf, cf, tets, p1 = _mesh(n, 1)
+    so, _ = _oracle_system(pf, cf, 1, lk)
+    xo = op.pcg(so.csr(), so.b, oa.jacobi_inverse(oa.matrix_diagonal(so)))[0]
+    assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+    idx, data = A.to_bcoo(appended=True)
+    assert idx.shape[0] == A.nnz + plan_dirichlet(fem)
+    xm = jno.solve.cg(tol=1e-8, precision="mixed")(A, b, M=jno.precond.jacobi())
+    assert np.linalg.norm(xm.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+    Amf, bmf = fem.matrix_free({"logk": lk})
+    xf = jno.solve.cg(tol=1e-8)(Amf, bmf, M=jno.precond.jacobi())
+    assert np.linalg.norm(xf.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+
+
+def plan_dirichlet(fem):
+    return fem.plan.n_dirichlet
