@@ -147,6 +147,24 @@ int femk_pcg_matfree(const femk_plan* plan, const double* param_dev, int coef_mo
                      double atol, int32_t maxiter, int32_t* iters_out, double* relres_out, void* stream);
 
 /*
+ * Allocation-free Jacobi-PCG: the same iteration and result as femk_pcg, for callers that must
+ * not allocate device memory during the call -- an XLA FFI handler (device memory is owned by XLA's
+ * allocator), a framework whose caching allocator already holds nearly all of HBM, or a real-time
+ * loop with a fixed memory budget. The plan (built once at set-up) and the caller's vectors are
+ * the only other memory used; it calls no cudaMalloc/cudaFree and no allocating library routine.
+ * Its workspace is one file-scope device array sized for FEMK_NOALLOC_MAX_N DOFs (about 8.5 MB),
+ * which every GPU that loads the library holds until the process exits. Larger systems are
+ * rejected with FEMK_EINVAL. The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) with the plan's device current; make that first call before any stream
+ * capture. All calls share the array, so calls that overlap on the GPU (two streams, two
+ * threads) race and must be serialised by the caller. No counterpart in the reference.
+ */
+#define FEMK_NOALLOC_MAX_N 262144
+int femk_pcg_noalloc(const femk_plan* plan, const double* vals_dev, const double* b_dev, double* x_dev,
+                     const double* inv_diag_dev, double tol, double atol, int32_t maxiter, int32_t* iters_out,
+                     double* relres_out, void* stream);
+
+/*
  * Mixed precision: inner CG on FP32 values and vectors, FP64 outer residual b - A x with the FP64
  * values and an FP64 solution. Converges to the same stopping rule as femk_pcg (on the true FP64
  * residual). mode = FEMK_MIXED_*. inner_iters_out counts FP32 iterations, outer_out FP64

@@ -13,6 +13,8 @@
 // M = jno.precond.jacobi() (jno/precond.py:106-111) and LinearOperator.mv (solver_api.py:137-148).
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <string>
 
 #include "femk_element.cuh"
 #include "femk_internal.cuh"
@@ -609,4 +611,148 @@ extern "C" int femk_pcg_matfree(const femk_plan* p, const double* param, int mod
   FEMK_CHECK_ARG(mode >= 0 && mode <= 2 && (mode == 2 || param), "femk_pcg_matfree: bad coefficient");
   MatFree m{param, mode, scale};
   return pcg_run(p, nullptr, &m, b, x, dinv, tol, atol, maxiter, iters_out, relres_out, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free PCG. Same kernels and the same iteration as femk_pcg, but the solver vectors,
+// the reduction partials and the solver state live in one file-scope device array instead of
+// plan-owned cudaMalloc'd workspace, and the host loop uses no events and no pinned memory.
+// For callers that must not allocate device memory while they run: code inside an XLA FFI
+// handler (device memory belongs to XLA's allocator), frameworks whose caching allocator already
+// holds nearly all of HBM, and real-time loops with a fixed memory budget.
+// ---------------------------------------------------------------------------------------------
+namespace femk {
+namespace {
+
+constexpr int64_t kNoAllocMaxN = FEMK_NOALLOC_MAX_N;
+constexpr int64_t kNoAllocPartials = 3 * 4096;  // NV <= 3 values per block, up to 4096 blocks
+constexpr int64_t kNoAllocStateDoubles = (sizeof(CgState) + sizeof(double) - 1) / sizeof(double);
+constexpr int64_t kNoAllocDoubles = 4 * kNoAllocMaxN + kNoAllocPartials + kNoAllocStateDoubles;
+
+// 4 vectors of kNoAllocMaxN doubles (r, z, p, q) + reduction partials + CgState: about 8.5 MB,
+// held by every device that loads the library until the process exits. Shared by every call.
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+// Device address of g_noalloc_scratch per device, looked up once with that device current.
+constexpr int kMaxDevices = 64;
+static double* g_noalloc_addr[kMaxDevices] = {};
+static std::mutex g_noalloc_mu;
+
+int noalloc_scratch(int device, double** out) {
+  if (device < 0 || device >= kMaxDevices) {
+    set_error("femk_pcg_noalloc: device index out of range");
+    return FEMK_EINVAL;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void* addr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (e != cudaSuccess || addr == nullptr) {
+      set_error(std::string("femk_pcg_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+      return FEMK_ECUDA;
+    }
+    g_noalloc_addr[device] = (double*)addr;
+  }
+  *out = g_noalloc_addr[device];
+  return FEMK_OK;
+}
+
+template <int MODE>
+int launch_csr_into(const femk_plan* p, const double* vals, const double* x, double* y, const double* b,
+                    const double* dinv, double* z, double* pout, double* partials, CgState* st, double tol2,
+                    double atol2, cudaStream_t s) {
+  const int grid = spmv_grid(p);
+  switch (lanes_for(p)) {
+    case 4:
+      k_csr<4, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, partials, st, tol2, atol2);
+      break;
+    case 8:
+      k_csr<8, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, partials, st, tol2, atol2);
+      break;
+    case 16:
+      k_csr<16, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, partials, st, tol2, atol2);
+      break;
+    default:
+      k_csr<32, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, partials, st, tol2, atol2);
+  }
+  FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}
+
+}  // namespace
+}  // namespace femk
+
+extern "C" int femk_pcg_noalloc(const femk_plan* p, const double* vals, const double* b, double* x,
+                                const double* dinv, double tol, double atol, int32_t maxiter, int32_t* iters_out,
+                                double* relres_out, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && vals && b && x, "femk_pcg_noalloc: NULL argument");
+  FEMK_CHECK_ARG(tol >= 0.0 && atol >= 0.0, "femk_pcg_noalloc: negative tolerance");
+  if (p->n > kNoAllocMaxN) {
+    set_error("femk_pcg_noalloc: the system has " + std::to_string(p->n) + " DOFs; this entry point holds at most " +
+              std::to_string(kNoAllocMaxN) + " (FEMK_NOALLOC_MAX_N). Use femk_pcg for larger systems.");
+    return FEMK_EINVAL;
+  }
+  FEMK_CHECK_ARG((int64_t)spmv_grid(p) * 3 <= kNoAllocPartials && (int64_t)p->n_sm * 8 * 3 <= kNoAllocPartials,
+                 "femk_pcg_noalloc: too many SMs for the static reduction scratch");
+  int cur = -1;
+  FEMK_CUDA_TRY(cudaGetDevice(&cur));
+  FEMK_CHECK_ARG(cur == p->device, "femk_pcg_noalloc: make the plan's device current before the call");
+  double* scratch = nullptr;
+  FEMK_TRY(noalloc_scratch(cur, &scratch));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t n = p->n;
+  double* r = scratch;
+  double* z = r + kNoAllocMaxN;
+  double* pv = z + kNoAllocMaxN;
+  double* q = pv + kNoAllocMaxN;
+  double* partials = q + kNoAllocMaxN;
+  CgState* st = (CgState*)(partials + kNoAllocPartials);
+  // the state of the previous call is overwritten before any kernel reads it (ticket = 0 included)
+  CgState init{};
+  init.maxiter = maxiter;
+  init.precond = dinv ? 1 : 0;
+  FEMK_CUDA_TRY(cudaMemcpyAsync(st, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
+  const double tol2 = tol * tol, atol2 = atol * atol;
+  const int vgrid = p->n_sm * (2048 / kThreads);
+  FEMK_TRY(launch_csr_into<kInit>(p, vals, x, r, b, dinv, z, pv, partials, st, tol2, atol2, s));
+  CgState h{};
+  int64_t enq = 0;
+  while (enq < maxiter) {
+    const int64_t todo = std::min<int64_t>(kChunk, (int64_t)maxiter - enq);
+    for (int64_t it = 0; it < todo; ++it) {
+      FEMK_TRY(launch_csr_into<kCgStep>(p, vals, pv, q, nullptr, nullptr, nullptr, nullptr, partials, st, 0.0, 0.0, s));
+      k_update<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, x, r, z, pv, q, dinv, partials, st);
+      k_pupdate<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, pv, z, st);
+    }
+    FEMK_CUDA_TRY(cudaGetLastError());
+    enq += todo;
+    FEMK_CUDA_TRY(cudaMemcpyAsync(&h, st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+    FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h.done) break;
+  }
+  FEMK_CUDA_TRY(cudaMemcpyAsync(&h, st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  if (iters_out) *iters_out = h.iter;
+  const CgState fin = h;
+  if (relres_out) {
+    FEMK_TRY(launch_csr_into<kResid>(p, vals, x, nullptr, b, nullptr, nullptr, nullptr, partials, st, 0.0, 0.0, s));
+    FEMK_CUDA_TRY(cudaMemcpyAsync(&h, st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+    FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+    *relres_out = std::sqrt(h.pq) / (std::sqrt(h.bb) + 1e-30);
+  }
+  if (fin.status == FEMK_BREAKDOWN) {
+    set_error("femk_pcg_noalloc: <p, A p> <= 0 (operator not symmetric positive definite)");
+    return FEMK_BREAKDOWN;
+  }
+  if (fin.status == FEMK_NONFINITE) {
+    set_error("femk_pcg_noalloc: non-finite value in a CG reduction");
+    return FEMK_NONFINITE;
+  }
+  const double rs = fin.precond ? fin.rr : fin.gamma;
+  if (rs > fin.atol2) {
+    set_error("femk_pcg_noalloc: iteration cap reached above tolerance");
+    return FEMK_NOT_CONVERGED;
+  }
+  return FEMK_OK;
 }
