@@ -125,6 +125,12 @@ int femk_jacobi_matfree(const femk_plan* plan, const double* param_dev, int coef
 int femk_spmv(const femk_plan* plan, const double* vals_dev, const double* x_dev, double* y_dev,
               void* stream);
 
+/* Gather CSR values into the solver's sliced-ELL copy held by the plan (32-row slices, column-major,
+ * thread per row). femk_pcg does this itself at the start of every solve; this entry point and
+ * femk_spmv_prepared expose the operator each PCG iteration multiplies with. No reference counterpart. */
+int femk_prepare_operator(const femk_plan* plan, const double* vals_dev, void* stream);
+int femk_spmv_prepared(const femk_plan* plan, const double* x_dev, double* y_dev, void* stream);
+
 /* y = A x without an assembled matrix: per-element K_e x_e from coordinates and k_e. */
 int femk_spmv_matfree(const femk_plan* plan, const double* param_dev, int coef_mode,
                       double coef_scale, const double* x_dev, double* y_dev, void* stream);

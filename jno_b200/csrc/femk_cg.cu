@@ -18,6 +18,7 @@
 
 #include "femk_element.cuh"
 #include "femk_internal.cuh"
+#include "femk_spmv.cuh"
 
 namespace femk {
 namespace {
@@ -86,31 +87,14 @@ __device__ __forceinline__ bool grid_finish(double* partials, uint32_t* ticket, 
   return true;
 }
 
-// ---------------------------------------------------------------------------------------------
-// CSR row sum: L lanes per row, rows of a warp processed together (shuffles stay converged)
-// ---------------------------------------------------------------------------------------------
-template <int L>
-__device__ __forceinline__ double csr_row(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
-                                          const double* __restrict__ vals, const double* __restrict__ x, int64_t row,
-                                          bool valid, int sub) {
-  double s = 0.0;
-  if (valid) {
-    const int32_t beg = __ldg(indptr + row), end = __ldg(indptr + row + 1);
-    for (int32_t k = beg + sub; k < end; k += L) s += __ldcs(vals + k) * __ldg(x + __ldcs(indices + k));
-  }
-#pragma unroll
-  for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  return s;
-}
-
 enum SpmvMode { kPlain = 0, kCgStep = 1, kInit = 2, kResid = 3 };
 
-// One kernel for every CSR-SpMV use of the solver:
+// One kernel for every CSR-SpMV use of the solver (L lanes per row, U rows in flight per lane group):
 //  kPlain : y = A x
 //  kCgStep: q = A p, <p, q>                     (finish: alpha)
 //  kInit  : r = b - A x, z = D^-1 r, p = z, <r,z>, <r,r>, <b,b>   (finish: gamma, rr, atol2, done)
 //  kResid : w = b - A x, <w,w>, <b,b>           (finish: stored in st->pq / st->bb)
-template <int L, int MODE>
+template <int L, int U, int MODE>
 __global__ void __launch_bounds__(kThreads) k_csr(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
                                                  const double* __restrict__ vals, int64_t n, const double* __restrict__ x,
                                                  double* __restrict__ y, const double* __restrict__ b,
@@ -123,23 +107,26 @@ __global__ void __launch_bounds__(kThreads) k_csr(const int32_t* __restrict__ in
   const int sub = lane % L;
   const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
-  constexpr int RPW = 32 / L;  // rows per warp step
+  constexpr int RPW = 32 / L;  // rows per lane-group step
   double acc[NV];
 #pragma unroll
   for (int j = 0; j < NV; ++j) acc[j] = 0.0;
-  for (int64_t base = warp * RPW; base < n; base += nwarps * RPW) {
-    const int64_t row = base + lane / L;
-    const bool valid = row < n;
-    const double s = csr_row<L>(indptr, indices, vals, x, row, valid, sub);
-    if (valid && sub == 0) {
+  for (int64_t base = warp * RPW * U; base < n; base += nwarps * RPW * U) {
+    double s[U];
+    int64_t rows[U];
+    csr_rows<L, U, double, int32_t>(indptr, indices, vals, x, n, base, lane, s, rows);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t row = rows[u];
+      if (row >= n || sub != 0) continue;
       if (MODE == kPlain) {
-        y[row] = s;
+        y[row] = s[u];
       } else if (MODE == kCgStep) {
-        y[row] = s;
-        acc[0] += __ldg(x + row) * s;
+        y[row] = s[u];
+        acc[0] += __ldg(x + row) * s[u];
       } else if (MODE == kInit) {
         const double bi = b[row];
-        const double ri = bi - s;
+        const double ri = bi - s[u];
         const double zi = dinv ? dinv[row] * ri : ri;
         y[row] = ri;
         z[row] = zi;
@@ -149,7 +136,7 @@ __global__ void __launch_bounds__(kThreads) k_csr(const int32_t* __restrict__ in
         acc[2] += bi * bi;
       } else {
         const double bi = b[row];
-        const double wi = bi - s;
+        const double wi = bi - s[u];
         acc[0] += wi * wi;
         acc[1] += bi * bi;
       }
@@ -180,9 +167,96 @@ __global__ void __launch_bounds__(kThreads) k_csr(const int32_t* __restrict__ in
     const double rs = st->precond ? tot[1] : tot[0];
     st->done = (!(rs > st->atol2) || st->maxiter <= 0 || st->status != FEMK_OK) ? 1 : 0;
     st->rr_since = tot[1];
+    st->beta = 0.0;
   } else {
     st->pq = tot[0];
     st->bb = tot[1];
+  }
+}
+
+// The same modes on the sliced-ELL copy of the operator: one thread per row, 32-row slices.
+template <int MODE, typename IDX>
+__global__ void __launch_bounds__(kThreads) k_sell(const int64_t* __restrict__ sptr, const IDX* __restrict__ scols,
+                                                  const double* __restrict__ svals, int64_t n, int64_t nslices,
+                                                  const double* __restrict__ x, double* __restrict__ y,
+                                                  const double* __restrict__ b, const double* __restrict__ dinv,
+                                                  double* __restrict__ z, double* __restrict__ pout,
+                                                  double* __restrict__ partials, CgState* st, double tol2,
+                                                  double atol2) {
+  constexpr int NV = MODE == kPlain ? 1 : (MODE == kCgStep ? 1 : (MODE == kInit ? 3 : 2));
+  if (MODE == kCgStep && st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
+  double acc[NV];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+  for (int64_t sl = warp; sl < nslices; sl += nwarps) {
+    const int64_t row = sl * 32 + lane;
+    if (row >= n) continue;
+    const int64_t b0 = __ldg(sptr + sl);
+    const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
+    const double sv = sell_row(svals, scols, b0 + lane, w, row, GatherX<double>{x});
+    if (MODE == kPlain) {
+      y[row] = sv;
+    } else if (MODE == kCgStep) {
+      y[row] = sv;
+      acc[0] += __ldg(x + row) * sv;
+    } else if (MODE == kInit) {
+      const double bi = b[row];
+      const double ri = bi - sv;
+      const double zi = dinv ? dinv[row] * ri : ri;
+      y[row] = ri;
+      z[row] = zi;
+      pout[row] = zi;
+      acc[0] += ri * zi;
+      acc[1] += ri * ri;
+      acc[2] += bi * bi;
+    } else {
+      const double bi = b[row];
+      const double wi = bi - sv;
+      acc[0] += wi * wi;
+      acc[1] += bi * bi;
+    }
+  }
+  if (MODE == kPlain) return;
+  block_reduce_store<NV>(acc, partials);
+  double tot[NV];
+  if (!grid_finish<NV>(partials, &st->ticket, tot)) return;
+  if (threadIdx.x != 0) return;
+  if (MODE == kCgStep) {
+    st->pq = tot[0];
+    st->alpha = st->gamma / tot[0];
+    if (!isfinite(tot[0])) {
+      st->status = FEMK_NONFINITE;
+      st->done = 1;
+    } else if (!(tot[0] > 0.0)) {
+      st->status = FEMK_BREAKDOWN;
+      st->done = 1;
+    }
+  } else if (MODE == kInit) {
+    st->gamma = tot[0];
+    st->rr = tot[1];
+    st->bb = tot[2];
+    st->atol2 = fmax(tol2 * tot[2], atol2);
+    st->iter = 0;
+    st->status = isfinite(tot[0]) && isfinite(tot[1]) ? FEMK_OK : FEMK_NONFINITE;
+    const double rs = st->precond ? tot[1] : tot[0];
+    st->done = (!(rs > st->atol2) || st->maxiter <= 0 || st->status != FEMK_OK) ? 1 : 0;
+    st->rr_since = tot[1];
+    st->beta = 0.0;
+  } else {
+    st->pq = tot[0];
+    st->bb = tot[1];
+  }
+}
+
+template <typename T>
+__global__ void k_sell_gather(const int32_t* __restrict__ src, int64_t m, const double* __restrict__ vals,
+                              T* __restrict__ out) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t k = __ldcs(src + j);
+    out[j] = k >= 0 ? (T)__ldcs(vals + k) : T(0);
   }
 }
 
@@ -228,6 +302,53 @@ __global__ void __launch_bounds__(kThreads) k_pupdate(int64_t n, double* __restr
   const double beta = st->beta;
   for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads)
     p[i] = z[i] + beta * p[i];
+}
+
+// CG step with the direction update folded in: p_new = z + beta p_old is formed at every gather
+// (and stored by the row's owner), q = A p_new, <p_new, q> -> alpha. Double-buffered p, so no
+// separate p-update pass and no grid-wide wait between the two.
+template <int L, int U>
+__global__ void __launch_bounds__(kThreads) k_cg_step(const int32_t* __restrict__ indptr,
+                                                     const int32_t* __restrict__ indices,
+                                                     const double* __restrict__ vals, int64_t n,
+                                                     const double* __restrict__ z, const double* __restrict__ pold,
+                                                     double* __restrict__ pnew, double* __restrict__ q,
+                                                     double* __restrict__ partials, CgState* st) {
+  if (st->done) return;
+  const GatherDirection g{z, pold, st->beta};
+  const int lane = threadIdx.x & 31;
+  const int sub = lane % L;
+  const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
+  constexpr int RPW = 32 / L;
+  double acc[1] = {0.0};
+  for (int64_t base = warp * RPW * U; base < n; base += nwarps * RPW * U) {
+    double sv[U];
+    int64_t rows[U];
+    csr_rows_g<L, U, double, int32_t>(indptr, indices, vals, g, n, base, lane, sv, rows);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t row = rows[u];
+      if (row >= n || sub != 0) continue;
+      const double pn = g(row);
+      pnew[row] = pn;
+      q[row] = sv[u];
+      acc[0] += pn * sv[u];
+    }
+  }
+  block_reduce_store<1>(acc, partials);
+  double tot[1];
+  if (!grid_finish<1>(partials, &st->ticket, tot)) return;
+  if (threadIdx.x != 0) return;
+  st->pq = tot[0];
+  st->alpha = st->gamma / tot[0];
+  if (!isfinite(tot[0])) {
+    st->status = FEMK_NONFINITE;
+    st->done = 1;
+  } else if (!(tot[0] > 0.0)) {
+    st->status = FEMK_BREAKDOWN;
+    st->done = 1;
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -384,33 +505,48 @@ __global__ void k_invert_diag(double* __restrict__ d, int64_t n, const uint8_t* 
 // ---------------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------------
-int lanes_for(const femk_plan* p) {
-  const double avg = p->n > 0 ? (double)p->nnz / (double)p->n : 1.0;
-  if (avg <= 5.0) return 4;
-  if (avg <= 10.0) return 8;
-  if (avg <= 20.0) return 16;
-  return 32;
-}
-
 int spmv_grid(const femk_plan* p) { return p->n_sm * (2048 / kThreads); }
+
+template <int MODE>
+int launch_csr_p(const femk_plan* p, const double* vals, const double* x, double* y, const double* b,
+                 const double* dinv, double* z, double* pout, double* partials, CgState* st, double tol2, double atol2,
+                 cudaStream_t s) {
+  const bool ok = with_spmv_cfg(p->spmv_L, p->spmv_U, [&](auto Lc, auto Uc) {
+    constexpr int L = decltype(Lc)::value, U = decltype(Uc)::value;
+    const int grid = wave_grid(k_csr<L, U, MODE>, kThreads, p);
+    k_csr<L, U, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b,
+                                                                           dinv, z, pout, partials, st, tol2, atol2);
+  });
+  if (!ok) {
+    set_error("unsupported SpMV configuration");
+    return FEMK_EINVAL;
+  }
+  FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}
 
 template <int MODE>
 int launch_csr(const femk_plan* p, const double* vals, const double* x, double* y, const double* b, const double* dinv,
                double* z, double* pout, CgState* st, double tol2, double atol2, cudaStream_t s) {
-  const int grid = spmv_grid(p);
-  switch (lanes_for(p)) {
-    case 4:
-      k_csr<4, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
-      break;
-    case 8:
-      k_csr<8, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
-      break;
-    case 16:
-      k_csr<16, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
-      break;
-    default:
-      k_csr<32, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
-  }
+  return launch_csr_p<MODE>(p, vals, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2, s);
+}
+
+// The operator of a solve: the sliced-ELL copy (values gathered by prepare_sell) or the CSR.
+template <int MODE>
+int launch_op(const femk_plan* p, bool sell, const double* vals, const double* x, double* y, const double* b,
+              const double* dinv, double* z, double* pout, CgState* st, double tol2, double atol2, cudaStream_t s) {
+  if (!sell) return launch_csr<MODE>(p, vals, x, y, b, dinv, z, pout, st, tol2, atol2, s);
+  const int grid = wave_grid(k_sell<MODE, int32_t>, kThreads, p);
+  k_sell<MODE, int32_t><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
+      p->sell_ptr, p->sell_cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}
+
+int prepare_sell(femk_plan* p, const double* vals, cudaStream_t s) {
+  if (!p->sell_vals) FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals, sizeof(double) * (p->sell_nnz + 1)));
+  k_sell_gather<double><<<::femk::counted_launch() + p->n_sm * 8, 256, 0, s>>>(p->sell_src, p->sell_nnz, vals,
+                                                                              p->sell_vals);
   FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;
 }
@@ -444,82 +580,200 @@ int launch_matfree(const femk_plan* p, const MatFree& m, const double* x, double
   return FEMK_OK;
 }
 
-int pcg_run(const femk_plan* p, const double* vals, const MatFree* mf, const double* b, double* x, const double* dinv,
+// One chunk of kChunk CG iterations on stream ws (CSR operator). Fused: 2 kernels per iteration
+// with the direction double-buffered in P0/P1 (chunks have even length, so every chunk starts
+// with p in P0); otherwise the three-kernel form.
+int enqueue_chunk(const femk_plan* p, const double* vals, double* x, const double* dinv, bool fused, bool sell,
+                  int64_t iters, cudaStream_t ws) {
+  const int64_t n = p->n;
+  double* r = p->work;
+  double* z = r + n;
+  double* P0 = z + n;
+  double* q = P0 + n;
+  double* P1 = q + n;
+  CgState* st = p->state;
+  for (int64_t it = 0; it < iters; ++it) {
+    if (fused) {
+      double* pold = (it & 1) ? P1 : P0;
+      double* pnew = (it & 1) ? P0 : P1;
+      const bool ok = with_spmv_cfg(p->spmv_L, p->spmv_U, [&](auto Lc, auto Uc) {
+        constexpr int L = decltype(Lc)::value, U = decltype(Uc)::value;
+        k_cg_step<L, U><<<::femk::counted_launch() + wave_grid(k_cg_step<L, U>, kThreads, p), kThreads, 0, ws>>>(
+            p->indptr, p->indices, vals, n, z, pold, pnew, q, p->partials, st);
+      });
+      if (!ok) {
+        set_error("unsupported SpMV configuration");
+        return FEMK_EINVAL;
+      }
+      k_update<<<::femk::counted_launch() + wave_grid(k_update, kThreads, p), kThreads, 0, ws>>>(n, x, r, z, pnew, q,
+                                                                                               dinv, p->partials, st);
+    } else {
+      FEMK_TRY(launch_op<kCgStep>(p, sell, vals, P0, q, nullptr, nullptr, nullptr, nullptr, st, 0.0, 0.0, ws));
+      k_update<<<::femk::counted_launch() + wave_grid(k_update, kThreads, p), kThreads, 0, ws>>>(n, x, r, z, P0, q,
+                                                                                               dinv, p->partials, st);
+      k_pupdate<<<::femk::counted_launch() + wave_grid(k_pupdate, kThreads, p), kThreads, 0, ws>>>(n, P0, z, st);
+    }
+  }
+  FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}
+
+// Capture one chunk into a CUDA graph (re-captured when the operand pointers change).
+int ensure_chunk_graph(femk_plan* p, const double* vals, double* x, const double* dinv, bool fused, bool sell) {
+  if (sell && !p->sell_vals) {
+    set_error("femk_pcg: sliced-ELL values missing at graph capture");
+    return FEMK_EINVAL;
+  }
+  const void* key[5] = {vals, x, dinv, (const void*)(intptr_t)((fused ? 1 : 2) + (sell ? 4 : 0)), p->sell_vals};
+  bool same = p->cg_exec != nullptr;
+  for (int i = 0; i < 5; ++i) same = same && key[i] == p->cg_key[i];
+  if (same) return FEMK_OK;
+  // occupancy queries happen before capture begins
+  with_spmv_cfg(p->spmv_L, p->spmv_U, [&](auto Lc, auto Uc) {
+    constexpr int L = decltype(Lc)::value, U = decltype(Uc)::value;
+    (void)wave_grid(k_cg_step<L, U>, kThreads, p);
+    (void)wave_grid(k_csr<L, U, kCgStep>, kThreads, p);
+  });
+  (void)wave_grid(k_sell<kCgStep, int32_t>, kThreads, p);
+  (void)wave_grid(k_update, kThreads, p);
+  (void)wave_grid(k_pupdate, kThreads, p);
+  cudaGraph_t g = nullptr;
+  set_capturing(true);
+  cudaError_t e = cudaStreamBeginCapture(p->cg_stream, cudaStreamCaptureModeThreadLocal);
+  int st = e == cudaSuccess ? enqueue_chunk(p, vals, x, dinv, fused, sell, kChunk, p->cg_stream) : FEMK_ECUDA;
+  const cudaError_t e2 = cudaStreamEndCapture(p->cg_stream, &g);
+  set_capturing(false);
+  if (e != cudaSuccess || e2 != cudaSuccess || st != FEMK_OK) {
+    if (g) cudaGraphDestroy(g);
+    set_error(std::string("femk_pcg: graph capture failed: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+    return st != FEMK_OK ? st : FEMK_ECUDA;
+  }
+  bool updated = false;
+  if (p->cg_exec) {
+    cudaGraphExecUpdateResultInfo info;
+    updated = cudaGraphExecUpdate(p->cg_exec, g, &info) == cudaSuccess;
+    if (!updated) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(p->cg_exec);
+      p->cg_exec = nullptr;
+    }
+  }
+  if (!updated) {
+    const cudaError_t e3 = cudaGraphInstantiate(&p->cg_exec, g, 0);
+    if (e3 != cudaSuccess) {
+      cudaGraphDestroy(g);
+      p->cg_exec = nullptr;
+      set_error(std::string("femk_pcg: graph instantiation failed: ") + cudaGetErrorString(e3));
+      return FEMK_ECUDA;
+    }
+  }
+  cudaGraphDestroy(g);
+  for (int i = 0; i < 5; ++i) p->cg_key[i] = key[i];
+  p->cg_nodes = (fused ? 2 : 3) * kChunk;
+  return FEMK_OK;
+}
+
+int ensure_cg_stream(femk_plan* p) {
+  if (p->cg_stream) return FEMK_OK;
+  FEMK_CUDA_TRY(cudaStreamCreateWithFlags(&p->cg_stream, cudaStreamNonBlocking));
+  for (int i = 0; i < 3; ++i) FEMK_CUDA_TRY(cudaEventCreateWithFlags(&p->cg_ev[i], cudaEventDisableTiming));
+  return FEMK_OK;
+}
+
+int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const double* b, double* x, const double* dinv,
             double tol, double atol, int32_t maxiter, int32_t* iters_out, double* relres_out, cudaStream_t s) {
-  FEMK_TRY(ensure_workspace(const_cast<femk_plan*>(p)));
+  femk_plan* p = const_cast<femk_plan*>(pc);
+  FEMK_TRY(ensure_workspace(p));
+  FEMK_TRY(ensure_cg_stream(p));
   const int64_t n = p->n;
   double* r = p->work;
   double* z = r + n;
   double* pv = z + n;
   double* q = pv + n;
   CgState* st = p->state;
+  const bool fused = !mf && p->cg_fused;
+  const bool graph = !mf && p->cg_graph;
+  const bool sell = !mf && !fused && p->use_sell && p->sell_src;
+  // all solver work runs on the plan's stream, ordered after the caller's stream and before
+  // whatever the caller enqueues next
+  cudaStream_t ws = p->cg_stream;
+  FEMK_CUDA_TRY(cudaEventRecord(p->cg_ev[2], s));
+  FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->cg_ev[2], 0));
+  // the sliced-ELL values buffer must exist before a graph that reads it is captured
+  if (sell) FEMK_TRY(prepare_sell(p, vals, ws));
+  if (graph) FEMK_TRY(ensure_chunk_graph(p, vals, x, dinv, fused, sell));
   CgState init{};
   init.maxiter = maxiter;
   init.precond = dinv ? 1 : 0;
-  FEMK_CUDA_TRY(cudaMemcpyAsync(st, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
+  FEMK_CUDA_TRY(cudaMemcpyAsync(st, &init, sizeof(CgState), cudaMemcpyHostToDevice, ws));
   const double tol2 = tol * tol, atol2 = atol * atol;
-  const int vgrid = p->n_sm * (2048 / kThreads);
   if (mf) {
-    FEMK_TRY(launch_matfree(p, *mf, x, q, s));
-    k_init_from_ax<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, b, q, dinv, r, z, pv, p->partials, st, tol2, atol2);
+    FEMK_TRY(launch_matfree(p, *mf, x, q, ws));
+    k_init_from_ax<<<::femk::counted_launch() + wave_grid(k_init_from_ax, kThreads, p), kThreads, 0, ws>>>(
+        n, b, q, dinv, r, z, pv, p->partials, st, tol2, atol2);
   } else {
-    FEMK_TRY(launch_csr<kInit>(p, vals, x, r, b, dinv, z, pv, st, tol2, atol2, s));
+    FEMK_TRY(launch_op<kInit>(p, sell, vals, x, r, b, dinv, z, pv, st, tol2, atol2, ws));
   }
   FEMK_CUDA_TRY(cudaGetLastError());
-  cudaEvent_t ev[2];
-  FEMK_CUDA_TRY(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-  FEMK_CUDA_TRY(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
   CgState* hs = p->state_host;
   int status = FEMK_OK;
   int64_t enq = 0;  // iterations enqueued
   int chunk_id = 0;
   bool have_prev = false;
   while (true) {
-    // enqueue one chunk
-    const int64_t todo = std::min<int64_t>(kChunk, (int64_t)maxiter - enq);
-    for (int64_t it = 0; it < todo; ++it) {
-      if (mf) {
-        FEMK_TRY(launch_matfree(p, *mf, pv, q, s, st));
-        k_dot_pq<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, pv, q, p->partials, st);
-      } else {
-        FEMK_TRY(launch_csr<kCgStep>(p, vals, pv, q, nullptr, nullptr, nullptr, nullptr, st, 0.0, 0.0, s));
+    if (graph) {
+      FEMK_CUDA_TRY(cudaGraphLaunch(p->cg_exec, ws));
+      count_launches(p->cg_nodes);
+      enq += kChunk;  // iterations past convergence or maxiter return at entry
+    } else if (mf) {
+      const int64_t todo = std::min<int64_t>(kChunk, (int64_t)maxiter - enq);
+      for (int64_t it = 0; it < todo; ++it) {
+        FEMK_TRY(launch_matfree(p, *mf, pv, q, ws, st));
+        k_dot_pq<<<::femk::counted_launch() + wave_grid(k_dot_pq, kThreads, p), kThreads, 0, ws>>>(n, pv, q,
+                                                                                                  p->partials, st);
+        k_update<<<::femk::counted_launch() + wave_grid(k_update, kThreads, p), kThreads, 0, ws>>>(
+            n, x, r, z, pv, q, dinv, p->partials, st);
+        k_pupdate<<<::femk::counted_launch() + wave_grid(k_pupdate, kThreads, p), kThreads, 0, ws>>>(n, pv, z, st);
       }
-      k_update<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, x, r, z, pv, q, dinv, p->partials, st);
-      k_pupdate<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, pv, z, st);
+      FEMK_CUDA_TRY(cudaGetLastError());
+      enq += todo;
+    } else {
+      const int64_t todo = std::min<int64_t>(kChunk, (int64_t)maxiter - enq);
+      FEMK_TRY(enqueue_chunk(p, vals, x, dinv, fused, sell, todo, ws));
+      enq += todo;
     }
-    FEMK_CUDA_TRY(cudaGetLastError());
-    enq += todo;
     CgState* slot_h = hs + (chunk_id & 1);
-    FEMK_CUDA_TRY(cudaMemcpyAsync(slot_h, st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
-    FEMK_CUDA_TRY(cudaEventRecord(ev[chunk_id & 1], s));
+    FEMK_CUDA_TRY(cudaMemcpyAsync(slot_h, st, sizeof(CgState), cudaMemcpyDeviceToHost, ws));
+    FEMK_CUDA_TRY(cudaEventRecord(p->cg_ev[chunk_id & 1], ws));
     // look at the previous chunk's flag while this one runs
     if (have_prev) {
-      FEMK_CUDA_TRY(cudaEventSynchronize(ev[(chunk_id - 1) & 1]));
+      FEMK_CUDA_TRY(cudaEventSynchronize(p->cg_ev[(chunk_id - 1) & 1]));
       if (hs[(chunk_id - 1) & 1].done) break;
     }
     have_prev = true;
     if (enq >= maxiter) break;
     ++chunk_id;
   }
-  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
-  cudaEventDestroy(ev[0]);
-  cudaEventDestroy(ev[1]);
+  FEMK_CUDA_TRY(cudaStreamSynchronize(ws));
   CgState fin{};
   FEMK_CUDA_TRY(cudaMemcpy(&fin, st, sizeof(CgState), cudaMemcpyDeviceToHost));
-  // the final chunk may have ended exactly at maxiter without the flag being observed: fin is exact
   if (iters_out) *iters_out = fin.iter;
   if (fin.status != FEMK_OK) status = fin.status;
   if (relres_out) {
     if (mf) {
-      FEMK_TRY(launch_matfree(p, *mf, x, q, s));
-      k_resid_from_ax<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, b, q, p->partials, st);
+      FEMK_TRY(launch_matfree(p, *mf, x, q, ws));
+      k_resid_from_ax<<<::femk::counted_launch() + wave_grid(k_resid_from_ax, kThreads, p), kThreads, 0, ws>>>(
+          n, b, q, p->partials, st);
     } else {
-      FEMK_TRY(launch_csr<kResid>(p, vals, x, nullptr, b, nullptr, nullptr, nullptr, st, 0.0, 0.0, s));
+      FEMK_TRY(launch_op<kResid>(p, sell, vals, x, nullptr, b, nullptr, nullptr, nullptr, st, 0.0, 0.0, ws));
     }
-    FEMK_CUDA_TRY(cudaMemcpyAsync(hs, st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
-    FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+    FEMK_CUDA_TRY(cudaMemcpyAsync(hs, st, sizeof(CgState), cudaMemcpyDeviceToHost, ws));
+    FEMK_CUDA_TRY(cudaStreamSynchronize(ws));
     *relres_out = std::sqrt(hs->pq) / (std::sqrt(hs->bb) + 1e-30);
   }
+  // the caller's stream continues after the solve
+  FEMK_CUDA_TRY(cudaEventRecord(p->cg_ev[2], ws));
+  FEMK_CUDA_TRY(cudaStreamWaitEvent(s, p->cg_ev[2], 0));
   if (status == FEMK_OK) {
     const double rs = fin.precond ? fin.rr : fin.gamma;
     if (rs > fin.atol2) {
@@ -538,7 +792,7 @@ int pcg_run(const femk_plan* p, const double* vals, const MatFree* mf, const dou
 
 int ensure_workspace(femk_plan* p) {
   if (p->work) return FEMK_OK;
-  FEMK_CUDA_TRY(cudaMalloc(&p->work, sizeof(double) * 4 * (p->n + 1)));
+  FEMK_CUDA_TRY(cudaMalloc(&p->work, sizeof(double) * 5 * (p->n + 1)));
   FEMK_CUDA_TRY(cudaMalloc(&p->partials, sizeof(double) * 4 * (int64_t)p->n_sm * 64));
   FEMK_CUDA_TRY(cudaMalloc(&p->state, sizeof(CgState)));
   FEMK_CUDA_TRY(cudaMemset(p->state, 0, sizeof(CgState)));
@@ -566,6 +820,21 @@ extern "C" int femk_spmv(const femk_plan* p, const double* vals, const double* x
   clear_error();
   FEMK_CHECK_ARG(p && vals && x && y, "femk_spmv: NULL argument");
   return spmv_csr(p, vals, x, y, (cudaStream_t)stream);
+}
+
+extern "C" int femk_prepare_operator(const femk_plan* p, const double* vals, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && vals, "femk_prepare_operator: NULL argument");
+  FEMK_CHECK_ARG(p->sell_src, "femk_prepare_operator: the plan has no sliced-ELL layout");
+  return prepare_sell(const_cast<femk_plan*>(p), vals, (cudaStream_t)stream);
+}
+
+extern "C" int femk_spmv_prepared(const femk_plan* p, const double* x, double* y, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && x && y, "femk_spmv_prepared: NULL argument");
+  FEMK_CHECK_ARG(p->sell_vals, "femk_spmv_prepared: call femk_prepare_operator first");
+  return launch_op<kPlain>(p, true, nullptr, x, y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.0, 0.0,
+                           (cudaStream_t)stream);
 }
 
 extern "C" int femk_spmv_matfree(const femk_plan* p, const double* param, int mode, double scale, const double* x,
@@ -661,22 +930,7 @@ template <int MODE>
 int launch_csr_into(const femk_plan* p, const double* vals, const double* x, double* y, const double* b,
                     const double* dinv, double* z, double* pout, double* partials, CgState* st, double tol2,
                     double atol2, cudaStream_t s) {
-  const int grid = spmv_grid(p);
-  switch (lanes_for(p)) {
-    case 4:
-      k_csr<4, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, partials, st, tol2, atol2);
-      break;
-    case 8:
-      k_csr<8, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, partials, st, tol2, atol2);
-      break;
-    case 16:
-      k_csr<16, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, partials, st, tol2, atol2);
-      break;
-    default:
-      k_csr<32, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b, dinv, z, pout, partials, st, tol2, atol2);
-  }
-  FEMK_CUDA_TRY(cudaGetLastError());
-  return FEMK_OK;
+  return launch_csr_p<MODE>(p, vals, x, y, b, dinv, z, pout, partials, st, tol2, atol2, s);
 }
 
 }  // namespace
@@ -714,7 +968,6 @@ extern "C" int femk_pcg_noalloc(const femk_plan* p, const double* vals, const do
   init.precond = dinv ? 1 : 0;
   FEMK_CUDA_TRY(cudaMemcpyAsync(st, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
   const double tol2 = tol * tol, atol2 = atol * atol;
-  const int vgrid = p->n_sm * (2048 / kThreads);
   FEMK_TRY(launch_csr_into<kInit>(p, vals, x, r, b, dinv, z, pv, partials, st, tol2, atol2, s));
   CgState h{};
   int64_t enq = 0;
@@ -722,8 +975,8 @@ extern "C" int femk_pcg_noalloc(const femk_plan* p, const double* vals, const do
     const int64_t todo = std::min<int64_t>(kChunk, (int64_t)maxiter - enq);
     for (int64_t it = 0; it < todo; ++it) {
       FEMK_TRY(launch_csr_into<kCgStep>(p, vals, pv, q, nullptr, nullptr, nullptr, nullptr, partials, st, 0.0, 0.0, s));
-      k_update<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, x, r, z, pv, q, dinv, partials, st);
-      k_pupdate<<<::femk::counted_launch() + vgrid, kThreads, 0, s>>>(n, pv, z, st);
+      k_update<<<::femk::counted_launch() + wave_grid(k_update, kThreads, p), kThreads, 0, s>>>(n, x, r, z, pv, q, dinv, partials, st);
+      k_pupdate<<<::femk::counted_launch() + wave_grid(k_pupdate, kThreads, p), kThreads, 0, s>>>(n, pv, z, st);
     }
     FEMK_CUDA_TRY(cudaGetLastError());
     enq += todo;

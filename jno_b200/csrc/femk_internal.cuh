@@ -18,6 +18,10 @@ void clear_error();
 // Every kernel launch of the library is written `k<<<counted_launch() + grid, ...>>>`: the call adds
 // one to a process-wide counter (read by femk_kernel_launches) and returns 0.
 int counted_launch();
+// Launches made while a stream is being captured are not executions: capture brackets its
+// recording with set_capturing(true/false) and each graph launch adds its kernel count.
+void set_capturing(bool on);
+void count_launches(int64_t k);
 
 // Return FEMK_ECUDA with a message if a CUDA runtime call failed.
 #define FEMK_CUDA_TRY(expr)                                                              \
@@ -83,15 +87,39 @@ struct femk_plan {
   int32_t* inc_elem = nullptr;  // i32[ntet*nd]
   int16_t* cols16 = nullptr;    // i16[nnz] col - row, when every entry fits
   int max_row = 0;              // longest CSR row
+  int spmv_L = 16, spmv_U = 2;  // SpMV lanes per row / rows in flight per lane group
+  // sliced-ELL solver layout (SELL-32), built with the pattern
+  int64_t n_slices = 0, sell_nnz = 0;
+  int64_t* sell_ptr = nullptr;   // i64[n_slices+1] first entry of each slice
+  int32_t* sell_src = nullptr;   // i32[sell_nnz] CSR position of each entry, -1 = padding
+  int32_t* sell_cols = nullptr;  // i32[sell_nnz]
+  int16_t* sell_c16 = nullptr;   // i16[sell_nnz] col - row, when the bandwidth fits
+  double* sell_vals = nullptr;   // f64[sell_nnz] values gathered for the current solve
+  float* sell_vals32 = nullptr;  // f32[sell_nnz] FP32 values for the mixed-precision inner solve
+  int use_sell = 1;
   // solver workspace (allocated on first use)
-  double* work = nullptr;       // 4*n doubles: r, z, p, q
+  double* work = nullptr;       // 5*n doubles: r, z, p, q, p' (double-buffered direction)
   double* partials = nullptr;   // reduction partials
   femk::CgState* state = nullptr;
   femk::CgState* state_host = nullptr;  // pinned mirror
-  float* work32 = nullptr;      // FP32 inner vectors (mixed precision)
+  float* work32 = nullptr;      // FP32 inner vectors (mixed precision): r, z, p, q, e, D^-1
   float* vals32 = nullptr;      // FP32 copy of the values (mixed precision)
-  double* work64b = nullptr;    // FP64 extra vectors for mixed precision (x_base, r64)
+  double* work64b = nullptr;    // mixed-precision solver state
   int n_sm = 148;
+  // CG launch machinery: plan-owned stream, events, and the captured chunk graph
+  int cg_fused = 0, cg_graph = 1;
+  cudaStream_t cg_stream = nullptr;
+  cudaEvent_t cg_ev[3] = {nullptr, nullptr, nullptr};
+  cudaGraphExec_t cg_exec = nullptr;
+  const void* cg_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  int cg_nodes = 0;
+  // the same for the mixed-precision solver
+  cudaStream_t mx_stream = nullptr;
+  cudaEvent_t mx_ev[3] = {nullptr, nullptr, nullptr};
+  cudaGraphExec_t mx_exec = nullptr;
+  const void* mx_key[4] = {nullptr, nullptr, nullptr, nullptr};
+  int mx_nodes = 0;
+  void* mx_host = nullptr;  // pinned state mirrors
 };
 
 namespace femk {
@@ -109,6 +137,17 @@ inline int blocks_for(int64_t n, int threads, int cap = 1 << 30) {
 int scan_exclusive_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
 
 int ensure_workspace(femk_plan* p);
+
+// Blocks of `threads` threads of kernel `fn` resident per SM (occupancy), cached per kernel.
+int resident_blocks(const void* fn, int threads);
+
+// One full wave of a grid-stride kernel: SMs x resident blocks (at most 8 per SM, which the
+// reduction partial buffers are sized for).
+template <typename K>
+inline int wave_grid(K kernel, int threads, const femk_plan* p) {
+  const int b = resident_blocks((const void*)kernel, threads);
+  return p->n_sm * (b < 8 ? b : 8);
+}
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

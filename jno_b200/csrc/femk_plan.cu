@@ -11,8 +11,10 @@
 //
 // Everything here is integer work: one thread (or warp) per element/row, no sorting library.
 #include <climits>
+#include <cstdlib>
 
 #include "femk_internal.cuh"
+#include "femk_spmv.cuh"
 
 namespace femk {
 namespace {
@@ -36,17 +38,33 @@ __global__ void k_count(const int32_t* __restrict__ cells, int64_t m, int64_t n,
   }
 }
 
+// Connectivity check before any kernel indexes with it: every id in [0, nvert) and the four
+// vertices of a tet pairwise distinct. Reads tets only; writes the error flag.
+__global__ void k_validate_tets(const int32_t* __restrict__ tets, int64_t ntet, int64_t nvert, int* __restrict__ err) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = tets[c * 4 + q];
+    bool bad = false;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) bad |= v[q] < 0 || v[q] >= nvert;
+    bad |= v[0] == v[1] || v[0] == v[2] || v[0] == v[3] || v[1] == v[2] || v[1] == v[3] || v[2] == v[3];
+    if (bad) atomicOr(err, 1);
+  }
+}
+
 __global__ void k_to_i32(const int64_t* __restrict__ in, int64_t n, int32_t* __restrict__ out) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     out[i] = (int32_t)in[i];
 }
 
 template <int ND>
-__global__ void k_fill(const int32_t* __restrict__ cells, int64_t ntet, const int32_t* __restrict__ ptr,
+__global__ void k_fill(const int32_t* __restrict__ cells, int64_t ntet, int64_t n, const int32_t* __restrict__ ptr,
                        int32_t* __restrict__ cursor, int32_t* __restrict__ inc) {
   const int64_t m = ntet * ND;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
     const int32_t v = cells[t];
+    if (v < 0 || v >= n) continue;  // rejected earlier by k_validate_tets / k_count
     const int32_t pos = atomicAdd(&cursor[v], 1);
     inc[ptr[v] + pos] = (int32_t)(t / ND);
   }
@@ -247,6 +265,43 @@ __global__ void k_compact(const uint8_t* __restrict__ mask, const int64_t* __res
     if (mask[i]) list[pos[i]] = (int32_t)i;
 }
 
+// Width of each 32-row slice (its longest row) and its entry count.
+__global__ void k_sell_width(const int32_t* __restrict__ indptr, int64_t n, int64_t nslices, int64_t* __restrict__ len) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t sl = warp; sl < nslices; sl += nwarps) {
+    const int64_t row = sl * 32 + lane;
+    int w = row < n ? indptr[row + 1] - indptr[row] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) w = max(w, __shfl_xor_sync(0xffffffffu, w, o));
+    if (lane == 0) len[sl] = (int64_t)w * 32;
+  }
+}
+
+__global__ void k_sell_fill(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices, int64_t n,
+                            int64_t nslices, const int64_t* __restrict__ sptr, int32_t* __restrict__ src,
+                            int32_t* __restrict__ cols, int16_t* __restrict__ c16) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t sl = warp; sl < nslices; sl += nwarps) {
+    const int64_t row = sl * 32 + lane;
+    const int64_t w = (sptr[sl + 1] - sptr[sl]) / 32;
+    const int32_t beg = row < n ? indptr[row] : 0;
+    const int32_t len = row < n ? indptr[row + 1] - beg : 0;
+    const int64_t self = row < n ? row : n - 1;
+    for (int64_t k = 0; k < w; ++k) {
+      const int64_t j = sptr[sl] + k * 32 + lane;
+      const bool real = k < len;
+      const int32_t col = real ? indices[beg + k] : (int32_t)self;
+      src[j] = real ? beg + (int32_t)k : -1;
+      cols[j] = col;
+      if (c16) c16[j] = (int16_t)(col - self);
+    }
+  }
+}
+
 __global__ void k_cols16(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices, int64_t n,
                          int16_t* __restrict__ c16, int* __restrict__ bad) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -303,13 +358,19 @@ int build_incidence(const int32_t* cells, int64_t ntet, int64_t n, int32_t** ptr
   const int64_t m = ntet * ND;
   k_count<<<::femk::counted_launch() + blocks_for(m, kThreads, 65535 * 4), kThreads, 0, s>>>(cells, m, n, (unsigned long long*)cnt.p, d_err);
   FEMK_CUDA_TRY(cudaGetLastError());
+  int h_err = 0;
+  FEMK_TRY(read_err(d_err, s, &h_err));
+  if (h_err) {
+    set_error("femk_plan_create: connectivity references a DOF outside [0, n)");
+    return FEMK_EINVAL;
+  }
   FEMK_TRY(scan_exclusive_i64((const int64_t*)cnt.p, (int64_t*)scan.p, n, s));
   FEMK_TRY(dev_alloc(ptr_out, n + 1, s));
   FEMK_TRY(dev_alloc(inc_out, m, s));
   k_to_i32<<<::femk::counted_launch() + blocks_for(n + 1, kThreads, 65535 * 4), kThreads, 0, s>>>((const int64_t*)scan.p, n + 1, *ptr_out);
   FEMK_CUDA_TRY(cudaMalloc(&cur.p, sizeof(int32_t) * (n + 1)));
   FEMK_CUDA_TRY(cudaMemsetAsync(cur.p, 0, sizeof(int32_t) * (n + 1), s));
-  k_fill<ND><<<::femk::counted_launch() + blocks_for(m, kThreads, 65535 * 4), kThreads, 0, s>>>(cells, ntet, *ptr_out, (int32_t*)cur.p, *inc_out);
+  k_fill<ND><<<::femk::counted_launch() + blocks_for(m, kThreads, 65535 * 4), kThreads, 0, s>>>(cells, ntet, n, *ptr_out, (int32_t*)cur.p, *inc_out);
   k_sort_lists<<<::femk::counted_launch() + blocks_for(n, 128, 65535 * 4), 128, 0, s>>>(*ptr_out, n, *inc_out);
   FEMK_CUDA_TRY(cudaGetLastError());
   FEMK_CUDA_TRY(cudaStreamSynchronize(s));  // temporaries are freed on return
@@ -338,6 +399,7 @@ int build_pattern(femk_plan* p, int* d_err, int* h_err, cudaStream_t s) {
     return FEMK_EINVAL;
   }
   p->nnz = nnz;
+  choose_spmv_cfg(n > 0 ? (double)nnz / (double)n : 1.0, &p->spmv_L, &p->spmv_U);
   FEMK_TRY(dev_alloc(&p->indptr, n + 1, s));
   FEMK_TRY(dev_alloc(&p->indices, nnz, s));
   k_to_i32<<<::femk::counted_launch() + blocks_for(n + 1, kThreads, 65535 * 4), kThreads, 0, s>>>((const int64_t*)rowptr.p, n + 1, p->indptr);
@@ -368,6 +430,27 @@ int build_pattern(femk_plan* p, int* d_err, int* h_err, cudaStream_t s) {
     cudaFree(p->cols16);
     p->cols16 = nullptr;
   }
+  // sliced-ELL copy of the pattern for the solver
+  p->n_slices = (n + 31) / 32;
+  Temp slen;
+  FEMK_CUDA_TRY(cudaMalloc(&slen.p, sizeof(int64_t) * (p->n_slices + 1)));
+  FEMK_TRY(dev_alloc(&p->sell_ptr, p->n_slices + 1, s));
+  const int sgrid = blocks_for(p->n_slices * 32, kThreads, p->n_sm * 64);
+  k_sell_width<<<::femk::counted_launch() + sgrid, kThreads, 0, s>>>(p->indptr, n, p->n_slices, (int64_t*)slen.p);
+  FEMK_TRY(scan_exclusive_i64((const int64_t*)slen.p, p->sell_ptr, p->n_slices, s));
+  FEMK_CUDA_TRY(cudaMemcpyAsync(&p->sell_nnz, p->sell_ptr + p->n_slices, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  if (p->sell_nnz >= INT32_MAX) {
+    p->use_sell = 0;
+    return FEMK_OK;
+  }
+  FEMK_TRY(dev_alloc(&p->sell_src, p->sell_nnz, s));
+  FEMK_TRY(dev_alloc(&p->sell_cols, p->sell_nnz, s));
+  if (p->cols16) FEMK_TRY(dev_alloc(&p->sell_c16, p->sell_nnz, s));
+  k_sell_fill<<<::femk::counted_launch() + sgrid, kThreads, 0, s>>>(p->indptr, p->indices, n, p->n_slices, p->sell_ptr,
+                                                                    p->sell_src, p->sell_cols, p->sell_c16);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
   return FEMK_OK;
 }
 
@@ -408,6 +491,14 @@ int create_impl(femk_plan* p, const double* xyz, const int32_t* tets, const uint
   FEMK_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), s));
   int h_err = 0;
 
+  k_validate_tets<<<::femk::counted_launch() + blocks_for(p->ntet, kThreads, 65535 * 4), kThreads, 0, s>>>(
+      tets, p->ntet, p->nvert, d_err);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  FEMK_TRY(read_err(d_err, s, &h_err));
+  if (h_err) {
+    set_error("femk_plan_create: a tet references a vertex outside [0, nvert) or repeats a vertex");
+    return FEMK_EINVAL;
+  }
   FEMK_TRY(dev_alloc(&p->xyz, p->nvert * 3, s));
   // vertex incidence (P1 connectivity): used by P2 numbering and by the boundary test
   int32_t* vptr = nullptr;
@@ -483,12 +574,22 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
   int cur = 0;
   cudaGetDevice(&cur);
   cudaSetDevice(p->device);
-  void* ptrs[] = {p->xyz,   p->points,  p->cells,    p->indptr,  p->indices, p->slot,   p->diag,
-                  p->dmask, p->dlist,   p->inc_ptr,  p->inc_elem, p->cols16, p->work,   p->partials,
-                  p->state, p->work32,  p->vals32,   p->work64b};
+  void* ptrs[] = {p->xyz,      p->points,    p->cells,     p->indptr,    p->indices,   p->slot,
+                  p->diag,     p->dmask,     p->dlist,     p->inc_ptr,   p->inc_elem,  p->cols16,
+                  p->work,     p->partials,  p->state,     p->work32,    p->vals32,    p->work64b,
+                  p->sell_ptr, p->sell_src,  p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->state_host) cudaFreeHost(p->state_host);
+  if (p->cg_exec) cudaGraphExecDestroy(p->cg_exec);
+  for (cudaEvent_t e : p->cg_ev)
+    if (e) cudaEventDestroy(e);
+  if (p->cg_stream) cudaStreamDestroy(p->cg_stream);
+  if (p->mx_exec) cudaGraphExecDestroy(p->mx_exec);
+  for (cudaEvent_t e : p->mx_ev)
+    if (e) cudaEventDestroy(e);
+  if (p->mx_stream) cudaStreamDestroy(p->mx_stream);
+  if (p->mx_host) cudaFreeHost(p->mx_host);
   cudaSetDevice(cur);
   delete p;
   return FEMK_OK;
@@ -510,6 +611,9 @@ extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int3
   cudaDeviceGetAttribute(&p->n_sm, cudaDevAttrMultiProcessorCount, p->device);
   p->order = order;
   p->nd = order == 1 ? 4 : 10;
+  if (const char* e = std::getenv("FEMK_CG_FUSED")) p->cg_fused = std::atoi(e) != 0;
+  if (const char* e = std::getenv("FEMK_CG_GRAPH")) p->cg_graph = std::atoi(e) != 0;
+  if (const char* e = std::getenv("FEMK_SELL")) p->use_sell = std::atoi(e) != 0;
   p->nvert = nvert;
   p->ntet = ntet;
   const int st = femk::create_impl(p, xyz_dev, tets_dev, dirichlet_mask_dev, s);

@@ -1,0 +1,148 @@
+// CSR row sums with several rows' loads in flight per lane group (device, FP64 or FP32).
+//
+// A warp owns RPW*U consecutive rows per step: lanes [g*L, (g+1)*L) work on rows base + u*RPW + g,
+// u = 0..U-1 (RPW = 32/L). All U row extents are loaded first, then the first L-wide slice of
+// every row's values and columns, then all U gathers of x, so each lane keeps U independent
+// chains of HBM loads in flight instead of one. Rows longer than L continue in a tail loop (rare
+// for P1, where interior rows hold 15 entries). Values and column indices are streamed with
+// evict-first loads (__ldcs) so they do not push the solver vectors out of L2; x is gathered
+// through the read-only path.
+#pragma once
+
+#include <stdint.h>
+
+#include <type_traits>
+
+namespace femk {
+
+// column of entry k of `row`: an absolute int32 index, or an int16 offset from the row
+__device__ __forceinline__ int64_t col_at(const int32_t* __restrict__ cols, int32_t k, int64_t) {
+  return (int64_t)__ldcs(cols + k);
+}
+__device__ __forceinline__ int64_t col_at(const int16_t* __restrict__ cols, int32_t k, int64_t row) {
+  return row + (int64_t)__ldcs(cols + k);
+}
+
+// gather functors: x[j], or the CG direction z[j] + beta p[j] formed on the fly
+template <typename V>
+struct GatherX {
+  const V* __restrict__ x;
+  __device__ __forceinline__ V operator()(int64_t j) const { return __ldg(x + j); }
+};
+struct GatherDirection {
+  const double* __restrict__ z;
+  const double* __restrict__ p;
+  double beta;
+  __device__ __forceinline__ double operator()(int64_t j) const { return fma(beta, __ldg(p + j), __ldg(z + j)); }
+};
+struct GatherDirection32 {
+  const float* __restrict__ z;
+  const float* __restrict__ p;
+  float beta;
+  __device__ __forceinline__ float operator()(int64_t j) const { return fmaf(beta, __ldg(p + j), __ldg(z + j)); }
+};
+
+template <int L, int U, typename V, typename I, typename G>
+__device__ __forceinline__ void csr_rows_g(const int32_t* __restrict__ indptr, const I* __restrict__ cols,
+                                           const V* __restrict__ vals, const G& gx, int64_t n, int64_t base, int lane,
+                                           V (&s)[U], int64_t (&row)[U]) {
+  constexpr int RPW = 32 / L;
+  const int sub = lane % L;
+  int32_t beg[U], end[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    row[u] = base + u * RPW + lane / L;
+    const bool valid = row[u] < n;
+    beg[u] = valid ? __ldg(indptr + row[u]) : 0;
+    end[u] = valid ? __ldg(indptr + row[u] + 1) : 0;
+  }
+  V v[U];
+  int64_t c[U];
+  bool ok[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int32_t k = beg[u] + sub;
+    ok[u] = k < end[u];
+    v[u] = ok[u] ? __ldcs(vals + k) : V(0);
+    c[u] = ok[u] ? col_at(cols, k, row[u]) : 0;
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u) s[u] = ok[u] ? v[u] * gx(c[u]) : V(0);
+#pragma unroll
+  for (int u = 0; u < U; ++u)
+    for (int32_t k = beg[u] + sub + L; k < end[u]; k += L) s[u] += __ldcs(vals + k) * gx(col_at(cols, k, row[u]));
+#pragma unroll
+  for (int u = 0; u < U; ++u)
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) s[u] += __shfl_xor_sync(0xffffffffu, s[u], o);
+}
+
+template <int L, int U, typename V, typename I>
+__device__ __forceinline__ void csr_rows(const int32_t* __restrict__ indptr, const I* __restrict__ cols,
+                                         const V* __restrict__ vals, const V* __restrict__ x, int64_t n, int64_t base,
+                                         int lane, V (&s)[U], int64_t (&row)[U]) {
+  csr_rows_g<L, U, V, I>(indptr, cols, vals, GatherX<V>{x}, n, base, lane, s, row);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Sliced ELL (SELL-32): rows in slices of 32 (one warp), each slice padded to its longest row and
+// stored column-major, entry k of row 32s+l at sell_ptr[s] + 32k + l. A thread owns a row: no
+// row-pointer chase per row, no shuffles, and the loads of up to 8 entries are issued before any
+// of them is used. Padding entries carry value 0 and the row's own column.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ int64_t sell_col(const int32_t* __restrict__ cols, int64_t j, int64_t) {
+  return (int64_t)__ldcs(cols + j);
+}
+__device__ __forceinline__ int64_t sell_col(const int16_t* __restrict__ cols, int64_t j, int64_t row) {
+  return row + (int64_t)__ldcs(cols + j);
+}
+
+template <typename V, typename I, typename G>
+__device__ __forceinline__ V sell_row(const V* __restrict__ vals, const I* __restrict__ cols, int64_t base, int32_t w,
+                                      int64_t row, const G& gx) {
+  constexpr int B = 8;
+  V acc = V(0);
+  for (int32_t k0 = 0; k0 < w; k0 += B) {
+    V v[B];
+    int64_t c[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const bool ok = k0 + u < w;
+      const int64_t j = base + (int64_t)(k0 + u) * 32;
+      v[u] = ok ? __ldcs(vals + j) : V(0);
+      c[u] = ok ? sell_col(cols, j, row) : row;
+    }
+#pragma unroll
+    for (int u = 0; u < B; ++u)
+      if (k0 + u < w) acc += v[u] * gx(c[u]);
+  }
+  return acc;
+}
+
+// Call f(integral_constant<L>, integral_constant<U>) for a supported (lanes per row, rows in
+// flight) pair; returns false for an unsupported one.
+template <typename F>
+inline bool with_spmv_cfg(int L, int U, F&& f) {
+  using std::integral_constant;
+#define FEMK_CFG(l, u)                                                  \
+  if (L == l && U == u) {                                               \
+    f(integral_constant<int, l>{}, integral_constant<int, u>{});        \
+    return true;                                                        \
+  }
+  FEMK_CFG(4, 4)
+  FEMK_CFG(8, 2)
+  FEMK_CFG(8, 4)
+  FEMK_CFG(16, 1)
+  FEMK_CFG(16, 2)
+  FEMK_CFG(16, 4)
+  FEMK_CFG(32, 1)
+  FEMK_CFG(32, 2)
+#undef FEMK_CFG
+  return false;
+}
+
+// Default (L, U) from the mean row length; FEMK_SPMV_CFG="L,U" in the environment overrides it
+// (tuning sweeps). Called once per plan.
+void choose_spmv_cfg(double mean_row, int* L, int* U);
+
+}  // namespace femk

@@ -1,19 +1,60 @@
 // Error reporting, version, and a device exclusive scan used by the plan build.
 #include <atomic>
+#include <mutex>
+#include <unordered_map>
+#include <cstdio>
+#include <cstdlib>
 
 #include "femk_internal.cuh"
+#include "femk_spmv.cuh"
 
 namespace femk {
 
 static thread_local std::string g_last_error;
 static std::atomic<int64_t> g_launches{0};
 
+static thread_local bool g_capturing = false;
+
 int counted_launch() {
-  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (!g_capturing) g_launches.fetch_add(1, std::memory_order_relaxed);
   return 0;
 }
 
+void set_capturing(bool on) { g_capturing = on; }
+
+void count_launches(int64_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
 void set_error(const std::string& msg) { g_last_error = msg; }
+
+int resident_blocks(const void* fn, int threads) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(fn);
+  if (it != cache.end()) return it->second;
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, threads, 0) != cudaSuccess || b < 1) b = 1;
+  cache[fn] = b;
+  return b;
+}
+
+void choose_spmv_cfg(double mean_row, int* L, int* U) {
+  // measured on B200 at P1 128^3 (mean 14.8) and P2 64^3 (mean 28.4): 8 lanes x 2 rows in flight
+  // beats 16x1/16x2/32x1/32x2 and 4x4, 8x4 by 20-60%
+  if (mean_row <= 6.0) {
+    *L = 4, *U = 4;
+  } else if (mean_row <= 40.0) {
+    *L = 8, *U = 2;
+  } else {
+    *L = 16, *U = 2;
+  }
+  const char* env = std::getenv("FEMK_SPMV_CFG");
+  int l = 0, u = 0;
+  if (env && std::sscanf(env, "%d,%d", &l, &u) == 2 && with_spmv_cfg(l, u, [](auto, auto) {})) {
+    *L = l;
+    *U = u;
+  }
+}
 void clear_error() { g_last_error.clear(); }
 
 namespace {

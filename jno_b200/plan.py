@@ -35,8 +35,17 @@ class FemPlan:
             raise RuntimeError("jno_b200 needs a CUDA device (B200, sm_100a); there is no CPU path")
         lib = _lib.load()
         self._lib = lib
+        t = np.asarray(tets.cpu().numpy() if isinstance(tets, torch.Tensor) else tets)
+        nv = int(points.shape[0])
+        if t.ndim != 2 or t.shape[1] != 4 or t.size == 0:
+            raise ValueError("tets must be a non-empty [T, 4] array")
+        if t.min() < 0 or t.max() >= nv:
+            raise ValueError(f"tets reference vertices outside [0, {nv})")
+        srt = np.sort(t, axis=1)
+        if np.any(srt[:, 1:] == srt[:, :-1]):
+            raise ValueError("a tet repeats a vertex")
         xyz = _device_tensor(points, torch.float64)
-        cells = _device_tensor(tets, torch.int32)
+        cells = _device_tensor(t, torch.int32)
         if xyz.ndim != 2 or xyz.shape[1] != 3 or cells.ndim != 2 or cells.shape[1] != 4:
             raise ValueError("points must be [nv, 3] and tets [T, 4]")
         mask = None if dirichlet_mask is None else _device_tensor(dirichlet_mask, torch.uint8)
@@ -144,6 +153,15 @@ class FemPlan:
     def spmv(self, vals, x, out=None):
         out = torch.empty(self.n, dtype=torch.float64, device=self.device) if out is None else out
         _lib.check(self._lib.femk_spmv(self._h, _lib.ptr(vals), _lib.ptr(x), _lib.ptr(out), _lib.stream_handle()))
+        return out
+
+    def prepare_operator(self, vals):
+        """Gather CSR values into the plan's sliced-ELL solver copy (what each CG iteration uses)."""
+        _lib.check(self._lib.femk_prepare_operator(self._h, _lib.ptr(vals), _lib.stream_handle()))
+
+    def spmv_prepared(self, x, out=None):
+        out = torch.empty(self.n, dtype=torch.float64, device=self.device) if out is None else out
+        _lib.check(self._lib.femk_spmv_prepared(self._h, _lib.ptr(x), _lib.ptr(out), _lib.stream_handle()))
         return out
 
     def spmv_matfree(self, param, x, mode=_lib.COEF_EXP, scale=1.0, out=None):

@@ -225,10 +225,14 @@ def test_status_paths_do_not_fault():
     vneg, bneg = plan.assemble(-torch.ones(len(tets), dtype=torch.float64, device="cuda"), mode=1)
     with pytest.raises(FemkError):
         plan.pcg(vneg, bneg, inv_diag=None)
-    # out-of-range connectivity is rejected before any indexed access
+    # out-of-range or degenerate connectivity is rejected on the host before any GPU work
     bad = tets.copy()
     bad[3, 2] = 10**6
-    with pytest.raises(FemkError):
+    with pytest.raises(ValueError):
+        _plan(p1, bad, 1)
+    bad = tets.copy()
+    bad[3, 2] = bad[3, 1]
+    with pytest.raises(ValueError):
         _plan(p1, bad, 1)
     # the guard of _maybe_residual_check raises on a non-solution
     import jno_b200 as jno
