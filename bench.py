@@ -212,6 +212,110 @@ def roofline_traffic():
     return float(m.group(1)) if m else None
 
 
+
+def p2_variants(args, world, dev, timed):
+    """P2 tets at 64^3 hexes (2.15M DOF): FP64 and mixed assemble + solve, 3 steps each."""
+    import torch
+
+    from jno_b200.plan import FemPlan
+
+    pts, tets = make_mesh(64)
+    plan = FemPlan(pts, tets, 2)
+    fields = [torch.as_tensor(f, device=dev) for f in logk_fields(plan.ntet, 3)]
+    vals = torch.empty(plan.nnz, dtype=torch.float64, device=dev)
+    b = torch.empty(plan.n, dtype=torch.float64, device=dev)
+    inv = torch.empty(plan.n, dtype=torch.float64, device=dev)
+    x = torch.empty(plan.n, dtype=torch.float64, device=dev)
+    info = {"it": [], "inner": []}
+
+    def s64(i):
+        plan.assemble(fields[i % 3], vals=vals, b=b)
+        plan.jacobi(vals, out=inv)
+        x.zero_()
+        info["it"].append(plan.pcg(vals, b, x, inv, tol=1e-8)[1])
+
+    def s32(i):
+        plan.assemble(fields[i % 3], vals=vals, b=b)
+        plan.jacobi(vals, out=inv)
+        x.zero_()
+        info["inner"].append(plan.pcg_mixed(vals, b, inv, x, tol=1e-8)[1])
+
+    ms64 = timed(s64, 3, 1) / 3
+    ms32 = timed(s32, 3, 1) / 3
+    x_ref = torch.zeros_like(x)
+    plan.assemble(fields[0], vals=vals, b=b)
+    plan.jacobi(vals, out=inv)
+    plan.pcg(vals, b, x_ref, inv, tol=1e-12, relres=False)
+    x.zero_()
+    plan.pcg_mixed(vals, b, inv, x, tol=1e-8)
+    err = (torch.linalg.norm(x - x_ref) / torch.linalg.norm(x_ref)).item()
+    base = {"workload": f"P2 64^3 Kuhn tets ({plan.ntet:,} tets, {plan.n:,} DOF, {plan.nnz:,} nnz)"}
+    return {
+        "p2_64_fp64": {**base, "value": world * plan.n / (ms64 / 1e3), "unit": "DOF/s", "ms_per_step": ms64,
+                       "iters": float(np.mean(info["it"]))},
+        "p2_64_mixed": {**base, "value": world * plan.n / (ms32 / 1e3), "unit": "DOF/s", "ms_per_step": ms32,
+                        "inner_iters": float(np.mean(info["inner"])), "speedup_vs_fp64": ms64 / ms32,
+                        "err_vs_fp64_tight": err},
+    }
+
+
+def adjoint_variant(dev, n=64, n_fd=32):
+    """Adjoint config: J = 1/2 sum_i M_ii (u_i - u*_i)^2 at P1 64^3, dJ/dlogk by the adjoint (forward
+    solve + transposed solve + element contraction), checked by FP64 central differences on n_fd
+    random elements."""
+    import torch
+
+    from jno_b200.autograd import solve_p0
+    from jno_b200.plan import FemPlan
+
+    pts, tets = make_mesh(n)
+    plan = FemPlan(pts, tets, 1)
+    logk = torch.as_tensor(np.random.default_rng(FIELD_SEED0).normal(0, 0.5, plan.ntet), device=dev)
+    lk_star = torch.as_tensor(np.random.default_rng(2000).normal(0, 0.5, plan.ntet), device=dev)
+    m = plan.lumped_mass()
+    with torch.no_grad():
+        ustar = solve_p0(plan, lk_star, tol=1e-12)
+
+    def J_of(v, tol):
+        with torch.no_grad():
+            u = solve_p0(plan, v, tol=tol)
+            return (0.5 * torch.sum(m * (u - ustar) ** 2)).item()
+
+    def grad_once(tol=1e-10):
+        lk = logk.clone().requires_grad_(True)
+        u = solve_p0(plan, lk, tol=tol)
+        J = 0.5 * torch.sum(m * (u - ustar) ** 2)
+        J.backward()
+        return lk.grad
+
+    grad_once()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        g = grad_once()
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) / reps * 1e3
+    g = grad_once(tol=1e-13).cpu().numpy()
+    rng = np.random.default_rng(7)
+    idx = rng.choice(plan.ntet, n_fd, replace=False)
+    base = logk.cpu().numpy()
+    eps = 1e-6
+    errs, errs_g = [], []
+    gmax = float(np.abs(g).max())
+    for c in idx:
+        e = np.zeros(plan.ntet)
+        e[c] = eps
+        fd = (J_of(torch.as_tensor(base + e, device=dev), 1e-14) - J_of(torch.as_tensor(base - e, device=dev), 1e-14)) / (2 * eps)
+        errs.append(abs(fd - g[c]) / max(abs(fd), 1e-300))
+        errs_g.append(abs(fd - g[c]) / gmax)
+    return {"workload": f"P1 {n}^3 ({plan.ntet:,} tets), gradient of a lumped-mass misfit w.r.t. per-element log k",
+            "ms_per_gradient": ms, "fd_checked_elements": n_fd, "fd_step": eps,
+            "max_rel_err_vs_fd": float(np.max(errs)), "median_rel_err_vs_fd": float(np.median(errs)),
+            "max_err_vs_fd_rel_to_max_grad": float(np.max(errs_g)),
+            "note": "forward + adjoint PCG at tol 1e-10 for the timing; 1e-13/1e-14 for the FD check"}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -326,21 +430,30 @@ def run_ours(args):
         asm_ms.append(e0.elapsed_time(e1))
         solve_ms.append(e1.elapsed_time(e2))
 
-    # ---- dominant kernel: CSR SpMV (same kernel template as the CG step), CUDA events
+    # ---- dominant kernel: the sliced-ELL SpMV every CG iteration runs (CUDA events, same stream)
     xr = torch.randn(ndof, dtype=torch.float64, device=dev)
     yr = torch.empty_like(xr)
-    for _ in range(5):
-        plan.spmv(vals, xr, yr)
-    torch.cuda.synchronize()
-    reps = 50
-    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s0.record()
-    for _ in range(reps):
-        plan.spmv(vals, xr, yr)
-    s1.record()
-    torch.cuda.synchronize()
-    spmv_ms = s0.elapsed_time(s1) / reps
-    spmv_bytes = 12 * nnz + 20 * ndof + 4
+    plan.prepare_operator(vals)
+
+    def time_launches(fn, reps=50):
+        for _ in range(5):
+            fn()
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(reps):
+            fn()
+        s1.record()
+        torch.cuda.synchronize()
+        return s0.elapsed_time(s1) / reps
+
+    sell_ms = time_launches(lambda: plan.spmv_prepared(xr, yr))
+    csr_ms = time_launches(lambda: plan.spmv(vals, xr, yr))
+    col_bytes = 2 if plan.cols16 else 4
+    # bytes the kernel must move: every stored sliced-ELL entry (value + column), slice offsets,
+    # x read once, y written once
+    sell_bytes = plan.sell_nnz * (8 + col_bytes) + 8 * ((ndof + 31) // 32 + 1) + 16 * ndof
+    csr_bytes = 12 * nnz + 20 * ndof + 4
     peak = 6547.5
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak_src = "fallback"
@@ -350,10 +463,14 @@ def run_ours(args):
             peak_src = "measured"
         except Exception:
             pass
-    achieved = spmv_bytes / (spmv_ms / 1e3) / 1e9
+    achieved = sell_bytes / (sell_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": roofline_traffic(), "kernel": "k_csr (FP64 CSR SpMV, 16 lanes/row)",
-                "bytes_per_launch": spmv_bytes, "ms_per_launch": spmv_ms, "peak_source": peak_src}
+                "traffic": roofline_traffic(),
+                "kernel": f"k_sell (FP64 sliced-ELL SpMV, {'int16' if plan.cols16 else 'int32'} column offsets)",
+                "bytes_per_launch": sell_bytes, "ms_per_launch": sell_ms, "peak_source": peak_src,
+                "csr_equivalent_GBps": csr_bytes / (sell_ms / 1e3) / 1e9,
+                "canonical_csr_kernel": {"ms": csr_ms, "GB/s": csr_bytes / (csr_ms / 1e3) / 1e9,
+                                         "bytes_per_launch": csr_bytes}}
 
     variants = {}
     if not args.no_variants:
@@ -400,7 +517,10 @@ def run_ours(args):
         ms_f = timed(fstep, fsteps, 1) / fsteps
         variants["matrix_free_fp64"] = {"value": world * ndof / (ms_f / 1e3), "unit": "DOF/s", "ms_per_step": ms_f,
                                         "iters": float(np.mean(mf_info["it"]))}
-        variants["spmv_csr_fp64"] = {"GB/s": achieved, "frac_of_peak": achieved / peak, "ms": spmv_ms}
+        variants["spmv_csr_fp64"] = {"GB/s": csr_bytes / (csr_ms / 1e3) / 1e9, "ms": csr_ms}
+        variants["spmv_sell_fp64"] = {"GB/s": achieved, "frac_of_peak": achieved / peak, "ms": sell_ms}
+        variants.update(p2_variants(args, world, dev, timed))
+        variants["adjoint_p1_64"] = adjoint_variant(dev)
 
     # ---- end to end through the public API with host buffers
     d = jno.domain.from_mesh(pts, tets)

@@ -52,6 +52,7 @@ typedef struct femk_plan_info {
   int64_t n_dirichlet;
   int32_t cols16;     /* 1 when every column fits an int16 offset from its row (compact inner format) */
   int32_t device;
+  int64_t sell_nnz;   /* stored entries of the solver's sliced-ELL copy (padding included), 0 if none */
 } femk_plan_info;
 
 /* Library version (major*10000 + minor*100 + patch). */

@@ -53,6 +53,7 @@ class PlanInfo(ctypes.Structure):
         ("n_dirichlet", ctypes.c_int64),
         ("cols16", ctypes.c_int32),
         ("device", ctypes.c_int32),
+        ("sell_nnz", ctypes.c_int64),
     ]
 
 

@@ -12,6 +12,7 @@
 // Replaces jno.solve.cg (jno/solve.py:191-206) -> jax.scipy.sparse.linalg.cg (jax 0.10.1) with
 // M = jno.precond.jacobi() (jno/precond.py:106-111) and LinearOperator.mv (solver_api.py:137-148).
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -19,6 +20,7 @@
 #include "femk_element.cuh"
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
+#include "femk_grid.cuh"
 
 namespace femk {
 namespace {
@@ -65,9 +67,19 @@ __device__ __forceinline__ bool grid_finish(double* partials, uint32_t* ticket, 
   double v[NV];
 #pragma unroll
   for (int j = 0; j < NV; ++j) v[j] = 0.0;
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += kThreads) {
+  // the partials of up to 4*kThreads blocks are loaded before any is added (one round trip)
+  for (int b0 = threadIdx.x; b0 < (int)gridDim.x; b0 += 4 * kThreads) {
+    double t[4][NV];
 #pragma unroll
-    for (int j = 0; j < NV; ++j) v[j] += __ldcg(partials + (int64_t)b * NV + j);
+    for (int u = 0; u < 4; ++u) {
+      const int b = b0 + u * kThreads;
+#pragma unroll
+      for (int j = 0; j < NV; ++j) t[u][j] = b < (int)gridDim.x ? __ldcg(partials + (int64_t)b * NV + j) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int j = 0; j < NV; ++j) v[j] += t[u][j];
   }
   __shared__ double red[NV][kThreads / 32];
 #pragma unroll
@@ -175,7 +187,7 @@ __global__ void __launch_bounds__(kThreads) k_csr(const int32_t* __restrict__ in
 }
 
 // The same modes on the sliced-ELL copy of the operator: one thread per row, 32-row slices.
-template <int MODE, typename IDX>
+template <int MODE, typename IDX, int B>
 __global__ void __launch_bounds__(kThreads) k_sell(const int64_t* __restrict__ sptr, const IDX* __restrict__ scols,
                                                   const double* __restrict__ svals, int64_t n, int64_t nslices,
                                                   const double* __restrict__ x, double* __restrict__ y,
@@ -196,7 +208,8 @@ __global__ void __launch_bounds__(kThreads) k_sell(const int64_t* __restrict__ s
     if (row >= n) continue;
     const int64_t b0 = __ldg(sptr + sl);
     const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
-    const double sv = sell_row(svals, scols, b0 + lane, w, row, GatherX<double>{x});
+    const double sv =
+        sell_row<double, IDX, GatherX<double>, B>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row, GatherX<double>{x});
     if (MODE == kPlain) {
       y[row] = sv;
     } else if (MODE == kCgStep) {
@@ -251,6 +264,108 @@ __global__ void __launch_bounds__(kThreads) k_sell(const int64_t* __restrict__ s
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Persistent Jacobi-PCG: the whole iteration loop in one cooperative launch on the sliced-ELL
+// operator. Per iteration three phases separated by grid barriers: q = A p with <p, q>; the x, r,
+// z updates with <r, z>, <r, r>; p = z + beta p. Every block forms alpha, beta and the stop test
+// from the same partial sums, so all blocks leave the loop together. CgState holds the state from
+// the init kernel on entry and the final state on exit.
+// ---------------------------------------------------------------------------------------------
+constexpr int kPersistThreads = 512;
+
+template <typename IDX>
+__global__ void __launch_bounds__(kPersistThreads, 2)
+    k_pcg_persist(const int64_t* __restrict__ sptr, const IDX* __restrict__ scols, const double* __restrict__ svals,
+                  int64_t n, int64_t nslices, const double* __restrict__ dinv, double* __restrict__ x,
+                  double* __restrict__ r, double* __restrict__ z, double* __restrict__ pv, double* __restrict__ q,
+                  double* __restrict__ partials, CgState* st, GridBar* bar) {
+  if (st->done) return;  // set by the init kernel; identical for every block
+  double gamma = st->gamma, rr = st->rr;
+  const double atol2 = st->atol2;
+  const int maxiter = st->maxiter;
+  const bool precond = st->precond != 0;
+  int iter = st->iter, status = FEMK_OK;
+  unsigned int gen = 0;
+  const int G = gridDim.x;
+  double* P1 = partials;
+  double* P2 = partials + G;
+  const int lane = threadIdx.x & 31;
+  const int64_t gwarp = (blockIdx.x * (int64_t)kPersistThreads + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)G * kPersistThreads) >> 5;
+  const int64_t gtid = blockIdx.x * (int64_t)kPersistThreads + threadIdx.x;
+  const int64_t nthr = (int64_t)G * kPersistThreads;
+  while (true) {
+    // phase 1: q = A p, <p, q>
+    double a1[1] = {0.0};
+    for (int64_t sl = gwarp; sl < nslices; sl += nwarps) {
+      const int64_t row = sl * 32 + lane;
+      if (row >= n) continue;
+      const int64_t b0 = __ldg(sptr + sl);
+      const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
+      const double sv = sell_row(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row, GatherXcg<double>{pv});
+      q[row] = sv;
+      a1[0] += __ldcg(pv + row) * sv;
+    }
+    block_partials<1, kPersistThreads>(a1, P1);
+    if (!grid_sync(bar, gen)) {
+      status = FEMK_TIMEOUT;
+      break;
+    }
+    double pq[1];
+    grid_totals<1>(P1, pq);
+    if (!isfinite(pq[0])) {
+      status = FEMK_NONFINITE;
+      break;
+    }
+    if (!(pq[0] > 0.0)) {
+      status = FEMK_BREAKDOWN;
+      break;
+    }
+    const double alpha = gamma / pq[0];
+    // phase 2: x += alpha p; r -= alpha q; z = D^-1 r; <r, z>, <r, r>
+    double a2[2] = {0.0, 0.0};
+    for (int64_t i = gtid; i < n; i += nthr) {
+      x[i] = x[i] + alpha * __ldcg(pv + i);
+      const double ri = r[i] - alpha * __ldcg(q + i);
+      const double zi = dinv ? dinv[i] * ri : ri;
+      r[i] = ri;
+      z[i] = zi;
+      a2[0] += ri * zi;
+      a2[1] += ri * ri;
+    }
+    block_partials<2, kPersistThreads>(a2, P2);
+    if (!grid_sync(bar, gen)) {
+      status = FEMK_TIMEOUT;
+      break;
+    }
+    double t2[2];
+    grid_totals<2>(P2, t2);
+    ++iter;
+    const double beta = t2[0] / gamma;
+    gamma = t2[0];
+    rr = t2[1];
+    if (!isfinite(t2[0]) || !isfinite(t2[1])) {
+      status = FEMK_NONFINITE;
+      break;
+    }
+    const double rs = precond ? rr : gamma;
+    if (!(rs > atol2) || iter >= maxiter) break;
+    // phase 3: p = z + beta p
+    for (int64_t i = gtid; i < n; i += nthr) pv[i] = z[i] + beta * pv[i];
+    if (!grid_sync(bar, gen)) {
+      status = FEMK_TIMEOUT;
+      break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->iter = iter;
+    st->gamma = gamma;
+    st->rr = rr;
+    st->status = status;
+    st->done = 1;
+  }
+}
+
 template <typename T>
 __global__ void k_sell_gather(const int32_t* __restrict__ src, int64_t m, const double* __restrict__ vals,
                               T* __restrict__ out) {
@@ -260,7 +375,23 @@ __global__ void k_sell_gather(const int32_t* __restrict__ src, int64_t m, const 
   }
 }
 
-// x += alpha p; r -= alpha q; z = D^-1 r; <r, z>, <r, r>; stop test; beta
+// x += alpha p; r -= alpha q; z = D^-1 r; <r, z>, <r, r>; stop test; beta.
+// VEC: every vector is 16-byte aligned, so two rows move per 16-byte load and each thread keeps
+// two such pairs in flight per trip (the plain form is for unaligned caller buffers).
+__device__ __forceinline__ void update_one(int64_t i, double alpha, double* __restrict__ x, double* __restrict__ r,
+                                           double* __restrict__ z, const double* __restrict__ p,
+                                           const double* __restrict__ q, const double* __restrict__ dinv,
+                                           double (&acc)[2]) {
+  x[i] = x[i] + alpha * p[i];
+  const double ri = r[i] - alpha * q[i];
+  const double zi = dinv ? dinv[i] * ri : ri;
+  r[i] = ri;
+  z[i] = zi;
+  acc[0] += ri * zi;
+  acc[1] += ri * ri;
+}
+
+template <bool VEC>
 __global__ void __launch_bounds__(kThreads) k_update(int64_t n, double* __restrict__ x, double* __restrict__ r,
                                                     double* __restrict__ z, const double* __restrict__ p,
                                                     const double* __restrict__ q, const double* __restrict__ dinv,
@@ -268,15 +399,52 @@ __global__ void __launch_bounds__(kThreads) k_update(int64_t n, double* __restri
   if (st->done) return;
   const double alpha = st->alpha;
   double acc[2] = {0.0, 0.0};
-  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
-    const double pi = p[i];
-    x[i] = x[i] + alpha * pi;
-    const double ri = r[i] - alpha * q[i];
-    const double zi = dinv ? dinv[i] * ri : ri;
-    r[i] = ri;
-    z[i] = zi;
-    acc[0] += ri * zi;
-    acc[1] += ri * ri;
+  const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  const int64_t nt = (int64_t)gridDim.x * kThreads;
+  if (VEC) {
+    const int64_t n2 = n >> 1;
+    double2* x2 = reinterpret_cast<double2*>(x);
+    double2* r2 = reinterpret_cast<double2*>(r);
+    double2* z2 = reinterpret_cast<double2*>(z);
+    const double2* p2 = reinterpret_cast<const double2*>(p);
+    const double2* q2 = reinterpret_cast<const double2*>(q);
+    const double2* d2 = reinterpret_cast<const double2*>(dinv);
+    for (int64_t i = tid; i < n2; i += 2 * nt) {
+      const int64_t j = i + nt;
+      const bool two = j < n2;
+      const double2 pa = p2[i], qa = q2[i], xa = x2[i], ra = r2[i];
+      double2 pb = pa, qb = qa, xb = xa, rb = ra, da = make_double2(1.0, 1.0), db = da;
+      if (two) {
+        pb = p2[j];
+        qb = q2[j];
+        xb = x2[j];
+        rb = r2[j];
+      }
+      if (dinv) {
+        da = d2[i];
+        if (two) db = d2[j];
+      }
+      double2 ro, zo;
+      x2[i] = make_double2(xa.x + alpha * pa.x, xa.y + alpha * pa.y);
+      ro = make_double2(ra.x - alpha * qa.x, ra.y - alpha * qa.y);
+      zo = make_double2(da.x * ro.x, da.y * ro.y);
+      r2[i] = ro;
+      z2[i] = zo;
+      acc[0] += ro.x * zo.x + ro.y * zo.y;
+      acc[1] += ro.x * ro.x + ro.y * ro.y;
+      if (two) {
+        x2[j] = make_double2(xb.x + alpha * pb.x, xb.y + alpha * pb.y);
+        ro = make_double2(rb.x - alpha * qb.x, rb.y - alpha * qb.y);
+        zo = make_double2(db.x * ro.x, db.y * ro.y);
+        r2[j] = ro;
+        z2[j] = zo;
+        acc[0] += ro.x * zo.x + ro.y * zo.y;
+        acc[1] += ro.x * ro.x + ro.y * ro.y;
+      }
+    }
+    if ((n & 1) && tid == 0) update_one(n - 1, alpha, x, r, z, p, q, dinv, acc);
+  } else {
+    for (int64_t i = tid; i < n; i += nt) update_one(i, alpha, x, r, z, p, q, dinv, acc);
   }
   block_reduce_store<2>(acc, partials);
   double tot[2];
@@ -296,12 +464,21 @@ __global__ void __launch_bounds__(kThreads) k_update(int64_t n, double* __restri
   }
 }
 
+// p = z + beta p on plan-owned (16-byte aligned) vectors, two rows per load
 __global__ void __launch_bounds__(kThreads) k_pupdate(int64_t n, double* __restrict__ p, const double* __restrict__ z,
                                                      const CgState* st) {
   if (st->done) return;
   const double beta = st->beta;
-  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads)
-    p[i] = z[i] + beta * p[i];
+  const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  const int64_t nt = (int64_t)gridDim.x * kThreads;
+  const int64_t n2 = n >> 1;
+  double2* p2 = reinterpret_cast<double2*>(p);
+  const double2* z2 = reinterpret_cast<const double2*>(z);
+  for (int64_t i = tid; i < n2; i += nt) {
+    const double2 a = p2[i], c = z2[i];
+    p2[i] = make_double2(c.x + beta * a.x, c.y + beta * a.y);
+  }
+  if ((n & 1) && tid == 0) p[n - 1] = z[n - 1] + beta * p[n - 1];
 }
 
 // CG step with the direction update folded in: p_new = z + beta p_old is formed at every gather
@@ -507,6 +684,21 @@ __global__ void k_invert_diag(double* __restrict__ d, int64_t n, const uint8_t* 
 // ---------------------------------------------------------------------------------------------
 int spmv_grid(const femk_plan* p) { return p->n_sm * (2048 / kThreads); }
 
+inline bool aligned16(const void* a) { return ((uintptr_t)a & 15u) == 0; }
+
+// k_update with two-row loads when every vector it touches is 16-byte aligned
+void launch_update(const femk_plan* p, double* x, double* r, double* z, const double* pv, const double* q,
+                   const double* dinv, double* partials, CgState* st, cudaStream_t s) {
+  const bool vec = aligned16(x) && aligned16(r) && aligned16(z) && aligned16(pv) && aligned16(q) &&
+                   (dinv == nullptr || aligned16(dinv));
+  if (vec)
+    k_update<true><<<::femk::counted_launch() + wave_grid(k_update<true>, kThreads, p), kThreads, 0, s>>>(
+        p->n, x, r, z, pv, q, dinv, partials, st);
+  else
+    k_update<false><<<::femk::counted_launch() + wave_grid(k_update<false>, kThreads, p), kThreads, 0, s>>>(
+        p->n, x, r, z, pv, q, dinv, partials, st);
+}
+
 template <int MODE>
 int launch_csr_p(const femk_plan* p, const double* vals, const double* x, double* y, const double* b,
                  const double* dinv, double* z, double* pout, double* partials, CgState* st, double tol2, double atol2,
@@ -536,9 +728,26 @@ template <int MODE>
 int launch_op(const femk_plan* p, bool sell, const double* vals, const double* x, double* y, const double* b,
               const double* dinv, double* z, double* pout, CgState* st, double tol2, double atol2, cudaStream_t s) {
   if (!sell) return launch_csr<MODE>(p, vals, x, y, b, dinv, z, pout, st, tol2, atol2, s);
-  const int grid = wave_grid(k_sell<MODE, int32_t>, kThreads, p);
-  k_sell<MODE, int32_t><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
-      p->sell_ptr, p->sell_cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+  // column offsets in 16 bits when the plan's bandwidth allows it (same values, 2 B less per entry)
+  auto go = [&](auto Bc, auto cols) {
+    constexpr int B = decltype(Bc)::value;
+    using I = std::remove_const_t<std::remove_pointer_t<decltype(cols)>>;
+    const int grid = wave_grid(k_sell<MODE, I, B>, kThreads, p);
+    k_sell<MODE, I, B><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
+        p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+  };
+  const bool c16 = p->sell_c16 && p->sell64_c16;
+  if (sell_batch() == 8) {
+    if (c16)
+      go(std::integral_constant<int, 8>{}, (const int16_t*)p->sell_c16);
+    else
+      go(std::integral_constant<int, 8>{}, (const int32_t*)p->sell_cols);
+  } else {
+    if (c16)
+      go(std::integral_constant<int, 16>{}, (const int16_t*)p->sell_c16);
+    else
+      go(std::integral_constant<int, 16>{}, (const int32_t*)p->sell_cols);
+  }
   FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;
 }
@@ -586,11 +795,12 @@ int launch_matfree(const femk_plan* p, const MatFree& m, const double* x, double
 int enqueue_chunk(const femk_plan* p, const double* vals, double* x, const double* dinv, bool fused, bool sell,
                   int64_t iters, cudaStream_t ws) {
   const int64_t n = p->n;
+  const int64_t vs = p->vstride;
   double* r = p->work;
-  double* z = r + n;
-  double* P0 = z + n;
-  double* q = P0 + n;
-  double* P1 = q + n;
+  double* z = r + vs;
+  double* P0 = z + vs;
+  double* q = P0 + vs;
+  double* P1 = q + vs;
   CgState* st = p->state;
   for (int64_t it = 0; it < iters; ++it) {
     if (fused) {
@@ -605,12 +815,10 @@ int enqueue_chunk(const femk_plan* p, const double* vals, double* x, const doubl
         set_error("unsupported SpMV configuration");
         return FEMK_EINVAL;
       }
-      k_update<<<::femk::counted_launch() + wave_grid(k_update, kThreads, p), kThreads, 0, ws>>>(n, x, r, z, pnew, q,
-                                                                                               dinv, p->partials, st);
+      launch_update(p, x, r, z, pnew, q, dinv, p->partials, st, ws);
     } else {
       FEMK_TRY(launch_op<kCgStep>(p, sell, vals, P0, q, nullptr, nullptr, nullptr, nullptr, st, 0.0, 0.0, ws));
-      k_update<<<::femk::counted_launch() + wave_grid(k_update, kThreads, p), kThreads, 0, ws>>>(n, x, r, z, P0, q,
-                                                                                               dinv, p->partials, st);
+      launch_update(p, x, r, z, P0, q, dinv, p->partials, st, ws);
       k_pupdate<<<::femk::counted_launch() + wave_grid(k_pupdate, kThreads, p), kThreads, 0, ws>>>(n, P0, z, st);
     }
   }
@@ -634,8 +842,12 @@ int ensure_chunk_graph(femk_plan* p, const double* vals, double* x, const double
     (void)wave_grid(k_cg_step<L, U>, kThreads, p);
     (void)wave_grid(k_csr<L, U, kCgStep>, kThreads, p);
   });
-  (void)wave_grid(k_sell<kCgStep, int32_t>, kThreads, p);
-  (void)wave_grid(k_update, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int32_t, 8>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int32_t, 16>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int16_t, 8>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int16_t, 16>, kThreads, p);
+  (void)wave_grid(k_update<true>, kThreads, p);
+  (void)wave_grid(k_update<false>, kThreads, p);
   (void)wave_grid(k_pupdate, kThreads, p);
   cudaGraph_t g = nullptr;
   set_capturing(true);
@@ -680,20 +892,48 @@ int ensure_cg_stream(femk_plan* p) {
   return FEMK_OK;
 }
 
+// Cooperative launch of k_pcg_persist over every resident block (at most 2 per SM).
+int launch_persistent(femk_plan* p, const double* dinv, double* x, cudaStream_t ws) {
+  const int64_t n = p->n;
+  const int64_t vs = p->vstride;
+  double* r = p->work;
+  double* z = r + vs;
+  double* pv = z + vs;
+  double* q = pv + vs;
+  FEMK_CUDA_TRY(cudaMemsetAsync(p->bar, 0, sizeof(GridBar), ws));
+  const bool c16 = p->sell_c16 != nullptr;
+  const void* fn = c16 ? (const void*)k_pcg_persist<int16_t> : (const void*)k_pcg_persist<int32_t>;
+  const int per_sm = std::min(2, resident_blocks(fn, kPersistThreads));
+  const int grid = p->n_sm * per_sm;
+  const void* cols = c16 ? (const void*)p->sell_c16 : (const void*)p->sell_cols;
+  const double* sv = p->sell_vals;
+  CgState* st = p->state;
+  GridBar* bar = (GridBar*)p->bar;
+  int64_t nslices = p->n_slices;
+  void* args[] = {(void*)&p->sell_ptr, (void*)&cols, (void*)&sv,       (void*)&n,  (void*)&nslices,
+                  (void*)&dinv,        (void*)&x,    (void*)&r,        (void*)&z,  (void*)&pv,
+                  (void*)&q,           (void*)&p->partials, (void*)&st, (void*)&bar};
+  counted_launch();
+  FEMK_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kPersistThreads), args, 0, ws));
+  return FEMK_OK;
+}
+
 int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const double* b, double* x, const double* dinv,
             double tol, double atol, int32_t maxiter, int32_t* iters_out, double* relres_out, cudaStream_t s) {
   femk_plan* p = const_cast<femk_plan*>(pc);
   FEMK_TRY(ensure_workspace(p));
   FEMK_TRY(ensure_cg_stream(p));
   const int64_t n = p->n;
+  const int64_t vs = p->vstride;
   double* r = p->work;
-  double* z = r + n;
-  double* pv = z + n;
-  double* q = pv + n;
+  double* z = r + vs;
+  double* pv = z + vs;
+  double* q = pv + vs;
   CgState* st = p->state;
   const bool fused = !mf && p->cg_fused;
   const bool graph = !mf && p->cg_graph;
   const bool sell = !mf && !fused && p->use_sell && p->sell_src;
+  const bool persist = sell && p->cg_persist && p->coop;
   // all solver work runs on the plan's stream, ordered after the caller's stream and before
   // whatever the caller enqueues next
   cudaStream_t ws = p->cg_stream;
@@ -701,7 +941,7 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
   FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->cg_ev[2], 0));
   // the sliced-ELL values buffer must exist before a graph that reads it is captured
   if (sell) FEMK_TRY(prepare_sell(p, vals, ws));
-  if (graph) FEMK_TRY(ensure_chunk_graph(p, vals, x, dinv, fused, sell));
+  if (graph && !persist) FEMK_TRY(ensure_chunk_graph(p, vals, x, dinv, fused, sell));
   CgState init{};
   init.maxiter = maxiter;
   init.precond = dinv ? 1 : 0;
@@ -720,7 +960,10 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
   int64_t enq = 0;  // iterations enqueued
   int chunk_id = 0;
   bool have_prev = false;
-  while (true) {
+  if (persist) {
+    FEMK_TRY(launch_persistent(p, dinv, x, ws));
+  }
+  while (!persist) {
     if (graph) {
       FEMK_CUDA_TRY(cudaGraphLaunch(p->cg_exec, ws));
       count_launches(p->cg_nodes);
@@ -731,8 +974,7 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
         FEMK_TRY(launch_matfree(p, *mf, pv, q, ws, st));
         k_dot_pq<<<::femk::counted_launch() + wave_grid(k_dot_pq, kThreads, p), kThreads, 0, ws>>>(n, pv, q,
                                                                                                   p->partials, st);
-        k_update<<<::femk::counted_launch() + wave_grid(k_update, kThreads, p), kThreads, 0, ws>>>(
-            n, x, r, z, pv, q, dinv, p->partials, st);
+        launch_update(p, x, r, z, pv, q, dinv, p->partials, st, ws);
         k_pupdate<<<::femk::counted_launch() + wave_grid(k_pupdate, kThreads, p), kThreads, 0, ws>>>(n, pv, z, st);
       }
       FEMK_CUDA_TRY(cudaGetLastError());
@@ -784,6 +1026,8 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
     set_error("femk_pcg: <p, A p> <= 0 (operator not symmetric positive definite)");
   } else if (status == FEMK_NONFINITE) {
     set_error("femk_pcg: non-finite value in a CG reduction");
+  } else if (status == FEMK_TIMEOUT) {
+    set_error("femk_pcg: a grid barrier of the persistent solver gave up waiting");
   }
   return status;
 }
@@ -792,11 +1036,12 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
 
 int ensure_workspace(femk_plan* p) {
   if (p->work) return FEMK_OK;
-  FEMK_CUDA_TRY(cudaMalloc(&p->work, sizeof(double) * 5 * (p->n + 1)));
+  FEMK_CUDA_TRY(cudaMalloc(&p->work, sizeof(double) * 5 * p->vstride));
   FEMK_CUDA_TRY(cudaMalloc(&p->partials, sizeof(double) * 4 * (int64_t)p->n_sm * 64));
   FEMK_CUDA_TRY(cudaMalloc(&p->state, sizeof(CgState)));
   FEMK_CUDA_TRY(cudaMemset(p->state, 0, sizeof(CgState)));
   FEMK_CUDA_TRY(cudaMallocHost(&p->state_host, 2 * sizeof(CgState)));
+  FEMK_CUDA_TRY(cudaMalloc(&p->bar, 64));
   return FEMK_OK;
 }
 
@@ -975,7 +1220,7 @@ extern "C" int femk_pcg_noalloc(const femk_plan* p, const double* vals, const do
     const int64_t todo = std::min<int64_t>(kChunk, (int64_t)maxiter - enq);
     for (int64_t it = 0; it < todo; ++it) {
       FEMK_TRY(launch_csr_into<kCgStep>(p, vals, pv, q, nullptr, nullptr, nullptr, nullptr, partials, st, 0.0, 0.0, s));
-      k_update<<<::femk::counted_launch() + wave_grid(k_update, kThreads, p), kThreads, 0, s>>>(n, x, r, z, pv, q, dinv, partials, st);
+      launch_update(p, x, r, z, pv, q, dinv, partials, st, s);
       k_pupdate<<<::femk::counted_launch() + wave_grid(k_pupdate, kThreads, p), kThreads, 0, s>>>(n, pv, z, st);
     }
     FEMK_CUDA_TRY(cudaGetLastError());

@@ -97,8 +97,10 @@ struct femk_plan {
   double* sell_vals = nullptr;   // f64[sell_nnz] values gathered for the current solve
   float* sell_vals32 = nullptr;  // f32[sell_nnz] FP32 values for the mixed-precision inner solve
   int use_sell = 1;
+  int sell64_c16 = 1;            // FP64 sliced-ELL streams int16 column offsets when available
   // solver workspace (allocated on first use)
-  double* work = nullptr;       // 5*n doubles: r, z, p, q, p' (double-buffered direction)
+  int64_t vstride = 0;          // solver vector stride: n rounded up to 64 (keeps every slot 512-byte aligned)
+  double* work = nullptr;       // 5 slots of vstride doubles: r, z, p, q, p' (double-buffered direction)
   double* partials = nullptr;   // reduction partials
   femk::CgState* state = nullptr;
   femk::CgState* state_host = nullptr;  // pinned mirror
@@ -107,7 +109,9 @@ struct femk_plan {
   double* work64b = nullptr;    // mixed-precision solver state
   int n_sm = 148;
   // CG launch machinery: plan-owned stream, events, and the captured chunk graph
-  int cg_fused = 0, cg_graph = 1;
+  int cg_fused = 0, cg_graph = 1, cg_persist = 0;
+  int coop = 0;                 // device supports cooperative launch
+  void* bar = nullptr;          // grid barrier of the persistent solvers
   cudaStream_t cg_stream = nullptr;
   cudaEvent_t cg_ev[3] = {nullptr, nullptr, nullptr};
   cudaGraphExec_t cg_exec = nullptr;

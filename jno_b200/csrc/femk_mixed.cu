@@ -21,6 +21,7 @@
 
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
+#include "femk_grid.cuh"
 
 namespace femk {
 namespace {
@@ -64,9 +65,19 @@ __device__ __forceinline__ bool reduce_finish(double (&v)[NV], double* partials,
   double s[NV];
 #pragma unroll
   for (int j = 0; j < NV; ++j) s[j] = 0.0;
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += kThreads)
+  for (int b0 = threadIdx.x; b0 < (int)gridDim.x; b0 += 4 * kThreads) {
+    double t[4][NV];
 #pragma unroll
-    for (int j = 0; j < NV; ++j) s[j] += __ldcg(partials + (int64_t)b * NV + j);
+    for (int u = 0; u < 4; ++u) {
+      const int b = b0 + u * kThreads;
+#pragma unroll
+      for (int j = 0; j < NV; ++j) t[u][j] = b < (int)gridDim.x ? __ldcg(partials + (int64_t)b * NV + j) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int j = 0; j < NV; ++j) s[j] += t[u][j];
+  }
 #pragma unroll
   for (int j = 0; j < NV; ++j) s[j] = warp_sum(s[j]);
   __syncthreads();
@@ -116,8 +127,8 @@ __device__ __forceinline__ void finish_alpha(MixedState* st, double pq) {
 }
 
 // q = A32 p, <p, q> -> alpha (sliced-ELL operator)
-template <typename IDX>
-__global__ void __launch_bounds__(kThreads) k_step32_sell(const int64_t* __restrict__ sptr, const IDX* __restrict__ cols,
+template <typename IDX, int B>
+__global__ void __launch_bounds__(kThreads, 8) k_step32_sell(const int64_t* __restrict__ sptr, const IDX* __restrict__ cols,
                                                          const float* __restrict__ vals, int64_t n, int64_t nslices,
                                                          const float* __restrict__ p, float* __restrict__ q,
                                                          double* __restrict__ partials, MixedState* st) {
@@ -131,7 +142,8 @@ __global__ void __launch_bounds__(kThreads) k_step32_sell(const int64_t* __restr
     if (row >= n) continue;
     const int64_t b0 = __ldg(sptr + sl);
     const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
-    const float sv = sell_row(vals, cols, b0 + lane, w, row, GatherX<float>{p});
+    const float sv =
+        sell_row<float, IDX, GatherX<float>, B>(vals + b0 + lane, cols + b0 + lane, w, (int32_t)row, GatherX<float>{p});
     q[row] = sv;
     acc = fmaf(__ldg(p + row), sv, acc);
   }
@@ -169,7 +181,8 @@ __global__ void __launch_bounds__(kThreads) k_step32(const int32_t* __restrict__
   finish_alpha(st, tot[0]);
 }
 
-// e += alpha p; r -= alpha q; z = D^-1 r; <r, z>, <r, r>; request a reliable update or set beta
+// e += alpha p; r -= alpha q; z = D^-1 r; <r, z>, <r, r>; request a reliable update or set beta.
+// All six vectors are plan-owned and 16-byte aligned: four rows per load.
 __global__ void __launch_bounds__(kThreads) k_update32(int64_t n, float* __restrict__ e, float* __restrict__ r,
                                                       float* __restrict__ z, const float* __restrict__ p,
                                                       const float* __restrict__ q, const float* __restrict__ dinv,
@@ -177,9 +190,39 @@ __global__ void __launch_bounds__(kThreads) k_update32(int64_t n, float* __restr
   if (st->done || st->hold) return;
   const float alpha = (float)st->alpha;
   float a0 = 0.f, a1 = 0.f;
-  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
-    const float pi = p[i];
-    e[i] = fmaf(alpha, pi, e[i]);
+  const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  const int64_t nt = (int64_t)gridDim.x * kThreads;
+  const int64_t n4 = n >> 2;
+  float4* e4 = reinterpret_cast<float4*>(e);
+  float4* r4 = reinterpret_cast<float4*>(r);
+  float4* z4 = reinterpret_cast<float4*>(z);
+  const float4* p4 = reinterpret_cast<const float4*>(p);
+  const float4* q4 = reinterpret_cast<const float4*>(q);
+  const float4* d4 = reinterpret_cast<const float4*>(dinv);
+  for (int64_t i = tid; i < n4; i += nt) {
+    const float4 pi = p4[i], qi = q4[i], di = d4[i], ri0 = r4[i];
+    float4 ei = e4[i];
+    ei.x = fmaf(alpha, pi.x, ei.x);
+    ei.y = fmaf(alpha, pi.y, ei.y);
+    ei.z = fmaf(alpha, pi.z, ei.z);
+    ei.w = fmaf(alpha, pi.w, ei.w);
+    float4 ri, zi;
+    ri.x = fmaf(-alpha, qi.x, ri0.x);
+    ri.y = fmaf(-alpha, qi.y, ri0.y);
+    ri.z = fmaf(-alpha, qi.z, ri0.z);
+    ri.w = fmaf(-alpha, qi.w, ri0.w);
+    zi.x = di.x * ri.x;
+    zi.y = di.y * ri.y;
+    zi.z = di.z * ri.z;
+    zi.w = di.w * ri.w;
+    e4[i] = ei;
+    r4[i] = ri;
+    z4[i] = zi;
+    a0 = fmaf(ri.x, zi.x, fmaf(ri.y, zi.y, fmaf(ri.z, zi.z, fmaf(ri.w, zi.w, a0))));
+    a1 = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, fmaf(ri.z, ri.z, fmaf(ri.w, ri.w, a1))));
+  }
+  for (int64_t i = 4 * n4 + tid; i < n; i += nt) {
+    e[i] = fmaf(alpha, p[i], e[i]);
     const float ri = fmaf(-alpha, q[i], r[i]);
     const float zi = dinv[i] * ri;
     r[i] = ri;
@@ -292,8 +335,177 @@ __global__ void k_pupdate32(int64_t n, float* __restrict__ p, const float* __res
   if (MODE == 0 && st->hold) return;
   if (MODE == 1 && st->need_update != 2) return;
   const float beta = (float)st->beta;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    p[i] = fmaf(beta, p[i], z[i]);
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t nt = (int64_t)gridDim.x * blockDim.x;
+  const int64_t n4 = n >> 2;
+  float4* p4 = reinterpret_cast<float4*>(p);
+  const float4* z4 = reinterpret_cast<const float4*>(z);
+  for (int64_t i = tid; i < n4; i += nt) {
+    const float4 a = p4[i], c = z4[i];
+    p4[i] = make_float4(fmaf(beta, a.x, c.x), fmaf(beta, a.y, c.y), fmaf(beta, a.z, c.z), fmaf(beta, a.w, c.w));
+  }
+  for (int64_t i = 4 * n4 + tid; i < n; i += nt) p[i] = fmaf(beta, p[i], z[i]);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Persistent form: the whole mixed solve in one cooperative launch. Phases per inner iteration:
+// A (q = A32 p, <p, q>), B (e, r, z updates, <r, z>, <r, r>, update decision), C (p = z + beta p);
+// on a reliable update two more phases run between B and C: U1 (x += e) and U2 (the FP64 true
+// residual on the FP64 sliced-ELL values). Vectors written by other blocks earlier in the launch
+// are read through L2 (__ldcg).
+// ---------------------------------------------------------------------------------------------
+constexpr int kPersistThreads = 512;
+
+template <typename IDX>
+__global__ void __launch_bounds__(kPersistThreads, 2)
+    k_mixed_persist(const int64_t* __restrict__ sptr, const IDX* __restrict__ scols, const float* __restrict__ sv32,
+                    const double* __restrict__ sv64, int64_t n, int64_t nslices, const double* __restrict__ b,
+                    double* __restrict__ x, const float* __restrict__ dinv, float* __restrict__ r,
+                    float* __restrict__ z, float* __restrict__ pv, float* __restrict__ q, float* __restrict__ e,
+                    double* __restrict__ partials, MixedState* st, GridBar* bar) {
+  if (st->done) return;
+  double gamma = st->gamma, rr_since = st->rr_since, rr64 = st->rr64, rr = st->rr;
+  const double atol2 = st->atol2, delta2 = st->delta2;
+  const int maxiter = st->maxiter, restart = st->restart;
+  int iter = st->iter, outer = st->outer, status = FEMK_OK;
+  unsigned int gen = 0;
+  const int G = gridDim.x;
+  double* P1 = partials;
+  double* P2 = partials + G;
+  double* P3 = partials + 3 * G;
+  const int lane = threadIdx.x & 31;
+  const int64_t gwarp = (blockIdx.x * (int64_t)kPersistThreads + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)G * kPersistThreads) >> 5;
+  const int64_t gtid = blockIdx.x * (int64_t)kPersistThreads + threadIdx.x;
+  const int64_t nthr = (int64_t)G * kPersistThreads;
+  while (true) {
+    // A: q = A32 p, <p, q>
+    float acc = 0.f;
+    for (int64_t sl = gwarp; sl < nslices; sl += nwarps) {
+      const int64_t row = sl * 32 + lane;
+      if (row >= n) continue;
+      const int64_t b0 = __ldg(sptr + sl);
+      const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
+      const float s32 = sell_row(sv32 + b0 + lane, scols + b0 + lane, w, (int32_t)row, GatherXcg<float>{pv});
+      q[row] = s32;
+      acc = fmaf(__ldcg(pv + row), s32, acc);
+    }
+    double a1[1] = {(double)acc};
+    block_partials<1, kPersistThreads>(a1, P1);
+    if (!grid_sync(bar, gen)) {
+      status = FEMK_TIMEOUT;
+      break;
+    }
+    double pq[1];
+    grid_totals<1>(P1, pq);
+    if (!isfinite(pq[0])) {
+      status = FEMK_NONFINITE;
+      break;
+    }
+    if (!(pq[0] > 0.0)) {
+      status = FEMK_BREAKDOWN;
+      break;
+    }
+    const float falpha = (float)(gamma / pq[0]);
+    // B: e += alpha p; r -= alpha q; z = D^-1 r; <r, z>, <r, r>
+    float f0 = 0.f, f1 = 0.f;
+    for (int64_t i = gtid; i < n; i += nthr) {
+      e[i] = fmaf(falpha, __ldcg(pv + i), e[i]);
+      const float ri = fmaf(-falpha, __ldcg(q + i), __ldcg(r + i));
+      const float zi = dinv[i] * ri;
+      r[i] = ri;
+      z[i] = zi;
+      f0 = fmaf(ri, zi, f0);
+      f1 = fmaf(ri, ri, f1);
+    }
+    double a2[2] = {(double)f0, (double)f1};
+    block_partials<2, kPersistThreads>(a2, P2);
+    if (!grid_sync(bar, gen)) {
+      status = FEMK_TIMEOUT;
+      break;
+    }
+    double t2[2];
+    grid_totals<2>(P2, t2);
+    ++iter;
+    rr = t2[1];
+    if (!isfinite(t2[0]) || !isfinite(t2[1])) {
+      status = FEMK_NONFINITE;
+      break;
+    }
+    const bool cap = iter >= maxiter;
+    double beta;
+    if (!(t2[1] > atol2) || t2[1] < delta2 * rr_since || cap) {
+      // U1: x += e; e = 0
+      for (int64_t i = gtid; i < n; i += nthr) {
+        x[i] += (double)e[i];
+        e[i] = 0.f;
+      }
+      if (!grid_sync(bar, gen)) {
+        status = FEMK_TIMEOUT;
+        break;
+      }
+      // U2: r64 = b - A64 x; r = fp32(r64); z = D^-1 r; <r, z>, <r64, r64>
+      double d[2] = {0.0, 0.0};
+      for (int64_t sl = gwarp; sl < nslices; sl += nwarps) {
+        const int64_t row = sl * 32 + lane;
+        if (row >= n) continue;
+        const int64_t b0 = __ldg(sptr + sl);
+        const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
+        const double s64 = sell_row(sv64 + b0 + lane, scols + b0 + lane, w, (int32_t)row, GatherXcg<double>{x});
+        const double r64 = b[row] - s64;
+        const float rf = (float)r64;
+        const float zf = dinv[row] * rf;
+        r[row] = rf;
+        z[row] = zf;
+        d[0] += (double)rf * (double)zf;
+        d[1] += r64 * r64;
+      }
+      block_partials<2, kPersistThreads>(d, P3);
+      if (!grid_sync(bar, gen)) {
+        status = FEMK_TIMEOUT;
+        break;
+      }
+      double t3[2];
+      grid_totals<2>(P3, t3);
+      ++outer;
+      rr64 = t3[1];
+      rr_since = t3[1];
+      if (!isfinite(t3[0]) || !isfinite(t3[1])) {
+        status = FEMK_NONFINITE;
+        break;
+      }
+      if (!(t3[1] > atol2) || cap) break;
+      beta = restart ? 0.0 : t3[0] / gamma;
+      gamma = t3[0];
+    } else {
+      beta = t2[0] / gamma;
+      gamma = t2[0];
+    }
+    // C: p = z + beta p
+    const float fbeta = (float)beta;
+    for (int64_t i = gtid; i < n; i += nthr) pv[i] = fmaf(fbeta, __ldcg(pv + i), __ldcg(z + i));
+    if (!grid_sync(bar, gen)) {
+      status = FEMK_TIMEOUT;
+      break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->iter = iter;
+    st->outer = outer;
+    st->gamma = gamma;
+    st->rr = rr;
+    st->rr64 = rr64;
+    st->status = status;
+    st->done = 1;
+  }
+}
+
+__global__ void k_gather64(const int32_t* __restrict__ src, int64_t m, const double* __restrict__ vals,
+                           double* __restrict__ out) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t k = __ldcs(src + j);
+    out[j] = k >= 0 ? __ldcs(vals + k) : 0.0;
+  }
 }
 
 template <bool INIT>
@@ -309,14 +521,19 @@ void launch_true_resid(const femk_plan* p, const double* vals, const double* x, 
 
 void launch_step32(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s) {
   if (p->sell_vals32) {
-    if (p->sell_c16) {
-      k_step32_sell<int16_t><<<::femk::counted_launch() + wave_grid(k_step32_sell<int16_t>, kThreads, p), kThreads, 0,
-                               s>>>(p->sell_ptr, p->sell_c16, p->sell_vals32, p->n, p->n_slices, pv, q, p->partials, st);
-    } else {
-      k_step32_sell<int32_t><<<::femk::counted_launch() + wave_grid(k_step32_sell<int32_t>, kThreads, p), kThreads, 0,
-                               s>>>(p->sell_ptr, p->sell_cols, p->sell_vals32, p->n, p->n_slices, pv, q, p->partials,
-                                    st);
-    }
+    auto go = [&](auto Bc) {
+      constexpr int B = decltype(Bc)::value;
+      if (p->sell_c16) {
+        k_step32_sell<int16_t, B><<<::femk::counted_launch() + wave_grid(k_step32_sell<int16_t, B>, kThreads, p),
+                                    kThreads, 0, s>>>(p->sell_ptr, p->sell_c16, p->sell_vals32, p->n, p->n_slices, pv,
+                                                      q, p->partials, st);
+      } else {
+        k_step32_sell<int32_t, B><<<::femk::counted_launch() + wave_grid(k_step32_sell<int32_t, B>, kThreads, p),
+                                    kThreads, 0, s>>>(p->sell_ptr, p->sell_cols, p->sell_vals32, p->n, p->n_slices,
+                                                      pv, q, p->partials, st);
+      }
+    };
+    go(std::integral_constant<int, 8>{});
     return;
   }
   with_spmv_cfg(p->spmv_L, p->spmv_U, [&](auto Lc, auto Uc) {
@@ -337,14 +554,14 @@ struct MixedPtrs {
 };
 
 MixedPtrs mixed_ptrs(const femk_plan* p) {
-  const int64_t n = p->n;
+  const int64_t vs = p->vstride;
   MixedPtrs m;
   m.r = p->work32;
-  m.z = m.r + n;
-  m.pv = m.z + n;
-  m.q = m.pv + n;
-  m.e = m.q + n;
-  m.d32 = m.e + n;
+  m.z = m.r + vs;
+  m.pv = m.z + vs;
+  m.q = m.pv + vs;
+  m.e = m.q + vs;
+  m.d32 = m.e + vs;
   m.st = (MixedState*)p->work64b;
   return m;
 }
@@ -368,9 +585,11 @@ int enqueue_mixed_chunk(const femk_plan* p, const double* vals, const double* b,
 
 int ensure_mixed(femk_plan* p) {
   FEMK_TRY(ensure_workspace(p));
-  if (!p->work32) FEMK_CUDA_TRY(cudaMalloc(&p->work32, sizeof(float) * 6 * (p->n + 1)));
+  if (!p->work32) FEMK_CUDA_TRY(cudaMalloc(&p->work32, sizeof(float) * 6 * p->vstride));
   if (p->use_sell && p->sell_src) {
     if (!p->sell_vals32) FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals32, sizeof(float) * (p->sell_nnz + 1)));
+    if (p->cg_persist && p->coop && !p->sell_vals)
+      FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals, sizeof(double) * (p->sell_nnz + 1)));
   } else if (!p->vals32) {
     FEMK_CUDA_TRY(cudaMalloc(&p->vals32, sizeof(float) * (p->nnz + 1)));
   }
@@ -400,8 +619,10 @@ int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double
     (void)wave_grid(k_step32<L, U, int16_t>, kThreads, p);
     (void)wave_grid(k_step32<L, U, int32_t>, kThreads, p);
   });
-  (void)wave_grid(k_step32_sell<int16_t>, kThreads, p);
-  (void)wave_grid(k_step32_sell<int32_t>, kThreads, p);
+  (void)wave_grid(k_step32_sell<int16_t, 8>, kThreads, p);
+  (void)wave_grid(k_step32_sell<int32_t, 8>, kThreads, p);
+  (void)wave_grid(k_step32_sell<int16_t, 16>, kThreads, p);
+  (void)wave_grid(k_step32_sell<int32_t, 16>, kThreads, p);
   (void)wave_grid(k_update32, kThreads, p);
   (void)wave_grid(k_pupdate32<0>, 256, p);
   (void)wave_grid(k_pupdate32<1>, 256, p);
@@ -461,7 +682,10 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   cudaStream_t ws = p->mx_stream;
   FEMK_CUDA_TRY(cudaEventRecord(p->mx_ev[2], s));
   FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->mx_ev[2], 0));
-  if (p->cg_graph) FEMK_TRY(ensure_mixed_graph(p, vals, b, x));
+  const bool persist = p->cg_persist && p->coop && p->sell_vals32 && p->sell_vals;
+  if (p->cg_graph && !persist) FEMK_TRY(ensure_mixed_graph(p, vals, b, x));
+  if (persist)
+    k_gather64<<<::femk::counted_launch() + p->n_sm * 8, 256, 0, ws>>>(p->sell_src, p->sell_nnz, vals, p->sell_vals);
   const int g1 = p->n_sm * 8;
   if (p->sell_vals32)
     k_gather32<<<::femk::counted_launch() + g1, 256, 0, ws>>>(p->sell_src, p->sell_nnz, vals, p->sell_vals32);
@@ -484,7 +708,27 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   // a chunk performs at least one inner iteration unless the solve is done, so maxiter + 1 chunks
   // bound the loop
   const int64_t max_chunks = (int64_t)maxiter + 1;
-  while (true) {
+  if (persist) {
+    FEMK_CUDA_TRY(cudaMemsetAsync(p->bar, 0, sizeof(GridBar), ws));
+    const bool c16 = p->sell_c16 != nullptr;
+    const void* fn = c16 ? (const void*)k_mixed_persist<int16_t> : (const void*)k_mixed_persist<int32_t>;
+    const int per_sm = std::min(2, resident_blocks(fn, kPersistThreads));
+    const int grid = p->n_sm * per_sm;
+    const void* cols = c16 ? (const void*)p->sell_c16 : (const void*)p->sell_cols;
+    const float* sv32 = p->sell_vals32;
+    const double* sv64 = p->sell_vals;
+    int64_t nn = n, ns = p->n_slices;
+    float *r = m.r, *z = m.z, *pv = m.pv, *q = m.q, *e = m.e;
+    const float* d32 = m.d32;
+    MixedState* stp = m.st;
+    GridBar* bar = (GridBar*)p->bar;
+    void* args[] = {(void*)&p->sell_ptr, (void*)&cols, (void*)&sv32, (void*)&sv64, (void*)&nn, (void*)&ns,
+                    (void*)&b, (void*)&x, (void*)&d32, (void*)&r, (void*)&z, (void*)&pv, (void*)&q, (void*)&e,
+                    (void*)&p->partials, (void*)&stp, (void*)&bar};
+    counted_launch();
+    FEMK_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kPersistThreads), args, 0, ws));
+  }
+  while (!persist) {
     if (p->cg_graph) {
       FEMK_CUDA_TRY(cudaGraphLaunch(p->mx_exec, ws));
       count_launches(p->mx_nodes);
@@ -517,6 +761,10 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   if (fin.status == FEMK_NONFINITE) {
     set_error("femk_pcg_mixed: non-finite value in a reduction");
     return FEMK_NONFINITE;
+  }
+  if (fin.status == FEMK_TIMEOUT) {
+    set_error("femk_pcg_mixed: a grid barrier of the persistent solver gave up waiting");
+    return FEMK_TIMEOUT;
   }
   if (fin.rr64 > fin.atol2) {
     set_error("femk_pcg_mixed: iteration cap reached above tolerance");

@@ -557,6 +557,7 @@ int create_impl(femk_plan* p, const double* xyz, const int32_t* tets, const uint
     set_error("femk_plan_create: inconsistent connectivity (edge lookup failed)");
     return FEMK_EINVAL;
   }
+  p->vstride = (p->n + 63) & ~int64_t(63);
   int st = p->nd == 4 ? build_pattern<4>(p, d_err, &h_err, s) : build_pattern<10>(p, d_err, &h_err, s);
   if (st == FEMK_OK) st = build_dirichlet(p, mask, vptr, vinc, s);
   if (vptr != p->inc_ptr) {
@@ -577,7 +578,8 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
   void* ptrs[] = {p->xyz,      p->points,    p->cells,     p->indptr,    p->indices,   p->slot,
                   p->diag,     p->dmask,     p->dlist,     p->inc_ptr,   p->inc_elem,  p->cols16,
                   p->work,     p->partials,  p->state,     p->work32,    p->vals32,    p->work64b,
-                  p->sell_ptr, p->sell_src,  p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32};
+                  p->sell_ptr, p->sell_src,  p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32,
+                  p->bar};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->state_host) cudaFreeHost(p->state_host);
@@ -614,6 +616,9 @@ extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int3
   if (const char* e = std::getenv("FEMK_CG_FUSED")) p->cg_fused = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_CG_GRAPH")) p->cg_graph = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_SELL")) p->use_sell = std::atoi(e) != 0;
+  if (const char* e = std::getenv("FEMK_SELL64_C16")) p->sell64_c16 = std::atoi(e) != 0;
+  if (const char* e = std::getenv("FEMK_CG_PERSIST")) p->cg_persist = std::atoi(e) != 0;
+  cudaDeviceGetAttribute(&p->coop, cudaDevAttrCooperativeLaunch, p->device);
   p->nvert = nvert;
   p->ntet = ntet;
   const int st = femk::create_impl(p, xyz_dev, tets_dev, dirichlet_mask_dev, s);
@@ -636,6 +641,7 @@ extern "C" int femk_plan_get_info(const femk_plan* p, femk_plan_info* out) {
   out->n_dirichlet = p->n_dir;
   out->cols16 = p->cols16 ? 1 : 0;
   out->device = p->device;
+  out->sell_nnz = p->sell_src ? p->sell_nnz : 0;
   return FEMK_OK;
 }
 

@@ -29,6 +29,13 @@ struct GatherX {
   const V* __restrict__ x;
   __device__ __forceinline__ V operator()(int64_t j) const { return __ldg(x + j); }
 };
+// x[j] through L2 only: for vectors that other blocks rewrite inside the same (persistent) launch,
+// where the non-coherent read-only path could return a stale line
+template <typename V>
+struct GatherXcg {
+  const V* __restrict__ x;
+  __device__ __forceinline__ V operator()(int64_t j) const { return __ldcg(x + j); }
+};
 struct GatherDirection {
   const double* __restrict__ z;
   const double* __restrict__ p;
@@ -90,27 +97,26 @@ __device__ __forceinline__ void csr_rows(const int32_t* __restrict__ indptr, con
 // row-pointer chase per row, no shuffles, and the loads of up to 8 entries are issued before any
 // of them is used. Padding entries carry value 0 and the row's own column.
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ int64_t sell_col(const int32_t* __restrict__ cols, int64_t j, int64_t) {
-  return (int64_t)__ldcs(cols + j);
-}
-__device__ __forceinline__ int64_t sell_col(const int16_t* __restrict__ cols, int64_t j, int64_t row) {
-  return row + (int64_t)__ldcs(cols + j);
+__device__ __forceinline__ int32_t sell_col(const int32_t* __restrict__ cb, int32_t j, int32_t) { return __ldcs(cb + j); }
+__device__ __forceinline__ int32_t sell_col(const int16_t* __restrict__ cb, int32_t j, int32_t row) {
+  return row + (int32_t)__ldcs(cb + j);
 }
 
-template <typename V, typename I, typename G>
-__device__ __forceinline__ V sell_row(const V* __restrict__ vals, const I* __restrict__ cols, int64_t base, int32_t w,
-                                      int64_t row, const G& gx) {
-  constexpr int B = 8;
+// Row sum of one thread's row. vals/cols point at the row's first entry (slice base + lane);
+// entry k sits at offset 32k. Index arithmetic is 32-bit (n < 2^31 is checked at plan build).
+template <typename V, typename I, typename G, int B = 8>
+__device__ __forceinline__ V sell_row(const V* __restrict__ vb, const I* __restrict__ cb, int32_t w, int32_t row,
+                                      const G& gx) {
   V acc = V(0);
   for (int32_t k0 = 0; k0 < w; k0 += B) {
     V v[B];
-    int64_t c[B];
+    int32_t c[B];
 #pragma unroll
     for (int u = 0; u < B; ++u) {
       const bool ok = k0 + u < w;
-      const int64_t j = base + (int64_t)(k0 + u) * 32;
-      v[u] = ok ? __ldcs(vals + j) : V(0);
-      c[u] = ok ? sell_col(cols, j, row) : row;
+      const int32_t j = (k0 + u) * 32;
+      v[u] = ok ? __ldcs(vb + j) : V(0);
+      c[u] = ok ? sell_col(cb, j, row) : row;
     }
 #pragma unroll
     for (int u = 0; u < B; ++u)
@@ -118,6 +124,10 @@ __device__ __forceinline__ V sell_row(const V* __restrict__ vals, const I* __res
   }
   return acc;
 }
+
+// entries per batch of the FP64 sliced-ELL row loop (FEMK_SELL_BATCH=8|16 overrides for tuning);
+// the FP32 loop always uses 8 (16 doubles its registers and halves its occupancy)
+int sell_batch();
 
 // Call f(integral_constant<L>, integral_constant<U>) for a supported (lanes per row, rows in
 // flight) pair; returns false for an unsupported one.

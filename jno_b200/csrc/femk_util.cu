@@ -38,6 +38,15 @@ int resident_blocks(const void* fn, int threads) {
   return b;
 }
 
+int sell_batch() {
+  static int b = [] {
+    const char* e = std::getenv("FEMK_SELL_BATCH");
+    const int v = e ? std::atoi(e) : 16;  // B200: 63 vs 66 us per FP64 SpMV at P1 128^3
+    return v == 8 ? 8 : 16;
+  }();
+  return b;
+}
+
 void choose_spmv_cfg(double mean_row, int* L, int* U) {
   // measured on B200 at P1 128^3 (mean 14.8) and P2 64^3 (mean 28.4): 8 lanes x 2 rows in flight
   // beats 16x1/16x2/32x1/32x2 and 4x4, 8x4 by 20-60%

@@ -67,6 +67,7 @@ class FemPlan:
         self.nnz = info.nnz
         self.n_dirichlet = info.n_dirichlet
         self.cols16 = bool(info.cols16)
+        self.sell_nnz = int(info.sell_nnz)
         self.device = torch.device("cuda", info.device)
         self._pattern = None
 
