@@ -53,6 +53,8 @@ typedef struct femk_plan_info {
   int32_t cols16;     /* 1 when every column fits an int16 offset from its row (compact inner format) */
   int32_t device;
   int64_t sell_nnz;   /* stored entries of the solver's sliced-ELL copy (padding included), 0 if none */
+  int32_t batch_graph; /* 1 when the last femk_pcg_batched ran as a replayed CUDA graph */
+  int32_t pad;
 } femk_plan_info;
 
 /* Library version (major*10000 + minor*100 + patch). */
@@ -180,6 +182,21 @@ int femk_pcg_noalloc(const femk_plan* plan, const double* vals_dev, const double
 int femk_pcg_mixed(const femk_plan* plan, const double* vals_dev, const double* b_dev, double* x_dev,
                    const double* inv_diag_dev, double tol, double atol, int32_t maxiter, int mode,
                    int32_t* inner_iters_out, int32_t* outer_out, double* relres_out, void* stream);
+
+/*
+ * Batched Jacobi-PCG: nprob independent systems held by one plan built on their disjoint union
+ * (vertex ids offset per problem), problem k owning rows [row_off[k], row_off[k+1]) (host array,
+ * row_off[0] = 0, row_off[nprob] = n). One persistent cooperative launch runs every problem's CG
+ * (jax cg semantics, per-problem alpha/beta/stop test) until all have stopped; rows are processed
+ * in warp tiles of tile_rows (never crossing a problem) with blocks_per_sm (1 or 2) blocks of 16
+ * warps per SM -- the schedule an autotuner chooses. iters_out / relres_out / status_out are host arrays of nprob
+ * (may be NULL). Returns the first non-OK problem status, FEMK_TIMEOUT if a grid barrier gave up.
+ * No reference counterpart (jNO batches by vmap over right-hand sides only).
+ */
+int femk_pcg_batched(const femk_plan* plan, int32_t nprob, const int64_t* row_off_host, const double* vals_dev,
+                     const double* b_dev, double* x_dev, const double* inv_diag_dev, double tol, double atol,
+                     int32_t maxiter, int32_t tile_rows, int32_t blocks_per_sm, int32_t* iters_out_host,
+                     double* relres_out_host, int32_t* status_out_host, void* stream);
 
 /*
  * Adjoint contraction: grad[c] = -k_c * (m o lam)_e^T K_hat_e (m o u)_e, m = 1 - dirichlet mask,

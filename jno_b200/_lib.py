@@ -54,6 +54,8 @@ class PlanInfo(ctypes.Structure):
         ("cols16", ctypes.c_int32),
         ("device", ctypes.c_int32),
         ("sell_nnz", ctypes.c_int64),
+        ("batch_graph", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
     ]
 
 
@@ -85,6 +87,7 @@ SIGNATURES = {
     "femk_pcg_matfree": [_P, _P, _I, _D, _P, _P, _P, _D, _D, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_D), _P],
     "femk_pcg_mixed": [_P, _P, _P, _P, _P, _D, _D, _I32, _I, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
                        ctypes.POINTER(_D), _P],
+    "femk_pcg_batched": [_P, _I32, _P, _P, _P, _P, _P, _D, _D, _I32, _I32, _I32, _P, _P, _P, _P],
     "femk_adjoint_grad": [_P, _P, _I, _D, _P, _P, _P, _P],
     "femk_lumped_mass": [_P, _P, _P],
 }

@@ -1,0 +1,441 @@
+// Batched Jacobi-PCG: many independent problems of uneven size solved in one persistent
+// cooperative launch (captured in a CUDA graph and replayed for repeated solves).
+//
+// The problems live in one plan built on their disjoint union (vertex ids offset per problem), so
+// the plan build and one femk_assemble call serve all of them; problem k owns the contiguous rows
+// [row_off[k], row_off[k+1]). Rows are cut into tiles that never cross a problem; a tile is one
+// warp's work item, and every grid phase walks the tiles of the still-active problems (tile t on
+// warp t mod W, W = warps in the grid, no block-wide synchronisation inside a phase):
+//   phase 0 (once): r = b - A x0, z = D^-1 r, p = z, per-tile <r,z>, <r,r>, <b,b>
+//   phase 1: q = A p, per-tile <p, q>          | owner pass: alpha_k
+//   phase 2: x, r, z updates, <r,z>, <r,r>     | owner pass: beta_k, stop test of problem k
+//   phase 3: p = z + beta_k p
+//   phase R (once): per-problem ||b - A x|| for the residual guard
+// After every reduction phase an owner pass (block b finishes problems b, b + G, ...) sums the
+// problem's tile partials in a fixed order and writes its scalars, so tiles can be small (the
+// largest problems keep every SM busy after the small ones have converged) without each tile
+// re-reducing its problem. Barriers are the bounded-spin grid barriers of femk_grid.cuh. No reference counterpart (jNO batches only by vmap over
+// right-hand sides, tests/test_fem_solver_slots.py:123-132).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "femk_grid.cuh"
+#include "femk_internal.cuh"
+#include "femk_spmv.cuh"
+
+namespace femk {
+namespace {
+
+constexpr int kBT = 512;  // threads per block
+constexpr int kL = 8, kU = 2;
+
+struct BatchArgs {
+  const int32_t* indptr;
+  const int32_t* indices;
+  const double* vals;
+  const int32_t* tile_r0;
+  const int32_t* tile_r1;
+  const int32_t* tile_prob;
+  const int32_t* prob_t0;
+  const int32_t* prob_t1;
+  int32_t ntiles, nprob, maxiter;
+  double tol2, atol2_abs;
+  const double* b;
+  double* x;
+  const double* dinv;
+  double *r, *z, *p, *q;
+  double* P;      // partials: [7][ntiles]
+  double* gam;    // [2][nprob]
+  double* atol2;  // [nprob]
+  double* rr;     // [nprob]
+  double* relres; // [nprob]
+  int32_t* iter;  // [nprob]
+  int32_t* done;  // [nprob]
+  int32_t* status;
+  int32_t* active;
+  GridBar* bar;
+};
+
+// One warp computes (A v)[row] for the rows of its tile; the epilogue functor sees (row, Av).
+template <typename F>
+__device__ __forceinline__ void tile_spmv(const BatchArgs& a, int32_t r0, int32_t r1, const double* __restrict__ v,
+                                          F&& epi) {
+  const int lane = threadIdx.x & 31;
+  const int sub = lane % kL;
+  constexpr int RPW = 32 / kL;
+  for (int64_t base = r0; base < r1; base += RPW * kU) {
+    double sv[kU];
+    int64_t rows[kU];
+    csr_rows_g<kL, kU, double, int32_t>(a.indptr, a.indices, a.vals, GatherXcg<double>{v}, r1, base, lane, sv, rows);
+#pragma unroll
+    for (int u = 0; u < kU; ++u)
+      if (rows[u] < r1 && sub == 0) epi(rows[u], sv[u]);
+  }
+}
+
+// sum of problem k's tile partials P[j][t], t in [t0, t1): whole block, fixed order, broadcast
+__device__ __forceinline__ double prob_sum(const BatchArgs& a, int j, int32_t k) {
+  __shared__ double part[kBT / 32];
+  const int32_t t0 = a.prob_t0[k], t1 = a.prob_t1[k];
+  double t = 0.0;
+  for (int32_t i = t0 + threadIdx.x; i < t1; i += kBT) t += __ldcg(a.P + (int64_t)j * a.ntiles + i);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = t;
+  __syncthreads();
+  double out = 0.0;
+#pragma unroll
+  for (int w = 0; w < kBT / 32; ++w) out += part[w];
+  __syncthreads();
+  return out;
+}
+
+// warp sum of NV values, stored by lane 0 as tile t's partials P[slot0 + j][t]
+template <int NV>
+__device__ __forceinline__ void tile_partial(double (&v)[NV], double* P, int ntiles, int32_t t, const int slot0) {
+#pragma unroll
+  for (int j = 0; j < NV; ++j)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_xor_sync(0xffffffffu, v[j], o);
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) P[(int64_t)(slot0 + j) * ntiles + t] = v[j];
+  }
+}
+
+// done[k] read once per warp (lane 0, broadcast), so the whole warp takes the same branch
+__device__ __forceinline__ bool warp_done(const int32_t* done, int32_t k) {
+  int d = (threadIdx.x & 31) == 0 ? __ldcg(done + k) : 0;
+  d = __shfl_sync(0xffffffffu, d, 0);
+  return d != 0;
+}
+
+// done[k] read once per block (a problem's owner may retire it while other blocks run its tiles;
+// every thread of a block must take the same branch around the barriers inside the tile loop)
+__device__ __forceinline__ bool block_done(const int32_t* done, int32_t k) {
+  __shared__ int32_t d;
+  if (threadIdx.x == 0) d = __ldcg(done + k);
+  __syncthreads();
+  const bool out = d != 0;
+  __syncthreads();
+  return out;
+}
+
+__device__ __forceinline__ void retire(const BatchArgs& a, int32_t k, int32_t status) {
+  a.status[k] = status;
+  a.done[k] = 1;
+  atomicSub(a.active, 1);
+}
+
+// Owner pass: block b finishes problems k = b, b + G, ... from their tile partials.
+#define FEMK_OWNER_LOOP for (int32_t k = blockIdx.x; k < a.nprob; k += gridDim.x)
+
+__global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
+  unsigned int gen = 0;
+  const int32_t gw = (int32_t)((blockIdx.x * (int64_t)kBT + threadIdx.x) >> 5);  // global warp
+  const int32_t NW = (int32_t)(((int64_t)gridDim.x * kBT) >> 5);
+  const int lane = threadIdx.x & 31;
+  // ---- phase 0: residual of x0
+  for (int32_t t = gw; t < a.ntiles; t += NW) {
+    const int32_t r0 = a.tile_r0[t], r1 = a.tile_r1[t];
+    double acc[3] = {0.0, 0.0, 0.0};
+    tile_spmv(a, r0, r1, a.x, [&](int64_t row, double s) {
+      const double bi = a.b[row];
+      const double ri = bi - s;
+      const double zi = a.dinv ? a.dinv[row] * ri : ri;
+      a.r[row] = ri;
+      a.z[row] = zi;
+      a.p[row] = zi;
+      acc[0] += ri * zi;
+      acc[1] += ri * ri;
+      acc[2] += bi * bi;
+    });
+    tile_partial<3>(acc, a.P, a.ntiles, t, 0);
+  }
+  if (!grid_sync(a.bar, gen)) return;
+  FEMK_OWNER_LOOP {
+    const double rz = prob_sum(a, 0, k), rr = prob_sum(a, 1, k), bb = prob_sum(a, 2, k);
+    if (threadIdx.x == 0) {
+      const double at2 = fmax(a.tol2 * bb, a.atol2_abs);
+      a.gam[k] = rz;
+      a.rr[k] = rr;
+      a.atol2[k] = at2;
+      a.iter[k] = 0;
+      const double rs = a.dinv ? rr : rz;
+      if (!isfinite(rz) || !isfinite(rr))
+        retire(a, k, FEMK_NONFINITE);
+      else if (!(rs > at2) || a.maxiter <= 0)
+        retire(a, k, FEMK_OK);
+    }
+  }
+  if (!grid_sync(a.bar, gen)) return;
+  double* alpha = a.gam + a.nprob;  // per-problem step scalars of the current iteration
+  double* beta = alpha;             // (alpha is dead once phase 2 is done; beta reuses the slot)
+  while (ld_acquire_u32((const unsigned int*)a.active) != 0u) {
+    // ---- phase 1: q = A p, <p, q>
+    for (int32_t t = gw; t < a.ntiles; t += NW) {
+      const int32_t k = a.tile_prob[t];
+      if (warp_done(a.done, k)) continue;
+      double acc[1] = {0.0};
+      tile_spmv(a, a.tile_r0[t], a.tile_r1[t], a.p, [&](int64_t row, double s) {
+        a.q[row] = s;
+        acc[0] += __ldcg(a.p + row) * s;
+      });
+      tile_partial<1>(acc, a.P, a.ntiles, t, 3);
+    }
+    if (!grid_sync(a.bar, gen)) return;
+    FEMK_OWNER_LOOP {
+      if (block_done(a.done, k)) continue;
+      const double pq = prob_sum(a, 3, k);
+      if (threadIdx.x == 0) {
+        if (!(pq > 0.0) || !isfinite(pq))
+          retire(a, k, isfinite(pq) ? FEMK_BREAKDOWN : FEMK_NONFINITE);
+        else
+          alpha[k] = a.gam[k] / pq;
+      }
+    }
+    if (!grid_sync(a.bar, gen)) return;
+    // ---- phase 2: x, r, z updates; <r, z>, <r, r>
+    for (int32_t t = gw; t < a.ntiles; t += NW) {
+      const int32_t k = a.tile_prob[t];
+      if (warp_done(a.done, k)) continue;
+      const double al = __ldcg(alpha + k);
+      double acc[2] = {0.0, 0.0};
+      for (int32_t i = a.tile_r0[t] + lane; i < a.tile_r1[t]; i += 32) {
+        a.x[i] = a.x[i] + al * __ldcg(a.p + i);
+        const double ri = __ldcg(a.r + i) - al * __ldcg(a.q + i);
+        const double zi = a.dinv ? a.dinv[i] * ri : ri;
+        a.r[i] = ri;
+        a.z[i] = zi;
+        acc[0] += ri * zi;
+        acc[1] += ri * ri;
+      }
+      tile_partial<2>(acc, a.P, a.ntiles, t, 4);
+    }
+    if (!grid_sync(a.bar, gen)) return;
+    FEMK_OWNER_LOOP {
+      if (block_done(a.done, k)) continue;
+      const double rz = prob_sum(a, 4, k), rr = prob_sum(a, 5, k);
+      if (threadIdx.x == 0) {
+        const int32_t itk = a.iter[k] + 1;
+        const double rs = a.dinv ? rr : rz;
+        const bool finite = isfinite(rz) && isfinite(rr);
+        beta[k] = rz / a.gam[k];
+        a.gam[k] = rz;
+        a.rr[k] = rr;
+        a.iter[k] = itk;
+        if (!finite || !(rs > a.atol2[k]) || itk >= a.maxiter) retire(a, k, finite ? FEMK_OK : FEMK_NONFINITE);
+      }
+    }
+    if (!grid_sync(a.bar, gen)) return;
+    // ---- phase 3: p = z + beta p
+    for (int32_t t = gw; t < a.ntiles; t += NW) {
+      const int32_t k = a.tile_prob[t];
+      if (warp_done(a.done, k)) continue;
+      const double be = __ldcg(beta + k);
+      for (int32_t i = a.tile_r0[t] + lane; i < a.tile_r1[t]; i += 32)
+        a.p[i] = __ldcg(a.z + i) + be * __ldcg(a.p + i);
+    }
+    if (!grid_sync(a.bar, gen)) return;
+  }
+  // ---- phase R: per-problem ||b - A x||, ||b||
+  for (int32_t t = gw; t < a.ntiles; t += NW) {
+    double acc[2] = {0.0, 0.0};
+    tile_spmv(a, a.tile_r0[t], a.tile_r1[t], a.x, [&](int64_t row, double s) {
+      const double bi = a.b[row];
+      const double w = bi - s;
+      acc[0] += w * w;
+      acc[1] += bi * bi;
+    });
+    tile_partial<2>(acc, a.P, a.ntiles, t, 5);
+  }
+  if (!grid_sync(a.bar, gen)) return;
+  FEMK_OWNER_LOOP {
+    const double ww = prob_sum(a, 5, k), bb = prob_sum(a, 6, k);
+    if (threadIdx.x == 0) a.relres[k] = sqrt(ww) / (sqrt(bb) + 1e-30);
+  }
+}
+
+__global__ void k_batch_reset(int32_t* done, int32_t* status, int32_t* active, int32_t nprob, GridBar* bar) {
+  for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nprob; k += gridDim.x * blockDim.x) {
+    done[k] = 0;
+    status[k] = FEMK_OK;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *active = nprob;
+    bar->count = 0;
+    bar->gen = 0;
+    bar->timeout = 0;
+  }
+}
+
+}  // namespace
+}  // namespace femk
+
+using namespace femk;
+
+extern "C" int femk_pcg_batched(const femk_plan* pc, int32_t nprob, const int64_t* row_off, const double* vals,
+                                const double* b, double* x, const double* dinv, double tol, double atol,
+                                int32_t maxiter, int32_t tile_rows, int32_t blocks_per_sm, int32_t* iters_out,
+                                double* relres_out, int32_t* status_out, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(pc && row_off && vals && b && x, "femk_pcg_batched: NULL argument");
+  FEMK_CHECK_ARG(nprob >= 1, "femk_pcg_batched: nprob must be >= 1");
+  FEMK_CHECK_ARG(tile_rows >= 32 && tile_rows <= (1 << 20), "femk_pcg_batched: tile_rows out of range");
+  FEMK_CHECK_ARG(blocks_per_sm >= 1 && blocks_per_sm <= 2, "femk_pcg_batched: blocks_per_sm must be 1 or 2");
+  FEMK_CHECK_ARG(pc->coop, "femk_pcg_batched: the device does not support cooperative launch");
+  femk_plan* p = const_cast<femk_plan*>(pc);
+  FEMK_CHECK_ARG(row_off[0] == 0 && row_off[nprob] == p->n, "femk_pcg_batched: row_off must span [0, n)");
+  // tiles
+  std::vector<int32_t> r0, r1, tp, t0(nprob), t1(nprob);
+  for (int32_t k = 0; k < nprob; ++k) {
+    FEMK_CHECK_ARG(row_off[k + 1] > row_off[k], "femk_pcg_batched: empty problem");
+    t0[k] = (int32_t)r0.size();
+    for (int64_t s0 = row_off[k]; s0 < row_off[k + 1]; s0 += tile_rows) {
+      r0.push_back((int32_t)s0);
+      r1.push_back((int32_t)std::min<int64_t>(s0 + tile_rows, row_off[k + 1]));
+      tp.push_back(k);
+    }
+    t1[k] = (int32_t)r0.size();
+  }
+  const int32_t ntiles = (int32_t)r0.size();
+  cudaStream_t s = (cudaStream_t)stream;
+  FEMK_TRY(ensure_workspace(p));
+  // batch workspace: ints (tiles + per-problem), doubles (partials + per-problem)
+  const int64_t nint = 3 * (int64_t)ntiles + 5 * (int64_t)nprob + 8;
+  const int64_t ndbl = 7 * (int64_t)ntiles + 6 * (int64_t)nprob + 8;
+  const int64_t bytes = nint * 4 + 64 + ndbl * 8;
+  if (p->batch_bytes < bytes) {
+    if (p->batch_ws) cudaFree(p->batch_ws);
+    p->batch_ws = nullptr;
+    p->batch_bytes = 0;
+    FEMK_CUDA_TRY(cudaMalloc(&p->batch_ws, bytes));
+    p->batch_bytes = bytes;
+  }
+  int32_t* ib = (int32_t*)p->batch_ws;
+  double* db = (double*)((char*)p->batch_ws + ((nint * 4 + 63) & ~int64_t(63)));
+  BatchArgs a;
+  a.indptr = p->indptr;
+  a.indices = p->indices;
+  a.vals = vals;
+  a.tile_r0 = ib;
+  a.tile_r1 = ib + ntiles;
+  a.tile_prob = ib + 2 * ntiles;
+  a.prob_t0 = ib + 3 * ntiles;
+  a.prob_t1 = a.prob_t0 + nprob;
+  a.iter = const_cast<int32_t*>(a.prob_t1) + nprob;
+  a.done = a.iter + nprob;
+  a.status = a.done + nprob;
+  a.active = a.status + nprob;
+  a.ntiles = ntiles;
+  a.nprob = nprob;
+  a.maxiter = maxiter;
+  a.tol2 = tol * tol;
+  a.atol2_abs = atol * atol;
+  a.b = b;
+  a.x = x;
+  a.dinv = dinv;
+  const int64_t vs = p->vstride;
+  a.r = p->work;
+  a.z = a.r + vs;
+  a.p = a.z + vs;
+  a.q = a.p + vs;
+  a.P = db;
+  a.gam = db + 7 * (int64_t)ntiles;
+  a.atol2 = a.gam + 2 * nprob;
+  a.rr = a.atol2 + nprob;
+  a.relres = a.rr + nprob;
+  a.bar = (GridBar*)p->bar;
+  // tile tables: uploaded only when the schedule changes (pageable copies stay outside the graph)
+  uint64_t h = 1469598103934665603ull;
+  for (int32_t k = 0; k <= nprob; ++k) h = (h ^ (uint64_t)row_off[k]) * 1099511628211ull;
+  h = (h ^ (uint64_t)tile_rows) * 1099511628211ull;
+  const bool same_tiles = p->batch_key[0] == (const void*)(uintptr_t)h && p->batch_key[1] == p->batch_ws;
+  if (!same_tiles) {
+    FEMK_CUDA_TRY(cudaMemcpyAsync(ib, r0.data(), 4 * ntiles, cudaMemcpyHostToDevice, s));
+    FEMK_CUDA_TRY(cudaMemcpyAsync(ib + ntiles, r1.data(), 4 * ntiles, cudaMemcpyHostToDevice, s));
+    FEMK_CUDA_TRY(cudaMemcpyAsync(ib + 2 * ntiles, tp.data(), 4 * ntiles, cudaMemcpyHostToDevice, s));
+    FEMK_CUDA_TRY(cudaMemcpyAsync(ib + 3 * ntiles, t0.data(), 4 * nprob, cudaMemcpyHostToDevice, s));
+    FEMK_CUDA_TRY(cudaMemcpyAsync(ib + 3 * ntiles + nprob, t1.data(), 4 * nprob, cudaMemcpyHostToDevice, s));
+  }
+  const int per_sm = std::min(blocks_per_sm, resident_blocks((const void*)k_batch_pcg, kBT));
+  const int grid = p->n_sm * std::max(1, per_sm);
+  // the solve itself (reset + one cooperative launch) is one CUDA graph, replayed while the
+  // operands and the schedule stay the same; a device that refuses to capture the cooperative
+  // launch gets the same two launches directly
+  const void* key[8] = {(const void*)(uintptr_t)h, p->batch_ws, vals, b, x, dinv,
+                        (const void*)(uintptr_t)grid, (const void*)(uintptr_t)((uint64_t)maxiter << 1)};
+  bool have = p->batch_exec != nullptr;
+  for (int i = 0; i < 8 && have; ++i) have = key[i] == p->batch_key[i];
+  if (!have && p->batch_graph_ok) {
+    if (p->batch_exec) cudaGraphExecDestroy(p->batch_exec);
+    p->batch_exec = nullptr;
+    if (!p->batch_stream) FEMK_CUDA_TRY(cudaStreamCreateWithFlags(&p->batch_stream, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    set_capturing(true);
+    cudaError_t e = cudaStreamBeginCapture(p->batch_stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      k_batch_reset<<<8, 256, 0, p->batch_stream>>>(a.done, a.status, a.active, nprob, a.bar);
+      void* cargs[] = {(void*)&a};
+      cudaError_t el = cudaLaunchCooperativeKernel((const void*)k_batch_pcg, dim3(grid), dim3(kBT), cargs, 0,
+                                                   p->batch_stream);
+      cudaError_t ee = cudaStreamEndCapture(p->batch_stream, &g);
+      if (el == cudaSuccess && ee == cudaSuccess && g) e = cudaGraphInstantiate(&p->batch_exec, g, 0);
+      else e = el != cudaSuccess ? el : ee;
+    }
+    set_capturing(false);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess || !p->batch_exec) {
+      cudaGetLastError();
+      p->batch_exec = nullptr;
+      p->batch_graph_ok = 0;  // fall back to direct launches from now on
+    } else {
+      for (int i = 0; i < 8; ++i) p->batch_key[i] = key[i];
+      have = true;
+    }
+  }
+  if (have && p->batch_exec) {
+    if (!p->batch_ev) FEMK_CUDA_TRY(cudaEventCreateWithFlags(&p->batch_ev, cudaEventDisableTiming));
+    FEMK_CUDA_TRY(cudaEventRecord(p->batch_ev, s));
+    FEMK_CUDA_TRY(cudaStreamWaitEvent(p->batch_stream, p->batch_ev, 0));
+    FEMK_CUDA_TRY(cudaGraphLaunch(p->batch_exec, p->batch_stream));
+    count_launches(2);
+    p->batch_graph_used = 1;
+    FEMK_CUDA_TRY(cudaEventRecord(p->batch_ev, p->batch_stream));
+    FEMK_CUDA_TRY(cudaStreamWaitEvent(s, p->batch_ev, 0));
+  } else {
+    k_batch_reset<<<::femk::counted_launch() + 8, 256, 0, s>>>(a.done, a.status, a.active, nprob, a.bar);
+    FEMK_CUDA_TRY(cudaGetLastError());
+    void* args[] = {(void*)&a};
+    counted_launch();
+    FEMK_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_batch_pcg, dim3(grid), dim3(kBT), args, 0, s));
+    p->batch_key[0] = (const void*)(uintptr_t)h;
+    p->batch_key[1] = p->batch_ws;
+    p->batch_graph_used = 0;
+  }
+  std::vector<int32_t> it(nprob), stv(nprob);
+  std::vector<double> rel(nprob);
+  unsigned int timeout = 0;
+  FEMK_CUDA_TRY(cudaMemcpyAsync(it.data(), a.iter, 4 * nprob, cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaMemcpyAsync(stv.data(), a.status, 4 * nprob, cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaMemcpyAsync(rel.data(), a.relres, 8 * nprob, cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaMemcpyAsync(&timeout, &a.bar->timeout, 4, cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  if (iters_out) std::copy(it.begin(), it.end(), iters_out);
+  if (relres_out) std::copy(rel.begin(), rel.end(), relres_out);
+  if (status_out) std::copy(stv.begin(), stv.end(), status_out);
+  if (timeout) {
+    set_error("femk_pcg_batched: a grid barrier gave up waiting");
+    return FEMK_TIMEOUT;
+  }
+  int worst = FEMK_OK;
+  for (int32_t k = 0; k < nprob; ++k) {
+    if (stv[k] != FEMK_OK) worst = stv[k];
+  }
+  if (worst != FEMK_OK) {
+    set_error("femk_pcg_batched: at least one problem did not solve (see status_out)");
+    return worst;
+  }
+  return FEMK_OK;
+}

@@ -124,6 +124,15 @@ struct femk_plan {
   const void* mx_key[4] = {nullptr, nullptr, nullptr, nullptr};
   int mx_nodes = 0;
   void* mx_host = nullptr;  // pinned state mirrors
+  // batched solver workspace (tiles, per-problem state, partials)
+  void* batch_ws = nullptr;
+  int64_t batch_bytes = 0;
+  const void* batch_key[8] = {};
+  cudaGraphExec_t batch_exec = nullptr;
+  cudaStream_t batch_stream = nullptr;
+  cudaEvent_t batch_ev = nullptr;
+  int batch_graph_ok = 1;
+  int batch_graph_used = 0;
 };
 
 namespace femk {

@@ -579,7 +579,7 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
                   p->diag,     p->dmask,     p->dlist,     p->inc_ptr,   p->inc_elem,  p->cols16,
                   p->work,     p->partials,  p->state,     p->work32,    p->vals32,    p->work64b,
                   p->sell_ptr, p->sell_src,  p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32,
-                  p->bar};
+                  p->bar,      p->batch_ws};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->state_host) cudaFreeHost(p->state_host);
@@ -592,6 +592,9 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
     if (e) cudaEventDestroy(e);
   if (p->mx_stream) cudaStreamDestroy(p->mx_stream);
   if (p->mx_host) cudaFreeHost(p->mx_host);
+  if (p->batch_exec) cudaGraphExecDestroy(p->batch_exec);
+  if (p->batch_ev) cudaEventDestroy(p->batch_ev);
+  if (p->batch_stream) cudaStreamDestroy(p->batch_stream);
   cudaSetDevice(cur);
   delete p;
   return FEMK_OK;
@@ -642,6 +645,8 @@ extern "C" int femk_plan_get_info(const femk_plan* p, femk_plan_info* out) {
   out->cols16 = p->cols16 ? 1 : 0;
   out->device = p->device;
   out->sell_nnz = p->sell_src ? p->sell_nnz : 0;
+  out->batch_graph = p->batch_graph_used;
+  out->pad = 0;
   return FEMK_OK;
 }
 

@@ -205,6 +205,28 @@ class FemPlan:
         _lib.check(st, allow=(_lib.FEMK_NOT_CONVERGED,))
         return x, inner.value, outer.value, rr.value, st
 
+    def pcg_batched(self, row_off, vals, b, x=None, inv_diag=None, tol=1e-8, atol=0.0, maxiter=20_000,
+                    tile_rows=2048, blocks_per_sm=2):
+        """Independent Jacobi-PCGs of the problems owning rows [row_off[k], row_off[k+1]).
+
+        Returns (x, iterations i32[nprob], relres f64[nprob], status i32[nprob], return status)."""
+        ro = np.ascontiguousarray(np.asarray(row_off, dtype=np.int64))
+        nprob = ro.size - 1
+        x = torch.zeros(self.n, dtype=torch.float64, device=self.device) if x is None else x
+        it = np.zeros(nprob, dtype=np.int32)
+        rel = np.zeros(nprob, dtype=np.float64)
+        stv = np.zeros(nprob, dtype=np.int32)
+        c = ctypes.c_void_p
+        st = self._lib.femk_pcg_batched(self._h, nprob, c(ro.ctypes.data), _lib.ptr(vals), _lib.ptr(b), _lib.ptr(x),
+                                        _lib.ptr(inv_diag), float(tol), float(atol), int(maxiter), int(tile_rows),
+                                        int(blocks_per_sm), c(it.ctypes.data), c(rel.ctypes.data), c(stv.ctypes.data),
+                                        _lib.stream_handle())
+        _lib.check(st, allow=(_lib.FEMK_NOT_CONVERGED,))
+        info = _lib.PlanInfo()
+        _lib.check(self._lib.femk_plan_get_info(self._h, ctypes.byref(info)))
+        self.batch_graph = bool(info.batch_graph)
+        return x, it, rel, stv, st
+
     def adjoint_grad(self, param, u, lam, mode=_lib.COEF_EXP, scale=1.0, out=None):
         out = torch.empty(self.ntet, dtype=torch.float64, device=self.device) if out is None else out
         _lib.check(self._lib.femk_adjoint_grad(self._h, _lib.ptr(param), int(mode), float(scale), _lib.ptr(u),

@@ -101,3 +101,15 @@ def test_product_never_imports_the_oracle():
             if fn.endswith((".py", ".cu", ".cuh")):
                 src = open(os.path.join(dirpath, fn)).read()
                 assert "import oracle" not in src and "from oracle" not in src, fn
+
+
+def test_batched_workload_is_deterministic():
+    from jno_b200.batch import batched_workload
+
+    s1, p1 = batched_workload(count=6, seed=42, lo=2, hi=5)
+    s2, p2 = batched_workload(count=6, seed=42, lo=2, hi=5)
+    assert np.array_equal(s1, s2) and s1.min() >= 2 and s1.max() <= 5
+    for (a, b_, c), (d, e, f) in zip(p1, p2):
+        assert np.array_equal(a, d) and np.array_equal(b_, e) and np.array_equal(c, f)
+        n = int(round((len(b_) / 6) ** (1 / 3)))
+        assert len(a) == (n + 1) ** 3

@@ -1,0 +1,73 @@
+"""GPU: the batched persistent PCG against per-problem oracle solves (same iteration, jax cg
+semantics per problem), and the schedule autotuner."""
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from oracle import assemble as oa  # noqa: E402
+from oracle import mesh as om  # noqa: E402
+from oracle import pcg as op  # noqa: E402
+
+
+def _problems(sides):
+    out = []
+    for i, n in enumerate(sides):
+        pts, tets = om.equi_distant_box(n, n, n)
+        pts = om.jitter_interior(pts, n, n, n, seed=100 + i)
+        out.append((pts, tets, om.logk_field(len(tets), 500 + i)))
+    return out
+
+
+@pytest.mark.parametrize("tile_rows,bps", [(32, 2), (64, 1), (2048, 2)])
+def test_batched_matches_per_problem_oracle(tile_rows, bps):
+    from jno_b200.batch import BatchedPoisson
+
+    sides = [3, 5, 1, 8, 4, 6, 2, 12]
+    probs = _problems(sides)
+    batch = BatchedPoisson([(p, t) for p, t, _ in probs])
+    vals, b = batch.assemble([lk for _, _, lk in probs])
+    x, it, rel = batch.solve(vals, b, tol=1e-8, schedule={"tile_rows": tile_rows, "blocks_per_sm": bps})
+    xs = batch.split(x)
+    for k, (pts, tets, lk) in enumerate(probs):
+        bnd = om.boundary_nodes(tets, 1)
+        s = oa.assemble(pts, tets, 1, bnd, np.exp(lk))
+        xo, ito, _ = op.pcg(s.csr(), s.b, oa.jacobi_inverse(oa.matrix_diagonal(s)), tol=1e-8)
+        assert abs(int(it[k]) - ito) <= 1, (k, it[k], ito)
+        nx = max(np.linalg.norm(xo), 1e-300)
+        assert np.linalg.norm(xs[k] - xo) <= 1e-7 * nx + 1e-300, k
+        if np.linalg.norm(s.b) > 0:
+            assert rel[k] <= 2e-8
+    assert it[2] == 0  # a single voxel has no interior DOF: b = 0, no iteration
+
+
+def test_autotuner_caches_a_schedule(tmp_path, monkeypatch):
+    from jno_b200 import tuner
+    from jno_b200.batch import BatchedPoisson
+
+    monkeypatch.setenv("JNO_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    monkeypatch.setattr(tuner, "CANDIDATES", [(64, 1), (128, 2)])
+    probs = _problems([4, 7, 3])
+    batch = BatchedPoisson([(p, t) for p, t, _ in probs])
+    vals, b = batch.assemble([lk for _, _, lk in probs])
+    inv = batch.plan.jacobi(vals)
+    sched = tuner.batched_schedule(batch, vals, b, inv, 1e-8)
+    assert (sched["tile_rows"], sched["blocks_per_sm"]) in [(64, 1), (128, 2)]
+    assert set(sched["tried"]) == {"64x1", "128x2"}
+    assert tuner.batched_schedule(batch, vals, b, inv, 1e-8) == sched  # served from the cache
+
+
+def test_batched_replay_is_bitwise_reproducible():
+    """The second solve replays the captured graph; the reductions have a fixed order, so the
+    result is bit-identical."""
+    from jno_b200.batch import BatchedPoisson
+
+    probs = _problems([5, 9, 3, 7])
+    batch = BatchedPoisson([(p, t) for p, t, _ in probs])
+    vals, b = batch.assemble([lk for _, _, lk in probs])
+    sched = {"tile_rows": 64, "blocks_per_sm": 2}
+    x1, it1, rel1 = batch.solve(vals, b, schedule=sched)
+    x2, it2, rel2 = batch.solve(vals, b, schedule=sched)
+    assert torch.equal(x1, x2) and np.array_equal(it1, it2) and np.array_equal(rel1, rel2)
