@@ -41,6 +41,8 @@ def parse_args():
     ap.add_argument("--order", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--solver", choices=["fp64", "mixed", "matfree"], default="fp64",
+                    help="solver of the timed step (fp64 is the headline; the others serve profiling runs)")
     return ap.parse_args()
 
 
@@ -205,7 +207,7 @@ def run_reference(args):
 # ------------------------------------------------------------------------------------------ ours
 def roofline_traffic():
     """DRAM bytes per SpMV launch from the committed ncu summary, if one exists."""
-    path = os.path.join(ROOT, "profiles", "csr_spmv_p1_128.md")
+    path = os.path.join(ROOT, "profiles", "sell_spmv_fp64_p1_128.md")
     if not os.path.exists(path):
         return None
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
@@ -398,7 +400,13 @@ def run_ours(args):
         if record:
             e1.record()
         x.zero_()
-        _, it, rel, st = plan.pcg(vals, b, x, inv, tol=1e-8)
+        if args.solver == "mixed":
+            _, it, _, rel, st = plan.pcg_mixed(vals, b, inv, x, tol=1e-8)
+        elif args.solver == "matfree":
+            plan.jacobi_matfree(lk, out=inv)
+            _, it, rel, st = plan.pcg_matfree(lk, b, x, inv, tol=1e-8)
+        else:
+            _, it, rel, st = plan.pcg(vals, b, x, inv, tol=1e-8)
         if record:
             e2.record()
             phase["pending"] = (e0, e1, e2)
@@ -482,8 +490,16 @@ def run_ours(args):
         torch.cuda.synchronize()
         return s0.elapsed_time(s1) / reps
 
-    sell_ms = time_launches(lambda: plan.spmv_prepared(xr, yr))
+    sell_standalone_ms = time_launches(lambda: plan.spmv_prepared(xr, yr))
     csr_ms = time_launches(lambda: plan.spmv(vals, xr, yr))
+    # the same kernel as it runs inside the CG loop: library-recorded CUDA events around every
+    # step SpMV of two profiled solves (graph replay is off while profiling)
+    plan.set_profiling(True)
+    for i in range(2):
+        step(i)
+    step_ms_tot, upd_ms_tot, pup_ms_tot, prof_iters = plan.profile()
+    plan.set_profiling(False)
+    sell_ms = step_ms_tot / max(prof_iters, 1)
     col_bytes = 2 if plan.cols16 else 4
     # bytes the kernel must move: every stored sliced-ELL entry (value + column), slice offsets,
     # x read once, y written once
@@ -503,6 +519,10 @@ def run_ours(args):
                 "traffic": roofline_traffic(),
                 "kernel": f"k_sell (FP64 sliced-ELL SpMV, {'int16' if plan.cols16 else 'int32'} column offsets)",
                 "bytes_per_launch": sell_bytes, "ms_per_launch": sell_ms, "peak_source": peak_src,
+                "timing": f"CUDA events around each CG-step SpMV inside {prof_iters} profiled iterations",
+                "in_loop_ms": {"step_spmv": sell_ms, "update": upd_ms_tot / max(prof_iters, 1),
+                               "p_update": pup_ms_tot / max(prof_iters, 1)},
+                "standalone_ms": sell_standalone_ms,
                 "csr_equivalent_GBps": csr_bytes / (sell_ms / 1e3) / 1e9,
                 "canonical_csr_kernel": {"ms": csr_ms, "GB/s": csr_bytes / (csr_ms / 1e3) / 1e9,
                                          "bytes_per_launch": csr_bytes}}
@@ -553,7 +573,8 @@ def run_ours(args):
         variants["matrix_free_fp64"] = {"value": world * ndof / (ms_f / 1e3), "unit": "DOF/s", "ms_per_step": ms_f,
                                         "iters": float(np.mean(mf_info["it"]))}
         variants["spmv_csr_fp64"] = {"GB/s": csr_bytes / (csr_ms / 1e3) / 1e9, "ms": csr_ms}
-        variants["spmv_sell_fp64"] = {"GB/s": achieved, "frac_of_peak": achieved / peak, "ms": sell_ms}
+        variants["spmv_sell_fp64"] = {"GB/s": achieved, "frac_of_peak": achieved / peak, "ms_in_loop": sell_ms,
+                                      "ms_standalone": sell_standalone_ms}
         variants.update(p2_variants(args, world, dev, timed))
         variants["adjoint_p1_64"] = adjoint_variant(dev)
         variants["batched_256"] = batched_variant(dev)
@@ -599,6 +620,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded jittered Kuhn cube, lognormal P0 k)",
             "config": {"workload": workload_desc(args.n, args.order, T, ndof, nnz), "order": args.order,
+                       "solver": args.solver,
                        "n_hex_side": args.n, "ntet": T, "dofs": ndof, "nnz": nnz, "tol": 1e-8,
                        "iterations_mean": iters_mean, "max_relres": float(np.max(rel_seen)),
                        "assemble_ms": float(np.mean(asm_ms)), "solve_ms": float(np.mean(solve_ms)),

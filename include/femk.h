@@ -134,6 +134,13 @@ int femk_spmv(const femk_plan* plan, const double* vals_dev, const double* x_dev
 int femk_prepare_operator(const femk_plan* plan, const double* vals_dev, void* stream);
 int femk_spmv_prepared(const femk_plan* plan, const double* x_dev, double* y_dev, void* stream);
 
+/* Opt-in CUDA-event timing of the FP64 CG loop's kernels (step SpMV, x/r/z update, p update),
+ * accumulated over the iterations that ran since profiling was switched on. While it is on,
+ * femk_pcg enqueues its chunks directly instead of replaying the chunk graph. */
+int femk_set_profiling(femk_plan* plan, int on);
+int femk_get_profile(const femk_plan* plan, double* step_ms, double* update_ms, double* pupdate_ms,
+                     int64_t* iterations);
+
 /* y = A x without an assembled matrix: per-element K_e x_e from coordinates and k_e. */
 int femk_spmv_matfree(const femk_plan* plan, const double* param_dev, int coef_mode,
                       double coef_scale, const double* x_dev, double* y_dev, void* stream);

@@ -81,6 +81,8 @@ SIGNATURES = {
     "femk_spmv": [_P, _P, _P, _P, _P],
     "femk_prepare_operator": [_P, _P, _P],
     "femk_spmv_prepared": [_P, _P, _P, _P],
+    "femk_set_profiling": [_P, _I],
+    "femk_get_profile": [_P, _P, _P, _P, _P],
     "femk_spmv_matfree": [_P, _P, _I, _D, _P, _P, _P],
     "femk_pcg": [_P, _P, _P, _P, _P, _D, _D, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_D), _P],
     "femk_pcg_noalloc": [_P, _P, _P, _P, _P, _D, _D, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_D), _P],

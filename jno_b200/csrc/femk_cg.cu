@@ -21,6 +21,7 @@
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
 #include "femk_grid.cuh"
+#include "femk_l2.cuh"
 
 namespace femk {
 namespace {
@@ -187,7 +188,7 @@ __global__ void __launch_bounds__(kThreads) k_csr(const int32_t* __restrict__ in
 }
 
 // The same modes on the sliced-ELL copy of the operator: one thread per row, 32-row slices.
-template <int MODE, typename IDX, int B>
+template <int MODE, typename IDX, int B, int H = 0>
 __global__ void __launch_bounds__(kThreads) k_sell(const int64_t* __restrict__ sptr, const IDX* __restrict__ scols,
                                                   const double* __restrict__ svals, int64_t n, int64_t nslices,
                                                   const double* __restrict__ x, double* __restrict__ y,
@@ -208,8 +209,19 @@ __global__ void __launch_bounds__(kThreads) k_sell(const int64_t* __restrict__ s
     if (row >= n) continue;
     const int64_t b0 = __ldg(sptr + sl);
     const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
-    const double sv =
-        sell_row<double, IDX, GatherX<double>, B>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row, GatherX<double>{x});
+    double sv;
+    if (H == 1)
+      sv = sell_row<double, IDX, GatherXL<double>, B, true>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row,
+                                                           GatherXL<double>{x, l2_evict_last()});
+    else if (H == 2)
+      sv = sell_row<double, IDX, GatherX<double>, B, true>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row,
+                                                          GatherX<double>{x});
+    else if (H == 4)
+      sv = sell_row<double, IDX, GatherXL<double>, B, false>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row,
+                                                            GatherXL<double>{x, l2_evict_last()});
+    else
+      sv = sell_row<double, IDX, GatherX<double>, B>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row,
+                                                    GatherX<double>{x});
     if (MODE == kPlain) {
       y[row] = sv;
     } else if (MODE == kCgStep) {
@@ -391,7 +403,7 @@ __device__ __forceinline__ void update_one(int64_t i, double alpha, double* __re
   acc[1] += ri * ri;
 }
 
-template <bool VEC>
+template <bool VEC, bool H = false>
 __global__ void __launch_bounds__(kThreads) k_update(int64_t n, double* __restrict__ x, double* __restrict__ r,
                                                     double* __restrict__ z, const double* __restrict__ p,
                                                     const double* __restrict__ q, const double* __restrict__ dinv,
@@ -409,35 +421,44 @@ __global__ void __launch_bounds__(kThreads) k_update(int64_t n, double* __restri
     const double2* p2 = reinterpret_cast<const double2*>(p);
     const double2* q2 = reinterpret_cast<const double2*>(q);
     const double2* d2 = reinterpret_cast<const double2*>(dinv);
+    uint64_t pol = 0;
+    if (H) pol = l2_evict_last();
+    auto ld = [&](const double2* a) { return H ? ld_last2(a, pol) : *a; };
+    auto st2 = [&](double2* a, double2 v) {
+      if (H)
+        st_last2(a, v, pol);
+      else
+        *a = v;
+    };
     for (int64_t i = tid; i < n2; i += 2 * nt) {
       const int64_t j = i + nt;
       const bool two = j < n2;
-      const double2 pa = p2[i], qa = q2[i], xa = x2[i], ra = r2[i];
+      const double2 pa = ld(p2 + i), qa = ld(q2 + i), xa = ld(x2 + i), ra = ld(r2 + i);
       double2 pb = pa, qb = qa, xb = xa, rb = ra, da = make_double2(1.0, 1.0), db = da;
       if (two) {
-        pb = p2[j];
-        qb = q2[j];
-        xb = x2[j];
-        rb = r2[j];
+        pb = ld(p2 + j);
+        qb = ld(q2 + j);
+        xb = ld(x2 + j);
+        rb = ld(r2 + j);
       }
       if (dinv) {
-        da = d2[i];
-        if (two) db = d2[j];
+        da = ld(d2 + i);
+        if (two) db = ld(d2 + j);
       }
       double2 ro, zo;
-      x2[i] = make_double2(xa.x + alpha * pa.x, xa.y + alpha * pa.y);
+      st2(x2 + i, make_double2(xa.x + alpha * pa.x, xa.y + alpha * pa.y));
       ro = make_double2(ra.x - alpha * qa.x, ra.y - alpha * qa.y);
       zo = make_double2(da.x * ro.x, da.y * ro.y);
-      r2[i] = ro;
-      z2[i] = zo;
+      st2(r2 + i, ro);
+      st2(z2 + i, zo);
       acc[0] += ro.x * zo.x + ro.y * zo.y;
       acc[1] += ro.x * ro.x + ro.y * ro.y;
       if (two) {
-        x2[j] = make_double2(xb.x + alpha * pb.x, xb.y + alpha * pb.y);
+        st2(x2 + j, make_double2(xb.x + alpha * pb.x, xb.y + alpha * pb.y));
         ro = make_double2(rb.x - alpha * qb.x, rb.y - alpha * qb.y);
         zo = make_double2(db.x * ro.x, db.y * ro.y);
-        r2[j] = ro;
-        z2[j] = zo;
+        st2(r2 + j, ro);
+        st2(z2 + j, zo);
         acc[0] += ro.x * zo.x + ro.y * zo.y;
         acc[1] += ro.x * ro.x + ro.y * ro.y;
       }
@@ -465,6 +486,7 @@ __global__ void __launch_bounds__(kThreads) k_update(int64_t n, double* __restri
 }
 
 // p = z + beta p on plan-owned (16-byte aligned) vectors, two rows per load
+template <bool H = false>
 __global__ void __launch_bounds__(kThreads) k_pupdate(int64_t n, double* __restrict__ p, const double* __restrict__ z,
                                                      const CgState* st) {
   if (st->done) return;
@@ -474,9 +496,16 @@ __global__ void __launch_bounds__(kThreads) k_pupdate(int64_t n, double* __restr
   const int64_t n2 = n >> 1;
   double2* p2 = reinterpret_cast<double2*>(p);
   const double2* z2 = reinterpret_cast<const double2*>(z);
+  uint64_t pol = 0;
+  if (H) pol = l2_evict_last();
   for (int64_t i = tid; i < n2; i += nt) {
-    const double2 a = p2[i], c = z2[i];
-    p2[i] = make_double2(c.x + beta * a.x, c.y + beta * a.y);
+    const double2 a = H ? ld_last2(p2 + i, pol) : p2[i];
+    const double2 c = H ? ld_last2(z2 + i, pol) : z2[i];
+    const double2 o = make_double2(c.x + beta * a.x, c.y + beta * a.y);
+    if (H)
+      st_last2(p2 + i, o, pol);
+    else
+      p2[i] = o;
   }
   if ((n & 1) && tid == 0) p[n - 1] = z[n - 1] + beta * p[n - 1];
 }
@@ -686,12 +715,25 @@ int spmv_grid(const femk_plan* p) { return p->n_sm * (2048 / kThreads); }
 
 inline bool aligned16(const void* a) { return ((uintptr_t)a & 15u) == 0; }
 
+void launch_pupdate(const femk_plan* p, double* pv, const double* z, const CgState* st, cudaStream_t s) {
+  if (p->l2_mode != 0)
+    k_pupdate<true><<<::femk::counted_launch() + wave_grid(k_pupdate<true>, kThreads, p), kThreads, 0, s>>>(p->n, pv,
+                                                                                                         z, st);
+  else
+    k_pupdate<false><<<::femk::counted_launch() + wave_grid(k_pupdate<false>, kThreads, p), kThreads, 0, s>>>(
+        p->n, pv, z, st);
+}
+
 // k_update with two-row loads when every vector it touches is 16-byte aligned
 void launch_update(const femk_plan* p, double* x, double* r, double* z, const double* pv, const double* q,
                    const double* dinv, double* partials, CgState* st, cudaStream_t s) {
   const bool vec = aligned16(x) && aligned16(r) && aligned16(z) && aligned16(pv) && aligned16(q) &&
                    (dinv == nullptr || aligned16(dinv));
-  if (vec)
+  const int hm = p->l2_mode;
+  if (vec && (hm == 1 || hm == 2 || hm == 3 || hm == 4))
+    k_update<true, true><<<::femk::counted_launch() + wave_grid(k_update<true, true>, kThreads, p), kThreads, 0, s>>>(
+        p->n, x, r, z, pv, q, dinv, partials, st);
+  else if (vec)
     k_update<true><<<::femk::counted_launch() + wave_grid(k_update<true>, kThreads, p), kThreads, 0, s>>>(
         p->n, x, r, z, pv, q, dinv, partials, st);
   else
@@ -732,9 +774,24 @@ int launch_op(const femk_plan* p, bool sell, const double* vals, const double* x
   auto go = [&](auto Bc, auto cols) {
     constexpr int B = decltype(Bc)::value;
     using I = std::remove_const_t<std::remove_pointer_t<decltype(cols)>>;
-    const int grid = wave_grid(k_sell<MODE, I, B>, kThreads, p);
-    k_sell<MODE, I, B><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
-        p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+    const int hm = p->l2_mode;
+    if (hm == 1) {
+      const int grid = wave_grid(k_sell<MODE, I, B, 1>, kThreads, p);
+      k_sell<MODE, I, B, 1><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
+          p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+    } else if (hm == 2) {
+      const int grid = wave_grid(k_sell<MODE, I, B, 2>, kThreads, p);
+      k_sell<MODE, I, B, 2><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
+          p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+    } else if (hm == 4) {
+      const int grid = wave_grid(k_sell<MODE, I, B, 4>, kThreads, p);
+      k_sell<MODE, I, B, 4><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
+          p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+    } else {
+      const int grid = wave_grid(k_sell<MODE, I, B>, kThreads, p);
+      k_sell<MODE, I, B><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
+          p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+    }
   };
   const bool c16 = p->sell_c16 && p->sell64_c16;
   if (sell_batch() == 8) {
@@ -792,6 +849,14 @@ int launch_matfree(const femk_plan* p, const MatFree& m, const double* x, double
 // One chunk of kChunk CG iterations on stream ws (CSR operator). Fused: 2 kernels per iteration
 // with the direction double-buffered in P0/P1 (chunks have even length, so every chunk starts
 // with p in P0); otherwise the three-kernel form.
+// Opt-in per-kernel timing of the CG loop (femk_set_profiling): events around the three kernels
+// of every iteration of a chunk; the chunked path runs without graph replay while it is on.
+struct ProfData {
+  cudaEvent_t ev[kChunk][4];
+  double ms[3] = {0.0, 0.0, 0.0};  // step SpMV, update, p update
+  int64_t iters = 0;
+};
+
 int enqueue_chunk(const femk_plan* p, const double* vals, double* x, const double* dinv, bool fused, bool sell,
                   int64_t iters, cudaStream_t ws) {
   const int64_t n = p->n;
@@ -817,9 +882,14 @@ int enqueue_chunk(const femk_plan* p, const double* vals, double* x, const doubl
       }
       launch_update(p, x, r, z, pnew, q, dinv, p->partials, st, ws);
     } else {
+      ProfData* pd = (ProfData*)p->prof;
+      if (pd) cudaEventRecord(pd->ev[it][0], ws);
       FEMK_TRY(launch_op<kCgStep>(p, sell, vals, P0, q, nullptr, nullptr, nullptr, nullptr, st, 0.0, 0.0, ws));
+      if (pd) cudaEventRecord(pd->ev[it][1], ws);
       launch_update(p, x, r, z, P0, q, dinv, p->partials, st, ws);
-      k_pupdate<<<::femk::counted_launch() + wave_grid(k_pupdate, kThreads, p), kThreads, 0, ws>>>(n, P0, z, st);
+      if (pd) cudaEventRecord(pd->ev[it][2], ws);
+      launch_pupdate(p, P0, z, st, ws);
+      if (pd) cudaEventRecord(pd->ev[it][3], ws);
     }
   }
   FEMK_CUDA_TRY(cudaGetLastError());
@@ -846,9 +916,23 @@ int ensure_chunk_graph(femk_plan* p, const double* vals, double* x, const double
   (void)wave_grid(k_sell<kCgStep, int32_t, 16>, kThreads, p);
   (void)wave_grid(k_sell<kCgStep, int16_t, 8>, kThreads, p);
   (void)wave_grid(k_sell<kCgStep, int16_t, 16>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int16_t, 16, 1>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int32_t, 16, 1>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int16_t, 8, 1>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int32_t, 8, 1>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int16_t, 16, 2>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int32_t, 16, 2>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int16_t, 8, 2>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int32_t, 8, 2>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int16_t, 16, 4>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int32_t, 16, 4>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int16_t, 8, 4>, kThreads, p);
+  (void)wave_grid(k_sell<kCgStep, int32_t, 8, 4>, kThreads, p);
+  (void)wave_grid(k_update<true, true>, kThreads, p);
+  (void)wave_grid(k_pupdate<true>, kThreads, p);
   (void)wave_grid(k_update<true>, kThreads, p);
   (void)wave_grid(k_update<false>, kThreads, p);
-  (void)wave_grid(k_pupdate, kThreads, p);
+  (void)wave_grid(k_pupdate<false>, kThreads, p);
   cudaGraph_t g = nullptr;
   set_capturing(true);
   cudaError_t e = cudaStreamBeginCapture(p->cg_stream, cudaStreamCaptureModeThreadLocal);
@@ -931,7 +1015,8 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
   double* q = pv + vs;
   CgState* st = p->state;
   const bool fused = !mf && p->cg_fused;
-  const bool graph = !mf && p->cg_graph;
+  ProfData* pd = (!mf && !fused) ? (ProfData*)p->prof : nullptr;
+  const bool graph = !mf && p->cg_graph && !pd;
   const bool sell = !mf && !fused && p->use_sell && p->sell_src;
   const bool persist = sell && p->cg_persist && p->coop;
   // all solver work runs on the plan's stream, ordered after the caller's stream and before
@@ -975,13 +1060,25 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
         k_dot_pq<<<::femk::counted_launch() + wave_grid(k_dot_pq, kThreads, p), kThreads, 0, ws>>>(n, pv, q,
                                                                                                   p->partials, st);
         launch_update(p, x, r, z, pv, q, dinv, p->partials, st, ws);
-        k_pupdate<<<::femk::counted_launch() + wave_grid(k_pupdate, kThreads, p), kThreads, 0, ws>>>(n, pv, z, st);
+        launch_pupdate(p, pv, z, st, ws);
       }
       FEMK_CUDA_TRY(cudaGetLastError());
       enq += todo;
     } else {
       const int64_t todo = std::min<int64_t>(kChunk, (int64_t)maxiter - enq);
       FEMK_TRY(enqueue_chunk(p, vals, x, dinv, fused, sell, todo, ws));
+      if (pd) {  // time the iterations of this chunk that ran (later ones return at entry)
+        CgState now{};
+        FEMK_CUDA_TRY(cudaMemcpyAsync(&now, st, sizeof(CgState), cudaMemcpyDeviceToHost, ws));
+        FEMK_CUDA_TRY(cudaStreamSynchronize(ws));
+        const int64_t real = std::min<int64_t>(todo, std::max<int64_t>(0, (int64_t)now.iter - enq));
+        for (int64_t it = 0; it < real; ++it)
+          for (int k = 0; k < 3; ++k) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, pd->ev[it][k], pd->ev[it][k + 1]) == cudaSuccess) pd->ms[k] += t;
+          }
+        pd->iters += real;
+      }
       enq += todo;
     }
     CgState* slot_h = hs + (chunk_id & 1);
@@ -1065,6 +1162,38 @@ extern "C" int femk_spmv(const femk_plan* p, const double* vals, const double* x
   clear_error();
   FEMK_CHECK_ARG(p && vals && x && y, "femk_spmv: NULL argument");
   return spmv_csr(p, vals, x, y, (cudaStream_t)stream);
+}
+
+extern "C" int femk_set_profiling(femk_plan* p, int on) {
+  clear_error();
+  FEMK_CHECK_ARG(p, "femk_set_profiling: NULL plan");
+  ProfData* pd = (ProfData*)p->prof;
+  if (pd) {
+    for (auto& row : pd->ev)
+      for (cudaEvent_t e : row)
+        if (e) cudaEventDestroy(e);
+    delete pd;
+    p->prof = nullptr;
+  }
+  if (on) {
+    pd = new ProfData();
+    for (auto& row : pd->ev)
+      for (cudaEvent_t& e : row) FEMK_CUDA_TRY(cudaEventCreate(&e));
+    p->prof = pd;
+  }
+  return FEMK_OK;
+}
+
+extern "C" int femk_get_profile(const femk_plan* p, double* step_ms, double* update_ms, double* pupdate_ms,
+                                int64_t* iterations) {
+  clear_error();
+  FEMK_CHECK_ARG(p, "femk_get_profile: NULL plan");
+  const ProfData* pd = (const ProfData*)p->prof;
+  if (step_ms) *step_ms = pd ? pd->ms[0] : 0.0;
+  if (update_ms) *update_ms = pd ? pd->ms[1] : 0.0;
+  if (pupdate_ms) *pupdate_ms = pd ? pd->ms[2] : 0.0;
+  if (iterations) *iterations = pd ? pd->iters : 0;
+  return FEMK_OK;
 }
 
 extern "C" int femk_prepare_operator(const femk_plan* p, const double* vals, void* stream) {
@@ -1200,7 +1329,6 @@ extern "C" int femk_pcg_noalloc(const femk_plan* p, const double* vals, const do
   double* scratch = nullptr;
   FEMK_TRY(noalloc_scratch(cur, &scratch));
   cudaStream_t s = (cudaStream_t)stream;
-  const int64_t n = p->n;
   double* r = scratch;
   double* z = r + kNoAllocMaxN;
   double* pv = z + kNoAllocMaxN;
@@ -1221,7 +1349,7 @@ extern "C" int femk_pcg_noalloc(const femk_plan* p, const double* vals, const do
     for (int64_t it = 0; it < todo; ++it) {
       FEMK_TRY(launch_csr_into<kCgStep>(p, vals, pv, q, nullptr, nullptr, nullptr, nullptr, partials, st, 0.0, 0.0, s));
       launch_update(p, x, r, z, pv, q, dinv, partials, st, s);
-      k_pupdate<<<::femk::counted_launch() + wave_grid(k_pupdate, kThreads, p), kThreads, 0, s>>>(n, pv, z, st);
+      launch_pupdate(p, pv, z, st, s);
     }
     FEMK_CUDA_TRY(cudaGetLastError());
     enq += todo;

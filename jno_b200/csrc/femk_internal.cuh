@@ -97,6 +97,7 @@ struct femk_plan {
   double* sell_vals = nullptr;   // f64[sell_nnz] values gathered for the current solve
   float* sell_vals32 = nullptr;  // f32[sell_nnz] FP32 values for the mixed-precision inner solve
   int use_sell = 1;
+  int l2_mode = 0;               // L2 eviction hints of the FP64 CG kernels (see l2_hints in femk_spmv.cuh)
   int sell64_c16 = 1;            // FP64 sliced-ELL streams int16 column offsets when available
   // solver workspace (allocated on first use)
   int64_t vstride = 0;          // solver vector stride: n rounded up to 64 (keeps every slot 512-byte aligned)
@@ -132,6 +133,7 @@ struct femk_plan {
   cudaStream_t batch_stream = nullptr;
   cudaEvent_t batch_ev = nullptr;
   int batch_graph_ok = 1;
+  void* prof = nullptr;         // per-kernel CG timing (femk_set_profiling)
   int batch_graph_used = 0;
 };
 

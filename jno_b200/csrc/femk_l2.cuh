@@ -1,0 +1,64 @@
+// L2 eviction-priority hints (PTX createpolicy + L2::cache_hint), per access.
+//
+// The CG matrix stream (values + column offsets, ~3x the L2 size per SpMV at P1 128^3) is loaded
+// with evict_first so it does not push the solver vectors (r, z, p, q, x, D^-1) out of L2; the
+// vector loads and stores carry evict_last so they stay resident across the kernels of an
+// iteration. Hints only: no device or context state changes.
+#pragma once
+
+#include <stdint.h>
+
+namespace femk {
+
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+// streaming (read-once) loads, no L1 allocation
+__device__ __forceinline__ double ld_first(const double* a, uint64_t pol) {
+  double v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_first(const float* a, uint64_t pol) {
+  float v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ int32_t ld_first(const int32_t* a, uint64_t pol) {
+  int32_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ int16_t ld_first(const int16_t* a, uint64_t pol) {
+  int16_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s16 %0, [%1], %2;" : "=h"(v) : "l"(a), "l"(pol));
+  return v;
+}
+
+// vector traffic kept in L2
+__device__ __forceinline__ double2 ld_last2(const double2* a, uint64_t pol) {
+  double2 v;
+  asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_last2(double2* a, double2 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(a), "d"(v.x), "d"(v.y), "l"(pol) : "memory");
+}
+__device__ __forceinline__ double ld_last(const double* a, uint64_t pol) {
+  double v;
+  asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_last(double* a, double v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
+}
+
+}  // namespace femk

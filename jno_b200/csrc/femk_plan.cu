@@ -572,6 +572,7 @@ int create_impl(femk_plan* p, const double* xyz, const int32_t* tets, const uint
 
 extern "C" int femk_plan_destroy(femk_plan* p) {
   if (!p) return FEMK_OK;
+  if (p->prof) femk_set_profiling(p, 0);
   int cur = 0;
   cudaGetDevice(&cur);
   cudaSetDevice(p->device);
@@ -620,6 +621,9 @@ extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int3
   if (const char* e = std::getenv("FEMK_CG_GRAPH")) p->cg_graph = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_SELL")) p->use_sell = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_SELL64_C16")) p->sell64_c16 = std::atoi(e) != 0;
+  // measured on B200 (FP64 PCG to 1e-8): P1 128^3 48.7 ms with hints (mode 1) vs 52.0 ms without;
+  // P2 64^3 117 ms without vs 168 ms with, so P2 plans stream without them
+  p->l2_mode = std::getenv("FEMK_L2HINT") ? femk::l2_hints() : (order == 1 ? 1 : 0);
   if (const char* e = std::getenv("FEMK_CG_PERSIST")) p->cg_persist = std::atoi(e) != 0;
   cudaDeviceGetAttribute(&p->coop, cudaDevAttrCooperativeLaunch, p->device);
   p->nvert = nvert;

@@ -13,6 +13,8 @@
 
 #include <type_traits>
 
+#include "femk_l2.cuh"
+
 namespace femk {
 
 // column of entry k of `row`: an absolute int32 index, or an int16 offset from the row
@@ -36,6 +38,26 @@ struct GatherXcg {
   const V* __restrict__ x;
   __device__ __forceinline__ V operator()(int64_t j) const { return __ldcg(x + j); }
 };
+// x[j] through the read-only path with an L2 evict_last hint (vectors stay resident)
+template <typename V>
+struct GatherXL {
+  const V* __restrict__ x;
+  uint64_t pol;
+  __device__ __forceinline__ V operator()(int64_t j) const;
+};
+template <>
+__device__ __forceinline__ double GatherXL<double>::operator()(int64_t j) const {
+  double v;
+  asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(x + j), "l"(pol));
+  return v;
+}
+template <>
+__device__ __forceinline__ float GatherXL<float>::operator()(int64_t j) const {
+  float v;
+  asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(x + j), "l"(pol));
+  return v;
+}
+
 struct GatherDirection {
   const double* __restrict__ z;
   const double* __restrict__ p;
@@ -104,10 +126,12 @@ __device__ __forceinline__ int32_t sell_col(const int16_t* __restrict__ cb, int3
 
 // Row sum of one thread's row. vals/cols point at the row's first entry (slice base + lane);
 // entry k sits at offset 32k. Index arithmetic is 32-bit (n < 2^31 is checked at plan build).
-template <typename V, typename I, typename G, int B = 8>
+template <typename V, typename I, typename G, int B = 8, bool HINT = false>
 __device__ __forceinline__ V sell_row(const V* __restrict__ vb, const I* __restrict__ cb, int32_t w, int32_t row,
                                       const G& gx) {
   V acc = V(0);
+  uint64_t pol = 0;
+  if (HINT) pol = l2_evict_first();
   for (int32_t k0 = 0; k0 < w; k0 += B) {
     V v[B];
     int32_t c[B];
@@ -115,8 +139,13 @@ __device__ __forceinline__ V sell_row(const V* __restrict__ vb, const I* __restr
     for (int u = 0; u < B; ++u) {
       const bool ok = k0 + u < w;
       const int32_t j = (k0 + u) * 32;
-      v[u] = ok ? __ldcs(vb + j) : V(0);
-      c[u] = ok ? sell_col(cb, j, row) : row;
+      if (HINT) {
+        v[u] = ok ? ld_first(vb + j, pol) : V(0);
+        c[u] = ok ? (sizeof(I) == 2 ? row + (int32_t)ld_first(cb + j, pol) : (int32_t)ld_first(cb + j, pol)) : row;
+      } else {
+        v[u] = ok ? __ldcs(vb + j) : V(0);
+        c[u] = ok ? sell_col(cb, j, row) : row;
+      }
     }
 #pragma unroll
     for (int u = 0; u < B; ++u)
@@ -124,6 +153,12 @@ __device__ __forceinline__ V sell_row(const V* __restrict__ vb, const I* __restr
   }
   return acc;
 }
+
+// L2 eviction hints of the FP64 CG kernels, chosen per plan (FEMK_L2HINT overrides, for comparison runs):
+// 0 none; 1 matrix evict_first + x gathers and vector kernels evict_last; 2 matrix evict_first +
+// vector kernels evict_last (plain gathers); 3 vector kernels only; 4 matrix ld.global.cs (already
+// evict-first) + x gathers and vector kernels evict_last
+int l2_hints();
 
 // entries per batch of the FP64 sliced-ELL row loop (FEMK_SELL_BATCH=8|16 overrides for tuning);
 // the FP32 loop always uses 8 (16 doubles its registers and halves its occupancy)

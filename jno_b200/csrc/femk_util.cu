@@ -38,6 +38,15 @@ int resident_blocks(const void* fn, int threads) {
   return b;
 }
 
+int l2_hints() {
+  static int h = [] {
+    const char* e = std::getenv("FEMK_L2HINT");
+    const int v = e ? std::atoi(e) : 1;
+    return v >= 0 && v <= 4 ? v : 1;
+  }();
+  return h;
+}
+
 int sell_batch() {
   static int b = [] {
     const char* e = std::getenv("FEMK_SELL_BATCH");

@@ -165,6 +165,16 @@ class FemPlan:
         _lib.check(self._lib.femk_spmv_prepared(self._h, _lib.ptr(x), _lib.ptr(out), _lib.stream_handle()))
         return out
 
+    def set_profiling(self, on=True):
+        _lib.check(self._lib.femk_set_profiling(self._h, 1 if on else 0))
+
+    def profile(self):
+        """(step SpMV ms, update ms, p-update ms, iterations) accumulated while profiling is on."""
+        v = [ctypes.c_double(0.0) for _ in range(3)]
+        it = ctypes.c_int64(0)
+        _lib.check(self._lib.femk_get_profile(self._h, *[ctypes.byref(x) for x in v], ctypes.byref(it)))
+        return v[0].value, v[1].value, v[2].value, it.value
+
     def spmv_matfree(self, param, x, mode=_lib.COEF_EXP, scale=1.0, out=None):
         out = torch.empty(self.n, dtype=torch.float64, device=self.device) if out is None else out
         _lib.check(self._lib.femk_spmv_matfree(self._h, _lib.ptr(param), int(mode), float(scale), _lib.ptr(x),

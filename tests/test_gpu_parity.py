@@ -275,3 +275,19 @@ def test_jno_surface_end_to_end():
 
 def plan_dirichlet(fem):
     return fem.plan.n_dirichlet
+
+
+def test_profiled_solve_matches_and_times_every_iteration():
+    pf, cf, tets, p1 = _mesh(12, 1)
+    logk = om.logk_field(len(tets), 1003)
+    plan = _plan(p1, tets, 1)
+    vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
+    inv = plan.jacobi(vals)
+    u0, it0, _, _ = plan.pcg(vals, b, inv_diag=inv)
+    plan.set_profiling(True)
+    u1, it1, _, _ = plan.pcg(vals, b, inv_diag=inv)
+    step, upd, pup, iters = plan.profile()
+    plan.set_profiling(False)
+    assert it1 == it0 and iters == it1
+    assert torch.equal(u0, u1)  # same kernels, same order: bit-identical with or without graph replay
+    assert step > 0 and upd > 0 and pup > 0
