@@ -111,6 +111,20 @@ int femk_plan_export(const femk_plan* plan, int32_t* indptr_dev, int32_t* indice
 int femk_assemble(const femk_plan* plan, const double* param_dev, int coef_mode, double coef_scale,
                   double f, const double* g_dev, double* vals_dev, double* b_dev, void* stream);
 
+/*
+ * Compact export of assembled values: the canonical CSR entries with |v| > 0, in CSR order (rows
+ * ascending, columns ascending). Exact zeros (the zeroed Dirichlet rows and columns, values that
+ * summed to 0) and NaNs are dropped.
+ *   vals_dev f64[nnz] (from femk_assemble), indptr_out_dev i32[n+1],
+ *   indices_out_dev i32[cap], vals_out_dev f64[cap], *nnz_out = kept entries.
+ * The call waits on `stream` for the count (one 8-byte device-to-host read) and returns
+ * FEMK_EINVAL without writing entries when it exceeds cap; cap = plan nnz always suffices.
+ * Replaces compress_eager (jno/utils/solver/fem_utils.py:4063-4091) on the non-parametric linear
+ * route (jno/utils/solver/fem_native.py:3371-3379).
+ */
+int femk_compact(const femk_plan* plan, const double* vals_dev, int32_t* indptr_out_dev, int32_t* indices_out_dev,
+                 double* vals_out_dev, int64_t cap, int64_t* nnz_out, void* stream);
+
 /* Unit-coefficient element matrices K_hat f64[ntet*nd*nd] and loads F_hat f64[ntet*nd]
  * (either may be NULL). Replaces the per-cell jacfwd of fem_native.py:2333-2334 for k = 1. */
 int femk_element_matrices(const femk_plan* plan, double* khat_dev, double* fhat_dev, void* stream);

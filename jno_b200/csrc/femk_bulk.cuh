@@ -1,0 +1,180 @@
+// Sliced-ELL SpMV with the matrix streamed into shared memory by the bulk-copy (TMA) engine.
+//
+// The thread-per-row SELL kernel issues every matrix load itself and then gathers x through the
+// columns it loaded: two dependent round trips per slice, so a warp has DRAM bytes in flight only
+// during the first. Here each warp keeps a ring of S slice buffers in shared memory: lane 0 issues
+// one cp.async.bulk for a slice's values and one for its columns (completion counted in bytes on
+// the stage's mbarrier) S slices ahead of the slice the warp computes, so the copy engine keeps the
+// next slices' bytes in flight while the lanes gather and accumulate the current one.
+//
+// Slice layout (unchanged from the SELL-32 operator): slice s holds entries [sptr[s], sptr[s+1]),
+// column-major, entry k of row 32s + l at sptr[s] + 32k + l; the width w = (sptr[s+1]-sptr[s])/32
+// must be <= WMAX. Values start 256-byte and columns 64-byte aligned (sptr is a multiple of 32),
+// and both byte counts are multiples of 16, as cp.async.bulk requires.
+//
+// Row sums are accumulated in k order exactly as sell_row does (acc += v_k * x[c_k]), so a row's
+// result is bit-identical to the register-streaming kernel's.
+//
+// Waits are bounded: a stage that does not complete within kBulkSpinCycles sets *err and the warp
+// stops issuing; before returning it waits (bounded again) for the copies it has in flight, so no
+// copy lands in shared memory after the block has exited.
+#pragma once
+
+#include <stdint.h>
+
+#include "femk_l2.cuh"
+#include "femk_spmv.cuh"
+
+namespace femk {
+
+constexpr long long kBulkSpinCycles = 2000000000LL;  // about one second at the B200 boost clock
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred P;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// bounded wait for the phase with the given parity to complete; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > kBulkSpinCycles) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar, uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
+      ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+      : "memory");
+}
+
+// Shared memory one warp needs: S stages of [32*WMAX values][32*WMAX columns] + S mbarriers + S widths.
+template <typename V, typename IDX, int WMAX, int S>
+struct BulkRing {
+  static constexpr int kVal = 32 * WMAX * (int)sizeof(V);
+  static constexpr int kCol = ((32 * WMAX * (int)sizeof(IDX)) + 127) / 128 * 128;
+  static constexpr int kStage = kVal + kCol;
+  static constexpr int kHead = 128;  // S mbarriers (8 B) + S widths (4 B), padded
+  static constexpr int kWarpBytes = kHead + S * kStage;
+  static_assert(S * 12 <= kHead, "ring header too small");
+  static_assert(kVal % 128 == 0, "stage alignment");
+};
+
+// Every slice of this warp (global warp g takes slices g, g + NW, ...): for each row,
+// epi(row, row_sum). Returns false if a wait timed out (and sets *err to errval).
+template <typename V, typename IDX, int WMAX, int S, typename G, typename Epi>
+__device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64_t* __restrict__ sptr,
+                                               const IDX* __restrict__ cols, const V* __restrict__ vals, int64_t n,
+                                               int64_t nslices, int64_t g, int64_t NW, const G& gx, Epi&& epi,
+                                               int* err, int errval) {
+  using R = BulkRing<V, IDX, WMAX, S>;
+  const int lane = threadIdx.x & 31;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(wsmem);
+  int32_t* wid = reinterpret_cast<int32_t*>(wsmem + 8 * S);
+  unsigned char* stages = wsmem + R::kHead;
+  uint64_t pol = 0;
+  if (lane == 0) {
+    pol = l2_evict_first();
+    for (int s = 0; s < S; ++s) mbar_init(bar + s, 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+  // lane 0: stream slice `sl` into stage `s`
+  auto issue = [&](int64_t sl, int s) {
+    const int64_t b0 = __ldg(sptr + sl);
+    const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
+    wid[s] = w;
+    const uint32_t vb = (uint32_t)(32 * w * (int)sizeof(V));
+    const uint32_t cb = (uint32_t)(32 * w * (int)sizeof(IDX));
+    unsigned char* st = stages + s * R::kStage;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(bar + s, vb + cb);  // with w == 0 this arrival alone completes the phase
+    if (w > 0) {
+      bulk_g2s(st, vals + b0, vb, bar + s, pol);
+      bulk_g2s(st + R::kVal, cols + b0, cb, bar + s, pol);
+    }
+  };
+  int64_t issued = 0;  // slices issued so far (lane 0's count; slice i lives in stage i % S)
+  if (lane == 0)
+    for (int s = 0; s < S; ++s) {
+      const int64_t sl = g + (int64_t)s * NW;
+      if (sl >= nslices) break;
+      issue(sl, s);
+      ++issued;
+    }
+  __syncwarp();
+  bool ok = true;
+  int64_t i = 0;
+  for (int64_t sl = g; sl < nslices; sl += NW, ++i) {
+    const int s = (int)(i % S);
+    const uint32_t parity = (uint32_t)((i / S) & 1);
+    // warp-uniform outcome: a lane that timed out takes the whole warp out of the loop
+    if (!__all_sync(0xffffffffu, mbar_wait(bar + s, parity))) {
+      ok = false;
+      break;
+    }
+    const int32_t w = wid[s];
+    const V* sv = reinterpret_cast<const V*>(stages + s * R::kStage);
+    const IDX* sc = reinterpret_cast<const IDX*>(stages + s * R::kStage + R::kVal);
+    const int64_t row = sl * 32 + lane;
+    const bool live = row < n;  // rows past n in the last slice gather nothing
+    V xg[WMAX];
+#pragma unroll
+    for (int k = 0; k < WMAX; ++k) {
+      if (k < w && live) {
+        const IDX c = sc[k * 32 + lane];
+        xg[k] = gx(sizeof(IDX) == 2 ? (int64_t)row + (int64_t)c : (int64_t)c);
+      }
+    }
+    V acc = V(0);
+#pragma unroll
+    for (int k = 0; k < WMAX; ++k)
+      if (k < w && live) acc += sv[k * 32 + lane] * xg[k];
+    __syncwarp();  // every lane is done with stage s before it is refilled
+    if (lane == 0) {
+      const int64_t nsl = g + (i + S) * NW;
+      if (nsl < nslices) {
+        issue(nsl, s);
+        ++issued;
+      }
+    }
+    __syncwarp();
+    if (live) epi(row, acc);
+  }
+  if (!ok) {
+    if (lane == 0) {
+      atomicExch(err, errval);
+      // drain: wait (bounded) for every copy this warp still has in flight
+      for (int64_t j = i; j < issued; ++j) mbar_wait(bar + (int)(j % S), (uint32_t)((j / S) & 1));
+    }
+    __syncwarp();
+  }
+  return ok;
+}
+
+}  // namespace femk

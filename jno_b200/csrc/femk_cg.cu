@@ -17,6 +17,7 @@
 #include <mutex>
 #include <string>
 
+#include "femk_bulk.cuh"
 #include "femk_element.cuh"
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
@@ -32,9 +33,9 @@ constexpr int kChunk = 16;  // iterations enqueued between looks at the done fla
 // ---------------------------------------------------------------------------------------------
 // reductions: per-block partials + last-block finish
 // ---------------------------------------------------------------------------------------------
-template <int NV>
+template <int NV, int THREADS = kThreads>
 __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* partials) {
-  __shared__ double red[NV][kThreads / 32];
+  __shared__ double red[NV][THREADS / 32];
 #pragma unroll
   for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
   if ((threadIdx.x & 31) == 0) {
@@ -46,14 +47,14 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* part
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
       double t = 0.0;
-      for (int w = 0; w < kThreads / 32; ++w) t += red[j][w];
+      for (int w = 0; w < THREADS / 32; ++w) t += red[j][w];
       partials[(int64_t)blockIdx.x * NV + j] = t;
     }
   }
 }
 
 // Returns true in every thread of the last block to finish; `out` then holds the grid totals.
-template <int NV>
+template <int NV, int THREADS = kThreads>
 __device__ __forceinline__ bool grid_finish(double* partials, uint32_t* ticket, double (&out)[NV]) {
   __shared__ bool last;
   __threadfence();
@@ -68,12 +69,12 @@ __device__ __forceinline__ bool grid_finish(double* partials, uint32_t* ticket, 
   double v[NV];
 #pragma unroll
   for (int j = 0; j < NV; ++j) v[j] = 0.0;
-  // the partials of up to 4*kThreads blocks are loaded before any is added (one round trip)
-  for (int b0 = threadIdx.x; b0 < (int)gridDim.x; b0 += 4 * kThreads) {
+  // the partials of up to 4*THREADS blocks are loaded before any is added (one round trip)
+  for (int b0 = threadIdx.x; b0 < (int)gridDim.x; b0 += 4 * THREADS) {
     double t[4][NV];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      const int b = b0 + u * kThreads;
+      const int b = b0 + u * THREADS;
 #pragma unroll
       for (int j = 0; j < NV; ++j) t[u][j] = b < (int)gridDim.x ? __ldcg(partials + (int64_t)b * NV + j) : 0.0;
     }
@@ -82,7 +83,7 @@ __device__ __forceinline__ bool grid_finish(double* partials, uint32_t* ticket, 
 #pragma unroll
       for (int j = 0; j < NV; ++j) v[j] += t[u][j];
   }
-  __shared__ double red[NV][kThreads / 32];
+  __shared__ double red[NV][THREADS / 32];
 #pragma unroll
   for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
   if ((threadIdx.x & 31) == 0) {
@@ -93,7 +94,7 @@ __device__ __forceinline__ bool grid_finish(double* partials, uint32_t* ticket, 
 #pragma unroll
   for (int j = 0; j < NV; ++j) {
     double t = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) t += red[j][w];
+    for (int w = 0; w < THREADS / 32; ++w) t += red[j][w];
     out[j] = t;
   }
   if (threadIdx.x == 0) *ticket = 0u;
@@ -115,6 +116,7 @@ __global__ void __launch_bounds__(kThreads) k_csr(const int32_t* __restrict__ in
                                                  double* __restrict__ pout, double* __restrict__ partials, CgState* st,
                                                  double tol2, double atol2) {
   constexpr int NV = MODE == kPlain ? 1 : (MODE == kCgStep ? 1 : (MODE == kInit ? 3 : 2));
+  if (MODE == kCgStep && blockIdx.x == 0 && threadIdx.x == 0) st->xpend = 0;  // the last x update is applied
   if (MODE == kCgStep && st->done) return;
   const int lane = threadIdx.x & 31;
   const int sub = lane % L;
@@ -181,6 +183,7 @@ __global__ void __launch_bounds__(kThreads) k_csr(const int32_t* __restrict__ in
     st->done = (!(rs > st->atol2) || st->maxiter <= 0 || st->status != FEMK_OK) ? 1 : 0;
     st->rr_since = tot[1];
     st->beta = 0.0;
+    st->xpend = 0;
   } else {
     st->pq = tot[0];
     st->bb = tot[1];
@@ -197,6 +200,7 @@ __global__ void __launch_bounds__(kThreads) k_sell(const int64_t* __restrict__ s
                                                   double* __restrict__ partials, CgState* st, double tol2,
                                                   double atol2) {
   constexpr int NV = MODE == kPlain ? 1 : (MODE == kCgStep ? 1 : (MODE == kInit ? 3 : 2));
+  if (MODE == kCgStep && blockIdx.x == 0 && threadIdx.x == 0) st->xpend = 0;  // the last x update is applied
   if (MODE == kCgStep && st->done) return;
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
@@ -270,9 +274,53 @@ __global__ void __launch_bounds__(kThreads) k_sell(const int64_t* __restrict__ s
     st->done = (!(rs > st->atol2) || st->maxiter <= 0 || st->status != FEMK_OK) ? 1 : 0;
     st->rr_since = tot[1];
     st->beta = 0.0;
+    st->xpend = 0;
   } else {
     st->pq = tot[0];
     st->bb = tot[1];
+  }
+}
+
+// The same SpMV (kPlain, kCgStep) with the sliced-ELL stream moved into shared memory by bulk
+// copies (femk_bulk.cuh): WPB warps per block, S slices in flight per warp, widths up to WMAX.
+template <int MODE, typename IDX, int WMAX, int S, int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_sell_bulk(const int64_t* __restrict__ sptr,
+                                                       const IDX* __restrict__ scols,
+                                                       const double* __restrict__ svals, int64_t n, int64_t nslices,
+                                                       const double* __restrict__ x, double* __restrict__ y,
+                                                       double* __restrict__ partials, CgState* st, int* err) {
+  extern __shared__ __align__(128) unsigned char bulk_smem[];
+  using R = BulkRing<double, IDX, WMAX, S>;
+  if (MODE == kCgStep) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->xpend = 0;  // the last x update is applied
+    if (st->done) return;
+  }
+  const int wib = threadIdx.x >> 5;
+  const int64_t g = (int64_t)blockIdx.x * WPB + wib;
+  const int64_t NW = (int64_t)gridDim.x * WPB;
+  double acc[1] = {0.0};
+  int* errp = MODE == kCgStep ? &st->status : err;
+  const bool ok = sell_bulk_rows<double, IDX, WMAX, S>(
+      bulk_smem + wib * R::kWarpBytes, sptr, scols, svals, n, nslices, g, NW, GatherXL<double>{x, l2_evict_last()},
+      [&](int64_t row, double sv) {
+        y[row] = sv;
+        if (MODE == kCgStep) acc[0] += __ldg(x + row) * sv;
+      },
+      errp, FEMK_TIMEOUT);
+  if (MODE == kPlain) return;
+  if (!ok && (threadIdx.x & 31) == 0) st->done = 1;
+  block_reduce_store<1, WPB * 32>(acc, partials);
+  double tot[1];
+  if (!grid_finish<1, WPB * 32>(partials, &st->ticket, tot)) return;
+  if (threadIdx.x != 0) return;
+  st->pq = tot[0];
+  st->alpha = st->gamma / tot[0];
+  if (!isfinite(tot[0])) {
+    st->status = FEMK_NONFINITE;
+    st->done = 1;
+  } else if (!(tot[0] > 0.0)) {
+    st->status = FEMK_BREAKDOWN;
+    st->done = 1;
   }
 }
 
@@ -510,6 +558,127 @@ __global__ void __launch_bounds__(kThreads) k_pupdate(int64_t n, double* __restr
   if ((n & 1) && tid == 0) p[n - 1] = z[n - 1] + beta * p[n - 1];
 }
 
+// Split form of the two vector kernels (the default on aligned vectors): z is never stored and x
+// is updated in the direction kernel, which reads p once for both uses.
+//   k_update_r : r -= alpha q; <r, D^-1 r>, <r, r>; stop test; beta     (reads r, q, D^-1; writes r)
+//   k_pupdate_x: x += alpha p; p = D^-1 r + beta p                         (reads x, p, r, D^-1; writes x, p)
+// Every value is formed by the same floating-point operations as in k_update + k_pupdate. The
+// iteration that meets the stop test still owes its x update: k_update_r raises st->xpend, the
+// direction kernel applies x (and p only while the solve runs), and the next CG-step SpMV clears it.
+template <bool H>
+__global__ void __launch_bounds__(kThreads) k_update_r(int64_t n, double* __restrict__ r, const double* __restrict__ q,
+                                                      const double* __restrict__ dinv, double* __restrict__ partials,
+                                                      CgState* st) {
+  if (st->done) return;
+  const double alpha = st->alpha;
+  double acc[2] = {0.0, 0.0};
+  const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  const int64_t nt = (int64_t)gridDim.x * kThreads;
+  const int64_t n2 = n >> 1;
+  double2* r2 = reinterpret_cast<double2*>(r);
+  const double2* q2 = reinterpret_cast<const double2*>(q);
+  const double2* d2 = reinterpret_cast<const double2*>(dinv);
+  uint64_t pol = 0;
+  if (H) pol = l2_evict_last();
+  auto ld = [&](const double2* a) { return H ? ld_last2(a, pol) : *a; };
+  auto one = [&](double2 ra, double2 qa, double2 da, double2* dst) {
+    const double2 ro = make_double2(fma(-alpha, qa.x, ra.x), fma(-alpha, qa.y, ra.y));
+    const double2 zo = make_double2(da.x * ro.x, da.y * ro.y);
+    if (H)
+      st_last2(dst, ro, pol);
+    else
+      *dst = ro;
+    acc[0] += ro.x * zo.x + ro.y * zo.y;
+    acc[1] += ro.x * ro.x + ro.y * ro.y;
+  };
+  for (int64_t i = tid; i < n2; i += 2 * nt) {
+    const int64_t j = i + nt;
+    const bool two = j < n2;
+    const double2 ra = ld(r2 + i), qa = ld(q2 + i);
+    double2 rb = ra, qb = qa, da = make_double2(1.0, 1.0), db = da;
+    if (two) {
+      rb = ld(r2 + j);
+      qb = ld(q2 + j);
+    }
+    if (dinv) {
+      da = ld(d2 + i);
+      if (two) db = ld(d2 + j);
+    }
+    one(ra, qa, da, r2 + i);
+    if (two) one(rb, qb, db, r2 + j);
+  }
+  if ((n & 1) && tid == 0) {
+    const int64_t i = n - 1;
+    const double ri = fma(-alpha, q[i], r[i]);
+    const double zi = dinv ? dinv[i] * ri : ri;
+    r[i] = ri;
+    acc[0] += ri * zi;
+    acc[1] += ri * ri;
+  }
+  block_reduce_store<2>(acc, partials);
+  double tot[2];
+  if (!grid_finish<2>(partials, &st->ticket, tot)) return;
+  if (threadIdx.x != 0) return;
+  const double gamma_new = tot[0];
+  st->beta = gamma_new / st->gamma;
+  st->gamma = gamma_new;
+  st->rr = tot[1];
+  st->iter += 1;
+  st->xpend = 1;
+  const double rs = st->precond ? tot[1] : gamma_new;
+  if (!isfinite(gamma_new) || !isfinite(tot[1])) {
+    st->status = FEMK_NONFINITE;
+    st->done = 1;
+  } else if (!(rs > st->atol2) || st->iter >= st->maxiter) {
+    st->done = 1;
+  }
+}
+
+template <bool H>
+__global__ void __launch_bounds__(kThreads) k_pupdate_x(int64_t n, double* __restrict__ x, double* __restrict__ p,
+                                                       const double* __restrict__ r, const double* __restrict__ dinv,
+                                                       const CgState* st) {
+  if (!st->xpend) return;
+  const bool dir = !st->done;
+  const double alpha = st->alpha, beta = st->beta;
+  const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  const int64_t nt = (int64_t)gridDim.x * kThreads;
+  const int64_t n2 = n >> 1;
+  double2* x2 = reinterpret_cast<double2*>(x);
+  double2* p2 = reinterpret_cast<double2*>(p);
+  const double2* r2 = reinterpret_cast<const double2*>(r);
+  const double2* d2 = reinterpret_cast<const double2*>(dinv);
+  uint64_t pol = 0;
+  if (H) pol = l2_evict_last();
+  auto ld = [&](const double2* a) { return H ? ld_last2(a, pol) : *a; };
+  auto st2 = [&](double2* a, double2 v) {
+    if (H)
+      st_last2(a, v, pol);
+    else
+      *a = v;
+  };
+  if (dir) {
+    for (int64_t i = tid; i < n2; i += nt) {
+      const double2 pa = ld(p2 + i), xa = ld(x2 + i), ra = ld(r2 + i);
+      const double2 da = dinv ? ld(d2 + i) : make_double2(1.0, 1.0);
+      st2(x2 + i, make_double2(fma(alpha, pa.x, xa.x), fma(alpha, pa.y, xa.y)));
+      st2(p2 + i, make_double2(fma(beta, pa.x, da.x * ra.x), fma(beta, pa.y, da.y * ra.y)));
+    }
+    if ((n & 1) && tid == 0) {
+      const int64_t i = n - 1;
+      const double pi = p[i];
+      x[i] = fma(alpha, pi, x[i]);
+      p[i] = fma(beta, pi, (dinv ? dinv[i] : 1.0) * r[i]);
+    }
+  } else {
+    for (int64_t i = tid; i < n2; i += nt) {
+      const double2 pa = ld(p2 + i), xa = ld(x2 + i);
+      st2(x2 + i, make_double2(fma(alpha, pa.x, xa.x), fma(alpha, pa.y, xa.y)));
+    }
+    if ((n & 1) && tid == 0) x[n - 1] = fma(alpha, p[n - 1], x[n - 1]);
+  }
+}
+
 // CG step with the direction update folded in: p_new = z + beta p_old is formed at every gather
 // (and stored by the row's owner), q = A p_new, <p_new, q> -> alpha. Double-buffered p, so no
 // separate p-update pass and no grid-wide wait between the two.
@@ -741,6 +910,31 @@ void launch_update(const femk_plan* p, double* x, double* r, double* z, const do
         p->n, x, r, z, pv, q, dinv, partials, st);
 }
 
+// the split vector kernels (k_update_r, k_pupdate_x); false when a caller vector is not 16-byte aligned
+bool split_ok(const femk_plan* p, const double* x, const double* dinv) {
+  return p->cg_split && aligned16(x) && (dinv == nullptr || aligned16(dinv));
+}
+
+void launch_update_r(const femk_plan* p, double* r, const double* q, const double* dinv, CgState* st,
+                     cudaStream_t s) {
+  if (p->l2_mode != 0)
+    k_update_r<true><<<::femk::counted_launch() + wave_grid(k_update_r<true>, kThreads, p), kThreads, 0, s>>>(
+        p->n, r, q, dinv, p->partials, st);
+  else
+    k_update_r<false><<<::femk::counted_launch() + wave_grid(k_update_r<false>, kThreads, p), kThreads, 0, s>>>(
+        p->n, r, q, dinv, p->partials, st);
+}
+
+void launch_pupdate_x(const femk_plan* p, double* x, double* pv, const double* r, const double* dinv,
+                      const CgState* st, cudaStream_t s) {
+  if (p->l2_mode != 0)
+    k_pupdate_x<true><<<::femk::counted_launch() + wave_grid(k_pupdate_x<true>, kThreads, p), kThreads, 0, s>>>(
+        p->n, x, pv, r, dinv, st);
+  else
+    k_pupdate_x<false><<<::femk::counted_launch() + wave_grid(k_pupdate_x<false>, kThreads, p), kThreads, 0, s>>>(
+        p->n, x, pv, r, dinv, st);
+}
+
 template <int MODE>
 int launch_csr_p(const femk_plan* p, const double* vals, const double* x, double* y, const double* b,
                  const double* dinv, double* z, double* pout, double* partials, CgState* st, double tol2, double atol2,
@@ -765,11 +959,63 @@ int launch_csr(const femk_plan* p, const double* vals, const double* x, double* 
   return launch_csr_p<MODE>(p, vals, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2, s);
 }
 
+// Bulk-copy CG-step SpMV (k_sell_bulk) in the plan's configuration: p->bulk_stages slices in flight
+// per warp, p->bulk_warps warps per block. Returns false (nothing launched) when the plan does not
+// use it: switched off, rows wider than 32 entries, or no 16-bit column offsets.
+template <int S, int WPB, int WMAX>
+bool launch_sell_bulk_cfg(const femk_plan* p, const double* x, double* y, CgState* st, cudaStream_t s,
+                          bool prime) {
+  auto kern = k_sell_bulk<kCgStep, int16_t, WMAX, S, WPB>;
+  constexpr int kSmem = WPB * BulkRing<double, int16_t, WMAX, S>::kWarpBytes;
+  static int per_sm = -1;  // per instantiation: opt-in shared memory size + occupancy, queried once
+  if (per_sm < 0) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WPB * 32, kSmem) != cudaSuccess) {
+      cudaGetLastError();
+      per_sm = 0;
+    }
+  }
+  if (per_sm <= 0) return false;
+  if (prime) return true;
+  const int grid = p->n_sm * std::min(per_sm, 8);
+  kern<<<::femk::counted_launch() + grid, WPB * 32, kSmem, s>>>(p->sell_ptr, p->sell_c16, p->sell_vals, p->n,
+                                                                p->n_slices, x, y, p->partials, st, nullptr);
+  return true;
+}
+
+// prime = true only sets the kernel attribute and reads the occupancy (before a graph capture)
+bool launch_sell_bulk(const femk_plan* p, const double* x, double* y, CgState* st, cudaStream_t s,
+                      bool prime = false) {
+  if (!p->bulk_cfg || !p->sell_c16 || !p->sell64_c16 || p->max_row > 32) return false;
+  if (!aligned16(p->sell_vals) || !aligned16(p->sell_c16)) return false;  // bulk copies start on 16 B
+  const bool narrow = p->max_row <= 16;
+#define FEMK_BULK_CFG(code, S, WPB)                                                         \
+  case code:                                                                                \
+    return narrow ? launch_sell_bulk_cfg<S, WPB, 16>(p, x, y, st, s, prime)                        \
+                  : launch_sell_bulk_cfg<S, WPB, 32>(p, x, y, st, s, prime);
+  switch (p->bulk_cfg) {
+    FEMK_BULK_CFG(24, 2, 4)
+    FEMK_BULK_CFG(28, 2, 8)
+    FEMK_BULK_CFG(34, 3, 4)
+    FEMK_BULK_CFG(38, 3, 8)
+    FEMK_BULK_CFG(44, 4, 4)
+    FEMK_BULK_CFG(42, 4, 2)
+    FEMK_BULK_CFG(62, 6, 2)
+    default:
+      return false;
+  }
+#undef FEMK_BULK_CFG
+}
+
 // The operator of a solve: the sliced-ELL copy (values gathered by prepare_sell) or the CSR.
 template <int MODE>
 int launch_op(const femk_plan* p, bool sell, const double* vals, const double* x, double* y, const double* b,
               const double* dinv, double* z, double* pout, CgState* st, double tol2, double atol2, cudaStream_t s) {
   if (!sell) return launch_csr<MODE>(p, vals, x, y, b, dinv, z, pout, st, tol2, atol2, s);
+  if (MODE == kCgStep && launch_sell_bulk(p, x, y, st, s)) {
+    FEMK_CUDA_TRY(cudaGetLastError());
+    return FEMK_OK;
+  }
   // column offsets in 16 bits when the plan's bandwidth allows it (same values, 2 B less per entry)
   auto go = [&](auto Bc, auto cols) {
     constexpr int B = decltype(Bc)::value;
@@ -883,12 +1129,19 @@ int enqueue_chunk(const femk_plan* p, const double* vals, double* x, const doubl
       launch_update(p, x, r, z, pnew, q, dinv, p->partials, st, ws);
     } else {
       ProfData* pd = (ProfData*)p->prof;
+      const bool split = split_ok(p, x, dinv);
       if (pd) cudaEventRecord(pd->ev[it][0], ws);
       FEMK_TRY(launch_op<kCgStep>(p, sell, vals, P0, q, nullptr, nullptr, nullptr, nullptr, st, 0.0, 0.0, ws));
       if (pd) cudaEventRecord(pd->ev[it][1], ws);
-      launch_update(p, x, r, z, P0, q, dinv, p->partials, st, ws);
+      if (split)
+        launch_update_r(p, r, q, dinv, st, ws);
+      else
+        launch_update(p, x, r, z, P0, q, dinv, p->partials, st, ws);
       if (pd) cudaEventRecord(pd->ev[it][2], ws);
-      launch_pupdate(p, P0, z, st, ws);
+      if (split)
+        launch_pupdate_x(p, x, P0, r, dinv, st, ws);
+      else
+        launch_pupdate(p, P0, z, st, ws);
       if (pd) cudaEventRecord(pd->ev[it][3], ws);
     }
   }
@@ -933,6 +1186,11 @@ int ensure_chunk_graph(femk_plan* p, const double* vals, double* x, const double
   (void)wave_grid(k_update<true>, kThreads, p);
   (void)wave_grid(k_update<false>, kThreads, p);
   (void)wave_grid(k_pupdate<false>, kThreads, p);
+  (void)wave_grid(k_update_r<true>, kThreads, p);
+  (void)wave_grid(k_update_r<false>, kThreads, p);
+  (void)wave_grid(k_pupdate_x<true>, kThreads, p);
+  (void)wave_grid(k_pupdate_x<false>, kThreads, p);
+  if (sell) (void)launch_sell_bulk(p, nullptr, nullptr, nullptr, nullptr, true);
   cudaGraph_t g = nullptr;
   set_capturing(true);
   cudaError_t e = cudaStreamBeginCapture(p->cg_stream, cudaStreamCaptureModeThreadLocal);

@@ -65,6 +65,7 @@ struct CgState {
   double rr_since;  // rr at the last reliable update
   int32_t inner;    // FP32 iterations
   int32_t outer;    // FP64 residual evaluations
+  int32_t xpend;    // split update: 1 while x += alpha p of the current iteration is still to be applied
 };
 
 }  // namespace femk
@@ -111,6 +112,8 @@ struct femk_plan {
   int n_sm = 148;
   // CG launch machinery: plan-owned stream, events, and the captured chunk graph
   int cg_fused = 0, cg_graph = 1, cg_persist = 0;
+  int cg_split = 1;             // split vector kernels (k_update_r + k_pupdate_x) on aligned vectors
+  int bulk_cfg = 0;             // bulk-copy CG-step SpMV: 10 * stages + warps per block, 0 = off
   int coop = 0;                 // device supports cooperative launch
   void* bar = nullptr;          // grid barrier of the persistent solvers
   cudaStream_t cg_stream = nullptr;

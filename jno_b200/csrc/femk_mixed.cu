@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "femk_bulk.cuh"
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
 #include "femk_grid.cuh"
@@ -38,9 +39,9 @@ struct MixedState {
   uint32_t ticket;
 };
 
-template <int NV>
+template <int NV, int THREADS = kThreads>
 __device__ __forceinline__ bool reduce_finish(double (&v)[NV], double* partials, uint32_t* ticket, double (&out)[NV]) {
-  __shared__ double red[NV][kThreads / 32];
+  __shared__ double red[NV][THREADS / 32];
   __shared__ bool last;
 #pragma unroll
   for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
@@ -53,7 +54,7 @@ __device__ __forceinline__ bool reduce_finish(double (&v)[NV], double* partials,
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
       double t = 0.0;
-      for (int w = 0; w < kThreads / 32; ++w) t += red[j][w];
+      for (int w = 0; w < THREADS / 32; ++w) t += red[j][w];
       partials[(int64_t)blockIdx.x * NV + j] = t;
     }
     __threadfence();
@@ -65,11 +66,11 @@ __device__ __forceinline__ bool reduce_finish(double (&v)[NV], double* partials,
   double s[NV];
 #pragma unroll
   for (int j = 0; j < NV; ++j) s[j] = 0.0;
-  for (int b0 = threadIdx.x; b0 < (int)gridDim.x; b0 += 4 * kThreads) {
+  for (int b0 = threadIdx.x; b0 < (int)gridDim.x; b0 += 4 * THREADS) {
     double t[4][NV];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      const int b = b0 + u * kThreads;
+      const int b = b0 + u * THREADS;
 #pragma unroll
       for (int j = 0; j < NV; ++j) t[u][j] = b < (int)gridDim.x ? __ldcg(partials + (int64_t)b * NV + j) : 0.0;
     }
@@ -89,7 +90,7 @@ __device__ __forceinline__ bool reduce_finish(double (&v)[NV], double* partials,
 #pragma unroll
   for (int j = 0; j < NV; ++j) {
     double t = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) t += red[j][w];
+    for (int w = 0; w < THREADS / 32; ++w) t += red[j][w];
     out[j] = t;
   }
   if (threadIdx.x == 0) *ticket = 0u;
@@ -149,6 +150,34 @@ __global__ void __launch_bounds__(kThreads, 8) k_step32_sell(const int64_t* __re
   }
   double v[1] = {(double)acc}, tot[1];
   if (!reduce_finish<1>(v, partials, &st->ticket, tot)) return;
+  if (threadIdx.x) return;
+  finish_alpha(st, tot[0]);
+}
+
+// The same step with the FP32 sliced-ELL stream moved into shared memory by bulk copies
+// (femk_bulk.cuh): WPB warps per block, S slices in flight per warp, widths up to WMAX.
+template <int WMAX, int S, int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_step32_bulk(const int64_t* __restrict__ sptr,
+                                                         const int16_t* __restrict__ cols,
+                                                         const float* __restrict__ vals, int64_t n, int64_t nslices,
+                                                         const float* __restrict__ p, float* __restrict__ q,
+                                                         double* __restrict__ partials, MixedState* st) {
+  extern __shared__ __align__(128) unsigned char bulk_smem[];
+  using R = BulkRing<float, int16_t, WMAX, S>;
+  if (st->done || st->hold) return;
+  const int wib = threadIdx.x >> 5;
+  float acc = 0.f;
+  const bool ok = sell_bulk_rows<float, int16_t, WMAX, S>(
+      bulk_smem + wib * R::kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * WPB + wib,
+      (int64_t)gridDim.x * WPB, GatherX<float>{p},
+      [&](int64_t row, float sv) {
+        q[row] = sv;
+        acc = fmaf(__ldg(p + row), sv, acc);
+      },
+      &st->status, FEMK_TIMEOUT);
+  if (!ok && (threadIdx.x & 31) == 0) st->done = 1;
+  double v[1] = {(double)acc}, tot[1];
+  if (!reduce_finish<1, WPB * 32>(v, partials, &st->ticket, tot)) return;
   if (threadIdx.x) return;
   finish_alpha(st, tot[0]);
 }
@@ -519,7 +548,54 @@ void launch_true_resid(const femk_plan* p, const double* vals, const double* x, 
   });
 }
 
+template <int S, int WPB, int WMAX>
+bool launch_step32_bulk_cfg(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
+                            bool prime) {
+  auto kern = k_step32_bulk<WMAX, S, WPB>;
+  constexpr int kSmem = WPB * BulkRing<float, int16_t, WMAX, S>::kWarpBytes;
+  static int per_sm = -1;  // per instantiation: opt-in shared memory size + occupancy, queried once
+  if (per_sm < 0) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WPB * 32, kSmem) != cudaSuccess) {
+      cudaGetLastError();
+      per_sm = 0;
+    }
+  }
+  if (per_sm <= 0) return false;
+  if (prime) return true;
+  const int grid = p->n_sm * std::min(per_sm, 8);
+  kern<<<::femk::counted_launch() + grid, WPB * 32, kSmem, s>>>(p->sell_ptr, p->sell_c16, p->sell_vals32, p->n,
+                                                                p->n_slices, pv, q, p->partials, st);
+  return true;
+}
+
+// bulk-copy FP32 step in the plan's configuration (same code as the FP64 CG step, bulk_cfg)
+// prime = true only sets the kernel attribute and reads the occupancy (before a graph capture)
+bool launch_step32_bulk(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
+                        bool prime = false) {
+  if (!p->bulk_cfg || !p->sell_vals32 || !p->sell_c16 || p->max_row > 32) return false;
+  if (((uintptr_t)p->sell_vals32 & 15u) || ((uintptr_t)p->sell_c16 & 15u)) return false;
+  const bool narrow = p->max_row <= 16;
+#define FEMK_BULK_CFG(code, S, WPB)                                                          \
+  case code:                                                                                 \
+    return narrow ? launch_step32_bulk_cfg<S, WPB, 16>(p, pv, q, st, s, prime)                      \
+                  : launch_step32_bulk_cfg<S, WPB, 32>(p, pv, q, st, s, prime);
+  switch (p->bulk_cfg) {
+    FEMK_BULK_CFG(24, 2, 4)
+    FEMK_BULK_CFG(28, 2, 8)
+    FEMK_BULK_CFG(34, 3, 4)
+    FEMK_BULK_CFG(38, 3, 8)
+    FEMK_BULK_CFG(44, 4, 4)
+    FEMK_BULK_CFG(42, 4, 2)
+    FEMK_BULK_CFG(62, 6, 2)
+    default:
+      return false;
+  }
+#undef FEMK_BULK_CFG
+}
+
 void launch_step32(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s) {
+  if (launch_step32_bulk(p, pv, q, st, s)) return;
   if (p->sell_vals32) {
     auto go = [&](auto Bc) {
       constexpr int B = decltype(Bc)::value;
@@ -623,6 +699,7 @@ int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double
   (void)wave_grid(k_step32_sell<int32_t, 8>, kThreads, p);
   (void)wave_grid(k_step32_sell<int16_t, 16>, kThreads, p);
   (void)wave_grid(k_step32_sell<int32_t, 16>, kThreads, p);
+  (void)launch_step32_bulk(p, nullptr, nullptr, nullptr, nullptr, true);
   (void)wave_grid(k_update32, kThreads, p);
   (void)wave_grid(k_pupdate32<0>, 256, p);
   (void)wave_grid(k_pupdate32<1>, 256, p);

@@ -625,6 +625,8 @@ extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int3
   // P2 64^3 117 ms without vs 168 ms with, so P2 plans stream without them
   p->l2_mode = std::getenv("FEMK_L2HINT") ? femk::l2_hints() : (order == 1 ? 1 : 0);
   if (const char* e = std::getenv("FEMK_CG_PERSIST")) p->cg_persist = std::atoi(e) != 0;
+  if (const char* e = std::getenv("FEMK_CG_SPLIT")) p->cg_split = std::atoi(e) != 0;
+  if (const char* e = std::getenv("FEMK_BULK")) p->bulk_cfg = std::atoi(e);
   cudaDeviceGetAttribute(&p->coop, cudaDevAttrCooperativeLaunch, p->device);
   p->nvert = nvert;
   p->ntet = ntet;

@@ -3,9 +3,10 @@
 Mirrors jno/_fem.py:3742 (``fem``), :1132 (``class FEM``: ``.operator`` :1207, ``.solve`` :1294,
 ``.dofs`` :2575) and ``FemLinearSystem`` (jno/trace/__init__.py:3584-3690): a form with a P0
 parameter returns a :class:`FemLinearSystem` re-assembled on each ``evaluate({name: value})``; a
-form without one is assembled once into ``(A, b)``. The quadrature degree the reference infers
-(P1 -> 2, P2 -> 4, _fem.py:4551,4573) integrates these forms exactly, as the closed-form element
-kernels do, so ``quad_degree`` is accepted for signature parity and only validated.
+form without one is assembled once into ``(A, b)`` with ``A`` compacted (exact zeros dropped).
+The quadrature degree the reference infers (P1 -> 2, P2 -> 4, _fem.py:4551,4573) integrates
+these forms exactly, as the closed-form element kernels do, so ``quad_degree`` is accepted for
+signature parity and only validated.
 """
 
 import numpy as np
@@ -100,7 +101,10 @@ class FEM:
         if self.form.param is not None:
             return FemLinearSystem(self)
         if self._eager is None:
-            self._eager = self._assemble({})
+            # linear non-parametric route: Dirichlet elimination, then compress_eager drops the exact
+            # zeros (jno/utils/solver/fem_native.py:3371-3379)
+            A, b = self._assemble({})
+            self._eager = (A.compact(), b)
         return self._eager
 
     @property

@@ -129,6 +129,17 @@ class FemPlan:
                                            _lib.ptr(vals), _lib.ptr(b), _lib.stream_handle()))
         return vals, b
 
+    def compact(self, vals):
+        """(indptr i32[n+1], indices i32[m], data f64[m]): the entries of ``vals`` with ``|v| > 0``
+        in CSR order (``compress_eager``, jno/utils/solver/fem_utils.py:4063-4091)."""
+        indptr = torch.empty(self.n + 1, dtype=torch.int32, device=self.device)
+        indices = torch.empty(self.nnz, dtype=torch.int32, device=self.device)
+        data = torch.empty(self.nnz, dtype=torch.float64, device=self.device)
+        m = ctypes.c_int64(-1)
+        _lib.check(self._lib.femk_compact(self._h, _lib.ptr(vals), _lib.ptr(indptr), _lib.ptr(indices), _lib.ptr(data),
+                                          self.nnz, ctypes.byref(m), _lib.stream_handle()))
+        return indptr, indices[: m.value], data[: m.value]
+
     def element_matrices(self):
         khat = torch.empty(self.ntet, self.nd, self.nd, dtype=torch.float64, device=self.device)
         fhat = torch.empty(self.ntet, self.nd, dtype=torch.float64, device=self.device)

@@ -79,14 +79,14 @@ class LinearSolver:
             if not isinstance(op, CsrMatrix) or inv is None:
                 raise ValueError("precision='mixed' needs an assembled CsrMatrix and M=jacobi()")
             mode = _lib.MIXED_RELIABLE if self.refine == "reliable" else _lib.MIXED_RESTART
-            x, inner, outer, rel, st = plan.pcg_mixed(op.data, b, inv, x, self.tol, self.atol, self.maxiter, mode)
+            x, inner, outer, rel, st = plan.pcg_mixed(op.solver_values, b, inv, x, self.tol, self.atol, self.maxiter, mode)
             self.last_info = SolveInfo(inner, rel, st, outer)
         elif isinstance(op, MatrixFreeOperator):
             x, it, rel, st = plan.pcg_matfree(op.param, b, x, inv, op.mode, op.scale, self.tol, self.atol,
                                               self.maxiter)
             self.last_info = SolveInfo(it, rel, st)
         else:
-            x, it, rel, st = plan.pcg(op.data, b, x, inv, self.tol, self.atol, self.maxiter)
+            x, it, rel, st = plan.pcg(op.solver_values, b, x, inv, self.tol, self.atol, self.maxiter)
             self.last_info = SolveInfo(it, rel, st)
         rel = self.last_info.relres
         if not math.isfinite(rel) or rel > 1e-4:

@@ -4,7 +4,9 @@ The pattern is the reference's compress-plan unique set (jno/utils/solver/fem_ut
 values are FP64 with Dirichlet rows/columns stored as explicit zeros and a unit diagonal (the
 parametric route, fem_native.py:3311-3339). ``to_bcoo(appended=True)`` rebuilds the reference's
 exact BCOO layout (compressed triplets with the Dirichlet entries zeroed, then one ``(d, d, 1)``
-triplet per Dirichlet DOF appended, fem_utils.py:3354-3359).
+triplet per Dirichlet DOF appended, fem_utils.py:3354-3359). ``compact()`` is the non-parametric
+route's operator: the same entries with the exact zeros dropped (``compress_eager``,
+fem_utils.py:4063-4091), computed on the device.
 """
 
 import torch
@@ -27,19 +29,28 @@ class CsrMatrix:
     def nnz(self):
         return int(self.data.numel())
 
+    @property
+    def solver_values(self):
+        """Values on the plan's canonical pattern: what the SpMV and CG kernels stream."""
+        return self.data
+
+    def compact(self):
+        """:class:`CompactCsrMatrix` of the entries with ``|v| > 0`` (``compress_eager``)."""
+        return CompactCsrMatrix(self)
+
     def __matmul__(self, x):
-        return self.plan.spmv(self.data, _as_cuda(x, self.data.device))
+        return self.plan.spmv(self.solver_values, _as_cuda(x, self.data.device))
 
     mv = __matmul__
 
     def diag(self):
         """Sum of the stored on-diagonal entries (``matrix_diagonal``, jno/utils/solver/linear.py:88-94)."""
         ex = self.plan.export()
-        return self.data[ex["diag_slot"].long()]
+        return self.solver_values[ex["diag_slot"].long()]
 
     def jacobi_inverse(self):
         if self._inv_diag is None:
-            self._inv_diag = self.plan.jacobi(self.data)
+            self._inv_diag = self.plan.jacobi(self.solver_values)
         return self._inv_diag
 
     def todense(self):
@@ -74,6 +85,39 @@ class CsrMatrix:
         idx = torch.cat([idx, torch.stack([d, d], dim=1)])
         data = torch.cat([data, torch.ones(d.numel(), dtype=data.dtype, device=data.device)])
         return idx, data
+
+
+class CompactCsrMatrix(CsrMatrix):
+    """The operator of the non-parametric route: ``indptr``/``indices``/``data`` hold only the
+    entries with ``|v| > 0`` (rows ascending, columns ascending), as ``compress_eager`` leaves them.
+
+    The solver kernels keep streaming the canonical-pattern values: the dropped entries are exact
+    zeros (or NaN, which the residual guard reports either way), so products and solves equal those
+    of the compact matrix.
+    """
+
+    def __init__(self, full):
+        self.plan = full.plan
+        self.shape = full.shape
+        self.assembly = full.assembly
+        self._full = full.solver_values
+        self.indptr, self.indices, self.data = full.plan.compact(self._full)
+        self._inv_diag = None
+
+    @property
+    def solver_values(self):
+        return self._full
+
+    def compact(self):
+        return self
+
+    def to_bcoo(self, appended=False):
+        """(indices i32[m, 2], data f64[m]); the compact form has no appended diagonal triplets."""
+        rows = torch.repeat_interleave(
+            torch.arange(self.plan.n, device=self.data.device, dtype=torch.int32),
+            (self.indptr[1:] - self.indptr[:-1]).long(),
+        )
+        return torch.stack([rows, self.indices], dim=1), self.data.clone()
 
 
 class MatrixFreeOperator:

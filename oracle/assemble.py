@@ -131,14 +131,22 @@ def assemble(points, cells, order, dirichlet, coef, f=1.0, g=None, plan=None, el
     return System(np.asarray(indptr), np.asarray(indices), data, b, isd, n)
 
 
+def compact_csr(indptr, indices, data):
+    """``compress_eager``'s selection (jno/utils/solver/fem_utils.py:4083-4087) on a CSR in plan
+    order: keep the entries with ``abs(data) > 0`` (exact zeros and NaN go), order unchanged."""
+    indptr = np.asarray(indptr, dtype=np.int64)
+    keep = np.abs(np.asarray(data)) > 0.0
+    rows = np.repeat(np.arange(indptr.size - 1), np.diff(indptr))
+    counts = np.bincount(rows[keep], minlength=indptr.size - 1)
+    new_ptr = np.zeros(indptr.size, dtype=np.int64)
+    np.cumsum(counts, out=new_ptr[1:])
+    return new_ptr.astype(np.int32), np.asarray(indices)[keep].astype(np.int32), np.asarray(data)[keep]
+
+
 def compact(system):
-    """``compress_eager`` pattern: drop exact zeros (value-dependent; non-parametric route only)."""
-    A = system.csr()
-    keep = A.data != 0.0
-    rows = np.repeat(np.arange(system.n), np.diff(A.indptr))[keep]
-    B = sp.csr_matrix((A.data[keep], (rows, A.indices[keep])), shape=A.shape)
-    B.sort_indices()
-    return B
+    """``compress_eager`` operator of an assembled system as a scipy CSR (non-parametric route)."""
+    ip, ind, dat = compact_csr(system.indptr, system.indices, system.data)
+    return sp.csr_matrix((dat, ind, ip), shape=(system.n, system.n))
 
 
 def matrix_diagonal(system):

@@ -291,3 +291,102 @@ def test_profiled_solve_matches_and_times_every_iteration():
     assert it1 == it0 and iters == it1
     assert torch.equal(u0, u1)  # same kernels, same order: bit-identical with or without graph replay
     assert step > 0 and upd > 0 and pup > 0
+
+
+@pytest.mark.parametrize("n,order,jitter", [(3, 1, True), (8, 1, True), (6, 1, False), (3, 2, True), (4, 2, False)])
+def test_compact_export_matches_compress_eager(n, order, jitter):
+    """femk_compact keeps exactly the entries compress_eager keeps (|v| > 0, plan order)."""
+    pf, cf, tets, p1 = om.kuhn_cube(n, order=order, seed=4, amp=0.1 if jitter else 0.0)
+    logk = om.logk_field(len(tets), 1004)
+    plan = _plan(p1, tets, order)
+    x, y, z = pf.T
+    g = 1.0 + x - 2.0 * y + 0.5 * z
+    vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"), g=torch.as_tensor(g, device="cuda"))
+    ip, ind, dat = plan.compact(vals)
+    ex = plan.export()
+    # selection rule, bit-exact, on the same (device-assembled) values
+    ipo, indo, dato = oa.compact_csr(ex["indptr"].cpu().numpy(), ex["indices"].cpu().numpy(), vals.cpu().numpy())
+    assert np.array_equal(ip.cpu().numpy(), ipo)
+    assert np.array_equal(ind.cpu().numpy(), indo)
+    assert np.array_equal(dat.cpu().numpy(), dato)
+    assert ind.numel() < plan.nnz  # the Dirichlet rows/columns always go
+    # against the oracle's own assembly: same kept pattern on jittered meshes, values within 1e-12
+    s, _ = _oracle_system(pf, cf, order, logk, g=g)
+    B = oa.compact(s)
+    if jitter:
+        assert np.array_equal(ip.cpu().numpy(), B.indptr) and np.array_equal(ind.cpu().numpy(), B.indices)
+        assert np.abs(dat.cpu().numpy() - B.data).max() <= VAL_TOL * np.abs(B.data).max()
+    A = B.toarray()
+    D = np.zeros((plan.n, plan.n))
+    rows = np.repeat(np.arange(plan.n), np.diff(ip.cpu().numpy()))
+    D[rows, ind.cpu().numpy()] = dat.cpu().numpy()
+    assert np.abs(D - A).max() <= VAL_TOL * np.abs(A).max()
+
+
+def test_compact_export_drops_nan_and_signed_zero_and_checks_capacity():
+    import ctypes
+
+    from jno_b200 import _lib
+
+    pf, cf, tets, p1 = _mesh(3, 1)
+    plan = _plan(p1, tets, 1)
+    vals, b = plan.assemble(torch.zeros(len(tets), dtype=torch.float64, device="cuda"))
+    ex = plan.export()
+    planted = vals.clone()
+    nz = torch.nonzero(planted != 0).flatten()
+    planted[nz[5]] = float("nan")
+    planted[nz[9]] = -0.0
+    planted[nz[11]] = float("inf")  # |inf| > 0: kept
+    ip, ind, dat = plan.compact(planted)
+    ipo, indo, dato = oa.compact_csr(ex["indptr"].cpu().numpy(), ex["indices"].cpu().numpy(), planted.cpu().numpy())
+    assert np.array_equal(ip.cpu().numpy(), ipo) and np.array_equal(ind.cpu().numpy(), indo)
+    assert np.array_equal(dat.cpu().numpy(), dato)
+    assert ind.numel() == nz.numel() - 2
+    # a capacity below the kept count is refused before any entry is written
+    lib = _lib.load()
+    out_ptr = torch.full((plan.n + 1,), -7, dtype=torch.int32, device="cuda")
+    out_idx = torch.full((8,), -7, dtype=torch.int32, device="cuda")
+    out_val = torch.full((8,), -7.0, dtype=torch.float64, device="cuda")
+    m = ctypes.c_int64(-1)
+    st = lib.femk_compact(plan.handle, _lib.ptr(vals), _lib.ptr(out_ptr), _lib.ptr(out_idx), _lib.ptr(out_val), 8,
+                          ctypes.byref(m), _lib.stream_handle())
+    torch.cuda.synchronize()
+    assert st == _lib.FEMK_EINVAL and b"cap" in lib.femk_last_error_string()
+    assert torch.all(out_idx == -7) and torch.all(out_val == -7.0)
+
+
+def test_jno_surface_non_parametric_route():
+    """A form without a parameter: (A, b) with A compacted, inhomogeneous Dirichlet lifted into b
+    (jno/utils/solver/fem_native.py:3371-3379), solved through fem.solve()."""
+    import jno_b200 as jno
+
+    n = 6
+    d = jno.domain(jno.domain.equi_distant_box(nx=n, ny=n, nz=n), jitter=0.1, seed=0)
+    u, v = d.fem_symbols()
+    xi, yi, zi = d.variable("interior", split=True)
+    xb, yb, zb = d.variable("boundary", split=True)
+    ui, vi = u.bind(x=xi, y=yi, z=zi), v.bind(x=xi, y=yi, z=zi)
+    fem = jno.fem([2.0 * (ui.x * vi.x + ui.y * vi.y + ui.z * vi.z) - 1.0 * vi,
+                   u(xb, yb, zb) - (1.0 + xb + 2.0 * yb - zb)])
+    A, b = fem.operator
+    pf, cf, tets, p1 = _mesh(n, 1)
+    g = 1.0 + pf[:, 0] + 2.0 * pf[:, 1] - pf[:, 2]
+    bnd = om.boundary_nodes(cf, 1)
+    so = oa.assemble(pf, cf, 1, bnd, np.full(len(tets), 2.0), f=1.0, g=g)
+    B = oa.compact(so)
+    assert A.nnz == B.nnz
+    assert np.array_equal(A.indptr.cpu().numpy(), B.indptr) and np.array_equal(A.indices.cpu().numpy(), B.indices)
+    assert np.abs(A.data.cpu().numpy() - B.data).max() <= VAL_TOL * np.abs(B.data).max()
+    assert np.abs(b.cpu().numpy() - so.b).max() <= 1e-11 * np.abs(so.b).max()
+    idx, data = A.to_bcoo()
+    assert idx.shape == (B.nnz, 2)
+    xs = fem.solve()
+    xo = op.pcg(B, so.b, oa.jacobi_inverse(oa.matrix_diagonal(so)), tol=1e-8)[0]
+    assert np.linalg.norm(xs.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+    assert np.abs(xs.cpu().numpy()[bnd] - g[bnd]).max() <= 1e-7 * np.abs(g).max()
+    yv = torch.as_tensor(np.random.default_rng(1).standard_normal(plan_n(fem)), device="cuda")
+    assert np.abs((A @ yv).cpu().numpy() - B @ yv.cpu().numpy()).max() <= 1e-12 * np.abs(B @ yv.cpu().numpy()).max()
+
+
+def plan_n(fem):
+    return fem.plan.n
