@@ -221,6 +221,29 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+# ------------------------------------------------------------------------------------------ replicas
+def replica_field(i, rank):
+    """k field of step i on `rank`: ranks start at different fields (independent problems)."""
+    return (i + rank) % N_FIELDS
+
+
+def max_over_ranks(ms, world, device=None):
+    """The job's time: the slowest rank's (an all-reduce MAX; one rank returns its own)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(ndof, world, ms_step):
+    """DOF/s of the whole job: every rank solves its own ndof-DOF problem per step."""
+    return world * ndof / (ms_step / 1e3)
+
+
 # ------------------------------------------------------------------------------------------ ours
 def roofline_traffic():
     """DRAM bytes per SpMV launch from the committed ncu summary, if one exists."""
@@ -408,7 +431,7 @@ def run_ours(args):
     phase = {"asm": [], "solve": []}
 
     def step(i, record=False):
-        lk = fields[(i + rank) % N_FIELDS]
+        lk = fields[replica_field(i, rank)]
         if record:
             e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
             e0.record()
@@ -447,12 +470,7 @@ def run_ours(args):
             fn(warmup + i)
         end.record()
         barrier()
-        ms = start.elapsed_time(end)
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = t.item()
-        return ms
+        return max_over_ranks(start.elapsed_time(end), world, dev)
 
     # ---- headline: FP64 CSR
     for i in range(args.warmup):
@@ -472,13 +490,9 @@ def run_ours(args):
     barrier()
     launches = lib.femk_kernel_launches() - launches0
     clk = clocks.stop()
-    ms_total = start.elapsed_time(end)
-    if world > 1:
-        t = torch.tensor([ms_total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = t.item()
+    ms_total = max_over_ranks(start.elapsed_time(end), world, dev)
     ms_step = ms_total / args.steps
-    value = world * ndof / (ms_step / 1e3)
+    value = whole_job_value(ndof, world, ms_step)
     iters_mean = float(np.mean(iters_seen))
 
     # phase split (separate short run with events between phases)
@@ -594,6 +608,25 @@ def run_ours(args):
         ms_f = timed(fstep, fsteps, 1) / fsteps
         variants["matrix_free_fp64"] = {"value": world * ndof / (ms_f / 1e3), "unit": "DOF/s", "ms_per_step": ms_f,
                                         "iters": float(np.mean(mf_info["it"]))}
+        # Jacobi-BiCGStab (the reference's steady fem.solve() default) on the same systems
+        bi_info = {}
+
+        def bstep(i):
+            lk = fields[i % N_FIELDS]
+            plan.assemble(lk, vals=vals, b=b)
+            plan.jacobi(vals, out=inv)
+            x.zero_()
+            _, it, rel, st = plan.bicgstab(vals, b, x, inv, tol=1e-8)
+            if st != 0 or rel > 1e-4:
+                raise RuntimeError(f"BiCGStab failed: status {st}, relres {rel}")
+            bi_info.setdefault("it", []).append(it)
+            bi_info.setdefault("rel", []).append(rel)
+
+        bsteps = min(args.steps, 10)
+        ms_b = timed(bstep, bsteps, 2) / bsteps
+        variants["bicgstab_fp64"] = {"value": world * ndof / (ms_b / 1e3), "unit": "DOF/s", "ms_per_step": ms_b,
+                                     "iters": float(np.mean(bi_info["it"])), "max_relres": float(np.max(bi_info["rel"])),
+                                     "note": "2 SpMVs per iteration; stop rule <r, r> <= tol^2 <b, b>"}
         variants["spmv_csr_fp64"] = {"GB/s": csr_bytes / (csr_ms / 1e3) / 1e9, "ms": csr_ms}
         # compress_eager export of the non-parametric route (count + scan + fill, one host read)
         plan.assemble(fields[0], vals=vals, b=b)
@@ -624,7 +657,7 @@ def run_ours(args):
     out_host = torch.empty(ndof, dtype=torch.float64).pin_memory()
 
     def estep(i):
-        lk = host_fields[(i + rank) % N_FIELDS].to(dev, non_blocking=True)
+        lk = host_fields[replica_field(i, rank)].to(dev, non_blocking=True)
         A, bb = system.evaluate({"logk": lk})
         xs = solver(A, bb, M=jno.precond.jacobi())
         out_host.copy_(xs, non_blocking=True)

@@ -177,6 +177,19 @@ int femk_pcg_matfree(const femk_plan* plan, const double* param_dev, int coef_mo
                      double atol, int32_t maxiter, int32_t* iters_out, double* relres_out, void* stream);
 
 /*
+ * Jacobi-preconditioned BiCGStab with jax.scipy.sparse.linalg.bicgstab semantics (jax 0.10.1):
+ * stop when <r, r> <= max(tol^2 <b, b>, atol^2) or after maxiter iterations; a breakdown
+ * (<rhat, r> = 0, alpha = 0 or omega = 0) ends the loop with x as it stands and returns
+ * FEMK_BREAKDOWN. x holds x0 on entry and the solution on return; inv_diag may be NULL (no
+ * preconditioner). *iters_out = iterations run, *relres_out = ||b - A x|| / (||b|| + 1e-30).
+ * Replaces jno.solve.bicgstab (jno/solve.py:209-213) and the steady fem.solve() default
+ * (jno/_fem.py:110-116, Jacobi-BiCGStab).
+ */
+int femk_bicgstab(const femk_plan* plan, const double* vals_dev, const double* b_dev, double* x_dev,
+                  const double* inv_diag_dev, double tol, double atol, int32_t maxiter, int32_t* iters_out,
+                  double* relres_out, void* stream);
+
+/*
  * Allocation-free Jacobi-PCG: the same iteration and result as femk_pcg, for callers that must
  * not allocate device memory during the call -- an XLA FFI handler (device memory is owned by XLA's
  * allocator), a framework whose caching allocator already holds nearly all of HBM, or a real-time

@@ -87,6 +87,7 @@ SIGNATURES = {
     "femk_spmv_matfree": [_P, _P, _I, _D, _P, _P, _P],
     "femk_pcg": [_P, _P, _P, _P, _P, _D, _D, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_D), _P],
     "femk_pcg_noalloc": [_P, _P, _P, _P, _P, _D, _D, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_D), _P],
+    "femk_bicgstab": [_P, _P, _P, _P, _P, _D, _D, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_D), _P],
     "femk_pcg_matfree": [_P, _P, _I, _D, _P, _P, _P, _D, _D, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_D), _P],
     "femk_pcg_mixed": [_P, _P, _P, _P, _P, _D, _D, _I32, _I, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
                        ctypes.POINTER(_D), _P],

@@ -85,8 +85,17 @@ struct BulkRing {
   static_assert(kVal % 128 == 0, "stage alignment");
 };
 
+// Blocks per SM that the ring's shared memory allows (at most 16): the kernels ask the compiler for
+// registers that let this many blocks be resident.
+template <typename V, typename IDX, int WMAX, int S, int WPB>
+constexpr int bulk_min_blocks() {
+  constexpr int per_block = WPB * BulkRing<V, IDX, WMAX, S>::kWarpBytes + 1024;
+  constexpr int b = (227 * 1024) / per_block;
+  return b < 1 ? 1 : (b > 16 ? 16 : b);
+}
+
 // Every slice of this warp (global warp g takes slices g, g + NW, ...): for each row,
-// epi(row, row_sum). Returns false if a wait timed out (and sets *err to errval).
+// epi(row, row_sum, x[row]). Returns false if a wait timed out (and sets *err to errval).
 template <typename V, typename IDX, int WMAX, int S, typename G, typename Epi>
 __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64_t* __restrict__ sptr,
                                                const IDX* __restrict__ cols, const V* __restrict__ vals, int64_t n,
@@ -104,10 +113,9 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
     mbar_fence_init();
   }
   __syncwarp();
-  // lane 0: stream slice `sl` into stage `s`
-  auto issue = [&](int64_t sl, int s) {
-    const int64_t b0 = __ldg(sptr + sl);
-    const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
+  // lane 0: stream slice entries [b0, b1) into stage `s`
+  auto issue = [&](int64_t b0, int64_t b1, int s) {
+    const int32_t w = (int32_t)((b1 - b0) >> 5);
     wid[s] = w;
     const uint32_t vb = (uint32_t)(32 * w * (int)sizeof(V));
     const uint32_t cb = (uint32_t)(32 * w * (int)sizeof(IDX));
@@ -124,7 +132,7 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
     for (int s = 0; s < S; ++s) {
       const int64_t sl = g + (int64_t)s * NW;
       if (sl >= nslices) break;
-      issue(sl, s);
+      issue(__ldg(sptr + sl), __ldg(sptr + sl + 1), s);
       ++issued;
     }
   __syncwarp();
@@ -133,6 +141,14 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
   for (int64_t sl = g; sl < nslices; sl += NW, ++i) {
     const int s = (int)(i % S);
     const uint32_t parity = (uint32_t)((i / S) & 1);
+    // lane 0 reads the offsets of the slice that refills this stage now, so that load overlaps
+    // the gathers below instead of delaying the refill
+    const int64_t nsl = sl + (int64_t)S * NW;
+    int64_t nb0 = 0, nb1 = 0;
+    if (lane == 0 && nsl < nslices) {
+      nb0 = __ldg(sptr + nsl);
+      nb1 = __ldg(sptr + nsl + 1);
+    }
     // warp-uniform outcome: a lane that timed out takes the whole warp out of the loop
     if (!__all_sync(0xffffffffu, mbar_wait(bar + s, parity))) {
       ok = false;
@@ -144,11 +160,13 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
     const int64_t row = sl * 32 + lane;
     const bool live = row < n;  // rows past n in the last slice gather nothing
     V xg[WMAX];
+    V xrow = V(0);  // x[row], from the diagonal entry's gather (every row stores its diagonal)
 #pragma unroll
     for (int k = 0; k < WMAX; ++k) {
       if (k < w && live) {
         const IDX c = sc[k * 32 + lane];
         xg[k] = gx(sizeof(IDX) == 2 ? (int64_t)row + (int64_t)c : (int64_t)c);
+        if (sizeof(IDX) == 2 ? c == 0 : (int64_t)c == row) xrow = xg[k];
       }
     }
     V acc = V(0);
@@ -156,15 +174,12 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
     for (int k = 0; k < WMAX; ++k)
       if (k < w && live) acc += sv[k * 32 + lane] * xg[k];
     __syncwarp();  // every lane is done with stage s before it is refilled
-    if (lane == 0) {
-      const int64_t nsl = g + (i + S) * NW;
-      if (nsl < nslices) {
-        issue(nsl, s);
-        ++issued;
-      }
+    if (lane == 0 && nsl < nslices) {
+      issue(nb0, nb1, s);
+      ++issued;
     }
     __syncwarp();
-    if (live) epi(row, acc);
+    if (live) epi(row, acc, xrow);
   }
   if (!ok) {
     if (lane == 0) {

@@ -18,6 +18,7 @@
 #include <string>
 
 #include "femk_bulk.cuh"
+#include "femk_reduce.cuh"
 #include "femk_element.cuh"
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
@@ -29,77 +30,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kChunk = 16;  // iterations enqueued between looks at the done flag
-
-// ---------------------------------------------------------------------------------------------
-// reductions: per-block partials + last-block finish
-// ---------------------------------------------------------------------------------------------
-template <int NV, int THREADS = kThreads>
-__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* partials) {
-  __shared__ double red[NV][THREADS / 32];
-#pragma unroll
-  for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
-  if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-    for (int j = 0; j < NV; ++j) red[j][threadIdx.x >> 5] = v[j];
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int j = 0; j < NV; ++j) {
-      double t = 0.0;
-      for (int w = 0; w < THREADS / 32; ++w) t += red[j][w];
-      partials[(int64_t)blockIdx.x * NV + j] = t;
-    }
-  }
-}
-
-// Returns true in every thread of the last block to finish; `out` then holds the grid totals.
-template <int NV, int THREADS = kThreads>
-__device__ __forceinline__ bool grid_finish(double* partials, uint32_t* ticket, double (&out)[NV]) {
-  __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const uint32_t t = atomicAdd(ticket, 1u);
-    last = (t == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!last) return false;
-  __threadfence();
-  double v[NV];
-#pragma unroll
-  for (int j = 0; j < NV; ++j) v[j] = 0.0;
-  // the partials of up to 4*THREADS blocks are loaded before any is added (one round trip)
-  for (int b0 = threadIdx.x; b0 < (int)gridDim.x; b0 += 4 * THREADS) {
-    double t[4][NV];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int b = b0 + u * THREADS;
-#pragma unroll
-      for (int j = 0; j < NV; ++j) t[u][j] = b < (int)gridDim.x ? __ldcg(partials + (int64_t)b * NV + j) : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int j = 0; j < NV; ++j) v[j] += t[u][j];
-  }
-  __shared__ double red[NV][THREADS / 32];
-#pragma unroll
-  for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
-  if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-    for (int j = 0; j < NV; ++j) red[j][threadIdx.x >> 5] = v[j];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int j = 0; j < NV; ++j) {
-    double t = 0.0;
-    for (int w = 0; w < THREADS / 32; ++w) t += red[j][w];
-    out[j] = t;
-  }
-  if (threadIdx.x == 0) *ticket = 0u;
-  return true;
-}
 
 enum SpmvMode { kPlain = 0, kCgStep = 1, kInit = 2, kResid = 3 };
 
@@ -284,13 +214,15 @@ __global__ void __launch_bounds__(kThreads) k_sell(const int64_t* __restrict__ s
 // The same SpMV (kPlain, kCgStep) with the sliced-ELL stream moved into shared memory by bulk
 // copies (femk_bulk.cuh): WPB warps per block, S slices in flight per warp, widths up to WMAX.
 template <int MODE, typename IDX, int WMAX, int S, int WPB>
-__global__ void __launch_bounds__(WPB * 32) k_sell_bulk(const int64_t* __restrict__ sptr,
+__global__ void __launch_bounds__(WPB * 32, (bulk_min_blocks<double, IDX, WMAX, S, WPB>())) k_sell_bulk(const int64_t* __restrict__ sptr,
                                                        const IDX* __restrict__ scols,
                                                        const double* __restrict__ svals, int64_t n, int64_t nslices,
                                                        const double* __restrict__ x, double* __restrict__ y,
                                                        double* __restrict__ partials, CgState* st, int* err) {
   extern __shared__ __align__(128) unsigned char bulk_smem[];
   using R = BulkRing<double, IDX, WMAX, S>;
+  pdl_wait();
+  pdl_trigger();
   if (MODE == kCgStep) {
     if (blockIdx.x == 0 && threadIdx.x == 0) st->xpend = 0;  // the last x update is applied
     if (st->done) return;
@@ -302,9 +234,9 @@ __global__ void __launch_bounds__(WPB * 32) k_sell_bulk(const int64_t* __restric
   int* errp = MODE == kCgStep ? &st->status : err;
   const bool ok = sell_bulk_rows<double, IDX, WMAX, S>(
       bulk_smem + wib * R::kWarpBytes, sptr, scols, svals, n, nslices, g, NW, GatherXL<double>{x, l2_evict_last()},
-      [&](int64_t row, double sv) {
+      [&](int64_t row, double sv, double xrow) {
         y[row] = sv;
-        if (MODE == kCgStep) acc[0] += __ldg(x + row) * sv;
+        if (MODE == kCgStep) acc[0] += xrow * sv;
       },
       errp, FEMK_TIMEOUT);
   if (MODE == kPlain) return;
@@ -569,6 +501,8 @@ template <bool H>
 __global__ void __launch_bounds__(kThreads) k_update_r(int64_t n, double* __restrict__ r, const double* __restrict__ q,
                                                       const double* __restrict__ dinv, double* __restrict__ partials,
                                                       CgState* st) {
+  pdl_wait();
+  pdl_trigger();
   if (st->done) return;
   const double alpha = st->alpha;
   double acc[2] = {0.0, 0.0};
@@ -638,6 +572,8 @@ template <bool H>
 __global__ void __launch_bounds__(kThreads) k_pupdate_x(int64_t n, double* __restrict__ x, double* __restrict__ p,
                                                        const double* __restrict__ r, const double* __restrict__ dinv,
                                                        const CgState* st) {
+  pdl_wait();
+  pdl_trigger();
   if (!st->xpend) return;
   const bool dir = !st->done;
   const double alpha = st->alpha, beta = st->beta;
@@ -917,22 +853,15 @@ bool split_ok(const femk_plan* p, const double* x, const double* dinv) {
 
 void launch_update_r(const femk_plan* p, double* r, const double* q, const double* dinv, CgState* st,
                      cudaStream_t s) {
-  if (p->l2_mode != 0)
-    k_update_r<true><<<::femk::counted_launch() + wave_grid(k_update_r<true>, kThreads, p), kThreads, 0, s>>>(
-        p->n, r, q, dinv, p->partials, st);
-  else
-    k_update_r<false><<<::femk::counted_launch() + wave_grid(k_update_r<false>, kThreads, p), kThreads, 0, s>>>(
-        p->n, r, q, dinv, p->partials, st);
+  auto kern = p->l2_mode != 0 ? k_update_r<true> : k_update_r<false>;
+  (void)launch_ex(p->pdl != 0, kern, wave_grid(kern, kThreads, p), kThreads, 0, s, p->n, r, q, dinv, p->partials,
+                  st);
 }
 
 void launch_pupdate_x(const femk_plan* p, double* x, double* pv, const double* r, const double* dinv,
                       const CgState* st, cudaStream_t s) {
-  if (p->l2_mode != 0)
-    k_pupdate_x<true><<<::femk::counted_launch() + wave_grid(k_pupdate_x<true>, kThreads, p), kThreads, 0, s>>>(
-        p->n, x, pv, r, dinv, st);
-  else
-    k_pupdate_x<false><<<::femk::counted_launch() + wave_grid(k_pupdate_x<false>, kThreads, p), kThreads, 0, s>>>(
-        p->n, x, pv, r, dinv, st);
+  auto kern = p->l2_mode != 0 ? k_pupdate_x<true> : k_pupdate_x<false>;
+  (void)launch_ex(p->pdl != 0, kern, wave_grid(kern, kThreads, p), kThreads, 0, s, p->n, x, pv, r, dinv, st);
 }
 
 template <int MODE>
@@ -977,9 +906,10 @@ bool launch_sell_bulk_cfg(const femk_plan* p, const double* x, double* y, CgStat
   }
   if (per_sm <= 0) return false;
   if (prime) return true;
-  const int grid = p->n_sm * std::min(per_sm, 8);
-  kern<<<::femk::counted_launch() + grid, WPB * 32, kSmem, s>>>(p->sell_ptr, p->sell_c16, p->sell_vals, p->n,
-                                                                p->n_slices, x, y, p->partials, st, nullptr);
+  const int grid = p->n_sm * std::min(per_sm, 16);
+  (void)launch_ex(p->pdl != 0, kern, grid, WPB * 32, kSmem, s, (const int64_t*)p->sell_ptr,
+                  (const int16_t*)p->sell_c16, (const double*)p->sell_vals, p->n, p->n_slices, x, y, p->partials, st,
+                  (int*)nullptr);
   return true;
 }
 
@@ -994,6 +924,9 @@ bool launch_sell_bulk(const femk_plan* p, const double* x, double* y, CgState* s
     return narrow ? launch_sell_bulk_cfg<S, WPB, 16>(p, x, y, st, s, prime)                        \
                   : launch_sell_bulk_cfg<S, WPB, 32>(p, x, y, st, s, prime);
   switch (p->bulk_cfg) {
+    FEMK_BULK_CFG(12, 1, 2)
+    FEMK_BULK_CFG(14, 1, 4)
+    FEMK_BULK_CFG(22, 2, 2)
     FEMK_BULK_CFG(24, 2, 4)
     FEMK_BULK_CFG(28, 2, 8)
     FEMK_BULK_CFG(34, 3, 4)

@@ -113,7 +113,9 @@ struct femk_plan {
   // CG launch machinery: plan-owned stream, events, and the captured chunk graph
   int cg_fused = 0, cg_graph = 1, cg_persist = 0;
   int cg_split = 1;             // split vector kernels (k_update_r + k_pupdate_x) on aligned vectors
-  int bulk_cfg = 0;             // bulk-copy CG-step SpMV: 10 * stages + warps per block, 0 = off
+  int bulk_cfg = 0;             // bulk-copy FP64 CG-step SpMV: 10 * stages + warps per block, 0 = off
+  int bulk32_cfg = 0;           // the same for the FP32 step of the mixed solver
+  int pdl = 0;                  // programmatic dependent launch inside the CG / mixed chunks
   int coop = 0;                 // device supports cooperative launch
   void* bar = nullptr;          // grid barrier of the persistent solvers
   cudaStream_t cg_stream = nullptr;
@@ -137,6 +139,14 @@ struct femk_plan {
   cudaEvent_t batch_ev = nullptr;
   int batch_graph_ok = 1;
   void* prof = nullptr;         // per-kernel CG timing (femk_set_profiling)
+  // BiCGStab workspace (8 vectors), state, stream, events and captured chunk graph
+  void* bicg_ws = nullptr;
+  void* bicg_state = nullptr;
+  void* bicg_host = nullptr;
+  cudaStream_t bicg_stream = nullptr;
+  cudaEvent_t bicg_ev[3] = {nullptr, nullptr, nullptr};
+  cudaGraphExec_t bicg_exec = nullptr;
+  const void* bicg_key[2] = {nullptr, nullptr};
   int batch_graph_used = 0;
 };
 
@@ -165,6 +175,31 @@ template <typename K>
 inline int wave_grid(K kernel, int threads, const femk_plan* p) {
   const int b = resident_blocks((const void*)kernel, threads);
   return p->n_sm * (b < 8 ? b : 8);
+}
+
+// Programmatic dependent launch: a kernel launched with launch_ex(pdl = true) may start while its
+// predecessor on the stream is still running; it must call pdl_wait() before touching anything the
+// predecessor writes (a no-op for a kernel launched without the attribute). pdl_trigger() lets the
+// next PDL-launched kernel begin launching.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// counted launch through cudaLaunchKernelEx, with the programmatic-serialization attribute when pdl
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_ex(bool pdl, void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t s,
+                             Args... args) {
+  counted_launch();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

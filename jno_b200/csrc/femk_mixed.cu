@@ -37,6 +37,7 @@ struct MixedState {
   int32_t hold;         // iterations return at entry until the chunk-end update
   int32_t outer, restart;
   uint32_t ticket;
+  int32_t epend;  // split update: 1 while e += alpha p of the current iteration is still to be applied
 };
 
 template <int NV, int THREADS = kThreads>
@@ -133,6 +134,7 @@ __global__ void __launch_bounds__(kThreads, 8) k_step32_sell(const int64_t* __re
                                                          const float* __restrict__ vals, int64_t n, int64_t nslices,
                                                          const float* __restrict__ p, float* __restrict__ q,
                                                          double* __restrict__ partials, MixedState* st) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->epend = 0;  // the last e update is applied
   if (st->done || st->hold) return;
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
@@ -157,22 +159,25 @@ __global__ void __launch_bounds__(kThreads, 8) k_step32_sell(const int64_t* __re
 // The same step with the FP32 sliced-ELL stream moved into shared memory by bulk copies
 // (femk_bulk.cuh): WPB warps per block, S slices in flight per warp, widths up to WMAX.
 template <int WMAX, int S, int WPB>
-__global__ void __launch_bounds__(WPB * 32) k_step32_bulk(const int64_t* __restrict__ sptr,
+__global__ void __launch_bounds__(WPB * 32, (bulk_min_blocks<float, int16_t, WMAX, S, WPB>())) k_step32_bulk(const int64_t* __restrict__ sptr,
                                                          const int16_t* __restrict__ cols,
                                                          const float* __restrict__ vals, int64_t n, int64_t nslices,
                                                          const float* __restrict__ p, float* __restrict__ q,
                                                          double* __restrict__ partials, MixedState* st) {
   extern __shared__ __align__(128) unsigned char bulk_smem[];
   using R = BulkRing<float, int16_t, WMAX, S>;
+  pdl_wait();
+  pdl_trigger();
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->epend = 0;  // the last e update is applied
   if (st->done || st->hold) return;
   const int wib = threadIdx.x >> 5;
   float acc = 0.f;
   const bool ok = sell_bulk_rows<float, int16_t, WMAX, S>(
       bulk_smem + wib * R::kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * WPB + wib,
       (int64_t)gridDim.x * WPB, GatherX<float>{p},
-      [&](int64_t row, float sv) {
+      [&](int64_t row, float sv, float prow) {
         q[row] = sv;
-        acc = fmaf(__ldg(p + row), sv, acc);
+        acc = fmaf(prow, sv, acc);
       },
       &st->status, FEMK_TIMEOUT);
   if (!ok && (threadIdx.x & 31) == 0) st->done = 1;
@@ -187,6 +192,7 @@ template <int L, int U, typename IDX>
 __global__ void __launch_bounds__(kThreads) k_step32(const int32_t* __restrict__ indptr, const IDX* __restrict__ cols,
                                                     const float* __restrict__ vals, int64_t n, const float* __restrict__ p,
                                                     float* __restrict__ q, double* __restrict__ partials, MixedState* st) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->epend = 0;  // the last e update is applied
   if (st->done || st->hold) return;
   const int lane = threadIdx.x & 31, sub = lane % L;
   const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
@@ -280,6 +286,105 @@ __global__ void __launch_bounds__(kThreads) k_update32(int64_t n, float* __restr
   }
 }
 
+// Split form of k_update32 + k_pupdate32<0> (same floating-point operations, z not stored):
+//   k_update32_r : r -= alpha q; <r, D^-1 r>, <r, r>; update request or beta   (reads r, q, D^-1)
+//   k_pupdate32_x: e += alpha p; p = D^-1 r + beta p (p only while not held)   (reads e, p, r, D^-1)
+// The iteration that requests a reliable update still owes its e update: k_update32_r raises
+// st->epend and the next step kernel clears it.
+__global__ void __launch_bounds__(kThreads) k_update32_r(int64_t n, float* __restrict__ r, const float* __restrict__ q,
+                                                        const float* __restrict__ dinv, double* __restrict__ partials,
+                                                        MixedState* st) {
+  pdl_wait();
+  pdl_trigger();
+  if (st->done || st->hold) return;
+  const float alpha = (float)st->alpha;
+  float a0 = 0.f, a1 = 0.f;
+  const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  const int64_t nt = (int64_t)gridDim.x * kThreads;
+  const int64_t n4 = n >> 2;
+  float4* r4 = reinterpret_cast<float4*>(r);
+  const float4* q4 = reinterpret_cast<const float4*>(q);
+  const float4* d4 = reinterpret_cast<const float4*>(dinv);
+  for (int64_t i = tid; i < n4; i += nt) {
+    const float4 qi = q4[i], di = d4[i], ri0 = r4[i];
+    float4 ri, zi;
+    ri.x = fmaf(-alpha, qi.x, ri0.x);
+    ri.y = fmaf(-alpha, qi.y, ri0.y);
+    ri.z = fmaf(-alpha, qi.z, ri0.z);
+    ri.w = fmaf(-alpha, qi.w, ri0.w);
+    zi.x = di.x * ri.x;
+    zi.y = di.y * ri.y;
+    zi.z = di.z * ri.z;
+    zi.w = di.w * ri.w;
+    r4[i] = ri;
+    a0 = fmaf(ri.x, zi.x, fmaf(ri.y, zi.y, fmaf(ri.z, zi.z, fmaf(ri.w, zi.w, a0))));
+    a1 = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, fmaf(ri.z, ri.z, fmaf(ri.w, ri.w, a1))));
+  }
+  for (int64_t i = 4 * n4 + tid; i < n; i += nt) {
+    const float ri = fmaf(-alpha, q[i], r[i]);
+    const float zi = dinv[i] * ri;
+    r[i] = ri;
+    a0 = fmaf(ri, zi, a0);
+    a1 = fmaf(ri, ri, a1);
+  }
+  double v[2] = {(double)a0, (double)a1}, tot[2];
+  if (!reduce_finish<2>(v, partials, &st->ticket, tot)) return;
+  if (threadIdx.x) return;
+  st->iter += 1;
+  st->rr = tot[1];
+  st->epend = 1;
+  if (!isfinite(tot[0]) || !isfinite(tot[1])) {
+    st->status = FEMK_NONFINITE;
+    st->done = 1;
+    return;
+  }
+  const bool conv = !(tot[1] > st->atol2);
+  const bool drop = tot[1] < st->delta2 * st->rr_since;
+  if (conv || drop || st->iter >= st->maxiter) {
+    st->need_update = 1;
+    st->hold = 1;
+  } else {
+    st->beta = tot[0] / st->gamma;
+    st->gamma = tot[0];
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_pupdate32_x(int64_t n, float* __restrict__ e, float* __restrict__ p,
+                                                         const float* __restrict__ r, const float* __restrict__ dinv,
+                                                         const MixedState* st) {
+  pdl_wait();
+  pdl_trigger();
+  if (st->done || !st->epend) return;
+  const bool dir = !st->hold;
+  const float alpha = (float)st->alpha, beta = (float)st->beta;
+  const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  const int64_t nt = (int64_t)gridDim.x * kThreads;
+  const int64_t n4 = n >> 2;
+  float4* e4 = reinterpret_cast<float4*>(e);
+  float4* p4 = reinterpret_cast<float4*>(p);
+  const float4* r4 = reinterpret_cast<const float4*>(r);
+  const float4* d4 = reinterpret_cast<const float4*>(dinv);
+  for (int64_t i = tid; i < n4; i += nt) {
+    const float4 pi = p4[i];
+    float4 ei = e4[i];
+    ei.x = fmaf(alpha, pi.x, ei.x);
+    ei.y = fmaf(alpha, pi.y, ei.y);
+    ei.z = fmaf(alpha, pi.z, ei.z);
+    ei.w = fmaf(alpha, pi.w, ei.w);
+    e4[i] = ei;
+    if (dir) {
+      const float4 ri = r4[i], di = d4[i];
+      p4[i] = make_float4(fmaf(beta, pi.x, di.x * ri.x), fmaf(beta, pi.y, di.y * ri.y),
+                          fmaf(beta, pi.z, di.z * ri.z), fmaf(beta, pi.w, di.w * ri.w));
+    }
+  }
+  for (int64_t i = 4 * n4 + tid; i < n; i += nt) {
+    const float pi = p[i];
+    e[i] = fmaf(alpha, pi, e[i]);
+    if (dir) p[i] = fmaf(beta, pi, dinv[i] * r[i]);
+  }
+}
+
 // x += e; e = 0 (only at a requested update)
 __global__ void k_fold(int64_t n, double* __restrict__ x, float* __restrict__ e, const MixedState* st) {
   if (st->done || st->need_update != 1) return;
@@ -338,6 +443,7 @@ __global__ void __launch_bounds__(kThreads) k_true_resid(const int32_t* __restri
     st->iter = 0;
     st->need_update = 0;
     st->hold = 0;
+    st->epend = 0;
     st->status = isfinite(tot[0]) && isfinite(tot[1]) ? FEMK_OK : FEMK_NONFINITE;
     st->done = (!(tot[1] > st->atol2) || st->maxiter <= 0 || st->status != FEMK_OK) ? 1 : 0;
     return;
@@ -563,24 +669,28 @@ bool launch_step32_bulk_cfg(const femk_plan* p, const float* pv, float* q, Mixed
   }
   if (per_sm <= 0) return false;
   if (prime) return true;
-  const int grid = p->n_sm * std::min(per_sm, 8);
-  kern<<<::femk::counted_launch() + grid, WPB * 32, kSmem, s>>>(p->sell_ptr, p->sell_c16, p->sell_vals32, p->n,
-                                                                p->n_slices, pv, q, p->partials, st);
+  const int grid = p->n_sm * std::min(per_sm, 16);
+  (void)launch_ex(p->pdl != 0, kern, grid, WPB * 32, kSmem, s, (const int64_t*)p->sell_ptr,
+                  (const int16_t*)p->sell_c16, (const float*)p->sell_vals32, p->n, p->n_slices, pv, q, p->partials,
+                  st);
   return true;
 }
 
-// bulk-copy FP32 step in the plan's configuration (same code as the FP64 CG step, bulk_cfg)
+// bulk-copy FP32 step in the plan's configuration (bulk32_cfg: 10 * stages + warps per block)
 // prime = true only sets the kernel attribute and reads the occupancy (before a graph capture)
 bool launch_step32_bulk(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
                         bool prime = false) {
-  if (!p->bulk_cfg || !p->sell_vals32 || !p->sell_c16 || p->max_row > 32) return false;
+  if (!p->bulk32_cfg || !p->sell_vals32 || !p->sell_c16 || p->max_row > 32) return false;
   if (((uintptr_t)p->sell_vals32 & 15u) || ((uintptr_t)p->sell_c16 & 15u)) return false;
   const bool narrow = p->max_row <= 16;
 #define FEMK_BULK_CFG(code, S, WPB)                                                          \
   case code:                                                                                 \
     return narrow ? launch_step32_bulk_cfg<S, WPB, 16>(p, pv, q, st, s, prime)                      \
                   : launch_step32_bulk_cfg<S, WPB, 32>(p, pv, q, st, s, prime);
-  switch (p->bulk_cfg) {
+  switch (p->bulk32_cfg) {
+    FEMK_BULK_CFG(12, 1, 2)
+    FEMK_BULK_CFG(14, 1, 4)
+    FEMK_BULK_CFG(22, 2, 2)
     FEMK_BULK_CFG(24, 2, 4)
     FEMK_BULK_CFG(28, 2, 8)
     FEMK_BULK_CFG(34, 3, 4)
@@ -648,9 +758,17 @@ int enqueue_mixed_chunk(const femk_plan* p, const double* vals, const double* b,
   const int64_t n = p->n;
   for (int it = 0; it < kChunk; ++it) {
     launch_step32(p, m.pv, m.q, m.st, s);
-    k_update32<<<::femk::counted_launch() + wave_grid(k_update32, kThreads, p), kThreads, 0, s>>>(
-        n, m.e, m.r, m.z, m.pv, m.q, m.d32, p->partials, m.st);
-    k_pupdate32<0><<<::femk::counted_launch() + wave_grid(k_pupdate32<0>, 256, p), 256, 0, s>>>(n, m.pv, m.z, m.st);
+    if (p->cg_split) {
+      (void)launch_ex(p->pdl != 0, k_update32_r, wave_grid(k_update32_r, kThreads, p), kThreads, 0, s, n, m.r,
+                      (const float*)m.q, (const float*)m.d32, p->partials, m.st);
+      (void)launch_ex(p->pdl != 0, k_pupdate32_x, wave_grid(k_pupdate32_x, kThreads, p), kThreads, 0, s, n, m.e,
+                      m.pv, (const float*)m.r, (const float*)m.d32, (const MixedState*)m.st);
+    } else {
+      k_update32<<<::femk::counted_launch() + wave_grid(k_update32, kThreads, p), kThreads, 0, s>>>(
+          n, m.e, m.r, m.z, m.pv, m.q, m.d32, p->partials, m.st);
+      k_pupdate32<0><<<::femk::counted_launch() + wave_grid(k_pupdate32<0>, 256, p), 256, 0, s>>>(n, m.pv, m.z,
+                                                                                                   m.st);
+    }
   }
   k_fold<<<::femk::counted_launch() + wave_grid(k_fold, 256, p), 256, 0, s>>>(n, x, m.e, m.st);
   launch_true_resid<false>(p, vals, x, b, m.d32, m.r, m.z, nullptr, m.st, 0.0, 0.0, s);
@@ -701,6 +819,8 @@ int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double
   (void)wave_grid(k_step32_sell<int32_t, 16>, kThreads, p);
   (void)launch_step32_bulk(p, nullptr, nullptr, nullptr, nullptr, true);
   (void)wave_grid(k_update32, kThreads, p);
+  (void)wave_grid(k_update32_r, kThreads, p);
+  (void)wave_grid(k_pupdate32_x, kThreads, p);
   (void)wave_grid(k_pupdate32<0>, 256, p);
   (void)wave_grid(k_pupdate32<1>, 256, p);
   (void)wave_grid(k_fold, 256, p);

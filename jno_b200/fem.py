@@ -15,7 +15,7 @@ import torch
 from . import _lib
 from .plan import FemPlan
 from .precond import jacobi
-from .solve import cg
+from .solve import bicgstab, cg
 from .sparse import CsrMatrix, MatrixFreeOperator
 from .trace import classify_dirichlet, classify_volume, evaluate_on
 
@@ -51,8 +51,8 @@ class FemLinearSystem:
         return self.evaluate({self._fem.form.param: 0.0})[1]
 
 
-def _solve(A, b, linear, precond, x0):
-    solver = cg() if linear is None else linear
+def _solve(A, b, linear, precond, x0, default=cg):
+    solver = default() if linear is None else linear
     M = jacobi() if precond is None else precond
     return solver(A, b, M=M, x0=x0)
 
@@ -125,7 +125,8 @@ class FEM:
         if self.form.param is not None:
             return self.operator.solve(args, linear, precond, x0)
         A, b = self.operator
-        return _solve(A, b, linear, precond, x0)
+        # steady linear default of the reference: Jacobi-preconditioned BiCGStab (jno/_fem.py:110-116)
+        return _solve(A, b, linear, precond, x0, default=bicgstab)
 
 
 def fem(terms, quad_degree=None, element_type=None, chunk=None, dirichlet_mask=None):

@@ -214,6 +214,18 @@ class FemPlan:
         _lib.check(st, allow=(_lib.FEMK_NOT_CONVERGED,))
         return x, it.value, rr.value, st
 
+    def bicgstab(self, vals, b, x=None, inv_diag=None, tol=1e-8, atol=0.0, maxiter=20_000):
+        """Jacobi-BiCGStab (jax bicgstab semantics). Returns (x, iterations, relres, status);
+        a breakdown is reported as FEMK_BREAKDOWN with x as the iteration left it."""
+        x = torch.zeros(self.n, dtype=torch.float64, device=self.device) if x is None else x
+        it = ctypes.c_int32(0)
+        rr = ctypes.c_double(float("nan"))
+        st = self._lib.femk_bicgstab(self._h, _lib.ptr(vals), _lib.ptr(b), _lib.ptr(x), _lib.ptr(inv_diag), float(tol),
+                                     float(atol), int(maxiter), ctypes.byref(it), ctypes.byref(rr),
+                                     _lib.stream_handle())
+        _lib.check(st, allow=(_lib.FEMK_NOT_CONVERGED, _lib.FEMK_BREAKDOWN))
+        return x, it.value, rr.value, st
+
     def pcg_mixed(self, vals, b, inv_diag, x=None, tol=1e-8, atol=0.0, maxiter=20_000, mode=_lib.MIXED_RELIABLE):
         """FP32-inner / FP64-refined PCG. Returns (x, inner iterations, outer updates, relres, status)."""
         x = torch.zeros(self.n, dtype=torch.float64, device=self.device) if x is None else x

@@ -7,6 +7,8 @@ preconditioner (<r, z> without one) or at maxiter. After the solve the eager res
 ``_maybe_residual_check`` (solver_api.py:224-240) raises ``RuntimeError`` when
 ``||b - A x|| / (||b|| + 1e-30) > 1e-4``.
 
+``bicgstab(tol, atol, maxiter)`` is ``jax.scipy.sparse.linalg.bicgstab`` on the same operator.
+
 Extensions with no reference counterpart: ``precision="mixed"`` (FP32 inner CG with FP64 reliable
 updates, ``refine="reliable"`` or classic restarted refinement ``refine="restart"``) and matrix-free
 operators (:class:`~jno_b200.sparse.MatrixFreeOperator`).
@@ -81,6 +83,11 @@ class LinearSolver:
             mode = _lib.MIXED_RELIABLE if self.refine == "reliable" else _lib.MIXED_RESTART
             x, inner, outer, rel, st = plan.pcg_mixed(op.solver_values, b, inv, x, self.tol, self.atol, self.maxiter, mode)
             self.last_info = SolveInfo(inner, rel, st, outer)
+        elif self.name == "bicgstab":
+            if not isinstance(op, CsrMatrix):
+                raise TypeError("the B200 BiCGStab takes an assembled CsrMatrix")
+            x, it, rel, st = plan.bicgstab(op.solver_values, b, x, inv, self.tol, self.atol, self.maxiter)
+            self.last_info = SolveInfo(it, rel, st)
         elif isinstance(op, MatrixFreeOperator):
             x, it, rel, st = plan.pcg_matfree(op.param, b, x, inv, op.mode, op.scale, self.tol, self.atol,
                                               self.maxiter)
@@ -100,3 +107,10 @@ class LinearSolver:
 def cg(*, tol=1e-8, atol=0.0, maxiter=20_000, precision="fp64", refine="reliable"):
     """Jacobi-preconditionable CG on the B200 kernels (``jax.scipy.sparse.linalg.cg`` semantics)."""
     return LinearSolver(tol, atol, maxiter, precision, refine)
+
+
+def bicgstab(*, tol=1e-8, atol=0.0, maxiter=20_000):
+    """BiCGStab on the B200 kernels (``jax.scipy.sparse.linalg.bicgstab`` semantics,
+    jno/solve.py:209-213); with ``M=jno.precond.jacobi()`` it is the steady ``fem.solve()`` default
+    (jno/_fem.py:110-116)."""
+    return LinearSolver(tol, atol, maxiter, name="bicgstab")

@@ -51,6 +51,68 @@ def pcg(A, b, inv_diag=None, x0=None, tol=1e-8, atol=0.0, maxiter=20_000):
     return x, k, hist
 
 
+def bicgstab(A, b, inv_diag=None, x0=None, tol=1e-8, atol=0.0, maxiter=20_000):
+    """``jax.scipy.sparse.linalg.bicgstab`` (jax 0.10.1), called by ``jno.solve.bicgstab``
+    (``jno/solve.py:209-213``) and by the ``fem.solve()`` steady default with the Jacobi
+    preconditioner (``jno/_fem.py:110-116``). Its published algorithm, restated:
+
+        r = b - A x0;  rhat = r;  rho = alpha = omega = 1;  p = q = r;  k = 0
+        atol2 = max(tol^2 <b, b>, atol^2)
+        while <r, r> > atol2 and k < maxiter and k >= 0:
+            rho' = <rhat, r>;  beta = rho' / rho * alpha / omega
+            p = r + beta (p - omega q);  phat = M p;  q = A phat
+            alpha = rho' / <rhat, q>;  s = r - alpha q;  early = <s, s> < atol2
+            shat = M s;  t = A shat;  omega = <t, s> / <t, t>
+            x = x + alpha phat            if early else  x + (alpha phat + omega shat)
+            r = s                         if early else  s - omega t
+            k = -10 if rho' == 0 else (-11 if omega == 0 or alpha == 0 else k + 1);  rho = rho'
+
+    Returns (x, k): k < 0 reports a breakdown (the loop ends there, x as it stands).
+    """
+    b = np.asarray(b, dtype=np.float64)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
+
+    def M(v):
+        return v if inv_diag is None else inv_diag * v
+
+    r = b - A @ x
+    rhat = r.copy()
+    p = r.copy()
+    q = r.copy()
+    rho = alpha = omega = 1.0
+    atol2 = max(tol * tol * float(np.dot(b, b)), atol * atol)
+    k = 0
+    while float(np.dot(r, r)) > atol2 and k < maxiter and k >= 0:
+        rho_ = float(np.dot(rhat, r))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            beta = float(np.float64(rho_) / rho * alpha / omega)
+        p = r + beta * (p - omega * q)
+        phat = M(p)
+        q = A @ phat
+        with np.errstate(divide="ignore", invalid="ignore"):
+            alpha = float(np.float64(rho_) / np.dot(rhat, q))
+        s = r - alpha * q
+        early = float(np.dot(s, s)) < atol2
+        shat = M(s)
+        t = A @ shat
+        with np.errstate(divide="ignore", invalid="ignore"):
+            omega = float(np.dot(t, s) / np.dot(t, t))
+        if early:
+            x = x + alpha * phat
+            r = s
+        else:
+            x = x + (alpha * phat + omega * shat)
+            r = s - omega * t
+        if rho_ == 0.0:
+            k = -10
+        elif omega == 0.0 or alpha == 0.0:
+            k = -11
+        else:
+            k += 1
+        rho = rho_
+    return x, k
+
+
 def residual_check(A, b, x, rtol=1e-4):
     """Relative true residual; raises RuntimeError like ``_maybe_residual_check``."""
     rel = float(np.linalg.norm(b - A @ x) / (np.linalg.norm(b) + 1e-30))

@@ -380,8 +380,8 @@ def test_jno_surface_non_parametric_route():
     assert np.abs(b.cpu().numpy() - so.b).max() <= 1e-11 * np.abs(so.b).max()
     idx, data = A.to_bcoo()
     assert idx.shape == (B.nnz, 2)
-    xs = fem.solve()
-    xo = op.pcg(B, so.b, oa.jacobi_inverse(oa.matrix_diagonal(so)), tol=1e-8)[0]
+    xs = fem.solve()  # the reference's steady default: Jacobi-BiCGStab
+    xo = op.bicgstab(B, so.b, oa.jacobi_inverse(oa.matrix_diagonal(so)), tol=1e-8)[0]
     assert np.linalg.norm(xs.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
     assert np.abs(xs.cpu().numpy()[bnd] - g[bnd]).max() <= 1e-7 * np.abs(g).max()
     yv = torch.as_tensor(np.random.default_rng(1).standard_normal(plan_n(fem)), device="cuda")
@@ -390,3 +390,50 @@ def test_jno_surface_non_parametric_route():
 
 def plan_n(fem):
     return fem.plan.n
+
+
+@pytest.mark.parametrize("n,order,bulk", [(8, 1, True), (8, 1, False), (24, 1, True), (4, 2, True)])
+def test_bicgstab_matches_oracle(n, order, bulk, monkeypatch):
+    """femk_bicgstab against the oracle's restatement of jax.scipy.sparse.linalg.bicgstab."""
+    if not bulk:
+        monkeypatch.setenv("FEMK_BULK", "0")
+    pf, cf, tets, p1 = _mesh(n, order)
+    logk = om.logk_field(len(tets), 1005)
+    plan = _plan(p1, tets, order)
+    vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
+    inv = plan.jacobi(vals)
+    u, it, rel, st = plan.bicgstab(vals, b, inv_diag=inv, tol=1e-8)
+    s, _ = _oracle_system(pf, cf, order, logk)
+    A = s.csr()
+    xo, ko = op.bicgstab(A, s.b, oa.jacobi_inverse(oa.matrix_diagonal(s)), tol=1e-8)
+    assert st == 0 and ko > 0
+    assert abs(it - ko) <= 2, (it, ko)
+    uu = u.cpu().numpy()
+    assert np.linalg.norm(uu - xo) <= 1e-7 * np.linalg.norm(xo)
+    assert abs(rel - op.residual_check(A, s.b, uu)) <= 1e-12
+    # a second solve from the first solution's neighbourhood reuses the captured graph
+    u2, it2, rel2, st2 = plan.bicgstab(vals, b, inv_diag=inv, tol=1e-8)
+    assert st2 == 0 and it2 == it and torch.equal(u2, u)
+    # no preconditioner, through the jno surface
+    import jno_b200 as jno
+    from jno_b200.sparse import CsrMatrix
+
+    xn = jno.solve.bicgstab(tol=1e-8)(CsrMatrix(plan, vals), b)
+    xon, _ = op.bicgstab(A, s.b, None, tol=1e-8)
+    assert np.linalg.norm(xn.cpu().numpy() - xon) <= 1e-7 * np.linalg.norm(xon)
+
+
+def test_bicgstab_status_paths():
+    pf, cf, tets, p1 = _mesh(4, 1)
+    plan = _plan(p1, tets, 1)
+    vals, b = plan.assemble(torch.zeros(len(tets), dtype=torch.float64, device="cuda"))
+    inv = plan.jacobi(vals)
+    u, it, rel, st = plan.bicgstab(vals, b, inv_diag=inv, maxiter=1)
+    assert st == 4 and it == 1  # iteration cap: NOT_CONVERGED, x written
+    u, it, rel, st = plan.bicgstab(vals, torch.zeros_like(b), inv_diag=inv)
+    assert st == 0 and it == 0 and torch.all(u == 0)
+    import jno_b200 as jno
+    from jno_b200.sparse import CsrMatrix
+
+    with pytest.raises(RuntimeError, match="jno.solve.bicgstab did not solve"):
+        jno.solve.bicgstab(maxiter=1)(CsrMatrix(plan, vals), b, M=jno.precond.jacobi())

@@ -166,3 +166,22 @@ def test_pcg_zero_rhs_takes_no_iteration():
     A = np.eye(3)
     x, it, _ = op.pcg(A, np.zeros(3), np.ones(3))
     assert it == 0 and np.all(x == 0)
+
+
+def test_bicgstab_matches_direct_and_stops_like_jax():
+    n = 6
+    pts, tets = om.equi_distant_box(n, n, n)
+    pts = om.jitter_interior(pts, n, n, n, seed=0)
+    bnd = om.boundary_nodes(tets, 1)
+    s = oa.assemble(pts, tets, 1, bnd, np.exp(om.logk_field(len(tets), 1000)))
+    A = s.csr()
+    inv = oa.jacobi_inverse(oa.matrix_diagonal(s))
+    x, k = op.bicgstab(A, s.b, inv, tol=1e-8)
+    xd = _solve_direct(s)
+    assert k > 3 and np.linalg.norm(s.b - A @ x) <= 1e-8 * np.linalg.norm(s.b) * 1.0000001
+    assert np.abs(x - xd).max() <= 1e-7 * np.abs(xd).max()
+    # zero right-hand side: no iteration; a cap of one iteration stops after one
+    x0, k0 = op.bicgstab(A, np.zeros_like(s.b), inv)
+    assert k0 == 0 and np.all(x0 == 0)
+    _, k1 = op.bicgstab(A, s.b, inv, maxiter=1)
+    assert k1 == 1
