@@ -537,9 +537,13 @@ def run_ours(args):
         raise RuntimeError("the profiled FP64 solves recorded no SpMV timings")
     sell_ms = step_ms_tot / max(prof_iters, 1)
     col_bytes = 2 if plan.cols16 else 4
-    # bytes the kernel must move: every stored sliced-ELL entry (value + column), slice offsets,
-    # x read once, y written once
-    sell_bytes = plan.sell_nnz * (8 + col_bytes) + 8 * ((ndof + 31) // 32 + 1) + 16 * ndof
+    nsl = (ndof + 31) // 32
+    tables = plan.cols16 and plan.sell_col_units != plan.sell_nnz
+    # bytes the kernel must move: every stored sliced-ELL value, the column entries it streams (per-slice
+    # tables: a slice whose rows share one offset sequence stores it once), slice offsets (and table
+    # offsets), x read once, y written once
+    sell_bytes = (plan.sell_nnz * 8 + plan.sell_col_units * col_bytes + 8 * (nsl + 1) * (2 if tables else 1)
+                  + 16 * ndof)
     csr_bytes = 12 * nnz + 20 * ndof + 4
     peak = 6547.5
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -553,8 +557,11 @@ def run_ours(args):
     achieved = sell_bytes / (sell_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": roofline_traffic(),
-                "kernel": f"k_sell (FP64 sliced-ELL SpMV, {'int16' if plan.cols16 else 'int32'} column offsets)",
+                "kernel": (f"k_sell_bulk (FP64 sliced-ELL CG-step SpMV, bulk-copy ring, "
+                           f"{'int16' if plan.cols16 else 'int32'} column offsets"
+                           f"{', per-slice column tables' if tables else ''})"),
                 "bytes_per_launch": sell_bytes, "ms_per_launch": sell_ms, "peak_source": peak_src,
+                "column_entries": plan.sell_col_units, "stored_entries": plan.sell_nnz,
                 "timing": f"CUDA events around each CG-step SpMV inside {prof_iters} profiled iterations",
                 "in_loop_ms": {"step_spmv": sell_ms, "update": upd_ms_tot / max(prof_iters, 1),
                                "p_update": pup_ms_tot / max(prof_iters, 1)},

@@ -35,6 +35,9 @@ extern "C" {
 #define FEMK_COEF_EXP 0      /* g = exp  : jno.np.exp(logk) * ...  (P0 log-conductivity) */
 #define FEMK_COEF_LINEAR 1   /* g = id   : rho * ...               (P0 linear parameter) */
 #define FEMK_COEF_CONST 2    /* g = 1    : param ignored (may be NULL) */
+/* nodal P1 parameters (param f64[nvert], one value per P1 vertex; P1 plans only) */
+#define FEMK_COEF_NODAL_EXP 3    /* k = exp(linear log-field), 4-point degree-2 quadrature mean */
+#define FEMK_COEF_NODAL_LINEAR 4 /* k = linear field, element mean (exact) */
 
 /* precision modes for femk_pcg_mixed */
 #define FEMK_MIXED_RELIABLE 0 /* FP32 inner CG with FP64 reliable updates (no restart) */
@@ -55,6 +58,8 @@ typedef struct femk_plan_info {
   int64_t sell_nnz;   /* stored entries of the solver's sliced-ELL copy (padding included), 0 if none */
   int32_t batch_graph; /* 1 when the last femk_pcg_batched ran as a replayed CUDA graph */
   int32_t pad;
+  int64_t sell_col_units; /* column entries the CG-step SpMV streams per product (int16 units when
+                             cols16: per-slice tables, a shared-offset slice stored once) */
 } femk_plan_info;
 
 /* Library version (major*10000 + minor*100 + patch). */
@@ -99,7 +104,8 @@ int femk_plan_export(const femk_plan* plan, int32_t* indptr_dev, int32_t* indice
 
 /*
  * Parametric assembly of  k_e * grad u . grad v - f v  with symmetric Dirichlet u = g.
- *   param_dev f64[ntet] (per-element P0 value, see FEMK_COEF_*), coef_scale multiplies k_e,
+ *   param_dev f64[ntet] (per-element P0 value) or f64[nvert] (nodal P1 modes), see FEMK_COEF_*;
+ *   coef_scale multiplies k_e,
  *   f       constant source, g_dev f64[n] Dirichlet values or NULL (= 0),
  *   vals_dev f64[nnz] (canonical CSR values, explicit zeros kept) or NULL to assemble the load only
  *   (matrix-free use), b_dev f64[n].

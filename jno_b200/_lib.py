@@ -22,6 +22,7 @@ FEMK_EBOUNDS = 7
 FEMK_BREAKDOWN = 8
 
 COEF_EXP, COEF_LINEAR, COEF_CONST = 0, 1, 2
+COEF_NODAL_EXP, COEF_NODAL_LINEAR = 3, 4  # nodal P1 parameters (one value per P1 vertex)
 MIXED_RELIABLE, MIXED_RESTART = 0, 1
 
 _STATUS_NAMES = {
@@ -56,6 +57,7 @@ class PlanInfo(ctypes.Structure):
         ("sell_nnz", ctypes.c_int64),
         ("batch_graph", ctypes.c_int32),
         ("pad", ctypes.c_int32),
+        ("sell_col_units", ctypes.c_int64),
     ]
 
 

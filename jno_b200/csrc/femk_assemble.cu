@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(kThreads) k_assemble(const double* __restrict_
     tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
     double VG[4][4];
     gram(T, VG);
-    const double k = coef_of(param, mode, scale, c);
+    const double k = coef_any(param, mode, scale, c, dof);
     bool dir[ND];
 #pragma unroll
     for (int a = 0; a < ND; ++a) dir[a] = __ldg(dmask + dof[a]) != 0;
@@ -140,8 +140,8 @@ extern "C" int femk_assemble(const femk_plan* p, const double* param, int mode, 
                              const double* g, double* vals, double* b, void* stream) {
   clear_error();
   FEMK_CHECK_ARG(p && b, "femk_assemble: NULL plan/b");
-  FEMK_CHECK_ARG(mode >= 0 && mode <= 2, "femk_assemble: unknown coef_mode");
-  FEMK_CHECK_ARG(mode == 2 || param, "femk_assemble: param is NULL");
+  FEMK_CHECK_ARG(coef_mode_ok(p, mode, param),
+                 "femk_assemble: unknown coef_mode, NULL param, or a nodal mode on a P2 plan");
   cudaStream_t s = (cudaStream_t)stream;
   if (vals) FEMK_CUDA_TRY(cudaMemsetAsync(vals, 0, sizeof(double) * p->nnz, s));
   FEMK_CUDA_TRY(cudaMemsetAsync(b, 0, sizeof(double) * p->n, s));

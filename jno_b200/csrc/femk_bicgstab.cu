@@ -70,7 +70,7 @@ struct Epi {
   const double* b;
   Vecs v;
   double* acc;
-  __device__ __forceinline__ void operator()(int64_t row, double sv, double = 0.0) const {
+  __device__ __forceinline__ void operator()(int64_t row, double sv) const {
     if (KIND == kInitR) {
       const double bi = b[row];
       const double ri = bi - sv;
@@ -158,7 +158,8 @@ __global__ void __launch_bounds__(kBulkW * 32) k_bicg_bulk(const int64_t* __rest
                                                           const int16_t* __restrict__ cols,
                                                           const double* __restrict__ vals, int64_t n, int64_t nslices,
                                                           const double* __restrict__ x, const double* __restrict__ b,
-                                                          Vecs v, double* __restrict__ partials, BicgState* st) {
+                                                          Vecs v, double* __restrict__ partials, BicgState* st,
+                                                          const int64_t* __restrict__ cptr) {
   extern __shared__ __align__(128) unsigned char bulk_smem[];
   using R = BulkRing<double, int16_t, WMAX, kBulkS>;
   if (kind_skips<KIND>(st)) return;
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(kBulkW * 32) k_bicg_bulk(const int64_t* __rest
   const bool ok = sell_bulk_rows<double, int16_t, WMAX, kBulkS>(
       bulk_smem + wib * R::kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * kBulkW + wib,
       (int64_t)gridDim.x * kBulkW, GatherXL<double>{x, l2_evict_last()}, Epi<KIND>{b, v, acc}, &st->status,
-      FEMK_TIMEOUT);
+      FEMK_TIMEOUT, cptr);
   if (!ok && (threadIdx.x & 31) == 0) st->done = 1;
   finish<KIND, kBulkW * 32>(st, acc, partials);
 }
@@ -266,14 +267,17 @@ bool launch_bulk_kind(const femk_plan* p, const double* x, const double* b, cons
   }
   if (per_sm <= 0) return false;
   if (prime) return true;
+  const bool tab = p->sell_cu != nullptr;
   kern<<<counted_launch() + p->n_sm * std::min(per_sm, 16), kBulkW * 32, kSmem, s>>>(
-      p->sell_ptr, p->sell_c16, p->sell_vals, p->n, p->n_slices, x, b, v, p->partials, st);
+      p->sell_ptr, tab ? p->sell_cu : p->sell_c16, p->sell_vals, p->n, p->n_slices, x, b, v, p->partials, st,
+      tab ? p->sell_cuptr : nullptr);
   return true;
 }
 
 bool bulk_usable(const femk_plan* p) {
   return p->bulk_cfg != 0 && p->sell_c16 && p->sell64_c16 && p->max_row <= 32 &&
-         ((uintptr_t)p->sell_vals & 15u) == 0 && ((uintptr_t)p->sell_c16 & 15u) == 0;
+         ((uintptr_t)p->sell_vals & 15u) == 0 && ((uintptr_t)p->sell_c16 & 15u) == 0 &&
+         ((uintptr_t)p->sell_cu & 15u) == 0;
 }
 
 template <int KIND>

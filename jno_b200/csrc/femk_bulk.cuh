@@ -85,26 +85,21 @@ struct BulkRing {
   static_assert(kVal % 128 == 0, "stage alignment");
 };
 
-// Blocks per SM that the ring's shared memory allows (at most 16): the kernels ask the compiler for
-// registers that let this many blocks be resident.
-template <typename V, typename IDX, int WMAX, int S, int WPB>
-constexpr int bulk_min_blocks() {
-  constexpr int per_block = WPB * BulkRing<V, IDX, WMAX, S>::kWarpBytes + 1024;
-  constexpr int b = (227 * 1024) / per_block;
-  return b < 1 ? 1 : (b > 16 ? 16 : b);
-}
-
 // Every slice of this warp (global warp g takes slices g, g + NW, ...): for each row,
-// epi(row, row_sum, x[row]). Returns false if a wait timed out (and sets *err to errval).
+// epi(row, row_sum). Returns false if a wait timed out (and sets *err to errval).
+//
+// cptr == NULL: cols holds one column (or offset) per stored entry, like vals. cptr != NULL: cols is
+// the per-slice column table (int16 offsets): slice s's table starts at cptr[s] and holds either w
+// offsets shared by all 32 rows (padded to 8) or the 32*w per-entry offsets.
 template <typename V, typename IDX, int WMAX, int S, typename G, typename Epi>
 __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64_t* __restrict__ sptr,
                                                const IDX* __restrict__ cols, const V* __restrict__ vals, int64_t n,
                                                int64_t nslices, int64_t g, int64_t NW, const G& gx, Epi&& epi,
-                                               int* err, int errval) {
+                                               int* err, int errval, const int64_t* __restrict__ cptr = nullptr) {
   using R = BulkRing<V, IDX, WMAX, S>;
   const int lane = threadIdx.x & 31;
   uint64_t* bar = reinterpret_cast<uint64_t*>(wsmem);
-  int32_t* wid = reinterpret_cast<int32_t*>(wsmem + 8 * S);
+  int32_t* wid = reinterpret_cast<int32_t*>(wsmem + 8 * S);  // slice width; negative: shared offsets
   unsigned char* stages = wsmem + R::kHead;
   uint64_t pol = 0;
   if (lane == 0) {
@@ -113,18 +108,24 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
     mbar_fence_init();
   }
   __syncwarp();
-  // lane 0: stream slice entries [b0, b1) into stage `s`
-  auto issue = [&](int64_t b0, int64_t b1, int s) {
-    const int32_t w = (int32_t)((b1 - b0) >> 5);
-    wid[s] = w;
+  // lane 0: stream slice `sl` into stage `s`
+  auto issue = [&](int64_t sl, int s) {
+    const int64_t b0 = __ldg(sptr + sl);
+    const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
+    int64_t c0 = b0, cn = 32 * (int64_t)w;
+    if (cptr) {
+      c0 = __ldg(cptr + sl);
+      cn = __ldg(cptr + sl + 1) - c0;
+    }
+    wid[s] = cn == 32 * (int64_t)w ? w : -w;
     const uint32_t vb = (uint32_t)(32 * w * (int)sizeof(V));
-    const uint32_t cb = (uint32_t)(32 * w * (int)sizeof(IDX));
+    const uint32_t cb = (uint32_t)(cn * (int64_t)sizeof(IDX));
     unsigned char* st = stages + s * R::kStage;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(bar + s, vb + cb);  // with w == 0 this arrival alone completes the phase
     if (w > 0) {
       bulk_g2s(st, vals + b0, vb, bar + s, pol);
-      bulk_g2s(st + R::kVal, cols + b0, cb, bar + s, pol);
+      bulk_g2s(st + R::kVal, cols + c0, cb, bar + s, pol);
     }
   };
   int64_t issued = 0;  // slices issued so far (lane 0's count; slice i lives in stage i % S)
@@ -132,7 +133,7 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
     for (int s = 0; s < S; ++s) {
       const int64_t sl = g + (int64_t)s * NW;
       if (sl >= nslices) break;
-      issue(__ldg(sptr + sl), __ldg(sptr + sl + 1), s);
+      issue(sl, s);
       ++issued;
     }
   __syncwarp();
@@ -141,32 +142,25 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
   for (int64_t sl = g; sl < nslices; sl += NW, ++i) {
     const int s = (int)(i % S);
     const uint32_t parity = (uint32_t)((i / S) & 1);
-    // lane 0 reads the offsets of the slice that refills this stage now, so that load overlaps
-    // the gathers below instead of delaying the refill
-    const int64_t nsl = sl + (int64_t)S * NW;
-    int64_t nb0 = 0, nb1 = 0;
-    if (lane == 0 && nsl < nslices) {
-      nb0 = __ldg(sptr + nsl);
-      nb1 = __ldg(sptr + nsl + 1);
-    }
     // warp-uniform outcome: a lane that timed out takes the whole warp out of the loop
     if (!__all_sync(0xffffffffu, mbar_wait(bar + s, parity))) {
       ok = false;
       break;
     }
-    const int32_t w = wid[s];
+    const int32_t ws = wid[s];
+    const int32_t w = ws < 0 ? -ws : ws;
+    const int cstride = ws < 0 ? 1 : 32;  // shared offsets: every lane reads entry k (a broadcast)
+    const int clane = ws < 0 ? 0 : lane;
     const V* sv = reinterpret_cast<const V*>(stages + s * R::kStage);
     const IDX* sc = reinterpret_cast<const IDX*>(stages + s * R::kStage + R::kVal);
     const int64_t row = sl * 32 + lane;
     const bool live = row < n;  // rows past n in the last slice gather nothing
     V xg[WMAX];
-    V xrow = V(0);  // x[row], from the diagonal entry's gather (every row stores its diagonal)
 #pragma unroll
     for (int k = 0; k < WMAX; ++k) {
       if (k < w && live) {
-        const IDX c = sc[k * 32 + lane];
+        const IDX c = sc[k * cstride + clane];
         xg[k] = gx(sizeof(IDX) == 2 ? (int64_t)row + (int64_t)c : (int64_t)c);
-        if (sizeof(IDX) == 2 ? c == 0 : (int64_t)c == row) xrow = xg[k];
       }
     }
     V acc = V(0);
@@ -174,12 +168,15 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
     for (int k = 0; k < WMAX; ++k)
       if (k < w && live) acc += sv[k * 32 + lane] * xg[k];
     __syncwarp();  // every lane is done with stage s before it is refilled
-    if (lane == 0 && nsl < nslices) {
-      issue(nb0, nb1, s);
-      ++issued;
+    if (lane == 0) {
+      const int64_t nsl = g + (i + S) * NW;
+      if (nsl < nslices) {
+        issue(nsl, s);
+        ++issued;
+      }
     }
     __syncwarp();
-    if (live) epi(row, acc, xrow);
+    if (live) epi(row, acc);
   }
   if (!ok) {
     if (lane == 0) {

@@ -214,11 +214,12 @@ __global__ void __launch_bounds__(kThreads) k_sell(const int64_t* __restrict__ s
 // The same SpMV (kPlain, kCgStep) with the sliced-ELL stream moved into shared memory by bulk
 // copies (femk_bulk.cuh): WPB warps per block, S slices in flight per warp, widths up to WMAX.
 template <int MODE, typename IDX, int WMAX, int S, int WPB>
-__global__ void __launch_bounds__(WPB * 32, (bulk_min_blocks<double, IDX, WMAX, S, WPB>())) k_sell_bulk(const int64_t* __restrict__ sptr,
+__global__ void __launch_bounds__(WPB * 32) k_sell_bulk(const int64_t* __restrict__ sptr,
                                                        const IDX* __restrict__ scols,
                                                        const double* __restrict__ svals, int64_t n, int64_t nslices,
                                                        const double* __restrict__ x, double* __restrict__ y,
-                                                       double* __restrict__ partials, CgState* st, int* err) {
+                                                       double* __restrict__ partials, CgState* st, int* err,
+                                                       const int64_t* __restrict__ cptr) {
   extern __shared__ __align__(128) unsigned char bulk_smem[];
   using R = BulkRing<double, IDX, WMAX, S>;
   pdl_wait();
@@ -234,11 +235,11 @@ __global__ void __launch_bounds__(WPB * 32, (bulk_min_blocks<double, IDX, WMAX, 
   int* errp = MODE == kCgStep ? &st->status : err;
   const bool ok = sell_bulk_rows<double, IDX, WMAX, S>(
       bulk_smem + wib * R::kWarpBytes, sptr, scols, svals, n, nslices, g, NW, GatherXL<double>{x, l2_evict_last()},
-      [&](int64_t row, double sv, double xrow) {
+      [&](int64_t row, double sv) {
         y[row] = sv;
-        if (MODE == kCgStep) acc[0] += xrow * sv;
+        if (MODE == kCgStep) acc[0] += __ldg(x + row) * sv;
       },
-      errp, FEMK_TIMEOUT);
+      errp, FEMK_TIMEOUT, cptr);
   if (MODE == kPlain) return;
   if (!ok && (threadIdx.x & 31) == 0) st->done = 1;
   block_reduce_store<1, WPB * 32>(acc, partials);
@@ -686,7 +687,7 @@ __global__ void __launch_bounds__(128) k_matfree(const double* __restrict__ xyz,
     tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
     double VG[4][4];
     gram(T, VG);
-    const double k = coef_of(param, mode, scale, c);
+    const double k = coef_any(param, mode, scale, c, dof);
 #pragma unroll
     for (int a = 0; a < ND; ++a) {
       if (dir[a]) continue;
@@ -719,7 +720,7 @@ __global__ void k_matfree_diag(const double* __restrict__ xyz, const int32_t* __
     tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
     double VG[4][4];
     gram(T, VG);
-    const double k = coef_of(param, mode, scale, c);
+    const double k = coef_any(param, mode, scale, c, dof);
 #pragma unroll
     for (int a = 0; a < ND; ++a)
       if (!__ldg(dmask + dof[a])) atomicAdd(d + dof[a], k * khat<ND>(VG, a, a));
@@ -907,9 +908,10 @@ bool launch_sell_bulk_cfg(const femk_plan* p, const double* x, double* y, CgStat
   if (per_sm <= 0) return false;
   if (prime) return true;
   const int grid = p->n_sm * std::min(per_sm, 16);
+  const bool tab = p->sell_cu != nullptr;  // per-slice column tables (shared-offset slices stored once)
   (void)launch_ex(p->pdl != 0, kern, grid, WPB * 32, kSmem, s, (const int64_t*)p->sell_ptr,
-                  (const int16_t*)p->sell_c16, (const double*)p->sell_vals, p->n, p->n_slices, x, y, p->partials, st,
-                  (int*)nullptr);
+                  (const int16_t*)(tab ? p->sell_cu : p->sell_c16), (const double*)p->sell_vals, p->n, p->n_slices, x,
+                  y, p->partials, st, (int*)nullptr, (const int64_t*)(tab ? p->sell_cuptr : nullptr));
   return true;
 }
 
@@ -918,6 +920,7 @@ bool launch_sell_bulk(const femk_plan* p, const double* x, double* y, CgState* s
                       bool prime = false) {
   if (!p->bulk_cfg || !p->sell_c16 || !p->sell64_c16 || p->max_row > 32) return false;
   if (!aligned16(p->sell_vals) || !aligned16(p->sell_c16)) return false;  // bulk copies start on 16 B
+  if (p->sell_cu && !aligned16(p->sell_cu)) return false;
   const bool narrow = p->max_row <= 16;
 #define FEMK_BULK_CFG(code, S, WPB)                                                         \
   case code:                                                                                \
@@ -925,15 +928,10 @@ bool launch_sell_bulk(const femk_plan* p, const double* x, double* y, CgState* s
                   : launch_sell_bulk_cfg<S, WPB, 32>(p, x, y, st, s, prime);
   switch (p->bulk_cfg) {
     FEMK_BULK_CFG(12, 1, 2)
-    FEMK_BULK_CFG(14, 1, 4)
     FEMK_BULK_CFG(22, 2, 2)
     FEMK_BULK_CFG(24, 2, 4)
     FEMK_BULK_CFG(28, 2, 8)
     FEMK_BULK_CFG(34, 3, 4)
-    FEMK_BULK_CFG(38, 3, 8)
-    FEMK_BULK_CFG(44, 4, 4)
-    FEMK_BULK_CFG(42, 4, 2)
-    FEMK_BULK_CFG(62, 6, 2)
     default:
       return false;
   }
@@ -1406,7 +1404,7 @@ extern "C" int femk_spmv_matfree(const femk_plan* p, const double* param, int mo
                                  double* y, void* stream) {
   clear_error();
   FEMK_CHECK_ARG(p && x && y, "femk_spmv_matfree: NULL argument");
-  FEMK_CHECK_ARG(mode >= 0 && mode <= 2 && (mode == 2 || param), "femk_spmv_matfree: bad coefficient");
+  FEMK_CHECK_ARG(coef_mode_ok(p, mode, param), "femk_spmv_matfree: bad coefficient");
   MatFree m{param, mode, scale};
   return launch_matfree(p, m, x, y, (cudaStream_t)stream);
 }
@@ -1415,7 +1413,7 @@ extern "C" int femk_jacobi_matfree(const femk_plan* p, const double* param, int 
                                    void* stream) {
   clear_error();
   FEMK_CHECK_ARG(p && inv, "femk_jacobi_matfree: NULL argument");
-  FEMK_CHECK_ARG(mode >= 0 && mode <= 2 && (mode == 2 || param), "femk_jacobi_matfree: bad coefficient");
+  FEMK_CHECK_ARG(coef_mode_ok(p, mode, param), "femk_jacobi_matfree: bad coefficient");
   cudaStream_t s = (cudaStream_t)stream;
   FEMK_CUDA_TRY(cudaMemsetAsync(inv, 0, sizeof(double) * p->n, s));
   const int grid = blocks_for(p->ntet, 128, p->n_sm * 16);
@@ -1442,7 +1440,7 @@ extern "C" int femk_pcg_matfree(const femk_plan* p, const double* param, int mod
                                 int32_t* iters_out, double* relres_out, void* stream) {
   clear_error();
   FEMK_CHECK_ARG(p && b && x, "femk_pcg_matfree: NULL argument");
-  FEMK_CHECK_ARG(mode >= 0 && mode <= 2 && (mode == 2 || param), "femk_pcg_matfree: bad coefficient");
+  FEMK_CHECK_ARG(coef_mode_ok(p, mode, param), "femk_pcg_matfree: bad coefficient");
   MatFree m{param, mode, scale};
   return pcg_run(p, nullptr, &m, b, x, dinv, tol, atol, maxiter, iters_out, relres_out, (cudaStream_t)stream);
 }

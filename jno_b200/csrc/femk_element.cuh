@@ -7,6 +7,8 @@
 // quadrature of degree 2 (P1) / 4 (P2), exact for these degree <= 2 integrands).
 #pragma once
 
+#include "../../include/femk.h"
+
 #include <stdint.h>
 
 namespace femk {
@@ -90,6 +92,31 @@ __device__ __forceinline__ double coef_of(const double* __restrict__ param, int 
   if (mode == 2) return scale;
   const double p = __ldg(param + c);
   return mode == 0 ? scale * exp(p) : scale * p;
+}
+
+// Element coefficient of a nodal P1 parameter (one value per P1 vertex, interpolated linearly).
+// P1 stiffness integrands are constant on an element, so K_e = V G * mean_q k(x_q):
+//  * linear k (FEMK_COEF_NODAL_LINEAR): the quadrature mean of a linear field is the vertex mean;
+//  * exp of a linear log-field (FEMK_COEF_NODAL_EXP): the symmetric 4-point degree-2 tetrahedron
+//    rule (points with barycentric coordinates (b, a, a, a) and its permutations,
+//    a = (5 - sqrt 5) / 20, b = (5 + 3 sqrt 5) / 20, equal weights), the rule for quadrature degree 2
+//    that P1 forms are integrated with (jno/_fem.py:4551).
+__device__ __forceinline__ double coef_nodal(const double* __restrict__ param, int mode, double scale, int32_t v0,
+                                             int32_t v1, int32_t v2, int32_t v3) {
+  const double p0 = __ldg(param + v0), p1 = __ldg(param + v1), p2 = __ldg(param + v2), p3 = __ldg(param + v3);
+  if (mode == FEMK_COEF_NODAL_LINEAR) return scale * (0.25 * (p0 + p1 + p2 + p3));
+  constexpr double a = 0.13819660112501051518, b = 0.58541019662496845446;
+  const double s = p0 + p1 + p2 + p3;
+  const double e = exp(a * s + (b - a) * p0) + exp(a * s + (b - a) * p1) + exp(a * s + (b - a) * p2) +
+                   exp(a * s + (b - a) * p3);
+  return scale * (0.25 * e);
+}
+
+// the element coefficient for any FEMK_COEF_* mode; dof[0..3] are the element's vertex DOFs
+__device__ __forceinline__ double coef_any(const double* __restrict__ param, int mode, double scale, int64_t c,
+                                           const int32_t* dof) {
+  if (mode >= FEMK_COEF_NODAL_EXP) return coef_nodal(param, mode, scale, dof[0], dof[1], dof[2], dof[3]);
+  return coef_of(param, mode, scale, c);
 }
 
 }  // namespace femk

@@ -41,6 +41,10 @@ void count_launches(int64_t k);
     }                                       \
   } while (0)
 
+// A coefficient mode is valid for a plan: P0 modes anywhere, nodal P1 modes on P1 plans only;
+// every mode but CONST reads param.
+inline bool coef_mode_ok(const femk_plan* p, int mode, const double* param);
+
 #define FEMK_TRY(expr)          \
   do {                          \
     int _s = (expr);            \
@@ -97,8 +101,15 @@ struct femk_plan {
   int16_t* sell_c16 = nullptr;   // i16[sell_nnz] col - row, when the bandwidth fits
   double* sell_vals = nullptr;   // f64[sell_nnz] values gathered for the current solve
   float* sell_vals32 = nullptr;  // f32[sell_nnz] FP32 values for the mixed-precision inner solve
+  // per-slice column tables of the bulk-copy SpMV (int16 offsets): a slice whose rows share one
+  // offset sequence stores it once (padded to 8), any other slice its 32*w per-entry offsets
+  int sell_uni = 1;
+  int64_t* sell_cuptr = nullptr;  // i64[n_slices+1] first table entry of each slice
+  int16_t* sell_cu = nullptr;     // i16[sell_cu_len]
+  int64_t sell_cu_len = 0;
   int use_sell = 1;
   int l2_mode = 0;               // L2 eviction hints of the FP64 CG kernels (see l2_hints in femk_spmv.cuh)
+  int l2_mode32 = 0;             // the same for the FP32 kernels of the mixed solver (0 off, 1 on)
   int sell64_c16 = 1;            // FP64 sliced-ELL streams int16 column offsets when available
   // solver workspace (allocated on first use)
   int64_t vstride = 0;          // solver vector stride: n rounded up to 64 (keeps every slot 512-byte aligned)
@@ -151,6 +162,12 @@ struct femk_plan {
 };
 
 namespace femk {
+
+inline bool coef_mode_ok(const femk_plan* p, int mode, const double* param) {
+  if (mode < FEMK_COEF_EXP || mode > FEMK_COEF_NODAL_LINEAR) return false;
+  if (mode >= FEMK_COEF_NODAL_EXP && p->order != 1) return false;
+  return mode == FEMK_COEF_CONST || param != nullptr;
+}
 
 // grid-size helpers
 inline int blocks_for(int64_t n, int threads, int cap = 1 << 30) {

@@ -52,6 +52,18 @@ __device__ __forceinline__ double2 ld_last2(const double2* a, uint64_t pol) {
 __device__ __forceinline__ void st_last2(double2* a, double2 v, uint64_t pol) {
   asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(a), "d"(v.x), "d"(v.y), "l"(pol) : "memory");
 }
+__device__ __forceinline__ float4 ld_last4(const float4* a, uint64_t pol) {
+  float4 v;
+  asm volatile("ld.global.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_last4(float4* a, float4 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(a), "f"(v.x), "f"(v.y), "f"(v.z),
+               "f"(v.w), "l"(pol)
+               : "memory");
+}
 __device__ __forceinline__ double ld_last(const double* a, uint64_t pol) {
   double v;
   asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));

@@ -18,6 +18,7 @@
 // No reference counterpart: jNO runs x64 throughout (tests/test_fem_3d.py:37-46).
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "femk_bulk.cuh"
 #include "femk_internal.cuh"
@@ -158,12 +159,13 @@ __global__ void __launch_bounds__(kThreads, 8) k_step32_sell(const int64_t* __re
 
 // The same step with the FP32 sliced-ELL stream moved into shared memory by bulk copies
 // (femk_bulk.cuh): WPB warps per block, S slices in flight per warp, widths up to WMAX.
-template <int WMAX, int S, int WPB>
-__global__ void __launch_bounds__(WPB * 32, (bulk_min_blocks<float, int16_t, WMAX, S, WPB>())) k_step32_bulk(const int64_t* __restrict__ sptr,
+template <int WMAX, int S, int WPB, bool H>
+__global__ void __launch_bounds__(WPB * 32) k_step32_bulk(const int64_t* __restrict__ sptr,
                                                          const int16_t* __restrict__ cols,
                                                          const float* __restrict__ vals, int64_t n, int64_t nslices,
                                                          const float* __restrict__ p, float* __restrict__ q,
-                                                         double* __restrict__ partials, MixedState* st) {
+                                                         double* __restrict__ partials, MixedState* st,
+                                                         const int64_t* __restrict__ cptr) {
   extern __shared__ __align__(128) unsigned char bulk_smem[];
   using R = BulkRing<float, int16_t, WMAX, S>;
   pdl_wait();
@@ -172,14 +174,18 @@ __global__ void __launch_bounds__(WPB * 32, (bulk_min_blocks<float, int16_t, WMA
   if (st->done || st->hold) return;
   const int wib = threadIdx.x >> 5;
   float acc = 0.f;
+  using G = std::conditional_t<H, GatherXL<float>, GatherX<float>>;
+  G gx;
+  gx.x = p;
+  if constexpr (H) gx.pol = l2_evict_last();
   const bool ok = sell_bulk_rows<float, int16_t, WMAX, S>(
       bulk_smem + wib * R::kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * WPB + wib,
-      (int64_t)gridDim.x * WPB, GatherX<float>{p},
-      [&](int64_t row, float sv, float prow) {
+      (int64_t)gridDim.x * WPB, gx,
+      [&](int64_t row, float sv) {
         q[row] = sv;
-        acc = fmaf(prow, sv, acc);
+        acc = fmaf(__ldg(p + row), sv, acc);
       },
-      &st->status, FEMK_TIMEOUT);
+      &st->status, FEMK_TIMEOUT, cptr);
   if (!ok && (threadIdx.x & 31) == 0) st->done = 1;
   double v[1] = {(double)acc}, tot[1];
   if (!reduce_finish<1, WPB * 32>(v, partials, &st->ticket, tot)) return;
@@ -291,6 +297,7 @@ __global__ void __launch_bounds__(kThreads) k_update32(int64_t n, float* __restr
 //   k_pupdate32_x: e += alpha p; p = D^-1 r + beta p (p only while not held)   (reads e, p, r, D^-1)
 // The iteration that requests a reliable update still owes its e update: k_update32_r raises
 // st->epend and the next step kernel clears it.
+template <bool H>
 __global__ void __launch_bounds__(kThreads) k_update32_r(int64_t n, float* __restrict__ r, const float* __restrict__ q,
                                                         const float* __restrict__ dinv, double* __restrict__ partials,
                                                         MixedState* st) {
@@ -305,8 +312,12 @@ __global__ void __launch_bounds__(kThreads) k_update32_r(int64_t n, float* __res
   float4* r4 = reinterpret_cast<float4*>(r);
   const float4* q4 = reinterpret_cast<const float4*>(q);
   const float4* d4 = reinterpret_cast<const float4*>(dinv);
+  uint64_t pol = 0;
+  if (H) pol = l2_evict_last();
   for (int64_t i = tid; i < n4; i += nt) {
-    const float4 qi = q4[i], di = d4[i], ri0 = r4[i];
+    const float4 qi = H ? ld_last4(q4 + i, pol) : q4[i];
+    const float4 di = H ? ld_last4(d4 + i, pol) : d4[i];
+    const float4 ri0 = H ? ld_last4(r4 + i, pol) : r4[i];
     float4 ri, zi;
     ri.x = fmaf(-alpha, qi.x, ri0.x);
     ri.y = fmaf(-alpha, qi.y, ri0.y);
@@ -316,7 +327,10 @@ __global__ void __launch_bounds__(kThreads) k_update32_r(int64_t n, float* __res
     zi.y = di.y * ri.y;
     zi.z = di.z * ri.z;
     zi.w = di.w * ri.w;
-    r4[i] = ri;
+    if (H)
+      st_last4(r4 + i, ri, pol);
+    else
+      r4[i] = ri;
     a0 = fmaf(ri.x, zi.x, fmaf(ri.y, zi.y, fmaf(ri.z, zi.z, fmaf(ri.w, zi.w, a0))));
     a1 = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, fmaf(ri.z, ri.z, fmaf(ri.w, ri.w, a1))));
   }
@@ -349,6 +363,7 @@ __global__ void __launch_bounds__(kThreads) k_update32_r(int64_t n, float* __res
   }
 }
 
+template <bool H>
 __global__ void __launch_bounds__(kThreads) k_pupdate32_x(int64_t n, float* __restrict__ e, float* __restrict__ p,
                                                          const float* __restrict__ r, const float* __restrict__ dinv,
                                                          const MixedState* st) {
@@ -364,18 +379,27 @@ __global__ void __launch_bounds__(kThreads) k_pupdate32_x(int64_t n, float* __re
   float4* p4 = reinterpret_cast<float4*>(p);
   const float4* r4 = reinterpret_cast<const float4*>(r);
   const float4* d4 = reinterpret_cast<const float4*>(dinv);
+  uint64_t pol = 0;
+  if (H) pol = l2_evict_last();
+  auto ld = [&](const float4* a) { return H ? ld_last4(a, pol) : *a; };
+  auto st4 = [&](float4* a, float4 v) {
+    if (H)
+      st_last4(a, v, pol);
+    else
+      *a = v;
+  };
   for (int64_t i = tid; i < n4; i += nt) {
-    const float4 pi = p4[i];
-    float4 ei = e4[i];
+    const float4 pi = ld(p4 + i);
+    float4 ei = ld(e4 + i);
     ei.x = fmaf(alpha, pi.x, ei.x);
     ei.y = fmaf(alpha, pi.y, ei.y);
     ei.z = fmaf(alpha, pi.z, ei.z);
     ei.w = fmaf(alpha, pi.w, ei.w);
-    e4[i] = ei;
+    st4(e4 + i, ei);
     if (dir) {
-      const float4 ri = r4[i], di = d4[i];
-      p4[i] = make_float4(fmaf(beta, pi.x, di.x * ri.x), fmaf(beta, pi.y, di.y * ri.y),
-                          fmaf(beta, pi.z, di.z * ri.z), fmaf(beta, pi.w, di.w * ri.w));
+      const float4 ri = ld(r4 + i), di = ld(d4 + i);
+      st4(p4 + i, make_float4(fmaf(beta, pi.x, di.x * ri.x), fmaf(beta, pi.y, di.y * ri.y),
+                              fmaf(beta, pi.z, di.z * ri.z), fmaf(beta, pi.w, di.w * ri.w)));
     }
   }
   for (int64_t i = 4 * n4 + tid; i < n; i += nt) {
@@ -654,10 +678,10 @@ void launch_true_resid(const femk_plan* p, const double* vals, const double* x, 
   });
 }
 
-template <int S, int WPB, int WMAX>
-bool launch_step32_bulk_cfg(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
-                            bool prime) {
-  auto kern = k_step32_bulk<WMAX, S, WPB>;
+template <int S, int WPB, int WMAX, bool H>
+bool launch_step32_bulk_h(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
+                          bool prime) {
+  auto kern = k_step32_bulk<WMAX, S, WPB, H>;
   constexpr int kSmem = WPB * BulkRing<float, int16_t, WMAX, S>::kWarpBytes;
   static int per_sm = -1;  // per instantiation: opt-in shared memory size + occupancy, queried once
   if (per_sm < 0) {
@@ -670,10 +694,18 @@ bool launch_step32_bulk_cfg(const femk_plan* p, const float* pv, float* q, Mixed
   if (per_sm <= 0) return false;
   if (prime) return true;
   const int grid = p->n_sm * std::min(per_sm, 16);
+  const bool tab = p->sell_cu != nullptr;  // per-slice column tables (shared-offset slices stored once)
   (void)launch_ex(p->pdl != 0, kern, grid, WPB * 32, kSmem, s, (const int64_t*)p->sell_ptr,
-                  (const int16_t*)p->sell_c16, (const float*)p->sell_vals32, p->n, p->n_slices, pv, q, p->partials,
-                  st);
+                  (const int16_t*)(tab ? p->sell_cu : p->sell_c16), (const float*)p->sell_vals32, p->n, p->n_slices,
+                  pv, q, p->partials, st, (const int64_t*)(tab ? p->sell_cuptr : nullptr));
   return true;
+}
+
+template <int S, int WPB, int WMAX>
+bool launch_step32_bulk_cfg(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
+                            bool prime) {
+  return p->l2_mode32 != 0 ? launch_step32_bulk_h<S, WPB, WMAX, true>(p, pv, q, st, s, prime)
+                         : launch_step32_bulk_h<S, WPB, WMAX, false>(p, pv, q, st, s, prime);
 }
 
 // bulk-copy FP32 step in the plan's configuration (bulk32_cfg: 10 * stages + warps per block)
@@ -682,6 +714,7 @@ bool launch_step32_bulk(const femk_plan* p, const float* pv, float* q, MixedStat
                         bool prime = false) {
   if (!p->bulk32_cfg || !p->sell_vals32 || !p->sell_c16 || p->max_row > 32) return false;
   if (((uintptr_t)p->sell_vals32 & 15u) || ((uintptr_t)p->sell_c16 & 15u)) return false;
+  if (p->sell_cu && ((uintptr_t)p->sell_cu & 15u)) return false;
   const bool narrow = p->max_row <= 16;
 #define FEMK_BULK_CFG(code, S, WPB)                                                          \
   case code:                                                                                 \
@@ -689,15 +722,10 @@ bool launch_step32_bulk(const femk_plan* p, const float* pv, float* q, MixedStat
                   : launch_step32_bulk_cfg<S, WPB, 32>(p, pv, q, st, s, prime);
   switch (p->bulk32_cfg) {
     FEMK_BULK_CFG(12, 1, 2)
-    FEMK_BULK_CFG(14, 1, 4)
     FEMK_BULK_CFG(22, 2, 2)
     FEMK_BULK_CFG(24, 2, 4)
     FEMK_BULK_CFG(28, 2, 8)
     FEMK_BULK_CFG(34, 3, 4)
-    FEMK_BULK_CFG(38, 3, 8)
-    FEMK_BULK_CFG(44, 4, 4)
-    FEMK_BULK_CFG(42, 4, 2)
-    FEMK_BULK_CFG(62, 6, 2)
     default:
       return false;
   }
@@ -759,10 +787,12 @@ int enqueue_mixed_chunk(const femk_plan* p, const double* vals, const double* b,
   for (int it = 0; it < kChunk; ++it) {
     launch_step32(p, m.pv, m.q, m.st, s);
     if (p->cg_split) {
-      (void)launch_ex(p->pdl != 0, k_update32_r, wave_grid(k_update32_r, kThreads, p), kThreads, 0, s, n, m.r,
-                      (const float*)m.q, (const float*)m.d32, p->partials, m.st);
-      (void)launch_ex(p->pdl != 0, k_pupdate32_x, wave_grid(k_pupdate32_x, kThreads, p), kThreads, 0, s, n, m.e,
-                      m.pv, (const float*)m.r, (const float*)m.d32, (const MixedState*)m.st);
+      auto ku = p->l2_mode32 != 0 ? k_update32_r<true> : k_update32_r<false>;
+      auto kp = p->l2_mode32 != 0 ? k_pupdate32_x<true> : k_pupdate32_x<false>;
+      (void)launch_ex(p->pdl != 0, ku, wave_grid(ku, kThreads, p), kThreads, 0, s, n, m.r, (const float*)m.q,
+                      (const float*)m.d32, p->partials, m.st);
+      (void)launch_ex(p->pdl != 0, kp, wave_grid(kp, kThreads, p), kThreads, 0, s, n, m.e, m.pv, (const float*)m.r,
+                      (const float*)m.d32, (const MixedState*)m.st);
     } else {
       k_update32<<<::femk::counted_launch() + wave_grid(k_update32, kThreads, p), kThreads, 0, s>>>(
           n, m.e, m.r, m.z, m.pv, m.q, m.d32, p->partials, m.st);
@@ -819,8 +849,10 @@ int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double
   (void)wave_grid(k_step32_sell<int32_t, 16>, kThreads, p);
   (void)launch_step32_bulk(p, nullptr, nullptr, nullptr, nullptr, true);
   (void)wave_grid(k_update32, kThreads, p);
-  (void)wave_grid(k_update32_r, kThreads, p);
-  (void)wave_grid(k_pupdate32_x, kThreads, p);
+  (void)wave_grid(k_update32_r<true>, kThreads, p);
+  (void)wave_grid(k_update32_r<false>, kThreads, p);
+  (void)wave_grid(k_pupdate32_x<true>, kThreads, p);
+  (void)wave_grid(k_pupdate32_x<false>, kThreads, p);
   (void)wave_grid(k_pupdate32<0>, 256, p);
   (void)wave_grid(k_pupdate32<1>, 256, p);
   (void)wave_grid(k_fold, 256, p);

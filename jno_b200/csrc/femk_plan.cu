@@ -377,6 +377,8 @@ int build_incidence(const int32_t* cells, int64_t ntet, int64_t n, int32_t** ptr
   return FEMK_OK;
 }
 
+int build_uniform_columns(femk_plan* p, cudaStream_t s);
+
 template <int ND>
 int build_pattern(femk_plan* p, int* d_err, int* h_err, cudaStream_t s) {
   const int64_t n = p->n;
@@ -449,6 +451,64 @@ int build_pattern(femk_plan* p, int* d_err, int* h_err, cudaStream_t s) {
   if (p->cols16) FEMK_TRY(dev_alloc(&p->sell_c16, p->sell_nnz, s));
   k_sell_fill<<<::femk::counted_launch() + sgrid, kThreads, 0, s>>>(p->indptr, p->indices, n, p->n_slices, p->sell_ptr,
                                                                     p->sell_src, p->sell_cols, p->sell_c16);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  return build_uniform_columns(p, s);
+}
+
+// Per-slice column table of the bulk-copy SpMV: a slice whose 32 rows share one column-offset
+// sequence (every row of an interior stretch of a structured mesh line) stores it once
+// (w offsets, padded to 8 = 16 bytes); any other slice keeps its 32*w per-entry offsets.
+// len[s] = entries of slice s's table; the table of slice s starts at cptr[s] (a multiple of 8).
+__global__ void k_sell_uni_len(const int64_t* __restrict__ sptr, const int16_t* __restrict__ c16, int64_t nslices,
+                               int64_t* __restrict__ len) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t sl = warp; sl < nslices; sl += nwarps) {
+    const int64_t b0 = sptr[sl];
+    const int64_t w = (sptr[sl + 1] - b0) / 32;
+    bool uni = true;
+    for (int64_t k = 0; k < w && uni; ++k) {
+      const int16_t c = c16[b0 + 32 * k + lane];
+      uni = __all_sync(0xffffffffu, c == __shfl_sync(0xffffffffu, c, 0));
+    }
+    if (lane == 0) len[sl] = uni ? (w + 7) / 8 * 8 : 32 * w;
+  }
+}
+
+__global__ void k_sell_uni_fill(const int64_t* __restrict__ sptr, const int16_t* __restrict__ c16, int64_t nslices,
+                                const int64_t* __restrict__ cptr, int16_t* __restrict__ cu) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t sl = warp; sl < nslices; sl += nwarps) {
+    const int64_t b0 = sptr[sl];
+    const int64_t w = (sptr[sl + 1] - b0) / 32;
+    const int64_t c0 = cptr[sl], len = cptr[sl + 1] - c0;
+    if (len == 32 * w) {
+      for (int64_t j = lane; j < len; j += 32) cu[c0 + j] = c16[b0 + j];
+    } else {
+      for (int64_t k = lane; k < len; k += 32) cu[c0 + k] = k < w ? c16[b0 + 32 * k] : (int16_t)0;
+    }
+  }
+}
+
+int build_uniform_columns(femk_plan* p, cudaStream_t s) {
+  if (!p->sell_c16 || !p->sell_uni) return FEMK_OK;
+  Temp len;
+  FEMK_CUDA_TRY(cudaMalloc(&len.p, sizeof(int64_t) * (p->n_slices + 1)));
+  FEMK_TRY(dev_alloc(&p->sell_cuptr, p->n_slices + 1, s));
+  const int sgrid = blocks_for(p->n_slices * 32, kThreads, p->n_sm * 64);
+  k_sell_uni_len<<<::femk::counted_launch() + sgrid, kThreads, 0, s>>>(p->sell_ptr, p->sell_c16, p->n_slices,
+                                                                       (int64_t*)len.p);
+  FEMK_TRY(scan_exclusive_i64((const int64_t*)len.p, p->sell_cuptr, p->n_slices, s));
+  FEMK_CUDA_TRY(cudaMemcpyAsync(&p->sell_cu_len, p->sell_cuptr + p->n_slices, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                s));
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  FEMK_TRY(dev_alloc(&p->sell_cu, p->sell_cu_len, s));
+  k_sell_uni_fill<<<::femk::counted_launch() + sgrid, kThreads, 0, s>>>(p->sell_ptr, p->sell_c16, p->n_slices,
+                                                                        p->sell_cuptr, p->sell_cu);
   FEMK_CUDA_TRY(cudaGetLastError());
   FEMK_CUDA_TRY(cudaStreamSynchronize(s));
   return FEMK_OK;
@@ -580,7 +640,7 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
                   p->diag,     p->dmask,     p->dlist,     p->inc_ptr,   p->inc_elem,  p->cols16,
                   p->work,     p->partials,  p->state,     p->work32,    p->vals32,    p->work64b,
                   p->sell_ptr, p->sell_src,  p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32,
-                  p->bar,      p->batch_ws,  p->bicg_ws,   p->bicg_state};
+                  p->bar,      p->batch_ws,  p->bicg_ws,   p->bicg_state, p->sell_cuptr, p->sell_cu};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->state_host) cudaFreeHost(p->state_host);
@@ -638,6 +698,9 @@ extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int3
   if (const char* e = std::getenv("FEMK_BULK")) p->bulk_cfg = std::atoi(e);
   if (const char* e = std::getenv("FEMK_BULK32")) p->bulk32_cfg = std::atoi(e);
   if (const char* e = std::getenv("FEMK_PDL")) p->pdl = std::atoi(e) != 0;
+  if (const char* e = std::getenv("FEMK_SELL_UNI")) p->sell_uni = std::atoi(e) != 0;
+  p->l2_mode32 = p->l2_mode != 0;
+  if (const char* e = std::getenv("FEMK_L2HINT32")) p->l2_mode32 = std::atoi(e) != 0;
   cudaDeviceGetAttribute(&p->coop, cudaDevAttrCooperativeLaunch, p->device);
   p->nvert = nvert;
   p->ntet = ntet;
@@ -664,6 +727,7 @@ extern "C" int femk_plan_get_info(const femk_plan* p, femk_plan_info* out) {
   out->sell_nnz = p->sell_src ? p->sell_nnz : 0;
   out->batch_graph = p->batch_graph_used;
   out->pad = 0;
+  out->sell_col_units = p->sell_cu ? p->sell_cu_len : (p->sell_src ? p->sell_nnz : 0);
   return FEMK_OK;
 }
 

@@ -84,11 +84,15 @@ class FEM:
             raise KeyError(f"missing runtime parameter {name!r}")
         v = args[name]
         if isinstance(v, (int, float)):
-            return torch.full((self.plan.ntet,), float(v), dtype=torch.float64, device=self.plan.device)
+            nodal = self.form.mode in (_lib.COEF_NODAL_EXP, _lib.COEF_NODAL_LINEAR)
+            size = self.plan.nvert if nodal else self.plan.ntet
+            return torch.full((size,), float(v), dtype=torch.float64, device=self.plan.device)
         t = v if isinstance(v, torch.Tensor) else torch.as_tensor(np.asarray(v))
         t = t.to(device=self.plan.device, dtype=torch.float64).reshape(-1).contiguous()
-        if t.numel() != self.plan.ntet:
-            raise ValueError(f"parameter {name!r} is P0: it needs {self.plan.ntet} values, got {t.numel()}")
+        nodal = self.form.mode in (_lib.COEF_NODAL_EXP, _lib.COEF_NODAL_LINEAR)
+        want, kind = (self.plan.nvert, "nodal P1") if nodal else (self.plan.ntet, "P0")
+        if t.numel() != want:
+            raise ValueError(f"parameter {name!r} is {kind}: it needs {want} values, got {t.numel()}")
         return t
 
     def _assemble(self, args):

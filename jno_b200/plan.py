@@ -68,6 +68,7 @@ class FemPlan:
         self.n_dirichlet = info.n_dirichlet
         self.cols16 = bool(info.cols16)
         self.sell_nnz = int(info.sell_nnz)
+        self.sell_col_units = int(info.sell_col_units)
         self.device = torch.device("cuda", info.device)
         self._pattern = None
 
@@ -120,8 +121,10 @@ class FemPlan:
         """(vals f64[nnz], b f64[n]) of ``k_e grad u . grad v - f v`` with Dirichlet ``u = g``."""
         if mode != _lib.COEF_CONST:
             param = _device_tensor(param, torch.float64)
-            if param.numel() != self.ntet:
-                raise ValueError(f"a P0 parameter needs {self.ntet} values, got {param.numel()}")
+            want = self.nvert if mode in (_lib.COEF_NODAL_EXP, _lib.COEF_NODAL_LINEAR) else self.ntet
+            if param.numel() != want:
+                kind = "nodal P1" if want == self.nvert else "P0"
+                raise ValueError(f"a {kind} parameter needs {want} values, got {param.numel()}")
         g = None if g is None else _device_tensor(g, torch.float64)
         vals = torch.empty(self.nnz, dtype=torch.float64, device=self.device) if vals is None else vals
         b = torch.empty(self.n, dtype=torch.float64, device=self.device) if b is None else b

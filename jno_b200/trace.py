@@ -4,9 +4,10 @@ It mirrors the reference's DSL surface for this path only (``d.fem_symbols``, ``
 ``jno.np.exp``, ``jno.np.parameter``, ``u(xb, yb, zb) - g``; jno/trace/__init__.py,
 jno/architectures/models.py:58-142) and classifies a form into the kernel arguments:
 
-    coef * (ui.x*vi.x + ui.y*vi.y + ui.z*vi.z) - f * vi,   coef in {c, c*p, c*exp(p)}, p a P0 parameter
+    coef * (ui.x*vi.x + ui.y*vi.y + ui.z*vi.z) - f * vi,   coef in {c, c*p, c*exp(p)}
 
-Anything else raises ``NotImplementedError``: other physics is outside this path.
+with p a P0 parameter (one value per element) or, in P1 forms, a nodal P1 parameter (one value per
+vertex). Anything else raises ``NotImplementedError``: other physics is outside this path.
 """
 
 import numbers
@@ -122,16 +123,22 @@ class TraceOn(Expr):
 
 
 class Param(Expr):
-    """``jno.np.parameter(<P0 symbol>, name=...)``: one value per element (models.py:92-107)."""
+    """``jno.np.parameter(<symbol>, name=...)`` (jno/architectures/models.py:85-117): one value per
+    element for a P0 symbol, one value per P1 vertex (``nodal``) for a P1 symbol."""
 
-    def __init__(self, sym, name):
-        self.sym, self.name = sym, name
+    def __init__(self, sym, name, nodal=False):
+        self.sym, self.name, self.nodal = sym, name, nodal
 
 
 def parameter(sym, name="param", **_):
-    if not isinstance(sym, FieldSymbol) or sym.space != "P0":
-        raise NotImplementedError("only P0 (per-element) field parameters are on the B200 path")
-    return Param(sym, name)
+    if not isinstance(sym, FieldSymbol):
+        raise NotImplementedError("jno.np.parameter takes a field symbol on the B200 path")
+    if sym.space == "P0":
+        return Param(sym, name)
+    if sym.order != 1:
+        # the reference raises the same way for higher-order symbols (models.py:109-113)
+        raise NotImplementedError("nodal field parameters support P1 (order=1) symbols only")
+    return Param(sym, name, nodal=True)
 
 
 def exp(a):
@@ -163,13 +170,13 @@ def _coef_key(factors):
     exps = [f for f in factors if isinstance(f, Exp)]
     other = [f for f in factors if not isinstance(f, (Param, Exp))]
     if other:
-        raise NotImplementedError("a spatially varying coefficient is outside the B200 path (P0 parameters only)")
+        raise NotImplementedError("a spatially varying coefficient is outside the B200 path (parameters only)")
     if not params and not exps:
         return ("const",)
     if len(params) == 1 and not exps:
-        return ("linear", params[0].name)
+        return ("nodal_linear" if params[0].nodal else "linear", params[0].name)
     if len(exps) == 1 and not params and isinstance(exps[0].a, Param):
-        return ("exp", exps[0].a.name)
+        return ("nodal_exp" if exps[0].a.nodal else "exp", exps[0].a.name)
     raise NotImplementedError("only c, c*p and c*exp(p) coefficients are on the B200 path")
 
 
@@ -216,7 +223,10 @@ def classify_volume(expr):
     scale, key = scales.pop(), keys.pop()
     from . import _lib
 
-    mode = {"const": _lib.COEF_CONST, "linear": _lib.COEF_LINEAR, "exp": _lib.COEF_EXP}[key[0]]
+    mode = {"const": _lib.COEF_CONST, "linear": _lib.COEF_LINEAR, "exp": _lib.COEF_EXP,
+            "nodal_linear": _lib.COEF_NODAL_LINEAR, "nodal_exp": _lib.COEF_NODAL_EXP}[key[0]]
+    if key[0].startswith("nodal") and order != 1:
+        raise NotImplementedError("a nodal P1 parameter in a P2 form is outside the B200 path")
     return WeakForm(order, mode, scale, key[1] if len(key) > 1 else None, source, domain)
 
 

@@ -112,3 +112,26 @@ def element_matrices_quadrature(X, order, npts=4):
     K = np.einsum("q,t,tqaD,tqbD->tab", w, meas, dphys, dphys)
     F = np.einsum("q,t,qa->ta", w, meas, phi)
     return K, F
+
+
+# symmetric 4-point degree-2 tetrahedron rule: barycentric (b, a, a, a) and permutations, weights 1/4
+_Q4_A = (5.0 - np.sqrt(5.0)) / 20.0
+_Q4_B = (5.0 + 3.0 * np.sqrt(5.0)) / 20.0
+
+
+def nodal_coefficient(tets, values, mode):
+    """Per-element k_e of a nodal P1 parameter for P1 stiffness (whose integrand is constant per
+    element, so K_e = V G mean_q k(x_q)).
+
+    The reference passes a nodal field parameter as the cell's local nodal values
+    (``_runtime_vals``, ``jno/utils/solver/fem_native.py:1597-1630``) and interpolates them to the
+    quadrature points of the degree-2 rule P1 forms use (``jno/_fem.py:4551``); basix (which
+    supplies that rule) is absent here, so the symmetric 4-point rule is used.
+    ``mode`` "linear": k = p_h (the vertex mean, exact); "exp": k = exp(p_h) averaged over the rule.
+    """
+    p = np.asarray(values, dtype=np.float64)[np.asarray(tets)]
+    if mode == "linear":
+        return 0.25 * p.sum(axis=1)
+    lam = np.full((4, 4), _Q4_A) + np.eye(4) * (_Q4_B - _Q4_A)  # lam[q, i]
+    return 0.25 * np.exp(p @ lam.T).sum(axis=1)
+

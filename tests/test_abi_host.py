@@ -78,8 +78,15 @@ def test_form_classification():
         classify_volume(ui.x * vi.x + ui.y * vi.y)
     with pytest.raises(NotImplementedError):
         classify_volume(logk * (ui.x * vi.x) + ui.y * vi.y + ui.z * vi.z)
+    # a P1 symbol gives a nodal parameter (models.py:85-117); P2 symbols are refused like the reference
+    k = jno.np.parameter(u, name="nodal")
+    f = classify_volume(jno.np.exp(k) * (ui.x * vi.x + ui.y * vi.y + ui.z * vi.z) - 1.0 * vi)
+    assert (f.mode, f.param) == (_lib.COEF_NODAL_EXP, "nodal")
+    f = classify_volume(k * (ui.x * vi.x + ui.y * vi.y + ui.z * vi.z))
+    assert f.mode == _lib.COEF_NODAL_LINEAR
+    u2, _ = d.fem_symbols(order=2)
     with pytest.raises(NotImplementedError):
-        jno.np.parameter(u, name="nodal")
+        jno.np.parameter(u2, name="p2")
 
 
 def test_product_has_no_cpu_fallback():

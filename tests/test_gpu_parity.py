@@ -407,7 +407,9 @@ def test_bicgstab_matches_oracle(n, order, bulk, monkeypatch):
     A = s.csr()
     xo, ko = op.bicgstab(A, s.b, oa.jacobi_inverse(oa.matrix_diagonal(s)), tol=1e-8)
     assert st == 0 and ko > 0
-    assert abs(it - ko) <= 2, (it, ko)
+    # BiCGStab's iteration count moves with the summation order of its dot products (the grid shape
+    # of the reductions); the contract is the stop rule and the solution
+    assert abs(it - ko) <= max(2, ko // 10), (it, ko)
     uu = u.cpu().numpy()
     assert np.linalg.norm(uu - xo) <= 1e-7 * np.linalg.norm(xo)
     assert abs(rel - op.residual_check(A, s.b, uu)) <= 1e-12
@@ -437,3 +439,75 @@ def test_bicgstab_status_paths():
 
     with pytest.raises(RuntimeError, match="jno.solve.bicgstab did not solve"):
         jno.solve.bicgstab(maxiter=1)(CsrMatrix(plan, vals), b, M=jno.precond.jacobi())
+
+
+def test_column_tables_give_bit_identical_solves(monkeypatch):
+    """The bulk-copy SpMV reads shared-offset slices from per-slice column tables; rows sum in the
+    same order either way, so FP64 and mixed solves are bit-identical with and without the tables
+    (64^3 hexes: z-lines of 65 rows, so many 32-row slices lie inside one line's interior)."""
+    pf, cf, tets, p1 = _mesh(64, 1)
+    lk = torch.as_tensor(om.logk_field(len(tets), 1006), device="cuda")
+    out = {}
+    vals = b = inv = None
+    for uni in ("1", "0"):
+        monkeypatch.setenv("FEMK_SELL_UNI", uni)
+        plan = _plan(p1, tets, 1)
+        if uni == "1":
+            assert plan.sell_col_units < 0.7 * plan.sell_nnz  # about half the slices share their offsets
+            # one assembly for both plans (same pattern): the FP64 atomics of two assemblies may
+            # round differently in the last bit
+            vals, b = plan.assemble(lk)
+            inv = plan.jacobi(vals)
+        else:
+            assert plan.sell_col_units == plan.sell_nnz
+        u, it, rel, st = plan.pcg(vals, b, inv_diag=inv, tol=1e-8)
+        um, inner, outer, relm, stm = plan.pcg_mixed(vals, b, inv, tol=1e-8)
+        ub, itb, relb, stb = plan.bicgstab(vals, b, inv_diag=inv, tol=1e-8)
+        assert st == 0 and stm == 0 and stb == 0 and rel <= 2e-8 and relm <= 1e-8 and relb <= 2e-8
+        out[uni] = (u, it, um, inner, ub, itb)
+    a, c = out["1"], out["0"]
+    assert a[1] == c[1] and torch.equal(a[0], c[0])
+    assert a[3] == c[3] and torch.equal(a[2], c[2])
+    assert a[5] == c[5] and torch.equal(a[4], c[4])
+
+
+@pytest.mark.parametrize("mode", ["exp", "linear"])
+def test_nodal_p1_parameter_matches_oracle(mode):
+    """A nodal P1 coefficient (jno.np.parameter of a P1 symbol) through assembly, the matrix-free
+    operator and the jno surface."""
+    from jno_b200 import _lib
+
+    n = 6
+    pf, cf, tets, p1 = _mesh(n, 1)
+    rng = np.random.default_rng(11)
+    nodal = rng.normal(0.0, 0.5, p1.shape[0]) if mode == "exp" else rng.uniform(0.5, 2.0, p1.shape[0])
+    cmode = _lib.COEF_NODAL_EXP if mode == "exp" else _lib.COEF_NODAL_LINEAR
+    plan = _plan(p1, tets, 1)
+    pv = torch.as_tensor(nodal, device="cuda")
+    vals, b = plan.assemble(pv, mode=cmode)
+    ke = oe.nodal_coefficient(tets, nodal, mode)
+    bnd = om.boundary_nodes(cf, 1)
+    s = oa.assemble(pf, cf, 1, bnd, ke)
+    assert np.abs(vals.cpu().numpy() - s.data).max() <= VAL_TOL * np.abs(s.data).max()
+    xv = torch.as_tensor(rng.standard_normal(plan.n), device="cuda")
+    ym = plan.spmv_matfree(pv, xv, mode=cmode).cpu().numpy()
+    yo = s.csr() @ xv.cpu().numpy()
+    assert np.abs(ym - yo).max() <= 1e-12 * np.abs(yo).max()
+    # the jno surface: parameter(<P1 symbol>) is nodal
+    import jno_b200 as jno
+
+    d = jno.domain(jno.domain.equi_distant_box(nx=n, ny=n, nz=n), jitter=0.1, seed=0)
+    u, v = d.fem_symbols()
+    kf, _ = d.fem_symbols(names=("k", "kt"))
+    xi, yi, zi = d.variable("interior", split=True)
+    xb, yb, zb = d.variable("boundary", split=True)
+    ui, vi = u.bind(x=xi, y=yi, z=zi), v.bind(x=xi, y=yi, z=zi)
+    k = jno.np.parameter(kf, name="k")
+    coef = jno.np.exp(k) if mode == "exp" else k
+    fem = jno.fem([coef * (ui.x * vi.x + ui.y * vi.y + ui.z * vi.z) - 1.0 * vi, u(xb, yb, zb) - 0.0])
+    A, bb = fem.operator.evaluate({"k": nodal})
+    x = jno.solve.cg(tol=1e-10)(A, bb, M=jno.precond.jacobi())
+    xo = op.pcg(s.csr(), s.b, oa.jacobi_inverse(oa.matrix_diagonal(s)), tol=1e-10)[0]
+    assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-8 * np.linalg.norm(xo)
+    with pytest.raises(ValueError):
+        fem.operator.evaluate({"k": np.zeros(len(tets))})  # P0-sized input for a nodal parameter

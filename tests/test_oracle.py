@@ -185,3 +185,22 @@ def test_bicgstab_matches_direct_and_stops_like_jax():
     assert k0 == 0 and np.all(x0 == 0)
     _, k1 = op.bicgstab(A, s.b, inv, maxiter=1)
     assert k1 == 1
+
+
+def test_nodal_coefficient_rule():
+    """The 4-point rule integrates degree-2 polynomials exactly; a linear nodal field's element
+    mean is its vertex mean; a constant log-field gives exp of it."""
+    pts, tets = om.equi_distant_box(2, 2, 2)
+    rng = np.random.default_rng(9)
+    vals = rng.normal(size=pts.shape[0])
+    lin = oe.nodal_coefficient(tets, vals, "linear")
+    assert np.allclose(lin, vals[tets].mean(axis=1), rtol=0, atol=1e-15)
+    assert np.allclose(oe.nodal_coefficient(tets, np.full(pts.shape[0], 0.3), "exp"), np.exp(0.3), rtol=1e-15)
+    # the rule against a collapsed-Gauss rule on a quadratic in barycentric coordinates
+    xi, w = oe._collapsed_gauss(6)
+    lam = np.column_stack([1.0 - xi.sum(axis=1), xi])
+    f = lam[:, 0] * lam[:, 1] + 0.5 * lam[:, 2] ** 2 + lam[:, 3]
+    exact = (w * f).sum() * 6.0  # mean over the unit tet (volume 1/6)
+    lamq = np.full((4, 4), oe._Q4_A) + np.eye(4) * (oe._Q4_B - oe._Q4_A)
+    fq = lamq[:, 0] * lamq[:, 1] + 0.5 * lamq[:, 2] ** 2 + lamq[:, 3]
+    assert abs(fq.mean() - exact) <= 1e-14
