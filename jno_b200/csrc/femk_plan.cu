@@ -692,14 +692,16 @@ extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int3
   if (const char* e = std::getenv("FEMK_CG_PERSIST")) p->cg_persist = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_CG_SPLIT")) p->cg_split = std::atoi(e) != 0;
   // bulk-copy SpMV configurations, measured on B200 at P1 128^3 (to 1e-8): FP64 2 stages x 4 warps
-  // (39.9 ms/step vs 45.8 ms register-streamed), FP32 2 stages x 8 warps (29.7 vs 32.5 ms)
+  // (39.9-40.7 ms/step vs 45.8 ms register-streamed), FP32 2 stages x 8 warps (29.7-31.7 vs 32.5 ms)
   p->bulk_cfg = 24;
   p->bulk32_cfg = 28;
   if (const char* e = std::getenv("FEMK_BULK")) p->bulk_cfg = std::atoi(e);
   if (const char* e = std::getenv("FEMK_BULK32")) p->bulk32_cfg = std::atoi(e);
   if (const char* e = std::getenv("FEMK_PDL")) p->pdl = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_SELL_UNI")) p->sell_uni = std::atoi(e) != 0;
-  p->l2_mode32 = p->l2_mode != 0;
+  // FP32 kernels stream without hints: measured on B200 at P1 128^3, mixed solve 31.7 ms without
+  // vs 32.8 ms with evict-last vectors and gathers
+  p->l2_mode32 = 0;
   if (const char* e = std::getenv("FEMK_L2HINT32")) p->l2_mode32 = std::atoi(e) != 0;
   cudaDeviceGetAttribute(&p->coop, cudaDevAttrCooperativeLaunch, p->device);
   p->nvert = nvert;
