@@ -57,7 +57,7 @@ typedef struct femk_plan_info {
   int32_t device;
   int64_t sell_nnz;   /* stored entries of the solver's sliced-ELL copy (padding included), 0 if none */
   int32_t batch_graph; /* 1 when the last femk_pcg_batched ran as a replayed CUDA graph */
-  int32_t pad;
+  int32_t tiles;       /* 1 when the plan built the staged-x tiles of the CG-step SpMV */
   int64_t sell_col_units; /* column entries the CG-step SpMV streams per product (int16 units when
                              cols16: per-slice tables, a shared-offset slice stored once) */
 } femk_plan_info;

@@ -56,7 +56,7 @@ class PlanInfo(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("sell_nnz", ctypes.c_int64),
         ("batch_graph", ctypes.c_int32),
-        ("pad", ctypes.c_int32),
+        ("tiles", ctypes.c_int32),
         ("sell_col_units", ctypes.c_int64),
     ]
 

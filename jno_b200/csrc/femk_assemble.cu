@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(kThreads) k_assemble(const double* __restrict_
     tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
     double VG[4][4];
     gram(T, VG);
-    const double k = coef_any(param, mode, scale, c, dof);
+    const double k = coef_of(param, mode, scale, c);
     bool dir[ND];
 #pragma unroll
     for (int a = 0; a < ND; ++a) dir[a] = __ldg(dmask + dof[a]) != 0;
@@ -52,6 +52,15 @@ __global__ void __launch_bounds__(kThreads) k_assemble(const double* __restrict_
       atomicAdd(b + dof[a], rhs);
     }
   }
+}
+
+// k_e of a nodal P1 parameter (coef_nodal, unscaled) for every element: the kernels that take a
+// coefficient then read it as a P0 linear parameter (FEMK_COEF_LINEAR with the caller's scale)
+__global__ void k_nodal_coef(const int32_t* __restrict__ cells, int nd, int64_t ntet, const double* __restrict__ param,
+                             int mode, double* __restrict__ ke) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x)
+    ke[c] = coef_nodal(param, mode, 1.0, __ldg(cells + c * nd), __ldg(cells + c * nd + 1), __ldg(cells + c * nd + 2),
+                       __ldg(cells + c * nd + 3));
 }
 
 __global__ void k_dirichlet_rows(const int32_t* __restrict__ dlist, int64_t nd, const int32_t* __restrict__ diag,
@@ -134,6 +143,25 @@ __global__ void k_adjoint(const double* __restrict__ xyz, const int32_t* __restr
 }  // namespace
 }  // namespace femk
 
+namespace femk {
+
+int resolve_coef(const femk_plan* pc, const double* param, int mode, cudaStream_t s, const double** param_out,
+                 int* mode_out) {
+  *param_out = param;
+  *mode_out = mode;
+  if (mode != FEMK_COEF_NODAL_EXP && mode != FEMK_COEF_NODAL_LINEAR) return FEMK_OK;
+  femk_plan* p = const_cast<femk_plan*>(pc);
+  if (!p->coef_tmp) FEMK_CUDA_TRY(cudaMalloc(&p->coef_tmp, sizeof(double) * (p->ntet > 0 ? p->ntet : 1)));
+  k_nodal_coef<<<counted_launch() + blocks_for(p->ntet, 256, p->n_sm * 16), 256, 0, s>>>(p->cells, p->nd, p->ntet,
+                                                                                       param, mode, p->coef_tmp);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  *param_out = p->coef_tmp;
+  *mode_out = FEMK_COEF_LINEAR;
+  return FEMK_OK;
+}
+
+}  // namespace femk
+
 using namespace femk;
 
 extern "C" int femk_assemble(const femk_plan* p, const double* param, int mode, double scale, double f,
@@ -143,6 +171,7 @@ extern "C" int femk_assemble(const femk_plan* p, const double* param, int mode, 
   FEMK_CHECK_ARG(coef_mode_ok(p, mode, param),
                  "femk_assemble: unknown coef_mode, NULL param, or a nodal mode on a P2 plan");
   cudaStream_t s = (cudaStream_t)stream;
+  FEMK_TRY(resolve_coef(p, param, mode, s, &param, &mode));
   if (vals) FEMK_CUDA_TRY(cudaMemsetAsync(vals, 0, sizeof(double) * p->nnz, s));
   FEMK_CUDA_TRY(cudaMemsetAsync(b, 0, sizeof(double) * p->n, s));
   const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);

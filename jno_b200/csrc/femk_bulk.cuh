@@ -56,14 +56,38 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return done != 0;
 }
 
+// try_wait that lets the hardware suspend the thread until the phase completes (or the hint, in
+// nanoseconds, elapses) instead of returning at once: waiting warps stop taking issue slots
+__device__ __forceinline__ bool mbar_try_wait_suspend(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred P;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2, %3;\n\t"
+      "selp.b32 %0, 1, 0, P;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(1000000u)
+      : "memory");
+  return done != 0;
+}
+
 // bounded wait for the phase with the given parity to complete; false on timeout
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity)) {
+  while (!mbar_try_wait_suspend(bar, parity)) {
     if (clock64() - t0 > kBulkSpinCycles) return false;
   }
   return true;
+}
+
+// Warp-wide wait: lane 0 waits (bounded), then every lane observes the completed phase once (its
+// own acquire of the bulk-copy writes). Returns the same outcome in every lane.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity) {
+  bool ok = true;
+  if ((threadIdx.x & 31) == 0) ok = mbar_wait(bar, parity);
+  ok = __shfl_sync(0xffffffffu, ok, 0);
+  if (ok) ok = mbar_try_wait(bar, parity);
+  return __all_sync(0xffffffffu, ok);
 }
 
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar, uint64_t pol) {
@@ -71,6 +95,12 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
       ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
       : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s_plain(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
 }
 
 // Shared memory one warp needs: S stages of [32*WMAX values][32*WMAX columns] + S mbarriers + S widths.
@@ -142,8 +172,8 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
   for (int64_t sl = g; sl < nslices; sl += NW, ++i) {
     const int s = (int)(i % S);
     const uint32_t parity = (uint32_t)((i / S) & 1);
-    // warp-uniform outcome: a lane that timed out takes the whole warp out of the loop
-    if (!__all_sync(0xffffffffu, mbar_wait(bar + s, parity))) {
+    // warp-uniform outcome: a timed-out wait takes the whole warp out of the loop
+    if (!mbar_wait_warp(bar + s, parity)) {
       ok = false;
       break;
     }

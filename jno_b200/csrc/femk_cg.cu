@@ -18,6 +18,7 @@
 #include <string>
 
 #include "femk_bulk.cuh"
+#include "femk_tile.cuh"
 #include "femk_reduce.cuh"
 #include "femk_element.cuh"
 #include "femk_internal.cuh"
@@ -221,7 +222,7 @@ __global__ void __launch_bounds__(WPB * 32) k_sell_bulk(const int64_t* __restric
                                                        double* __restrict__ partials, CgState* st, int* err,
                                                        const int64_t* __restrict__ cptr) {
   extern __shared__ __align__(128) unsigned char bulk_smem[];
-  using R = BulkRing<double, IDX, WMAX, S>;
+  constexpr int kWarpBytes = BulkRing<double, IDX, WMAX, S>::kWarpBytes;
   pdl_wait();
   pdl_trigger();
   if (MODE == kCgStep) {
@@ -234,7 +235,7 @@ __global__ void __launch_bounds__(WPB * 32) k_sell_bulk(const int64_t* __restric
   double acc[1] = {0.0};
   int* errp = MODE == kCgStep ? &st->status : err;
   const bool ok = sell_bulk_rows<double, IDX, WMAX, S>(
-      bulk_smem + wib * R::kWarpBytes, sptr, scols, svals, n, nslices, g, NW, GatherXL<double>{x, l2_evict_last()},
+      bulk_smem + wib * kWarpBytes, sptr, scols, svals, n, nslices, g, NW, GatherXL<double>{x, l2_evict_last()},
       [&](int64_t row, double sv) {
         y[row] = sv;
         if (MODE == kCgStep) acc[0] += __ldg(x + row) * sv;
@@ -245,6 +246,43 @@ __global__ void __launch_bounds__(WPB * 32) k_sell_bulk(const int64_t* __restric
   block_reduce_store<1, WPB * 32>(acc, partials);
   double tot[1];
   if (!grid_finish<1, WPB * 32>(partials, &st->ticket, tot)) return;
+  if (threadIdx.x != 0) return;
+  st->pq = tot[0];
+  st->alpha = st->gamma / tot[0];
+  if (!isfinite(tot[0])) {
+    st->status = FEMK_NONFINITE;
+    st->done = 1;
+  } else if (!(tot[0] > 0.0)) {
+    st->status = FEMK_BREAKDOWN;
+    st->done = 1;
+  }
+}
+
+// The CG-step SpMV with matrix and x staged per tile in shared memory (femk_tile.cuh).
+template <int WMAX>
+__global__ void __launch_bounds__(kTileW * 32) k_sell_tile(const TileMeta* __restrict__ meta, int64_t ntiles,
+                                                          int xcap, const int64_t* __restrict__ sptr,
+                                                          const int64_t* __restrict__ cptr,
+                                                          const int16_t* __restrict__ slots,
+                                                          const double* __restrict__ svals, int64_t n,
+                                                          int64_t nslices, const double* __restrict__ x,
+                                                          double* __restrict__ y, double* __restrict__ partials,
+                                                          CgState* st) {
+  extern __shared__ __align__(128) unsigned char tile_smem[];
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->xpend = 0;  // the last x update is applied
+  if (st->done) return;
+  double acc[1] = {0.0};
+  const bool ok = sell_tile_rows<double, kTileW, WMAX>(
+      tile_smem, xcap, meta, ntiles, sptr, cptr, slots, svals, x, n, nslices,
+      [&](int64_t row, double sv, double xrow) {
+        y[row] = sv;
+        acc[0] += xrow * sv;
+      },
+      &st->status, FEMK_TIMEOUT);
+  if (!ok && threadIdx.x == 0) st->done = 1;
+  block_reduce_store<1, kTileW * 32>(acc, partials);
+  double tot[1];
+  if (!grid_finish<1, kTileW * 32>(partials, &st->ticket, tot)) return;
   if (threadIdx.x != 0) return;
   st->pq = tot[0];
   st->alpha = st->gamma / tot[0];
@@ -687,7 +725,7 @@ __global__ void __launch_bounds__(128) k_matfree(const double* __restrict__ xyz,
     tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
     double VG[4][4];
     gram(T, VG);
-    const double k = coef_any(param, mode, scale, c, dof);
+    const double k = coef_of(param, mode, scale, c);
 #pragma unroll
     for (int a = 0; a < ND; ++a) {
       if (dir[a]) continue;
@@ -720,7 +758,7 @@ __global__ void k_matfree_diag(const double* __restrict__ xyz, const int32_t* __
     tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
     double VG[4][4];
     gram(T, VG);
-    const double k = coef_any(param, mode, scale, c, dof);
+    const double k = coef_of(param, mode, scale, c);
 #pragma unroll
     for (int a = 0; a < ND; ++a)
       if (!__ldg(dmask + dof[a])) atomicAdd(d + dof[a], k * khat<ND>(VG, a, a));
@@ -915,9 +953,42 @@ bool launch_sell_bulk_cfg(const femk_plan* p, const double* x, double* y, CgStat
   return true;
 }
 
+// Staged-x CG-step SpMV when the plan built its tiles (tile_ok); false: nothing launched.
+template <int WMAX>
+bool launch_sell_tile_w(const femk_plan* p, const double* x, double* y, CgState* st, cudaStream_t s, bool prime) {
+  auto kern = k_sell_tile<WMAX>;
+  static int attr_ok = -1;  // per instantiation: opt in to the largest stage size once
+  if (attr_ok < 0) {
+    const int most = 2 * TileStage<double, kTileW, WMAX>::bytes(4096) + 16;
+    attr_ok = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, most) == cudaSuccess;
+    if (!attr_ok) cudaGetLastError();
+  }
+  if (!attr_ok) return false;
+  const int smem = 2 * TileStage<double, kTileW, WMAX>::bytes(p->tile_xcap) + 16;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileW * 32, smem) != cudaSuccess || per_sm <= 0) {
+    cudaGetLastError();
+    return false;
+  }
+  if (prime) return true;
+  const int grid = (int)std::min<int64_t>(p->ntiles, (int64_t)p->n_sm * std::min(per_sm, 16));
+  kern<<<::femk::counted_launch() + grid, kTileW * 32, smem, s>>>(
+      (const TileMeta*)p->tile_meta, p->ntiles, p->tile_xcap, p->sell_ptr, p->sell_cuptr, p->tile_slots,
+      p->sell_vals, p->n, p->n_slices, x, y, p->partials, st);
+  return true;
+}
+
+bool launch_sell_tile(const femk_plan* p, const double* x, double* y, CgState* st, cudaStream_t s, bool prime) {
+  if (!p->tile_ok || !p->tile64 || !p->sell_vals || ((uintptr_t)p->sell_vals & 15u) || ((uintptr_t)x & 15u))
+    return false;
+  return p->max_row <= 16 ? launch_sell_tile_w<16>(p, x, y, st, s, prime)
+                          : launch_sell_tile_w<32>(p, x, y, st, s, prime);
+}
+
 // prime = true only sets the kernel attribute and reads the occupancy (before a graph capture)
 bool launch_sell_bulk(const femk_plan* p, const double* x, double* y, CgState* st, cudaStream_t s,
                       bool prime = false) {
+  if (launch_sell_tile(p, x, y, st, s, prime)) return true;
   if (!p->bulk_cfg || !p->sell_c16 || !p->sell64_c16 || p->max_row > 32) return false;
   if (!aligned16(p->sell_vals) || !aligned16(p->sell_c16)) return false;  // bulk copies start on 16 B
   if (p->sell_cu && !aligned16(p->sell_cu)) return false;
@@ -1405,6 +1476,7 @@ extern "C" int femk_spmv_matfree(const femk_plan* p, const double* param, int mo
   clear_error();
   FEMK_CHECK_ARG(p && x && y, "femk_spmv_matfree: NULL argument");
   FEMK_CHECK_ARG(coef_mode_ok(p, mode, param), "femk_spmv_matfree: bad coefficient");
+  FEMK_TRY(resolve_coef(p, param, mode, (cudaStream_t)stream, &param, &mode));
   MatFree m{param, mode, scale};
   return launch_matfree(p, m, x, y, (cudaStream_t)stream);
 }
@@ -1415,6 +1487,7 @@ extern "C" int femk_jacobi_matfree(const femk_plan* p, const double* param, int 
   FEMK_CHECK_ARG(p && inv, "femk_jacobi_matfree: NULL argument");
   FEMK_CHECK_ARG(coef_mode_ok(p, mode, param), "femk_jacobi_matfree: bad coefficient");
   cudaStream_t s = (cudaStream_t)stream;
+  FEMK_TRY(resolve_coef(p, param, mode, s, &param, &mode));
   FEMK_CUDA_TRY(cudaMemsetAsync(inv, 0, sizeof(double) * p->n, s));
   const int grid = blocks_for(p->ntet, 128, p->n_sm * 16);
   if (p->nd == 4)
@@ -1441,6 +1514,7 @@ extern "C" int femk_pcg_matfree(const femk_plan* p, const double* param, int mod
   clear_error();
   FEMK_CHECK_ARG(p && b && x, "femk_pcg_matfree: NULL argument");
   FEMK_CHECK_ARG(coef_mode_ok(p, mode, param), "femk_pcg_matfree: bad coefficient");
+  FEMK_TRY(resolve_coef(p, param, mode, (cudaStream_t)stream, &param, &mode));
   MatFree m{param, mode, scale};
   return pcg_run(p, nullptr, &m, b, x, dinv, tol, atol, maxiter, iters_out, relres_out, (cudaStream_t)stream);
 }

@@ -112,11 +112,4 @@ __device__ __forceinline__ double coef_nodal(const double* __restrict__ param, i
   return scale * (0.25 * e);
 }
 
-// the element coefficient for any FEMK_COEF_* mode; dof[0..3] are the element's vertex DOFs
-__device__ __forceinline__ double coef_any(const double* __restrict__ param, int mode, double scale, int64_t c,
-                                           const int32_t* dof) {
-  if (mode >= FEMK_COEF_NODAL_EXP) return coef_nodal(param, mode, scale, dof[0], dof[1], dof[2], dof[3]);
-  return coef_of(param, mode, scale, c);
-}
-
 }  // namespace femk

@@ -12,6 +12,8 @@
 
 namespace femk {
 
+constexpr int kTileW = 4;  // slices (warps) per tile of the staged-x SpMV
+
 void set_error(const std::string& msg);
 void clear_error();
 
@@ -107,6 +109,13 @@ struct femk_plan {
   int64_t* sell_cuptr = nullptr;  // i64[n_slices+1] first table entry of each slice
   int16_t* sell_cu = nullptr;     // i16[sell_cu_len]
   int64_t sell_cu_len = 0;
+  // staged-x SpMV (femk_tile.cuh): per-tile x windows and slot tables, built with the plan
+  int tile_on = 0, tile_ok = 0;   // opt-in (FEMK_TILE=1): measured slower than the bulk-copy kernel
+  int tile64 = 1, tile32 = 1;     // use the staged-x kernel for the FP64 CG step / the FP32 step
+  int64_t ntiles = 0;
+  int tile_xcap = 0;              // largest staged x of any tile (elements, multiple of 4)
+  void* tile_meta = nullptr;      // TileMeta[ntiles]
+  int16_t* tile_slots = nullptr;  // i16[sell_cu_len] slot table (layout of sell_cu)
   int use_sell = 1;
   int l2_mode = 0;               // L2 eviction hints of the FP64 CG kernels (see l2_hints in femk_spmv.cuh)
   int l2_mode32 = 0;             // the same for the FP32 kernels of the mixed solver (0 off, 1 on)
@@ -150,6 +159,7 @@ struct femk_plan {
   cudaEvent_t batch_ev = nullptr;
   int batch_graph_ok = 1;
   void* prof = nullptr;         // per-kernel CG timing (femk_set_profiling)
+  double* coef_tmp = nullptr;   // f64[ntet] element coefficients of a nodal parameter
   // BiCGStab workspace (8 vectors), state, stream, events and captured chunk graph
   void* bicg_ws = nullptr;
   void* bicg_state = nullptr;
@@ -182,6 +192,11 @@ inline int blocks_for(int64_t n, int threads, int cap = 1 << 30) {
 int scan_exclusive_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
 
 int ensure_workspace(femk_plan* p);
+
+// Nodal P1 coefficient modes become a per-element coefficient (plan-owned f64[ntet], computed on
+// stream s) read as FEMK_COEF_LINEAR; other modes pass through unchanged.
+int resolve_coef(const femk_plan* p, const double* param, int mode, cudaStream_t s, const double** param_out,
+                 int* mode_out);
 
 // Blocks of `threads` threads of kernel `fn` resident per SM (occupancy), cached per kernel.
 int resident_blocks(const void* fn, int threads);

@@ -21,6 +21,7 @@
 #include <type_traits>
 
 #include "femk_bulk.cuh"
+#include "femk_tile.cuh"
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
 #include "femk_grid.cuh"
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(WPB * 32) k_step32_bulk(const int64_t* __restr
                                                          double* __restrict__ partials, MixedState* st,
                                                          const int64_t* __restrict__ cptr) {
   extern __shared__ __align__(128) unsigned char bulk_smem[];
-  using R = BulkRing<float, int16_t, WMAX, S>;
+  constexpr int kWarpBytes = BulkRing<float, int16_t, WMAX, S>::kWarpBytes;
   pdl_wait();
   pdl_trigger();
   if (blockIdx.x == 0 && threadIdx.x == 0) st->epend = 0;  // the last e update is applied
@@ -179,7 +180,7 @@ __global__ void __launch_bounds__(WPB * 32) k_step32_bulk(const int64_t* __restr
   gx.x = p;
   if constexpr (H) gx.pol = l2_evict_last();
   const bool ok = sell_bulk_rows<float, int16_t, WMAX, S>(
-      bulk_smem + wib * R::kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * WPB + wib,
+      bulk_smem + wib * kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * WPB + wib,
       (int64_t)gridDim.x * WPB, gx,
       [&](int64_t row, float sv) {
         q[row] = sv;
@@ -189,6 +190,34 @@ __global__ void __launch_bounds__(WPB * 32) k_step32_bulk(const int64_t* __restr
   if (!ok && (threadIdx.x & 31) == 0) st->done = 1;
   double v[1] = {(double)acc}, tot[1];
   if (!reduce_finish<1, WPB * 32>(v, partials, &st->ticket, tot)) return;
+  if (threadIdx.x) return;
+  finish_alpha(st, tot[0]);
+}
+
+// The same step with matrix and p staged per tile in shared memory (femk_tile.cuh).
+template <int WMAX>
+__global__ void __launch_bounds__(kTileW * 32) k_step32_tile(const TileMeta* __restrict__ meta, int64_t ntiles,
+                                                            int xcap, const int64_t* __restrict__ sptr,
+                                                            const int64_t* __restrict__ cptr,
+                                                            const int16_t* __restrict__ slots,
+                                                            const float* __restrict__ vals, int64_t n,
+                                                            int64_t nslices, const float* __restrict__ p,
+                                                            float* __restrict__ q, double* __restrict__ partials,
+                                                            MixedState* st) {
+  extern __shared__ __align__(128) unsigned char tile_smem[];
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->epend = 0;  // the last e update is applied
+  if (st->done || st->hold) return;
+  float acc = 0.f;
+  const bool ok = sell_tile_rows<float, kTileW, WMAX>(
+      tile_smem, xcap, meta, ntiles, sptr, cptr, slots, vals, p, n, nslices,
+      [&](int64_t row, float sv, float prow) {
+        q[row] = sv;
+        acc = fmaf(prow, sv, acc);
+      },
+      &st->status, FEMK_TIMEOUT);
+  if (!ok && threadIdx.x == 0) st->done = 1;
+  double v[1] = {(double)acc}, tot[1];
+  if (!reduce_finish<1, kTileW * 32>(v, partials, &st->ticket, tot)) return;
   if (threadIdx.x) return;
   finish_alpha(st, tot[0]);
 }
@@ -705,7 +734,7 @@ template <int S, int WPB, int WMAX>
 bool launch_step32_bulk_cfg(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
                             bool prime) {
   return p->l2_mode32 != 0 ? launch_step32_bulk_h<S, WPB, WMAX, true>(p, pv, q, st, s, prime)
-                         : launch_step32_bulk_h<S, WPB, WMAX, false>(p, pv, q, st, s, prime);
+                           : launch_step32_bulk_h<S, WPB, WMAX, false>(p, pv, q, st, s, prime);
 }
 
 // bulk-copy FP32 step in the plan's configuration (bulk32_cfg: 10 * stages + warps per block)
@@ -732,7 +761,42 @@ bool launch_step32_bulk(const femk_plan* p, const float* pv, float* q, MixedStat
 #undef FEMK_BULK_CFG
 }
 
+template <int WMAX>
+bool launch_step32_tile_w(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
+                          bool prime) {
+  auto kern = k_step32_tile<WMAX>;
+  static int attr_ok = -1;  // per instantiation: opt in to the largest stage size once
+  if (attr_ok < 0) {
+    const int most = 2 * TileStage<float, kTileW, WMAX>::bytes(4096) + 16;
+    attr_ok = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, most) == cudaSuccess;
+    if (!attr_ok) cudaGetLastError();
+  }
+  if (!attr_ok) return false;
+  const int smem = 2 * TileStage<float, kTileW, WMAX>::bytes(p->tile_xcap) + 16;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileW * 32, smem) != cudaSuccess || per_sm <= 0) {
+    cudaGetLastError();
+    return false;
+  }
+  if (prime) return true;
+  const int grid = (int)std::min<int64_t>(p->ntiles, (int64_t)p->n_sm * std::min(per_sm, 16));
+  kern<<<::femk::counted_launch() + grid, kTileW * 32, smem, s>>>(
+      (const TileMeta*)p->tile_meta, p->ntiles, p->tile_xcap, p->sell_ptr, p->sell_cuptr, p->tile_slots,
+      p->sell_vals32, p->n, p->n_slices, pv, q, p->partials, st);
+  return true;
+}
+
+// staged-x FP32 step when the plan built its tiles; false: nothing launched
+bool launch_step32_tile(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
+                        bool prime = false) {
+  if (!p->tile_ok || !p->tile32 || !p->sell_vals32 || ((uintptr_t)p->sell_vals32 & 15u) || ((uintptr_t)pv & 15u))
+    return false;
+  return p->max_row <= 16 ? launch_step32_tile_w<16>(p, pv, q, st, s, prime)
+                          : launch_step32_tile_w<32>(p, pv, q, st, s, prime);
+}
+
 void launch_step32(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s) {
+  if (launch_step32_tile(p, pv, q, st, s)) return;
   if (launch_step32_bulk(p, pv, q, st, s)) return;
   if (p->sell_vals32) {
     auto go = [&](auto Bc) {
@@ -848,6 +912,7 @@ int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double
   (void)wave_grid(k_step32_sell<int16_t, 16>, kThreads, p);
   (void)wave_grid(k_step32_sell<int32_t, 16>, kThreads, p);
   (void)launch_step32_bulk(p, nullptr, nullptr, nullptr, nullptr, true);
+  (void)launch_step32_tile(p, nullptr, nullptr, nullptr, nullptr, true);
   (void)wave_grid(k_update32, kThreads, p);
   (void)wave_grid(k_update32_r<true>, kThreads, p);
   (void)wave_grid(k_update32_r<false>, kThreads, p);

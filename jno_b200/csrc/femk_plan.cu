@@ -10,11 +10,16 @@
 //  * Dirichlet: every node on a facet owned by exactly one tet (jno/_fem.py:2695).
 //
 // Everything here is integer work: one thread (or warp) per element/row, no sorting library.
+#include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cstdlib>
+#include <thread>
+#include <vector>
 
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
+#include "femk_tile.cuh"
 
 namespace femk {
 namespace {
@@ -378,6 +383,7 @@ int build_incidence(const int32_t* cells, int64_t ntet, int64_t n, int32_t** ptr
 }
 
 int build_uniform_columns(femk_plan* p, cudaStream_t s);
+int build_tiles(femk_plan* p, cudaStream_t s);
 
 template <int ND>
 int build_pattern(femk_plan* p, int* d_err, int* h_err, cudaStream_t s) {
@@ -511,6 +517,139 @@ int build_uniform_columns(femk_plan* p, cudaStream_t s) {
                                                                         p->sell_cuptr, p->sell_cu);
   FEMK_CUDA_TRY(cudaGetLastError());
   FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  return build_tiles(p, s);
+}
+
+// Tiles of the staged-x SpMV (femk_tile.cuh): kTileW consecutive slices each. Built on the host
+// from the CSR pattern and the per-slice column tables (a one-off cost of the plan): per tile the
+// x windows covering its columns (column runs closer than kTileGap merged, starts and lengths on
+// 4-element boundaries, clamped to the solver vectors' padded length) and a slot table in the
+// layout of the column tables. A plan whose tiles need more than kTileMaxWin windows or more than
+// kTileXCap staged values, or whose shared-offset slices do not map to consecutive slots, keeps
+// the bulk-copy kernel instead (tile_ok = 0).
+constexpr int kTileGap = 16;
+constexpr int kTileXCap = 4096;
+
+int build_tiles(femk_plan* p, cudaStream_t s) {
+  if (!p->sell_cu || !p->tile_on || p->max_row > 32) return FEMK_OK;
+  const int64_t n = p->n, ns = p->n_slices, W = kTileW;
+  const int64_t vlim = (n + 63) / 64 * 64;  // solver vectors hold n rounded up to 64 elements
+  std::vector<int32_t> indptr(n + 1), indices(p->nnz);
+  std::vector<int64_t> sptr(ns + 1), cptr(ns + 1);
+  FEMK_CUDA_TRY(cudaMemcpyAsync(indptr.data(), p->indptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaMemcpyAsync(indices.data(), p->indices, sizeof(int32_t) * p->nnz, cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaMemcpyAsync(sptr.data(), p->sell_ptr, sizeof(int64_t) * (ns + 1), cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaMemcpyAsync(cptr.data(), p->sell_cuptr, sizeof(int64_t) * (ns + 1), cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  const int64_t ntiles = (ns + W - 1) / W;
+  std::vector<TileMeta> meta(ntiles);
+  std::vector<int16_t> tab(p->sell_cu_len, 0);
+  std::atomic<int> bad{0};
+  std::atomic<int> xcap{4};
+  auto work = [&](int64_t t0, int64_t t1) {
+    std::vector<int32_t> cols;
+    for (int64_t t = t0; t < t1 && !bad.load(std::memory_order_relaxed); ++t) {
+      const int64_t s0 = t * W, s1 = std::min(ns, s0 + W);
+      const int64_t r0 = s0 * 32, r1 = std::min(n, s1 * 32);
+      cols.assign(indices.begin() + indptr[r0], indices.begin() + indptr[r1]);
+      std::sort(cols.begin(), cols.end());
+      cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+      TileMeta m{};
+      int nwin = 0;
+      int64_t lo = cols[0], hi = cols[0];
+      auto close = [&](int64_t a, int64_t b) -> bool {  // [a, b] inclusive -> aligned window
+        const int64_t st = a / 4 * 4, en = std::min(vlim, (b + 1 + 3) / 4 * 4);
+        if (nwin > 0 && st <= (int64_t)m.wstart[nwin - 1] + m.wlen[nwin - 1]) {  // overlaps after rounding
+          m.wlen[nwin - 1] = (int32_t)(en - m.wstart[nwin - 1]);
+          return true;
+        }
+        if (nwin == kTileMaxWin) return false;
+        m.wstart[nwin] = (int32_t)st;
+        m.wlen[nwin] = (int32_t)(en - st);
+        ++nwin;
+        return true;
+      };
+      bool ok = true;
+      for (size_t j = 1; j < cols.size() && ok; ++j) {
+        if (cols[j] - hi <= kTileGap) {
+          hi = cols[j];
+        } else {
+          ok = close(lo, hi);
+          lo = hi = cols[j];
+        }
+      }
+      ok = ok && close(lo, hi);
+      int64_t xlen = 0;
+      int32_t base[kTileMaxWin];
+      for (int j = 0; j < nwin; ++j) {
+        base[j] = (int32_t)xlen;
+        xlen += m.wlen[j];
+      }
+      if (!ok || xlen > kTileXCap) {
+        bad = 1;
+        return;
+      }
+      m.nwin = nwin;
+      m.xlen = (int32_t)xlen;
+      auto slot = [&](int64_t c) -> int64_t {
+        for (int j = 0; j < nwin; ++j)
+          if (c >= m.wstart[j] && c < (int64_t)m.wstart[j] + m.wlen[j]) return base[j] + (c - m.wstart[j]);
+        return -1;
+      };
+      const int64_t sr = slot(r0);
+      m.self_base = (int32_t)(sr - r0);
+      m.v0 = sptr[s0];
+      m.v1 = sptr[s1];
+      m.c0 = cptr[s0];
+      m.c1 = cptr[s1];
+      for (int64_t sl = s0; sl < s1 && ok; ++sl) {
+        const int64_t w = (sptr[sl + 1] - sptr[sl]) / 32;
+        const bool uni = (cptr[sl + 1] - cptr[sl]) != 32 * w;
+        for (int64_t k = 0; k < w && ok; ++k)
+          for (int l = 0; l < 32 && ok; ++l) {
+            const int64_t row = sl * 32 + l;
+            const int64_t self = row < n ? row : n - 1;
+            const int64_t len = row < n ? indptr[row + 1] - indptr[row] : 0;
+            const int64_t col = k < len ? indices[indptr[row] + k] : self;
+            const int64_t sv = slot(col);
+            if (sv < 0 || sv >= xlen || (row < n && slot(row) != row + m.self_base)) {
+              ok = false;
+            } else if (uni) {
+              if (l == 0) tab[cptr[sl] + k] = (int16_t)sv;
+              else if ((int64_t)tab[cptr[sl] + k] + l != sv) ok = false;
+            } else {
+              tab[cptr[sl] + 32 * k + l] = (int16_t)sv;
+            }
+          }
+      }
+      if (!ok) {
+        bad = 1;
+        return;
+      }
+      meta[t] = m;
+      int cur = xcap.load();
+      while ((int)xlen > cur && !xcap.compare_exchange_weak(cur, (int)xlen)) {
+      }
+    }
+  };
+  const int nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  const int64_t per = (ntiles + nth - 1) / nth;
+  for (int i = 0; i < nth; ++i) {
+    const int64_t a = i * per, b = std::min(ntiles, a + per);
+    if (a < b) pool.emplace_back(work, a, b);
+  }
+  for (auto& th : pool) th.join();
+  if (bad) return FEMK_OK;  // the plan keeps the bulk-copy kernel
+  FEMK_TRY(dev_alloc((char**)&p->tile_meta, (int64_t)sizeof(TileMeta) * ntiles, s));
+  FEMK_TRY(dev_alloc(&p->tile_slots, p->sell_cu_len, s));
+  FEMK_CUDA_TRY(cudaMemcpyAsync(p->tile_meta, meta.data(), sizeof(TileMeta) * ntiles, cudaMemcpyHostToDevice, s));
+  FEMK_CUDA_TRY(cudaMemcpyAsync(p->tile_slots, tab.data(), sizeof(int16_t) * p->sell_cu_len, cudaMemcpyHostToDevice,
+                                s));
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  p->ntiles = ntiles;
+  p->tile_xcap = (xcap.load() + 3) / 4 * 4;
+  p->tile_ok = 1;
   return FEMK_OK;
 }
 
@@ -640,7 +779,8 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
                   p->diag,     p->dmask,     p->dlist,     p->inc_ptr,   p->inc_elem,  p->cols16,
                   p->work,     p->partials,  p->state,     p->work32,    p->vals32,    p->work64b,
                   p->sell_ptr, p->sell_src,  p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32,
-                  p->bar,      p->batch_ws,  p->bicg_ws,   p->bicg_state, p->sell_cuptr, p->sell_cu};
+                  p->bar,      p->batch_ws,  p->bicg_ws,   p->bicg_state, p->sell_cuptr, p->sell_cu,
+                  p->tile_meta, p->tile_slots, p->coef_tmp};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->state_host) cudaFreeHost(p->state_host);
@@ -699,6 +839,9 @@ extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int3
   if (const char* e = std::getenv("FEMK_BULK32")) p->bulk32_cfg = std::atoi(e);
   if (const char* e = std::getenv("FEMK_PDL")) p->pdl = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_SELL_UNI")) p->sell_uni = std::atoi(e) != 0;
+  if (const char* e = std::getenv("FEMK_TILE")) p->tile_on = std::atoi(e) != 0;
+  if (const char* e = std::getenv("FEMK_TILE64")) p->tile64 = std::atoi(e) != 0;
+  if (const char* e = std::getenv("FEMK_TILE32")) p->tile32 = std::atoi(e) != 0;
   // FP32 kernels stream without hints: measured on B200 at P1 128^3, mixed solve 31.7 ms without
   // vs 32.8 ms with evict-last vectors and gathers
   p->l2_mode32 = 0;
@@ -728,7 +871,7 @@ extern "C" int femk_plan_get_info(const femk_plan* p, femk_plan_info* out) {
   out->device = p->device;
   out->sell_nnz = p->sell_src ? p->sell_nnz : 0;
   out->batch_graph = p->batch_graph_used;
-  out->pad = 0;
+  out->tiles = p->tile_ok;
   out->sell_col_units = p->sell_cu ? p->sell_cu_len : (p->sell_src ? p->sell_nnz : 0);
   return FEMK_OK;
 }

@@ -69,6 +69,7 @@ class FemPlan:
         self.cols16 = bool(info.cols16)
         self.sell_nnz = int(info.sell_nnz)
         self.sell_col_units = int(info.sell_col_units)
+        self.tiles = bool(info.tiles)
         self.device = torch.device("cuda", info.device)
         self._pattern = None
 
