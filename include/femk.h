@@ -241,6 +241,8 @@ int femk_pcg_batched(const femk_plan* plan, int32_t nprob, const int64_t* row_of
 /*
  * Adjoint contraction: grad[c] = -k_c * (m o lam)_e^T K_hat_e (m o u)_e, m = 1 - dirichlet mask,
  * k_c = coef_scale * exp(param_c) (FEMK_COEF_EXP) or coef_scale (FEMK_COEF_LINEAR: d/dparam).
+ * Nodal P1 modes: grad f64[nvert], grad[i] = sum over elements e holding vertex i of
+ * -(m o lam)_e^T K_hat_e (m o u)_e * dk_e/dparam_i.
  * Replaces jax.grad through custom_linear_solve + segment_sum + jacfwd (no jNO function).
  */
 int femk_adjoint_grad(const femk_plan* plan, const double* param_dev, int coef_mode, double coef_scale,

@@ -1,4 +1,5 @@
-"""``torch.autograd.Function`` binding: u = solve(A(logk), b) with a hand-written adjoint.
+"""``torch.autograd.Function`` binding: u = solve(A(logk), b) with a hand-written adjoint (P0 or
+nodal P1 parameters).
 
 Forward: fused assembly + Jacobi-PCG (FP64, or the mixed FP32/FP64 solver). Backward: one more
 PCG on the same kernels for lambda = A^-T dJ/du (A is symmetric), then the per-element contraction
@@ -40,4 +41,13 @@ class _SolveP0(torch.autograd.Function):
 
 def solve_p0(plan, param, mode=_lib.COEF_EXP, scale=1.0, f=1.0, tol=1e-8, maxiter=20_000, precision="fp64"):
     """Differentiable ``u(param)`` for ``scale * g(param_e) grad u . grad v - f v`` with u = 0 on the boundary."""
+    return _SolveP0.apply(param, plan, mode, scale, f, tol, maxiter, precision)
+
+
+def solve_nodal(plan, param, mode=_lib.COEF_NODAL_EXP, scale=1.0, f=1.0, tol=1e-8, maxiter=20_000,
+                precision="fp64"):
+    """The same for a nodal P1 parameter (one value per vertex): the backward pass spreads each
+    element's dJ/dk_e onto its vertices by dk_e/dparam_i."""
+    if mode not in (_lib.COEF_NODAL_EXP, _lib.COEF_NODAL_LINEAR):
+        raise ValueError("solve_nodal takes FEMK_COEF_NODAL_EXP or FEMK_COEF_NODAL_LINEAR")
     return _SolveP0.apply(param, plan, mode, scale, f, tol, maxiter, precision)

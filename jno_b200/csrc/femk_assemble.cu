@@ -140,6 +140,57 @@ __global__ void k_adjoint(const double* __restrict__ xyz, const int32_t* __restr
   }
 }
 
+// Nodal P1 parameter: the element's dJ/dk_e = -(m o lam)^T K_hat (m o u) spread onto its four
+// vertex values by dk_e/dp_i (linear: scale / 4; exp with the 4-point rule, L_q = a S + (b - a) p_q:
+// scale / 4 * (a sum_q exp(L_q) + (b - a) exp(L_i))). grad f64[nvert] must start at zero.
+__global__ void k_adjoint_nodal(const double* __restrict__ xyz, const int32_t* __restrict__ cells, int64_t ntet,
+                                const uint8_t* __restrict__ dmask, const double* __restrict__ param, int mode,
+                                double scale, const double* __restrict__ u, const double* __restrict__ lam,
+                                double* __restrict__ grad) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t dof[4];
+    double ue[4], le[4], pv[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      dof[a] = __ldg(cells + c * 4 + a);
+      const bool d = __ldg(dmask + dof[a]) != 0;
+      ue[a] = d ? 0.0 : __ldg(u + dof[a]);
+      le[a] = d ? 0.0 : __ldg(lam + dof[a]);
+      pv[a] = __ldg(param + dof[a]);
+    }
+    TetGeom T;
+    tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
+    double VG[4][4];
+    gram(T, VG);
+    double acc = 0.0;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      double row = 0.0;
+#pragma unroll
+      for (int bb = 0; bb < 4; ++bb) row += khat<4>(VG, a, bb) * ue[bb];
+      acc += le[a] * row;
+    }
+    double dk[4];
+    if (mode == FEMK_COEF_NODAL_LINEAR) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) dk[i] = 0.25 * scale;
+    } else {
+      constexpr double qa = 0.13819660112501051518, qb = 0.58541019662496845446;
+      const double S = pv[0] + pv[1] + pv[2] + pv[3];
+      double e[4], es = 0.0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        e[i] = exp(qa * S + (qb - qa) * pv[i]);
+        es += e[i];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) dk[i] = 0.25 * scale * (qa * es + (qb - qa) * e[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) atomicAdd(grad + dof[i], -acc * dk[i]);
+  }
+}
+
 }  // namespace
 }  // namespace femk
 
@@ -218,10 +269,20 @@ extern "C" int femk_adjoint_grad(const femk_plan* p, const double* param, int mo
                                  const double* lam, double* grad, void* stream) {
   clear_error();
   FEMK_CHECK_ARG(p && u && lam && grad, "femk_adjoint_grad: NULL argument");
-  FEMK_CHECK_ARG(mode == 0 || mode == 1, "femk_adjoint_grad: coef_mode must be EXP or LINEAR");
-  FEMK_CHECK_ARG(mode == 1 || param, "femk_adjoint_grad: param is NULL");
+  FEMK_CHECK_ARG(mode == FEMK_COEF_EXP || mode == FEMK_COEF_LINEAR || mode == FEMK_COEF_NODAL_EXP ||
+                     mode == FEMK_COEF_NODAL_LINEAR,
+                 "femk_adjoint_grad: coef_mode must be a P0 or nodal EXP/LINEAR mode");
+  FEMK_CHECK_ARG(coef_mode_ok(p, mode, param) && (mode == FEMK_COEF_LINEAR || param),
+                 "femk_adjoint_grad: param is NULL or a nodal mode on a P2 plan");
   cudaStream_t s = (cudaStream_t)stream;
   const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);
+  if (mode == FEMK_COEF_NODAL_EXP || mode == FEMK_COEF_NODAL_LINEAR) {
+    FEMK_CUDA_TRY(cudaMemsetAsync(grad, 0, sizeof(double) * p->nvert, s));
+    k_adjoint_nodal<<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param,
+                                                                         mode, scale, u, lam, grad);
+    FEMK_CUDA_TRY(cudaGetLastError());
+    return FEMK_OK;
+  }
   if (p->nd == 4)
     k_adjoint<4><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param, mode, scale, u, lam, grad);
   else

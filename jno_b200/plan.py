@@ -265,7 +265,9 @@ class FemPlan:
         return x, it, rel, stv, st
 
     def adjoint_grad(self, param, u, lam, mode=_lib.COEF_EXP, scale=1.0, out=None):
-        out = torch.empty(self.ntet, dtype=torch.float64, device=self.device) if out is None else out
+        nodal = mode in (_lib.COEF_NODAL_EXP, _lib.COEF_NODAL_LINEAR)
+        size = self.nvert if nodal else self.ntet
+        out = torch.empty(size, dtype=torch.float64, device=self.device) if out is None else out
         _lib.check(self._lib.femk_adjoint_grad(self._h, _lib.ptr(param), int(mode), float(scale), _lib.ptr(u),
                                                _lib.ptr(lam), _lib.ptr(out), _lib.stream_handle()))
         return out

@@ -52,3 +52,30 @@ def gradient(points, cells, order, dirichlet, logk, ustar, mass, tol=1e-12):
     ue = (m * u)[cells]
     grad = -np.exp(logk) * np.einsum("ta,tab,tb->t", le, Khat, ue)
     return misfit(u, ustar, mass), grad
+
+
+def gradient_nodal(points, cells, dirichlet, values, mode, ustar, mass, tol=1e-12):
+    """(J, dJ/dp f64[nvert]) for a nodal P1 parameter p: the element gradient dJ/dk_e (as above,
+    with k_e from ``element.nodal_coefficient``) spread onto the vertices by dk_e/dp_i."""
+    from .assemble import jacobi_inverse, matrix_diagonal
+    from .element import _Q4_A, _Q4_B, nodal_coefficient
+
+    ke = nodal_coefficient(cells, values, mode)
+    sysm = assemble(points, cells, 1, dirichlet, ke)
+    A = sysm.csr()
+    inv = jacobi_inverse(matrix_diagonal(sysm))
+    u, _, _ = pcg(A, sysm.b, inv, tol=tol)
+    lam, _, _ = pcg(A.T.tocsr(), mass * (u - ustar), inv, tol=tol)
+    m = (~sysm.dirichlet).astype(np.float64)
+    Khat, _ = element_matrices(points[cells[:, :4]], 1)
+    dJdk = -np.einsum("ta,tab,tb->t", (m * lam)[cells], Khat, (m * u)[cells])
+    p = np.asarray(values, dtype=np.float64)[cells]
+    if mode == "linear":
+        dk = np.full(p.shape, 0.25)
+    else:
+        lamq = np.full((4, 4), _Q4_A) + np.eye(4) * (_Q4_B - _Q4_A)
+        e = np.exp(p @ lamq.T)
+        dk = 0.25 * (_Q4_A * e.sum(axis=1, keepdims=True) + (_Q4_B - _Q4_A) * e)
+    grad = np.bincount(cells.reshape(-1), weights=(dJdk[:, None] * dk).reshape(-1), minlength=points.shape[0])
+    return misfit(u, ustar, mass), grad
+

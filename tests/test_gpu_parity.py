@@ -520,3 +520,42 @@ def test_nodal_p1_parameter_matches_oracle(mode):
     assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-8 * np.linalg.norm(xo)
     with pytest.raises(ValueError):
         fem.operator.evaluate({"k": np.zeros(len(tets))})  # P0-sized input for a nodal parameter
+
+
+@pytest.mark.parametrize("mode", ["exp", "linear"])
+def test_nodal_adjoint_matches_oracle_and_fd(mode):
+    """dJ/dp for a nodal P1 parameter: oracle chain rule (1e-8) and central differences."""
+    from jno_b200 import _lib
+    from jno_b200.autograd import solve_nodal
+
+    n = 5
+    pf, cf, tets, p1 = _mesh(n, 1)
+    rng = np.random.default_rng(13)
+    vals = rng.normal(0.0, 0.4, p1.shape[0]) if mode == "exp" else rng.uniform(0.5, 2.0, p1.shape[0])
+    cmode = _lib.COEF_NODAL_EXP if mode == "exp" else _lib.COEF_NODAL_LINEAR
+    bnd = om.boundary_nodes(cf, 1)
+    ustar, _, _ = oadj.solve(pf, cf, 1, bnd, om.logk_field(len(tets), 2001))
+    mass = oadj.lumped_mass(pf, cf, 1)
+    J_o, g_o = oadj.gradient_nodal(pf, cf, bnd, vals, mode, ustar, mass)
+    plan = _plan(p1, tets, 1)
+    m = plan.lumped_mass()
+    us = torch.as_tensor(ustar, device="cuda")
+    pv = torch.as_tensor(vals, device="cuda").requires_grad_(True)
+    u = solve_nodal(plan, pv, cmode, tol=1e-13)
+    J = 0.5 * torch.sum(m * (u - us) ** 2)
+    J.backward()
+    g = pv.grad.cpu().numpy()
+    assert abs(J.item() - J_o) <= 1e-10 * abs(J_o)
+    assert np.abs(g - g_o).max() <= 1e-8 * np.abs(g_o).max()
+
+    def Jof(v):
+        with torch.no_grad():
+            uu = solve_nodal(plan, torch.as_tensor(v, device="cuda"), cmode, tol=1e-14)
+            return (0.5 * torch.sum(m * (uu - us) ** 2)).item()
+
+    interior = np.setdiff1d(np.arange(p1.shape[0]), bnd)
+    for i in rng.choice(interior, 6, replace=False):
+        e = np.zeros(p1.shape[0])
+        e[i] = 1e-6
+        fd = (Jof(vals + e) - Jof(vals - e)) / 2e-6
+        assert abs(fd - g[i]) <= 1e-6 * np.abs(g).max() + 1e-6 * abs(g[i])

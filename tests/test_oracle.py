@@ -204,3 +204,29 @@ def test_nodal_coefficient_rule():
     lamq = np.full((4, 4), oe._Q4_A) + np.eye(4) * (oe._Q4_B - oe._Q4_A)
     fq = lamq[:, 0] * lamq[:, 1] + 0.5 * lamq[:, 2] ** 2 + lamq[:, 3]
     assert abs(fq.mean() - exact) <= 1e-14
+
+
+@pytest.mark.parametrize("mode", ["exp", "linear"])
+def test_oracle_nodal_gradient_matches_fd(mode):
+    from oracle import adjoint as oadj
+
+    n = 3
+    pf, cf, tets, p1 = om.kuhn_cube(n, 1, seed=2)
+    rng = np.random.default_rng(5)
+    vals = rng.normal(0.0, 0.4, pf.shape[0]) if mode == "exp" else rng.uniform(0.5, 2.0, pf.shape[0])
+    bnd = om.boundary_nodes(cf, 1)
+    ustar = rng.normal(size=pf.shape[0])
+    mass = oadj.lumped_mass(pf, cf, 1)
+    J, g = oadj.gradient_nodal(pf, cf, bnd, vals, mode, ustar, mass, tol=1e-14)
+
+    def Jof(v):
+        s = oa.assemble(pf, cf, 1, bnd, oe.nodal_coefficient(cf, v, mode))
+        u = _solve_direct(s)
+        return oadj.misfit(u, ustar, mass)
+
+    interior = np.setdiff1d(np.arange(pf.shape[0]), bnd)
+    for i in interior[:5]:
+        e = np.zeros(pf.shape[0])
+        e[i] = 1e-6
+        fd = (Jof(vals + e) - Jof(vals - e)) / 2e-6
+        assert abs(fd - g[i]) <= 1e-6 * np.abs(g).max() + 1e-6 * abs(g[i])
