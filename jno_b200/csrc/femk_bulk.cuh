@@ -22,6 +22,8 @@
 
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "femk_l2.cuh"
 #include "femk_spmv.cuh"
 
@@ -179,24 +181,51 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
     }
     const int32_t ws = wid[s];
     const int32_t w = ws < 0 ? -ws : ws;
-    const int cstride = ws < 0 ? 1 : 32;  // shared offsets: every lane reads entry k (a broadcast)
-    const int clane = ws < 0 ? 0 : lane;
-    const V* sv = reinterpret_cast<const V*>(stages + s * R::kStage);
+    const V* sv = reinterpret_cast<const V*>(stages + s * R::kStage) + lane;
     const IDX* sc = reinterpret_cast<const IDX*>(stages + s * R::kStage + R::kVal);
     const int64_t row = sl * 32 + lane;
     const bool live = row < n;  // rows past n in the last slice gather nothing
-    V xg[WMAX];
+    V acc = V(0);
+    // Row sum in k order. The common widths (WMAX, WMAX - 1) run without per-entry predicates, and
+    // the shared-offset and per-entry column layouts each get compile-time strides, so an entry costs
+    // a shared load of its column, the gather, a shared load of its value and one FMA.
+    auto run = [&](auto KC, auto UC) {
+      constexpr int K = decltype(KC)::value;
+      constexpr bool U = decltype(UC)::value;
+      const IDX* cb = U ? sc : sc + lane;
+      V xg[K];
 #pragma unroll
-    for (int k = 0; k < WMAX; ++k) {
-      if (k < w && live) {
-        const IDX c = sc[k * cstride + clane];
-        xg[k] = gx(sizeof(IDX) == 2 ? (int64_t)row + (int64_t)c : (int64_t)c);
+      for (int k = 0; k < K; ++k) {
+        const IDX c = cb[U ? k : k * 32];
+        xg[k] = gx(sizeof(IDX) == 2 ? (int32_t)row + (int32_t)c : (int32_t)c);
+      }
+#pragma unroll
+      for (int k = 0; k < K; ++k) acc += sv[k * 32] * xg[k];
+    };
+    if (live) {
+      using std::integral_constant;
+      const bool u = ws < 0;
+      if (w == WMAX) {
+        u ? run(integral_constant<int, WMAX>{}, std::true_type{}) : run(integral_constant<int, WMAX>{}, std::false_type{});
+      } else if (w == WMAX - 1) {
+        u ? run(integral_constant<int, WMAX - 1>{}, std::true_type{})
+          : run(integral_constant<int, WMAX - 1>{}, std::false_type{});
+      } else {
+        const int cstride = u ? 1 : 32;  // shared offsets: every lane reads entry k (a broadcast)
+        const int clane = u ? 0 : lane;
+        V xg[WMAX];
+#pragma unroll
+        for (int k = 0; k < WMAX; ++k) {
+          if (k < w) {
+            const IDX c = sc[k * cstride + clane];
+            xg[k] = gx(sizeof(IDX) == 2 ? (int32_t)row + (int32_t)c : (int32_t)c);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < WMAX; ++k)
+          if (k < w) acc += sv[k * 32] * xg[k];
       }
     }
-    V acc = V(0);
-#pragma unroll
-    for (int k = 0; k < WMAX; ++k)
-      if (k < w && live) acc += sv[k * 32 + lane] * xg[k];
     __syncwarp();  // every lane is done with stage s before it is refilled
     if (lane == 0) {
       const int64_t nsl = g + (i + S) * NW;

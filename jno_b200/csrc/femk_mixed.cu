@@ -750,11 +750,15 @@ bool launch_step32_bulk(const femk_plan* p, const float* pv, float* q, MixedStat
     return narrow ? launch_step32_bulk_cfg<S, WPB, 16>(p, pv, q, st, s, prime)                      \
                   : launch_step32_bulk_cfg<S, WPB, 32>(p, pv, q, st, s, prime);
   switch (p->bulk32_cfg) {
+    FEMK_BULK_CFG(11, 1, 1)
     FEMK_BULK_CFG(12, 1, 2)
+    FEMK_BULK_CFG(14, 1, 4)
+    FEMK_BULK_CFG(18, 1, 8)
     FEMK_BULK_CFG(22, 2, 2)
     FEMK_BULK_CFG(24, 2, 4)
     FEMK_BULK_CFG(28, 2, 8)
     FEMK_BULK_CFG(34, 3, 4)
+    FEMK_BULK_CFG(38, 3, 8)
     default:
       return false;
   }

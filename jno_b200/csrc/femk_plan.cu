@@ -833,7 +833,7 @@ extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int3
   if (const char* e = std::getenv("FEMK_CG_SPLIT")) p->cg_split = std::atoi(e) != 0;
   // bulk-copy SpMV configurations, measured on B200 at P1 128^3 (to 1e-8): FP64 2 stages x 4 warps
   // (39.9-40.7 ms/step vs 45.8 ms register-streamed), FP32 2 stages x 8 warps (29.7-31.7 vs 32.5 ms)
-  p->bulk_cfg = 24;
+  p->bulk_cfg = 12;
   p->bulk32_cfg = 28;
   if (const char* e = std::getenv("FEMK_BULK")) p->bulk_cfg = std::atoi(e);
   if (const char* e = std::getenv("FEMK_BULK32")) p->bulk32_cfg = std::atoi(e);

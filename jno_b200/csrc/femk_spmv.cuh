@@ -30,6 +30,7 @@ template <typename V>
 struct GatherX {
   const V* __restrict__ x;
   __device__ __forceinline__ V operator()(int64_t j) const { return __ldg(x + j); }
+  __device__ __forceinline__ V operator()(int32_t j) const { return __ldg(x + j); }  // 32-bit index math
 };
 // x[j] through L2 only: for vectors that other blocks rewrite inside the same (persistent) launch,
 // where the non-coherent read-only path could return a stale line
@@ -44,6 +45,7 @@ struct GatherXL {
   const V* __restrict__ x;
   uint64_t pol;
   __device__ __forceinline__ V operator()(int64_t j) const;
+  __device__ __forceinline__ V operator()(int32_t j) const { return (*this)((int64_t)j); }
 };
 template <>
 __device__ __forceinline__ double GatherXL<double>::operator()(int64_t j) const {

@@ -559,3 +559,54 @@ def test_nodal_adjoint_matches_oracle_and_fd(mode):
         e[i] = 1e-6
         fd = (Jof(vals + e) - Jof(vals - e)) / 2e-6
         assert abs(fd - g[i]) <= 1e-6 * np.abs(g).max() + 1e-6 * abs(g[i])
+
+
+def test_p2_surface_recovers_harmonic_quadratic():
+    """Port of tests/test_fem_higher_order.py:133-150 onto the B200 path: P2 through jno.fem with
+    u = xy + yz + xz on the boundary, f = 0, fem.solve() (Jacobi-BiCGStab) recovers it to 1e-9."""
+    import jno_b200 as jno
+
+    n = 3
+    d = jno.domain(jno.domain.equi_distant_box(nx=n, ny=n, nz=n), jitter=0.1, seed=7)
+    u, phi = d.fem_symbols(order=2)
+    xi, yi, zi = d.variable("interior", split=True)
+    cb = d.variable("boundary", split=True)
+    ui, vi = u.bind(x=xi, y=yi, z=zi), phi.bind(x=xi, y=yi, z=zi)
+    bc = u(cb[0], cb[1], cb[2]) - (cb[0] * cb[1] + cb[1] * cb[2] + cb[0] * cb[2])
+    fem = jno.fem([ui.x * vi.x + ui.y * vi.y + ui.z * vi.z, bc])
+    assert fem.dofs > (n + 1) ** 3  # vertices + edge nodes
+    pts = fem.points.cpu().numpy()
+    sol = fem.solve(linear=jno.solve.bicgstab(tol=1e-12)).cpu().numpy()
+    exact = pts[:, 0] * pts[:, 1] + pts[:, 1] * pts[:, 2] + pts[:, 0] * pts[:, 2]
+    assert np.linalg.norm(exact - sol) / np.linalg.norm(exact) < 1e-9
+
+
+def test_p0_linearity_and_support_on_device():
+    """Port of tests/test_topology_optimisation.py:210-237 onto the CUDA assembly: the operator is
+    linear in the P0 values (sum of single-element assemblies) and an element's contribution stays
+    on its own DOFs."""
+    from jno_b200 import _lib
+
+    n = 3
+    pf, cf, tets, p1 = _mesh(n, 1)
+    plan = _plan(p1, tets, 1)
+    T = len(tets)
+    ex = plan.export()
+    dm = ex["dirichlet_mask"].cpu().numpy().astype(bool)
+    ip, ind = ex["indptr"].cpu().numpy(), ex["indices"].cpu().numpy()
+    rows = np.repeat(np.arange(plan.n), np.diff(ip))
+    free = ~(dm[rows] | dm[ind])
+    full, _ = plan.assemble(torch.ones(T, dtype=torch.float64, device="cuda"), mode=_lib.COEF_LINEAR)
+    acc = torch.zeros_like(full)
+    for j in range(T):
+        e = torch.zeros(T, dtype=torch.float64, device="cuda")
+        e[j] = 1.0
+        vj, _ = plan.assemble(e, mode=_lib.COEF_LINEAR)
+        acc += vj
+        if j == 40:
+            cell = set(tets[j].tolist())
+            vjn = vj.cpu().numpy()
+            off = np.array([(r not in cell or c not in cell) for r, c in zip(rows, ind)])
+            assert np.abs(vjn[off & free]).max() == 0.0
+    a, fl = acc.cpu().numpy(), full.cpu().numpy()
+    assert np.abs(a[free] - fl[free]).max() <= 1e-12 * np.abs(fl).max()
