@@ -29,7 +29,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kChunk = 8;              // iterations per enqueued (graph-replayed) chunk
-constexpr int kBulkS = 2, kBulkW = 4;  // bulk-copy SpMV ring: 2 slices in flight per warp, 4 warps
+constexpr int kBulkS = 1, kBulkW = 4;  // bulk-copy SpMV ring: 1 slice buffer per warp, 4 warps (the CG step's)
 
 struct BicgState {
   double rho;     // <rhat, r> of the previous iteration

@@ -893,14 +893,14 @@ bool split_ok(const femk_plan* p, const double* x, const double* dinv) {
 void launch_update_r(const femk_plan* p, double* r, const double* q, const double* dinv, CgState* st,
                      cudaStream_t s) {
   auto kern = p->l2_mode != 0 ? k_update_r<true> : k_update_r<false>;
-  (void)launch_ex(p->pdl != 0, kern, wave_grid(kern, kThreads, p), kThreads, 0, s, p->n, r, q, dinv, p->partials,
+  (void)launch_ex(p->pdl != 0, kern, vec_grid(kern, kThreads, p), kThreads, 0, s, p->n, r, q, dinv, p->partials,
                   st);
 }
 
 void launch_pupdate_x(const femk_plan* p, double* x, double* pv, const double* r, const double* dinv,
                       const CgState* st, cudaStream_t s) {
   auto kern = p->l2_mode != 0 ? k_pupdate_x<true> : k_pupdate_x<false>;
-  (void)launch_ex(p->pdl != 0, kern, wave_grid(kern, kThreads, p), kThreads, 0, s, p->n, x, pv, r, dinv, st);
+  (void)launch_ex(p->pdl != 0, kern, vec_grid(kern, kThreads, p), kThreads, 0, s, p->n, x, pv, r, dinv, st);
 }
 
 template <int MODE>

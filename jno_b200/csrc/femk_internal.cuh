@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <string>
 
 #include "../../include/femk.h"
@@ -136,6 +137,7 @@ struct femk_plan {
   int bulk_cfg = 0;             // bulk-copy FP64 CG-step SpMV: 10 * stages + warps per block, 0 = off
   int bulk32_cfg = 0;           // the same for the FP32 step of the mixed solver
   int pdl = 0;                  // programmatic dependent launch inside the CG / mixed chunks
+  int vec_blocks = 0;           // blocks per SM of the CG vector kernels (0: one full wave)
   int coop = 0;                 // device supports cooperative launch
   void* bar = nullptr;          // grid barrier of the persistent solvers
   cudaStream_t cg_stream = nullptr;
@@ -207,6 +209,14 @@ template <typename K>
 inline int wave_grid(K kernel, int threads, const femk_plan* p) {
   const int b = resident_blocks((const void*)kernel, threads);
   return p->n_sm * (b < 8 ? b : 8);
+}
+
+// Grid of the CG vector kernels: one wave, or p->vec_blocks blocks per SM when set (fewer blocks
+// mean fewer partials for the last-block reduction to add).
+template <typename K>
+inline int vec_grid(K kernel, int threads, const femk_plan* p) {
+  const int w = wave_grid(kernel, threads, p);
+  return p->vec_blocks > 0 ? std::min(w, p->n_sm * p->vec_blocks) : w;
 }
 
 // Programmatic dependent launch: a kernel launched with launch_ex(pdl = true) may start while its

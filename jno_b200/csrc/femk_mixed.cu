@@ -18,6 +18,7 @@
 // No reference counterpart: jNO runs x64 throughout (tests/test_fem_3d.py:37-46).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <type_traits>
 
 #include "femk_bulk.cuh"
@@ -857,9 +858,9 @@ int enqueue_mixed_chunk(const femk_plan* p, const double* vals, const double* b,
     if (p->cg_split) {
       auto ku = p->l2_mode32 != 0 ? k_update32_r<true> : k_update32_r<false>;
       auto kp = p->l2_mode32 != 0 ? k_pupdate32_x<true> : k_pupdate32_x<false>;
-      (void)launch_ex(p->pdl != 0, ku, wave_grid(ku, kThreads, p), kThreads, 0, s, n, m.r, (const float*)m.q,
+      (void)launch_ex(p->pdl != 0, ku, vec_grid(ku, kThreads, p), kThreads, 0, s, n, m.r, (const float*)m.q,
                       (const float*)m.d32, p->partials, m.st);
-      (void)launch_ex(p->pdl != 0, kp, wave_grid(kp, kThreads, p), kThreads, 0, s, n, m.e, m.pv, (const float*)m.r,
+      (void)launch_ex(p->pdl != 0, kp, vec_grid(kp, kThreads, p), kThreads, 0, s, n, m.e, m.pv, (const float*)m.r,
                       (const float*)m.d32, (const MixedState*)m.st);
     } else {
       k_update32<<<::femk::counted_launch() + wave_grid(k_update32, kThreads, p), kThreads, 0, s>>>(
@@ -994,6 +995,7 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   MixedState init{};
   init.maxiter = maxiter;
   init.delta2 = mode == FEMK_MIXED_RESTART ? 1e-8 : 1e-2;  // inner reduction per segment: 1e-4 / 0.1
+  if (const char* e = std::getenv("FEMK_MIXED_DELTA2")) init.delta2 = std::atof(e);  // tuning runs
   init.restart = mode == FEMK_MIXED_RESTART ? 1 : 0;
   FEMK_CUDA_TRY(cudaMemcpyAsync(m.st, &init, sizeof(MixedState), cudaMemcpyHostToDevice, ws));
   const double tol2 = tol * tol, atol2 = atol * atol;

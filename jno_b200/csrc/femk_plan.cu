@@ -831,13 +831,15 @@ extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int3
   p->l2_mode = std::getenv("FEMK_L2HINT") ? femk::l2_hints() : (order == 1 ? 1 : 0);
   if (const char* e = std::getenv("FEMK_CG_PERSIST")) p->cg_persist = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_CG_SPLIT")) p->cg_split = std::atoi(e) != 0;
-  // bulk-copy SpMV configurations, measured on B200 at P1 128^3 (to 1e-8): FP64 2 stages x 4 warps
-  // (39.9-40.7 ms/step vs 45.8 ms register-streamed), FP32 2 stages x 8 warps (29.7-31.7 vs 32.5 ms)
-  p->bulk_cfg = 12;
+  // bulk-copy SpMV configurations, measured on B200 at P1 128^3 (to 1e-8): FP64 1 stage x 4 warps
+  // (38.4 ms/step; 2 x 4: 43.2, 1 x 2: 40.4, register-streamed: 45.8), FP32 2 stages x 8 warps
+  // (27.1 ms; 1 x 8: 27.2, 2 x 4: 29.5)
+  p->bulk_cfg = 14;
   p->bulk32_cfg = 28;
   if (const char* e = std::getenv("FEMK_BULK")) p->bulk_cfg = std::atoi(e);
   if (const char* e = std::getenv("FEMK_BULK32")) p->bulk32_cfg = std::atoi(e);
   if (const char* e = std::getenv("FEMK_PDL")) p->pdl = std::atoi(e) != 0;
+  if (const char* e = std::getenv("FEMK_VEC_BLOCKS")) p->vec_blocks = std::atoi(e);
   if (const char* e = std::getenv("FEMK_SELL_UNI")) p->sell_uni = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_TILE")) p->tile_on = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_TILE64")) p->tile64 = std::atoi(e) != 0;
