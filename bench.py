@@ -301,6 +301,51 @@ def p2_variants(args, world, dev, timed):
     }
 
 
+def tri_variants(world, dev, timed, n1=1024, n2=512):
+    """2-D triangles: P1 on 1024^2 rectangles (1.05M DOF) FP64 and mixed, P2 on 512^2 (1.05M DOF)
+    FP64; jittered +-0.1h, k = exp(N(0, 0.5^2)) per triangle, assemble + Jacobi-PCG to 1e-8, 3 steps."""
+    import torch
+
+    from jno_b200.domain import jitter_interior_2d, rect_points_tris
+    from jno_b200.plan import FemPlan
+
+    out = {}
+    for order, nh in ((1, n1), (2, n2)):
+        pts, tris = rect_points_tris(nh, nh)
+        pts = jitter_interior_2d(pts, nh, nh, seed=0)[:, :2]
+        plan = FemPlan(pts, tris, order)
+        fields = [torch.as_tensor(f, device=dev) for f in logk_fields(plan.ntet, 3)]
+        vals = torch.empty(plan.nnz, dtype=torch.float64, device=dev)
+        b = torch.empty(plan.n, dtype=torch.float64, device=dev)
+        inv = torch.empty(plan.n, dtype=torch.float64, device=dev)
+        x = torch.empty(plan.n, dtype=torch.float64, device=dev)
+        info = {"it": [], "inner": []}
+
+        def s64(i):
+            plan.assemble(fields[i % 3], vals=vals, b=b)
+            plan.jacobi(vals, out=inv)
+            x.zero_()
+            info["it"].append(plan.pcg(vals, b, x, inv, tol=1e-8)[1])
+
+        def s32(i):
+            plan.assemble(fields[i % 3], vals=vals, b=b)
+            plan.jacobi(vals, out=inv)
+            x.zero_()
+            info["inner"].append(plan.pcg_mixed(vals, b, inv, x, tol=1e-8)[1])
+
+        base = {"workload": f"P{order} {nh}^2 triangles ({plan.ntet:,} triangles, {plan.n:,} DOF, {plan.nnz:,} nnz)"}
+        ms64 = timed(s64, 3, 1) / 3
+        out[f"tri_p{order}_{nh}_fp64"] = {**base, "value": world * plan.n / (ms64 / 1e3), "unit": "DOF/s",
+                                          "ms_per_step": ms64, "iters": float(np.mean(info["it"]))}
+        if order == 1:
+            ms32 = timed(s32, 3, 1) / 3
+            out[f"tri_p{order}_{nh}_mixed"] = {**base, "value": world * plan.n / (ms32 / 1e3), "unit": "DOF/s",
+                                               "ms_per_step": ms32, "inner_iters": float(np.mean(info["inner"])),
+                                               "speedup_vs_fp64": ms64 / ms32}
+        del plan
+    return out
+
+
 def batched_variant(dev, count=256, reps=3):
     """256 independent P1 problems, sides log-uniform in [8, 48] hexes (master seed 42), own jitter
     and lognormal k each: one assembly launch over the disjoint union + one persistent batched-PCG
@@ -646,6 +691,7 @@ def run_ours(args):
         variants["spmv_sell_fp64"] = {"GB/s": achieved, "frac_of_peak": achieved / peak, "ms_in_loop": sell_ms,
                                       "ms_standalone": sell_standalone_ms}
         variants.update(p2_variants(args, world, dev, timed))
+        variants.update(tri_variants(world, dev, timed))
         variants["adjoint_p1_64"] = adjoint_variant(dev)
         variants["batched_256"] = batched_variant(dev)
 

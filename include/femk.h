@@ -47,8 +47,8 @@ typedef struct femk_plan femk_plan;
 
 typedef struct femk_plan_info {
   int32_t order;      /* 1 or 2 */
-  int32_t ndof_local; /* 4 or 10 */
-  int64_t ntet;       /* elements */
+  int32_t ndof_local; /* 4 or 10 (tetrahedra), 3 or 6 (triangles) */
+  int64_t ntet;       /* elements (tetrahedra, or triangles on a 2-D plan) */
   int64_t nvert;      /* P1 vertices */
   int64_t n;          /* DOFs (rows) */
   int64_t nnz;        /* stored entries of the canonical CSR (= compress-plan nse) */
@@ -60,6 +60,7 @@ typedef struct femk_plan_info {
   int32_t tiles;       /* 1 when the plan built the staged-x tiles of the CG-step SpMV */
   int64_t sell_col_units; /* column entries the CG-step SpMV streams per product (int16 units when
                              cols16: per-slice tables, a shared-offset slice stored once) */
+  int32_t dim;            /* 2 (triangles) or 3 (tetrahedra) */
 } femk_plan_info;
 
 /* Library version (major*10000 + minor*100 + patch). */
@@ -85,6 +86,22 @@ const char* femk_last_error_string(void);
  */
 int femk_plan_create(const double* xyz_dev, int64_t nvert, const int32_t* tets_dev, int64_t ntet,
                      int order, const uint8_t* dirichlet_mask_dev, void* stream, femk_plan** out);
+
+/*
+ * femk_plan_create for a simplex mesh of either dimension:
+ *   dim 3: coords_dev f64[nvert*3], cells_dev i32[ncell*4] tetrahedra (= femk_plan_create);
+ *   dim 2: coords_dev f64[nvert*2] (x, y per vertex), cells_dev i32[ncell*3] triangles. P2 adds
+ *          one midpoint DOF per edge (basix triangle edge order (1,2),(0,2),(0,1),
+ *          jno/utils/solver/fem_topology.py:36); boundary facets are the edges owned by one triangle.
+ * The 2-D plan keeps 3 coordinates per node (z = 0): femk_plan_export writes points f64[n*3].
+ * Every other entry point takes a 2-D plan as it is (ndof_local 3 / 6); the nodal modes work on
+ * P1 triangles with the 3-point degree-2 rule. Replaces the dim == 2 branch of _get_mesh
+ * (jno/utils/solver/fem_native.py:218-288, pts[:, :dim]) over Geometries.equi_distant_rect
+ * (jno/domain/geometries.py:44-100) and the same pattern / facet steps as femk_plan_create.
+ */
+int femk_plan_create_simplex(const double* coords_dev, int dim, int64_t nvert, const int32_t* cells_dev,
+                             int64_t ncell, int order, const uint8_t* dirichlet_mask_dev, void* stream,
+                             femk_plan** out);
 
 int femk_plan_destroy(femk_plan* plan);
 

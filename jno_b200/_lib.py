@@ -58,6 +58,7 @@ class PlanInfo(ctypes.Structure):
         ("batch_graph", ctypes.c_int32),
         ("tiles", ctypes.c_int32),
         ("sell_col_units", ctypes.c_int64),
+        ("dim", ctypes.c_int32),
     ]
 
 
@@ -73,6 +74,7 @@ SIGNATURES = {
     "femk_kernel_launches": [],
     "femk_last_error_string": [],
     "femk_plan_create": [_P, _I64, _P, _I64, _I, _P, _P, ctypes.POINTER(_P)],
+    "femk_plan_create_simplex": [_P, _I, _I64, _P, _I64, _I, _P, _P, ctypes.POINTER(_P)],
     "femk_plan_destroy": [_P],
     "femk_plan_get_info": [_P, ctypes.POINTER(PlanInfo)],
     "femk_plan_export": [_P, _P, _P, _P, _P, _P, _P, _P, _P],

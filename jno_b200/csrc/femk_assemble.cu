@@ -27,9 +27,9 @@ __global__ void __launch_bounds__(kThreads) k_assemble(const double* __restrict_
     int32_t dof[ND];
 #pragma unroll
     for (int a = 0; a < ND; ++a) dof[a] = __ldg(cells + c * ND + a);
-    TetGeom T;
-    tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
-    double VG[4][4];
+    Geom<Cell<ND>::NV> T;
+    cell_geometry(xyz, dof, T);
+    double VG[Cell<ND>::NV][Cell<ND>::NV];
     gram(T, VG);
     const double k = coef_of(param, mode, scale, c);
     bool dir[ND];
@@ -56,11 +56,15 @@ __global__ void __launch_bounds__(kThreads) k_assemble(const double* __restrict_
 
 // k_e of a nodal P1 parameter (coef_nodal, unscaled) for every element: the kernels that take a
 // coefficient then read it as a P0 linear parameter (FEMK_COEF_LINEAR with the caller's scale)
-__global__ void k_nodal_coef(const int32_t* __restrict__ cells, int nd, int64_t ntet, const double* __restrict__ param,
+template <int NV>
+__global__ void k_nodal_coef(const int32_t* __restrict__ cells, int64_t ntet, const double* __restrict__ param,
                              int mode, double* __restrict__ ke) {
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x)
-    ke[c] = coef_nodal(param, mode, 1.0, __ldg(cells + c * nd), __ldg(cells + c * nd + 1), __ldg(cells + c * nd + 2),
-                       __ldg(cells + c * nd + 3));
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t v[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i] = __ldg(cells + c * NV + i);
+    ke[c] = coef_nodal<NV>(param, mode, 1.0, v);
+  }
 }
 
 __global__ void k_dirichlet_rows(const int32_t* __restrict__ dlist, int64_t nd, const int32_t* __restrict__ diag,
@@ -76,9 +80,12 @@ template <int ND>
 __global__ void k_element_matrices(const double* __restrict__ xyz, const int32_t* __restrict__ cells, int64_t ntet,
                                    double* __restrict__ khat_out, double* __restrict__ fhat_out) {
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
-    TetGeom T;
-    tet_geometry(xyz, cells[c * ND], cells[c * ND + 1], cells[c * ND + 2], cells[c * ND + 3], T);
-    double VG[4][4];
+    int32_t dof[Cell<ND>::NV];
+#pragma unroll
+    for (int a = 0; a < Cell<ND>::NV; ++a) dof[a] = cells[c * ND + a];
+    Geom<Cell<ND>::NV> T;
+    cell_geometry(xyz, dof, T);
+    double VG[Cell<ND>::NV][Cell<ND>::NV];
     gram(T, VG);
     if (khat_out) {
 #pragma unroll
@@ -101,8 +108,8 @@ __global__ void k_lumped_mass(const double* __restrict__ xyz, const int32_t* __r
     int32_t dof[ND];
 #pragma unroll
     for (int a = 0; a < ND; ++a) dof[a] = cells[c * ND + a];
-    TetGeom T;
-    tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
+    Geom<Cell<ND>::NV> T;
+    cell_geometry(xyz, dof, T);
 #pragma unroll
     for (int a = 0; a < ND; ++a) atomicAdd(m + dof[a], fhat<ND>(T.vol, a));
   }
@@ -123,9 +130,9 @@ __global__ void k_adjoint(const double* __restrict__ xyz, const int32_t* __restr
       ue[a] = d ? 0.0 : __ldg(u + dof[a]);
       le[a] = d ? 0.0 : __ldg(lam + dof[a]);
     }
-    TetGeom T;
-    tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
-    double VG[4][4];
+    Geom<Cell<ND>::NV> T;
+    cell_geometry(xyz, dof, T);
+    double VG[Cell<ND>::NV][Cell<ND>::NV];
     gram(T, VG);
     double acc = 0.0;
 #pragma unroll
@@ -140,54 +147,57 @@ __global__ void k_adjoint(const double* __restrict__ xyz, const int32_t* __restr
   }
 }
 
-// Nodal P1 parameter: the element's dJ/dk_e = -(m o lam)^T K_hat (m o u) spread onto its four
-// vertex values by dk_e/dp_i (linear: scale / 4; exp with the 4-point rule, L_q = a S + (b - a) p_q:
-// scale / 4 * (a sum_q exp(L_q) + (b - a) exp(L_i))). grad f64[nvert] must start at zero.
+// Nodal P1 parameter: the element's dJ/dk_e = -(m o lam)^T K_hat (m o u) spread onto its NV
+// vertex values by dk_e/dp_i (linear: scale / NV; exp with the degree-2 rule, L_q = a S + (b - a) p_q:
+// scale / NV * (a sum_q exp(L_q) + (b - a) exp(L_i))). grad f64[nvert] must start at zero.
+template <int NV>
 __global__ void k_adjoint_nodal(const double* __restrict__ xyz, const int32_t* __restrict__ cells, int64_t ntet,
                                 const uint8_t* __restrict__ dmask, const double* __restrict__ param, int mode,
                                 double scale, const double* __restrict__ u, const double* __restrict__ lam,
                                 double* __restrict__ grad) {
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
-    int32_t dof[4];
-    double ue[4], le[4], pv[4];
+    int32_t dof[NV];
+    double ue[NV], le[NV], pv[NV];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      dof[a] = __ldg(cells + c * 4 + a);
+    for (int a = 0; a < NV; ++a) {
+      dof[a] = __ldg(cells + c * NV + a);
       const bool d = __ldg(dmask + dof[a]) != 0;
       ue[a] = d ? 0.0 : __ldg(u + dof[a]);
       le[a] = d ? 0.0 : __ldg(lam + dof[a]);
       pv[a] = __ldg(param + dof[a]);
     }
-    TetGeom T;
-    tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
-    double VG[4][4];
+    Geom<NV> T;
+    cell_geometry(xyz, dof, T);
+    double VG[NV][NV];
     gram(T, VG);
     double acc = 0.0;
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
+    for (int a = 0; a < NV; ++a) {
       double row = 0.0;
 #pragma unroll
-      for (int bb = 0; bb < 4; ++bb) row += khat<4>(VG, a, bb) * ue[bb];
+      for (int bb = 0; bb < NV; ++bb) row += khat<NV>(VG, a, bb) * ue[bb];
       acc += le[a] * row;
     }
-    double dk[4];
+    double dk[NV];
     if (mode == FEMK_COEF_NODAL_LINEAR) {
 #pragma unroll
-      for (int i = 0; i < 4; ++i) dk[i] = 0.25 * scale;
+      for (int i = 0; i < NV; ++i) dk[i] = NodalRule<NV>::w * scale;
     } else {
-      constexpr double qa = 0.13819660112501051518, qb = 0.58541019662496845446;
-      const double S = pv[0] + pv[1] + pv[2] + pv[3];
-      double e[4], es = 0.0;
+      constexpr double qa = NodalRule<NV>::a, qb = NodalRule<NV>::b;
+      double S = 0.0;
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
+      for (int i = 0; i < NV; ++i) S += pv[i];
+      double e[NV], es = 0.0;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
         e[i] = exp(qa * S + (qb - qa) * pv[i]);
         es += e[i];
       }
 #pragma unroll
-      for (int i = 0; i < 4; ++i) dk[i] = 0.25 * scale * (qa * es + (qb - qa) * e[i]);
+      for (int i = 0; i < NV; ++i) dk[i] = NodalRule<NV>::w * scale * (qa * es + (qb - qa) * e[i]);
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i) atomicAdd(grad + dof[i], -acc * dk[i]);
+    for (int i = 0; i < NV; ++i) atomicAdd(grad + dof[i], -acc * dk[i]);
   }
 }
 
@@ -203,8 +213,11 @@ int resolve_coef(const femk_plan* pc, const double* param, int mode, cudaStream_
   if (mode != FEMK_COEF_NODAL_EXP && mode != FEMK_COEF_NODAL_LINEAR) return FEMK_OK;
   femk_plan* p = const_cast<femk_plan*>(pc);
   if (!p->coef_tmp) FEMK_CUDA_TRY(cudaMalloc(&p->coef_tmp, sizeof(double) * (p->ntet > 0 ? p->ntet : 1)));
-  k_nodal_coef<<<counted_launch() + blocks_for(p->ntet, 256, p->n_sm * 16), 256, 0, s>>>(p->cells, p->nd, p->ntet,
-                                                                                       param, mode, p->coef_tmp);
+  const int grid = blocks_for(p->ntet, 256, p->n_sm * 16);
+  if (p->nd == 3)
+    k_nodal_coef<3><<<counted_launch() + grid, 256, 0, s>>>(p->cells, p->ntet, param, mode, p->coef_tmp);
+  else
+    k_nodal_coef<4><<<counted_launch() + grid, 256, 0, s>>>(p->cells, p->ntet, param, mode, p->coef_tmp);
   FEMK_CUDA_TRY(cudaGetLastError());
   *param_out = p->coef_tmp;
   *mode_out = FEMK_COEF_LINEAR;
@@ -226,10 +239,7 @@ extern "C" int femk_assemble(const femk_plan* p, const double* param, int mode, 
   if (vals) FEMK_CUDA_TRY(cudaMemsetAsync(vals, 0, sizeof(double) * p->nnz, s));
   FEMK_CUDA_TRY(cudaMemsetAsync(b, 0, sizeof(double) * p->n, s));
   const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);
-  if (p->nd == 4)
-    k_assemble<4><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->slot, p->dmask, param, mode, scale, f, g, vals, b);
-  else
-    k_assemble<10><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->slot, p->dmask, param, mode, scale, f, g, vals, b);
+  FEMK_BY_ND(p->nd, k_assemble<ND><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->slot, p->dmask, param, mode, scale, f, g, vals, b));
   FEMK_CUDA_TRY(cudaGetLastError());
   if (p->n_dir > 0) {
     k_dirichlet_rows<<<::femk::counted_launch() + blocks_for(p->n_dir, 256, 65535), 256, 0, s>>>(p->dlist, p->n_dir, p->diag, g, vals, b);
@@ -243,10 +253,7 @@ extern "C" int femk_element_matrices(const femk_plan* p, double* khat_out, doubl
   FEMK_CHECK_ARG(p, "femk_element_matrices: NULL plan");
   cudaStream_t s = (cudaStream_t)stream;
   const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);
-  if (p->nd == 4)
-    k_element_matrices<4><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, khat_out, fhat_out);
-  else
-    k_element_matrices<10><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, khat_out, fhat_out);
+  FEMK_BY_ND(p->nd, k_element_matrices<ND><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, khat_out, fhat_out));
   FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;
 }
@@ -257,10 +264,7 @@ extern "C" int femk_lumped_mass(const femk_plan* p, double* mass, void* stream) 
   cudaStream_t s = (cudaStream_t)stream;
   FEMK_CUDA_TRY(cudaMemsetAsync(mass, 0, sizeof(double) * p->n, s));
   const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);
-  if (p->nd == 4)
-    k_lumped_mass<4><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, mass);
-  else
-    k_lumped_mass<10><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, mass);
+  FEMK_BY_ND(p->nd, k_lumped_mass<ND><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, mass));
   FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;
 }
@@ -278,15 +282,16 @@ extern "C" int femk_adjoint_grad(const femk_plan* p, const double* param, int mo
   const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);
   if (mode == FEMK_COEF_NODAL_EXP || mode == FEMK_COEF_NODAL_LINEAR) {
     FEMK_CUDA_TRY(cudaMemsetAsync(grad, 0, sizeof(double) * p->nvert, s));
-    k_adjoint_nodal<<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param,
-                                                                         mode, scale, u, lam, grad);
+    if (p->nd == 3)
+      k_adjoint_nodal<3><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask,
+                                                                              param, mode, scale, u, lam, grad);
+    else
+      k_adjoint_nodal<4><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask,
+                                                                              param, mode, scale, u, lam, grad);
     FEMK_CUDA_TRY(cudaGetLastError());
     return FEMK_OK;
   }
-  if (p->nd == 4)
-    k_adjoint<4><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param, mode, scale, u, lam, grad);
-  else
-    k_adjoint<10><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param, mode, scale, u, lam, grad);
+  FEMK_BY_ND(p->nd, k_adjoint<ND><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param, mode, scale, u, lam, grad));
   FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;
 }

@@ -721,9 +721,9 @@ __global__ void __launch_bounds__(128) k_matfree(const double* __restrict__ xyz,
       dir[a] = __ldg(dmask + dof[a]) != 0;
       xe[a] = dir[a] ? 0.0 : __ldg(x + dof[a]);
     }
-    TetGeom T;
-    tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
-    double VG[4][4];
+    Geom<Cell<ND>::NV> T;
+    cell_geometry(xyz, dof, T);
+    double VG[Cell<ND>::NV][Cell<ND>::NV];
     gram(T, VG);
     const double k = coef_of(param, mode, scale, c);
 #pragma unroll
@@ -754,9 +754,9 @@ __global__ void k_matfree_diag(const double* __restrict__ xyz, const int32_t* __
     int32_t dof[ND];
 #pragma unroll
     for (int a = 0; a < ND; ++a) dof[a] = __ldg(cells + c * ND + a);
-    TetGeom T;
-    tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], T);
-    double VG[4][4];
+    Geom<Cell<ND>::NV> T;
+    cell_geometry(xyz, dof, T);
+    double VG[Cell<ND>::NV][Cell<ND>::NV];
     gram(T, VG);
     const double k = coef_of(param, mode, scale, c);
 #pragma unroll
@@ -1086,10 +1086,7 @@ int launch_matfree(const femk_plan* p, const MatFree& m, const double* x, double
                    const CgState* st = nullptr) {
   k_zero<<<::femk::counted_launch() + p->n_sm * 8, 256, 0, s>>>(y, p->n, st);
   const int grid = blocks_for(p->ntet, 128, p->n_sm * 16);
-  if (p->nd == 4)
-    k_matfree<4><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, m.param, m.mode, m.scale, x, y, st);
-  else
-    k_matfree<10><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, m.param, m.mode, m.scale, x, y, st);
+  FEMK_BY_ND(p->nd, k_matfree<ND><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, m.param, m.mode, m.scale, x, y, st));
   FEMK_CUDA_TRY(cudaGetLastError());
   if (p->n_dir > 0) {
     k_dirichlet_identity<<<::femk::counted_launch() + blocks_for(p->n_dir, 256, 65535), 256, 0, s>>>(p->dlist, p->n_dir, x, y, st);
@@ -1494,10 +1491,7 @@ extern "C" int femk_jacobi_matfree(const femk_plan* p, const double* param, int 
   FEMK_TRY(resolve_coef(p, param, mode, s, &param, &mode));
   FEMK_CUDA_TRY(cudaMemsetAsync(inv, 0, sizeof(double) * p->n, s));
   const int grid = blocks_for(p->ntet, 128, p->n_sm * 16);
-  if (p->nd == 4)
-    k_matfree_diag<4><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param, mode, scale, inv);
-  else
-    k_matfree_diag<10><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param, mode, scale, inv);
+  FEMK_BY_ND(p->nd, k_matfree_diag<ND><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param, mode, scale, inv));
   k_invert_diag<<<::femk::counted_launch() + blocks_for(p->n, 256, p->n_sm * 8), 256, 0, s>>>(inv, p->n, p->dmask);
   FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;

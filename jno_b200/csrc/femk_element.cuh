@@ -1,10 +1,15 @@
 // Per-element geometry and closed-form P1/P2 stiffness entries (device, FP64).
 //
-// Affine map of jno/utils/solver/fem_native.py:1480-1497: J = [x1-x0, x2-x0, x3-x0] (columns),
+// Affine map of jno/utils/solver/fem_native.py:1480-1497: J = [x1-x0, ..., x_dim-x0] (columns),
 // meas = |det J|, grad phi = dphi/dxi . J^-1. The rows of J^-1 are the barycentric gradients
-// g1..g3 (g0 = -(g1+g2+g3)); they are formed from the adjugate (cross products of the edges).
-// Stiffness entries are the exact integrals of k grad phi_b . grad phi_a (the reference uses basix
-// quadrature of degree 2 (P1) / 4 (P2), exact for these degree <= 2 integrands).
+// g1..g_dim (g0 = -(g1+...+g_dim)); they are formed from the adjugate (cross products of the edges
+// of a tetrahedron, rotated edges of a triangle). Stiffness entries are the exact integrals of
+// k grad phi_b . grad phi_a (the reference uses basix quadrature of degree 2 (P1) / 4 (P2), exact
+// for these degree <= 2 integrands). Coordinates are stored x, y, z per vertex; a triangle reads
+// x and y.
+//
+// An element is named by its local dof count ND: 3 / 6 = P1 / P2 triangle, 4 / 10 = P1 / P2
+// tetrahedron (basix dof order: the vertices, then one midpoint per edge).
 #pragma once
 
 #include "../../include/femk.h"
@@ -13,16 +18,36 @@
 
 namespace femk {
 
+template <int ND>
+struct Cell {
+  static constexpr int NV = (ND == 3 || ND == 6) ? 3 : 4;  // vertices
+  static constexpr int DIM = NV - 1;
+  static constexpr bool P2 = ND == 6 || ND == 10;
+};
+
 // basix P2 tetrahedron edge order (jno/utils/solver/fem_topology.py:44):
 // (2,3),(1,3),(1,2),(0,3),(0,2),(0,1)
 __host__ __device__ constexpr int edge_a(int e) { return e == 0 ? 2 : (e <= 2 ? 1 : 0); }
 __host__ __device__ constexpr int edge_b(int e) { return e == 0 || e == 1 || e == 3 ? 3 : (e == 2 || e == 4 ? 2 : 1); }
+// basix P2 triangle edge order (jno/utils/solver/fem_topology.py:36): (1,2),(0,2),(0,1)
+__host__ __device__ constexpr int tri_edge_a(int e) { return e == 0 ? 1 : 0; }
+__host__ __device__ constexpr int tri_edge_b(int e) { return e == 2 ? 1 : 2; }
+template <int NV>
+__host__ __device__ constexpr int cell_edge_a(int e) {
+  return NV == 3 ? tri_edge_a(e) : edge_a(e);
+}
+template <int NV>
+__host__ __device__ constexpr int cell_edge_b(int e) {
+  return NV == 3 ? tri_edge_b(e) : edge_b(e);
+}
 
-struct TetGeom {
-  double g[4][3];  // barycentric gradients
-  double vol;      // |det J| / 6
-  double det;      // signed det J
+template <int NV>
+struct Geom {
+  double g[NV][NV - 1];  // barycentric gradients
+  double vol;            // element measure: |det J| / 6 (tetrahedron), |det J| / 2 (triangle)
+  double det;            // signed det J
 };
+using TetGeom = Geom<4>;
 
 __device__ __forceinline__ void tet_geometry(const double* __restrict__ xyz, int32_t v0, int32_t v1, int32_t v2,
                                              int32_t v3, TetGeom& G) {
@@ -50,42 +75,85 @@ __device__ __forceinline__ void tet_geometry(const double* __restrict__ xyz, int
   G.vol = fabs(det) * (1.0 / 6.0);
 }
 
-// Gram matrix of the barycentric gradients, scaled by the volume: VG[i][j] = V g_i . g_j
-__device__ __forceinline__ void gram(const TetGeom& T, double VG[4][4]) {
+__device__ __forceinline__ void tri_geometry(const double* __restrict__ xyz, int32_t v0, int32_t v1, int32_t v2,
+                                             Geom<3>& G) {
+  const double x0 = __ldg(xyz + (int64_t)v0 * 3), y0 = __ldg(xyz + (int64_t)v0 * 3 + 1);
+  const double e1x = __ldg(xyz + (int64_t)v1 * 3) - x0, e1y = __ldg(xyz + (int64_t)v1 * 3 + 1) - y0;
+  const double e2x = __ldg(xyz + (int64_t)v2 * 3) - x0, e2y = __ldg(xyz + (int64_t)v2 * 3 + 1) - y0;
+  const double det = e1x * e2y - e1y * e2x;
+  const double inv = 1.0 / det;
+  G.g[1][0] = e2y * inv;
+  G.g[1][1] = -e2x * inv;
+  G.g[2][0] = -e1y * inv;
+  G.g[2][1] = e1x * inv;
+  G.g[0][0] = -(G.g[1][0] + G.g[2][0]);
+  G.g[0][1] = -(G.g[1][1] + G.g[2][1]);
+  G.det = det;
+  G.vol = fabs(det) * 0.5;
+}
+
+// geometry of the element whose first NV local dofs (its vertices) are dof[0..NV)
+__device__ __forceinline__ void cell_geometry(const double* __restrict__ xyz, const int32_t* dof, Geom<4>& G) {
+  tet_geometry(xyz, dof[0], dof[1], dof[2], dof[3], G);
+}
+__device__ __forceinline__ void cell_geometry(const double* __restrict__ xyz, const int32_t* dof, Geom<3>& G) {
+  tri_geometry(xyz, dof[0], dof[1], dof[2], G);
+}
+
+// Gram matrix of the barycentric gradients, scaled by the measure: VG[i][j] = V g_i . g_j
+template <int NV>
+__device__ __forceinline__ void gram(const Geom<NV>& T, double VG[NV][NV]) {
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < NV; ++i)
 #pragma unroll
-    for (int j = i; j < 4; ++j) {
-      const double v = T.vol * (T.g[i][0] * T.g[j][0] + T.g[i][1] * T.g[j][1] + T.g[i][2] * T.g[j][2]);
+    for (int j = i; j < NV; ++j) {
+      double d = T.g[i][0] * T.g[j][0];
+#pragma unroll
+      for (int k = 1; k < NV - 1; ++k) d += T.g[i][k] * T.g[j][k];
+      const double v = T.vol * d;
       VG[i][j] = v;
       VG[j][i] = v;
     }
 }
 
 // Unit-coefficient stiffness entry K_hat[a][b] from the scaled Gram matrix (a, b compile-time).
+// P2 basis: phi_i = lambda_i (2 lambda_i - 1), phi_e = 4 lambda_j lambda_l on edge e = (j, l); with
+// int lambda_i lambda_j = V (1 + delta_ij) / ((d+1)(d+2)) and int lambda_i = V / (d+1) in d dims.
 template <int ND>
-__device__ __forceinline__ double khat(const double VG[4][4], int a, int b) {
-  if (ND == 4) return VG[a][b];
-  if (a < 4 && b < 4) return VG[a][b] * (a == b ? 0.6 : -0.2);
-  if (a >= 4 && b >= 4) {
-    const int i = edge_a(a - 4), j = edge_b(a - 4), l = edge_a(b - 4), m = edge_b(b - 4);
-    return 0.8 * (VG[i][l] * (1 + (j == m)) + VG[i][m] * (1 + (j == l)) + VG[j][l] * (1 + (i == m)) +
-                  VG[j][m] * (1 + (i == l)));
+__device__ __forceinline__ double khat(const double VG[Cell<ND>::NV][Cell<ND>::NV], int a, int b) {
+  constexpr int NV = Cell<ND>::NV;
+  if (!Cell<ND>::P2) return VG[a][b];
+  // tetrahedron / triangle moments of the P2 gradient products
+  constexpr double vv_d = NV == 4 ? 0.6 : 1.0;          // int (4 l_i - 1)^2 / V
+  constexpr double vv_o = NV == 4 ? -0.2 : -1.0 / 3.0;  // int (4 l_i - 1)(4 l_j - 1) / V
+  constexpr double ee = NV == 4 ? 0.8 : 4.0 / 3.0;      // 16 int l_a l_b / V for a != b
+  constexpr double ve_d = NV == 4 ? 0.15 : 1.0 / 3.0;   // int (4 l_i - 1) l_i / V
+  constexpr double ve_o = NV == 4 ? -0.05 : 0.0;        // int (4 l_i - 1) l_l / V, l != i
+  if (a < NV && b < NV) return VG[a][b] * (a == b ? vv_d : vv_o);
+  if (a >= NV && b >= NV) {
+    const int i = cell_edge_a<NV>(a - NV), j = cell_edge_b<NV>(a - NV);
+    const int l = cell_edge_a<NV>(b - NV), m = cell_edge_b<NV>(b - NV);
+    return ee * (VG[i][l] * (1 + (j == m)) + VG[i][m] * (1 + (j == l)) + VG[j][l] * (1 + (i == m)) +
+                 VG[j][m] * (1 + (i == l)));
   }
   // vertex i against edge (j, l)
-  const int i = a < 4 ? a : b;
-  const int e = a < 4 ? b - 4 : a - 4;
-  const int j = edge_a(e), l = edge_b(e);
-  const double cil = i == l ? 0.15 : -0.05;
-  const double cij = i == j ? 0.15 : -0.05;
+  const int i = a < NV ? a : b;
+  const int e = a < NV ? b - NV : a - NV;
+  const int j = cell_edge_a<NV>(e), l = cell_edge_b<NV>(e);
+  const double cil = i == l ? ve_d : ve_o;
+  const double cij = i == j ? ve_d : ve_o;
   return 4.0 * (VG[i][j] * cil + VG[i][l] * cij);
 }
 
-// Unit-source load integral(phi_a)
+// Unit-source load integral(phi_a): P1 V / (d+1); P2 vertex V (2 - d) / ((d+1)(d+2)), edge
+// 4 V / ((d+1)(d+2)) (a triangle's P2 vertex functions integrate to exactly 0)
 template <int ND>
 __device__ __forceinline__ double fhat(double vol, int a) {
+  constexpr int NV = Cell<ND>::NV;
   if (ND == 4) return 0.25 * vol;
-  return a < 4 ? -0.05 * vol : 0.2 * vol;
+  if (ND == 3) return vol * (1.0 / 3.0);
+  if (NV == 4) return a < 4 ? -0.05 * vol : 0.2 * vol;
+  return a < 3 ? 0.0 : vol * (1.0 / 3.0);
 }
 
 __device__ __forceinline__ double coef_of(const double* __restrict__ param, int mode, double scale, int64_t c) {
@@ -97,19 +165,33 @@ __device__ __forceinline__ double coef_of(const double* __restrict__ param, int 
 // Element coefficient of a nodal P1 parameter (one value per P1 vertex, interpolated linearly).
 // P1 stiffness integrands are constant on an element, so K_e = V G * mean_q k(x_q):
 //  * linear k (FEMK_COEF_NODAL_LINEAR): the quadrature mean of a linear field is the vertex mean;
-//  * exp of a linear log-field (FEMK_COEF_NODAL_EXP): the symmetric 4-point degree-2 tetrahedron
-//    rule (points with barycentric coordinates (b, a, a, a) and its permutations,
-//    a = (5 - sqrt 5) / 20, b = (5 + 3 sqrt 5) / 20, equal weights), the rule for quadrature degree 2
-//    that P1 forms are integrated with (jno/_fem.py:4551).
-__device__ __forceinline__ double coef_nodal(const double* __restrict__ param, int mode, double scale, int32_t v0,
-                                             int32_t v1, int32_t v2, int32_t v3) {
-  const double p0 = __ldg(param + v0), p1 = __ldg(param + v1), p2 = __ldg(param + v2), p3 = __ldg(param + v3);
-  if (mode == FEMK_COEF_NODAL_LINEAR) return scale * (0.25 * (p0 + p1 + p2 + p3));
-  constexpr double a = 0.13819660112501051518, b = 0.58541019662496845446;
-  const double s = p0 + p1 + p2 + p3;
-  const double e = exp(a * s + (b - a) * p0) + exp(a * s + (b - a) * p1) + exp(a * s + (b - a) * p2) +
-                   exp(a * s + (b - a) * p3);
-  return scale * (0.25 * e);
+//  * exp of a linear log-field (FEMK_COEF_NODAL_EXP): the symmetric degree-2 rule, the rule for
+//    quadrature degree 2 that P1 forms are integrated with (jno/_fem.py:4551) -- on a tetrahedron
+//    4 points with barycentric coordinates (b, a, a, a) and permutations, a = (5 - sqrt 5) / 20,
+//    b = (5 + 3 sqrt 5) / 20; on a triangle 3 points (2/3, 1/6, 1/6) and permutations; equal weights.
+//    Point q has L_q = a S + (b - a) p_q, S the vertex sum.
+template <int NV>
+struct NodalRule {
+  static constexpr double a = NV == 4 ? 0.13819660112501051518 : 1.0 / 6.0;
+  static constexpr double b = NV == 4 ? 0.58541019662496845446 : 2.0 / 3.0;
+  static constexpr double w = 1.0 / NV;  // weight of a point in the mean
+};
+
+template <int NV>
+__device__ __forceinline__ double coef_nodal(const double* __restrict__ param, int mode, double scale,
+                                             const int32_t* v) {
+  double p[NV], s = 0.0;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    p[i] = __ldg(param + v[i]);
+    s += p[i];
+  }
+  if (mode == FEMK_COEF_NODAL_LINEAR) return scale * (NodalRule<NV>::w * s);
+  constexpr double a = NodalRule<NV>::a, b = NodalRule<NV>::b;
+  double e = 0.0;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) e += exp(a * s + (b - a) * p[i]);
+  return scale * (NodalRule<NV>::w * e);
 }
 
 }  // namespace femk

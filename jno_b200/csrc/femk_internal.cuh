@@ -54,6 +54,30 @@ inline bool coef_mode_ok(const femk_plan* p, int mode, const double* param);
     if (_s != FEMK_OK) return _s; \
   } while (0)
 
+// Runs the statement with the constant ND bound to a plan's local dof count: 3 / 6 = P1 / P2
+// triangle, 4 / 10 = P1 / P2 tetrahedron.
+#define FEMK_BY_ND(nd, ...)                \
+  do {                                     \
+    switch (nd) {                          \
+      case 3: {                            \
+        constexpr int ND = 3;              \
+        __VA_ARGS__;                       \
+      } break;                             \
+      case 6: {                            \
+        constexpr int ND = 6;              \
+        __VA_ARGS__;                       \
+      } break;                             \
+      case 4: {                            \
+        constexpr int ND = 4;              \
+        __VA_ARGS__;                       \
+      } break;                             \
+      default: {                           \
+        constexpr int ND = 10;             \
+        __VA_ARGS__;                       \
+      } break;                             \
+    }                                      \
+  } while (0)
+
 // Device-side solver scalars of one CG run. Lives in plan-owned device memory.
 struct CgState {
   double gamma;     // <r, z>
@@ -80,9 +104,10 @@ struct CgState {
 struct femk_plan {
   int device = 0;
   int order = 1, nd = 4;
-  int64_t ntet = 0, nvert = 0, n = 0, nnz = 0, n_dir = 0;
+  int dim = 3, nv = 4;  // spatial dimension, vertices per element (triangles: 2, 3)
+  int64_t ntet = 0, nvert = 0, n = 0, nnz = 0, n_dir = 0;  // ntet: elements (tetrahedra or triangles)
   // pattern (plan-owned device memory)
-  double* xyz = nullptr;        // f64[nvert*3] P1 vertex coordinates
+  double* xyz = nullptr;        // f64[nvert*3] P1 vertex coordinates (z = 0 in 2-D)
   double* points = nullptr;     // f64[n*3] DOF coordinates
   int32_t* cells = nullptr;     // i32[ntet*nd]
   int32_t* indptr = nullptr;    // i32[n+1]

@@ -17,6 +17,7 @@
 #include <thread>
 #include <vector>
 
+#include "femk_element.cuh"
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
 #include "femk_tile.cuh"
@@ -24,10 +25,24 @@
 namespace femk {
 namespace {
 
-__constant__ int c_edge[6][2] = {{2, 3}, {1, 3}, {1, 2}, {0, 3}, {0, 2}, {0, 1}};
-__constant__ int c_face[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
-// local edge index of the vertex pair (i, j); -1 on the diagonal
-__constant__ int c_edge_of[4][4] = {{-1, 5, 4, 3}, {5, -1, 2, 1}, {4, 2, -1, 0}, {3, 1, 0, -1}};
+// Simplex topology: NV vertices, NE = NV (NV - 1) / 2 edges in basix order (cell_edge_a/b), and
+// NV facets, facet f being the NV - 1 vertices other than f (the facet set of a tetrahedron /
+// triangle; only the set matters to the boundary test).
+template <int NV>
+__host__ __device__ constexpr int n_edges() {
+  return NV * (NV - 1) / 2;
+}
+// local edge index of the vertex pair (i, j), i != j
+template <int NV>
+__device__ __forceinline__ int local_edge(int i, int j) {
+  int found = 0;
+#pragma unroll
+  for (int e = 0; e < n_edges<NV>(); ++e) {
+    const int a = cell_edge_a<NV>(e), b = cell_edge_b<NV>(e);
+    if ((a == i && b == j) || (a == j && b == i)) found = e;
+  }
+  return found;
+}
 
 constexpr int kThreads = 256;
 
@@ -43,17 +58,22 @@ __global__ void k_count(const int32_t* __restrict__ cells, int64_t m, int64_t n,
   }
 }
 
-// Connectivity check before any kernel indexes with it: every id in [0, nvert) and the four
-// vertices of a tet pairwise distinct. Reads tets only; writes the error flag.
-__global__ void k_validate_tets(const int32_t* __restrict__ tets, int64_t ntet, int64_t nvert, int* __restrict__ err) {
+// Connectivity check before any kernel indexes with it: every id in [0, nvert) and the NV
+// vertices of an element pairwise distinct. Reads the cells only; writes the error flag.
+template <int NV>
+__global__ void k_validate_cells(const int32_t* __restrict__ tets, int64_t ntet, int64_t nvert,
+                                 int* __restrict__ err) {
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
-    int32_t v[4];
+    int32_t v[NV];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) v[q] = tets[c * 4 + q];
+    for (int q = 0; q < NV; ++q) v[q] = tets[c * NV + q];
     bool bad = false;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) bad |= v[q] < 0 || v[q] >= nvert;
-    bad |= v[0] == v[1] || v[0] == v[2] || v[0] == v[3] || v[1] == v[2] || v[1] == v[3] || v[2] == v[3];
+    for (int q = 0; q < NV; ++q) {
+      bad |= v[q] < 0 || v[q] >= nvert;
+#pragma unroll
+      for (int r = q + 1; r < NV; ++r) bad |= v[q] == v[r];
+    }
     if (bad) atomicOr(err, 1);
   }
 }
@@ -91,27 +111,29 @@ __global__ void k_sort_lists(const int32_t* __restrict__ ptr, int64_t n, int32_t
   }
 }
 
-// For every (cell, local edge): the raw index c'*6+e' of the first cell containing the same edge.
+// For every (cell, local edge): the raw index c'*NE+e' of the first cell containing the same edge.
+template <int NV>
 __global__ void k_edge_first(const int32_t* __restrict__ tets, int64_t ntet, const int32_t* __restrict__ vptr,
                              const int32_t* __restrict__ vinc, int32_t* __restrict__ first_raw,
                              int64_t* __restrict__ is_first, int* __restrict__ err) {
-  const int64_t m = ntet * 6;
+  constexpr int NE = n_edges<NV>();
+  const int64_t m = ntet * NE;
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t c = r / 6;
-    const int e = (int)(r % 6);
-    const int32_t a = tets[c * 4 + c_edge[e][0]], b = tets[c * 4 + c_edge[e][1]];
+    const int64_t c = r / NE;
+    const int e = (int)(r % NE);
+    const int32_t a = tets[c * NV + cell_edge_a<NV>(e)], b = tets[c * NV + cell_edge_b<NV>(e)];
     const int32_t u = min(a, b), w = max(a, b);
     int64_t found = -1;
     for (int32_t j = vptr[u]; j < vptr[u + 1] && found < 0; ++j) {
       const int32_t c2 = vinc[j];
       int iu = -1, iw = -1;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int32_t t = tets[(int64_t)c2 * 4 + q];
+      for (int q = 0; q < NV; ++q) {
+        const int32_t t = tets[(int64_t)c2 * NV + q];
         if (t == u) iu = q;
         if (t == w) iw = q;
       }
-      if (iw >= 0 && iu >= 0) found = (int64_t)c2 * 6 + c_edge_of[iu][iw];
+      if (iw >= 0 && iu >= 0) found = (int64_t)c2 * NE + local_edge<NV>(iu, iw);
     }
     if (found < 0) {
       atomicOr(err, 2);
@@ -122,19 +144,23 @@ __global__ void k_edge_first(const int32_t* __restrict__ tets, int64_t ntet, con
   }
 }
 
+// P2 connectivity (vertices, then the edge midpoints numbered by first encounter) and midpoint
+// coordinates; xyz and points hold 3 coordinates per node.
+template <int NV>
 __global__ void k_p2_cells(const int32_t* __restrict__ tets, int64_t ntet, int64_t nvert,
                            const int32_t* __restrict__ first_raw, const int64_t* __restrict__ rank,
                            const double* __restrict__ xyz, int32_t* __restrict__ cells, double* __restrict__ points) {
-  const int64_t m = ntet * 6;
+  constexpr int NE = n_edges<NV>(), ND = NV + NE;
+  const int64_t m = ntet * NE;
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t c = r / 6;
-    const int e = (int)(r % 6);
+    const int64_t c = r / NE;
+    const int e = (int)(r % NE);
     const int64_t fr = first_raw[r];
     const int64_t id = nvert + rank[fr];
-    cells[c * 10 + 4 + e] = (int32_t)id;
-    if (e < 4) cells[c * 10 + e] = tets[c * 4 + e];
+    cells[c * ND + NV + e] = (int32_t)id;
+    if (e < NV) cells[c * ND + e] = tets[c * NV + e];  // NE >= NV
     if (fr == r) {
-      const int32_t a = tets[c * 4 + c_edge[e][0]], b = tets[c * 4 + c_edge[e][1]];
+      const int32_t a = tets[c * NV + cell_edge_a<NV>(e)], b = tets[c * NV + cell_edge_b<NV>(e)];
 #pragma unroll
       for (int k = 0; k < 3; ++k) points[id * 3 + k] = 0.5 * xyz[(int64_t)a * 3 + k] + 0.5 * xyz[(int64_t)b * 3 + k];
     }
@@ -221,40 +247,45 @@ __global__ void k_diag_slot(const int32_t* __restrict__ indptr, const int32_t* _
   }
 }
 
-// A facet is on the boundary when no other tet has all three of its vertices.
+// A facet (the NV - 1 vertices other than vertex f) is on the boundary when no other element has
+// all of its vertices; P2 marks the midpoints of the facet's edges too.
 template <int ND>
 __global__ void k_boundary(const int32_t* __restrict__ cells, int64_t ntet, const int32_t* __restrict__ vptr,
                            const int32_t* __restrict__ vinc, uint8_t* __restrict__ mask) {
-  const int64_t m = ntet * 4;
+  constexpr int NV = Cell<ND>::NV;
+  const int64_t m = ntet * NV;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t c = t / 4;
-    const int f = (int)(t % 4);
-    int32_t v0 = cells[c * ND + c_face[f][0]], v1 = cells[c * ND + c_face[f][1]], v2 = cells[c * ND + c_face[f][2]];
-    const int32_t lo = min(v0, min(v1, v2));
+    const int64_t c = t / NV;
+    const int f = (int)(t % NV);
+    int32_t v[NV - 1];
+    int32_t lo = INT_MAX;
+#pragma unroll
+    for (int q = 0, k = 0; q < NV; ++q)
+      if (q != f) {
+        v[k] = cells[c * ND + q];
+        lo = min(lo, v[k]);
+        ++k;
+      }
     bool shared = false;
     for (int32_t j = vptr[lo]; j < vptr[lo + 1] && !shared; ++j) {
       const int32_t c2 = vinc[j];
       if (c2 == c) continue;
       int hit = 0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < NV; ++q) {
         const int32_t w = cells[(int64_t)c2 * ND + q];
-        hit += (w == v0) + (w == v1) + (w == v2);
+#pragma unroll
+        for (int k = 0; k < NV - 1; ++k) hit += w == v[k];
       }
-      shared = hit == 3;
+      shared = hit == NV - 1;
     }
     if (shared) continue;
-    mask[v0] = 1;
-    mask[v1] = 1;
-    mask[v2] = 1;
-    if (ND == 10) {
 #pragma unroll
-      for (int e = 0; e < 6; ++e) {
-        const int a = c_edge[e][0], b = c_edge[e][1];
-        const bool ina = a == c_face[f][0] || a == c_face[f][1] || a == c_face[f][2];
-        const bool inb = b == c_face[f][0] || b == c_face[f][1] || b == c_face[f][2];
-        if (ina && inb) mask[cells[c * ND + 4 + e]] = 1;
-      }
+    for (int k = 0; k < NV - 1; ++k) mask[v[k]] = 1;
+    if (Cell<ND>::P2) {
+#pragma unroll
+      for (int e = 0; e < n_edges<NV>(); ++e)
+        if (cell_edge_a<NV>(e) != f && cell_edge_b<NV>(e) != f) mask[cells[c * ND + NV + e]] = 1;
     }
   }
 }
@@ -322,12 +353,16 @@ __global__ void k_cols16(const int32_t* __restrict__ indptr, const int32_t* __re
   }
 }
 
-__global__ void k_copy_xyz(const double* __restrict__ xyz, int64_t m, double* __restrict__ a,
+// coordinates with dim components per vertex -> 3 per vertex (z = 0 in 2-D) in a (and b)
+__global__ void k_copy_xyz(const double* __restrict__ in, int64_t nvert, int dim, double* __restrict__ a,
                            double* __restrict__ b) {
+  const int64_t m = nvert * 3;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
-    const double v = xyz[i];
-    a[i] = v;
-    if (b) b[i] = v;
+    const int64_t v = i / 3;
+    const int k = (int)(i % 3);
+    const double x = k < dim ? in[v * dim + k] : 0.0;
+    a[i] = x;
+    if (b) b[i] = x;
   }
 }
 
@@ -660,10 +695,9 @@ int build_dirichlet(femk_plan* p, const uint8_t* user_mask, const int32_t* vptr,
     FEMK_CUDA_TRY(cudaMemcpyAsync(p->dmask, user_mask, n, cudaMemcpyDeviceToDevice, s));
   } else {
     FEMK_CUDA_TRY(cudaMemsetAsync(p->dmask, 0, n, s));
-    if (p->nd == 4)
-      k_boundary<4><<<::femk::counted_launch() + blocks_for(p->ntet * 4, kThreads, 65535 * 4), kThreads, 0, s>>>(p->cells, p->ntet, vptr, vinc, p->dmask);
-    else
-      k_boundary<10><<<::femk::counted_launch() + blocks_for(p->ntet * 4, kThreads, 65535 * 4), kThreads, 0, s>>>(p->cells, p->ntet, vptr, vinc, p->dmask);
+    const int grid = blocks_for(p->ntet * p->nv, kThreads, 65535 * 4);
+    FEMK_BY_ND(p->nd, k_boundary<ND><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->cells, p->ntet, vptr,
+                                                                                         vinc, p->dmask));
     FEMK_CUDA_TRY(cudaGetLastError());
   }
   Temp flag, pos;
@@ -682,7 +716,9 @@ int build_dirichlet(femk_plan* p, const uint8_t* user_mask, const int32_t* vptr,
   return FEMK_OK;
 }
 
-int create_impl(femk_plan* p, const double* xyz, const int32_t* tets, const uint8_t* mask, cudaStream_t s) {
+template <int NV>
+int create_impl(femk_plan* p, const double* coords, const int32_t* tets, const uint8_t* mask, cudaStream_t s) {
+  constexpr int NE = n_edges<NV>(), ND2 = NV + NE;
   int* d_err = nullptr;
   FEMK_CUDA_TRY(cudaMalloc(&d_err, sizeof(int)));
   Temp err_guard;
@@ -690,43 +726,44 @@ int create_impl(femk_plan* p, const double* xyz, const int32_t* tets, const uint
   FEMK_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), s));
   int h_err = 0;
 
-  k_validate_tets<<<::femk::counted_launch() + blocks_for(p->ntet, kThreads, 65535 * 4), kThreads, 0, s>>>(
+  k_validate_cells<NV><<<::femk::counted_launch() + blocks_for(p->ntet, kThreads, 65535 * 4), kThreads, 0, s>>>(
       tets, p->ntet, p->nvert, d_err);
   FEMK_CUDA_TRY(cudaGetLastError());
   FEMK_TRY(read_err(d_err, s, &h_err));
   if (h_err) {
-    set_error("femk_plan_create: a tet references a vertex outside [0, nvert) or repeats a vertex");
+    set_error("femk_plan_create: an element references a vertex outside [0, nvert) or repeats a vertex");
     return FEMK_EINVAL;
   }
   FEMK_TRY(dev_alloc(&p->xyz, p->nvert * 3, s));
   // vertex incidence (P1 connectivity): used by P2 numbering and by the boundary test
   int32_t* vptr = nullptr;
   int32_t* vinc = nullptr;
-  FEMK_TRY(build_incidence<4>(tets, p->ntet, p->nvert, &vptr, &vinc, d_err, s));
+  FEMK_TRY(build_incidence<NV>(tets, p->ntet, p->nvert, &vptr, &vinc, d_err, s));
   FEMK_TRY(read_err(d_err, s, &h_err));
   if (h_err) {
     cudaFree(vptr);
     cudaFree(vinc);
-    set_error("femk_plan_create: a tet references a vertex outside [0, nvert)");
+    set_error("femk_plan_create: an element references a vertex outside [0, nvert)");
     return FEMK_EINVAL;
   }
+  const int cgrid = blocks_for(p->nvert * 3, kThreads, 65535 * 4);
   if (p->order == 1) {
     p->n = p->nvert;
-    FEMK_TRY(dev_alloc(&p->cells, p->ntet * 4, s));
-    FEMK_CUDA_TRY(cudaMemcpyAsync(p->cells, tets, sizeof(int32_t) * p->ntet * 4, cudaMemcpyDeviceToDevice, s));
+    FEMK_TRY(dev_alloc(&p->cells, p->ntet * NV, s));
+    FEMK_CUDA_TRY(cudaMemcpyAsync(p->cells, tets, sizeof(int32_t) * p->ntet * NV, cudaMemcpyDeviceToDevice, s));
     FEMK_TRY(dev_alloc(&p->points, p->n * 3, s));
-    k_copy_xyz<<<::femk::counted_launch() + blocks_for(p->nvert * 3, kThreads, 65535 * 4), kThreads, 0, s>>>(xyz, p->nvert * 3, p->xyz, p->points);
+    k_copy_xyz<<<::femk::counted_launch() + cgrid, kThreads, 0, s>>>(coords, p->nvert, p->dim, p->xyz, p->points);
     p->inc_ptr = vptr;
     p->inc_elem = vinc;
   } else {
-    k_copy_xyz<<<::femk::counted_launch() + blocks_for(p->nvert * 3, kThreads, 65535 * 4), kThreads, 0, s>>>(xyz, p->nvert * 3, p->xyz, nullptr);
-    const int64_t m = p->ntet * 6;
+    k_copy_xyz<<<::femk::counted_launch() + cgrid, kThreads, 0, s>>>(coords, p->nvert, p->dim, p->xyz, nullptr);
+    const int64_t m = p->ntet * NE;
     Temp first, isf, rank;
     FEMK_CUDA_TRY(cudaMalloc(&first.p, sizeof(int32_t) * m));
     FEMK_CUDA_TRY(cudaMalloc(&isf.p, sizeof(int64_t) * (m + 1)));
     FEMK_CUDA_TRY(cudaMalloc(&rank.p, sizeof(int64_t) * (m + 1)));
-    k_edge_first<<<::femk::counted_launch() + blocks_for(m, kThreads, 65535 * 4), kThreads, 0, s>>>(tets, p->ntet, vptr, vinc, (int32_t*)first.p,
-                                                                         (int64_t*)isf.p, d_err);
+    k_edge_first<NV><<<::femk::counted_launch() + blocks_for(m, kThreads, 65535 * 4), kThreads, 0, s>>>(
+        tets, p->ntet, vptr, vinc, (int32_t*)first.p, (int64_t*)isf.p, d_err);
     FEMK_CUDA_TRY(cudaGetLastError());
     FEMK_TRY(scan_exclusive_i64((const int64_t*)isf.p, (int64_t*)rank.p, m, s));
     int64_t nedge = 0;
@@ -739,13 +776,13 @@ int create_impl(femk_plan* p, const double* xyz, const int32_t* tets, const uint
       set_error("femk_plan_create: too many DOFs for int32 indices");
       return FEMK_EINVAL;
     }
-    FEMK_TRY(dev_alloc(&p->cells, p->ntet * 10, s));
+    FEMK_TRY(dev_alloc(&p->cells, p->ntet * ND2, s));
     FEMK_TRY(dev_alloc(&p->points, p->n * 3, s));
-    FEMK_CUDA_TRY(cudaMemcpyAsync(p->points, xyz, sizeof(double) * p->nvert * 3, cudaMemcpyDeviceToDevice, s));
-    k_p2_cells<<<::femk::counted_launch() + blocks_for(m, kThreads, 65535 * 4), kThreads, 0, s>>>(tets, p->ntet, p->nvert, (const int32_t*)first.p,
-                                                                       (const int64_t*)rank.p, xyz, p->cells, p->points);
+    FEMK_CUDA_TRY(cudaMemcpyAsync(p->points, p->xyz, sizeof(double) * p->nvert * 3, cudaMemcpyDeviceToDevice, s));
+    k_p2_cells<NV><<<::femk::counted_launch() + blocks_for(m, kThreads, 65535 * 4), kThreads, 0, s>>>(
+        tets, p->ntet, p->nvert, (const int32_t*)first.p, (const int64_t*)rank.p, p->xyz, p->cells, p->points);
     FEMK_CUDA_TRY(cudaGetLastError());
-    FEMK_TRY(build_incidence<10>(p->cells, p->ntet, p->n, &p->inc_ptr, &p->inc_elem, d_err, s));
+    FEMK_TRY(build_incidence<ND2>(p->cells, p->ntet, p->n, &p->inc_ptr, &p->inc_elem, d_err, s));
   }
   FEMK_TRY(read_err(d_err, s, &h_err));
   if (h_err) {
@@ -757,7 +794,8 @@ int create_impl(femk_plan* p, const double* xyz, const int32_t* tets, const uint
     return FEMK_EINVAL;
   }
   p->vstride = (p->n + 63) & ~int64_t(63);
-  int st = p->nd == 4 ? build_pattern<4>(p, d_err, &h_err, s) : build_pattern<10>(p, d_err, &h_err, s);
+  int st = FEMK_OK;
+  FEMK_BY_ND(p->nd, st = build_pattern<ND>(p, d_err, &h_err, s));
   if (st == FEMK_OK) st = build_dirichlet(p, mask, vptr, vinc, s);
   if (vptr != p->inc_ptr) {
     cudaFree(vptr);
@@ -806,22 +844,28 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
   return FEMK_OK;
 }
 
-extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int32_t* tets_dev, int64_t ntet,
-                                int order, const uint8_t* dirichlet_mask_dev, void* stream, femk_plan** out) {
+extern "C" int femk_plan_create_simplex(const double* coords_dev, int dim, int64_t nvert, const int32_t* cells_dev,
+                                        int64_t ncell, int order, const uint8_t* dirichlet_mask_dev, void* stream,
+                                        femk_plan** out) {
   femk::clear_error();
   FEMK_CHECK_ARG(out != nullptr, "femk_plan_create: out is NULL");
   *out = nullptr;
-  FEMK_CHECK_ARG(xyz_dev && tets_dev, "femk_plan_create: xyz/tets is NULL");
+  FEMK_CHECK_ARG(coords_dev && cells_dev, "femk_plan_create: coordinates/cells is NULL");
+  FEMK_CHECK_ARG(dim == 2 || dim == 3, "femk_plan_create: dim must be 2 (triangles) or 3 (tetrahedra)");
   FEMK_CHECK_ARG(order == 1 || order == 2, "femk_plan_create: order must be 1 or 2");
-  FEMK_CHECK_ARG(nvert >= 4 && ntet >= 1, "femk_plan_create: empty mesh");
-  FEMK_CHECK_ARG(ntet * (order == 1 ? 16 : 100) < INT32_MAX, "femk_plan_create: mesh too large for int32 slot map");
+  const int nv = dim + 1;
+  const int nd = order == 1 ? nv : nv * (nv + 1) / 2;  // P2: vertices + edges
+  FEMK_CHECK_ARG(nvert >= nv && ncell >= 1, "femk_plan_create: empty mesh");
+  FEMK_CHECK_ARG(ncell * nd * nd < INT32_MAX, "femk_plan_create: mesh too large for int32 slot map");
   FEMK_CHECK_ARG(nvert < INT32_MAX, "femk_plan_create: too many vertices");
   cudaStream_t s = (cudaStream_t)stream;
   femk_plan* p = new femk_plan();
   cudaGetDevice(&p->device);
   cudaDeviceGetAttribute(&p->n_sm, cudaDevAttrMultiProcessorCount, p->device);
   p->order = order;
-  p->nd = order == 1 ? 4 : 10;
+  p->dim = dim;
+  p->nv = nv;
+  p->nd = nd;
   if (const char* e = std::getenv("FEMK_CG_FUSED")) p->cg_fused = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_CG_GRAPH")) p->cg_graph = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_SELL")) p->use_sell = std::atoi(e) != 0;
@@ -850,14 +894,20 @@ extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int3
   if (const char* e = std::getenv("FEMK_L2HINT32")) p->l2_mode32 = std::atoi(e) != 0;
   cudaDeviceGetAttribute(&p->coop, cudaDevAttrCooperativeLaunch, p->device);
   p->nvert = nvert;
-  p->ntet = ntet;
-  const int st = femk::create_impl(p, xyz_dev, tets_dev, dirichlet_mask_dev, s);
+  p->ntet = ncell;
+  const int st = dim == 2 ? femk::create_impl<3>(p, coords_dev, cells_dev, dirichlet_mask_dev, s)
+                          : femk::create_impl<4>(p, coords_dev, cells_dev, dirichlet_mask_dev, s);
   if (st != FEMK_OK) {
     femk_plan_destroy(p);
     return st;
   }
   *out = p;
   return FEMK_OK;
+}
+
+extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int32_t* tets_dev, int64_t ntet,
+                                int order, const uint8_t* dirichlet_mask_dev, void* stream, femk_plan** out) {
+  return femk_plan_create_simplex(xyz_dev, 3, nvert, tets_dev, ntet, order, dirichlet_mask_dev, stream, out);
 }
 
 extern "C" int femk_plan_get_info(const femk_plan* p, femk_plan_info* out) {
@@ -875,6 +925,7 @@ extern "C" int femk_plan_get_info(const femk_plan* p, femk_plan_info* out) {
   out->batch_graph = p->batch_graph_used;
   out->tiles = p->tile_ok;
   out->sell_col_units = p->sell_cu ? p->sell_cu_len : (p->sell_src ? p->sell_nnz : 0);
+  out->dim = p->dim;
   return FEMK_OK;
 }
 

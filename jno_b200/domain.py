@@ -1,9 +1,14 @@
-"""Mesh front end: the structured Kuhn box and a ``jno.domain``-shaped holder (host, numpy).
+"""Mesh front end: the structured Kuhn box, the triangulated rectangle and a ``jno.domain``-shaped
+holder (host, numpy).
 
 ``equi_distant_box`` follows ``Geometries.equi_distant_box(..., cell="tetra")``
 (jno/domain/geometries.py:203-300): lattice points in C order ``idx = (i(ny+1) + j)(nz+1) + k`` and
-six Kuhn tets per voxel in (i, j, k, kuhn) order, corner bits ``(c>>2, c>>1, c)``. It returns a
-``constructor(geo) -> (mesh, 3, ds)`` like the reference; ``domain(constructor)`` builds the mesh.
+six Kuhn tets per voxel in (i, j, k, kuhn) order, corner bits ``(c>>2, c>>1, c)``.
+``equi_distant_rect`` follows ``Geometries.equi_distant_rect(..., cell="triangle")``
+(jno/domain/geometries.py:44-200): lattice points ``idx = i(ny+1) + j`` with z = 0 and two
+triangles ``(p00, p10, p11)``, ``(p00, p11, p01)`` per rectangle in (i, j) order. Both return a
+``constructor(geo) -> (mesh, dim, ds)`` like the reference; ``domain(constructor)`` builds the mesh,
+and the FEM reads its points as ``[:, :dim]`` (jno/utils/solver/fem_native.py:250).
 """
 
 import numpy as np
@@ -12,12 +17,14 @@ KUHN = ((0, 4, 6, 7), (0, 4, 5, 7), (0, 2, 6, 7), (0, 2, 3, 7), (0, 1, 5, 7), (0
 
 
 class Mesh:
-    """Minimal mesh record: ``points`` f64[nv, 3] and ``tets`` i64[T, 4]."""
+    """Minimal mesh record: ``points`` f64[nv, 3] and the simplex cells i64[T, dim+1]
+    (``tetra`` for dim 3, ``triangle`` for dim 2; a 2-D mesh has z = 0)."""
 
-    def __init__(self, points, tets):
+    def __init__(self, points, tets, dim=3):
         self.points = np.asarray(points, dtype=np.float64)
-        self.tets = np.asarray(tets, dtype=np.int64)
-        self.cells_dict = {"tetra": self.tets}
+        self.dim = dim
+        self.tets = np.asarray(tets, dtype=np.int64)  # the cells (tetrahedra, or triangles in 2-D)
+        self.cells_dict = {"tetra" if dim == 3 else "triangle": self.tets}
 
 
 def box_points_tets(nx, ny, nz, x_range=(0.0, 1.0), y_range=(0.0, 1.0), z_range=(0.0, 1.0)):
@@ -50,6 +57,45 @@ def equi_distant_box(x_range=(0, 1), y_range=(0, 1), z_range=(0, 1), nx=8, ny=8,
     return constructor
 
 
+def rect_points_tris(nx, ny, x_range=(0.0, 1.0), y_range=(0.0, 1.0)):
+    X = np.linspace(x_range[0], x_range[1], nx + 1)
+    Y = np.linspace(y_range[0], y_range[1], ny + 1)
+    xx, yy = np.meshgrid(X, Y, indexing="ij")
+    points = np.column_stack([xx.ravel(), yy.ravel(), np.zeros((nx + 1) * (ny + 1))])
+    I, J = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    I, J = I.ravel(), J.ravel()
+    p00, p10 = I * (ny + 1) + J, (I + 1) * (ny + 1) + J
+    p11, p01 = p10 + 1, p00 + 1
+    tris = np.stack([np.stack([p00, p10, p11], 1), np.stack([p00, p11, p01], 1)], axis=1)
+    return points, tris.reshape(-1, 3).astype(np.int64)
+
+
+def equi_distant_rect(x_range=(0, 1), y_range=(0, 1), nx=10, ny=10, cell="triangle"):
+    """Structured triangulated rectangle constructor (the reference's ``equi_distant_rect`` contract)."""
+    if cell != "triangle":
+        raise NotImplementedError("only cell='triangle' is on the B200 path (quadrilaterals are out of scope)")
+
+    def constructor(geo=None):
+        pts, tris = rect_points_tris(nx, ny, x_range, y_range)
+        ds = min((x_range[1] - x_range[0]) / nx, (y_range[1] - y_range[0]) / ny)
+        return Mesh(pts, tris, dim=2), 2, ds
+
+    constructor.lattice = (nx, ny, x_range, y_range)
+    return constructor
+
+
+def jitter_interior_2d(points, nx, ny, seed, amp=0.1, x_range=(0.0, 1.0), y_range=(0.0, 1.0)):
+    """``jitter_interior`` on the rectangle lattice: ``default_rng(seed).uniform(-amp, amp,
+    (n_interior, 2)) * h`` moves the interior vertices in x and y (z stays 0)."""
+    pts = np.array(points, dtype=np.float64, copy=True)
+    i, j = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), indexing="ij")
+    inner = ((i > 0) & (i < nx) & (j > 0) & (j < ny)).ravel()
+    h = np.array([(x_range[1] - x_range[0]) / nx, (y_range[1] - y_range[0]) / ny])
+    rng = np.random.default_rng(seed)
+    pts[inner, :2] += rng.uniform(-amp, amp, size=(int(inner.sum()), 2)) * h[None, :]
+    return pts
+
+
 def jitter_interior(points, nx, ny, nz, seed, amp=0.1, x_range=(0.0, 1.0), y_range=(0.0, 1.0), z_range=(0.0, 1.0)):
     """Synthetic workload input: move every interior lattice vertex by U(-amp h, amp h) per axis.
 
@@ -69,20 +115,29 @@ class domain:
 
     def __init__(self, constructor, jitter=None, seed=0):
         mesh, dim, ds = constructor(None)
-        if dim != 3:
-            raise NotImplementedError("only 3-D tetrahedral meshes are on the B200 path")
+        if dim not in (2, 3):
+            raise NotImplementedError("only 2-D triangle and 3-D tetrahedral meshes are on the B200 path")
         self.built_mesh = mesh
         self.dimension = dim
         self.ds = ds
         if jitter:
-            nx, ny, nz, xr, yr, zr = constructor.lattice
-            mesh.points = jitter_interior(mesh.points, nx, ny, nz, seed, jitter, xr, yr, zr)
+            if dim == 3:
+                nx, ny, nz, xr, yr, zr = constructor.lattice
+                mesh.points = jitter_interior(mesh.points, nx, ny, nz, seed, jitter, xr, yr, zr)
+            else:
+                nx, ny, xr, yr = constructor.lattice
+                mesh.points = jitter_interior_2d(mesh.points, nx, ny, seed, jitter, xr, yr)
 
     @classmethod
     def from_mesh(cls, points, tets):
+        """A domain over given cells: tetrahedra i64[T, 4], or triangles i64[T, 3] (2-D)."""
         obj = cls.__new__(cls)
-        obj.built_mesh = Mesh(points, tets)
-        obj.dimension = 3
+        dim = int(np.asarray(tets).shape[1]) - 1
+        pts = np.asarray(points, dtype=np.float64)
+        if pts.shape[1] == 2:
+            pts = np.column_stack([pts, np.zeros(pts.shape[0])])
+        obj.built_mesh = Mesh(pts, tets, dim=dim)
+        obj.dimension = dim
         obj.ds = None
         return obj
 
@@ -105,4 +160,4 @@ class domain:
 
         if region not in ("interior", "boundary"):
             raise NotImplementedError(f"region {region!r}: only 'interior' and 'boundary' are on the B200 path")
-        return tuple(Coordinate(region, a) for a in range(3))
+        return tuple(Coordinate(region, a) for a in range(self.dimension))

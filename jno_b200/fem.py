@@ -139,9 +139,11 @@ def fem(terms, quad_degree=None, element_type=None, chunk=None, dirichlet_mask=N
         raise ValueError("jno.fem takes a list of terms")
     vol, dirichlet = terms[0], list(terms[1:])
     form = classify_volume(vol)
-    if element_type not in (None, "TET4", "TET10"):
-        raise NotImplementedError(f"element_type={element_type!r} is outside the B200 path")
-    if element_type == "TET10":
+    dim = getattr(form.domain, "dimension", 3)
+    allowed = (None, "TET4", "TET10") if dim == 3 else (None, "TRI3", "TRI6")
+    if element_type not in allowed:
+        raise NotImplementedError(f"element_type={element_type!r} is outside the B200 path for a {dim}-D mesh")
+    if element_type in ("TET10", "TRI6"):
         form.order = 2
     need = 2 * form.order
     if quad_degree is not None and int(quad_degree) < need:
@@ -150,7 +152,7 @@ def fem(terms, quad_degree=None, element_type=None, chunk=None, dirichlet_mask=N
         raise NotImplementedError("one Dirichlet condition on the whole boundary is supported")
     d = form.domain
     mesh = d.built_mesh
-    plan = FemPlan(mesh.points, mesh.tets, form.order, dirichlet_mask)
+    plan = FemPlan(mesh.points[:, :dim], mesh.tets, form.order, dirichlet_mask)  # fem_native.py:250
     g_values = None
     if dirichlet:
         sym, gexpr = classify_dirichlet(dirichlet[0])

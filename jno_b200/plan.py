@@ -23,11 +23,12 @@ def _device_tensor(a, dtype):
 
 
 class FemPlan:
-    """P1/P2 tetrahedral assembly plan on the current CUDA device.
+    """P1/P2 simplex assembly plan on the current CUDA device.
 
-    ``points`` f64[nv, 3] and ``tets`` int[T, 4] describe the P1 mesh; ``order`` 2 adds the edge
-    midpoint DOFs in the reference's first-encounter numbering. ``dirichlet_mask`` (bool/uint8 per
-    DOF) overrides the default Dirichlet set (every node on a boundary facet).
+    ``points`` f64[nv, 3] with ``tets`` int[T, 4] (tetrahedra), or ``points`` f64[nv, 2] with
+    int[T, 3] triangles, describe the P1 mesh; ``order`` 2 adds the edge midpoint DOFs in the
+    reference's first-encounter numbering. ``dirichlet_mask`` (bool/uint8 per DOF) overrides the
+    default Dirichlet set (every node on a boundary facet).
     """
 
     def __init__(self, points, tets, order=1, dirichlet_mask=None):
@@ -37,22 +38,24 @@ class FemPlan:
         self._lib = lib
         t = np.asarray(tets.cpu().numpy() if isinstance(tets, torch.Tensor) else tets)
         nv = int(points.shape[0])
-        if t.ndim != 2 or t.shape[1] != 4 or t.size == 0:
-            raise ValueError("tets must be a non-empty [T, 4] array")
+        dim = int(points.shape[1]) if len(points.shape) == 2 else 0
+        if dim not in (2, 3):
+            raise ValueError("points must be [nv, 3] (tetrahedra) or [nv, 2] (triangles)")
+        kind = "tets" if dim == 3 else "triangles"
+        if t.ndim != 2 or t.shape[1] != dim + 1 or t.size == 0:
+            raise ValueError(f"{kind} must be a non-empty [T, {dim + 1}] array for [nv, {dim}] points")
         if t.min() < 0 or t.max() >= nv:
-            raise ValueError(f"tets reference vertices outside [0, {nv})")
+            raise ValueError(f"{kind} reference vertices outside [0, {nv})")
         srt = np.sort(t, axis=1)
         if np.any(srt[:, 1:] == srt[:, :-1]):
-            raise ValueError("a tet repeats a vertex")
+            raise ValueError(f"an element of the {kind} repeats a vertex")
         xyz = _device_tensor(points, torch.float64)
         cells = _device_tensor(t, torch.int32)
-        if xyz.ndim != 2 or xyz.shape[1] != 3 or cells.ndim != 2 or cells.shape[1] != 4:
-            raise ValueError("points must be [nv, 3] and tets [T, 4]")
         mask = None if dirichlet_mask is None else _device_tensor(dirichlet_mask, torch.uint8)
         handle = ctypes.c_void_p()
         _lib.check(
-            lib.femk_plan_create(
-                _lib.ptr(xyz), xyz.shape[0], _lib.ptr(cells), cells.shape[0], int(order), _lib.ptr(mask),
+            lib.femk_plan_create_simplex(
+                _lib.ptr(xyz), dim, xyz.shape[0], _lib.ptr(cells), cells.shape[0], int(order), _lib.ptr(mask),
                 _lib.stream_handle(), ctypes.byref(handle),
             )
         )
@@ -60,6 +63,7 @@ class FemPlan:
         info = _lib.PlanInfo()
         _lib.check(lib.femk_plan_get_info(self._h, ctypes.byref(info)))
         self.order = info.order
+        self.dim = info.dim
         self.nd = info.ndof_local
         self.ntet = info.ntet
         self.nvert = info.nvert
@@ -114,7 +118,7 @@ class FemPlan:
         out["indptr"], out["indices"] = indptr, indices
         out["slot"] = out["slot"].view(self.ntet, self.nd, self.nd)
         out["cells"] = out["cells"].view(self.ntet, self.nd)
-        out["points"] = out["points"].view(self.n, 3)
+        out["points"] = out["points"].view(self.n, 3)[:, : self.dim]  # a 2-D plan stores z = 0
         return out
 
     # ---------------------------------------------------------------- kernels

@@ -214,8 +214,10 @@ def classify_volume(expr):
             continue
         else:
             raise NotImplementedError("this term is outside the B200 path (-div(k grad u) = f only)")
-    if sorted(stiff) != [0, 1, 2]:
-        raise NotImplementedError("the form needs ui.x*vi.x + ui.y*vi.y + ui.z*vi.z")
+    dim = getattr(domain, "dimension", 3)
+    if sorted(stiff) != list(range(dim)):
+        raise NotImplementedError(
+            "the form needs ui.x*vi.x + ui.y*vi.y" + (" + ui.z*vi.z" if dim == 3 else "") + f" on a {dim}-D domain")
     scales = {s for s, _ in stiff.values()}
     keys = {k for _, k in stiff.values()}
     if len(scales) != 1 or len(keys) != 1:
@@ -231,7 +233,7 @@ def classify_volume(expr):
 
 
 def evaluate_on(expr, pts):
-    """Evaluate a Dirichlet value expression (constants and boundary coordinates) at points f64[m, 3]."""
+    """Evaluate a Dirichlet value expression (constants and boundary coordinates) at points f64[m, dim]."""
     if isinstance(expr, Const):
         return np.full(pts.shape[0], expr.v)
     if isinstance(expr, Coordinate):

@@ -16,12 +16,12 @@ The misfit is ``J = 1/2 sum_i M_ii (u_i - u*_i)^2`` with the lumped mass ``M_ii 
 import numpy as np
 
 from .assemble import assemble
-from .element import element_matrices
+from .element import element_matrices, vertices
 from .pcg import pcg
 
 
 def lumped_mass(points, cells, order):
-    _, F = element_matrices(points[cells[:, :4]], order)
+    _, F = element_matrices(vertices(points, cells), order)
     return np.bincount(cells.reshape(-1), weights=F.reshape(-1), minlength=points.shape[0])
 
 
@@ -47,7 +47,7 @@ def gradient(points, cells, order, dirichlet, logk, ustar, mass, tol=1e-12):
 
     lam, _, _ = pcg(A.T.tocsr(), mass * (u - ustar), jacobi_inverse(matrix_diagonal(sysm)), tol=tol)
     m = (~sysm.dirichlet).astype(np.float64)
-    Khat, _ = element_matrices(points[cells[:, :4]], order)
+    Khat, _ = element_matrices(vertices(points, cells), order)
     le = (m * lam)[cells]
     ue = (m * u)[cells]
     grad = -np.exp(logk) * np.einsum("ta,tab,tb->t", le, Khat, ue)
@@ -58,7 +58,7 @@ def gradient_nodal(points, cells, dirichlet, values, mode, ustar, mass, tol=1e-1
     """(J, dJ/dp f64[nvert]) for a nodal P1 parameter p: the element gradient dJ/dk_e (as above,
     with k_e from ``element.nodal_coefficient``) spread onto the vertices by dk_e/dp_i."""
     from .assemble import jacobi_inverse, matrix_diagonal
-    from .element import _Q4_A, _Q4_B, nodal_coefficient
+    from .element import nodal_coefficient, nodal_rule
 
     ke = nodal_coefficient(cells, values, mode)
     sysm = assemble(points, cells, 1, dirichlet, ke)
@@ -67,15 +67,17 @@ def gradient_nodal(points, cells, dirichlet, values, mode, ustar, mass, tol=1e-1
     u, _, _ = pcg(A, sysm.b, inv, tol=tol)
     lam, _, _ = pcg(A.T.tocsr(), mass * (u - ustar), inv, tol=tol)
     m = (~sysm.dirichlet).astype(np.float64)
-    Khat, _ = element_matrices(points[cells[:, :4]], 1)
+    Khat, _ = element_matrices(vertices(points, cells), 1)
     dJdk = -np.einsum("ta,tab,tb->t", (m * lam)[cells], Khat, (m * u)[cells])
     p = np.asarray(values, dtype=np.float64)[cells]
+    nv = p.shape[1]
     if mode == "linear":
-        dk = np.full(p.shape, 0.25)
+        dk = np.full(p.shape, 1.0 / nv)
     else:
-        lamq = np.full((4, 4), _Q4_A) + np.eye(4) * (_Q4_B - _Q4_A)
+        qa, qb = nodal_rule(nv)
+        lamq = np.full((nv, nv), qa) + np.eye(nv) * (qb - qa)
         e = np.exp(p @ lamq.T)
-        dk = 0.25 * (_Q4_A * e.sum(axis=1, keepdims=True) + (_Q4_B - _Q4_A) * e)
+        dk = (qa * e.sum(axis=1, keepdims=True) + (qb - qa) * e) / nv
     grad = np.bincount(cells.reshape(-1), weights=(dJdk[:, None] * dk).reshape(-1), minlength=points.shape[0])
     return misfit(u, ustar, mass), grad
 

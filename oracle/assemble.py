@@ -96,7 +96,7 @@ def assemble(points, cells, order, dirichlet, coef, f=1.0, g=None, plan=None, el
     Dirichlet node ids, ``g`` the per-node Dirichlet values (None = 0). ``plan`` may carry
     (indptr, indices, slot) to skip the pattern build. Returns a :class:`System`.
     """
-    from .element import element_matrices
+    from .element import element_matrices, vertices
 
     points = np.asarray(points, dtype=np.float64)
     cells = np.asarray(cells, dtype=np.int64)
@@ -110,7 +110,7 @@ def assemble(points, cells, order, dirichlet, coef, f=1.0, g=None, plan=None, el
         indptr, indices, slot = plan
         nse = indices.size
     if element is None:
-        Khat, Fhat = element_matrices(points[cells[:, :4]], order)
+        Khat, Fhat = element_matrices(vertices(points, cells), order)
     else:
         Khat, Fhat = element
     Ke = np.asarray(coef, dtype=np.float64)[:, None, None] * Khat

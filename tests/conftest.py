@@ -18,3 +18,10 @@ def golden():
     import numpy as np
 
     return np.load(os.path.join(ROOT, "tests", "golden", "reference_small.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden2d():
+    import numpy as np
+
+    return np.load(os.path.join(ROOT, "tests", "golden", "reference_small_2d.npz"))

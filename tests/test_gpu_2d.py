@@ -1,0 +1,351 @@
+"""GPU parity on 2-D triangle meshes (P1/P2): the CUDA path through the C ABI against the oracle
+and the reference-generated 2-D fixtures.
+
+Bars as for tetrahedra: integer/index outputs bit-exact; FP64 matrix values and loads within 1e-12
+of the oracle relative to the largest entry; solves to the 1e-8 stop rule with the solution within
+1e-7 of the oracle's; adjoint gradients within 1e-8 of the oracle's adjoint and 1e-6 of central
+differences.
+"""
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from oracle import adjoint as oadj  # noqa: E402
+from oracle import assemble as oa  # noqa: E402
+from oracle import element as oe  # noqa: E402
+from oracle import mesh as om  # noqa: E402
+from oracle import pcg as op  # noqa: E402
+
+VAL_TOL = 1e-12
+
+
+def _plan(points, tris, order):
+    from jno_b200.plan import FemPlan
+
+    return FemPlan(points, tris, order)
+
+
+def _mesh(n, order, seed=0, amp=0.1):
+    return om.unit_square(n, order=order, seed=seed, amp=amp)
+
+
+def _oracle_system(pf, cf, order, logk, f=1.0, g=None):
+    bnd = om.boundary_nodes(cf, order, nv=3)
+    return oa.assemble(pf, cf, order, bnd, np.exp(logk), f=f, g=g), bnd
+
+
+@pytest.mark.parametrize("n,order", [(2, 1), (5, 1), (33, 1), (2, 2), (5, 2), (17, 2)])
+def test_tri_plan_matches_oracle_bit_exact(n, order):
+    pf, cf, tris, p1 = _mesh(n, order)
+    plan = _plan(p1, tris, order)
+    assert plan.dim == 2 and plan.nd == (3 if order == 1 else 6)
+    ex = plan.export()
+    idx, inverse, nse = oa.compress_plan(cf)
+    indptr, indices = oa.plan_to_csr(idx, pf.shape[0])
+    assert plan.n == pf.shape[0] and plan.nnz == nse
+    assert np.array_equal(ex["cells"].cpu().numpy(), cf)
+    assert np.array_equal(ex["indptr"].cpu().numpy(), indptr)
+    assert np.array_equal(ex["indices"].cpu().numpy(), indices)
+    assert np.array_equal(ex["slot"].cpu().numpy().reshape(-1), inverse)
+    assert np.array_equal(ex["points"].cpu().numpy(), pf)
+    bnd = om.boundary_nodes(cf, order, nv=3)
+    assert np.array_equal(np.flatnonzero(ex["dirichlet_mask"].cpu().numpy()), bnd)
+    rows = np.repeat(np.arange(plan.n), np.diff(indptr))
+    assert np.array_equal(ex["diag_slot"].cpu().numpy(), np.flatnonzero(rows == indices))
+
+
+def test_tri_plan_golden_reference_fixture(golden2d):
+    """The device plan reproduces the reference-generated 2-D fixture directly (5x4, P1 and P2)."""
+    tag = "5x4"
+    plan1 = _plan(golden2d[f"{tag}/jittered"], golden2d[f"{tag}/tris"], 1)
+    ex = plan1.export()
+    assert np.array_equal(ex["indices"].cpu().numpy(), golden2d[f"{tag}/p1_idx"][:, 1])
+    assert np.array_equal(ex["slot"].cpu().numpy().reshape(-1), golden2d[f"{tag}/p1_inverse"])
+    assert np.array_equal(np.flatnonzero(ex["dirichlet_mask"].cpu().numpy()), golden2d[f"{tag}/p1_boundary"])
+    plan2 = _plan(golden2d[f"{tag}/jittered"], golden2d[f"{tag}/tris"], 2)
+    ex2 = plan2.export()
+    assert np.array_equal(ex2["cells"].cpu().numpy(), golden2d[f"{tag}/p2_cells"])
+    assert np.array_equal(ex2["points"].cpu().numpy(), golden2d[f"{tag}/p2_points"])
+    assert np.array_equal(ex2["slot"].cpu().numpy().reshape(-1), golden2d[f"{tag}/p2_inverse"])
+    assert np.array_equal(np.flatnonzero(ex2["dirichlet_mask"].cpu().numpy()), golden2d[f"{tag}/p2_boundary"])
+
+
+@pytest.mark.parametrize("n,order", [(4, 1), (32, 1), (4, 2), (16, 2)])
+def test_tri_assembly_matches_oracle(n, order):
+    pf, cf, tris, p1 = _mesh(n, order, seed=1)
+    logk = om.logk_field(len(tris), 1000)
+    plan = _plan(p1, tris, order)
+    vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
+    s, _ = _oracle_system(pf, cf, order, logk)
+    v = vals.cpu().numpy()
+    assert np.abs(v - s.data).max() <= VAL_TOL * np.abs(s.data).max()
+    assert np.abs(b.cpu().numpy() - s.b).max() <= VAL_TOL * np.abs(s.b).max()
+    assert np.array_equal(v == 0.0, s.data == 0.0)
+    kh, fh = plan.element_matrices()
+    K, F = oe.element_matrices(oe.vertices(pf, cf), order)
+    assert np.abs(kh.cpu().numpy() - K).max() <= VAL_TOL * np.abs(K).max()
+    assert np.abs(fh.cpu().numpy() - F).max() <= VAL_TOL * np.abs(F).max()
+    m = plan.lumped_mass().cpu().numpy()
+    mo = oadj.lumped_mass(pf, cf, order)
+    assert np.abs(m - mo).max() <= 1e-13 * np.abs(mo).max()
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_tri_inhomogeneous_dirichlet_patch(order):
+    """P1 reproduces a linear field, P2 a quadratic one (the 2-D forms of tests/test_fem_3d.py:76-89
+    and tests/test_fem_native_lagrange.py:377-395), through the CUDA assembly and CG."""
+    pf, cf, tris, p1 = _mesh(8, order, seed=3)
+    x, y = pf.T
+    if order == 1:
+        exact, f = 1 + 2 * x + 3 * y, 0.0
+    else:
+        exact, f = x**2 + 2 * y**2 + x * y, -6.0
+    plan = _plan(p1, tris, order)
+    vals, b = plan.assemble(None, mode=2, scale=1.0, f=f, g=torch.as_tensor(exact, device="cuda"))
+    s, _ = _oracle_system(pf, cf, order, np.zeros(len(tris)), f=f, g=exact)
+    assert np.abs(vals.cpu().numpy() - s.data).max() <= VAL_TOL * np.abs(s.data).max()
+    assert np.abs(b.cpu().numpy() - s.b).max() <= 1e-11 * np.abs(s.b).max()
+    u, it, rel, st = plan.pcg(vals, b, inv_diag=plan.jacobi(vals), tol=1e-13)
+    assert np.abs(u.cpu().numpy() - exact).max() < 1e-9
+
+
+@pytest.mark.parametrize("n,order", [(16, 1), (128, 1), (8, 2), (48, 2)])
+def test_tri_pcg_matches_oracle(n, order):
+    pf, cf, tris, p1 = _mesh(n, order)
+    logk = om.logk_field(len(tris), 1000)
+    plan = _plan(p1, tris, order)
+    vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
+    inv = plan.jacobi(vals)
+    u, it, rel, st = plan.pcg(vals, b, inv_diag=inv, tol=1e-8)
+    s, _ = _oracle_system(pf, cf, order, logk)
+    A = s.csr()
+    io = oa.jacobi_inverse(oa.matrix_diagonal(s))
+    xo, ito, _ = op.pcg(A, s.b, io, tol=1e-8)
+    assert st == 0 and abs(it - ito) <= 1, (it, ito)
+    uu = u.cpu().numpy()
+    assert np.linalg.norm(uu - xo) <= 1e-7 * np.linalg.norm(xo)
+    assert rel <= 2e-8 and abs(rel - op.residual_check(A, s.b, uu)) <= 1e-12
+    assert np.abs(inv.cpu().numpy() - io).max() <= 1e-12 * np.abs(io).max()
+    # mixed precision reaches the FP64 stop rule on the same operator
+    um, inner, outer, relm, stm = plan.pcg_mixed(vals, b, inv, tol=1e-8)
+    assert stm == 0 and relm <= 1e-8
+    assert np.linalg.norm(um.cpu().numpy() - xo) <= 1e-6 * np.linalg.norm(xo)
+    # BiCGStab (the steady default) against the oracle's jax restatement. Its iteration count moves
+    # with the summation order: a symmetric permutation of the oracle's own system (same math, other
+    # order) moves it by up to 17 % at P1 128^2 (303 -> 354); the contract is the stop rule and the
+    # solution
+    ub, itb, relb, stb = plan.bicgstab(vals, b, inv_diag=inv, tol=1e-8)
+    xb, kb = op.bicgstab(A, s.b, io, tol=1e-8)
+    assert stb == 0 and relb <= 2e-8 and abs(itb - kb) <= max(2, kb // 4), (itb, kb)
+    assert np.linalg.norm(ub.cpu().numpy() - xb) <= 1e-7 * np.linalg.norm(xb)
+
+
+@pytest.mark.parametrize("n,order", [(24, 1), (8, 2)])
+def test_tri_spmv_and_matrix_free_match(n, order):
+    pf, cf, tris, p1 = _mesh(n, order, seed=2)
+    logk = om.logk_field(len(tris), 7)
+    plan = _plan(p1, tris, order)
+    lk = torch.as_tensor(logk, device="cuda")
+    vals, b = plan.assemble(lk)
+    xv = torch.as_tensor(np.random.default_rng(0).standard_normal(plan.n), device="cuda")
+    s, _ = _oracle_system(pf, cf, order, logk)
+    yo = s.csr() @ xv.cpu().numpy()
+    assert np.abs(plan.spmv(vals, xv).cpu().numpy() - yo).max() <= 1e-12 * np.abs(yo).max()
+    plan.prepare_operator(vals)
+    assert np.abs(plan.spmv_prepared(xv).cpu().numpy() - yo).max() <= 1e-12 * np.abs(yo).max()
+    assert np.abs(plan.spmv_matfree(lk, xv).cpu().numpy() - yo).max() <= 1e-12 * np.abs(yo).max()
+    inv, inv_mf = plan.jacobi(vals), plan.jacobi_matfree(lk)
+    assert np.abs(inv.cpu().numpy() - inv_mf.cpu().numpy()).max() <= 1e-12 * inv.abs().max().item()
+    u1, it1, _, _ = plan.pcg(vals, b, inv_diag=inv)
+    u2, it2, rel2, _ = plan.pcg_matfree(lk, b, inv_diag=inv_mf)
+    assert abs(it1 - it2) <= 1 and rel2 <= 2e-8
+    assert torch.linalg.norm(u1 - u2) <= 1e-7 * torch.linalg.norm(u1)
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_tri_p0_adjoint_matches_oracle_and_fd(order):
+    from jno_b200.autograd import solve_p0
+
+    pf, cf, tris, p1 = _mesh(6, order)
+    logk = om.logk_field(len(tris), 1002)
+    bnd = om.boundary_nodes(cf, order, nv=3)
+    ustar, _, _ = oadj.solve(pf, cf, order, bnd, om.logk_field(len(tris), 2000))
+    mass = oadj.lumped_mass(pf, cf, order)
+    J_o, g_o = oadj.gradient(pf, cf, order, bnd, logk, ustar, mass)
+    plan = _plan(p1, tris, order)
+    m = plan.lumped_mass()
+    us = torch.as_tensor(ustar, device="cuda")
+    lk = torch.as_tensor(logk, device="cuda").requires_grad_(True)
+    u = solve_p0(plan, lk, tol=1e-13)
+    J = 0.5 * torch.sum(m * (u - us) ** 2)
+    J.backward()
+    g = lk.grad.cpu().numpy()
+    assert abs(J.item() - J_o) <= 1e-10 * abs(J_o)
+    assert np.abs(g - g_o).max() <= 1e-8 * np.abs(g_o).max()
+
+    def Jof(v):
+        with torch.no_grad():
+            uu = solve_p0(plan, torch.as_tensor(v, device="cuda"), tol=1e-14)
+            return (0.5 * torch.sum(m * (uu - us) ** 2)).item()
+
+    for c in np.random.default_rng(5).choice(len(tris), 6, replace=False):
+        e = np.zeros(len(tris))
+        e[c] = 1e-6
+        fd = (Jof(logk + e) - Jof(logk - e)) / 2e-6
+        assert abs(fd - g[c]) <= 1e-6 * np.abs(g).max() + 1e-6 * abs(g[c])
+
+
+@pytest.mark.parametrize("mode", ["exp", "linear"])
+def test_tri_nodal_parameter_and_adjoint(mode):
+    """A nodal P1 coefficient on triangles (3-point degree-2 rule): assembly, matrix-free product
+    and dJ/dp against the oracle's chain rule and central differences."""
+    from jno_b200 import _lib
+    from jno_b200.autograd import solve_nodal
+
+    pf, cf, tris, p1 = _mesh(8, 1)
+    rng = np.random.default_rng(11)
+    nodal = rng.normal(0.0, 0.5, p1.shape[0]) if mode == "exp" else rng.uniform(0.5, 2.0, p1.shape[0])
+    cmode = _lib.COEF_NODAL_EXP if mode == "exp" else _lib.COEF_NODAL_LINEAR
+    plan = _plan(p1, tris, 1)
+    pv = torch.as_tensor(nodal, device="cuda")
+    vals, b = plan.assemble(pv, mode=cmode)
+    bnd = om.boundary_nodes(cf, 1, nv=3)
+    s = oa.assemble(pf, cf, 1, bnd, oe.nodal_coefficient(tris, nodal, mode))
+    assert np.abs(vals.cpu().numpy() - s.data).max() <= VAL_TOL * np.abs(s.data).max()
+    xv = torch.as_tensor(rng.standard_normal(plan.n), device="cuda")
+    yo = s.csr() @ xv.cpu().numpy()
+    assert np.abs(plan.spmv_matfree(pv, xv, mode=cmode).cpu().numpy() - yo).max() <= 1e-12 * np.abs(yo).max()
+
+    ustar, _, _ = oadj.solve(pf, cf, 1, bnd, om.logk_field(len(tris), 2001))
+    mass = oadj.lumped_mass(pf, cf, 1)
+    J_o, g_o = oadj.gradient_nodal(pf, cf, bnd, nodal, mode, ustar, mass)
+    m = plan.lumped_mass()
+    us = torch.as_tensor(ustar, device="cuda")
+    pg = pv.clone().requires_grad_(True)
+    u = solve_nodal(plan, pg, cmode, tol=1e-13)
+    J = 0.5 * torch.sum(m * (u - us) ** 2)
+    J.backward()
+    g = pg.grad.cpu().numpy()
+    assert abs(J.item() - J_o) <= 1e-10 * abs(J_o)
+    assert np.abs(g - g_o).max() <= 1e-8 * np.abs(g_o).max()
+
+    def Jof(v):
+        with torch.no_grad():
+            uu = solve_nodal(plan, torch.as_tensor(v, device="cuda"), cmode, tol=1e-14)
+            return (0.5 * torch.sum(m * (uu - us) ** 2)).item()
+
+    interior = np.setdiff1d(np.arange(p1.shape[0]), bnd)
+    for i in rng.choice(interior, 5, replace=False):
+        e = np.zeros(p1.shape[0])
+        e[i] = 1e-6
+        fd = (Jof(nodal + e) - Jof(nodal - e)) / 2e-6
+        assert abs(fd - g[i]) <= 1e-6 * np.abs(g).max() + 1e-6 * abs(g[i])
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_tri_compact_export_matches_compress_eager(order):
+    pf, cf, tris, p1 = _mesh(7, order, seed=4)
+    logk = om.logk_field(len(tris), 1004)
+    plan = _plan(p1, tris, order)
+    g = 1.0 + pf[:, 0] - 2.0 * pf[:, 1]
+    vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"), g=torch.as_tensor(g, device="cuda"))
+    ip, ind, dat = plan.compact(vals)
+    ex = plan.export()
+    ipo, indo, dato = oa.compact_csr(ex["indptr"].cpu().numpy(), ex["indices"].cpu().numpy(), vals.cpu().numpy())
+    assert np.array_equal(ip.cpu().numpy(), ipo) and np.array_equal(ind.cpu().numpy(), indo)
+    assert np.array_equal(dat.cpu().numpy(), dato)
+    s, _ = _oracle_system(pf, cf, order, logk, g=g)
+    B = oa.compact(s)
+    assert np.array_equal(ip.cpu().numpy(), B.indptr) and np.array_equal(ind.cpu().numpy(), B.indices)
+    assert np.abs(dat.cpu().numpy() - B.data).max() <= VAL_TOL * np.abs(B.data).max()
+    assert np.abs(b.cpu().numpy() - s.b).max() <= 1e-11 * np.abs(s.b).max()
+
+
+def test_tri_jno_surface_end_to_end():
+    """The reference recipe on a 2-D domain (jno.domain.equi_distant_rect, P0 log k, jno.solve.cg)."""
+    import jno_b200 as jno
+
+    n = 16
+    d = jno.domain(jno.domain.equi_distant_rect(nx=n, ny=n), jitter=0.1, seed=0)
+    u, v = d.fem_symbols()
+    _r, s = d.fem_symbols(space="P0", names=("r", "s"))
+    xi, yi = d.variable("interior", split=True)
+    xb, yb = d.variable("boundary", split=True)
+    ui, vi = u.bind(x=xi, y=yi), v.bind(x=xi, y=yi)
+    logk = jno.np.parameter(s, name="logk")
+    fem = jno.fem([jno.np.exp(logk) * (ui.x * vi.x + ui.y * vi.y) - 1.0 * vi, u(xb, yb) - 0.0])
+    assert fem.dofs == (n + 1) ** 2 and fem.plan.dim == 2
+    lk = om.logk_field(2 * n * n, 1000)
+    A, b = fem.operator.evaluate({"logk": lk})
+    x = jno.solve.cg(tol=1e-8)(A, b, M=jno.precond.jacobi())
+    pf, cf, tris, p1 = _mesh(n, 1)
+    so, _ = _oracle_system(pf, cf, 1, lk)
+    xo = op.pcg(so.csr(), so.b, oa.jacobi_inverse(oa.matrix_diagonal(so)))[0]
+    assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+    Amf, bmf = fem.matrix_free({"logk": lk})
+    xf = jno.solve.cg(tol=1e-8)(Amf, bmf, M=jno.precond.jacobi())
+    assert np.linalg.norm(xf.cpu().numpy() - xo) <= 1e-7 * np.linalg.norm(xo)
+    with pytest.raises(NotImplementedError):
+        jno.fem([ui.x * vi.x - 1.0 * vi, u(xb, yb) - 0.0])  # the y stiffness term is missing
+
+
+def test_tri_surface_non_parametric_p2():
+    """A P2 form without a parameter on the rectangle: u = xy + x^2 - y^2 (harmonic) on the
+    boundary, f = 0; fem.solve() (Jacobi-BiCGStab) recovers it to 1e-9 (the 2-D form of
+    tests/test_fem_higher_order.py:133-150)."""
+    import jno_b200 as jno
+
+    d = jno.domain(jno.domain.equi_distant_rect(nx=6, ny=5), jitter=0.1, seed=7)
+    u, phi = d.fem_symbols(order=2)
+    xi, yi = d.variable("interior", split=True)
+    xb, yb = d.variable("boundary", split=True)
+    ui, vi = u.bind(x=xi, y=yi), phi.bind(x=xi, y=yi)
+    fem = jno.fem([ui.x * vi.x + ui.y * vi.y, u(xb, yb) - (xb * yb + xb * xb - yb * yb)])
+    pts = fem.points.cpu().numpy()
+    assert pts.shape[1] == 2 and fem.dofs == 13 * 11
+    sol = fem.solve(linear=jno.solve.bicgstab(tol=1e-12)).cpu().numpy()
+    exact = pts[:, 0] * pts[:, 1] + pts[:, 0] ** 2 - pts[:, 1] ** 2
+    assert np.linalg.norm(exact - sol) / np.linalg.norm(exact) < 1e-9
+
+
+@pytest.mark.parametrize("order,lo,hi", [(1, 1.7, 2.4), (2, 2.6, 3.4)])
+def test_tri_convergence_order(order, lo, hi):
+    """The gate of tests/test_fem_convergence.py:209-235 / :771-779 on the CUDA assembly and CG:
+    -Laplace u = 1 with u = x(1-x)/2 + sin(pi x) sinh(pi y) / sinh(pi) as Dirichlet data at every
+    boundary DOF; observed L2 order of P1 in [1.7, 2.4], of P2 in [2.6, 3.4] (true L2 error of the
+    device solution by CPU quadrature)."""
+    errs, hs = [], []
+    for n in (8, 16, 32):
+        pf, cf, tris, p1 = _mesh(n, order, seed=1)
+        plan = _plan(p1, tris, order)
+        g = oe.exact_poisson_2d(pf[:, 0], pf[:, 1])
+        vals, b = plan.assemble(None, mode=2, scale=1.0, f=1.0, g=torch.as_tensor(g, device="cuda"))
+        u, it, rel, st = plan.pcg(vals, b, inv_diag=plan.jacobi(vals), tol=1e-12)
+        assert st == 0
+        errs.append(oe.l2_error_2d(pf, cf, order, u.cpu().numpy(), oe.exact_poisson_2d))
+        hs.append(1.0 / n)
+    assert np.all(np.diff(errs) < 0), errs
+    p = np.polyfit(np.log(hs), np.log(errs), 1)[0]
+    assert lo <= p <= hi, (p, errs)
+
+
+def test_tri_status_paths():
+    pf, cf, tris, p1 = _mesh(4, 1)
+    bad = tris.copy()
+    bad[3, 2] = 10**6
+    with pytest.raises(ValueError):
+        _plan(p1, bad, 1)
+    bad = tris.copy()
+    bad[3, 2] = bad[3, 1]
+    with pytest.raises(ValueError):
+        _plan(p1, bad, 1)
+    with pytest.raises(ValueError):
+        _plan(p1, np.concatenate([tris, tris[:, :1]], axis=1), 1)  # [T, 4] cells with 2-D points
+    from jno_b200 import _lib
+
+    plan = _plan(p1, tris, 2)
+    with pytest.raises(_lib.FemkError):
+        plan.assemble(torch.zeros(plan.nvert, dtype=torch.float64, device="cuda"), mode=_lib.COEF_NODAL_EXP)
