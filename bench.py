@@ -302,8 +302,10 @@ def p2_variants(args, world, dev, timed):
 
 
 def tri_variants(world, dev, timed, n1=1024, n2=512):
-    """2-D triangles: P1 on 1024^2 rectangles (1.05M DOF) FP64 and mixed, P2 on 512^2 (1.05M DOF)
-    FP64; jittered +-0.1h, k = exp(N(0, 0.5^2)) per triangle, assemble + Jacobi-PCG to 1e-8, 3 steps."""
+    """2-D triangles: P1 on 1024^2 rectangles (1.05M DOF), P2 on 512^2 (1.05M DOF); jittered +-0.1h,
+    k = exp(N(0, 0.5^2)) per triangle, FP64 assemble + Jacobi-PCG to 1e-8, 3 steps. (The mixed solver
+    is not run here: at this condition number its FP32 inner CG needs more than 5x the FP64
+    iterations and misses the 20,000-iteration cap.)"""
     import torch
 
     from jno_b200.domain import jitter_interior_2d, rect_points_tris
@@ -319,7 +321,7 @@ def tri_variants(world, dev, timed, n1=1024, n2=512):
         b = torch.empty(plan.n, dtype=torch.float64, device=dev)
         inv = torch.empty(plan.n, dtype=torch.float64, device=dev)
         x = torch.empty(plan.n, dtype=torch.float64, device=dev)
-        info = {"it": [], "inner": []}
+        info = {"it": []}
 
         def s64(i):
             plan.assemble(fields[i % 3], vals=vals, b=b)
@@ -327,23 +329,38 @@ def tri_variants(world, dev, timed, n1=1024, n2=512):
             x.zero_()
             info["it"].append(plan.pcg(vals, b, x, inv, tol=1e-8)[1])
 
-        def s32(i):
-            plan.assemble(fields[i % 3], vals=vals, b=b)
-            plan.jacobi(vals, out=inv)
-            x.zero_()
-            info["inner"].append(plan.pcg_mixed(vals, b, inv, x, tol=1e-8)[1])
-
         base = {"workload": f"P{order} {nh}^2 triangles ({plan.ntet:,} triangles, {plan.n:,} DOF, {plan.nnz:,} nnz)"}
         ms64 = timed(s64, 3, 1) / 3
         out[f"tri_p{order}_{nh}_fp64"] = {**base, "value": world * plan.n / (ms64 / 1e3), "unit": "DOF/s",
                                           "ms_per_step": ms64, "iters": float(np.mean(info["it"]))}
-        if order == 1:
-            ms32 = timed(s32, 3, 1) / 3
-            out[f"tri_p{order}_{nh}_mixed"] = {**base, "value": world * plan.n / (ms32 / 1e3), "unit": "DOF/s",
-                                               "ms_per_step": ms32, "inner_iters": float(np.mean(info["inner"])),
-                                               "speedup_vs_fp64": ms64 / ms32}
         del plan
     return out
+
+
+def theta_variant(plan, fields, dev, timed, dt=1e-3, nsteps=10):
+    """Transient heat on the headline mesh (P1 128^3): the parametric route (k = exp(logk), rows
+    replaced), backward Euler, dt = 1e-3, u0 = sin(pi x) sin(pi y) sin(pi z): one step-operator
+    assembly + 10 Jacobi-BiCGStab steps to 1e-10 per march."""
+    import torch
+
+    from jno_b200 import _lib
+
+    pts = plan.export()["points"]
+    u0 = torch.sin(np.pi * pts[:, 0]) * torch.sin(np.pi * pts[:, 1]) * torch.sin(np.pi * pts[:, 2])
+    u = torch.empty_like(u0)
+    info = {}
+
+    def march(i):
+        S, R, q = plan.assemble_theta(fields[i % len(fields)], f=1.0, theta=1.0, dt=dt, dirichlet=_lib.DIRICHLET_ROWS)
+        u.copy_(u0)
+        _, iters, worst = plan.theta_march(S, R, q, u, nsteps)
+        info.setdefault("it", []).append(float(np.mean(iters)))
+        info.setdefault("res", []).append(worst)
+
+    ms = timed(march, 3, 1) / 3
+    return {"workload": f"P1 128^3 heat, backward Euler, dt={dt}, {nsteps} steps", "ms_per_march": ms,
+            "ms_per_step": ms / nsteps, "value": plan.n * nsteps / (ms / 1e3), "unit": "DOF-steps/s",
+            "bicgstab_iters_per_step": float(np.mean(info["it"])), "max_step_residual": float(np.max(info["res"]))}
 
 
 def batched_variant(dev, count=256, reps=3):
@@ -692,6 +709,7 @@ def run_ours(args):
                                       "ms_standalone": sell_standalone_ms}
         variants.update(p2_variants(args, world, dev, timed))
         variants.update(tri_variants(world, dev, timed))
+        variants["theta_p1_128"] = theta_variant(plan, fields, dev, timed)
         variants["adjoint_p1_64"] = adjoint_variant(dev)
         variants["batched_256"] = batched_variant(dev)
 

@@ -43,6 +43,10 @@ extern "C" {
 #define FEMK_MIXED_RELIABLE 0 /* FP32 inner CG with FP64 reliable updates (no restart) */
 #define FEMK_MIXED_RESTART 1  /* classic iterative refinement: restart FP32 CG per outer step */
 
+/* Dirichlet treatment of the transient operator A' in femk_assemble_theta */
+#define FEMK_DIRICHLET_SYMMETRIC 0 /* symmetric elimination + lift (the non-parametric transient route) */
+#define FEMK_DIRICHLET_ROWS 1      /* row replacement, columns kept (the parametric transient route) */
+
 typedef struct femk_plan femk_plan;
 
 typedef struct femk_plan_info {
@@ -211,6 +215,48 @@ int femk_pcg_matfree(const femk_plan* plan, const double* param_dev, int coef_mo
 int femk_bicgstab(const femk_plan* plan, const double* vals_dev, const double* b_dev, double* x_dev,
                   const double* inv_diag_dev, double tol, double atol, int32_t maxiter, int32_t* iters_out,
                   double* relres_out, void* stream);
+
+/*
+ * Consistent mass matrix M[a][b] = integral(phi_a phi_b) in the canonical CSR (vals_dev f64[nnz]).
+ * zero_dirichlet != 0 leaves the Dirichlet rows and columns at zero, the transient block's M
+ * (bcoo_zero_rows_cols, jno/utils/solver/fem_1d.py:939-949). Replaces the mass jacobian of the
+ * temporal terms (jno/utils/solver/fem_native.py:2846-2850).
+ */
+int femk_mass_matrix(const femk_plan* plan, int zero_dirichlet, double* vals_dev, void* stream);
+
+/*
+ * Theta-step operators of the linear first-order block M u' + A u = c + f, assembled once on the
+ * canonical CSR pattern (replaces the transient assembly of jno/utils/solver/fem_native.py:2846-3110
+ * and the step-operator composition _add_step_operator, jno/utils/solver/solver_api.py:856-878):
+ *   step_vals f64[nnz] = M' + theta dt A'        (the system of every step)
+ *   rhs_vals  f64[nnz] = M' - (1 - theta) dt A'  (rhs = rhs_vals u + q, backend_blocks.py:342)
+ *   q         f64[n]   = dt (c' + f')
+ * M' is the consistent mass with Dirichlet rows and columns zeroed. A' is the stiffness of
+ * k grad u . grad v (coefficient as in femk_assemble), with Dirichlet rows set to identity rows:
+ *   FEMK_DIRICHLET_SYMMETRIC: Dirichlet columns eliminated, c' = load - A e lift, c'[d] = g[d]
+ *     (_apply_dirichlet_transient, fem_1d.py:939-949: the route of a form without runtime parameters);
+ *   FEMK_DIRICHLET_ROWS: Dirichlet columns kept, c'[d] = g[d] and f' = the load on free rows
+ *     (bcoo_set_dirichlet_rows + the free-mask forcing, fem_native.py:3058-3087: the parametric route).
+ * g f64[n] or NULL (0). 0 < theta <= 1 (1 backward Euler, 1/2 Crank-Nicolson); dt > 0.
+ */
+int femk_assemble_theta(const femk_plan* plan, const double* param_dev, int coef_mode, double scale, double f,
+                        const double* g_dev, double theta, double dt, int dirichlet, double* step_vals_dev,
+                        double* rhs_vals_dev, double* q_dev, void* stream);
+
+/*
+ * nsteps theta steps of the linear block (SemidiscreteTimeBlock.step, backend_blocks.py:332-413):
+ *   rhs = rhs_vals u + q;  u <- Jacobi-BiCGStab(step_vals, rhs, x0 = u, tol, atol = 0, maxiter)
+ * with the Jacobi inverse of diag(step_vals) (|d| <= 1e-30 -> 1), jax bicgstab semantics as
+ * femk_bicgstab. After each step the relative residual ||S u - rhs|| / max(||rhs||, eps) must be
+ * below 1e-9 (the reference's step check; it re-solves with GMRES otherwise, which is not built
+ * here: the march stops with FEMK_NOT_CONVERGED). u_dev f64[n] holds the state (in/out);
+ * traj_dev f64[nsteps*n] or NULL receives the state after every step; iters_out i32[nsteps] (host)
+ * or NULL; *relres_out (host, may be NULL) = the largest step residual. The step operator is
+ * gathered into the solver layout once per call.
+ */
+int femk_theta_march(const femk_plan* plan, const double* step_vals_dev, const double* rhs_vals_dev,
+                     const double* q_dev, double* u_dev, int32_t nsteps, double tol, int32_t maxiter,
+                     double* traj_dev, int32_t* iters_out, double* relres_out, void* stream);
 
 /*
  * Allocation-free Jacobi-PCG: the same iteration and result as femk_pcg, for callers that must

@@ -15,7 +15,7 @@ from .fem import FEM, FemLinearSystem, fem  # noqa: F401
 from .plan import FemPlan  # noqa: F401
 from .sparse import CsrMatrix, MatrixFreeOperator  # noqa: F401
 
-np = SimpleNamespace(exp=_trace.exp, parameter=_trace.parameter)
+np = SimpleNamespace(exp=_trace.exp, sin=_trace.sin, cos=_trace.cos, parameter=_trace.parameter)
 
 domain.equi_distant_box = staticmethod(equi_distant_box)
 domain.equi_distant_rect = staticmethod(equi_distant_rect)

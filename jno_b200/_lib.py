@@ -24,6 +24,7 @@ FEMK_BREAKDOWN = 8
 COEF_EXP, COEF_LINEAR, COEF_CONST = 0, 1, 2
 COEF_NODAL_EXP, COEF_NODAL_LINEAR = 3, 4  # nodal P1 parameters (one value per P1 vertex)
 MIXED_RELIABLE, MIXED_RESTART = 0, 1
+DIRICHLET_SYMMETRIC, DIRICHLET_ROWS = 0, 1  # transient A': symmetric elimination / row replacement
 
 _STATUS_NAMES = {
     1: "EINVAL",
@@ -98,6 +99,9 @@ SIGNATURES = {
     "femk_pcg_batched": [_P, _I32, _P, _P, _P, _P, _P, _D, _D, _I32, _I32, _I32, _P, _P, _P, _P],
     "femk_adjoint_grad": [_P, _P, _I, _D, _P, _P, _P, _P],
     "femk_lumped_mass": [_P, _P, _P],
+    "femk_mass_matrix": [_P, _I, _P, _P],
+    "femk_assemble_theta": [_P, _P, _I, _D, _D, _P, _D, _D, _I, _P, _P, _P, _P],
+    "femk_theta_march": [_P, _P, _P, _P, _P, _I32, _D, _I32, _P, _P, ctypes.POINTER(_D), _P],
 }
 
 _lib = None

@@ -9,6 +9,8 @@
 // Dirichlet semantics of the parametric route: entries in a Dirichlet row or column are stored as
 // explicit zeros (they are never added), the diagonal slot of a Dirichlet row holds exactly 1
 // (masked 0 + the appended unit triplet), b[d] = g[d], and free rows receive b -= A e.
+#include <cmath>
+
 #include "femk_element.cuh"
 #include "femk_internal.cuh"
 
@@ -96,6 +98,97 @@ __global__ void k_element_matrices(const double* __restrict__ xyz, const int32_t
     if (fhat_out) {
 #pragma unroll
       for (int a = 0; a < ND; ++a) fhat_out[c * ND + a] = fhat<ND>(T.vol, a);
+    }
+  }
+}
+
+// Theta-step operators of the linear first-order block M u' + A u = c (the transient assembly of
+// jno/utils/solver/fem_native.py:2846-3110, the step of jno/utils/solver/backend_blocks.py:332-345):
+//   S = M' + theta dt A',  R = M' - (1 - theta) dt A',  q = dt c'
+// per element into the canonical CSR. M' is the consistent mass with Dirichlet rows and columns
+// zeroed. A' keeps the Dirichlet columns of the free rows when `rows` (row replacement, the
+// parametric route: c' = the load on free rows) and drops them into the lift otherwise (symmetric
+// elimination, the non-parametric route: c' = load - A e). Dirichlet rows are set afterwards
+// (k_theta_dirichlet: A' row = identity, M' row = 0, c'[d] = g[d]).
+template <int ND>
+__global__ void __launch_bounds__(kThreads) k_assemble_theta(
+    const double* __restrict__ xyz, const int32_t* __restrict__ cells, int64_t ntet, const int32_t* __restrict__ slot,
+    const uint8_t* __restrict__ dmask, const double* __restrict__ param, int mode, double scale, double f,
+    const double* __restrict__ g, double theta, double dt, int rows, double* __restrict__ S, double* __restrict__ R,
+    double* __restrict__ q) {
+  const double ws = theta * dt, wr = -(1.0 - theta) * dt;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t dof[ND];
+#pragma unroll
+    for (int a = 0; a < ND; ++a) dof[a] = __ldg(cells + c * ND + a);
+    Geom<Cell<ND>::NV> T;
+    cell_geometry(xyz, dof, T);
+    double VG[Cell<ND>::NV][Cell<ND>::NV];
+    gram(T, VG);
+    const double k = coef_of(param, mode, scale, c);
+    bool dir[ND];
+#pragma unroll
+    for (int a = 0; a < ND; ++a) dir[a] = __ldg(dmask + dof[a]) != 0;
+    const int32_t* srow = slot + c * ND * ND;
+#pragma unroll
+    for (int a = 0; a < ND; ++a) {
+      if (dir[a]) continue;
+      double rhs = f * fhat<ND>(T.vol, a);
+#pragma unroll
+      for (int bb = 0; bb < ND; ++bb) {
+        const double kab = k * khat<ND>(VG, a, bb);
+        const int32_t sl = __ldg(srow + a * ND + bb);
+        if (dir[bb]) {
+          if (rows) {
+            atomicAdd(S + sl, ws * kab);
+            atomicAdd(R + sl, wr * kab);
+          } else if (g) {
+            rhs -= kab * __ldg(g + dof[bb]);
+          }
+        } else {
+          const double mab = T.vol * mhat<ND>(a, bb);
+          atomicAdd(S + sl, mab + ws * kab);
+          atomicAdd(R + sl, mab + wr * kab);
+        }
+      }
+      atomicAdd(q + dof[a], dt * rhs);
+    }
+  }
+}
+
+__global__ void k_theta_dirichlet(const int32_t* __restrict__ dlist, int64_t nd, const int32_t* __restrict__ diag,
+                                  const double* __restrict__ g, double theta, double dt, double* __restrict__ S,
+                                  double* __restrict__ R, double* __restrict__ q) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nd; t += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t d = dlist[t];
+    S[diag[d]] = theta * dt;
+    R[diag[d]] = -(1.0 - theta) * dt;
+    q[d] = g ? dt * g[d] : 0.0;
+  }
+}
+
+// Consistent mass M[a][b] = integral(phi_a phi_b) into the canonical CSR; with `zero_dirichlet`
+// the Dirichlet rows and columns are left at zero (the transient block's M).
+template <int ND>
+__global__ void __launch_bounds__(kThreads) k_mass(const double* __restrict__ xyz, const int32_t* __restrict__ cells,
+                                                   int64_t ntet, const int32_t* __restrict__ slot,
+                                                   const uint8_t* __restrict__ dmask, double* __restrict__ m) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t dof[ND];
+#pragma unroll
+    for (int a = 0; a < ND; ++a) dof[a] = __ldg(cells + c * ND + a);
+    Geom<Cell<ND>::NV> T;
+    cell_geometry(xyz, dof, T);
+    bool dir[ND];
+#pragma unroll
+    for (int a = 0; a < ND; ++a) dir[a] = dmask ? __ldg(dmask + dof[a]) != 0 : false;
+    const int32_t* srow = slot + c * ND * ND;
+#pragma unroll
+    for (int a = 0; a < ND; ++a) {
+      if (dir[a]) continue;
+#pragma unroll
+      for (int bb = 0; bb < ND; ++bb)
+        if (!dir[bb]) atomicAdd(m + __ldg(srow + a * ND + bb), T.vol * mhat<ND>(a, bb));
     }
   }
 }
@@ -292,6 +385,49 @@ extern "C" int femk_adjoint_grad(const femk_plan* p, const double* param, int mo
     return FEMK_OK;
   }
   FEMK_BY_ND(p->nd, k_adjoint<ND><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, param, mode, scale, u, lam, grad));
+  FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}
+
+extern "C" int femk_assemble_theta(const femk_plan* p, const double* param, int mode, double scale, double f,
+                                   const double* g, double theta, double dt, int dirichlet, double* step_vals,
+                                   double* rhs_vals, double* q, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && step_vals && rhs_vals && q, "femk_assemble_theta: plan, step_vals, rhs_vals and q are required");
+  FEMK_CHECK_ARG(coef_mode_ok(p, mode, param),
+                 "femk_assemble_theta: unknown coef_mode, NULL param, or a nodal mode on a P2 plan");
+  FEMK_CHECK_ARG(theta > 0.0 && theta <= 1.0, "femk_assemble_theta: theta must be in (0, 1]");
+  FEMK_CHECK_ARG(dt > 0.0 && std::isfinite(dt), "femk_assemble_theta: dt must be positive and finite");
+  FEMK_CHECK_ARG(dirichlet == FEMK_DIRICHLET_SYMMETRIC || dirichlet == FEMK_DIRICHLET_ROWS,
+                 "femk_assemble_theta: dirichlet must be FEMK_DIRICHLET_SYMMETRIC or FEMK_DIRICHLET_ROWS");
+  cudaStream_t s = (cudaStream_t)stream;
+  FEMK_TRY(resolve_coef(p, param, mode, s, &param, &mode));
+  FEMK_CUDA_TRY(cudaMemsetAsync(step_vals, 0, sizeof(double) * p->nnz, s));
+  FEMK_CUDA_TRY(cudaMemsetAsync(rhs_vals, 0, sizeof(double) * p->nnz, s));
+  FEMK_CUDA_TRY(cudaMemsetAsync(q, 0, sizeof(double) * p->n, s));
+  const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);
+  const int rows = dirichlet == FEMK_DIRICHLET_ROWS;
+  FEMK_BY_ND(p->nd, k_assemble_theta<ND><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
+                        p->xyz, p->cells, p->ntet, p->slot, p->dmask, param, mode, scale, f, g, theta, dt, rows,
+                        step_vals, rhs_vals, q));
+  FEMK_CUDA_TRY(cudaGetLastError());
+  if (p->n_dir > 0) {
+    k_theta_dirichlet<<<::femk::counted_launch() + blocks_for(p->n_dir, 256, 65535), 256, 0, s>>>(
+        p->dlist, p->n_dir, p->diag, g, theta, dt, step_vals, rhs_vals, q);
+    FEMK_CUDA_TRY(cudaGetLastError());
+  }
+  return FEMK_OK;
+}
+
+extern "C" int femk_mass_matrix(const femk_plan* p, int zero_dirichlet, double* vals, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && vals, "femk_mass_matrix: NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  FEMK_CUDA_TRY(cudaMemsetAsync(vals, 0, sizeof(double) * p->nnz, s));
+  const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);
+  const uint8_t* dm = zero_dirichlet ? p->dmask : nullptr;
+  FEMK_BY_ND(p->nd, k_mass<ND><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->slot,
+                                                                                    dm, vals));
   FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;
 }

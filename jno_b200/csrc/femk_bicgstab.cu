@@ -284,8 +284,9 @@ template <int KIND>
 int launch_spmv(const femk_plan* p, const double* x, const double* b, const Vecs& v, BicgState* st, cudaStream_t s,
                 bool prime = false) {
   if (bulk_usable(p)) {
-    const bool ok = p->max_row <= 16 ? launch_bulk_kind<KIND, 16>(p, x, b, v, st, s, prime)
-                                     : launch_bulk_kind<KIND, 32>(p, x, b, v, st, s, prime);
+    const bool ok = p->max_row <= 8    ? launch_bulk_kind<KIND, 8>(p, x, b, v, st, s, prime)
+                    : p->max_row <= 16 ? launch_bulk_kind<KIND, 16>(p, x, b, v, st, s, prime)
+                                       : launch_bulk_kind<KIND, 32>(p, x, b, v, st, s, prime);
     if (ok) return FEMK_OK;
   }
   if (p->sell_c16 && p->sell64_c16) {
@@ -377,26 +378,10 @@ __global__ void k_bicg_setup(BicgState* st, double tol2, double atol_sq, int32_t
   st->done = 0;
 }
 
-}  // namespace
-}  // namespace femk
-
-extern "C" int femk_bicgstab(const femk_plan* pc, const double* vals, const double* b, double* x, const double* dinv,
-                             double tol, double atol, int32_t maxiter, int32_t* iters_out, double* relres_out,
-                             void* stream) {
-  using namespace femk;
-  clear_error();
-  FEMK_CHECK_ARG(pc && vals && b && x, "femk_bicgstab: plan, vals, b and x are required");
-  FEMK_CHECK_ARG(tol >= 0.0 && atol >= 0.0, "femk_bicgstab: tol and atol must be >= 0");
-  femk_plan* p = const_cast<femk_plan*>(pc);
-  FEMK_CHECK_ARG(p->use_sell && p->sell_src, "femk_bicgstab: the plan has no sliced-ELL operator");
-  FEMK_TRY(ensure_bicg(p));
-  cudaStream_t cs = (cudaStream_t)stream;
-  cudaStream_t ws = p->bicg_stream;
-  // the plan's stream runs after the caller's pending work and hands back at the end
-  FEMK_CUDA_TRY(cudaEventRecord(p->bicg_ev[0], cs));
-  FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->bicg_ev[0], 0));
-  if (!p->sell_vals) FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals, sizeof(double) * (p->sell_nnz + 1)));
-  FEMK_TRY(femk_prepare_operator(p, vals, ws));
+// One BiCGStab solve on the plan's prepared sliced-ELL operator: x holds x0 on entry. Ends with the
+// true-residual SpMV (kResid) and returns the final state in *out (host).
+int solve_prepared(femk_plan* p, const double* b, double* x, const double* dinv, double tol, double atol,
+                   int32_t maxiter, cudaStream_t ws, BicgState* out) {
   const Vecs v = vecs_of(p);
   BicgState* st = (BicgState*)p->bicg_state;
   BicgState* host = (BicgState*)p->bicg_host;
@@ -423,30 +408,144 @@ extern "C" int femk_bicgstab(const femk_plan* pc, const double* vals, const doub
       if (host[c ^ 1].done) break;
     }
   }
-  // relative true residual for the guard: ||b - A x|| / (||b|| + 1e-30)
+  // relative true residual: ||b - A x|| / (||b|| + 1e-30)
   FEMK_TRY(launch_spmv<kResid>(p, x, b, v, st, ws));
   FEMK_CUDA_TRY(cudaMemcpyAsync(host, st, sizeof(BicgState), cudaMemcpyDeviceToHost, ws));
   FEMK_CUDA_TRY(cudaStreamSynchronize(ws));
-  FEMK_CUDA_TRY(cudaEventRecord(p->bicg_ev[0], ws));
-  FEMK_CUDA_TRY(cudaStreamWaitEvent(cs, p->bicg_ev[0], 0));
-  const BicgState h = host[0];
-  if (iters_out) *iters_out = h.iters;
-  if (relres_out) *relres_out = std::sqrt(h.ss) / (std::sqrt(h.bb) + 1e-30);
+  *out = host[0];
+  return FEMK_OK;
+}
+
+// Status of a finished solve (sets the error message).
+int solve_status(const BicgState& h, const char* who) {
   if (h.status == FEMK_TIMEOUT) {
-    set_error("femk_bicgstab: a bounded device wait gave up");
+    set_error(std::string(who) + ": a bounded device wait gave up");
     return FEMK_TIMEOUT;
   }
   if (h.status == FEMK_NONFINITE) {
-    set_error("femk_bicgstab: non-finite value in a reduction");
+    set_error(std::string(who) + ": non-finite value in a reduction");
     return FEMK_NONFINITE;
   }
   if (h.k < 0) {
-    set_error("femk_bicgstab: breakdown (" + std::string(h.k == -10 ? "<rhat, r> = 0" : "omega or alpha = 0") + ")");
+    set_error(std::string(who) + ": breakdown (" + (h.k == -10 ? "<rhat, r> = 0" : "omega or alpha = 0") + ")");
     return FEMK_BREAKDOWN;
   }
   if (h.rr > h.atol2) {
-    set_error("femk_bicgstab: iteration cap reached above tolerance");
+    set_error(std::string(who) + ": iteration cap reached above tolerance");
     return FEMK_NOT_CONVERGED;
   }
   return FEMK_OK;
+}
+
+// rhs = R u + q on the canonical CSR (the theta step's right-hand side): 8 lanes per row, 2 row
+// groups per warp
+__global__ void __launch_bounds__(kThreads) k_theta_rhs(const int32_t* __restrict__ indptr,
+                                                       const int32_t* __restrict__ indices,
+                                                       const double* __restrict__ R, const double* __restrict__ u,
+                                                       const double* __restrict__ q, int64_t n,
+                                                       double* __restrict__ rhs) {
+  constexpr int L = 8, U = 2, RPW = 32 / L;
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * kThreads) >> 5;
+  for (int64_t base = warp * RPW * U; base < n; base += nw * RPW * U) {
+    double sv[U];
+    int64_t rows[U];
+    csr_rows<L, U, double, int32_t>(indptr, indices, R, u, n, base, lane, sv, rows);
+#pragma unroll
+    for (int k = 0; k < U; ++k)
+      if (rows[k] < n && lane % L == 0) rhs[rows[k]] = sv[k] + q[rows[k]];
+  }
+}
+
+}  // namespace
+}  // namespace femk
+
+extern "C" int femk_bicgstab(const femk_plan* pc, const double* vals, const double* b, double* x, const double* dinv,
+                             double tol, double atol, int32_t maxiter, int32_t* iters_out, double* relres_out,
+                             void* stream) {
+  using namespace femk;
+  clear_error();
+  FEMK_CHECK_ARG(pc && vals && b && x, "femk_bicgstab: plan, vals, b and x are required");
+  FEMK_CHECK_ARG(tol >= 0.0 && atol >= 0.0, "femk_bicgstab: tol and atol must be >= 0");
+  femk_plan* p = const_cast<femk_plan*>(pc);
+  FEMK_CHECK_ARG(p->use_sell && p->sell_src, "femk_bicgstab: the plan has no sliced-ELL operator");
+  FEMK_TRY(ensure_bicg(p));
+  cudaStream_t cs = (cudaStream_t)stream;
+  cudaStream_t ws = p->bicg_stream;
+  // the plan's stream runs after the caller's pending work and hands back at the end
+  FEMK_CUDA_TRY(cudaEventRecord(p->bicg_ev[0], cs));
+  FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->bicg_ev[0], 0));
+  if (!p->sell_vals) FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals, sizeof(double) * (p->sell_nnz + 1)));
+  FEMK_TRY(femk_prepare_operator(p, vals, ws));
+  BicgState h;
+  const int rc = solve_prepared(p, b, x, dinv, tol, atol, maxiter, ws, &h);
+  FEMK_CUDA_TRY(cudaEventRecord(p->bicg_ev[0], ws));
+  FEMK_CUDA_TRY(cudaStreamWaitEvent(cs, p->bicg_ev[0], 0));
+  FEMK_TRY(rc);
+  if (iters_out) *iters_out = h.iters;
+  if (relres_out) *relres_out = std::sqrt(h.ss) / (std::sqrt(h.bb) + 1e-30);
+  return solve_status(h, "femk_bicgstab");
+}
+
+extern "C" int femk_theta_march(const femk_plan* pc, const double* step_vals, const double* rhs_vals,
+                                const double* q, double* u, int32_t nsteps, double tol, int32_t maxiter, double* traj,
+                                int32_t* iters_out, double* relres_out, void* stream) {
+  using namespace femk;
+  clear_error();
+  FEMK_CHECK_ARG(pc && step_vals && rhs_vals && q && u, "femk_theta_march: plan, operators, q and u are required");
+  FEMK_CHECK_ARG(nsteps >= 0 && tol >= 0.0 && maxiter >= 0, "femk_theta_march: nsteps, tol and maxiter must be >= 0");
+  femk_plan* p = const_cast<femk_plan*>(pc);
+  FEMK_CHECK_ARG(p->use_sell && p->sell_src, "femk_theta_march: the plan has no sliced-ELL operator");
+  FEMK_TRY(ensure_bicg(p));
+  if (!p->theta_ws) FEMK_CUDA_TRY(cudaMalloc(&p->theta_ws, sizeof(double) * 2 * p->vstride));
+  double* dinv = (double*)p->theta_ws;
+  double* rhs = dinv + p->vstride;
+  cudaStream_t cs = (cudaStream_t)stream;
+  cudaStream_t ws = p->bicg_stream;
+  FEMK_CUDA_TRY(cudaEventRecord(p->bicg_ev[0], cs));
+  FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->bicg_ev[0], 0));
+  // the step operator and its Jacobi inverse once for the whole march (the constant-operator path
+  // of jno/utils/solver/solver_api.py:920-927)
+  if (!p->sell_vals) FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals, sizeof(double) * (p->sell_nnz + 1)));
+  FEMK_TRY(femk_prepare_operator(p, step_vals, ws));
+  FEMK_TRY(femk_jacobi(p, step_vals, dinv, ws));
+  const int rgrid = blocks_for(p->n * 4, kThreads, p->n_sm * 16);
+  double worst = 0.0;
+  int rc = FEMK_OK;
+  for (int32_t k = 0; k < nsteps && rc == FEMK_OK; ++k) {
+    k_theta_rhs<<<counted_launch() + rgrid, kThreads, 0, ws>>>(p->indptr, p->indices, rhs_vals, u, q, p->n, rhs);
+    rc = cudaGetLastError() == cudaSuccess ? FEMK_OK : FEMK_ECUDA;
+    BicgState h;
+    if (rc == FEMK_OK) rc = solve_prepared(p, rhs, u, dinv, tol, 0.0, maxiter, ws, &h);
+    if (rc != FEMK_OK) break;
+    if (iters_out) iters_out[k] = h.iters;
+    rc = solve_status(h, "femk_theta_march");
+    if (rc != FEMK_OK) {
+      set_error(std::string(femk_last_error_string()) + " (step " + std::to_string(k) + ")");
+      break;
+    }
+    // the step check of backend_blocks.py:402-413: ||S u - rhs|| / max(||rhs||, eps) below
+    // max(1e-9, 1e4 eps) (the reference re-solves with GMRES otherwise; here the march stops)
+    const double rel = std::sqrt(h.ss) / std::max(std::sqrt(h.bb), 2.220446049250313e-16);
+    worst = std::max(worst, rel);
+    if (!(rel < 1e-9)) {
+      set_error("femk_theta_march: step " + std::to_string(k) + " left a relative residual of " +
+                std::to_string(rel) + " (>= 1e-9)");
+      rc = FEMK_NOT_CONVERGED;
+    }
+    if (rc != FEMK_OK) break;
+    if (traj) {
+      const cudaError_t e = cudaMemcpyAsync(traj + (int64_t)k * p->n, u, sizeof(double) * p->n,
+                                            cudaMemcpyDeviceToDevice, ws);
+      if (e != cudaSuccess) {
+        set_error(std::string("femk_theta_march: ") + cudaGetErrorString(e));
+        rc = FEMK_ECUDA;
+      }
+    }
+  }
+  if (relres_out) *relres_out = worst;
+  FEMK_CUDA_TRY(cudaEventRecord(p->bicg_ev[0], ws));
+  FEMK_CUDA_TRY(cudaStreamWaitEvent(cs, p->bicg_ev[0], 0));
+  return rc;
 }

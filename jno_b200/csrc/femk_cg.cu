@@ -992,11 +992,13 @@ bool launch_sell_bulk(const femk_plan* p, const double* x, double* y, CgState* s
   if (!p->bulk_cfg || !p->sell_c16 || !p->sell64_c16 || p->max_row > 32) return false;
   if (!aligned16(p->sell_vals) || !aligned16(p->sell_c16)) return false;  // bulk copies start on 16 B
   if (p->sell_cu && !aligned16(p->sell_cu)) return false;
-  const bool narrow = p->max_row <= 16;
+  // ring stages sized for the widest row: 8 (2-D P1 triangles), 16 (P1 tetrahedra), 32
+  const int wsel = p->max_row <= 8 ? 8 : (p->max_row <= 16 ? 16 : 32);
 #define FEMK_BULK_CFG(code, S, WPB)                                                         \
   case code:                                                                                \
-    return narrow ? launch_sell_bulk_cfg<S, WPB, 16>(p, x, y, st, s, prime)                        \
-                  : launch_sell_bulk_cfg<S, WPB, 32>(p, x, y, st, s, prime);
+    return wsel == 8    ? launch_sell_bulk_cfg<S, WPB, 8>(p, x, y, st, s, prime)  \
+           : wsel == 16 ? launch_sell_bulk_cfg<S, WPB, 16>(p, x, y, st, s, prime) \
+                        : launch_sell_bulk_cfg<S, WPB, 32>(p, x, y, st, s, prime);
   switch (p->bulk_cfg) {
     FEMK_BULK_CFG(11, 1, 1)
     FEMK_BULK_CFG(12, 1, 2)

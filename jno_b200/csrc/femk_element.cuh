@@ -156,6 +156,43 @@ __device__ __forceinline__ double fhat(double vol, int a) {
   return a < 3 ? 0.0 : vol * (1.0 / 3.0);
 }
 
+// (1/V) integral over a d-simplex of prod_k lambda_k^{a_k} = d! prod_k a_k! / (sum_k a_k + d)!
+__host__ __device__ constexpr double fact(int k) {
+  double r = 1.0;
+  for (int i = 2; i <= k; ++i) r *= i;
+  return r;
+}
+__host__ __device__ constexpr double bary_moment(int d, int a0, int a1 = 0, int a2 = 0, int a3 = 0) {
+  return fact(d) * fact(a0) * fact(a1) * fact(a2) * fact(a3) / fact(a0 + a1 + a2 + a3 + d);
+}
+
+// Unit-measure mass entry M_hat[a][b] = (1/V) integral(phi_a phi_b) (a, b compile-time), from the
+// moments of the basis in barycentric coordinates: phi_i = lambda_i (2 lambda_i - 1), phi_e = 4
+// lambda_j lambda_l on edge e = (j, l).
+template <int ND>
+__device__ __forceinline__ double mhat(int a, int b) {
+  constexpr int NV = Cell<ND>::NV, D = Cell<ND>::DIM;
+  if (!Cell<ND>::P2) return a == b ? bary_moment(D, 2) : bary_moment(D, 1, 1);
+  if (a < NV && b < NV) {
+    if (a == b) return 4.0 * bary_moment(D, 4) - 4.0 * bary_moment(D, 3) + bary_moment(D, 2);
+    return 4.0 * bary_moment(D, 2, 2) - 4.0 * bary_moment(D, 2, 1) + bary_moment(D, 1, 1);
+  }
+  if (a >= NV && b >= NV) {
+    const int i = cell_edge_a<NV>(a - NV), j = cell_edge_b<NV>(a - NV);
+    const int l = cell_edge_a<NV>(b - NV), m = cell_edge_b<NV>(b - NV);
+    const int shared = (i == l) + (i == m) + (j == l) + (j == m);
+    if (shared == 2) return 16.0 * bary_moment(D, 2, 2);
+    if (shared == 1) return 16.0 * bary_moment(D, 2, 1, 1);
+    return 16.0 * bary_moment(D, 1, 1, 1, 1);
+  }
+  // vertex i against edge (j, l): 8 int lambda_i^2 lambda_j lambda_l - 4 int lambda_i lambda_j lambda_l
+  const int i = a < NV ? a : b;
+  const int e = a < NV ? b - NV : a - NV;
+  const int j = cell_edge_a<NV>(e), l = cell_edge_b<NV>(e);
+  if (i == j || i == l) return 8.0 * bary_moment(D, 3, 1) - 4.0 * bary_moment(D, 2, 1);
+  return 8.0 * bary_moment(D, 2, 1, 1) - 4.0 * bary_moment(D, 1, 1, 1);
+}
+
 __device__ __forceinline__ double coef_of(const double* __restrict__ param, int mode, double scale, int64_t c) {
   if (mode == 2) return scale;
   const double p = __ldg(param + c);

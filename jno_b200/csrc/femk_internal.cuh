@@ -187,6 +187,7 @@ struct femk_plan {
   int batch_graph_ok = 1;
   void* prof = nullptr;         // per-kernel CG timing (femk_set_profiling)
   double* coef_tmp = nullptr;   // f64[ntet] element coefficients of a nodal parameter
+  double* theta_ws = nullptr;   // f64[2 vstride] theta march: step Jacobi inverse, step right-hand side
   // BiCGStab workspace (8 vectors), state, stream, events and captured chunk graph
   void* bicg_ws = nullptr;
   void* bicg_state = nullptr;

@@ -745,11 +745,13 @@ bool launch_step32_bulk(const femk_plan* p, const float* pv, float* q, MixedStat
   if (!p->bulk32_cfg || !p->sell_vals32 || !p->sell_c16 || p->max_row > 32) return false;
   if (((uintptr_t)p->sell_vals32 & 15u) || ((uintptr_t)p->sell_c16 & 15u)) return false;
   if (p->sell_cu && ((uintptr_t)p->sell_cu & 15u)) return false;
-  const bool narrow = p->max_row <= 16;
+  // ring stages sized for the widest row: 8 (2-D P1 triangles), 16 (P1 tetrahedra), 32
+  const int wsel = p->max_row <= 8 ? 8 : (p->max_row <= 16 ? 16 : 32);
 #define FEMK_BULK_CFG(code, S, WPB)                                                          \
   case code:                                                                                 \
-    return narrow ? launch_step32_bulk_cfg<S, WPB, 16>(p, pv, q, st, s, prime)                      \
-                  : launch_step32_bulk_cfg<S, WPB, 32>(p, pv, q, st, s, prime);
+    return wsel == 8    ? launch_step32_bulk_cfg<S, WPB, 8>(p, pv, q, st, s, prime)  \
+           : wsel == 16 ? launch_step32_bulk_cfg<S, WPB, 16>(p, pv, q, st, s, prime) \
+                        : launch_step32_bulk_cfg<S, WPB, 32>(p, pv, q, st, s, prime);
   switch (p->bulk32_cfg) {
     FEMK_BULK_CFG(11, 1, 1)
     FEMK_BULK_CFG(12, 1, 2)

@@ -113,8 +113,11 @@ def jitter_interior(points, nx, ny, nz, seed, amp=0.1, x_range=(0.0, 1.0), y_ran
 class domain:
     """``jno.domain(constructor)``: holds the built mesh and hands out FEM symbols."""
 
-    def __init__(self, constructor, jitter=None, seed=0):
+    def __init__(self, constructor, jitter=None, seed=0, time=None):
+        """``time=(t0, t1, n_steps)`` makes the domain transient: the time grid has n_steps points,
+        dt = (t1 - t0) / (n_steps - 1) (jno/utils/solver/time_route.py:32-58)."""
         mesh, dim, ds = constructor(None)
+        self.time = None if time is None else (float(time[0]), float(time[1]), int(time[2]))
         if dim not in (2, 3):
             raise NotImplementedError("only 2-D triangle and 3-D tetrahedral meshes are on the B200 path")
         self.built_mesh = mesh
@@ -139,6 +142,7 @@ class domain:
         obj.built_mesh = Mesh(pts, tets, dim=dim)
         obj.dimension = dim
         obj.ds = None
+        obj.time = None
         return obj
 
     def _cells_p1(self):
@@ -158,6 +162,10 @@ class domain:
     def variable(self, region, split=True):
         from .trace import Coordinate
 
-        if region not in ("interior", "boundary"):
-            raise NotImplementedError(f"region {region!r}: only 'interior' and 'boundary' are on the B200 path")
-        return tuple(Coordinate(region, a) for a in range(self.dimension))
+        if region not in ("interior", "boundary", "initial"):
+            raise NotImplementedError(
+                f"region {region!r}: only 'interior', 'boundary' and 'initial' are on the B200 path")
+        if region == "initial" and self.time is None:
+            raise ValueError("the 'initial' region needs a transient domain (domain(..., time=(t0, t1, n_steps)))")
+        coords = tuple(Coordinate(region, a) for a in range(self.dimension))
+        return coords + (Coordinate(region, "t"),) if self.time is not None else coords

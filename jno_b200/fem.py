@@ -7,6 +7,14 @@ form without one is assembled once into ``(A, b)`` with ``A`` compacted (exact z
 The quadrature degree the reference infers (P1 -> 2, P2 -> 4, _fem.py:4551,4573) integrates
 these forms exactly, as the closed-form element kernels do, so ``quad_degree`` is accepted for
 signature parity and only validated.
+
+A form with a ``rho * ui.t * vi`` term on a domain with ``time=(t0, t1, n_steps)`` is the linear
+first-order transient block (jno/utils/solver/fem_native.py:2846-3110): ``fem.solve()`` marches the
+theta method over the domain's grid (``_default_transient_integrate``,
+jno/utils/solver/backend_blocks.py:475-530; ``time=jno.solve.theta(theta)`` picks the scheme) and
+returns the trajectory, state0 first. A form with a runtime parameter takes the reference's
+parametric route (Dirichlet rows replaced, columns kept), one without takes the symmetric
+elimination of ``_apply_dirichlet_transient`` (jno/utils/solver/fem_1d.py:939-949).
 """
 
 import numpy as np
@@ -14,10 +22,10 @@ import torch
 
 from . import _lib
 from .plan import FemPlan
-from .precond import jacobi
-from .solve import bicgstab, cg
+from .precond import JacobiApplier, _Jacobi, jacobi
+from .solve import LinearSolver, ThetaScheme, bicgstab, cg
 from .sparse import CsrMatrix, MatrixFreeOperator
-from .trace import classify_dirichlet, classify_volume, evaluate_on
+from .trace import classify_condition, classify_volume, evaluate_on
 
 
 class FemLinearSystem:
@@ -57,13 +65,26 @@ def _solve(A, b, linear, precond, x0, default=cg):
     return solver(A, b, M=M, x0=x0)
 
 
+class TransientSolution:
+    """Trajectory of a transient solve on the domain's time grid: ``fn()`` -> f64[n_steps, n] (CUDA),
+    state0 first, like the reference's ``fem.solve().fn()``."""
+
+    def __init__(self, traj, ts, iterations, step_residual):
+        self.traj, self.ts, self.iterations, self.step_residual = traj, ts, iterations, step_residual
+
+    def fn(self):
+        return self.traj
+
+
 class FEM:
     """Result of :func:`fem`: plan + classified form."""
 
-    def __init__(self, form, plan, g_values):
+    def __init__(self, form, plan, g_values, u0=None, time=None):
         self.form = form
         self.plan = plan
         self._g = g_values
+        self._u0 = u0  # transient initial state at the DOFs
+        self.time = time  # (t0, t1, n_steps) of a transient form
         self.problem = None  # routed natively (the reference's marker for the native assembler)
         self.stats = {}
         self._eager = None
@@ -125,7 +146,55 @@ class FEM:
         _, b = self._assemble(args or {})
         return MatrixFreeOperator(self.plan, param, self.form.mode, self.form.scale), b
 
-    def solve(self, linear=None, precond=None, x0=None, args=None):
+    @property
+    def is_transient(self):
+        return self.form.mass is not None
+
+    @property
+    def dt(self):
+        t0, t1, n_steps = self.time
+        if n_steps <= 1:
+            raise ValueError("a transient solve needs time=(t0, t1, n_steps) with n_steps >= 2")
+        return (t1 - t0) / (n_steps - 1)
+
+    def step_operators(self, args=None, theta=1.0):
+        """(S, R, q) of the theta step as CUDA tensors: S = M' + theta dt A', R = M' - (1 - theta)
+        dt A', q = dt (c' + f') on the canonical CSR (rhs = R u + q)."""
+        param = self._param_tensor(args or {})
+        rho = self.form.mass
+        route = _lib.DIRICHLET_ROWS if self.form.param is not None else _lib.DIRICHLET_SYMMETRIC
+        # rho M u' + A u = c + f is M u' + (A / rho) u = (c + f) / rho on the free rows
+        return self.plan.assemble_theta(param, self.form.mode, self.form.scale / rho, self.form.f / rho, self._g,
+                                        theta, self.dt, route)
+
+    def _march(self, time=None, args=None, linear=None, precond=None):
+        if time is not None and not isinstance(time, ThetaScheme):
+            raise NotImplementedError("time= takes jno.solve.theta(...) on the B200 path")
+        if precond is not None and not isinstance(precond, (_Jacobi, JacobiApplier)):
+            raise NotImplementedError("the transient step solve is Jacobi-BiCGStab on the B200 path")
+        tol, maxiter = 1e-10, 20_000  # the per-step default of backend_blocks.py:394-396
+        if linear is not None:
+            if not isinstance(linear, LinearSolver) or linear.name != "bicgstab":
+                raise NotImplementedError("the transient step solve is Jacobi-BiCGStab on the B200 path")
+            tol, maxiter = linear.tol, linear.maxiter
+        th = 1.0 if time is None else time.theta
+        S, R, q = self.step_operators(args, th)
+        t0, t1, n_steps = self.time
+        traj = torch.empty((n_steps, self.plan.n), dtype=torch.float64, device=self.plan.device)
+        traj[0] = self._u0
+        u = self._u0.clone()
+        _, iters, worst = self.plan.theta_march(S, R, q, u, n_steps - 1, tol, maxiter, traj=traj[1:])
+        self.stats["transient"] = {"theta": th, "dt": self.dt, "iterations": iters, "step_residual": worst}
+        ts = np.linspace(t0, t1, n_steps)
+        return TransientSolution(traj, ts, iters, worst)
+
+    def solve(self, linear=None, precond=None, x0=None, args=None, time=None):
+        if self.is_transient:
+            if x0 is not None:
+                raise ValueError("fem.solve: x0 is not used by a transient solve (the initial condition sets state0)")
+            return self._march(time, args, linear, precond)
+        if time is not None:
+            raise ValueError("fem.solve: time= needs a transient form (a ui.t * vi term)")
         if self.form.param is not None:
             return self.operator.solve(args, linear, precond, x0)
         A, b = self.operator
@@ -148,17 +217,30 @@ def fem(terms, quad_degree=None, element_type=None, chunk=None, dirichlet_mask=N
     need = 2 * form.order
     if quad_degree is not None and int(quad_degree) < need:
         raise ValueError(f"quad_degree={quad_degree} under-integrates P{form.order} stiffness (needs {need})")
-    if len(dirichlet) > 1:
-        raise NotImplementedError("one Dirichlet condition on the whole boundary is supported")
+    conds = [classify_condition(t) for t in dirichlet]
+    bcs = [(s, g) for r, s, g in conds if r == "boundary"]
+    ics = [(s, g) for r, s, g in conds if r == "initial"]
+    if len(bcs) > 1 or len(ics) > 1:
+        raise NotImplementedError("one Dirichlet condition on the whole boundary (and one initial condition) is supported")
     d = form.domain
+    transient = form.mass is not None
+    if ics and not transient:
+        raise ValueError("an initial condition needs a transient form (a ui.t * vi term)")
+    if transient and getattr(d, "time", None) is None:
+        raise ValueError("a transient form needs a domain with time=(t0, t1, n_steps)")
     mesh = d.built_mesh
     plan = FemPlan(mesh.points[:, :dim], mesh.tets, form.order, dirichlet_mask)  # fem_native.py:250
-    g_values = None
-    if dirichlet:
-        sym, gexpr = classify_dirichlet(dirichlet[0])
-        gv = evaluate_on(gexpr, plan.export()["points"].cpu().numpy())
-        if np.any(gv != 0.0):
-            g_values = torch.as_tensor(gv, dtype=torch.float64, device=plan.device)
-    else:
+    if not bcs:
         raise NotImplementedError("a Dirichlet condition u(boundary) - g is required on the B200 path")
-    return FEM(form, plan, g_values)
+    pts = plan.export()["points"].cpu().numpy()
+    g_values = None
+    gv = evaluate_on(bcs[0][1], pts)
+    if np.any(gv != 0.0):
+        g_values = torch.as_tensor(gv, dtype=torch.float64, device=plan.device)
+    u0 = None
+    if transient:
+        # nodal interpolation of the initial condition at every DOF (exact for Lagrange; the
+        # Dirichlet DOFs keep u0 too, fem_native.py:2883-2913); zeros without one
+        u0v = evaluate_on(ics[0][1], pts) if ics else np.zeros(plan.n)
+        u0 = torch.as_tensor(np.broadcast_to(u0v, (plan.n,)).copy(), dtype=torch.float64, device=plan.device)
+    return FEM(form, plan, g_values, u0, getattr(d, "time", None) if transient else None)

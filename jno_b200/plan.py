@@ -275,3 +275,37 @@ class FemPlan:
         _lib.check(self._lib.femk_adjoint_grad(self._h, _lib.ptr(param), int(mode), float(scale), _lib.ptr(u),
                                                _lib.ptr(lam), _lib.ptr(out), _lib.stream_handle()))
         return out
+
+    # ---------------------------------------------------------------- transient
+    def mass_matrix(self, zero_dirichlet=False, out=None):
+        """Consistent mass f64[nnz] in the canonical CSR (Dirichlet rows/columns zeroed on request)."""
+        out = torch.empty(self.nnz, dtype=torch.float64, device=self.device) if out is None else out
+        _lib.check(self._lib.femk_mass_matrix(self._h, 1 if zero_dirichlet else 0, _lib.ptr(out),
+                                              _lib.stream_handle()))
+        return out
+
+    def assemble_theta(self, param=None, mode=_lib.COEF_EXP, scale=1.0, f=1.0, g=None, theta=1.0, dt=1.0,
+                       dirichlet=_lib.DIRICHLET_ROWS):
+        """(step_vals, rhs_vals, q) of the theta step: S = M' + theta dt A', R = M' - (1 - theta) dt A',
+        q = dt (c' + f') on the canonical CSR."""
+        if mode != _lib.COEF_CONST:
+            param = _device_tensor(param, torch.float64)
+        g = None if g is None else _device_tensor(g, torch.float64)
+        S = torch.empty(self.nnz, dtype=torch.float64, device=self.device)
+        R = torch.empty(self.nnz, dtype=torch.float64, device=self.device)
+        q = torch.empty(self.n, dtype=torch.float64, device=self.device)
+        _lib.check(self._lib.femk_assemble_theta(self._h, _lib.ptr(param), int(mode), float(scale), float(f),
+                                                 _lib.ptr(g), float(theta), float(dt), int(dirichlet), _lib.ptr(S),
+                                                 _lib.ptr(R), _lib.ptr(q), _lib.stream_handle()))
+        return S, R, q
+
+    def theta_march(self, step_vals, rhs_vals, q, u, nsteps, tol=1e-10, maxiter=20_000, traj=None):
+        """Advance u (in place) by nsteps theta steps. Returns (u, iterations i32[nsteps], worst step
+        residual); traj f64[nsteps, n] receives every state when given."""
+        it = np.zeros(max(int(nsteps), 1), dtype=np.int32)
+        worst = ctypes.c_double(0.0)
+        _lib.check(self._lib.femk_theta_march(
+            self._h, _lib.ptr(step_vals), _lib.ptr(rhs_vals), _lib.ptr(q), _lib.ptr(u), int(nsteps), float(tol),
+            int(maxiter), _lib.ptr(traj), ctypes.c_void_p(it.ctypes.data), ctypes.byref(worst),
+            _lib.stream_handle()))
+        return u, it[: int(nsteps)], worst.value

@@ -11,7 +11,11 @@ preconditioner (<r, z> without one) or at maxiter. After the solve the eager res
 
 Extensions with no reference counterpart: ``precision="mixed"`` (FP32 inner CG with FP64 reliable
 updates, ``refine="reliable"`` or classic restarted refinement ``refine="restart"``) and matrix-free
-operators (:class:`~jno_b200.sparse.MatrixFreeOperator`).
+operators (:class:`~jno_b200.sparse.MatrixFreeOperator`). FP32 CG converges more slowly than FP64
+as the condition number grows (rounding delays the Krylov convergence; on 2-D P1 512^2 Jacobi-PCG
+the FP32 inner loop needs 3.4x the FP64 iterations), so a mixed solve that has not met the stop
+rule after ``mixed_maxiter`` FP32 iterations (default ``maxiter``) continues in FP64 from its
+iterate, and ``last_info.fallback`` records it.
 """
 
 import math
@@ -39,24 +43,27 @@ class LinearOperator:
 
 
 class SolveInfo:
-    def __init__(self, iterations, relres, status, outer=None):
+    def __init__(self, iterations, relres, status, outer=None, fallback=0):
         self.iterations, self.relres, self.status, self.outer = iterations, relres, status, outer
+        self.fallback = fallback  # FP64 iterations run after a mixed solve missed the stop rule
 
     def __repr__(self):
-        return f"SolveInfo(iterations={self.iterations}, relres={self.relres:.3e}, outer={self.outer})"
+        return (f"SolveInfo(iterations={self.iterations}, relres={self.relres:.3e}, outer={self.outer}, "
+                f"fallback={self.fallback})")
 
 
 class LinearSolver:
-    def __init__(self, tol, atol, maxiter, precision="fp64", refine="reliable", name="cg"):
+    def __init__(self, tol, atol, maxiter, precision="fp64", refine="reliable", name="cg", mixed_maxiter=None):
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         if refine not in ("reliable", "restart"):
             raise ValueError("refine must be 'reliable' or 'restart'")
         self.tol, self.atol = float(tol), float(atol)
         self.maxiter = 20_000 if maxiter is None else int(maxiter)
+        self.mixed_maxiter = self.maxiter if mixed_maxiter is None else int(mixed_maxiter)
         self.precision, self.refine, self.name = precision, refine, name
         self.direct = False
-        self.key = (type(self), name, (self.tol, self.atol, self.maxiter, precision, refine))
+        self.key = (type(self), name, (self.tol, self.atol, self.maxiter, precision, refine, self.mixed_maxiter))
         self.last_info = None
 
     def __eq__(self, other):
@@ -81,8 +88,13 @@ class LinearSolver:
             if not isinstance(op, CsrMatrix) or inv is None:
                 raise ValueError("precision='mixed' needs an assembled CsrMatrix and M=jacobi()")
             mode = _lib.MIXED_RELIABLE if self.refine == "reliable" else _lib.MIXED_RESTART
-            x, inner, outer, rel, st = plan.pcg_mixed(op.solver_values, b, inv, x, self.tol, self.atol, self.maxiter, mode)
-            self.last_info = SolveInfo(inner, rel, st, outer)
+            x, inner, outer, rel, st = plan.pcg_mixed(op.solver_values, b, inv, x, self.tol, self.atol,
+                                                      self.mixed_maxiter, mode)
+            fb = 0
+            if st == _lib.FEMK_NOT_CONVERGED:
+                # FP32 rounding stalled the inner loop: finish in FP64 from the mixed iterate
+                x, fb, rel, st = plan.pcg(op.solver_values, b, x, inv, self.tol, self.atol, self.maxiter)
+            self.last_info = SolveInfo(inner, rel, st, outer, fb)
         elif self.name == "bicgstab":
             if not isinstance(op, CsrMatrix):
                 raise TypeError("the B200 BiCGStab takes an assembled CsrMatrix")
@@ -104,9 +116,9 @@ class LinearSolver:
         return x
 
 
-def cg(*, tol=1e-8, atol=0.0, maxiter=20_000, precision="fp64", refine="reliable"):
+def cg(*, tol=1e-8, atol=0.0, maxiter=20_000, precision="fp64", refine="reliable", mixed_maxiter=None):
     """Jacobi-preconditionable CG on the B200 kernels (``jax.scipy.sparse.linalg.cg`` semantics)."""
-    return LinearSolver(tol, atol, maxiter, precision, refine)
+    return LinearSolver(tol, atol, maxiter, precision, refine, mixed_maxiter=mixed_maxiter)
 
 
 def bicgstab(*, tol=1e-8, atol=0.0, maxiter=20_000):
@@ -114,3 +126,19 @@ def bicgstab(*, tol=1e-8, atol=0.0, maxiter=20_000):
     jno/solve.py:209-213); with ``M=jno.precond.jacobi()`` it is the steady ``fem.solve()`` default
     (jno/_fem.py:110-116)."""
     return LinearSolver(tol, atol, maxiter, name="bicgstab")
+
+
+class ThetaScheme:
+    """``jno.solve.theta(theta)`` (jno/solve.py:1160-1170): the theta-method time scheme of a
+    transient ``fem.solve(time=...)`` -- 1 backward Euler (the default), 1/2 Crank-Nicolson."""
+
+    def __init__(self, theta=1.0):
+        theta = float(theta)
+        if not 0.0 < theta <= 1.0:
+            raise NotImplementedError("theta must be in (0, 1] on the B200 path (theta = 0 leaves the Dirichlet rows empty)")
+        self.theta = theta
+
+
+def theta(theta=1.0):
+    return ThetaScheme(theta)
+

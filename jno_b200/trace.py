@@ -4,10 +4,13 @@ It mirrors the reference's DSL surface for this path only (``d.fem_symbols``, ``
 ``jno.np.exp``, ``jno.np.parameter``, ``u(xb, yb, zb) - g``; jno/trace/__init__.py,
 jno/architectures/models.py:58-142) and classifies a form into the kernel arguments:
 
-    coef * (ui.x*vi.x + ui.y*vi.y + ui.z*vi.z) - f * vi,   coef in {c, c*p, c*exp(p)}
+    [rho * ui.t * vi +] coef * (ui.x*vi.x + ui.y*vi.y [+ ui.z*vi.z]) - f * vi,
+    coef in {c, c*p, c*exp(p)},  rho, c, f constants
 
 with p a P0 parameter (one value per element) or, in P1 forms, a nodal P1 parameter (one value per
-vertex). Anything else raises ``NotImplementedError``: other physics is outside this path.
+vertex). The optional ``ui.t * vi`` mass term makes the form the linear first-order transient block
+``M u' + A u = c`` (jno/utils/solver/fem_native.py:2846-3110), with ``u(initial) - u0`` giving its
+initial state. Anything else raises ``NotImplementedError``: other physics is outside this path.
 """
 
 import numbers
@@ -74,7 +77,19 @@ class Exp(Expr):
         self.a = a
 
 
+class Sin(Expr):
+    def __init__(self, a):
+        self.a = a
+
+
+class Cos(Expr):
+    def __init__(self, a):
+        self.a = a
+
+
 class Coordinate(Expr):
+    """A coordinate of a region: axis 0..dim-1, or "t" (the time variable of a transient domain)."""
+
     def __init__(self, region, axis):
         self.region, self.axis = region, axis
 
@@ -90,6 +105,8 @@ class FieldSymbol(Expr):
 
     def __call__(self, *coords):
         regions = {getattr(c, "region", None) for c in coords}
+        if regions == {"initial"}:
+            return TraceOn(self, "initial")
         if regions != {"boundary"}:
             raise NotImplementedError("Dirichlet conditions are supported on the whole 'boundary' only")
         return TraceOn(self, "boundary")
@@ -110,6 +127,10 @@ class Bound(Expr):
     @property
     def z(self):
         return Deriv(self.sym, 2)
+
+    @property
+    def t(self):
+        return Deriv(self.sym, "t")
 
 
 class Deriv(Expr):
@@ -148,6 +169,18 @@ def exp(a):
     return Exp(a)
 
 
+def sin(a):
+    """``jno.np.sin``: in initial and Dirichlet value expressions."""
+    a = _wrap(a)
+    return Const(float(np.sin(a.v))) if isinstance(a, Const) else Sin(a)
+
+
+def cos(a):
+    """``jno.np.cos``: in initial and Dirichlet value expressions."""
+    a = _wrap(a)
+    return Const(float(np.cos(a.v))) if isinstance(a, Const) else Cos(a)
+
+
 # ------------------------------------------------------------------------------ classification
 def _monomials(e):
     """Expand into a list of (scalar, [factors])."""
@@ -181,21 +214,31 @@ def _coef_key(factors):
 
 
 class WeakForm:
-    """Classified volume form: k_e = scale * g(param_e), source f, field order."""
+    """Classified volume form: k_e = scale * g(param_e), source f, field order; ``mass`` is the
+    constant coefficient of the ``ui.t * vi`` term of a transient form (None when steady)."""
 
-    def __init__(self, order, mode, scale, param, f, domain):
+    def __init__(self, order, mode, scale, param, f, domain, mass=None):
         self.order, self.mode, self.scale, self.param, self.f, self.domain = order, mode, scale, param, f, domain
+        self.mass = mass
 
 
 def classify_volume(expr):
     stiff = {}  # axis -> (scale, key)
     source = 0.0
+    mass = None
     order = None
     domain = None
     for c, factors in _monomials(expr):
         ders = [f for f in factors if isinstance(f, Deriv)]
         vals = [f for f in factors if isinstance(f, Bound)]
         rest = [f for f in factors if not isinstance(f, (Deriv, Bound))]
+        if len(ders) == 1 and ders[0].axis == "t":
+            if (len(vals) != 1 or rest or ders[0].sym.role != "trial" or vals[0].sym.role != "test"):
+                raise NotImplementedError("the transient term must read rho * ui.t * vi with a constant rho")
+            mass = (mass or 0.0) + c
+            continue
+        if any(d.axis == "t" for d in ders):
+            raise NotImplementedError("only the first-order ui.t * vi term is on the B200 path")
         if len(ders) == 2 and not vals:
             roles = {d.sym.role for d in ders}
             if roles != {"trial", "test"} or ders[0].axis != ders[1].axis:
@@ -229,7 +272,9 @@ def classify_volume(expr):
             "nodal_linear": _lib.COEF_NODAL_LINEAR, "nodal_exp": _lib.COEF_NODAL_EXP}[key[0]]
     if key[0].startswith("nodal") and order != 1:
         raise NotImplementedError("a nodal P1 parameter in a P2 form is outside the B200 path")
-    return WeakForm(order, mode, scale, key[1] if len(key) > 1 else None, source, domain)
+    if mass is not None and not mass > 0.0:
+        raise NotImplementedError("the ui.t * vi coefficient must be a positive constant")
+    return WeakForm(order, mode, scale, key[1] if len(key) > 1 else None, source, domain, mass)
 
 
 def evaluate_on(expr, pts):
@@ -237,6 +282,8 @@ def evaluate_on(expr, pts):
     if isinstance(expr, Const):
         return np.full(pts.shape[0], expr.v)
     if isinstance(expr, Coordinate):
+        if expr.axis == "t":
+            raise NotImplementedError("time-dependent boundary or initial values are outside the B200 path")
         return pts[:, expr.axis].copy()
     if isinstance(expr, Add):
         return evaluate_on(expr.a, pts) + evaluate_on(expr.b, pts)
@@ -244,14 +291,34 @@ def evaluate_on(expr, pts):
         return evaluate_on(expr.a, pts) * evaluate_on(expr.b, pts)
     if isinstance(expr, Exp):
         return np.exp(evaluate_on(expr.a, pts))
-    raise NotImplementedError("Dirichlet values may use constants and boundary coordinates only")
+    if isinstance(expr, Sin):
+        return np.sin(evaluate_on(expr.a, pts))
+    if isinstance(expr, Cos):
+        return np.cos(evaluate_on(expr.a, pts))
+    raise NotImplementedError("boundary and initial values may use constants, coordinates, exp, sin and cos only")
 
 
-def classify_dirichlet(expr):
+def classify_condition(expr):
+    """``u(boundary) - g`` or ``u(initial) - u0`` -> (region, symbol, value expression)."""
+    sym, g = classify_dirichlet(expr, regions=("boundary", "initial"))
+    return _condition_region(expr), sym, g
+
+
+def _condition_region(expr):
+    for _c, factors in _monomials(expr):
+        for f in factors:
+            if isinstance(f, TraceOn):
+                return f.region
+    return None
+
+
+def classify_dirichlet(expr, regions=("boundary",)):
     """``u(boundary) - g`` -> (symbol, g expression)."""
     traces, rest = [], []
     for c, factors in _monomials(expr):
         tr = [f for f in factors if isinstance(f, TraceOn)]
+        if any(t.region not in regions for t in tr):
+            raise NotImplementedError(f"a condition on {tr[0].region!r} is outside the B200 path")
         if tr:
             if len(tr) != 1 or len(factors) != 1 or c != 1.0:
                 raise NotImplementedError("Dirichlet terms must read u(boundary) - g")

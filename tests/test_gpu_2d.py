@@ -349,3 +349,26 @@ def test_tri_status_paths():
     plan = _plan(p1, tris, 2)
     with pytest.raises(_lib.FemkError):
         plan.assemble(torch.zeros(plan.nvert, dtype=torch.float64, device="cuda"), mode=_lib.COEF_NODAL_EXP)
+
+
+def test_tri_mixed_falls_back_to_fp64_when_fp32_stalls():
+    """jno.solve.cg(precision="mixed") finishes in FP64 from the mixed iterate when the FP32 inner
+    loop has not met the stop rule within mixed_maxiter; the result is the FP64 solution."""
+    import jno_b200 as jno
+    from jno_b200.sparse import CsrMatrix
+
+    pf, cf, tris, p1 = _mesh(64, 1)
+    logk = om.logk_field(len(tris), 1000)
+    plan = _plan(p1, tris, 1)
+    vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
+    A = CsrMatrix(plan, vals)
+    solver = jno.solve.cg(tol=1e-8, precision="mixed", mixed_maxiter=40)
+    x = solver(A, b, M=jno.precond.jacobi())
+    info = solver.last_info
+    assert info.fallback > 0 and info.status == 0 and info.relres <= 2e-8
+    x64 = jno.solve.cg(tol=1e-8)(A, b, M=jno.precond.jacobi())
+    assert (torch.linalg.norm(x - x64) / torch.linalg.norm(x64)).item() <= 1e-6
+    # no fallback when the FP32 loop converges within its budget
+    solver2 = jno.solve.cg(tol=1e-8, precision="mixed")
+    solver2(A, b, M=jno.precond.jacobi())
+    assert solver2.last_info.fallback == 0
