@@ -135,11 +135,12 @@ def test_tri_pcg_matches_oracle(n, order):
     assert np.linalg.norm(um.cpu().numpy() - xo) <= 1e-6 * np.linalg.norm(xo)
     # BiCGStab (the steady default) against the oracle's jax restatement. Its iteration count moves
     # with the summation order: a symmetric permutation of the oracle's own system (same math, other
-    # order) moves it by up to 17 % at P1 128^2 (303 -> 354); the contract is the stop rule and the
+    # order) moves it from 303 to 354 at P1 128^2, and the device's grid-shaped reductions have given
+    # 272-316 there (363 for the oracle's natural order); the contract is the stop rule and the
     # solution
     ub, itb, relb, stb = plan.bicgstab(vals, b, inv_diag=inv, tol=1e-8)
     xb, kb = op.bicgstab(A, s.b, io, tol=1e-8)
-    assert stb == 0 and relb <= 2e-8 and abs(itb - kb) <= max(2, kb // 4), (itb, kb)
+    assert stb == 0 and relb <= 2e-8 and abs(itb - kb) <= max(2, (2 * kb) // 5), (itb, kb)
     assert np.linalg.norm(ub.cpu().numpy() - xb) <= 1e-7 * np.linalg.norm(xb)
 
 
