@@ -43,7 +43,73 @@ def parse_args():
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--solver", choices=["fp64", "mixed", "matfree"], default="fp64",
                     help="solver of the timed step (fp64 is the headline; the others serve profiling runs)")
+    ap.add_argument("--path", choices=["tri", "theta"], default=None,
+                    help="time a secondary workload instead of the headline (kernel profiling): 'tri' = 2-D P1 "
+                         "triangles, n^2 rectangles (--n, default 1024), FP64 assemble + PCG; 'theta' = the P1 "
+                         "n^3 transient march (--n, default 128), step-operator assembly + 10 backward-Euler steps")
     return ap.parse_args()
+
+
+def run_path(args):
+    """One secondary workload, K timed steps after W warm-up on cuda:0 (CUDA events, inputs resident);
+    prints one JSON line. Serves the ncu launch lists of the 2-D and transient paths."""
+    import torch
+
+    from jno_b200 import _lib
+    from jno_b200.domain import jitter_interior_2d, rect_points_tris
+    from jno_b200.plan import FemPlan
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    info = {}
+    if args.path == "tri":
+        n = 1024 if args.n == 128 else args.n
+        pts, tris = rect_points_tris(n, n)
+        plan = FemPlan(jitter_interior_2d(pts, n, n, seed=0)[:, :2], tris, 1)
+        fields = [torch.as_tensor(f, device=dev) for f in logk_fields(plan.ntet, 3)]
+        vals = torch.empty(plan.nnz, dtype=torch.float64, device=dev)
+        b = torch.empty(plan.n, dtype=torch.float64, device=dev)
+        inv = torch.empty(plan.n, dtype=torch.float64, device=dev)
+        x = torch.empty(plan.n, dtype=torch.float64, device=dev)
+
+        def step(i):
+            plan.assemble(fields[i % 3], vals=vals, b=b)
+            plan.jacobi(vals, out=inv)
+            x.zero_()
+            info.setdefault("iters", []).append(plan.pcg(vals, b, x, inv, tol=1e-8)[1])
+
+        workload = f"P1 {n}^2 triangles ({plan.ntet:,} triangles, {plan.n:,} DOF), FP64 assemble + Jacobi-PCG to 1e-8"
+        metric, units = "DOF/s", plan.n
+    else:
+        n = args.n
+        pts, tets = make_mesh(n)
+        plan = FemPlan(pts, tets, 1)
+        fields = [torch.as_tensor(f, device=dev) for f in logk_fields(plan.ntet, 3)]
+        p = plan.export()["points"]
+        u0 = torch.sin(np.pi * p[:, 0]) * torch.sin(np.pi * p[:, 1]) * torch.sin(np.pi * p[:, 2])
+        u = torch.empty_like(u0)
+
+        def step(i):
+            S, R, q = plan.assemble_theta(fields[i % 3], f=1.0, theta=1.0, dt=1e-3, dirichlet=_lib.DIRICHLET_ROWS)
+            u.copy_(u0)
+            it = plan.theta_march(S, R, q, u, 10)[1]
+            info.setdefault("iters", []).append(float(np.mean(it)))
+
+        workload = f"P1 {n}^3 transient heat, backward Euler, dt=1e-3, 10 steps per march ({plan.n:,} DOF)"
+        metric, units = "DOF-steps/s", plan.n * 10
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        step(args.warmup + i)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    print(json.dumps({"path": args.path, "metric": metric, "value": units / (ms / 1e3), "ms_per_step": ms,
+                      "steps": args.steps, "warmup": args.warmup, "config": {"workload": workload},
+                      "iters": float(np.mean(info["iters"])), "gpu_launches_total": int(_lib.load().femk_kernel_launches())}))
 
 
 def workload_desc(n, order, T, ndof, nnz):
@@ -774,6 +840,8 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.path:
+        run_path(args)
     else:
         run_ours(args)
 

@@ -1,5 +1,5 @@
 /*
- * femk.h -- C ABI of the B200 (sm_100a) P1/P2 tetrahedral FEM assembly + Jacobi-PCG kernels.
+ * femk.h -- C ABI of the B200 (sm_100a) P1/P2 tetrahedral (and triangular) FEM assembly + Jacobi-PCG kernels.
  *
  * This is the drop-in boundary for jNO's hot path: parametric element assembly of
  * -div(k grad u) = f on Lagrange P1/P2 tetrahedra into the compress-plan CSR pattern, the Jacobi
