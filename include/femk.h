@@ -252,7 +252,8 @@ int femk_assemble_theta(const femk_plan* plan, const double* param_dev, int coef
  * here: the march stops with FEMK_NOT_CONVERGED). u_dev f64[n] holds the state (in/out);
  * traj_dev f64[nsteps*n] or NULL receives the state after every step; iters_out i32[nsteps] (host)
  * or NULL; *relres_out (host, may be NULL) = the largest step residual. The step operator is
- * gathered into the solver layout once per call.
+ * gathered into the plan's solver layout once per call: it replaces the operator a previous
+ * femk_prepare_operator left there (femk_spmv_prepared then applies S until the next prepare).
  */
 int femk_theta_march(const femk_plan* plan, const double* step_vals_dev, const double* rhs_vals_dev,
                      const double* q_dev, double* u_dev, int32_t nsteps, double tol, int32_t maxiter,

@@ -123,6 +123,10 @@ class FEM:
 
     @property
     def operator(self):
+        if self.is_transient:
+            raise NotImplementedError(
+                "a transient form has no single (A, b): use fem.solve() for the trajectory or "
+                "fem.step_operators(args, theta) for the theta-step operators")
         if self.form.param is not None:
             return FemLinearSystem(self)
         if self._eager is None:

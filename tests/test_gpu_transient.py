@@ -165,6 +165,10 @@ def test_jno_surface_heat_theta_override():
     assert np.abs(tp - top).max() <= 1e-8 * np.abs(top).max()
     with pytest.raises(ValueError):
         fem.solve(x0=torch.zeros(fem.dofs, dtype=torch.float64, device="cuda"))
+    with pytest.raises(NotImplementedError):
+        fem.operator  # noqa: B018 -- a transient form has no single (A, b)
+    S, R, q = fem.step_operators(theta=0.5)
+    assert S.numel() == fem.plan.nnz and q.numel() == fem.dofs
 
 
 def test_jno_surface_march_reaches_steady_state():
