@@ -455,13 +455,29 @@ def batched_variant(dev, count=256, reps=3):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
+    x64 = x.clone()
+    # the same batch in mixed precision (FP32 inner CG, per-problem FP64 reliable updates)
+    e0.record()
+    for _ in range(reps):
+        batch.plan.assemble(logk, vals=vals, b=b)
+        batch.plan.jacobi(vals, out=inv)
+        xm, itm, outm, relm, stvm, stm = batch.plan.pcg_batched_mixed(
+            batch.row_off, vals, b, inv, None, 1e-8, 0.0, 20_000, sched["tile_rows"], sched["blocks_per_sm"])
+    e1.record()
+    torch.cuda.synchronize()
+    ms_m = e0.elapsed_time(e1) / reps
+    err = max(float(torch.linalg.norm(xm[r0:r1] - x64[r0:r1]) / max(torch.linalg.norm(x64[r0:r1]).item(), 1e-300))
+              for r0, r1 in zip(batch.row_off[:-1], batch.row_off[1:]) if r1 > r0)
     return {"workload": f"{count} P1 problems, sides {int(sides.min())}..{int(sides.max())} hexes "
                         f"({batch.plan.ntet:,} tets, {batch.plan.n:,} DOF in total)",
             "value": batch.plan.n / (ms / 1e3), "unit": "DOF/s", "ms_per_batch": ms,
             "iters_min": int(it.min()), "iters_max": int(it.max()), "max_relres": float(rel.max()),
             "status_ok": bool(st == 0), "schedule": {k: sched[k] for k in ("tile_rows", "blocks_per_sm")},
-            "one_graph_launch": bool(getattr(batch.plan, "batch_graph", False)),
-            "precision": "fp64 (the mixed batched form is not built)"}
+            "one_graph_launch": bool(getattr(batch.plan, "batch_graph", False)), "precision": "fp64",
+            "mixed": {"value": batch.plan.n / (ms_m / 1e3), "unit": "DOF/s", "ms_per_batch": ms_m,
+                      "speedup_vs_fp64": ms / ms_m, "inner_iters_max": int(itm.max()),
+                      "fp64_updates_max": int(outm.max()), "max_relres": float(relm.max()),
+                      "status_ok": bool(stm == 0), "max_err_vs_fp64_batched": err}}
 
 
 def adjoint_variant(dev, n=64, n_fd=32):
@@ -728,6 +744,30 @@ def run_ours(args):
             "speedup_vs_fp64": ms_step / ms, "inner_iters": float(np.mean(mixed_info["inner"])),
             "fp64_updates": float(np.mean(mixed_info["outer"])), "max_relres": float(np.max(mixed_info["rel"])),
             "err_vs_fp64_tight": err}
+        # the mixed-precision config's 1e-10 refinement target, against FP64 CG at the same tolerance
+        m10 = {}
+
+        def m10step(i, mixed):
+            lk = fields[i % N_FIELDS]
+            plan.assemble(lk, vals=vals, b=b)
+            plan.jacobi(vals, out=inv)
+            x.zero_()
+            if mixed:
+                out = plan.pcg_mixed(vals, b, inv, x, tol=1e-10)
+                m10.setdefault("inner", []).append(out[1])
+                m10.setdefault("rel", []).append(out[3])
+            else:
+                m10.setdefault("it64", []).append(plan.pcg(vals, b, x, inv, tol=1e-10)[1])
+
+        k10 = min(args.steps, 5)
+        ms10_64 = timed(lambda i: m10step(i, False), k10, 1) / k10
+        ms10_m = timed(lambda i: m10step(i, True), k10, 1) / k10
+        m10step(N_FIELDS * 10, True)
+        variants["mixed_1e-10_vs_fp64_1e-10"] = {
+            "value": world * ndof / (ms10_m / 1e3), "unit": "DOF/s", "ms_per_step": ms10_m, "fp64_ms_per_step": ms10_64,
+            "speedup_vs_fp64": ms10_64 / ms10_m, "inner_iters": float(np.mean(m10["inner"])),
+            "fp64_iters": float(np.mean(m10["it64"])), "max_relres": float(np.max(m10["rel"])),
+            "err_vs_fp64_tight": torch.linalg.norm(x - x_ref).item() / ref_norm}
         # matrix-free FP64
         mf_info = {}
 

@@ -303,6 +303,21 @@ int femk_pcg_batched(const femk_plan* plan, int32_t nprob, const int64_t* row_of
                      double* relres_out_host, int32_t* status_out_host, void* stream);
 
 /*
+ * femk_pcg_batched in mixed precision: FP32 values (converted from vals_dev in the same graph)
+ * and FP32 inner vectors with FP32 SpMV accumulation, x in FP64, and per-problem FP64 reliable
+ * updates (r = fp32(b - A x) with the FP64 values once the FP32 <r, r> fell by 1e-4 since the last
+ * update, met the stop test or hit the cap; the direction is kept), as femk_pcg_mixed does for one
+ * problem. Problem k retires when its FP64 <r, r> <= max(tol^2 <b, b>, atol^2) or at maxiter FP32
+ * iterations. iters_out_host = FP32 iterations, outer_out_host = FP64 residual evaluations (may be
+ * NULL); the other arguments as femk_pcg_batched (inv_diag_dev may be NULL: no preconditioner).
+ * No reference counterpart.
+ */
+int femk_pcg_batched_mixed(const femk_plan* plan, int32_t nprob, const int64_t* row_off_host, const double* vals_dev,
+                           const double* b_dev, double* x_dev, const double* inv_diag_dev, double tol, double atol,
+                           int32_t maxiter, int32_t tile_rows, int32_t blocks_per_sm, int32_t* iters_out_host,
+                           int32_t* outer_out_host, double* relres_out_host, int32_t* status_out_host, void* stream);
+
+/*
  * Adjoint contraction: grad[c] = -k_c * (m o lam)_e^T K_hat_e (m o u)_e, m = 1 - dirichlet mask,
  * k_c = coef_scale * exp(param_c) (FEMK_COEF_EXP) or coef_scale (FEMK_COEF_LINEAR: d/dparam).
  * Nodal P1 modes: grad f64[nvert], grad[i] = sum over elements e holding vertex i of

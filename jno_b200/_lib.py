@@ -97,6 +97,7 @@ SIGNATURES = {
     "femk_pcg_mixed": [_P, _P, _P, _P, _P, _D, _D, _I32, _I, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
                        ctypes.POINTER(_D), _P],
     "femk_pcg_batched": [_P, _I32, _P, _P, _P, _P, _P, _D, _D, _I32, _I32, _I32, _P, _P, _P, _P],
+    "femk_pcg_batched_mixed": [_P, _I32, _P, _P, _P, _P, _P, _D, _D, _I32, _I32, _I32, _P, _P, _P, _P, _P],
     "femk_adjoint_grad": [_P, _P, _I, _D, _P, _P, _P, _P],
     "femk_lumped_mass": [_P, _P, _P],
     "femk_mass_matrix": [_P, _I, _P, _P],

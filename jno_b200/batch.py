@@ -51,14 +51,25 @@ class BatchedPoisson:
             logk = np.concatenate([np.asarray(v, dtype=np.float64) for v in logk])
         return self.plan.assemble(logk, mode=_lib.COEF_EXP)
 
-    def solve(self, vals, b, tol=1e-8, maxiter=20_000, schedule=None):
-        """All problems to the 1e-8 stop rule in one launch. Returns (x, iterations, relres)."""
+    def solve(self, vals, b, tol=1e-8, maxiter=20_000, schedule=None, precision="fp64"):
+        """All problems to the stop rule in one launch. Returns (x, iterations, relres).
+
+        ``precision="mixed"``: FP32 inner CG with per-problem FP64 reliable updates
+        (``femk_pcg_batched_mixed``); the iterations are then the FP32 ones and ``self.last_outer``
+        holds each problem's FP64 residual evaluations."""
         from .tuner import batched_schedule
 
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
         inv = self.plan.jacobi(vals)
         sched = schedule or batched_schedule(self, vals, b, inv, tol)
-        x, it, rel, stv, st = self.plan.pcg_batched(self.row_off, vals, b, None, inv, tol, 0.0, maxiter,
-                                                    sched["tile_rows"], sched["blocks_per_sm"])
+        if precision == "mixed":
+            x, it, outer, rel, stv, st = self.plan.pcg_batched_mixed(
+                self.row_off, vals, b, inv, None, tol, 0.0, maxiter, sched["tile_rows"], sched["blocks_per_sm"])
+            self.last_outer = outer
+        else:
+            x, it, rel, stv, st = self.plan.pcg_batched(self.row_off, vals, b, None, inv, tol, 0.0, maxiter,
+                                                        sched["tile_rows"], sched["blocks_per_sm"])
         if st != 0:
             raise RuntimeError(f"batched CG: status {st}, per-problem status {np.unique(stv)}")
         return x, it, rel

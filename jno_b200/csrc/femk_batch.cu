@@ -16,8 +16,17 @@
 // largest problems keep every SM busy after the small ones have converged) without each tile
 // re-reducing its problem. Barriers are the bounded-spin grid barriers of femk_grid.cuh. No reference counterpart (jNO batches only by vmap over
 // right-hand sides, tests/test_fem_solver_slots.py:123-132).
+//
+// The mixed-precision form (k_batch_mixed) runs the same phases on FP32 values and vectors (FP32
+// SpMV accumulation, dot products summed in FP64) with x kept in FP64, and gives every problem
+// FP64 reliable updates, as femk_pcg_mixed does for one problem: when its FP32 <r, r> fell by
+// delta2 since the last update, met the stop test or hit the cap, an update phase replaces r by
+// fp32(b - A x) with the FP64 values, keeps the direction, and retires the problem once the FP64
+// residual meets the stop rule. The update phase (two more grid barriers) runs only in the
+// iterations where some problem asked for one.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "femk_grid.cuh"
@@ -34,6 +43,14 @@ struct BatchArgs {
   const int32_t* indptr;
   const int32_t* indices;
   const double* vals;
+  // mixed precision: FP32 values and inner vectors, per-problem update bookkeeping
+  const float* vals32;
+  float *r32, *z32, *p32, *q32, *d32;
+  double* rr_since;  // [nprob] FP64 <r, r> at the last reliable update
+  int32_t* upd;      // [nprob] 1 while a reliable update is pending
+  int32_t* outer;    // [nprob] FP64 residual evaluations
+  int32_t* any_upd;  // [1] some problem requested an update this iteration
+  double delta2;
   const int32_t* tile_r0;
   const int32_t* tile_r1;
   const int32_t* tile_prob;
@@ -58,16 +75,22 @@ struct BatchArgs {
 };
 
 // One warp computes (A v)[row] for the rows of its tile; the epilogue functor sees (row, Av).
-template <typename F>
-__device__ __forceinline__ void tile_spmv(const BatchArgs& a, int32_t r0, int32_t r1, const double* __restrict__ v,
+// V = double: the FP64 values a.vals; V = float: the FP32 values a.vals32 (FP32 accumulation).
+template <typename V = double, typename F>
+__device__ __forceinline__ void tile_spmv(const BatchArgs& a, int32_t r0, int32_t r1, const V* __restrict__ v,
                                           F&& epi) {
   const int lane = threadIdx.x & 31;
   const int sub = lane % kL;
   constexpr int RPW = 32 / kL;
+  const V* vals;
+  if constexpr (sizeof(V) == 8)
+    vals = a.vals;
+  else
+    vals = a.vals32;
   for (int64_t base = r0; base < r1; base += RPW * kU) {
-    double sv[kU];
+    V sv[kU];
     int64_t rows[kU];
-    csr_rows_g<kL, kU, double, int32_t>(a.indptr, a.indices, a.vals, GatherXcg<double>{v}, r1, base, lane, sv, rows);
+    csr_rows_g<kL, kU, V, int32_t>(a.indptr, a.indices, vals, GatherXcg<V>{v}, r1, base, lane, sv, rows);
 #pragma unroll
     for (int u = 0; u < kU; ++u)
       if (rows[u] < r1 && sub == 0) epi(rows[u], sv[u]);
@@ -257,6 +280,195 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
   }
 }
 
+__global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
+  unsigned int gen = 0;
+  const int32_t gw = (int32_t)((blockIdx.x * (int64_t)kBT + threadIdx.x) >> 5);  // global warp
+  const int32_t NW = (int32_t)(((int64_t)gridDim.x * kBT) >> 5);
+  const int lane = threadIdx.x & 31;
+  // ---- phase 0: FP64 residual of x0, FP32 copies; <r, z> (FP32 data), <r64, r64>, <b, b>
+  for (int32_t t = gw; t < a.ntiles; t += NW) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    tile_spmv<double>(a, a.tile_r0[t], a.tile_r1[t], a.x, [&](int64_t row, double s) {
+      const double bi = a.b[row];
+      const double r64 = bi - s;
+      const float d = a.dinv ? (float)a.dinv[row] : 1.0f;
+      const float rf = (float)r64;
+      const float zf = d * rf;
+      a.d32[row] = d;
+      a.r32[row] = rf;
+      a.z32[row] = zf;
+      a.p32[row] = zf;
+      acc[0] += (double)rf * (double)zf;
+      acc[1] += r64 * r64;
+      acc[2] += bi * bi;
+    });
+    tile_partial<3>(acc, a.P, a.ntiles, t, 0);
+  }
+  if (!grid_sync(a.bar, gen)) return;
+  FEMK_OWNER_LOOP {
+    const double rz = prob_sum(a, 0, k), rr = prob_sum(a, 1, k), bb = prob_sum(a, 2, k);
+    if (threadIdx.x == 0) {
+      const double at2 = fmax(a.tol2 * bb, a.atol2_abs);
+      a.gam[k] = rz;
+      a.rr[k] = rr;
+      a.rr_since[k] = rr;
+      a.atol2[k] = at2;
+      a.iter[k] = 0;
+      a.outer[k] = 1;
+      a.upd[k] = 0;
+      if (!isfinite(rz) || !isfinite(rr))
+        retire(a, k, FEMK_NONFINITE);
+      else if (!(rr > at2) || a.maxiter <= 0)
+        retire(a, k, FEMK_OK);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *a.any_upd = 0;
+  if (!grid_sync(a.bar, gen)) return;
+  double* alpha = a.gam + a.nprob;
+  double* beta = alpha;
+  while (ld_acquire_u32((const unsigned int*)a.active) != 0u) {
+    // ---- phase 1: q = A32 p (FP32), <p, q>
+    for (int32_t t = gw; t < a.ntiles; t += NW) {
+      const int32_t k = a.tile_prob[t];
+      if (warp_done(a.done, k)) continue;
+      double acc[1] = {0.0};
+      tile_spmv<float>(a, a.tile_r0[t], a.tile_r1[t], a.p32, [&](int64_t row, float s) {
+        a.q32[row] = s;
+        acc[0] += (double)__ldcg(a.p32 + row) * (double)s;
+      });
+      tile_partial<1>(acc, a.P, a.ntiles, t, 3);
+    }
+    if (!grid_sync(a.bar, gen)) return;
+    FEMK_OWNER_LOOP {
+      if (block_done(a.done, k)) continue;
+      const double pq = prob_sum(a, 3, k);
+      if (threadIdx.x == 0) {
+        if (!(pq > 0.0) || !isfinite(pq))
+          retire(a, k, isfinite(pq) ? FEMK_BREAKDOWN : FEMK_NONFINITE);
+        else
+          alpha[k] = a.gam[k] / pq;
+      }
+    }
+    if (!grid_sync(a.bar, gen)) return;
+    // ---- phase 2: x += alpha p (FP64), r -= alpha q, z = D^-1 r (FP32); <r, z>, <r, r>
+    for (int32_t t = gw; t < a.ntiles; t += NW) {
+      const int32_t k = a.tile_prob[t];
+      if (warp_done(a.done, k)) continue;
+      const double al = __ldcg(alpha + k);
+      const float alf = (float)al;
+      double acc[2] = {0.0, 0.0};
+      for (int32_t i = a.tile_r0[t] + lane; i < a.tile_r1[t]; i += 32) {
+        const float pi = __ldcg(a.p32 + i);
+        a.x[i] = a.x[i] + al * (double)pi;
+        const float ri = fmaf(-alf, __ldcg(a.q32 + i), __ldcg(a.r32 + i));
+        const float zi = a.d32[i] * ri;
+        a.r32[i] = ri;
+        a.z32[i] = zi;
+        acc[0] += (double)ri * (double)zi;
+        acc[1] += (double)ri * (double)ri;
+      }
+      tile_partial<2>(acc, a.P, a.ntiles, t, 4);
+    }
+    if (!grid_sync(a.bar, gen)) return;
+    FEMK_OWNER_LOOP {
+      if (block_done(a.done, k)) continue;
+      const double rz = prob_sum(a, 4, k), rr = prob_sum(a, 5, k);
+      if (threadIdx.x == 0) {
+        const int32_t itk = a.iter[k] + 1;
+        a.iter[k] = itk;
+        if (!isfinite(rz) || !isfinite(rr)) {
+          retire(a, k, FEMK_NONFINITE);
+        } else if (!(rr > a.atol2[k]) || rr < a.delta2 * a.rr_since[k] || itk >= a.maxiter) {
+          a.upd[k] = 1;  // FP64 residual replacement before the next direction
+          atomicExch(a.any_upd, 1);
+        } else {
+          beta[k] = rz / a.gam[k];
+          a.gam[k] = rz;
+          a.rr[k] = rr;
+        }
+      }
+    }
+    if (!grid_sync(a.bar, gen)) return;
+    if (__ldcg(a.any_upd)) {
+      // ---- phase U: r = fp32(b - A64 x), z = D^-1 r for the problems that asked; <r, z>, <r64, r64>
+      for (int32_t t = gw; t < a.ntiles; t += NW) {
+        const int32_t k = a.tile_prob[t];
+        if (warp_done(a.done, k)) continue;
+        int u = lane == 0 ? __ldcg(a.upd + k) : 0;
+        if (!__shfl_sync(0xffffffffu, u, 0)) continue;
+        double acc[2] = {0.0, 0.0};
+        tile_spmv<double>(a, a.tile_r0[t], a.tile_r1[t], a.x, [&](int64_t row, double s) {
+          const double r64 = a.b[row] - s;
+          const float rf = (float)r64;
+          const float zf = a.d32[row] * rf;
+          a.r32[row] = rf;
+          a.z32[row] = zf;
+          acc[0] += (double)rf * (double)zf;
+          acc[1] += r64 * r64;
+        });
+        tile_partial<2>(acc, a.P, a.ntiles, t, 4);
+      }
+      if (!grid_sync(a.bar, gen)) return;
+      FEMK_OWNER_LOOP {
+        if (block_done(a.done, k)) continue;
+        __shared__ int32_t uk;
+        if (threadIdx.x == 0) uk = __ldcg(a.upd + k);
+        __syncthreads();
+        const bool pending = uk != 0;
+        __syncthreads();
+        if (!pending) continue;
+        const double rz = prob_sum(a, 4, k), rr = prob_sum(a, 5, k);
+        if (threadIdx.x == 0) {
+          a.upd[k] = 0;
+          a.outer[k] += 1;
+          a.rr[k] = rr;
+          if (!isfinite(rz) || !isfinite(rr))
+            retire(a, k, FEMK_NONFINITE);
+          else if (!(rr > a.atol2[k]) || a.iter[k] >= a.maxiter)
+            retire(a, k, FEMK_OK);
+          else {
+            beta[k] = rz / a.gam[k];  // residual replacement keeps the search direction
+            a.gam[k] = rz;
+            a.rr_since[k] = rr;
+          }
+        }
+      }
+      if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.any_upd, 0);
+      if (!grid_sync(a.bar, gen)) return;
+    }
+    // ---- phase 3: p = z + beta p
+    for (int32_t t = gw; t < a.ntiles; t += NW) {
+      const int32_t k = a.tile_prob[t];
+      if (warp_done(a.done, k)) continue;
+      const float be = (float)__ldcg(beta + k);
+      for (int32_t i = a.tile_r0[t] + lane; i < a.tile_r1[t]; i += 32)
+        a.p32[i] = fmaf(be, __ldcg(a.p32 + i), __ldcg(a.z32 + i));
+    }
+    if (!grid_sync(a.bar, gen)) return;
+  }
+  // ---- phase R: per-problem ||b - A x||, ||b|| (FP64)
+  for (int32_t t = gw; t < a.ntiles; t += NW) {
+    double acc[2] = {0.0, 0.0};
+    tile_spmv<double>(a, a.tile_r0[t], a.tile_r1[t], a.x, [&](int64_t row, double s) {
+      const double bi = a.b[row];
+      const double w = bi - s;
+      acc[0] += w * w;
+      acc[1] += bi * bi;
+    });
+    tile_partial<2>(acc, a.P, a.ntiles, t, 5);
+  }
+  if (!grid_sync(a.bar, gen)) return;
+  FEMK_OWNER_LOOP {
+    const double ww = prob_sum(a, 5, k), bb = prob_sum(a, 6, k);
+    if (threadIdx.x == 0) a.relres[k] = sqrt(ww) / (sqrt(bb) + 1e-30);
+  }
+}
+
+__global__ void k_to_f32(const double* __restrict__ in, int64_t n, float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
 __global__ void k_batch_reset(int32_t* done, int32_t* status, int32_t* active, int32_t nprob, GridBar* bar) {
   for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nprob; k += gridDim.x * blockDim.x) {
     done[k] = 0;
@@ -275,11 +487,12 @@ __global__ void k_batch_reset(int32_t* done, int32_t* status, int32_t* active, i
 
 using namespace femk;
 
-extern "C" int femk_pcg_batched(const femk_plan* pc, int32_t nprob, const int64_t* row_off, const double* vals,
-                                const double* b, double* x, const double* dinv, double tol, double atol,
-                                int32_t maxiter, int32_t tile_rows, int32_t blocks_per_sm, int32_t* iters_out,
-                                double* relres_out, int32_t* status_out, void* stream) {
-  clear_error();
+namespace {
+
+int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, const double* vals, const double* b,
+                 double* x, const double* dinv, double tol, double atol, int32_t maxiter, int32_t tile_rows,
+                 int32_t blocks_per_sm, int32_t* iters_out, int32_t* outer_out, double* relres_out,
+                 int32_t* status_out, void* stream, bool mixed, double delta2) {
   FEMK_CHECK_ARG(pc && row_off && vals && b && x, "femk_pcg_batched: NULL argument");
   FEMK_CHECK_ARG(nprob >= 1, "femk_pcg_batched: nprob must be >= 1");
   FEMK_CHECK_ARG(tile_rows >= 32 && tile_rows <= (1 << 20), "femk_pcg_batched: tile_rows out of range");
@@ -303,8 +516,8 @@ extern "C" int femk_pcg_batched(const femk_plan* pc, int32_t nprob, const int64_
   cudaStream_t s = (cudaStream_t)stream;
   FEMK_TRY(ensure_workspace(p));
   // batch workspace: ints (tiles + per-problem), doubles (partials + per-problem)
-  const int64_t nint = 3 * (int64_t)ntiles + 5 * (int64_t)nprob + 8;
-  const int64_t ndbl = 7 * (int64_t)ntiles + 6 * (int64_t)nprob + 8;
+  const int64_t nint = 3 * (int64_t)ntiles + 7 * (int64_t)nprob + 8;
+  const int64_t ndbl = 7 * (int64_t)ntiles + 7 * (int64_t)nprob + 8;
   const int64_t bytes = nint * 4 + 64 + ndbl * 8;
   if (p->batch_bytes < bytes) {
     if (p->batch_ws) cudaFree(p->batch_ws);
@@ -346,6 +559,23 @@ extern "C" int femk_pcg_batched(const femk_plan* pc, int32_t nprob, const int64_
   a.atol2 = a.gam + 2 * nprob;
   a.rr = a.atol2 + nprob;
   a.relres = a.rr + nprob;
+  a.rr_since = a.relres + nprob;
+  a.upd = a.active + 1;
+  a.outer = a.upd + nprob;
+  a.any_upd = a.outer + nprob;
+  a.delta2 = delta2;
+  a.vals32 = nullptr;
+  a.r32 = a.z32 = a.p32 = a.q32 = a.d32 = nullptr;
+  if (mixed) {
+    if (!p->vals32) FEMK_CUDA_TRY(cudaMalloc(&p->vals32, sizeof(float) * (p->nnz + 1)));
+    if (!p->work32) FEMK_CUDA_TRY(cudaMalloc(&p->work32, sizeof(float) * 6 * p->vstride));
+    a.vals32 = p->vals32;
+    a.r32 = p->work32;
+    a.z32 = a.r32 + vs;
+    a.p32 = a.z32 + vs;
+    a.q32 = a.p32 + vs;
+    a.d32 = a.q32 + vs;
+  }
   a.bar = (GridBar*)p->bar;
   // tile tables: uploaded only when the schedule changes (pageable copies stay outside the graph)
   uint64_t h = 1469598103934665603ull;
@@ -359,13 +589,16 @@ extern "C" int femk_pcg_batched(const femk_plan* pc, int32_t nprob, const int64_
     FEMK_CUDA_TRY(cudaMemcpyAsync(ib + 3 * ntiles, t0.data(), 4 * nprob, cudaMemcpyHostToDevice, s));
     FEMK_CUDA_TRY(cudaMemcpyAsync(ib + 3 * ntiles + nprob, t1.data(), 4 * nprob, cudaMemcpyHostToDevice, s));
   }
-  const int per_sm = std::min(blocks_per_sm, resident_blocks((const void*)k_batch_pcg, kBT));
+  const void* kern = mixed ? (const void*)k_batch_mixed : (const void*)k_batch_pcg;
+  const int per_sm = std::min(blocks_per_sm, resident_blocks(kern, kBT));
   const int grid = p->n_sm * std::max(1, per_sm);
+  const int cgrid = blocks_for(p->nnz, 256, p->n_sm * 8);
   // the solve itself (reset + one cooperative launch) is one CUDA graph, replayed while the
   // operands and the schedule stay the same; a device that refuses to capture the cooperative
   // launch gets the same two launches directly
   const void* key[8] = {(const void*)(uintptr_t)h, p->batch_ws, vals, b, x, dinv,
-                        (const void*)(uintptr_t)grid, (const void*)(uintptr_t)((uint64_t)maxiter << 1)};
+                        (const void*)(uintptr_t)grid,
+                        (const void*)(uintptr_t)(((uint64_t)maxiter << 1) | (mixed ? 1u : 0u))};
   bool have = p->batch_exec != nullptr;
   for (int i = 0; i < 8 && have; ++i) have = key[i] == p->batch_key[i];
   if (!have && p->batch_graph_ok) {
@@ -377,9 +610,9 @@ extern "C" int femk_pcg_batched(const femk_plan* pc, int32_t nprob, const int64_
     cudaError_t e = cudaStreamBeginCapture(p->batch_stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       k_batch_reset<<<8, 256, 0, p->batch_stream>>>(a.done, a.status, a.active, nprob, a.bar);
+      if (mixed) k_to_f32<<<cgrid, 256, 0, p->batch_stream>>>(vals, p->nnz, p->vals32);
       void* cargs[] = {(void*)&a};
-      cudaError_t el = cudaLaunchCooperativeKernel((const void*)k_batch_pcg, dim3(grid), dim3(kBT), cargs, 0,
-                                                   p->batch_stream);
+      cudaError_t el = cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), cargs, 0, p->batch_stream);
       cudaError_t ee = cudaStreamEndCapture(p->batch_stream, &g);
       if (el == cudaSuccess && ee == cudaSuccess && g) e = cudaGraphInstantiate(&p->batch_exec, g, 0);
       else e = el != cudaSuccess ? el : ee;
@@ -400,29 +633,32 @@ extern "C" int femk_pcg_batched(const femk_plan* pc, int32_t nprob, const int64_
     FEMK_CUDA_TRY(cudaEventRecord(p->batch_ev, s));
     FEMK_CUDA_TRY(cudaStreamWaitEvent(p->batch_stream, p->batch_ev, 0));
     FEMK_CUDA_TRY(cudaGraphLaunch(p->batch_exec, p->batch_stream));
-    count_launches(2);
+    count_launches(mixed ? 3 : 2);
     p->batch_graph_used = 1;
     FEMK_CUDA_TRY(cudaEventRecord(p->batch_ev, p->batch_stream));
     FEMK_CUDA_TRY(cudaStreamWaitEvent(s, p->batch_ev, 0));
   } else {
     k_batch_reset<<<::femk::counted_launch() + 8, 256, 0, s>>>(a.done, a.status, a.active, nprob, a.bar);
+    if (mixed) k_to_f32<<<::femk::counted_launch() + cgrid, 256, 0, s>>>(vals, p->nnz, p->vals32);
     FEMK_CUDA_TRY(cudaGetLastError());
     void* args[] = {(void*)&a};
     counted_launch();
-    FEMK_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_batch_pcg, dim3(grid), dim3(kBT), args, 0, s));
+    FEMK_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), args, 0, s));
     p->batch_key[0] = (const void*)(uintptr_t)h;
     p->batch_key[1] = p->batch_ws;
     p->batch_graph_used = 0;
   }
-  std::vector<int32_t> it(nprob), stv(nprob);
+  std::vector<int32_t> it(nprob), stv(nprob), outer(nprob);
   std::vector<double> rel(nprob);
   unsigned int timeout = 0;
   FEMK_CUDA_TRY(cudaMemcpyAsync(it.data(), a.iter, 4 * nprob, cudaMemcpyDeviceToHost, s));
+  if (mixed) FEMK_CUDA_TRY(cudaMemcpyAsync(outer.data(), a.outer, 4 * nprob, cudaMemcpyDeviceToHost, s));
   FEMK_CUDA_TRY(cudaMemcpyAsync(stv.data(), a.status, 4 * nprob, cudaMemcpyDeviceToHost, s));
   FEMK_CUDA_TRY(cudaMemcpyAsync(rel.data(), a.relres, 8 * nprob, cudaMemcpyDeviceToHost, s));
   FEMK_CUDA_TRY(cudaMemcpyAsync(&timeout, &a.bar->timeout, 4, cudaMemcpyDeviceToHost, s));
   FEMK_CUDA_TRY(cudaStreamSynchronize(s));
   if (iters_out) std::copy(it.begin(), it.end(), iters_out);
+  if (outer_out && mixed) std::copy(outer.begin(), outer.end(), outer_out);
   if (relres_out) std::copy(rel.begin(), rel.end(), relres_out);
   if (status_out) std::copy(stv.begin(), stv.end(), status_out);
   if (timeout) {
@@ -438,4 +674,27 @@ extern "C" int femk_pcg_batched(const femk_plan* pc, int32_t nprob, const int64_
     return worst;
   }
   return FEMK_OK;
+}
+
+}  // namespace
+
+extern "C" int femk_pcg_batched(const femk_plan* pc, int32_t nprob, const int64_t* row_off, const double* vals,
+                                const double* b, double* x, const double* dinv, double tol, double atol,
+                                int32_t maxiter, int32_t tile_rows, int32_t blocks_per_sm, int32_t* iters_out,
+                                double* relres_out, int32_t* status_out, void* stream) {
+  clear_error();
+  return batched_impl(pc, nprob, row_off, vals, b, x, dinv, tol, atol, maxiter, tile_rows, blocks_per_sm, iters_out,
+                      nullptr, relres_out, status_out, stream, false, 0.0);
+}
+
+extern "C" int femk_pcg_batched_mixed(const femk_plan* pc, int32_t nprob, const int64_t* row_off, const double* vals,
+                                      const double* b, double* x, const double* dinv, double tol, double atol,
+                                      int32_t maxiter, int32_t tile_rows, int32_t blocks_per_sm, int32_t* iters_out,
+                                      int32_t* outer_out, double* relres_out, int32_t* status_out, void* stream) {
+  clear_error();
+  // reliable-update threshold of the single-problem mixed solver (femk_pcg_mixed)
+  double delta2 = 1e-4;
+  if (const char* e = std::getenv("FEMK_MIXED_DELTA2")) delta2 = std::atof(e);  // tuning runs
+  return batched_impl(pc, nprob, row_off, vals, b, x, dinv, tol, atol, maxiter, tile_rows, blocks_per_sm, iters_out,
+                      outer_out, relres_out, status_out, stream, true, delta2);
 }

@@ -268,6 +268,30 @@ class FemPlan:
         self.batch_graph = bool(info.batch_graph)
         return x, it, rel, stv, st
 
+    def pcg_batched_mixed(self, row_off, vals, b, inv_diag, x=None, tol=1e-8, atol=0.0, maxiter=20_000,
+                          tile_rows=2048, blocks_per_sm=2):
+        """Mixed-precision form of :meth:`pcg_batched` (FP32 inner CG, FP64 reliable updates).
+
+        Returns (x, FP32 iterations i32[nprob], FP64 updates i32[nprob], relres f64[nprob],
+        status i32[nprob], return status)."""
+        ro = np.ascontiguousarray(np.asarray(row_off, dtype=np.int64))
+        nprob = ro.size - 1
+        x = torch.zeros(self.n, dtype=torch.float64, device=self.device) if x is None else x
+        it = np.zeros(nprob, dtype=np.int32)
+        outer = np.zeros(nprob, dtype=np.int32)
+        rel = np.zeros(nprob, dtype=np.float64)
+        stv = np.zeros(nprob, dtype=np.int32)
+        c = ctypes.c_void_p
+        st = self._lib.femk_pcg_batched_mixed(
+            self._h, nprob, c(ro.ctypes.data), _lib.ptr(vals), _lib.ptr(b), _lib.ptr(x), _lib.ptr(inv_diag),
+            float(tol), float(atol), int(maxiter), int(tile_rows), int(blocks_per_sm), c(it.ctypes.data),
+            c(outer.ctypes.data), c(rel.ctypes.data), c(stv.ctypes.data), _lib.stream_handle())
+        _lib.check(st, allow=(_lib.FEMK_NOT_CONVERGED,))
+        info = _lib.PlanInfo()
+        _lib.check(self._lib.femk_plan_get_info(self._h, ctypes.byref(info)))
+        self.batch_graph = bool(info.batch_graph)
+        return x, it, outer, rel, stv, st
+
     def adjoint_grad(self, param, u, lam, mode=_lib.COEF_EXP, scale=1.0, out=None):
         nodal = mode in (_lib.COEF_NODAL_EXP, _lib.COEF_NODAL_LINEAR)
         size = self.nvert if nodal else self.ntet

@@ -71,3 +71,33 @@ def test_batched_replay_is_bitwise_reproducible():
     x1, it1, rel1 = batch.solve(vals, b, schedule=sched)
     x2, it2, rel2 = batch.solve(vals, b, schedule=sched)
     assert torch.equal(x1, x2) and np.array_equal(it1, it2) and np.array_equal(rel1, rel2)
+
+
+@pytest.mark.parametrize("tile_rows,bps", [(32, 2), (2048, 1)])
+def test_batched_mixed_reaches_the_fp64_stop_rule(tile_rows, bps):
+    """The mixed-precision batched solve: every problem's FP64 residual meets the 1e-8 stop rule,
+    each solution is within 1e-6 of the per-problem FP64 oracle, the large problems take FP64
+    reliable updates, and the graph replay is bit-identical."""
+    from jno_b200.batch import BatchedPoisson
+
+    sides = [3, 5, 1, 8, 4, 6, 2, 12, 16]
+    probs = _problems(sides)
+    batch = BatchedPoisson([(p, t) for p, t, _ in probs])
+    vals, b = batch.assemble([lk for _, _, lk in probs])
+    sched = {"tile_rows": tile_rows, "blocks_per_sm": bps}
+    x, it, rel = batch.solve(vals, b, tol=1e-8, schedule=sched, precision="mixed")
+    outer = batch.last_outer.copy()
+    xs = batch.split(x)
+    for k, (pts, tets, lk) in enumerate(probs):
+        bnd = om.boundary_nodes(tets, 1)
+        s = oa.assemble(pts, tets, 1, bnd, np.exp(lk))
+        if np.linalg.norm(s.b) == 0:
+            assert it[k] == 0 and np.all(xs[k] == 0)
+            continue
+        xo, ito, _ = op.pcg(s.csr(), s.b, oa.jacobi_inverse(oa.matrix_diagonal(s)), tol=1e-12)
+        assert rel[k] <= 1e-8, (k, rel[k])
+        assert np.linalg.norm(xs[k] - xo) <= 1e-6 * np.linalg.norm(xo), k
+        assert outer[k] >= 1
+    assert outer[-1] >= 2  # the 16^3 problem needs FP64 reliable updates to reach 1e-8
+    x2, it2, rel2 = batch.solve(vals, b, tol=1e-8, schedule=sched, precision="mixed")
+    assert torch.equal(x, x2) and np.array_equal(it, it2)

@@ -188,3 +188,33 @@ def test_jno_surface_march_reaches_steady_state():
     fem_s = jno.fem([2.0 * (ui.x * vi.x + ui.y * vi.y) - 1.0 * vi, bc])
     steady = fem_s.solve(linear=jno.solve.bicgstab(tol=1e-12))
     assert (torch.linalg.norm(final - steady) / torch.linalg.norm(steady)).item() <= 1e-8
+
+
+def test_jno_surface_3d_parametric_crank_nicolson():
+    """The parametric route on the Kuhn box: exp(logk) P0 coefficient, source 1, u = 0.1 on the
+    boundary, u0 = sin(pi x) sin(pi y) sin(pi z), Crank-Nicolson over 5 steps, against the oracle."""
+    import jno_b200 as jno
+
+    n, time = 5, (0.0, 0.02, 6)
+    d = jno.domain(jno.domain.equi_distant_box(nx=n, ny=n, nz=n), jitter=0.1, seed=0, time=time)
+    u, v = d.fem_symbols()
+    _r, s = d.fem_symbols(space="P0", names=("r", "s"))
+    xi, yi, zi, ti = d.variable("interior", split=True)
+    xb, yb, zb, _ = d.variable("boundary", split=True)
+    ci = d.variable("initial", split=True)
+    ui, vi = u.bind(x=xi, y=yi, z=zi, t=ti), v.bind(x=xi, y=yi, z=zi, t=ti)
+    logk = jno.np.parameter(s, name="logk")
+    ic = jno.np.sin(np.pi * ci[0]) * jno.np.sin(np.pi * ci[1]) * jno.np.sin(np.pi * ci[2])
+    fem = jno.fem([ui.t * vi + jno.np.exp(logk) * (ui.x * vi.x + ui.y * vi.y + ui.z * vi.z) - 1.0 * vi,
+                   u(xb, yb, zb) - 0.1, u(ci[0], ci[1], ci[2]) - ic])
+    lk = om.logk_field(6 * n**3, 14)
+    sol = fem.solve(args={"logk": lk}, time=jno.solve.theta(0.5))
+    traj = sol.fn().cpu().numpy()
+    assert traj.shape == (6, fem.dofs) and np.allclose(sol.ts, np.linspace(0.0, 0.02, 6))
+    pf, cf, cells, p1 = om.kuhn_cube(n, 1, seed=0)
+    bnd = om.boundary_nodes(cf, 1)
+    u0 = np.sin(np.pi * pf[:, 0]) * np.sin(np.pi * pf[:, 1]) * np.sin(np.pi * pf[:, 2])
+    blk = ot.block(pf, cf, 1, bnd, np.exp(lk), f=1.0, g=np.full(pf.shape[0], 0.1), parametric=True)
+    to, _, _ = ot.march(blk, u0, 0.004, 5, theta=0.5)
+    assert np.abs(traj - to).max() <= 1e-8 * np.abs(to).max()
+    assert fem.stats["transient"]["step_residual"] < 1e-9
