@@ -1087,8 +1087,10 @@ __global__ void k_zero(double* __restrict__ y, int64_t n, const CgState* st) {
 int launch_matfree(const femk_plan* p, const MatFree& m, const double* x, double* y, cudaStream_t s,
                    const CgState* st = nullptr) {
   k_zero<<<::femk::counted_launch() + p->n_sm * 8, 256, 0, s>>>(y, p->n, st);
-  const int grid = blocks_for(p->ntet, 128, p->n_sm * 16);
-  FEMK_BY_ND(p->nd, k_matfree<ND><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, m.param, m.mode, m.scale, x, y, st));
+  if (!launch_matfree_cl(p, m.param, m.mode, m.scale, x, y, st, s)) {
+    const int grid = blocks_for(p->ntet, 128, p->n_sm * 16);
+    FEMK_BY_ND(p->nd, k_matfree<ND><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, m.param, m.mode, m.scale, x, y, st));
+  }
   FEMK_CUDA_TRY(cudaGetLastError());
   if (p->n_dir > 0) {
     k_dirichlet_identity<<<::femk::counted_launch() + blocks_for(p->n_dir, 256, 65535), 256, 0, s>>>(p->dlist, p->n_dir, x, y, st);
@@ -1480,6 +1482,7 @@ extern "C" int femk_spmv_matfree(const femk_plan* p, const double* param, int mo
   FEMK_CHECK_ARG(p && x && y, "femk_spmv_matfree: NULL argument");
   FEMK_CHECK_ARG(coef_mode_ok(p, mode, param), "femk_spmv_matfree: bad coefficient");
   FEMK_TRY(resolve_coef(p, param, mode, (cudaStream_t)stream, &param, &mode));
+  FEMK_TRY(ensure_clusters(const_cast<femk_plan*>(p), (cudaStream_t)stream));
   MatFree m{param, mode, scale};
   return launch_matfree(p, m, x, y, (cudaStream_t)stream);
 }
@@ -1515,6 +1518,7 @@ extern "C" int femk_pcg_matfree(const femk_plan* p, const double* param, int mod
   FEMK_CHECK_ARG(p && b && x, "femk_pcg_matfree: NULL argument");
   FEMK_CHECK_ARG(coef_mode_ok(p, mode, param), "femk_pcg_matfree: bad coefficient");
   FEMK_TRY(resolve_coef(p, param, mode, (cudaStream_t)stream, &param, &mode));
+  FEMK_TRY(ensure_clusters(const_cast<femk_plan*>(p), (cudaStream_t)stream));  // before any capture
   MatFree m{param, mode, scale};
   return pcg_run(p, nullptr, &m, b, x, dinv, tol, atol, maxiter, iters_out, relres_out, (cudaStream_t)stream);
 }

@@ -49,15 +49,15 @@ struct Geom {
 };
 using TetGeom = Geom<4>;
 
-__device__ __forceinline__ void tet_geometry(const double* __restrict__ xyz, int32_t v0, int32_t v1, int32_t v2,
-                                             int32_t v3, TetGeom& G) {
-  double x0[3], e1[3], e2[3], e3[3];
+// Geometry from vertex coordinates P[i] (x, y, z of vertex i); the loaders below read them from
+// the plan's coordinate array or from a shared-memory copy.
+__device__ __forceinline__ void tet_geometry_of(const double (&P)[4][3], Geom<4>& G) {
+  double e1[3], e2[3], e3[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    x0[k] = __ldg(xyz + (int64_t)v0 * 3 + k);
-    e1[k] = __ldg(xyz + (int64_t)v1 * 3 + k) - x0[k];
-    e2[k] = __ldg(xyz + (int64_t)v2 * 3 + k) - x0[k];
-    e3[k] = __ldg(xyz + (int64_t)v3 * 3 + k) - x0[k];
+    e1[k] = P[1][k] - P[0][k];
+    e2[k] = P[2][k] - P[0][k];
+    e3[k] = P[3][k] - P[0][k];
   }
   const double c23[3] = {e2[1] * e3[2] - e2[2] * e3[1], e2[2] * e3[0] - e2[0] * e3[2], e2[0] * e3[1] - e2[1] * e3[0]};
   const double c31[3] = {e3[1] * e1[2] - e3[2] * e1[1], e3[2] * e1[0] - e3[0] * e1[2], e3[0] * e1[1] - e3[1] * e1[0]};
@@ -75,11 +75,9 @@ __device__ __forceinline__ void tet_geometry(const double* __restrict__ xyz, int
   G.vol = fabs(det) * (1.0 / 6.0);
 }
 
-__device__ __forceinline__ void tri_geometry(const double* __restrict__ xyz, int32_t v0, int32_t v1, int32_t v2,
-                                             Geom<3>& G) {
-  const double x0 = __ldg(xyz + (int64_t)v0 * 3), y0 = __ldg(xyz + (int64_t)v0 * 3 + 1);
-  const double e1x = __ldg(xyz + (int64_t)v1 * 3) - x0, e1y = __ldg(xyz + (int64_t)v1 * 3 + 1) - y0;
-  const double e2x = __ldg(xyz + (int64_t)v2 * 3) - x0, e2y = __ldg(xyz + (int64_t)v2 * 3 + 1) - y0;
+__device__ __forceinline__ void tri_geometry_of(const double (&P)[3][3], Geom<3>& G) {
+  const double e1x = P[1][0] - P[0][0], e1y = P[1][1] - P[0][1];
+  const double e2x = P[2][0] - P[0][0], e2y = P[2][1] - P[0][1];
   const double det = e1x * e2y - e1y * e2x;
   const double inv = 1.0 / det;
   G.g[1][0] = e2y * inv;
@@ -90,6 +88,47 @@ __device__ __forceinline__ void tri_geometry(const double* __restrict__ xyz, int
   G.g[0][1] = -(G.g[1][1] + G.g[2][1]);
   G.det = det;
   G.vol = fabs(det) * 0.5;
+}
+
+__device__ __forceinline__ void tet_geometry(const double* __restrict__ xyz, int32_t v0, int32_t v1, int32_t v2,
+                                             int32_t v3, TetGeom& G) {
+  double P[4][3];
+  const int32_t v[4] = {v0, v1, v2, v3};
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) P[i][k] = __ldg(xyz + (int64_t)v[i] * 3 + k);
+  tet_geometry_of(P, G);
+}
+
+__device__ __forceinline__ void tri_geometry(const double* __restrict__ xyz, int32_t v0, int32_t v1, int32_t v2,
+                                             Geom<3>& G) {
+  double P[3][3];
+  const int32_t v[3] = {v0, v1, v2};
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 2; ++k) P[i][k] = __ldg(xyz + (int64_t)v[i] * 3 + k);
+  P[0][2] = P[1][2] = P[2][2] = 0.0;
+  tri_geometry_of(P, G);
+}
+
+// the same from a coordinate array in shared memory (3 per local slot), vertices at slots loc[0..NV)
+__device__ __forceinline__ void cell_geometry_at(const double* xs, const int* loc, Geom<4>& G) {
+  double P[4][3];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) P[i][k] = xs[loc[i] * 3 + k];
+  tet_geometry_of(P, G);
+}
+__device__ __forceinline__ void cell_geometry_at(const double* xs, const int* loc, Geom<3>& G) {
+  double P[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) P[i][k] = k < 2 ? xs[loc[i] * 3 + k] : 0.0;
+  tri_geometry_of(P, G);
 }
 
 // geometry of the element whose first NV local dofs (its vertices) are dof[0..NV)

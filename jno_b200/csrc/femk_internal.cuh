@@ -188,6 +188,15 @@ struct femk_plan {
   void* prof = nullptr;         // per-kernel CG timing (femk_set_profiling)
   double* coef_tmp = nullptr;   // f64[ntet] element coefficients of a nodal parameter
   double* theta_ws = nullptr;   // f64[2 vstride] theta march: step Jacobi inverse, step right-hand side
+  // element clusters of the matrix-free operator (built on first use): distinct DOFs per cluster
+  // of 128 consecutive elements and each element's local slots; cl_state 0 unbuilt, 1 ready, -1 off
+  int32_t* cl_ptr = nullptr;    // i32[ncl+1]
+  int32_t* cl_dof = nullptr;    // i32[cl_ptr[ncl]]
+  uint16_t* cl_loc = nullptr;   // u16[ntet*nd]
+  uint16_t* cl_off = nullptr;   // u16[cl_ptr[ncl] + ncl] per cluster: slot offsets into its pair list
+  uint16_t* cl_inv = nullptr;   // u16[ncl*128*nd] per cluster: (element, local dof) pairs sorted by slot
+  int64_t ncl = 0;
+  int cl_max = 0, cl_grid = 0, cl_state = 0;
   // BiCGStab workspace (8 vectors), state, stream, events and captured chunk graph
   void* bicg_ws = nullptr;
   void* bicg_state = nullptr;
@@ -225,6 +234,13 @@ int ensure_workspace(femk_plan* p);
 // stream s) read as FEMK_COEF_LINEAR; other modes pass through unchanged.
 int resolve_coef(const femk_plan* p, const double* param, int mode, cudaStream_t s, const double** param_out,
                  int* mode_out);
+
+// Matrix-free operator on element clusters staged in shared memory (femk_cluster.cu):
+// ensure_clusters builds the tables once (host work; call outside any graph capture),
+// launch_matfree_cl adds A x into y and returns false when the plan has none.
+int ensure_clusters(femk_plan* p, cudaStream_t s);
+bool launch_matfree_cl(const femk_plan* p, const double* param, int mode, double scale, const double* x, double* y,
+                       const CgState* st, cudaStream_t s);
 
 // Blocks of `threads` threads of kernel `fn` resident per SM (occupancy), cached per kernel.
 int resident_blocks(const void* fn, int threads);

@@ -610,3 +610,24 @@ def test_p0_linearity_and_support_on_device():
             assert np.abs(vjn[off & free]).max() == 0.0
     a, fl = acc.cpu().numpy(), full.cpu().numpy()
     assert np.abs(a[free] - fl[free]).max() <= 1e-12 * np.abs(fl).max()
+
+
+@pytest.mark.parametrize("n,order", [(8, 1), (4, 2)])
+def test_cluster_staged_matrix_free_matches(n, order, monkeypatch):
+    """The opt-in matrix-free operator on shared-memory-staged element clusters (FEMK_MATFREE_CL=1)
+    agrees with the assembled operator to 1e-12 and solves like it."""
+    monkeypatch.setenv("FEMK_MATFREE_CL", "1")
+    pf, cf, tets, p1 = _mesh(n, order, seed=5)
+    logk = om.logk_field(len(tets), 8)
+    plan = _plan(p1, tets, order)
+    lk = torch.as_tensor(logk, device="cuda")
+    vals, b = plan.assemble(lk)
+    xv = torch.as_tensor(np.random.default_rng(1).standard_normal(plan.n), device="cuda")
+    y = plan.spmv(vals, xv).cpu().numpy()
+    ym = plan.spmv_matfree(lk, xv).cpu().numpy()
+    assert np.abs(ym - y).max() <= 1e-12 * np.abs(y).max()
+    inv = plan.jacobi_matfree(lk)
+    u1, it1, _, _ = plan.pcg(vals, b, inv_diag=plan.jacobi(vals))
+    u2, it2, rel2, _ = plan.pcg_matfree(lk, b, inv_diag=inv)
+    assert abs(it1 - it2) <= 1 and rel2 <= 2e-8
+    assert torch.linalg.norm(u1 - u2) <= 1e-7 * torch.linalg.norm(u1)
