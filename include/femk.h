@@ -248,8 +248,10 @@ int femk_assemble_theta(const femk_plan* plan, const double* param_dev, int coef
  *   rhs = rhs_vals u + q;  u <- Jacobi-BiCGStab(step_vals, rhs, x0 = u, tol, atol = 0, maxiter)
  * with the Jacobi inverse of diag(step_vals) (|d| <= 1e-30 -> 1), jax bicgstab semantics as
  * femk_bicgstab. After each step the relative residual ||S u - rhs|| / max(||rhs||, eps) must be
- * below 1e-9 (the reference's step check; it re-solves with GMRES otherwise, which is not built
- * here: the march stops with FEMK_NOT_CONVERGED). u_dev f64[n] holds the state (in/out);
+ * below step_check: 1e-9 is the reference's check of its default step solve (tol 1e-10; it
+ * re-solves with GMRES otherwise, which is not built here: the march stops with
+ * FEMK_NOT_CONVERGED); step_check <= 0 skips the check, as the solver-slot path of
+ * compose_transient_step_solvers (jno/utils/solver/solver_api.py:929-945) does. u_dev f64[n] holds the state (in/out);
  * traj_dev f64[nsteps*n] or NULL receives the state after every step; iters_out i32[nsteps] (host)
  * or NULL; *relres_out (host, may be NULL) = the largest step residual. The step operator is
  * gathered into the plan's solver layout once per call: it replaces the operator a previous
@@ -257,7 +259,7 @@ int femk_assemble_theta(const femk_plan* plan, const double* param_dev, int coef
  */
 int femk_theta_march(const femk_plan* plan, const double* step_vals_dev, const double* rhs_vals_dev,
                      const double* q_dev, double* u_dev, int32_t nsteps, double tol, int32_t maxiter,
-                     double* traj_dev, int32_t* iters_out, double* relres_out, void* stream);
+                     double step_check, double* traj_dev, int32_t* iters_out, double* relres_out, void* stream);
 
 /*
  * Allocation-free Jacobi-PCG: the same iteration and result as femk_pcg, for callers that must

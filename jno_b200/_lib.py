@@ -102,7 +102,7 @@ SIGNATURES = {
     "femk_lumped_mass": [_P, _P, _P],
     "femk_mass_matrix": [_P, _I, _P, _P],
     "femk_assemble_theta": [_P, _P, _I, _D, _D, _P, _D, _D, _I, _P, _P, _P, _P],
-    "femk_theta_march": [_P, _P, _P, _P, _P, _I32, _D, _I32, _P, _P, ctypes.POINTER(_D), _P],
+    "femk_theta_march": [_P, _P, _P, _P, _P, _I32, _D, _I32, _D, _P, _P, ctypes.POINTER(_D), _P],
 }
 
 _lib = None

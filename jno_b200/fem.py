@@ -172,22 +172,44 @@ class FEM:
                                         theta, self.dt, route)
 
     def _march(self, time=None, args=None, linear=None, precond=None):
+        """The theta march. No slots: the default step solve of SemidiscreteTimeBlock.step
+        (Jacobi-BiCGStab at tol 1e-10 plus the 1e-9 step check, backend_blocks.py:386-413). With a
+        ``linear`` and/or ``precond`` slot: compose_transient_step_solvers (solver_api.py:911-945),
+        i.e. the slot solver (``jno.solve.bicgstab()`` when only ``precond`` is given) at its own
+        tolerance with the step operator's Jacobi preconditioner and no step check, the solver's
+        residual guard applying per step."""
         if time is not None and not isinstance(time, ThetaScheme):
             raise NotImplementedError("time= takes jno.solve.theta(...) on the B200 path")
         if precond is not None and not isinstance(precond, (_Jacobi, JacobiApplier)):
-            raise NotImplementedError("the transient step solve is Jacobi-BiCGStab on the B200 path")
-        tol, maxiter = 1e-10, 20_000  # the per-step default of backend_blocks.py:394-396
-        if linear is not None:
-            if not isinstance(linear, LinearSolver) or linear.name != "bicgstab":
-                raise NotImplementedError("the transient step solve is Jacobi-BiCGStab on the B200 path")
-            tol, maxiter = linear.tol, linear.maxiter
+            raise NotImplementedError("the transient step preconditioner is Jacobi on the B200 path")
+        slots = linear is not None or precond is not None
+        solver = linear if linear is not None else (bicgstab() if slots else None)
+        if solver is not None and (not isinstance(solver, LinearSolver) or solver.name not in ("bicgstab", "cg")
+                                   or solver.precision != "fp64"):
+            raise NotImplementedError("the transient step solve is Jacobi-BiCGStab or Jacobi-CG on the B200 path")
         th = 1.0 if time is None else time.theta
         S, R, q = self.step_operators(args, th)
         t0, t1, n_steps = self.time
         traj = torch.empty((n_steps, self.plan.n), dtype=torch.float64, device=self.plan.device)
         traj[0] = self._u0
         u = self._u0.clone()
-        _, iters, worst = self.plan.theta_march(S, R, q, u, n_steps - 1, tol, maxiter, traj=traj[1:])
+        if solver is None:  # the per-step default of backend_blocks.py:394-396
+            _, iters, worst = self.plan.theta_march(S, R, q, u, n_steps - 1, 1e-10, 20_000, traj=traj[1:])
+        elif solver.name == "bicgstab":
+            _, iters, worst = self.plan.theta_march(S, R, q, u, n_steps - 1, solver.tol, solver.maxiter,
+                                                    traj=traj[1:], step_check=0.0)
+        else:
+            inv = self.plan.jacobi(S)
+            iters, worst = [], 0.0
+            for k in range(1, n_steps):
+                rhs = self.plan.spmv(R, u) + q
+                _, it, rel, st = self.plan.pcg(S, rhs, u, inv, solver.tol, solver.atol, solver.maxiter)
+                iters.append(it)
+                worst = max(worst, rel)
+                traj[k] = u
+            iters = np.asarray(iters, dtype=np.int32)
+        if slots and not worst <= 1e-4:  # the slot solver's eager residual guard (solver_api.py:224-240)
+            raise RuntimeError(f"jno.solve.{solver.name} did not solve a transient step (relative residual {worst:.1e})")
         self.stats["transient"] = {"theta": th, "dt": self.dt, "iterations": iters, "step_residual": worst}
         ts = np.linspace(t0, t1, n_steps)
         return TransientSolution(traj, ts, iters, worst)

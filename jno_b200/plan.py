@@ -323,13 +323,15 @@ class FemPlan:
                                                  _lib.ptr(R), _lib.ptr(q), _lib.stream_handle()))
         return S, R, q
 
-    def theta_march(self, step_vals, rhs_vals, q, u, nsteps, tol=1e-10, maxiter=20_000, traj=None):
-        """Advance u (in place) by nsteps theta steps. Returns (u, iterations i32[nsteps], worst step
-        residual); traj f64[nsteps, n] receives every state when given."""
+    def theta_march(self, step_vals, rhs_vals, q, u, nsteps, tol=1e-10, maxiter=20_000, traj=None,
+                    step_check=1e-9):
+        """Advance u (in place) by nsteps theta steps (Jacobi-BiCGStab per step). Returns (u,
+        iterations i32[nsteps], worst step residual); traj f64[nsteps, n] receives every state when
+        given; a step whose relative residual is not below step_check stops the march (<= 0: none)."""
         it = np.zeros(max(int(nsteps), 1), dtype=np.int32)
         worst = ctypes.c_double(0.0)
         _lib.check(self._lib.femk_theta_march(
             self._h, _lib.ptr(step_vals), _lib.ptr(rhs_vals), _lib.ptr(q), _lib.ptr(u), int(nsteps), float(tol),
-            int(maxiter), _lib.ptr(traj), ctypes.c_void_p(it.ctypes.data), ctypes.byref(worst),
+            int(maxiter), float(step_check), _lib.ptr(traj), ctypes.c_void_p(it.ctypes.data), ctypes.byref(worst),
             _lib.stream_handle()))
         return u, it[: int(nsteps)], worst.value

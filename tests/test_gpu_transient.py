@@ -218,3 +218,21 @@ def test_jno_surface_3d_parametric_crank_nicolson():
     to, _, _ = ot.march(blk, u0, 0.004, 5, theta=0.5)
     assert np.abs(traj - to).max() <= 1e-8 * np.abs(to).max()
     assert fem.stats["transient"]["step_residual"] < 1e-9
+
+
+def test_jno_surface_transient_solver_slots_match_default():
+    """Port of tests/test_fem_solver_transient.py:54-69: with solver slots the per-step solve is
+    the slot solver at its own tolerance with the step operator's Jacobi preconditioner
+    (compose_transient_step_solvers); CG + Jacobi at 1e-10 and BiCGStab + Jacobi (the precond-only
+    slot, tolerance 1e-8) reproduce the default backward-Euler trajectory."""
+    import jno_b200 as jno
+
+    fem = _heat(jno, 10, (0.0, 0.2, 21))
+    ref = fem.solve().fn()
+    cg = fem.solve(linear=jno.solve.cg(tol=1e-10), precond=jno.precond.jacobi()).fn()
+    assert (cg - ref).abs().max().item() < 1e-8
+    bi = fem.solve(precond=jno.precond.jacobi()).fn()
+    assert (bi - ref).abs().max().item() < 1e-6
+    assert fem.stats["transient"]["step_residual"] <= 1e-4
+    with pytest.raises(NotImplementedError):
+        fem.solve(linear=jno.solve.cg(precision="mixed"))
