@@ -174,7 +174,10 @@ struct femk_plan {
   cudaStream_t mx_stream = nullptr;
   cudaEvent_t mx_ev[3] = {nullptr, nullptr, nullptr};
   cudaGraphExec_t mx_exec = nullptr;
-  const void* mx_key[4] = {nullptr, nullptr, nullptr, nullptr};
+  const void* mx_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  float* mx_zp = nullptr;  // f32[4 vstride]: the fused mixed form's two (z, p) pair buffers
+  int mx_fz = 0;           // the fused mixed form is enabled for this plan (FEMK_MIXED_FUSE)
+  int mx_fz_on = 0;        // ... and applies to the current solve (bulk-copy FP32 step, split updates)
   int mx_nodes = 0;
   void* mx_host = nullptr;  // pinned state mirrors
   // batched solver workspace (tiles, per-problem state, partials)

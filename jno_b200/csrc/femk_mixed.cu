@@ -41,6 +41,24 @@ struct MixedState {
   int32_t outer, restart;
   uint32_t ticket;
   int32_t epend;  // split update: 1 while e += alpha p of the current iteration is still to be applied
+  int32_t par;    // fused form: the (z, p) pair buffer the next step reads (flipped by each update)
+};
+
+// Fused form of the inner iteration (two kernels instead of three): z and p live interleaved as
+// float2 pairs in two buffers. The step gathers the pairs of its columns and forms
+// p = fmaf(beta, p, z) on the fly (the arithmetic of k_pupdate32_x), writes each row's new p into
+// the other buffer, and the update kernel then applies e += alpha p, r -= alpha q and z = D^-1 r
+// on that buffer and flips the parity. Same iterates as the three-kernel split. Opt-in
+// (FEMK_MIXED_FUSE=1): measured on B200 at P1 128^3 (same box, same 513 inner iterations) 31.9 ms
+// per mixed solve against 25.7 ms for the split. The step is bound by gather latency and issue,
+// and 8-byte pair gathers plus the p store cost more than the kernel they save.
+struct GatherZP {
+  const float2* zp;
+  float beta;
+  __device__ __forceinline__ float operator()(int32_t j) const {
+    const float2 v = __ldg(zp + j);
+    return fmaf(beta, v.y, v.x);
+  }
 };
 
 template <int NV, int THREADS = kThreads>
@@ -161,13 +179,16 @@ __global__ void __launch_bounds__(kThreads, 8) k_step32_sell(const int64_t* __re
 
 // The same step with the FP32 sliced-ELL stream moved into shared memory by bulk copies
 // (femk_bulk.cuh): WPB warps per block, S slices in flight per warp, widths up to WMAX.
-template <int WMAX, int S, int WPB, bool H>
+// K = 0 plain, 1 with L2 evict-last hints, 2 the fused form (p formed from the (z, p) pairs zp).
+template <int WMAX, int S, int WPB, int K>
 __global__ void __launch_bounds__(WPB * 32) k_step32_bulk(const int64_t* __restrict__ sptr,
                                                          const int16_t* __restrict__ cols,
                                                          const float* __restrict__ vals, int64_t n, int64_t nslices,
                                                          const float* __restrict__ p, float* __restrict__ q,
                                                          double* __restrict__ partials, MixedState* st,
-                                                         const int64_t* __restrict__ cptr) {
+                                                         const int64_t* __restrict__ cptr, float2* __restrict__ zp,
+                                                         int64_t zs) {
+  constexpr bool H = K == 1;
   extern __shared__ __align__(128) unsigned char bulk_smem[];
   constexpr int kWarpBytes = BulkRing<float, int16_t, WMAX, S>::kWarpBytes;
   pdl_wait();
@@ -176,18 +197,36 @@ __global__ void __launch_bounds__(WPB * 32) k_step32_bulk(const int64_t* __restr
   if (st->done || st->hold) return;
   const int wib = threadIdx.x >> 5;
   float acc = 0.f;
-  using G = std::conditional_t<H, GatherXL<float>, GatherX<float>>;
-  G gx;
-  gx.x = p;
-  if constexpr (H) gx.pol = l2_evict_last();
-  const bool ok = sell_bulk_rows<float, int16_t, WMAX, S>(
-      bulk_smem + wib * kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * WPB + wib,
-      (int64_t)gridDim.x * WPB, gx,
-      [&](int64_t row, float sv) {
-        q[row] = sv;
-        acc = fmaf(__ldg(p + row), sv, acc);
-      },
-      &st->status, FEMK_TIMEOUT, cptr);
+  bool ok;
+  if constexpr (K == 2) {
+    const int par = st->par;
+    const float2* zc = zp + (int64_t)par * zs;
+    float2* zn = zp + (int64_t)(par ^ 1) * zs;
+    const GatherZP gz{zc, (float)st->beta};
+    ok = sell_bulk_rows<float, int16_t, WMAX, S>(
+        bulk_smem + wib * kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * WPB + wib,
+        (int64_t)gridDim.x * WPB, gz,
+        [&](int64_t row, float sv) {
+          const float pn = gz((int32_t)row);
+          zn[row].y = pn;
+          q[row] = sv;
+          acc = fmaf(pn, sv, acc);
+        },
+        &st->status, FEMK_TIMEOUT, cptr);
+  } else {
+    using G = std::conditional_t<H, GatherXL<float>, GatherX<float>>;
+    G gx;
+    gx.x = p;
+    if constexpr (H) gx.pol = l2_evict_last();
+    ok = sell_bulk_rows<float, int16_t, WMAX, S>(
+        bulk_smem + wib * kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * WPB + wib,
+        (int64_t)gridDim.x * WPB, gx,
+        [&](int64_t row, float sv) {
+          q[row] = sv;
+          acc = fmaf(__ldg(p + row), sv, acc);
+        },
+        &st->status, FEMK_TIMEOUT, cptr);
+  }
   if (!ok && (threadIdx.x & 31) == 0) st->done = 1;
   double v[1] = {(double)acc}, tot[1];
   if (!reduce_finish<1, WPB * 32>(v, partials, &st->ticket, tot)) return;
@@ -440,6 +479,85 @@ __global__ void __launch_bounds__(kThreads) k_pupdate32_x(int64_t n, float* __re
 }
 
 // x += e; e = 0 (only at a requested update)
+// Fused form, after the step: zn = the pair buffer the step wrote p into. e += alpha p;
+// r -= alpha q; z = D^-1 r into zn; <r, z>, <r, r>; request a reliable update or set beta; flip par.
+__global__ void __launch_bounds__(kThreads) k_update32_fz(int64_t n, float* __restrict__ r, const float* __restrict__ q,
+                                                         const float* __restrict__ dinv, float* __restrict__ e,
+                                                         float2* __restrict__ zp, int64_t zs,
+                                                         double* __restrict__ partials, MixedState* st) {
+  if (st->done || st->hold) return;
+  const float alpha = (float)st->alpha;
+  float2* zn = zp + (int64_t)(st->par ^ 1) * zs;
+  float a0 = 0.f, a1 = 0.f;
+  const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  const int64_t nt = (int64_t)gridDim.x * kThreads;
+  const int64_t n4 = n >> 2;
+  float4* r4 = reinterpret_cast<float4*>(r);
+  float4* e4 = reinterpret_cast<float4*>(e);
+  const float4* q4 = reinterpret_cast<const float4*>(q);
+  const float4* d4 = reinterpret_cast<const float4*>(dinv);
+  float4* zn4 = reinterpret_cast<float4*>(zn);  // two (z, p) pairs per float4
+  for (int64_t i = tid; i < n4; i += nt) {
+    const float4 qi = q4[i], di = d4[i], ri0 = r4[i];
+    float4 ei = e4[i];
+    float4 za = zn4[2 * i], zb = zn4[2 * i + 1];  // (z0, p0, z1, p1), (z2, p2, z3, p3)
+    ei.x = fmaf(alpha, za.y, ei.x);
+    ei.y = fmaf(alpha, za.w, ei.y);
+    ei.z = fmaf(alpha, zb.y, ei.z);
+    ei.w = fmaf(alpha, zb.w, ei.w);
+    float4 ri, zi;
+    ri.x = fmaf(-alpha, qi.x, ri0.x);
+    ri.y = fmaf(-alpha, qi.y, ri0.y);
+    ri.z = fmaf(-alpha, qi.z, ri0.z);
+    ri.w = fmaf(-alpha, qi.w, ri0.w);
+    zi.x = di.x * ri.x;
+    zi.y = di.y * ri.y;
+    zi.z = di.z * ri.z;
+    zi.w = di.w * ri.w;
+    za.x = zi.x;
+    za.z = zi.y;
+    zb.x = zi.z;
+    zb.z = zi.w;
+    e4[i] = ei;
+    r4[i] = ri;
+    zn4[2 * i] = za;
+    zn4[2 * i + 1] = zb;
+    a0 = fmaf(ri.x, zi.x, fmaf(ri.y, zi.y, fmaf(ri.z, zi.z, fmaf(ri.w, zi.w, a0))));
+    a1 = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, fmaf(ri.z, ri.z, fmaf(ri.w, ri.w, a1))));
+  }
+  for (int64_t i = 4 * n4 + tid; i < n; i += nt) {
+    float2 v = zn[i];
+    e[i] = fmaf(alpha, v.y, e[i]);
+    const float ri = fmaf(-alpha, q[i], r[i]);
+    const float zi = dinv[i] * ri;
+    r[i] = ri;
+    v.x = zi;
+    zn[i] = v;
+    a0 = fmaf(ri, zi, a0);
+    a1 = fmaf(ri, ri, a1);
+  }
+  double v[2] = {(double)a0, (double)a1}, tot[2];
+  if (!reduce_finish<2>(v, partials, &st->ticket, tot)) return;
+  if (threadIdx.x) return;
+  st->iter += 1;
+  st->rr = tot[1];
+  st->par ^= 1;  // the next step reads the pairs written here
+  if (!isfinite(tot[0]) || !isfinite(tot[1])) {
+    st->status = FEMK_NONFINITE;
+    st->done = 1;
+    return;
+  }
+  const bool conv = !(tot[1] > st->atol2);
+  const bool drop = tot[1] < st->delta2 * st->rr_since;
+  if (conv || drop || st->iter >= st->maxiter) {
+    st->need_update = 1;
+    st->hold = 1;
+  } else {
+    st->beta = tot[0] / st->gamma;
+    st->gamma = tot[0];
+  }
+}
+
 __global__ void k_fold(int64_t n, double* __restrict__ x, float* __restrict__ e, const MixedState* st) {
   if (st->done || st->need_update != 1) return;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -457,8 +575,9 @@ __global__ void __launch_bounds__(kThreads) k_true_resid(const int32_t* __restri
                                                         const float* __restrict__ dinv, float* __restrict__ r,
                                                         float* __restrict__ z, float* __restrict__ p,
                                                         double* __restrict__ partials, MixedState* st, double tol2,
-                                                        double atol2) {
+                                                        double atol2, float2* __restrict__ zp, int64_t zs) {
   if (!INIT && (st->done || st->need_update != 1)) return;
+  float2* zc = zp ? zp + (int64_t)st->par * zs : nullptr;  // fused form: z into the pairs the next step reads
   const int lane = threadIdx.x & 31, sub = lane % L;
   const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
@@ -479,6 +598,12 @@ __global__ void __launch_bounds__(kThreads) k_true_resid(const int32_t* __restri
       r[row] = rf;
       z[row] = zf;
       if (INIT) p[row] = zf;
+      if (zc) {
+        if (INIT)
+          zc[row] = make_float2(zf, 0.f);  // beta = 0 at the start: the first step's p is z
+        else
+          zc[row].x = zf;
+      }
       a0 += (double)rf * (double)zf;
       a1 += r64 * r64;
       if (INIT) a2 += bi * bi;
@@ -699,19 +824,20 @@ __global__ void k_gather64(const int32_t* __restrict__ src, int64_t m, const dou
 
 template <bool INIT>
 void launch_true_resid(const femk_plan* p, const double* vals, const double* x, const double* b, const float* dinv,
-                       float* r, float* z, float* pv, MixedState* st, double tol2, double atol2, cudaStream_t s) {
+                       float* r, float* z, float* pv, MixedState* st, double tol2, double atol2, cudaStream_t s,
+                       float2* zp = nullptr) {
   with_spmv_cfg(p->spmv_L, p->spmv_U, [&](auto Lc, auto Uc) {
     constexpr int L = decltype(Lc)::value, U = decltype(Uc)::value;
     const int grid = wave_grid(k_true_resid<L, U, INIT>, kThreads, p);
     k_true_resid<L, U, INIT><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
-        p->indptr, p->indices, vals, p->n, x, b, dinv, r, z, pv, p->partials, st, tol2, atol2);
+        p->indptr, p->indices, vals, p->n, x, b, dinv, r, z, pv, p->partials, st, tol2, atol2, zp, p->vstride);
   });
 }
 
-template <int S, int WPB, int WMAX, bool H>
+template <int S, int WPB, int WMAX, int K>
 bool launch_step32_bulk_h(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
                           bool prime) {
-  auto kern = k_step32_bulk<WMAX, S, WPB, H>;
+  auto kern = k_step32_bulk<WMAX, S, WPB, K>;
   constexpr int kSmem = WPB * BulkRing<float, int16_t, WMAX, S>::kWarpBytes;
   static int per_sm = -1;  // per instantiation: opt-in shared memory size + occupancy, queried once
   if (per_sm < 0) {
@@ -727,15 +853,17 @@ bool launch_step32_bulk_h(const femk_plan* p, const float* pv, float* q, MixedSt
   const bool tab = p->sell_cu != nullptr;  // per-slice column tables (shared-offset slices stored once)
   (void)launch_ex(p->pdl != 0, kern, grid, WPB * 32, kSmem, s, (const int64_t*)p->sell_ptr,
                   (const int16_t*)(tab ? p->sell_cu : p->sell_c16), (const float*)p->sell_vals32, p->n, p->n_slices,
-                  pv, q, p->partials, st, (const int64_t*)(tab ? p->sell_cuptr : nullptr));
+                  pv, q, p->partials, st, (const int64_t*)(tab ? p->sell_cuptr : nullptr), (float2*)p->mx_zp,
+                  p->vstride);
   return true;
 }
 
 template <int S, int WPB, int WMAX>
 bool launch_step32_bulk_cfg(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
                             bool prime) {
-  return p->l2_mode32 != 0 ? launch_step32_bulk_h<S, WPB, WMAX, true>(p, pv, q, st, s, prime)
-                           : launch_step32_bulk_h<S, WPB, WMAX, false>(p, pv, q, st, s, prime);
+  if (p->mx_fz_on) return launch_step32_bulk_h<S, WPB, WMAX, 2>(p, pv, q, st, s, prime);
+  return p->l2_mode32 != 0 ? launch_step32_bulk_h<S, WPB, WMAX, 1>(p, pv, q, st, s, prime)
+                           : launch_step32_bulk_h<S, WPB, WMAX, 0>(p, pv, q, st, s, prime);
 }
 
 // bulk-copy FP32 step in the plan's configuration (bulk32_cfg: 10 * stages + warps per block)
@@ -855,6 +983,18 @@ MixedPtrs mixed_ptrs(const femk_plan* p) {
 int enqueue_mixed_chunk(const femk_plan* p, const double* vals, const double* b, double* x, cudaStream_t s) {
   const MixedPtrs m = mixed_ptrs(p);
   const int64_t n = p->n;
+  if (p->mx_fz_on) {  // fused form: step (p formed on the fly) + one update kernel per iteration
+    float2* zp = (float2*)p->mx_zp;
+    for (int it = 0; it < kChunk; ++it) {
+      launch_step32(p, m.pv, m.q, m.st, s);
+      (void)launch_ex(p->pdl != 0, k_update32_fz, vec_grid(k_update32_fz, kThreads, p), kThreads, 0, s, n, m.r,
+                      (const float*)m.q, (const float*)m.d32, m.e, zp, p->vstride, p->partials, m.st);
+    }
+    k_fold<<<::femk::counted_launch() + wave_grid(k_fold, 256, p), 256, 0, s>>>(n, x, m.e, m.st);
+    launch_true_resid<false>(p, vals, x, b, m.d32, m.r, m.z, nullptr, m.st, 0.0, 0.0, s, zp);
+    FEMK_CUDA_TRY(cudaGetLastError());
+    return FEMK_OK;
+  }
   for (int it = 0; it < kChunk; ++it) {
     launch_step32(p, m.pv, m.q, m.st, s);
     if (p->cg_split) {
@@ -903,9 +1043,10 @@ int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double
     set_error("femk_pcg_mixed: workspace missing at graph capture");
     return FEMK_EINVAL;
   }
-  const void* key[4] = {vals, b, x, p->sell_vals32 ? (const void*)p->sell_vals32 : (const void*)p->vals32};
+  const void* key[5] = {vals, b, x, p->sell_vals32 ? (const void*)p->sell_vals32 : (const void*)p->vals32,
+                        (const void*)(uintptr_t)(p->mx_fz_on ? 1 : 0)};
   bool same = p->mx_exec != nullptr;
-  for (int i = 0; i < 4; ++i) same = same && key[i] == p->mx_key[i];
+  for (int i = 0; i < 5; ++i) same = same && key[i] == p->mx_key[i];
   if (same) return FEMK_OK;
   // occupancy queries happen before capture begins
   with_spmv_cfg(p->spmv_L, p->spmv_U, [&](auto Lc, auto Uc) {
@@ -927,6 +1068,7 @@ int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double
   (void)wave_grid(k_pupdate32_x<false>, kThreads, p);
   (void)wave_grid(k_pupdate32<0>, 256, p);
   (void)wave_grid(k_pupdate32<1>, 256, p);
+  (void)wave_grid(k_update32_fz, kThreads, p);
   (void)wave_grid(k_fold, 256, p);
   cudaGraph_t g = nullptr;
   set_capturing(true);
@@ -959,7 +1101,7 @@ int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double
     }
   }
   cudaGraphDestroy(g);
-  for (int i = 0; i < 4; ++i) p->mx_key[i] = key[i];
+  for (int i = 0; i < 5; ++i) p->mx_key[i] = key[i];
   p->mx_nodes = 3 * kChunk + 3;
   return FEMK_OK;
 }
@@ -984,6 +1126,10 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   FEMK_CUDA_TRY(cudaEventRecord(p->mx_ev[2], s));
   FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->mx_ev[2], 0));
   const bool persist = p->cg_persist && p->coop && p->sell_vals32 && p->sell_vals;
+  // the fused form runs on the bulk-copy FP32 step with split updates only
+  p->mx_fz_on = p->mx_fz && !persist && p->cg_split && !(p->tile_ok && p->tile32) &&
+                launch_step32_bulk(p, nullptr, nullptr, nullptr, nullptr, true);
+  if (p->mx_fz_on && !p->mx_zp) FEMK_CUDA_TRY(cudaMalloc(&p->mx_zp, sizeof(float) * 4 * p->vstride));
   if (p->cg_graph && !persist) FEMK_TRY(ensure_mixed_graph(p, vals, b, x));
   if (persist)
     k_gather64<<<::femk::counted_launch() + p->n_sm * 8, 256, 0, ws>>>(p->sell_src, p->sell_nnz, vals, p->sell_vals);
@@ -1003,7 +1149,8 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   init.restart = mode == FEMK_MIXED_RESTART ? 1 : 0;
   FEMK_CUDA_TRY(cudaMemcpyAsync(m.st, &init, sizeof(MixedState), cudaMemcpyHostToDevice, ws));
   const double tol2 = tol * tol, atol2 = atol * atol;
-  launch_true_resid<true>(p, vals, x, b, m.d32, m.r, m.z, m.pv, m.st, tol2, atol2, ws);
+  launch_true_resid<true>(p, vals, x, b, m.d32, m.r, m.z, m.pv, m.st, tol2, atol2, ws,
+                          p->mx_fz_on ? (float2*)p->mx_zp : nullptr);
   FEMK_CUDA_TRY(cudaGetLastError());
   MixedState* hs = (MixedState*)p->mx_host;
   int64_t enq = 0;

@@ -819,7 +819,7 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
                   p->sell_ptr, p->sell_src,  p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32,
                   p->bar,      p->batch_ws,  p->bicg_ws,   p->bicg_state, p->sell_cuptr, p->sell_cu,
                   p->tile_meta, p->tile_slots, p->coef_tmp, p->theta_ws, p->cl_ptr, p->cl_dof, p->cl_loc,
-                  p->cl_off, p->cl_inv};
+                  p->cl_off, p->cl_inv, p->mx_zp};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->state_host) cudaFreeHost(p->state_host);
@@ -885,6 +885,7 @@ extern "C" int femk_plan_create_simplex(const double* coords_dev, int dim, int64
   if (const char* e = std::getenv("FEMK_BULK32")) p->bulk32_cfg = std::atoi(e);
   if (const char* e = std::getenv("FEMK_PDL")) p->pdl = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_VEC_BLOCKS")) p->vec_blocks = std::atoi(e);
+  if (const char* e = std::getenv("FEMK_MIXED_FUSE")) p->mx_fz = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_SELL_UNI")) p->sell_uni = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_TILE")) p->tile_on = std::atoi(e) != 0;
   if (const char* e = std::getenv("FEMK_TILE64")) p->tile64 = std::atoi(e) != 0;

@@ -631,3 +631,25 @@ def test_cluster_staged_matrix_free_matches(n, order, monkeypatch):
     u2, it2, rel2, _ = plan.pcg_matfree(lk, b, inv_diag=inv)
     assert abs(it1 - it2) <= 1 and rel2 <= 2e-8
     assert torch.linalg.norm(u1 - u2) <= 1e-7 * torch.linalg.norm(u1)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_mixed_fused_form_matches_split(mode, monkeypatch):
+    """The fused mixed iteration (FEMK_MIXED_FUSE=1: p formed from (z, p) pairs inside the step,
+    two kernels per iteration) runs the arithmetic of the three-kernel split: same inner and outer
+    counts and the same solution to rounding of the reductions' grid shapes."""
+    pf, cf, tets, p1 = _mesh(24, 1)
+    logk = om.logk_field(len(tets), 1001)
+    out = {}
+    for fuse in ("0", "1"):
+        monkeypatch.setenv("FEMK_MIXED_FUSE", fuse)
+        plan = _plan(p1, tets, 1)
+        vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
+        inv = plan.jacobi(vals)
+        u, inner, outer, rel, st = plan.pcg_mixed(vals, b, inv, tol=1e-8, mode=mode)
+        assert st == 0 and rel <= 1e-8
+        r = b - plan.spmv(vals, u)
+        assert (torch.linalg.norm(r) / torch.linalg.norm(b)).item() <= 1e-8
+        out[fuse] = (u, inner, outer)
+    assert abs(out["0"][1] - out["1"][1]) <= 2 and out["0"][2] == out["1"][2]
+    assert (torch.linalg.norm(out["0"][0] - out["1"][0]) / torch.linalg.norm(out["0"][0])).item() <= 1e-8
