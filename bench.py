@@ -267,8 +267,12 @@ def run_reference(args):
     x, iters, _ = op.pcg(A, sys_full.b, cpu.oa.jacobi_inverse(cpu.oa.matrix_diagonal(sys_full)), tol=1e-8)
     vals, totals = [], []
     desc = ""
-    for i in range(args.warmup + args.steps):
-        v, t, desc = cpu.sample(cpu.fields[0], iters, system=sys_full)
+    # one step is a bounded sample: about 4 s of host work at (1/8 of the tets, 20 PCG iterations),
+    # shrunk for long runs so that the whole --steps/--warmup run stays within a few minutes
+    n_samples = args.warmup + args.steps
+    slab, cg_iters = (8, 20) if n_samples <= 20 else ((16, 12) if n_samples <= 40 else (32, 8))
+    for i in range(n_samples):
+        v, t, desc = cpu.sample(cpu.fields[0], iters, slab_fraction=slab, cg_iters=cg_iters, system=sys_full)
         if i >= args.warmup:
             vals.append(v)
             totals.append(t)
