@@ -480,6 +480,41 @@ def test_spmv_layouts_agree(monkeypatch):
     assert abs(a[3] - c[3]) <= 3 and (torch.linalg.norm(a[2] - c[2]) / torch.linalg.norm(c[2])).item() <= 1e-7
 
 
+def test_canonical_csr_solver_path_matches(monkeypatch):
+    """A plan without the sliced-ELL operator (the path taken when the sliced-ELL entry count passes
+    2^31; forced here with FEMK_SELL=0) runs FP64 PCG and the mixed solver on the canonical-CSR
+    kernels. Its row sums are lane-split shuffle reductions, so it agrees with the sliced-ELL plan to
+    rounding, and both meet the oracle's solution."""
+    pf, cf, tets, p1 = _mesh(32, 1)
+    lk = torch.as_tensor(om.logk_field(len(tets), 1007), device="cuda")
+    for k in ("FEMK_TILE", "FEMK_SELL_UNI", "FEMK_SELL"):
+        monkeypatch.delenv(k, raising=False)
+    sell = _plan(p1, tets, 1)
+    vals, b = sell.assemble(lk)
+    inv = sell.jacobi(vals)
+    u, it, rel, st = sell.pcg(vals, b, inv_diag=inv, tol=1e-8)
+    um, inner, _, relm, stm = sell.pcg_mixed(vals, b, inv, tol=1e-8)
+    monkeypatch.setenv("FEMK_SELL", "0")
+    csr = _plan(p1, tets, 1)
+    uc, itc, relc, stc = csr.pcg(vals, b, inv_diag=inv, tol=1e-8)
+    umc, innerc, _, relmc, stmc = csr.pcg_mixed(vals, b, inv, tol=1e-8)
+    assert st == stm == stc == stmc == 0
+    assert relc <= 2e-8 and relmc <= 1e-8
+    assert abs(itc - it) <= 2 and abs(innerc - inner) <= 10
+    ref = torch.linalg.norm(u)
+    assert (torch.linalg.norm(uc - u) / ref).item() <= 1e-8
+    assert (torch.linalg.norm(umc - um) / ref).item() <= 1e-7
+    import scipy.sparse.linalg as spla
+
+    s = oa.assemble(pf, cf, 1, om.boundary_nodes(cf, 1), np.exp(lk.cpu().numpy()))
+    x_ref = spla.spsolve(s.csr().tocsc(), s.b)
+    assert np.linalg.norm(uc.cpu().numpy() - x_ref) <= 1e-6 * np.linalg.norm(x_ref)
+    from jno_b200._lib import FemkError
+
+    with pytest.raises(FemkError, match="sliced-ELL"):
+        csr.bicgstab(vals, b, inv_diag=inv, tol=1e-8)
+
+
 @pytest.mark.parametrize("mode", ["exp", "linear"])
 def test_nodal_p1_parameter_matches_oracle(mode):
     """A nodal P1 coefficient (jno.np.parameter of a P1 symbol) through assembly, the matrix-free
