@@ -109,15 +109,20 @@ extern "C" int femk_compact(const femk_plan* p, const double* vals, int32_t* ind
   FEMK_CHECK_ARG(vals && indptr_out && nnz_out, "femk_compact: vals, indptr_out and nnz_out are required");
   FEMK_CHECK_ARG(cap >= 0, "femk_compact: cap must be >= 0");
   cudaStream_t s = (cudaStream_t)stream;
-  int64_t* count = nullptr;
-  int64_t* offs = nullptr;
-  FEMK_CUDA_TRY(cudaMallocAsync(&count, sizeof(int64_t) * (p->n > 0 ? p->n : 1), s));
-  cudaError_t e = cudaMallocAsync(&offs, sizeof(int64_t) * (p->n + 1), s);
-  if (e != cudaSuccess) {
-    cudaFreeAsync(count, s);
-    set_error(std::string("femk_compact: ") + cudaGetErrorString(e));
-    return e == cudaErrorMemoryAllocation ? FEMK_ENOMEM : FEMK_ECUDA;
+  // plan-owned scratch (allocated on the first call): a per-call stream-ordered allocation went back
+  // to the driver at the count read's synchronize, and its cost varied between calls
+  femk_plan* pm = const_cast<femk_plan*>(p);
+  if (!pm->cmp_ws) {
+    const cudaError_t ea = cudaMalloc(&pm->cmp_ws, sizeof(int64_t) * (2 * p->n + 2));
+    if (ea != cudaSuccess) {
+      pm->cmp_ws = nullptr;
+      set_error(std::string("femk_compact: ") + cudaGetErrorString(ea));
+      return ea == cudaErrorMemoryAllocation ? FEMK_ENOMEM : FEMK_ECUDA;
+    }
   }
+  int64_t* count = pm->cmp_ws;
+  int64_t* offs = pm->cmp_ws + (p->n > 0 ? p->n : 1);
+  cudaError_t e = cudaSuccess;
   int st = FEMK_OK;
   const int64_t pairs = (p->n + 1) / 2;
   const int grid = blocks_for(pairs * 32, kThreads, p->n_sm * 8);
@@ -157,7 +162,5 @@ extern "C" int femk_compact(const femk_plan* p, const double* vals, int32_t* ind
       st = FEMK_ECUDA;
     }
   }
-  cudaFreeAsync(count, s);
-  cudaFreeAsync(offs, s);
   return st;
 }

@@ -191,6 +191,7 @@ struct femk_plan {
   void* prof = nullptr;         // per-kernel CG timing (femk_set_profiling)
   double* coef_tmp = nullptr;   // f64[ntet] element coefficients of a nodal parameter
   double* theta_ws = nullptr;   // f64[2 vstride] theta march: step Jacobi inverse, step right-hand side
+  int64_t* cmp_ws = nullptr;    // i64[2 n + 2] femk_compact: kept entries per row, then their exclusive scan
   // element clusters of the matrix-free operator (built on first use): distinct DOFs per cluster
   // of 128 consecutive elements and each element's local slots; cl_state 0 unbuilt, 1 ready, -1 off
   int32_t* cl_ptr = nullptr;    // i32[ncl+1]
