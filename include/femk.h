@@ -217,6 +217,22 @@ int femk_bicgstab(const femk_plan* plan, const double* vals_dev, const double* b
                   double* relres_out, void* stream);
 
 /*
+ * Restarted GMRES with jax.scipy.sparse.linalg.gmres semantics (jax 0.10.1, solve_method="batched"):
+ * restart cycles of m = min(restart, n) Arnoldi steps (classical Gram-Schmidt twice, the least
+ * squares by Cholesky of its normal equations), stopping when ||M (b - A x)|| <= ||M b||
+ * min(1, max(tol ||b||, atol) / ||b||) after a cycle, or after maxiter cycles (maxiter <= 0: jax's
+ * default 10 n). M = diag(inv_diag_dev), or the identity when NULL. x holds x0 on entry and the
+ * solution on return. 1 <= restart <= 64. *iters_out = Arnoldi steps, *cycles_out = restart cycles,
+ * *relres_out = ||b - A x|| / (||b|| + 1e-30) (each may be NULL). Returns FEMK_NOT_CONVERGED after
+ * maxiter cycles (x written). The Krylov basis is plan-owned ((restart + 3) vectors, allocated on
+ * first use). Replaces jno.solve.gmres (jno/solve.py:216-221); the theta march's step rescue
+ * (femk_theta_march) runs the same iteration.
+ */
+int femk_gmres(const femk_plan* plan, const double* vals_dev, const double* b_dev, double* x_dev,
+               const double* inv_diag_dev, double tol, double atol, int32_t restart, int64_t maxiter,
+               int32_t* iters_out, int32_t* cycles_out, double* relres_out, void* stream);
+
+/*
  * Consistent mass matrix M[a][b] = integral(phi_a phi_b) in the canonical CSR (vals_dev f64[nnz]).
  * zero_dirichlet != 0 leaves the Dirichlet rows and columns at zero, the transient block's M
  * (bcoo_zero_rows_cols, jno/utils/solver/fem_1d.py:939-949). Replaces the mass jacobian of the
@@ -248,18 +264,24 @@ int femk_assemble_theta(const femk_plan* plan, const double* param_dev, int coef
  *   rhs = rhs_vals u + q;  u <- Jacobi-BiCGStab(step_vals, rhs, x0 = u, tol, atol = 0, maxiter)
  * with the Jacobi inverse of diag(step_vals) (|d| <= 1e-30 -> 1), jax bicgstab semantics as
  * femk_bicgstab. After each step the relative residual ||S u - rhs|| / max(||rhs||, eps) must be
- * below step_check: 1e-9 is the reference's check of its default step solve (tol 1e-10; it
- * re-solves with GMRES otherwise, which is not built here: the march stops with
- * FEMK_NOT_CONVERGED); step_check <= 0 skips the check, as the solver-slot path of
- * compose_transient_step_solvers (jno/utils/solver/solver_api.py:929-945) does. u_dev f64[n] holds the state (in/out);
- * traj_dev f64[nsteps*n] or NULL receives the state after every step; iters_out i32[nsteps] (host)
- * or NULL; *relres_out (host, may be NULL) = the largest step residual. The step operator is
+ * below step_check: 1e-9 is the reference's check of its default step solve (tol 1e-10). A step
+ * that fails it, or whose BiCGStab stopped on its cap, a breakdown or a non-finite value, is
+ * re-solved from x0 = the previous state by the GMRES of femk_gmres with tol = 1e-10, atol = 0,
+ * restart = min(n, 40), the same Jacobi M and jax's default cap of 10 n restart cycles
+ * (backend_blocks.py:402-413); the march stops with FEMK_NOT_CONVERGED only if that GMRES does not
+ * converge. step_check <= 0 skips the check, as the solver-slot path of
+ * compose_transient_step_solvers (jno/utils/solver/solver_api.py:929-945) does; BiCGStab's status
+ * then stands. u_dev f64[n] holds the state (in/out); traj_dev f64[nsteps*n] or NULL receives the
+ * state after every step; iters_out i32[nsteps] (host) or NULL: BiCGStab iterations per step;
+ * gmres_out i32[nsteps] (host) or NULL: the rescue's Arnoldi steps per step (0 when the check
+ * held); *relres_out (host, may be NULL) = the largest BiCGStab step residual. The step operator is
  * gathered into the plan's solver layout once per call: it replaces the operator a previous
  * femk_prepare_operator left there (femk_spmv_prepared then applies S until the next prepare).
  */
 int femk_theta_march(const femk_plan* plan, const double* step_vals_dev, const double* rhs_vals_dev,
                      const double* q_dev, double* u_dev, int32_t nsteps, double tol, int32_t maxiter,
-                     double step_check, double* traj_dev, int32_t* iters_out, double* relres_out, void* stream);
+                     double step_check, double* traj_dev, int32_t* iters_out, int32_t* gmres_out,
+                     double* relres_out, void* stream);
 
 /*
  * Allocation-free Jacobi-PCG: the same iteration and result as femk_pcg, for callers that must

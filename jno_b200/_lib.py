@@ -93,6 +93,8 @@ SIGNATURES = {
     "femk_pcg": [_P, _P, _P, _P, _P, _D, _D, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_D), _P],
     "femk_pcg_noalloc": [_P, _P, _P, _P, _P, _D, _D, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_D), _P],
     "femk_bicgstab": [_P, _P, _P, _P, _P, _D, _D, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_D), _P],
+    "femk_gmres": [_P, _P, _P, _P, _P, _D, _D, _I32, ctypes.c_int64, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
+                   ctypes.POINTER(_D), _P],
     "femk_pcg_matfree": [_P, _P, _I, _D, _P, _P, _P, _D, _D, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_D), _P],
     "femk_pcg_mixed": [_P, _P, _P, _P, _P, _D, _D, _I32, _I, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
                        ctypes.POINTER(_D), _P],
@@ -102,7 +104,7 @@ SIGNATURES = {
     "femk_lumped_mass": [_P, _P, _P],
     "femk_mass_matrix": [_P, _I, _P, _P],
     "femk_assemble_theta": [_P, _P, _I, _D, _D, _P, _D, _D, _I, _P, _P, _P, _P],
-    "femk_theta_march": [_P, _P, _P, _P, _P, _I32, _D, _I32, _D, _P, _P, ctypes.POINTER(_D), _P],
+    "femk_theta_march": [_P, _P, _P, _P, _P, _I32, _D, _I32, _D, _P, _P, _P, ctypes.POINTER(_D), _P],
 }
 
 _lib = None

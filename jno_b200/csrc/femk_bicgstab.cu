@@ -490,8 +490,8 @@ extern "C" int femk_bicgstab(const femk_plan* pc, const double* vals, const doub
 
 extern "C" int femk_theta_march(const femk_plan* pc, const double* step_vals, const double* rhs_vals,
                                 const double* q, double* u, int32_t nsteps, double tol, int32_t maxiter,
-                                double step_check, double* traj, int32_t* iters_out, double* relres_out,
-                                void* stream) {
+                                double step_check, double* traj, int32_t* iters_out, int32_t* gmres_out,
+                                double* relres_out, void* stream) {
   using namespace femk;
   clear_error();
   FEMK_CHECK_ARG(pc && step_vals && rhs_vals && q && u, "femk_theta_march: plan, operators, q and u are required");
@@ -499,9 +499,10 @@ extern "C" int femk_theta_march(const femk_plan* pc, const double* step_vals, co
   femk_plan* p = const_cast<femk_plan*>(pc);
   FEMK_CHECK_ARG(p->use_sell && p->sell_src, "femk_theta_march: the plan has no sliced-ELL operator");
   FEMK_TRY(ensure_bicg(p));
-  if (!p->theta_ws) FEMK_CUDA_TRY(cudaMalloc(&p->theta_ws, sizeof(double) * 2 * p->vstride));
+  if (!p->theta_ws) FEMK_CUDA_TRY(cudaMalloc(&p->theta_ws, sizeof(double) * 3 * p->vstride));
   double* dinv = (double*)p->theta_ws;
   double* rhs = dinv + p->vstride;
+  double* uprev = rhs + p->vstride;  // the state before the step: the GMRES rescue's x0
   cudaStream_t cs = (cudaStream_t)stream;
   cudaStream_t ws = p->bicg_stream;
   FEMK_CUDA_TRY(cudaEventRecord(p->bicg_ev[0], cs));
@@ -517,24 +518,47 @@ extern "C" int femk_theta_march(const femk_plan* pc, const double* step_vals, co
   for (int32_t k = 0; k < nsteps && rc == FEMK_OK; ++k) {
     k_theta_rhs<<<counted_launch() + rgrid, kThreads, 0, ws>>>(p->indptr, p->indices, rhs_vals, u, q, p->n, rhs);
     rc = cudaGetLastError() == cudaSuccess ? FEMK_OK : FEMK_ECUDA;
+    if (rc == FEMK_OK && step_check > 0.0) {
+      const cudaError_t e = cudaMemcpyAsync(uprev, u, sizeof(double) * p->n, cudaMemcpyDeviceToDevice, ws);
+      if (e != cudaSuccess) {
+        set_error(std::string("femk_theta_march: ") + cudaGetErrorString(e));
+        rc = FEMK_ECUDA;
+      }
+    }
     BicgState h;
     if (rc == FEMK_OK) rc = solve_prepared(p, rhs, u, dinv, tol, 0.0, maxiter, ws, &h);
     if (rc != FEMK_OK) break;
     if (iters_out) iters_out[k] = h.iters;
-    rc = solve_status(h, "femk_theta_march");
-    if (rc != FEMK_OK) {
+    if (gmres_out) gmres_out[k] = 0;
+    const int sst = solve_status(h, "femk_theta_march");
+    // the reference ignores the step solve's own status: its step check decides. Without the check
+    // (the solver-slot path) the status stands; a bounded device wait that gave up always does.
+    if (sst == FEMK_TIMEOUT || (sst != FEMK_OK && !(step_check > 0.0))) {
+      rc = sst;
       set_error(std::string(femk_last_error_string()) + " (step " + std::to_string(k) + ")");
       break;
     }
     // the step check of backend_blocks.py:402-413: ||S u - rhs|| / max(||rhs||, eps) below
-    // max(1e-9, 1e4 eps) for the default step solve (the reference re-solves with GMRES otherwise;
-    // here the march stops); step_check <= 0 skips it (the solver-slot path, solver_api.py:929-945)
+    // max(1e-9, 1e4 eps) for the default step solve; a step that fails it (a NaN residual included)
+    // is re-solved from x0 = the previous state by GMRES (tol max(1e-10, 100 eps), restart min(n, 40),
+    // the step's Jacobi M, jax's cap of 10 n restart cycles). step_check <= 0 skips it (the
+    // solver-slot path, solver_api.py:929-945)
     const double rel = std::sqrt(h.ss) / std::max(std::sqrt(h.bb), 2.220446049250313e-16);
-    worst = std::max(worst, rel);
-    if (step_check > 0.0 && !(rel < step_check)) {
-      set_error("femk_theta_march: step " + std::to_string(k) + " left a relative residual of " +
-                std::to_string(rel) + " (>= " + std::to_string(step_check) + ")");
-      rc = FEMK_NOT_CONVERGED;
+    if (std::isfinite(rel)) worst = std::max(worst, rel);
+    if (step_check > 0.0 && (sst != FEMK_OK || !(rel < step_check))) {
+      if (!std::isfinite(rel)) worst = rel;
+      clear_error();
+      FEMK_CUDA_TRY(cudaMemcpyAsync(u, uprev, sizeof(double) * p->n, cudaMemcpyDeviceToDevice, ws));
+      GmresInfo gi;
+      rc = gmres_run(p, true, nullptr, rhs, u, dinv, 1e-10, 0.0, (int)std::min<int64_t>(p->n, 40), 10 * p->n, ws,
+                     &gi);
+      if (gmres_out) gmres_out[k] = (int32_t)std::min<int64_t>(gi.steps, INT32_MAX);
+      if (rc != FEMK_OK) {
+        const std::string why = femk_last_error_string();
+        set_error("femk_theta_march: step " + std::to_string(k) + " failed the residual check (" + std::to_string(rel) +
+                  " >= " + std::to_string(step_check) + ") and its GMRES rescue failed: " + why);
+        break;
+      }
     }
     if (rc != FEMK_OK) break;
     if (traj) {

@@ -190,7 +190,9 @@ struct femk_plan {
   int batch_graph_ok = 1;
   void* prof = nullptr;         // per-kernel CG timing (femk_set_profiling)
   double* coef_tmp = nullptr;   // f64[ntet] element coefficients of a nodal parameter
-  double* theta_ws = nullptr;   // f64[2 vstride] theta march: step Jacobi inverse, step right-hand side
+  double* theta_ws = nullptr;   // f64[3 vstride] theta march: step Jacobi inverse, step right-hand side, previous state
+  double* gm_ws = nullptr;      // GMRES: Krylov basis (restart + 1 vectors), w, q, partials, small arrays
+  int64_t gm_size = 0;          // doubles in gm_ws
   int64_t* cmp_ws = nullptr;    // i64[2 n + 2] femk_compact: kept entries per row, then their exclusive scan
   // element clusters of the matrix-free operator (built on first use): distinct DOFs per cluster
   // of 128 consecutive elements and each element's local slots; cl_state 0 unbuilt, 1 ready, -1 off
@@ -245,6 +247,16 @@ int resolve_coef(const femk_plan* p, const double* param, int mode, cudaStream_t
 int ensure_clusters(femk_plan* p, cudaStream_t s);
 bool launch_matfree_cl(const femk_plan* p, const double* param, int mode, double scale, const double* x, double* y,
                        const CgState* st, cudaStream_t s);
+
+// Restarted GMRES (femk_gmres.cu) on the plan's prepared sliced-ELL operator (sell) or the canonical
+// CSR values; x holds x0 on entry and the solution on return.
+struct GmresInfo {
+  int64_t steps = 0, cycles = 0;  // Arnoldi steps, restart cycles
+  double beta = 0.0;              // final ||M (b - A x)||
+  double rr = 0.0, bb = 0.0;      // final ||b - A x||^2 and ||b||^2
+};
+int gmres_run(femk_plan* p, bool sell, const double* vals, const double* b, double* x, const double* dinv,
+              double tol, double atol, int restart, int64_t maxiter, cudaStream_t s, GmresInfo* info);
 
 // Blocks of `threads` threads of kernel `fn` resident per SM (occupancy), cached per kernel.
 int resident_blocks(const void* fn, int threads);

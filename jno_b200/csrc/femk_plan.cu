@@ -819,7 +819,7 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
                   p->sell_ptr, p->sell_src,  p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32,
                   p->bar,      p->batch_ws,  p->bicg_ws,   p->bicg_state, p->sell_cuptr, p->sell_cu,
                   p->tile_meta, p->tile_slots, p->coef_tmp, p->theta_ws, p->cl_ptr, p->cl_dof, p->cl_loc,
-                  p->cl_off, p->cl_inv, p->mx_zp, p->cmp_ws};
+                  p->cl_off, p->cl_inv, p->mx_zp, p->cmp_ws, p->gm_ws};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->state_host) cudaFreeHost(p->state_host);

@@ -324,14 +324,31 @@ class FemPlan:
         return S, R, q
 
     def theta_march(self, step_vals, rhs_vals, q, u, nsteps, tol=1e-10, maxiter=20_000, traj=None,
-                    step_check=1e-9):
+                    step_check=1e-9, with_rescue=False):
         """Advance u (in place) by nsteps theta steps (Jacobi-BiCGStab per step). Returns (u,
-        iterations i32[nsteps], worst step residual); traj f64[nsteps, n] receives every state when
-        given; a step whose relative residual is not below step_check stops the march (<= 0: none)."""
+        iterations i32[nsteps], worst BiCGStab step residual), plus the GMRES rescue's Arnoldi steps
+        i32[nsteps] when with_rescue; traj f64[nsteps, n] receives every state when given. A step
+        whose relative residual is not below step_check (<= 0: no check) is re-solved by GMRES."""
         it = np.zeros(max(int(nsteps), 1), dtype=np.int32)
+        gm = np.zeros(max(int(nsteps), 1), dtype=np.int32)
         worst = ctypes.c_double(0.0)
         _lib.check(self._lib.femk_theta_march(
             self._h, _lib.ptr(step_vals), _lib.ptr(rhs_vals), _lib.ptr(q), _lib.ptr(u), int(nsteps), float(tol),
-            int(maxiter), float(step_check), _lib.ptr(traj), ctypes.c_void_p(it.ctypes.data), ctypes.byref(worst),
-            _lib.stream_handle()))
+            int(maxiter), float(step_check), _lib.ptr(traj), ctypes.c_void_p(it.ctypes.data),
+            ctypes.c_void_p(gm.ctypes.data), ctypes.byref(worst), _lib.stream_handle()))
+        if with_rescue:
+            return u, it[: int(nsteps)], worst.value, gm[: int(nsteps)]
         return u, it[: int(nsteps)], worst.value
+
+    def gmres(self, vals, b, x=None, inv_diag=None, tol=1e-8, atol=0.0, restart=30, maxiter=None):
+        """Restarted Jacobi-GMRES (jax gmres, solve_method="batched"). Returns (x, Arnoldi steps,
+        restart cycles, relres, status); maxiter None is jax's 10 n restart cycles."""
+        x = torch.zeros(self.n, dtype=torch.float64, device=self.device) if x is None else x
+        it = ctypes.c_int32(0)
+        cyc = ctypes.c_int32(0)
+        rr = ctypes.c_double(float("nan"))
+        st = self._lib.femk_gmres(self._h, _lib.ptr(vals), _lib.ptr(b), _lib.ptr(x), _lib.ptr(inv_diag), float(tol),
+                                  float(atol), int(restart), 0 if maxiter is None else int(maxiter), ctypes.byref(it),
+                                  ctypes.byref(cyc), ctypes.byref(rr), _lib.stream_handle())
+        _lib.check(st, allow=(_lib.FEMK_NOT_CONVERGED,))
+        return x, it.value, cyc.value, rr.value, st

@@ -7,7 +7,9 @@ preconditioner (<r, z> without one) or at maxiter. After the solve the eager res
 ``_maybe_residual_check`` (solver_api.py:224-240) raises ``RuntimeError`` when
 ``||b - A x|| / (||b|| + 1e-30) > 1e-4``.
 
-``bicgstab(tol, atol, maxiter)`` is ``jax.scipy.sparse.linalg.bicgstab`` on the same operator.
+``bicgstab(tol, atol, maxiter)`` is ``jax.scipy.sparse.linalg.bicgstab`` on the same operator, and
+``gmres(tol, atol, maxiter=None, restart=30)`` is ``jax.scipy.sparse.linalg.gmres`` (restarted,
+``solve_method="batched"``).
 
 Extensions with no reference counterpart: ``precision="mixed"`` (FP32 inner CG with FP64 reliable
 updates, ``refine="reliable"`` or classic restarted refinement ``refine="restart"``) and matrix-free
@@ -100,6 +102,12 @@ class LinearSolver:
                 raise TypeError("the B200 BiCGStab takes an assembled CsrMatrix")
             x, it, rel, st = plan.bicgstab(op.solver_values, b, x, inv, self.tol, self.atol, self.maxiter)
             self.last_info = SolveInfo(it, rel, st)
+        elif self.name == "gmres":
+            if not isinstance(op, CsrMatrix):
+                raise TypeError("the B200 GMRES takes an assembled CsrMatrix")
+            x, it, cyc, rel, st = plan.gmres(op.solver_values, b, x, inv, self.tol, self.atol, self.restart,
+                                             self.gmres_maxiter)
+            self.last_info = SolveInfo(it, rel, st, outer=cyc)
         elif isinstance(op, MatrixFreeOperator):
             x, it, rel, st = plan.pcg_matfree(op.param, b, x, inv, op.mode, op.scale, self.tol, self.atol,
                                               self.maxiter)
@@ -119,6 +127,17 @@ class LinearSolver:
 def cg(*, tol=1e-8, atol=0.0, maxiter=20_000, precision="fp64", refine="reliable", mixed_maxiter=None):
     """Jacobi-preconditionable CG on the B200 kernels (``jax.scipy.sparse.linalg.cg`` semantics)."""
     return LinearSolver(tol, atol, maxiter, precision, refine, mixed_maxiter=mixed_maxiter)
+
+
+def gmres(*, tol=1e-8, atol=0.0, maxiter=None, restart=30):
+    """Restarted GMRES on the B200 kernels (``jax.scipy.sparse.linalg.gmres`` with
+    ``solve_method="batched"``, jno/solve.py:216-221): ``maxiter`` counts restart cycles (None: jax's
+    10 n); ``last_info.iterations`` = Arnoldi steps, ``last_info.outer`` = cycles."""
+    s = LinearSolver(tol, atol, 20_000, name="gmres")
+    s.restart = int(restart)
+    s.gmres_maxiter = None if maxiter is None else int(maxiter)
+    s.key = s.key + (("gmres", s.restart, s.gmres_maxiter),)
+    return s
 
 
 def bicgstab(*, tol=1e-8, atol=0.0, maxiter=20_000):

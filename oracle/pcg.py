@@ -113,6 +113,83 @@ def bicgstab(A, b, inv_diag=None, x0=None, tol=1e-8, atol=0.0, maxiter=20_000):
     return x, k
 
 
+def _safe_normalize(v, thresh=None):
+    """(v / ||v||, ||v||), or (0, 0) when ||v|| <= thresh (default: machine epsilon, absolute)."""
+    nrm = float(np.linalg.norm(v))
+    t = np.finfo(np.float64).eps if thresh is None else thresh
+    if nrm > t:
+        return v / nrm, nrm
+    return np.zeros_like(v), 0.0
+
+
+def gmres(A, b, inv_diag=None, x0=None, tol=1e-8, atol=0.0, restart=20, maxiter=None):
+    """``jax.scipy.sparse.linalg.gmres`` with ``solve_method="batched"`` (jax 0.10.1), called by
+    ``jno.solve.gmres`` (``jno/solve.py:216-221``, default ``restart=30``) and by the rescue of a
+    failed theta step (``jno/utils/solver/backend_blocks.py:402-413``: ``restart=min(n, 40)``,
+    ``tol=max(1e-10, 100 eps)``). Its published algorithm, restated (M = the preconditioner):
+
+        m = min(restart, n);  maxiter = 10 n if None
+        atol' = max(tol ||b||, atol);  ptol = ||M b|| min(1, atol' / ||b||)
+        w, beta = normalize(M (b - A x0));  k = 0
+        while beta > ptol and k < maxiter:                      # one restart cycle per pass
+            V[:, 0] = w;  H = eye(m, m + 1)                   # row j of H = column j of the Hessenberg
+            for j in 0 .. m-1 (until breakdown):
+                v = M A V[:, j];  v0 = ||v||
+                classical Gram-Schmidt of v against V, twice ("twice is enough"; once if v0 = 0):
+                    h = V^T v;  v -= V h;  accumulate h
+                V[:, j+1], h[j+1] = normalize(v, threshold eps * v0);  H[j, :] = h
+                breakdown = h[j+1] == 0
+            y = solve(H H^T, H e1 beta) by Cholesky           # the normal equations of min ||H^T y - beta e1||
+            x = x + V[:, :m] y;  w, beta = normalize(M (b - A x));  k += 1
+
+    normalize(v, t) returns (v / ||v||, ||v||) when ||v|| > t (default t = eps), else (0, 0). The
+    stop test is on the preconditioned residual, checked once per restart cycle. Returns
+    (x, Arnoldi steps, restart cycles, final beta)."""
+    import scipy.linalg as sla
+
+    b = np.asarray(b, dtype=np.float64)
+    n = b.shape[0]
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
+
+    def M(v):
+        return v if inv_diag is None else inv_diag * v
+
+    m = min(int(restart), n)
+    maxiter = 10 * n if maxiter is None else int(maxiter)
+    eps = np.finfo(np.float64).eps
+    b_norm = float(np.linalg.norm(b))
+    atol_ = max(tol * b_norm, atol)
+    Mb_norm = float(np.linalg.norm(M(b)))
+    ptol = Mb_norm * min(1.0, atol_ / b_norm) if b_norm > 0 else 0.0
+    w, beta = _safe_normalize(M(b - A @ x))
+    steps = cycles = 0
+    while beta > ptol and cycles < maxiter:
+        V = np.zeros((n, m + 1))
+        V[:, 0] = w
+        H = np.eye(m, m + 1)
+        for j in range(m):
+            v = M(A @ V[:, j])
+            _, v0 = _safe_normalize(v)
+            h = np.zeros(m + 1)
+            for _ in range(2 if v0 > 0 else 1):
+                hj = V.T @ v
+                v = v - V @ hj
+                h += hj
+            unit, h[j + 1] = _safe_normalize(v, eps * v0)
+            V[:, j + 1] = unit
+            H[j, :] = h
+            steps += 1
+            if h[j + 1] == 0.0:
+                break
+        e1 = np.zeros(m + 1)
+        e1[0] = beta
+        y = sla.cho_solve(sla.cho_factor(H @ H.T), H @ e1)
+        x = x + V[:, :m] @ y
+        w, beta = _safe_normalize(M(b - A @ x))
+        cycles += 1
+    return x, steps, cycles, beta
+
+
 def residual_check(A, b, x, rtol=1e-4):
     """Relative true residual; raises RuntimeError like ``_maybe_residual_check``."""
     rel = float(np.linalg.norm(b - A @ x) / (np.linalg.norm(b) + 1e-30))

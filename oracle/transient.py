@@ -15,7 +15,9 @@ Restates, with the reference's separate operators applied one product at a time:
   ``rhs = M u - (1 - theta) dt (A u) + dt c + dt f``, ``step(w) = M w + theta dt (A w)``,
   ``inv = 1 / where(|d| > 1e-30, d, 1)`` with ``d = diag(M) + theta dt diag(A)``, then
   ``jax.scipy.sparse.linalg.bicgstab(step, rhs, x0=u, tol=1e-10, atol=0, maxiter=20000, M=inv)``
-  and the step check ``||step(u') - rhs|| / max(||rhs||, eps) < max(1e-9, 1e4 eps)``;
+  and the step check ``||step(u') - rhs|| / max(||rhs||, eps) < max(1e-9, 1e4 eps)``; a step that
+  fails it is re-solved from ``x0 = u`` by ``jax.scipy.sparse.linalg.gmres`` (``tol=max(1e-10,
+  100 eps)``, ``atol=0``, ``restart=min(n, 40)``, the same Jacobi ``M``; ``backend_blocks.py:402-413``);
 * ``_default_transient_integrate`` (``backend_blocks.py:475-530``): the grid of ``n_steps`` points
   from ``t0`` to ``t1`` (``_infer_time_window``, ``jno/utils/solver/time_route.py:32-58``,
   ``dt = (t1 - t0) / (n_steps - 1)``), trajectory = state0 followed by every step.
@@ -27,7 +29,7 @@ import scipy.sparse.linalg as spla
 
 from .assemble import assemble, compress_plan, plan_to_csr
 from .element import _collapsed_gauss, _collapsed_gauss_tri, _ref_basis, vertices
-from .pcg import bicgstab
+from .pcg import bicgstab, gmres
 
 
 def mass_matrices(X, order, npts=5):
@@ -85,8 +87,10 @@ def block(points, cells, order, dirichlet, coef, f=1.0, g=None, parametric=True)
     return Block(M, A, c, load)
 
 
-def step(blk, u, dt, theta=1.0, tol=1e-10, maxiter=20_000):
-    """One theta step; returns (u_next, bicgstab iteration count k, step residual)."""
+def step(blk, u, dt, theta=1.0, tol=1e-10, maxiter=20_000, info=None):
+    """One theta step; returns (u_next, bicgstab iteration count k, step residual). The step
+    residual is BiCGStab's; when it fails the check the GMRES rescue runs, and ``info`` (a dict,
+    optional) receives its Arnoldi steps and the rescued solution's residual."""
     M, A = blk.M, blk.A
     rhs = M @ u - (1.0 - theta) * dt * (A @ u) + dt * blk.c + dt * blk.f
     n = u.shape[0]
@@ -96,15 +100,20 @@ def step(blk, u, dt, theta=1.0, tol=1e-10, maxiter=20_000):
     wn, k = bicgstab(op, rhs, inv, x0=u, tol=tol, atol=0.0, maxiter=maxiter)
     eps = np.finfo(np.float64).eps
     r_rel = float(np.linalg.norm(op @ wn - rhs) / max(np.linalg.norm(rhs), eps))
+    if not (r_rel < max(1e-9, 1e4 * eps)):
+        wn, steps, _, _ = gmres(op, rhs, inv, x0=u, tol=max(1e-10, 100.0 * eps), atol=0.0, restart=min(n, 40))
+        if info is not None:
+            info["gmres_steps"] = info.get("gmres_steps", 0) + steps
+            info["rescued_residual"] = float(np.linalg.norm(op @ wn - rhs) / max(np.linalg.norm(rhs), eps))
     return wn, k, r_rel
 
 
-def march(blk, u0, dt, nsteps, theta=1.0, tol=1e-10):
-    """Trajectory f64[nsteps + 1, n] (state0 first), iteration counts, worst step residual."""
+def march(blk, u0, dt, nsteps, theta=1.0, tol=1e-10, maxiter=20_000, info=None):
+    """Trajectory f64[nsteps + 1, n] (state0 first), iteration counts, worst BiCGStab step residual."""
     u = np.array(u0, dtype=np.float64)
     traj, iters, worst = [u.copy()], [], 0.0
     for _ in range(nsteps):
-        u, k, r = step(blk, u, dt, theta, tol)
+        u, k, r = step(blk, u, dt, theta, tol, maxiter, info)
         traj.append(u.copy())
         iters.append(k)
         worst = max(worst, r)

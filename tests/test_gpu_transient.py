@@ -114,9 +114,12 @@ def test_march_status_paths():
     with pytest.raises(_lib.FemkError):
         plan.assemble_theta(lk, theta=1.0, dt=-1.0)
     S, R, q = plan.assemble_theta(lk, theta=1.0, dt=0.01)
+    with pytest.raises(_lib.FemkError, match="nsteps"):
+        plan.theta_march(S, R, q, torch.zeros(plan.n, dtype=torch.float64, device="cuda"), -1)
+    # the solver-slot path (no step check) keeps BiCGStab's own status: a capped step stops the march
     u = torch.as_tensor(np.sin(np.pi * pf[:, 0]), device="cuda").clone()
     with pytest.raises(_lib.FemkError, match="step 0"):
-        plan.theta_march(S, R, q, u, 3, maxiter=1)
+        plan.theta_march(S, R, q, u, 3, maxiter=1, step_check=0.0)
     u2 = torch.zeros(plan.n, dtype=torch.float64, device="cuda")
     _, iters, worst = plan.theta_march(S, R, q, u2, 0)
     assert iters.size == 0 and worst == 0.0

@@ -187,6 +187,37 @@ def test_bicgstab_matches_direct_and_stops_like_jax():
     assert k1 == 1
 
 
+def test_gmres_restatement_converges_restarts_and_breaks_down():
+    """The restated jax gmres: one long cycle and many short restart cycles reach the direct
+    solution; a non-symmetric system converges; a Krylov space that closes early (a diagonal with
+    three distinct values) breaks down after three steps with the exact answer; b = 0 runs no cycle."""
+    import scipy.sparse as sp
+
+    n = 6
+    pts, tets = om.equi_distant_box(n, n, n)
+    pts = om.jitter_interior(pts, n, n, n, seed=1)
+    s = oa.assemble(pts, tets, 1, om.boundary_nodes(tets, 1), np.exp(om.logk_field(len(tets), 3)))
+    A = s.csr()
+    inv = oa.jacobi_inverse(oa.matrix_diagonal(s))
+    xd = _solve_direct(s)
+    for restart, cycles_at_least in ((30, 1), (5, 5)):
+        x, steps, cycles, _ = op.gmres(A, s.b, inv, tol=1e-10, restart=restart)
+        assert cycles >= cycles_at_least and steps <= cycles * restart
+        assert np.linalg.norm(x - xd) <= 1e-8 * np.linalg.norm(xd)
+    skew = sp.random(A.shape[0], A.shape[0], density=5.0 / A.shape[0], random_state=1)
+    B = (A + 0.05 * (skew - skew.T)).tocsr()
+    import scipy.sparse.linalg as spla
+
+    xb = spla.spsolve(B.tocsc(), s.b)
+    x, _, _, _ = op.gmres(B, s.b, inv, tol=1e-10, restart=30)
+    assert np.linalg.norm(x - xb) <= 1e-8 * np.linalg.norm(xb)
+    D = sp.diags(np.repeat([1.0, 2.0, 5.0], 10)).tocsr()
+    x, steps, cycles, beta = op.gmres(D, np.ones(30), None, tol=1e-12, restart=20)
+    assert steps == 3 and cycles == 1 and np.abs(D @ x - 1.0).max() <= 1e-14
+    x0, steps0, cycles0, _ = op.gmres(A, np.zeros_like(s.b), inv)
+    assert steps0 == 0 and cycles0 == 0 and np.all(x0 == 0)
+
+
 def test_nodal_coefficient_rule():
     """The 4-point rule integrates degree-2 polynomials exactly; a linear nodal field's element
     mean is its vertex mean; a constant log-field gives exp of it."""

@@ -77,6 +77,19 @@ def test_long_march_reaches_the_steady_solution():
         assert np.abs(traj[-1] - steady).max() <= 1e-8 * np.abs(steady).max()
 
 
+def test_failed_step_check_is_rescued_by_gmres():
+    """A BiCGStab capped at one iteration fails every step check; the GMRES rescue
+    (backend_blocks.py:402-413) re-solves each step and the march lands on the uncapped one."""
+    pf, cf, bnd, u0 = _heat_2d(8, 1, seed=2)
+    blk = ot.block(pf, cf, 1, bnd, np.exp(om.logk_field(len(cf), 3)), f=1.0)
+    info = {}
+    a, it, worst = ot.march(blk, u0, 0.01, 3, maxiter=1, info=info)
+    b = ot.march(blk, u0, 0.01, 3)[0]
+    assert np.all(it == 1) and worst > 1e-9
+    assert info["gmres_steps"] > 0 and info["rescued_residual"] <= 1e-12
+    assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max()
+
+
 def test_routes_agree_for_homogeneous_dirichlet_and_differ_in_the_held_rows():
     """With g = 0 and u0 = 0 on the boundary both Dirichlet routes give the same trajectory; with
     theta = 1/2 and u0 != g on the boundary the parametric route's held rows follow
