@@ -750,15 +750,7 @@ def run_ours(args):
             "err_vs_fp64_tight": err}
         # the plain FP64 method: the same assemble + Jacobi-PCG with every CG-step SpMV on the
         # canonical CSR kernel (no sliced-ELL operator), on a second plan of the same mesh
-        prev = os.environ.get("FEMK_SELL")
-        os.environ["FEMK_SELL"] = "0"
-        try:
-            plan_csr = FemPlan(pts, tets, args.order)
-        finally:
-            if prev is None:
-                os.environ.pop("FEMK_SELL")
-            else:
-                os.environ["FEMK_SELL"] = prev
+        plan_csr = FemPlan(pts, tets, args.order, options={"solver_layout": 0})
         csr_info = {}
 
         def cstep(i):

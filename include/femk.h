@@ -61,7 +61,6 @@ typedef struct femk_plan_info {
   int32_t device;
   int64_t sell_nnz;   /* stored entries of the solver's sliced-ELL copy (padding included), 0 if none */
   int32_t batch_graph; /* 1 when the last femk_pcg_batched ran as a replayed CUDA graph */
-  int32_t tiles;       /* 1 when the plan built the staged-x tiles of the CG-step SpMV */
   int64_t sell_col_units; /* column entries the CG-step SpMV streams per product (int16 units when
                              cols16: per-slice tables, a shared-offset slice stored once) */
   int32_t dim;            /* 2 (triangles) or 3 (tetrahedra) */
@@ -106,6 +105,46 @@ int femk_plan_create(const double* xyz_dev, int64_t nvert, const int32_t* tets_d
 int femk_plan_create_simplex(const double* coords_dev, int dim, int64_t nvert, const int32_t* cells_dev,
                              int64_t ncell, int order, const uint8_t* dirichlet_mask_dev, void* stream,
                              femk_plan** out);
+
+/*
+ * Per-plan layout and tuning options of femk_plan_create_ex. femk_plan_options_default fills in the
+ * defaults, which are what femk_plan_create / femk_plan_create_simplex use; the library reads no
+ * environment variables. Layout options act when the plan is built; the others on every call that
+ * uses the plan. Every field is validated at creation (FEMK_EINVAL for an unknown value). No
+ * reference counterpart (jNO's assembly and solver have no such knobs).
+ */
+typedef struct femk_plan_options {
+  int32_t size;           /* sizeof(femk_plan_options): set by femk_plan_options_default */
+  int32_t solver_layout;  /* 1 (default): the CG loops multiply with a sliced-ELL (SELL-32) copy of the
+                             operator; 0: with the canonical CSR itself (the plain method) */
+  int32_t column_tables;  /* 1 (default): a slice whose 32 rows share one column-offset sequence stores it once */
+  int32_t cols16;         /* 1 (default): int16 column offsets in the FP64 sliced-ELL stream when they fit */
+  int32_t graph_replay;   /* 1 (default): CG / mixed chunks replayed as CUDA graphs; 0: launched one by one */
+  int32_t l2_hints;       /* L2 eviction hints of the FP64 CG kernels: -1 (default) on for P1, off for P2;
+                             0 off; 1 matrix evict-first, gathers and vectors evict-last; 2 matrix evict-first,
+                             vectors evict-last; 3 vectors evict-last only; 4 as 1 with streaming matrix loads */
+  int32_t ring64;         /* bulk-copy ring of the FP64 CG-step SpMV, 10 * stages + warps per block (14, 18,
+                             24, 28, 38); -1 (default): 14, 28 for rows of at most 8 entries; 0: thread-per-row kernel */
+  int32_t ring32;         /* the same for the FP32 step of femk_pcg_mixed; -1 (default): 28 */
+  int32_t csr_lanes;      /* CSR SpMV lanes per row (4, 8, 16, 32); 0 (default): from the mean row length */
+  int32_t csr_rows;       /* CSR rows in flight per lane group (1, 2, 4); 0 (default): with csr_lanes */
+  int32_t sell_batch;     /* entries in flight per thread of the thread-per-row FP64 kernel: 8 or 16 (default) */
+  int32_t vec_blocks;     /* blocks per SM of the FP64 CG vector kernels; 0 (default): one full wave */
+  int32_t split_updates;  /* 1 (default): FP64 CG vector updates as r-update + direction/x-update kernels */
+  int32_t test_skip_arrival; /* testing the bounded waits: the block with this index skips its first
+                                grid-barrier arrival in femk_pcg_batched*, so every other block waits out
+                                barrier_limit_ms and the call returns FEMK_TIMEOUT; -1 (default): none */
+  double mixed_delta2;    /* reliable update of the mixed solvers once <r, r> fell by this factor; 0 (default): 1e-4 */
+  double barrier_limit_ms; /* limit of each grid-barrier wait of femk_pcg_batched*, in milliseconds at the
+                              maximum SM clock; 0 (default): 2000 */
+} femk_plan_options;
+
+void femk_plan_options_default(femk_plan_options* opts);
+
+/* femk_plan_create_simplex with explicit options (NULL = the defaults). */
+int femk_plan_create_ex(const double* coords_dev, int dim, int64_t nvert, const int32_t* cells_dev, int64_t ncell,
+                        int order, const uint8_t* dirichlet_mask_dev, const femk_plan_options* opts, void* stream,
+                        femk_plan** out);
 
 int femk_plan_destroy(femk_plan* plan);
 
@@ -218,10 +257,10 @@ int femk_bicgstab(const femk_plan* plan, const double* vals_dev, const double* b
 
 /*
  * Restarted GMRES with jax.scipy.sparse.linalg.gmres semantics (jax 0.10.1, solve_method="batched"):
- * restart cycles of m = min(restart, n) Arnoldi steps (classical Gram-Schmidt twice, the least
+ * restart cycles of m = min(restart, n) Arnoldi steps (one classical Gram-Schmidt pass, the least
  * squares by Cholesky of its normal equations), stopping when ||M (b - A x)|| <= ||M b||
- * min(1, max(tol ||b||, atol) / ||b||) after a cycle, or after maxiter cycles (maxiter <= 0: jax's
- * default 10 n). M = diag(inv_diag_dev), or the identity when NULL. x holds x0 on entry and the
+ * min(1, max(tol ||b||, atol) / ||b||) after a cycle, or after maxiter cycles (maxiter < 0: jax's
+ * default 10 n; 0: no cycle). M = diag(inv_diag_dev), or the identity when NULL. x holds x0 on entry and the
  * solution on return. 1 <= restart <= 64. *iters_out = Arnoldi steps, *cycles_out = restart cycles,
  * *relres_out = ||b - A x|| / (||b|| + 1e-30) (each may be NULL). Returns FEMK_NOT_CONVERGED after
  * maxiter cycles (x written). The Krylov basis is plan-owned ((restart + 3) vectors, allocated on

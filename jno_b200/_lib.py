@@ -57,9 +57,31 @@ class PlanInfo(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("sell_nnz", ctypes.c_int64),
         ("batch_graph", ctypes.c_int32),
-        ("tiles", ctypes.c_int32),
         ("sell_col_units", ctypes.c_int64),
         ("dim", ctypes.c_int32),
+    ]
+
+
+class PlanOptions(ctypes.Structure):
+    """``femk_plan_options`` (include/femk.h): per-plan layout and tuning options."""
+
+    _fields_ = [
+        ("size", ctypes.c_int32),
+        ("solver_layout", ctypes.c_int32),
+        ("column_tables", ctypes.c_int32),
+        ("cols16", ctypes.c_int32),
+        ("graph_replay", ctypes.c_int32),
+        ("l2_hints", ctypes.c_int32),
+        ("ring64", ctypes.c_int32),
+        ("ring32", ctypes.c_int32),
+        ("csr_lanes", ctypes.c_int32),
+        ("csr_rows", ctypes.c_int32),
+        ("sell_batch", ctypes.c_int32),
+        ("vec_blocks", ctypes.c_int32),
+        ("split_updates", ctypes.c_int32),
+        ("test_skip_arrival", ctypes.c_int32),
+        ("mixed_delta2", ctypes.c_double),
+        ("barrier_limit_ms", ctypes.c_double),
     ]
 
 
@@ -76,6 +98,8 @@ SIGNATURES = {
     "femk_last_error_string": [],
     "femk_plan_create": [_P, _I64, _P, _I64, _I, _P, _P, ctypes.POINTER(_P)],
     "femk_plan_create_simplex": [_P, _I, _I64, _P, _I64, _I, _P, _P, ctypes.POINTER(_P)],
+    "femk_plan_options_default": [_P],
+    "femk_plan_create_ex": [_P, _I, _I64, _P, _I64, _I, _P, _P, _P, ctypes.POINTER(_P)],
     "femk_plan_destroy": [_P],
     "femk_plan_get_info": [_P, ctypes.POINTER(PlanInfo)],
     "femk_plan_export": [_P, _P, _P, _P, _P, _P, _P, _P, _P],
@@ -126,8 +150,8 @@ def load():
         for name, args in SIGNATURES.items():
             fn = getattr(lib, name)
             fn.argtypes = args
-            fn.restype = {"femk_last_error_string": ctypes.c_char_p, "femk_kernel_launches": ctypes.c_int64}.get(
-                name, ctypes.c_int)
+            fn.restype = {"femk_last_error_string": ctypes.c_char_p, "femk_kernel_launches": ctypes.c_int64,
+                          "femk_plan_options_default": None}.get(name, ctypes.c_int)
         _lib = lib
         return lib
 

@@ -72,6 +72,8 @@ struct BatchArgs {
   int32_t* status;
   int32_t* active;
   GridBar* bar;
+  long long spin;  // clock64 budget of each grid-barrier wait
+  int32_t skip;    // testing: block that skips its first barrier arrival (-1: none)
 };
 
 // One warp computes (A v)[row] for the rows of its tile; the epilogue functor sees (row, Av).
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
     });
     tile_partial<3>(acc, a.P, a.ntiles, t, 0);
   }
-  if (!grid_sync(a.bar, gen)) return;
+  if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   FEMK_OWNER_LOOP {
     const double rz = prob_sum(a, 0, k), rr = prob_sum(a, 1, k), bb = prob_sum(a, 2, k);
     if (threadIdx.x == 0) {
@@ -192,7 +194,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
         retire(a, k, FEMK_OK);
     }
   }
-  if (!grid_sync(a.bar, gen)) return;
+  if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   double* alpha = a.gam + a.nprob;  // per-problem step scalars of the current iteration
   double* beta = alpha;             // (alpha is dead once phase 2 is done; beta reuses the slot)
   while (ld_acquire_u32((const unsigned int*)a.active) != 0u) {
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
       });
       tile_partial<1>(acc, a.P, a.ntiles, t, 3);
     }
-    if (!grid_sync(a.bar, gen)) return;
+    if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
       if (block_done(a.done, k)) continue;
       const double pq = prob_sum(a, 3, k);
@@ -218,7 +220,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
           alpha[k] = a.gam[k] / pq;
       }
     }
-    if (!grid_sync(a.bar, gen)) return;
+    if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     // ---- phase 2: x, r, z updates; <r, z>, <r, r>
     for (int32_t t = gw; t < a.ntiles; t += NW) {
       const int32_t k = a.tile_prob[t];
@@ -236,7 +238,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
       }
       tile_partial<2>(acc, a.P, a.ntiles, t, 4);
     }
-    if (!grid_sync(a.bar, gen)) return;
+    if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
       if (block_done(a.done, k)) continue;
       const double rz = prob_sum(a, 4, k), rr = prob_sum(a, 5, k);
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
         if (!finite || !(rs > a.atol2[k]) || itk >= a.maxiter) retire(a, k, finite ? FEMK_OK : FEMK_NONFINITE);
       }
     }
-    if (!grid_sync(a.bar, gen)) return;
+    if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     // ---- phase 3: p = z + beta p
     for (int32_t t = gw; t < a.ntiles; t += NW) {
       const int32_t k = a.tile_prob[t];
@@ -260,7 +262,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
       for (int32_t i = a.tile_r0[t] + lane; i < a.tile_r1[t]; i += 32)
         a.p[i] = __ldcg(a.z + i) + be * __ldcg(a.p + i);
     }
-    if (!grid_sync(a.bar, gen)) return;
+    if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   }
   // ---- phase R: per-problem ||b - A x||, ||b||
   for (int32_t t = gw; t < a.ntiles; t += NW) {
@@ -273,7 +275,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
     });
     tile_partial<2>(acc, a.P, a.ntiles, t, 5);
   }
-  if (!grid_sync(a.bar, gen)) return;
+  if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   FEMK_OWNER_LOOP {
     const double ww = prob_sum(a, 5, k), bb = prob_sum(a, 6, k);
     if (threadIdx.x == 0) a.relres[k] = sqrt(ww) / (sqrt(bb) + 1e-30);
@@ -304,7 +306,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
     });
     tile_partial<3>(acc, a.P, a.ntiles, t, 0);
   }
-  if (!grid_sync(a.bar, gen)) return;
+  if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   FEMK_OWNER_LOOP {
     const double rz = prob_sum(a, 0, k), rr = prob_sum(a, 1, k), bb = prob_sum(a, 2, k);
     if (threadIdx.x == 0) {
@@ -323,7 +325,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) *a.any_upd = 0;
-  if (!grid_sync(a.bar, gen)) return;
+  if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   double* alpha = a.gam + a.nprob;
   double* beta = alpha;
   while (ld_acquire_u32((const unsigned int*)a.active) != 0u) {
@@ -338,7 +340,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
       });
       tile_partial<1>(acc, a.P, a.ntiles, t, 3);
     }
-    if (!grid_sync(a.bar, gen)) return;
+    if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
       if (block_done(a.done, k)) continue;
       const double pq = prob_sum(a, 3, k);
@@ -349,7 +351,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
           alpha[k] = a.gam[k] / pq;
       }
     }
-    if (!grid_sync(a.bar, gen)) return;
+    if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     // ---- phase 2: x += alpha p (FP64), r -= alpha q, z = D^-1 r (FP32); <r, z>, <r, r>
     for (int32_t t = gw; t < a.ntiles; t += NW) {
       const int32_t k = a.tile_prob[t];
@@ -369,7 +371,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
       }
       tile_partial<2>(acc, a.P, a.ntiles, t, 4);
     }
-    if (!grid_sync(a.bar, gen)) return;
+    if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
       if (block_done(a.done, k)) continue;
       const double rz = prob_sum(a, 4, k), rr = prob_sum(a, 5, k);
@@ -388,7 +390,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
         }
       }
     }
-    if (!grid_sync(a.bar, gen)) return;
+    if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     if (__ldcg(a.any_upd)) {
       // ---- phase U: r = fp32(b - A64 x), z = D^-1 r for the problems that asked; <r, z>, <r64, r64>
       for (int32_t t = gw; t < a.ntiles; t += NW) {
@@ -408,7 +410,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
         });
         tile_partial<2>(acc, a.P, a.ntiles, t, 4);
       }
-      if (!grid_sync(a.bar, gen)) return;
+      if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
       FEMK_OWNER_LOOP {
         if (block_done(a.done, k)) continue;
         __shared__ int32_t uk;
@@ -434,7 +436,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
         }
       }
       if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.any_upd, 0);
-      if (!grid_sync(a.bar, gen)) return;
+      if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     }
     // ---- phase 3: p = z + beta p
     for (int32_t t = gw; t < a.ntiles; t += NW) {
@@ -444,7 +446,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
       for (int32_t i = a.tile_r0[t] + lane; i < a.tile_r1[t]; i += 32)
         a.p32[i] = fmaf(be, __ldcg(a.p32 + i), __ldcg(a.z32 + i));
     }
-    if (!grid_sync(a.bar, gen)) return;
+    if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   }
   // ---- phase R: per-problem ||b - A x||, ||b|| (FP64)
   for (int32_t t = gw; t < a.ntiles; t += NW) {
@@ -457,7 +459,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
     });
     tile_partial<2>(acc, a.P, a.ntiles, t, 5);
   }
-  if (!grid_sync(a.bar, gen)) return;
+  if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   FEMK_OWNER_LOOP {
     const double ww = prob_sum(a, 5, k), bb = prob_sum(a, 6, k);
     if (threadIdx.x == 0) a.relres[k] = sqrt(ww) / (sqrt(bb) + 1e-30);
@@ -568,7 +570,7 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
   a.r32 = a.z32 = a.p32 = a.q32 = a.d32 = nullptr;
   if (mixed) {
     if (!p->vals32) FEMK_CUDA_TRY(cudaMalloc(&p->vals32, sizeof(float) * (p->nnz + 1)));
-    if (!p->work32) FEMK_CUDA_TRY(cudaMalloc(&p->work32, sizeof(float) * 6 * p->vstride));
+    if (!p->work32) FEMK_CUDA_TRY(cudaMalloc(&p->work32, sizeof(float) * kWork32Vectors * p->vstride));
     a.vals32 = p->vals32;
     a.r32 = p->work32;
     a.z32 = a.r32 + vs;
@@ -577,6 +579,8 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
     a.d32 = a.q32 + vs;
   }
   a.bar = (GridBar*)p->bar;
+  a.spin = p->barrier_spin;
+  a.skip = p->skip_arrival;
   // tile tables: uploaded only when the schedule changes (pageable copies stay outside the graph)
   uint64_t h = 1469598103934665603ull;
   for (int32_t k = 0; k <= nprob; ++k) h = (h ^ (uint64_t)row_off[k]) * 1099511628211ull;
@@ -693,8 +697,7 @@ extern "C" int femk_pcg_batched_mixed(const femk_plan* pc, int32_t nprob, const 
                                       int32_t* outer_out, double* relres_out, int32_t* status_out, void* stream) {
   clear_error();
   // reliable-update threshold of the single-problem mixed solver (femk_pcg_mixed)
-  double delta2 = 1e-4;
-  if (const char* e = std::getenv("FEMK_MIXED_DELTA2")) delta2 = std::atof(e);  // tuning runs
+  const double delta2 = pc && pc->mixed_delta2 > 0.0 ? pc->mixed_delta2 : 1e-4;
   return batched_impl(pc, nprob, row_off, vals, b, x, dinv, tol, atol, maxiter, tile_rows, blocks_per_sm, iters_out,
                       outer_out, relres_out, status_out, stream, true, delta2);
 }

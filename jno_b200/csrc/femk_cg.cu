@@ -18,12 +18,10 @@
 #include <string>
 
 #include "femk_bulk.cuh"
-#include "femk_tile.cuh"
 #include "femk_reduce.cuh"
 #include "femk_element.cuh"
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
-#include "femk_grid.cuh"
 #include "femk_l2.cuh"
 
 namespace femk {
@@ -223,8 +221,6 @@ __global__ void __launch_bounds__(WPB * 32) k_sell_bulk(const int64_t* __restric
                                                        const int64_t* __restrict__ cptr) {
   extern __shared__ __align__(128) unsigned char bulk_smem[];
   constexpr int kWarpBytes = BulkRing<double, IDX, WMAX, S>::kWarpBytes;
-  pdl_wait();
-  pdl_trigger();
   if (MODE == kCgStep) {
     if (blockIdx.x == 0 && threadIdx.x == 0) st->xpend = 0;  // the last x update is applied
     if (st->done) return;
@@ -254,145 +250,6 @@ __global__ void __launch_bounds__(WPB * 32) k_sell_bulk(const int64_t* __restric
     st->done = 1;
   } else if (!(tot[0] > 0.0)) {
     st->status = FEMK_BREAKDOWN;
-    st->done = 1;
-  }
-}
-
-// The CG-step SpMV with matrix and x staged per tile in shared memory (femk_tile.cuh).
-template <int WMAX>
-__global__ void __launch_bounds__(kTileW * 32) k_sell_tile(const TileMeta* __restrict__ meta, int64_t ntiles,
-                                                          int xcap, const int64_t* __restrict__ sptr,
-                                                          const int64_t* __restrict__ cptr,
-                                                          const int16_t* __restrict__ slots,
-                                                          const double* __restrict__ svals, int64_t n,
-                                                          int64_t nslices, const double* __restrict__ x,
-                                                          double* __restrict__ y, double* __restrict__ partials,
-                                                          CgState* st) {
-  extern __shared__ __align__(128) unsigned char tile_smem[];
-  if (blockIdx.x == 0 && threadIdx.x == 0) st->xpend = 0;  // the last x update is applied
-  if (st->done) return;
-  double acc[1] = {0.0};
-  const bool ok = sell_tile_rows<double, kTileW, WMAX>(
-      tile_smem, xcap, meta, ntiles, sptr, cptr, slots, svals, x, n, nslices,
-      [&](int64_t row, double sv, double xrow) {
-        y[row] = sv;
-        acc[0] += xrow * sv;
-      },
-      &st->status, FEMK_TIMEOUT);
-  if (!ok && threadIdx.x == 0) st->done = 1;
-  block_reduce_store<1, kTileW * 32>(acc, partials);
-  double tot[1];
-  if (!grid_finish<1, kTileW * 32>(partials, &st->ticket, tot)) return;
-  if (threadIdx.x != 0) return;
-  st->pq = tot[0];
-  st->alpha = st->gamma / tot[0];
-  if (!isfinite(tot[0])) {
-    st->status = FEMK_NONFINITE;
-    st->done = 1;
-  } else if (!(tot[0] > 0.0)) {
-    st->status = FEMK_BREAKDOWN;
-    st->done = 1;
-  }
-}
-
-// ---------------------------------------------------------------------------------------------
-// Persistent Jacobi-PCG: the whole iteration loop in one cooperative launch on the sliced-ELL
-// operator. Per iteration three phases separated by grid barriers: q = A p with <p, q>; the x, r,
-// z updates with <r, z>, <r, r>; p = z + beta p. Every block forms alpha, beta and the stop test
-// from the same partial sums, so all blocks leave the loop together. CgState holds the state from
-// the init kernel on entry and the final state on exit.
-// ---------------------------------------------------------------------------------------------
-constexpr int kPersistThreads = 512;
-
-template <typename IDX>
-__global__ void __launch_bounds__(kPersistThreads, 2)
-    k_pcg_persist(const int64_t* __restrict__ sptr, const IDX* __restrict__ scols, const double* __restrict__ svals,
-                  int64_t n, int64_t nslices, const double* __restrict__ dinv, double* __restrict__ x,
-                  double* __restrict__ r, double* __restrict__ z, double* __restrict__ pv, double* __restrict__ q,
-                  double* __restrict__ partials, CgState* st, GridBar* bar) {
-  if (st->done) return;  // set by the init kernel; identical for every block
-  double gamma = st->gamma, rr = st->rr;
-  const double atol2 = st->atol2;
-  const int maxiter = st->maxiter;
-  const bool precond = st->precond != 0;
-  int iter = st->iter, status = FEMK_OK;
-  unsigned int gen = 0;
-  const int G = gridDim.x;
-  double* P1 = partials;
-  double* P2 = partials + G;
-  const int lane = threadIdx.x & 31;
-  const int64_t gwarp = (blockIdx.x * (int64_t)kPersistThreads + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)G * kPersistThreads) >> 5;
-  const int64_t gtid = blockIdx.x * (int64_t)kPersistThreads + threadIdx.x;
-  const int64_t nthr = (int64_t)G * kPersistThreads;
-  while (true) {
-    // phase 1: q = A p, <p, q>
-    double a1[1] = {0.0};
-    for (int64_t sl = gwarp; sl < nslices; sl += nwarps) {
-      const int64_t row = sl * 32 + lane;
-      if (row >= n) continue;
-      const int64_t b0 = __ldg(sptr + sl);
-      const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
-      const double sv = sell_row(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row, GatherXcg<double>{pv});
-      q[row] = sv;
-      a1[0] += __ldcg(pv + row) * sv;
-    }
-    block_partials<1, kPersistThreads>(a1, P1);
-    if (!grid_sync(bar, gen)) {
-      status = FEMK_TIMEOUT;
-      break;
-    }
-    double pq[1];
-    grid_totals<1>(P1, pq);
-    if (!isfinite(pq[0])) {
-      status = FEMK_NONFINITE;
-      break;
-    }
-    if (!(pq[0] > 0.0)) {
-      status = FEMK_BREAKDOWN;
-      break;
-    }
-    const double alpha = gamma / pq[0];
-    // phase 2: x += alpha p; r -= alpha q; z = D^-1 r; <r, z>, <r, r>
-    double a2[2] = {0.0, 0.0};
-    for (int64_t i = gtid; i < n; i += nthr) {
-      x[i] = x[i] + alpha * __ldcg(pv + i);
-      const double ri = r[i] - alpha * __ldcg(q + i);
-      const double zi = dinv ? dinv[i] * ri : ri;
-      r[i] = ri;
-      z[i] = zi;
-      a2[0] += ri * zi;
-      a2[1] += ri * ri;
-    }
-    block_partials<2, kPersistThreads>(a2, P2);
-    if (!grid_sync(bar, gen)) {
-      status = FEMK_TIMEOUT;
-      break;
-    }
-    double t2[2];
-    grid_totals<2>(P2, t2);
-    ++iter;
-    const double beta = t2[0] / gamma;
-    gamma = t2[0];
-    rr = t2[1];
-    if (!isfinite(t2[0]) || !isfinite(t2[1])) {
-      status = FEMK_NONFINITE;
-      break;
-    }
-    const double rs = precond ? rr : gamma;
-    if (!(rs > atol2) || iter >= maxiter) break;
-    // phase 3: p = z + beta p
-    for (int64_t i = gtid; i < n; i += nthr) pv[i] = z[i] + beta * pv[i];
-    if (!grid_sync(bar, gen)) {
-      status = FEMK_TIMEOUT;
-      break;
-    }
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    st->iter = iter;
-    st->gamma = gamma;
-    st->rr = rr;
-    st->status = status;
     st->done = 1;
   }
 }
@@ -540,8 +397,6 @@ template <bool H>
 __global__ void __launch_bounds__(kThreads) k_update_r(int64_t n, double* __restrict__ r, const double* __restrict__ q,
                                                       const double* __restrict__ dinv, double* __restrict__ partials,
                                                       CgState* st) {
-  pdl_wait();
-  pdl_trigger();
   if (st->done) return;
   const double alpha = st->alpha;
   double acc[2] = {0.0, 0.0};
@@ -611,8 +466,6 @@ template <bool H>
 __global__ void __launch_bounds__(kThreads) k_pupdate_x(int64_t n, double* __restrict__ x, double* __restrict__ p,
                                                        const double* __restrict__ r, const double* __restrict__ dinv,
                                                        const CgState* st) {
-  pdl_wait();
-  pdl_trigger();
   if (!st->xpend) return;
   const bool dir = !st->done;
   const double alpha = st->alpha, beta = st->beta;
@@ -651,53 +504,6 @@ __global__ void __launch_bounds__(kThreads) k_pupdate_x(int64_t n, double* __res
       st2(x2 + i, make_double2(fma(alpha, pa.x, xa.x), fma(alpha, pa.y, xa.y)));
     }
     if ((n & 1) && tid == 0) x[n - 1] = fma(alpha, p[n - 1], x[n - 1]);
-  }
-}
-
-// CG step with the direction update folded in: p_new = z + beta p_old is formed at every gather
-// (and stored by the row's owner), q = A p_new, <p_new, q> -> alpha. Double-buffered p, so no
-// separate p-update pass and no grid-wide wait between the two.
-template <int L, int U>
-__global__ void __launch_bounds__(kThreads) k_cg_step(const int32_t* __restrict__ indptr,
-                                                     const int32_t* __restrict__ indices,
-                                                     const double* __restrict__ vals, int64_t n,
-                                                     const double* __restrict__ z, const double* __restrict__ pold,
-                                                     double* __restrict__ pnew, double* __restrict__ q,
-                                                     double* __restrict__ partials, CgState* st) {
-  if (st->done) return;
-  const GatherDirection g{z, pold, st->beta};
-  const int lane = threadIdx.x & 31;
-  const int sub = lane % L;
-  const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
-  constexpr int RPW = 32 / L;
-  double acc[1] = {0.0};
-  for (int64_t base = warp * RPW * U; base < n; base += nwarps * RPW * U) {
-    double sv[U];
-    int64_t rows[U];
-    csr_rows_g<L, U, double, int32_t>(indptr, indices, vals, g, n, base, lane, sv, rows);
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int64_t row = rows[u];
-      if (row >= n || sub != 0) continue;
-      const double pn = g(row);
-      pnew[row] = pn;
-      q[row] = sv[u];
-      acc[0] += pn * sv[u];
-    }
-  }
-  block_reduce_store<1>(acc, partials);
-  double tot[1];
-  if (!grid_finish<1>(partials, &st->ticket, tot)) return;
-  if (threadIdx.x != 0) return;
-  st->pq = tot[0];
-  st->alpha = st->gamma / tot[0];
-  if (!isfinite(tot[0])) {
-    st->status = FEMK_NONFINITE;
-    st->done = 1;
-  } else if (!(tot[0] > 0.0)) {
-    st->status = FEMK_BREAKDOWN;
-    st->done = 1;
   }
 }
 
@@ -893,14 +699,13 @@ bool split_ok(const femk_plan* p, const double* x, const double* dinv) {
 void launch_update_r(const femk_plan* p, double* r, const double* q, const double* dinv, CgState* st,
                      cudaStream_t s) {
   auto kern = p->l2_mode != 0 ? k_update_r<true> : k_update_r<false>;
-  (void)launch_ex(p->pdl != 0, kern, vec_grid(kern, kThreads, p), kThreads, 0, s, p->n, r, q, dinv, p->partials,
-                  st);
+  kern<<<::femk::counted_launch() + vec_grid(kern, kThreads, p), kThreads, 0, s>>>(p->n, r, q, dinv, p->partials, st);
 }
 
 void launch_pupdate_x(const femk_plan* p, double* x, double* pv, const double* r, const double* dinv,
                       const CgState* st, cudaStream_t s) {
   auto kern = p->l2_mode != 0 ? k_pupdate_x<true> : k_pupdate_x<false>;
-  (void)launch_ex(p->pdl != 0, kern, vec_grid(kern, kThreads, p), kThreads, 0, s, p->n, x, pv, r, dinv, st);
+  kern<<<::femk::counted_launch() + vec_grid(kern, kThreads, p), kThreads, 0, s>>>(p->n, x, pv, r, dinv, st);
 }
 
 template <int MODE>
@@ -947,48 +752,15 @@ bool launch_sell_bulk_cfg(const femk_plan* p, const double* x, double* y, CgStat
   if (prime) return true;
   const int grid = p->n_sm * std::min(per_sm, 16);
   const bool tab = p->sell_cu != nullptr;  // per-slice column tables (shared-offset slices stored once)
-  (void)launch_ex(p->pdl != 0, kern, grid, WPB * 32, kSmem, s, (const int64_t*)p->sell_ptr,
-                  (const int16_t*)(tab ? p->sell_cu : p->sell_c16), (const double*)p->sell_vals, p->n, p->n_slices, x,
-                  y, p->partials, st, (int*)nullptr, (const int64_t*)(tab ? p->sell_cuptr : nullptr));
+  kern<<<::femk::counted_launch() + grid, WPB * 32, kSmem, s>>>(
+      (const int64_t*)p->sell_ptr, (const int16_t*)(tab ? p->sell_cu : p->sell_c16), (const double*)p->sell_vals,
+      p->n, p->n_slices, x, y, p->partials, st, (int*)nullptr, (const int64_t*)(tab ? p->sell_cuptr : nullptr));
   return true;
-}
-
-// Staged-x CG-step SpMV when the plan built its tiles (tile_ok); false: nothing launched.
-template <int WMAX>
-bool launch_sell_tile_w(const femk_plan* p, const double* x, double* y, CgState* st, cudaStream_t s, bool prime) {
-  auto kern = k_sell_tile<WMAX>;
-  static int attr_ok = -1;  // per instantiation: opt in to the largest stage size once
-  if (attr_ok < 0) {
-    const int most = 2 * TileStage<double, kTileW, WMAX>::bytes(4096) + 16;
-    attr_ok = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, most) == cudaSuccess;
-    if (!attr_ok) cudaGetLastError();
-  }
-  if (!attr_ok) return false;
-  const int smem = 2 * TileStage<double, kTileW, WMAX>::bytes(p->tile_xcap) + 16;
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileW * 32, smem) != cudaSuccess || per_sm <= 0) {
-    cudaGetLastError();
-    return false;
-  }
-  if (prime) return true;
-  const int grid = (int)std::min<int64_t>(p->ntiles, (int64_t)p->n_sm * std::min(per_sm, 16));
-  kern<<<::femk::counted_launch() + grid, kTileW * 32, smem, s>>>(
-      (const TileMeta*)p->tile_meta, p->ntiles, p->tile_xcap, p->sell_ptr, p->sell_cuptr, p->tile_slots,
-      p->sell_vals, p->n, p->n_slices, x, y, p->partials, st);
-  return true;
-}
-
-bool launch_sell_tile(const femk_plan* p, const double* x, double* y, CgState* st, cudaStream_t s, bool prime) {
-  if (!p->tile_ok || !p->tile64 || !p->sell_vals || ((uintptr_t)p->sell_vals & 15u) || ((uintptr_t)x & 15u))
-    return false;
-  return p->max_row <= 16 ? launch_sell_tile_w<16>(p, x, y, st, s, prime)
-                          : launch_sell_tile_w<32>(p, x, y, st, s, prime);
 }
 
 // prime = true only sets the kernel attribute and reads the occupancy (before a graph capture)
 bool launch_sell_bulk(const femk_plan* p, const double* x, double* y, CgState* st, cudaStream_t s,
                       bool prime = false) {
-  if (launch_sell_tile(p, x, y, st, s, prime)) return true;
   if (!p->bulk_cfg || !p->sell_c16 || !p->sell64_c16 || p->max_row > 32) return false;
   if (!aligned16(p->sell_vals) || !aligned16(p->sell_c16)) return false;  // bulk copies start on 16 B
   if (p->sell_cu && !aligned16(p->sell_cu)) return false;
@@ -1048,7 +820,7 @@ int launch_op(const femk_plan* p, bool sell, const double* vals, const double* x
     }
   };
   const bool c16 = p->sell_c16 && p->sell64_c16;
-  if (sell_batch() == 8) {
+  if (p->sell_batch == 8) {
     if (c16)
       go(std::integral_constant<int, 8>{}, (const int16_t*)p->sell_c16);
     else
@@ -1087,10 +859,8 @@ __global__ void k_zero(double* __restrict__ y, int64_t n, const CgState* st) {
 int launch_matfree(const femk_plan* p, const MatFree& m, const double* x, double* y, cudaStream_t s,
                    const CgState* st = nullptr) {
   k_zero<<<::femk::counted_launch() + p->n_sm * 8, 256, 0, s>>>(y, p->n, st);
-  if (!launch_matfree_cl(p, m.param, m.mode, m.scale, x, y, st, s)) {
-    const int grid = blocks_for(p->ntet, 128, p->n_sm * 16);
-    FEMK_BY_ND(p->nd, k_matfree<ND><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, m.param, m.mode, m.scale, x, y, st));
-  }
+  const int grid = blocks_for(p->ntet, 128, p->n_sm * 16);
+  FEMK_BY_ND(p->nd, k_matfree<ND><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, m.param, m.mode, m.scale, x, y, st));
   FEMK_CUDA_TRY(cudaGetLastError());
   if (p->n_dir > 0) {
     k_dirichlet_identity<<<::femk::counted_launch() + blocks_for(p->n_dir, 256, 65535), 256, 0, s>>>(p->dlist, p->n_dir, x, y, st);
@@ -1099,9 +869,7 @@ int launch_matfree(const femk_plan* p, const MatFree& m, const double* x, double
   return FEMK_OK;
 }
 
-// One chunk of kChunk CG iterations on stream ws (CSR operator). Fused: 2 kernels per iteration
-// with the direction double-buffered in P0/P1 (chunks have even length, so every chunk starts
-// with p in P0); otherwise the three-kernel form.
+// One chunk of CG iterations on stream ws: the step SpMV and the two vector kernels per iteration.
 // Opt-in per-kernel timing of the CG loop (femk_set_profiling): events around the three kernels
 // of every iteration of a chunk; the chunked path runs without graph replay while it is on.
 struct ProfData {
@@ -1110,66 +878,48 @@ struct ProfData {
   int64_t iters = 0;
 };
 
-int enqueue_chunk(const femk_plan* p, const double* vals, double* x, const double* dinv, bool fused, bool sell,
-                  int64_t iters, cudaStream_t ws) {
-  const int64_t n = p->n;
+int enqueue_chunk(const femk_plan* p, const double* vals, double* x, const double* dinv, bool sell, int64_t iters,
+                  cudaStream_t ws) {
   const int64_t vs = p->vstride;
   double* r = p->work;
   double* z = r + vs;
   double* P0 = z + vs;
   double* q = P0 + vs;
-  double* P1 = q + vs;
   CgState* st = p->state;
+  ProfData* pd = (ProfData*)p->prof;
+  const bool split = split_ok(p, x, dinv);
   for (int64_t it = 0; it < iters; ++it) {
-    if (fused) {
-      double* pold = (it & 1) ? P1 : P0;
-      double* pnew = (it & 1) ? P0 : P1;
-      const bool ok = with_spmv_cfg(p->spmv_L, p->spmv_U, [&](auto Lc, auto Uc) {
-        constexpr int L = decltype(Lc)::value, U = decltype(Uc)::value;
-        k_cg_step<L, U><<<::femk::counted_launch() + wave_grid(k_cg_step<L, U>, kThreads, p), kThreads, 0, ws>>>(
-            p->indptr, p->indices, vals, n, z, pold, pnew, q, p->partials, st);
-      });
-      if (!ok) {
-        set_error("unsupported SpMV configuration");
-        return FEMK_EINVAL;
-      }
-      launch_update(p, x, r, z, pnew, q, dinv, p->partials, st, ws);
-    } else {
-      ProfData* pd = (ProfData*)p->prof;
-      const bool split = split_ok(p, x, dinv);
-      if (pd) cudaEventRecord(pd->ev[it][0], ws);
-      FEMK_TRY(launch_op<kCgStep>(p, sell, vals, P0, q, nullptr, nullptr, nullptr, nullptr, st, 0.0, 0.0, ws));
-      if (pd) cudaEventRecord(pd->ev[it][1], ws);
-      if (split)
-        launch_update_r(p, r, q, dinv, st, ws);
-      else
-        launch_update(p, x, r, z, P0, q, dinv, p->partials, st, ws);
-      if (pd) cudaEventRecord(pd->ev[it][2], ws);
-      if (split)
-        launch_pupdate_x(p, x, P0, r, dinv, st, ws);
-      else
-        launch_pupdate(p, P0, z, st, ws);
-      if (pd) cudaEventRecord(pd->ev[it][3], ws);
-    }
+    if (pd) cudaEventRecord(pd->ev[it][0], ws);
+    FEMK_TRY(launch_op<kCgStep>(p, sell, vals, P0, q, nullptr, nullptr, nullptr, nullptr, st, 0.0, 0.0, ws));
+    if (pd) cudaEventRecord(pd->ev[it][1], ws);
+    if (split)
+      launch_update_r(p, r, q, dinv, st, ws);
+    else
+      launch_update(p, x, r, z, P0, q, dinv, p->partials, st, ws);
+    if (pd) cudaEventRecord(pd->ev[it][2], ws);
+    if (split)
+      launch_pupdate_x(p, x, P0, r, dinv, st, ws);
+    else
+      launch_pupdate(p, P0, z, st, ws);
+    if (pd) cudaEventRecord(pd->ev[it][3], ws);
   }
   FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;
 }
 
 // Capture one chunk into a CUDA graph (re-captured when the operand pointers change).
-int ensure_chunk_graph(femk_plan* p, const double* vals, double* x, const double* dinv, bool fused, bool sell) {
+int ensure_chunk_graph(femk_plan* p, const double* vals, double* x, const double* dinv, bool sell) {
   if (sell && !p->sell_vals) {
     set_error("femk_pcg: sliced-ELL values missing at graph capture");
     return FEMK_EINVAL;
   }
-  const void* key[5] = {vals, x, dinv, (const void*)(intptr_t)((fused ? 1 : 2) + (sell ? 4 : 0)), p->sell_vals};
+  const void* key[5] = {vals, x, dinv, (const void*)(intptr_t)(sell ? 4 : 2), p->sell_vals};
   bool same = p->cg_exec != nullptr;
   for (int i = 0; i < 5; ++i) same = same && key[i] == p->cg_key[i];
   if (same) return FEMK_OK;
   // occupancy queries happen before capture begins
   with_spmv_cfg(p->spmv_L, p->spmv_U, [&](auto Lc, auto Uc) {
     constexpr int L = decltype(Lc)::value, U = decltype(Uc)::value;
-    (void)wave_grid(k_cg_step<L, U>, kThreads, p);
     (void)wave_grid(k_csr<L, U, kCgStep>, kThreads, p);
   });
   (void)wave_grid(k_sell<kCgStep, int32_t, 8>, kThreads, p);
@@ -1201,7 +951,7 @@ int ensure_chunk_graph(femk_plan* p, const double* vals, double* x, const double
   cudaGraph_t g = nullptr;
   set_capturing(true);
   cudaError_t e = cudaStreamBeginCapture(p->cg_stream, cudaStreamCaptureModeThreadLocal);
-  int st = e == cudaSuccess ? enqueue_chunk(p, vals, x, dinv, fused, sell, kChunk, p->cg_stream) : FEMK_ECUDA;
+  int st = e == cudaSuccess ? enqueue_chunk(p, vals, x, dinv, sell, kChunk, p->cg_stream) : FEMK_ECUDA;
   const cudaError_t e2 = cudaStreamEndCapture(p->cg_stream, &g);
   set_capturing(false);
   if (e != cudaSuccess || e2 != cudaSuccess || st != FEMK_OK) {
@@ -1230,7 +980,7 @@ int ensure_chunk_graph(femk_plan* p, const double* vals, double* x, const double
   }
   cudaGraphDestroy(g);
   for (int i = 0; i < 5; ++i) p->cg_key[i] = key[i];
-  p->cg_nodes = (fused ? 2 : 3) * kChunk;
+  p->cg_nodes = 3 * kChunk;
   return FEMK_OK;
 }
 
@@ -1238,32 +988,6 @@ int ensure_cg_stream(femk_plan* p) {
   if (p->cg_stream) return FEMK_OK;
   FEMK_CUDA_TRY(cudaStreamCreateWithFlags(&p->cg_stream, cudaStreamNonBlocking));
   for (int i = 0; i < 3; ++i) FEMK_CUDA_TRY(cudaEventCreateWithFlags(&p->cg_ev[i], cudaEventDisableTiming));
-  return FEMK_OK;
-}
-
-// Cooperative launch of k_pcg_persist over every resident block (at most 2 per SM).
-int launch_persistent(femk_plan* p, const double* dinv, double* x, cudaStream_t ws) {
-  const int64_t n = p->n;
-  const int64_t vs = p->vstride;
-  double* r = p->work;
-  double* z = r + vs;
-  double* pv = z + vs;
-  double* q = pv + vs;
-  FEMK_CUDA_TRY(cudaMemsetAsync(p->bar, 0, sizeof(GridBar), ws));
-  const bool c16 = p->sell_c16 != nullptr;
-  const void* fn = c16 ? (const void*)k_pcg_persist<int16_t> : (const void*)k_pcg_persist<int32_t>;
-  const int per_sm = std::min(2, resident_blocks(fn, kPersistThreads));
-  const int grid = p->n_sm * per_sm;
-  const void* cols = c16 ? (const void*)p->sell_c16 : (const void*)p->sell_cols;
-  const double* sv = p->sell_vals;
-  CgState* st = p->state;
-  GridBar* bar = (GridBar*)p->bar;
-  int64_t nslices = p->n_slices;
-  void* args[] = {(void*)&p->sell_ptr, (void*)&cols, (void*)&sv,       (void*)&n,  (void*)&nslices,
-                  (void*)&dinv,        (void*)&x,    (void*)&r,        (void*)&z,  (void*)&pv,
-                  (void*)&q,           (void*)&p->partials, (void*)&st, (void*)&bar};
-  counted_launch();
-  FEMK_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kPersistThreads), args, 0, ws));
   return FEMK_OK;
 }
 
@@ -1279,11 +1003,9 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
   double* pv = z + vs;
   double* q = pv + vs;
   CgState* st = p->state;
-  const bool fused = !mf && p->cg_fused;
-  ProfData* pd = (!mf && !fused) ? (ProfData*)p->prof : nullptr;
+  ProfData* pd = !mf ? (ProfData*)p->prof : nullptr;
   const bool graph = !mf && p->cg_graph && !pd;
-  const bool sell = !mf && !fused && p->use_sell && p->sell_src;
-  const bool persist = sell && p->cg_persist && p->coop;
+  const bool sell = !mf && p->use_sell && p->sell_src;
   // all solver work runs on the plan's stream, ordered after the caller's stream and before
   // whatever the caller enqueues next
   cudaStream_t ws = p->cg_stream;
@@ -1291,7 +1013,7 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
   FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->cg_ev[2], 0));
   // the sliced-ELL values buffer must exist before a graph that reads it is captured
   if (sell) FEMK_TRY(prepare_sell(p, vals, ws));
-  if (graph && !persist) FEMK_TRY(ensure_chunk_graph(p, vals, x, dinv, fused, sell));
+  if (graph) FEMK_TRY(ensure_chunk_graph(p, vals, x, dinv, sell));
   CgState init{};
   init.maxiter = maxiter;
   init.precond = dinv ? 1 : 0;
@@ -1310,10 +1032,7 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
   int64_t enq = 0;  // iterations enqueued
   int chunk_id = 0;
   bool have_prev = false;
-  if (persist) {
-    FEMK_TRY(launch_persistent(p, dinv, x, ws));
-  }
-  while (!persist) {
+  while (true) {
     if (graph) {
       FEMK_CUDA_TRY(cudaGraphLaunch(p->cg_exec, ws));
       count_launches(p->cg_nodes);
@@ -1331,7 +1050,7 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
       enq += todo;
     } else {
       const int64_t todo = std::min<int64_t>(kChunk, (int64_t)maxiter - enq);
-      FEMK_TRY(enqueue_chunk(p, vals, x, dinv, fused, sell, todo, ws));
+      FEMK_TRY(enqueue_chunk(p, vals, x, dinv, sell, todo, ws));
       if (pd) {  // time the iterations of this chunk that ran (later ones return at entry)
         CgState now{};
         FEMK_CUDA_TRY(cudaMemcpyAsync(&now, st, sizeof(CgState), cudaMemcpyDeviceToHost, ws));
@@ -1389,7 +1108,7 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
   } else if (status == FEMK_NONFINITE) {
     set_error("femk_pcg: non-finite value in a CG reduction");
   } else if (status == FEMK_TIMEOUT) {
-    set_error("femk_pcg: a grid barrier of the persistent solver gave up waiting");
+    set_error("femk_pcg: a bulk-copy wait of the CG-step SpMV gave up");
   }
   return status;
 }
@@ -1482,7 +1201,6 @@ extern "C" int femk_spmv_matfree(const femk_plan* p, const double* param, int mo
   FEMK_CHECK_ARG(p && x && y, "femk_spmv_matfree: NULL argument");
   FEMK_CHECK_ARG(coef_mode_ok(p, mode, param), "femk_spmv_matfree: bad coefficient");
   FEMK_TRY(resolve_coef(p, param, mode, (cudaStream_t)stream, &param, &mode));
-  FEMK_TRY(ensure_clusters(const_cast<femk_plan*>(p), (cudaStream_t)stream));
   MatFree m{param, mode, scale};
   return launch_matfree(p, m, x, y, (cudaStream_t)stream);
 }
@@ -1518,7 +1236,6 @@ extern "C" int femk_pcg_matfree(const femk_plan* p, const double* param, int mod
   FEMK_CHECK_ARG(p && b && x, "femk_pcg_matfree: NULL argument");
   FEMK_CHECK_ARG(coef_mode_ok(p, mode, param), "femk_pcg_matfree: bad coefficient");
   FEMK_TRY(resolve_coef(p, param, mode, (cudaStream_t)stream, &param, &mode));
-  FEMK_TRY(ensure_clusters(const_cast<femk_plan*>(p), (cudaStream_t)stream));  // before any capture
   MatFree m{param, mode, scale};
   return pcg_run(p, nullptr, &m, b, x, dinv, tol, atol, maxiter, iters_out, relres_out, (cudaStream_t)stream);
 }

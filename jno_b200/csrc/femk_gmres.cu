@@ -8,10 +8,10 @@
 //   while beta > ptol and cycles < maxiter:
 //     V_0 = w;  H = eye(m, m + 1)                 (row j of H is column j of the Hessenberg matrix)
 //     for j < m, until breakdown:
-//       v = M A V_j;  v0 = ||v||;  classical Gram-Schmidt against V twice (once when v0 = 0)
+//       v = M A V_j;  v0 = ||v||;  one classical Gram-Schmidt pass against V
 //       V_{j+1}, H[j, j+1] = normalize(v, threshold eps v0);  H[j, :j+1] = the projections
 //     y = (H H^T)^-1 H (beta e_0)                 (Cholesky: the normal equations of the (m+1) x m LSQ)
-//     x += V[:, :m] y;  w, beta = normalize(M (b - A x))
+//     x += V[:, :m] y;  w, beta = normalize(M (b - A x))   (columns past a breakdown are zero in jax)
 //
 // normalize(v, t) = (v / ||v||, ||v||) if ||v|| > t (default t = eps), else (0, 0). Vectors and the
 // Krylov basis live in HBM (the basis as m + 1 contiguous vectors of the plan's vector stride); every
@@ -167,7 +167,7 @@ int gm_sum(const Gm& g, const double* part, int ncol, int stride, int off, doubl
   return FEMK_OK;
 }
 
-// M (b - A x) normalised into dst; beta = its norm (0 at or under eps), rr = ||b - A x||^2
+// M (b - A x) normalised into dst; beta = its norm (0 at or under eps, non-finite kept), rr = ||b - A x||^2
 int gm_residual(const Gm& g, const double* b, const double* x, double* dst, double* beta, double* rr) {
   FEMK_TRY(gm_spmv(g, x, g.q));
   k_gm_resid<<<counted_launch() + g.grid, kGmThreads, 0, g.s>>>(b, g.q, g.dinv, g.p->n, g.w, g.part);
@@ -175,7 +175,8 @@ int gm_residual(const Gm& g, const double* b, const double* x, double* dst, doub
   double t[2];
   FEMK_TRY(gm_sum(g, g.part, 2, 2, 0, t));
   const double nrm = std::sqrt(t[0]);
-  *beta = nrm > 2.220446049250313e-16 ? nrm : 0.0;
+  // a NaN / Inf residual stays non-finite (NaN > eps is false and would read as convergence)
+  *beta = !std::isfinite(nrm) ? nrm : (nrm > 2.220446049250313e-16 ? nrm : 0.0);
   *rr = t[1];
   k_gm_div<<<counted_launch() + g.grid, kGmThreads, 0, g.s>>>(g.w, *beta, dst, g.p->n);
   FEMK_CUDA_TRY(cudaGetLastError());
@@ -273,6 +274,7 @@ int gmres_run(femk_plan* p, bool sell, const double* vals, const double* b, doub
   while (std::isfinite(beta) && beta > ptol && info->cycles < maxiter) {
     std::fill(H.begin(), H.end(), 0.0);
     for (int i = 0; i < m; ++i) H[(size_t)i * (m + 1) + i] = 1.0;
+    int used = 0;  // basis columns V[:, 0..used) written in this cycle (the update reads no others)
     for (int j = 0; j < m; ++j) {
       FEMK_TRY(gm_spmv(g, g.V + (int64_t)j * g.ld, g.w));
       k_gm_precond<<<counted_launch() + g.grid, kGmThreads, 0, s>>>(g.w, dinv, n, norm_part);
@@ -284,7 +286,8 @@ int gmres_run(femk_plan* p, bool sell, const double* vals, const double* b, doub
       const int ncol = j + 1;
       std::fill(h.begin(), h.end(), 0.0);
       double vnorm_sq = v0sq;
-      for (int pass = 0; pass < (v0 > 0.0 ? 2 : 1); ++pass) {
+      {  // one classical Gram-Schmidt pass: jax's _iterative_classical_gram_schmidt(max_iterations=2)
+         // stops after its first pass (its loop runs while k < max_iterations - 1, and k = 1 then)
         for (int j0 = 0; j0 < ncol; j0 += kGmCols)
           k_gm_project<<<counted_launch() + g.grid, kGmThreads, 0, s>>>(
               g.V, g.ld, j0, std::min(kGmCols, ncol - j0), g.w, n, g.part + (int64_t)(j0 / kGmCols) * g.grid * kGmCols);
@@ -307,6 +310,7 @@ int gmres_run(femk_plan* p, bool sell, const double* vals, const double* b, doub
       h[j + 1] = v1;
       for (int c = 0; c <= m; ++c) H[(size_t)j * (m + 1) + c] = h[c];
       info->steps += 1;
+      used = j + 1;
       if (v1 == 0.0) break;
     }
     // y = (H H^T)^-1 (H e_0 beta)
@@ -324,7 +328,9 @@ int gmres_run(femk_plan* p, bool sell, const double* vals, const double* b, doub
       return FEMK_BREAKDOWN;
     }
     FEMK_CUDA_TRY(cudaMemcpyAsync(g.small + 2 * (kGmMaxM + 1), y.data(), sizeof(double) * m, cudaMemcpyHostToDevice, s));
-    k_gm_update<<<counted_launch() + g.grid, kGmThreads, 0, s>>>(g.V, g.ld, g.small + 2 * (kGmMaxM + 1), m, x, n);
+    // y[c] is exactly 0 for c >= used (those rows of H are the identity), but the columns past a
+    // breakdown hold an earlier cycle's vectors or never-written memory: 0 * NaN would poison x
+    k_gm_update<<<counted_launch() + g.grid, kGmThreads, 0, s>>>(g.V, g.ld, g.small + 2 * (kGmMaxM + 1), used, x, n);
     FEMK_CUDA_TRY(cudaGetLastError());
     FEMK_TRY(gm_residual(g, b, x, g.V, &beta, &rr));
     info->cycles += 1;
@@ -358,7 +364,7 @@ extern "C" int femk_gmres(const femk_plan* pc, const double* vals, const double*
   const bool sell = p->use_sell && p->sell_src;
   if (sell) FEMK_TRY(femk_prepare_operator(p, vals, s));
   GmresInfo info;
-  const int64_t cap = maxiter > 0 ? maxiter : 10 * p->n;  // jax's default: 10 n restart cycles
+  const int64_t cap = maxiter >= 0 ? maxiter : 10 * p->n;  // negative: jax's default of 10 n restart cycles
   const int rc = gmres_run(p, sell, vals, b, x, inv_diag, tol, atol, restart, cap, s, &info);
   if (iters_out) *iters_out = (int32_t)std::min<int64_t>(info.steps, INT32_MAX);
   if (cycles_out) *cycles_out = (int32_t)std::min<int64_t>(info.cycles, INT32_MAX);

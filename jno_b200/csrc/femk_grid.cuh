@@ -5,8 +5,8 @@
 // the generation with acquire loads. Each wait is bounded by a clock64 budget: a block that runs
 // out of budget raises the timeout word and returns false, every other waiting block sees the
 // word and returns false too, and the kernel unwinds with FEMK_TIMEOUT instead of hanging. A
-// cooperative launch guarantees all blocks are resident, so the budget is never reached in a
-// correct run.
+// cooperative launch guarantees all blocks are resident, so the budget (the plan's
+// barrier_limit_ms, 2 s by default) is never reached in a correct run.
 //
 // Reductions are redundant instead of serial: every block writes its partial, crosses the
 // barrier, and then sums all partials itself in the same fixed order, so each block holds the
@@ -24,8 +24,6 @@ struct GridBar {
   unsigned int pad;
 };
 
-constexpr long long kBarrierSpinCycles = 4000000000LL;  // about 2 s at the B200 boost clock
-
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
   unsigned int v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -33,15 +31,19 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
 }
 
 // All threads of every block call this. `gen` is the caller's generation counter (kept by
-// thread 0; starts at 0 for a freshly zeroed GridBar). Returns false once any block timed out.
-__device__ __forceinline__ bool grid_sync(GridBar* bar, unsigned int& gen) {
+// thread 0; starts at 0 for a freshly zeroed GridBar). `limit` bounds the wait in clock64 cycles.
+// Returns false once any block timed out. The block numbered `skip` does not arrive at the first
+// barrier (gen == 0): that is how a test makes every other block wait out its limit (the plan's
+// test_skip_arrival option; -1 in every other launch).
+__device__ __forceinline__ bool grid_sync(GridBar* bar, unsigned int& gen, long long limit, int skip = -1) {
   __shared__ int ok_s;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
     const unsigned int target = gen + 1;
     __threadfence();
-    if (atomicAdd(&bar->count, 1u) == gridDim.x - 1) {
+    const bool arrive = !(gen == 0u && (int)blockIdx.x == skip);
+    if (arrive && atomicAdd(&bar->count, 1u) == gridDim.x - 1) {
       atomicExch(&bar->count, 0u);
       __threadfence();
       atomicExch(&bar->gen, target);
@@ -52,7 +54,7 @@ __device__ __forceinline__ bool grid_sync(GridBar* bar, unsigned int& gen) {
           ok = 0;
           break;
         }
-        if (clock64() - t0 > kBarrierSpinCycles) {
+        if (clock64() - t0 > limit) {
           atomicExch(&bar->timeout, 1u);
           ok = 0;
           break;

@@ -13,7 +13,7 @@
 
 namespace femk {
 
-constexpr int kTileW = 4;  // slices (warps) per tile of the staged-x SpMV
+constexpr int kWork32Vectors = 7;  // FP32 vectors of the mixed solvers (plan->work32 holds this many)
 
 void set_error(const std::string& msg);
 void clear_error();
@@ -135,36 +135,31 @@ struct femk_plan {
   int64_t* sell_cuptr = nullptr;  // i64[n_slices+1] first table entry of each slice
   int16_t* sell_cu = nullptr;     // i16[sell_cu_len]
   int64_t sell_cu_len = 0;
-  // staged-x SpMV (femk_tile.cuh): per-tile x windows and slot tables, built with the plan
-  int tile_on = 0, tile_ok = 0;   // opt-in (FEMK_TILE=1): measured slower than the bulk-copy kernel
-  int tile64 = 1, tile32 = 1;     // use the staged-x kernel for the FP64 CG step / the FP32 step
-  int64_t ntiles = 0;
-  int tile_xcap = 0;              // largest staged x of any tile (elements, multiple of 4)
-  void* tile_meta = nullptr;      // TileMeta[ntiles]
-  int16_t* tile_slots = nullptr;  // i16[sell_cu_len] slot table (layout of sell_cu)
   int use_sell = 1;
-  int l2_mode = 0;               // L2 eviction hints of the FP64 CG kernels (see l2_hints in femk_spmv.cuh)
-  int l2_mode32 = 0;             // the same for the FP32 kernels of the mixed solver (0 off, 1 on)
+  int l2_mode = 0;               // L2 eviction hints of the FP64 CG kernels (the l2_hints plan option)
   int sell64_c16 = 1;            // FP64 sliced-ELL streams int16 column offsets when available
+  int sell_batch = 16;           // entries in flight per thread of the thread-per-row FP64 sliced-ELL kernel
+  double mixed_delta2 = 0.0;     // reliable-update threshold of the mixed solvers (0: 1e-4)
+  long long barrier_spin = 0;    // clock64 budget of each grid-barrier wait of the batched solvers
+  int skip_arrival = -1;         // testing: block that skips its first grid-barrier arrival (-1: none)
   // solver workspace (allocated on first use)
   int64_t vstride = 0;          // solver vector stride: n rounded up to 64 (keeps every slot 512-byte aligned)
   double* work = nullptr;       // 5 slots of vstride doubles: r, z, p, q, p' (double-buffered direction)
   double* partials = nullptr;   // reduction partials
   femk::CgState* state = nullptr;
   femk::CgState* state_host = nullptr;  // pinned mirror
-  float* work32 = nullptr;      // FP32 inner vectors (mixed precision): r, z, p, q, e, D^-1
+  float* work32 = nullptr;      // kWork32Vectors FP32 vectors of the mixed solvers
   float* vals32 = nullptr;      // FP32 copy of the values (mixed precision)
   double* work64b = nullptr;    // mixed-precision solver state
   int n_sm = 148;
   // CG launch machinery: plan-owned stream, events, and the captured chunk graph
-  int cg_fused = 0, cg_graph = 1, cg_persist = 0;
+  int cg_graph = 1;
   int cg_split = 1;             // split vector kernels (k_update_r + k_pupdate_x) on aligned vectors
   int bulk_cfg = 0;             // bulk-copy FP64 CG-step SpMV: 10 * stages + warps per block, 0 = off
   int bulk32_cfg = 0;           // the same for the FP32 step of the mixed solver
-  int pdl = 0;                  // programmatic dependent launch inside the CG / mixed chunks
   int vec_blocks = 0;           // blocks per SM of the CG vector kernels (0: one full wave)
   int coop = 0;                 // device supports cooperative launch
-  void* bar = nullptr;          // grid barrier of the persistent solvers
+  void* bar = nullptr;          // grid barrier of the batched solvers
   cudaStream_t cg_stream = nullptr;
   cudaEvent_t cg_ev[3] = {nullptr, nullptr, nullptr};
   cudaGraphExec_t cg_exec = nullptr;
@@ -175,9 +170,6 @@ struct femk_plan {
   cudaEvent_t mx_ev[3] = {nullptr, nullptr, nullptr};
   cudaGraphExec_t mx_exec = nullptr;
   const void* mx_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-  float* mx_zp = nullptr;  // f32[4 vstride]: the fused mixed form's two (z, p) pair buffers
-  int mx_fz = 0;           // the fused mixed form is enabled for this plan (FEMK_MIXED_FUSE)
-  int mx_fz_on = 0;        // ... and applies to the current solve (bulk-copy FP32 step, split updates)
   int mx_nodes = 0;
   void* mx_host = nullptr;  // pinned state mirrors
   // batched solver workspace (tiles, per-problem state, partials)
@@ -194,15 +186,6 @@ struct femk_plan {
   double* gm_ws = nullptr;      // GMRES: Krylov basis (restart + 1 vectors), w, q, partials, small arrays
   int64_t gm_size = 0;          // doubles in gm_ws
   int64_t* cmp_ws = nullptr;    // i64[2 n + 2] femk_compact: kept entries per row, then their exclusive scan
-  // element clusters of the matrix-free operator (built on first use): distinct DOFs per cluster
-  // of 128 consecutive elements and each element's local slots; cl_state 0 unbuilt, 1 ready, -1 off
-  int32_t* cl_ptr = nullptr;    // i32[ncl+1]
-  int32_t* cl_dof = nullptr;    // i32[cl_ptr[ncl]]
-  uint16_t* cl_loc = nullptr;   // u16[ntet*nd]
-  uint16_t* cl_off = nullptr;   // u16[cl_ptr[ncl] + ncl] per cluster: slot offsets into its pair list
-  uint16_t* cl_inv = nullptr;   // u16[ncl*128*nd] per cluster: (element, local dof) pairs sorted by slot
-  int64_t ncl = 0;
-  int cl_max = 0, cl_grid = 0, cl_state = 0;
   // BiCGStab workspace (8 vectors), state, stream, events and captured chunk graph
   void* bicg_ws = nullptr;
   void* bicg_state = nullptr;
@@ -241,13 +224,6 @@ int ensure_workspace(femk_plan* p);
 int resolve_coef(const femk_plan* p, const double* param, int mode, cudaStream_t s, const double** param_out,
                  int* mode_out);
 
-// Matrix-free operator on element clusters staged in shared memory (femk_cluster.cu):
-// ensure_clusters builds the tables once (host work; call outside any graph capture),
-// launch_matfree_cl adds A x into y and returns false when the plan has none.
-int ensure_clusters(femk_plan* p, cudaStream_t s);
-bool launch_matfree_cl(const femk_plan* p, const double* param, int mode, double scale, const double* x, double* y,
-                       const CgState* st, cudaStream_t s);
-
 // Restarted GMRES (femk_gmres.cu) on the plan's prepared sliced-ELL operator (sell) or the canonical
 // CSR values; x holds x0 on entry and the solution on return.
 struct GmresInfo {
@@ -275,31 +251,6 @@ template <typename K>
 inline int vec_grid(K kernel, int threads, const femk_plan* p) {
   const int w = wave_grid(kernel, threads, p);
   return p->vec_blocks > 0 ? std::min(w, p->n_sm * p->vec_blocks) : w;
-}
-
-// Programmatic dependent launch: a kernel launched with launch_ex(pdl = true) may start while its
-// predecessor on the stream is still running; it must call pdl_wait() before touching anything the
-// predecessor writes (a no-op for a kernel launched without the attribute). pdl_trigger() lets the
-// next PDL-launched kernel begin launching.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
-// counted launch through cudaLaunchKernelEx, with the programmatic-serialization attribute when pdl
-template <typename... KArgs, typename... Args>
-inline cudaError_t launch_ex(bool pdl, void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t s,
-                             Args... args) {
-  counted_launch();
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)grid);
-  cfg.blockDim = dim3((unsigned)block);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = pdl ? 1 : 0;
-  return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

@@ -1,31 +1,38 @@
 // Mixed-precision Jacobi-PCG: FP32 values, vectors and SpMV accumulation in the inner CG; FP64
 // solution and FP64 true residual r = b - A x (FP64 values) at every reliable update.
 //
-// Inner step (FP32):  q = A32 p;  alpha = gamma / <p, q>;  e += alpha p;  r -= alpha q;  z = D^-1 r;
-//                     p = z + beta p
-// A reliable update is requested when <r, r> fell below delta^2 of its value at the previous
-// update, when the FP32 recurrence meets the stop test, or at the iteration cap. The iterations
-// left in the current chunk then return at entry, and the chunk ends with
-//     x += e;  e = 0;  r64 = b - A64 x;  r = fp32(r64);  z = D^-1 r;  gamma = <r, z>;  p = z + beta p
-// which keeps the search direction (FEMK_MIXED_RELIABLE, residual replacement) or restarts it
-// with beta = 0 (FEMK_MIXED_RESTART, classic iterative refinement). The solve stops only on the
-// FP64 true residual: <r64, r64> <= max(tol^2 <b, b>, atol^2) -- the stop rule of femk_pcg.
+// The inner iteration is preconditioned CG in the single-reduction form of Chronopoulos and Gear
+// (J. Comput. Appl. Math. 25, 1989): with u = D^-1 r, w = A u, s = A p,
 //
-// The FP32 operator is the plan's sliced-ELL copy: 4 B value + 2 B column offset (int16,
-// col - row) per entry when the bandwidth allows it, else 4 B + 4 B. Each chunk (16 iterations,
-// 3 kernels each, plus the 3 update kernels) is replayed as one CUDA graph.
+//   K_A  p = u + beta p;  s = w + beta s;  e += alpha p;  r -= alpha s;  u = D^-1 r
+//   K_B  w = A32 u;  gamma' = <r, u>,  delta = <w, u>,  rho = <r, r>       (one grid reduction)
+//        beta = gamma' / gamma;  alpha = gamma' / (delta - beta gamma' / alpha)
+//
+// Both inner products of an iteration come out of the SpMV's epilogue, so an iteration is two
+// kernels and one reduction (the textbook form needs three kernels and two reductions; the
+// denominator delta - beta gamma' / alpha equals <p, A p> in exact arithmetic).
+//
+// A reliable update is requested when rho fell below delta2 of its value at the previous update,
+// when the FP32 recurrence meets the stop test, or at the iteration cap. The iterations left in the
+// chunk then return at entry, and the chunk ends with
+//     x += e;  e = 0;  r64 = b - A64 x;  r = fp32(r64);  u = D^-1 r       (k_fold, k_true_resid)
+//     w = A32 u and the three products; beta = gamma'/gamma (0 to restart)  (K_B refresh)
+// which keeps the search direction (FEMK_MIXED_RELIABLE, residual replacement: p and s = A p are
+// unchanged) or restarts it (FEMK_MIXED_RESTART, classic iterative refinement). The solve stops
+// only on the FP64 true residual: <r64, r64> <= max(tol^2 <b, b>, atol^2), femk_pcg's stop rule.
+//
+// The FP32 operator is the plan's sliced-ELL copy: 4 B value + 2 B column offset (int16, col - row)
+// per entry when the bandwidth allows it, else 4 B + 4 B. Each chunk (16 iterations of 2 kernels,
+// plus the 3 update kernels) is replayed as one CUDA graph.
 //
 // No reference counterpart: jNO runs x64 throughout (tests/test_fem_3d.py:37-46).
 #include <algorithm>
 #include <cmath>
-#include <cstdlib>
 #include <type_traits>
 
 #include "femk_bulk.cuh"
-#include "femk_tile.cuh"
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
-#include "femk_grid.cuh"
 
 namespace femk {
 namespace {
@@ -34,31 +41,17 @@ constexpr int kThreads = 256;
 constexpr int kChunk = 16;
 
 struct MixedState {
-  double gamma, rr, rr64, bb, atol2, alpha, beta, rr_since, delta2;
+  double gamma;    // <r, u> of the current direction's residual
+  double gnew;     // <r, u> after a reliable update, waiting for the refresh step
+  double delta;    // <w, u>
+  double rr;       // FP32 recurrence <r, r>
+  double rr64, bb, atol2, alpha, beta, rr_since, delta2;
   int32_t iter, maxiter, done, status;
-  int32_t need_update;  // 1: update requested this chunk; 2: update done, direction pending
-  int32_t hold;         // iterations return at entry until the chunk-end update
+  int32_t need_update;  // 1: update requested this chunk; 2: update done, refresh step pending
+  int32_t hold;         // inner iterations return at entry until the refresh step
   int32_t outer, restart;
+  int32_t fresh;  // 1 until the first direction exists (beta = 0 at the first refresh)
   uint32_t ticket;
-  int32_t epend;  // split update: 1 while e += alpha p of the current iteration is still to be applied
-  int32_t par;    // fused form: the (z, p) pair buffer the next step reads (flipped by each update)
-};
-
-// Fused form of the inner iteration (two kernels instead of three): z and p live interleaved as
-// float2 pairs in two buffers. The step gathers the pairs of its columns and forms
-// p = fmaf(beta, p, z) on the fly (the arithmetic of k_pupdate32_x), writes each row's new p into
-// the other buffer, and the update kernel then applies e += alpha p, r -= alpha q and z = D^-1 r
-// on that buffer and flips the parity. Same iterates as the three-kernel split. Opt-in
-// (FEMK_MIXED_FUSE=1): measured on B200 at P1 128^3 (same box, same 513 inner iterations) 31.9 ms
-// per mixed solve against 25.7 ms for the split. The step is bound by gather latency and issue,
-// and 8-byte pair gathers plus the p store cost more than the kernel they save.
-struct GatherZP {
-  const float2* zp;
-  float beta;
-  __device__ __forceinline__ float operator()(int32_t j) const {
-    const float2 v = __ldg(zp + j);
-    return fmaf(beta, v.y, v.x);
-  }
 };
 
 template <int NV, int THREADS = kThreads>
@@ -137,427 +130,184 @@ __global__ void k_gather32(const int32_t* __restrict__ src, int64_t m, const dou
   }
 }
 
-__device__ __forceinline__ void finish_alpha(MixedState* st, double pq) {
-  st->alpha = st->gamma / pq;
-  st->need_update = 0;  // a pending direction update was applied before this step
-  if (!isfinite(pq)) {
+// K_B epilogue state: w[row] = (A u)[row] and the three products of the row
+struct StepEpi {
+  const float* __restrict__ u;
+  const float* __restrict__ r;
+  float* __restrict__ w;
+  float a[3];  // <w, u>, <r, u>, <r, r>
+  __device__ __forceinline__ void operator()(int64_t row, float wv) {
+    w[row] = wv;
+    const float ui = __ldg(u + row), ri = __ldg(r + row);
+    a[0] = fmaf(wv, ui, a[0]);
+    a[1] = fmaf(ri, ui, a[1]);
+    a[2] = fmaf(ri, ri, a[2]);
+  }
+};
+
+// Last block of K_B: the new scalars. REFRESH = the step after a reliable update (or the first one).
+template <bool REFRESH>
+__device__ __forceinline__ void step_finish(MixedState* st, const double (&t)[3]) {
+  const double delta = t[0], gnew = REFRESH ? st->gnew : t[1], rho = t[2];
+  st->delta = delta;
+  st->rr = rho;
+  if (!isfinite(delta) || !isfinite(gnew) || !isfinite(rho)) {
     st->status = FEMK_NONFINITE;
     st->done = 1;
-  } else if (!(pq > 0.0)) {
-    st->status = FEMK_BREAKDOWN;
+    return;
+  }
+  if (!REFRESH) {
+    st->iter += 1;
+    const bool conv = !(rho > st->atol2);
+    const bool drop = rho < st->delta2 * st->rr_since;
+    if (conv || drop || st->iter >= st->maxiter) {  // fold e into x and replace r at the chunk end
+      st->need_update = 1;
+      st->hold = 1;
+      return;
+    }
+  }
+  const double beta = (REFRESH && (st->restart || st->fresh)) ? 0.0 : gnew / st->gamma;
+  const double den = beta == 0.0 ? delta : delta - beta * gnew / st->alpha;  // <p, A p> of the new direction
+  if (!(den > 0.0)) {
+    st->status = isfinite(den) ? FEMK_BREAKDOWN : FEMK_NONFINITE;
     st->done = 1;
+    return;
+  }
+  st->beta = beta;
+  st->alpha = gnew / den;
+  st->gamma = gnew;
+  if (REFRESH) {
+    st->need_update = 0;
+    st->hold = 0;
+    st->fresh = 0;
   }
 }
 
-// q = A32 p, <p, q> -> alpha (sliced-ELL operator)
-template <typename IDX, int B>
+__device__ __forceinline__ bool step_skip(const MixedState* st, bool refresh) {
+  return st->done || (refresh ? st->need_update != 2 : st->hold != 0);
+}
+
+// K_B on the register-streamed sliced-ELL operator (one thread per row)
+template <typename IDX, bool REFRESH>
 __global__ void __launch_bounds__(kThreads, 8) k_step32_sell(const int64_t* __restrict__ sptr, const IDX* __restrict__ cols,
                                                          const float* __restrict__ vals, int64_t n, int64_t nslices,
-                                                         const float* __restrict__ p, float* __restrict__ q,
-                                                         double* __restrict__ partials, MixedState* st) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) st->epend = 0;  // the last e update is applied
-  if (st->done || st->hold) return;
+                                                         const float* __restrict__ u, const float* __restrict__ r,
+                                                         float* __restrict__ w, double* __restrict__ partials,
+                                                         MixedState* st) {
+  if (step_skip(st, REFRESH)) return;
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
-  float acc = 0.f;
+  StepEpi epi{u, r, w, {0.f, 0.f, 0.f}};
   for (int64_t sl = warp; sl < nslices; sl += nwarps) {
     const int64_t row = sl * 32 + lane;
     if (row >= n) continue;
     const int64_t b0 = __ldg(sptr + sl);
-    const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
-    const float sv =
-        sell_row<float, IDX, GatherX<float>, B>(vals + b0 + lane, cols + b0 + lane, w, (int32_t)row, GatherX<float>{p});
-    q[row] = sv;
-    acc = fmaf(__ldg(p + row), sv, acc);
+    const int32_t wd = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
+    epi(row, sell_row<float, IDX, GatherX<float>, 8>(vals + b0 + lane, cols + b0 + lane, wd, (int32_t)row,
+                                                     GatherX<float>{u}));
   }
-  double v[1] = {(double)acc}, tot[1];
-  if (!reduce_finish<1>(v, partials, &st->ticket, tot)) return;
+  double v[3] = {(double)epi.a[0], (double)epi.a[1], (double)epi.a[2]}, tot[3];
+  if (!reduce_finish<3>(v, partials, &st->ticket, tot)) return;
   if (threadIdx.x) return;
-  finish_alpha(st, tot[0]);
+  step_finish<REFRESH>(st, tot);
 }
 
-// The same step with the FP32 sliced-ELL stream moved into shared memory by bulk copies
-// (femk_bulk.cuh): WPB warps per block, S slices in flight per warp, widths up to WMAX.
-// K = 0 plain, 1 with L2 evict-last hints, 2 the fused form (p formed from the (z, p) pairs zp).
-template <int WMAX, int S, int WPB, int K>
+// K_B with the FP32 sliced-ELL stream moved into shared memory by bulk copies (femk_bulk.cuh):
+// WPB warps per block, S slices in flight per warp, widths up to WMAX.
+template <int WMAX, int S, int WPB, bool REFRESH>
 __global__ void __launch_bounds__(WPB * 32) k_step32_bulk(const int64_t* __restrict__ sptr,
                                                          const int16_t* __restrict__ cols,
                                                          const float* __restrict__ vals, int64_t n, int64_t nslices,
-                                                         const float* __restrict__ p, float* __restrict__ q,
-                                                         double* __restrict__ partials, MixedState* st,
-                                                         const int64_t* __restrict__ cptr, float2* __restrict__ zp,
-                                                         int64_t zs) {
-  constexpr bool H = K == 1;
+                                                         const float* __restrict__ u, const float* __restrict__ r,
+                                                         float* __restrict__ w, double* __restrict__ partials,
+                                                         MixedState* st, const int64_t* __restrict__ cptr) {
   extern __shared__ __align__(128) unsigned char bulk_smem[];
   constexpr int kWarpBytes = BulkRing<float, int16_t, WMAX, S>::kWarpBytes;
-  pdl_wait();
-  pdl_trigger();
-  if (blockIdx.x == 0 && threadIdx.x == 0) st->epend = 0;  // the last e update is applied
-  if (st->done || st->hold) return;
+  if (step_skip(st, REFRESH)) return;
   const int wib = threadIdx.x >> 5;
-  float acc = 0.f;
-  bool ok;
-  if constexpr (K == 2) {
-    const int par = st->par;
-    const float2* zc = zp + (int64_t)par * zs;
-    float2* zn = zp + (int64_t)(par ^ 1) * zs;
-    const GatherZP gz{zc, (float)st->beta};
-    ok = sell_bulk_rows<float, int16_t, WMAX, S>(
-        bulk_smem + wib * kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * WPB + wib,
-        (int64_t)gridDim.x * WPB, gz,
-        [&](int64_t row, float sv) {
-          const float pn = gz((int32_t)row);
-          zn[row].y = pn;
-          q[row] = sv;
-          acc = fmaf(pn, sv, acc);
-        },
-        &st->status, FEMK_TIMEOUT, cptr);
-  } else {
-    using G = std::conditional_t<H, GatherXL<float>, GatherX<float>>;
-    G gx;
-    gx.x = p;
-    if constexpr (H) gx.pol = l2_evict_last();
-    ok = sell_bulk_rows<float, int16_t, WMAX, S>(
-        bulk_smem + wib * kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * WPB + wib,
-        (int64_t)gridDim.x * WPB, gx,
-        [&](int64_t row, float sv) {
-          q[row] = sv;
-          acc = fmaf(__ldg(p + row), sv, acc);
-        },
-        &st->status, FEMK_TIMEOUT, cptr);
-  }
+  StepEpi epi{u, r, w, {0.f, 0.f, 0.f}};
+  const bool ok = sell_bulk_rows<float, int16_t, WMAX, S>(
+      bulk_smem + wib * kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * WPB + wib,
+      (int64_t)gridDim.x * WPB, GatherX<float>{u}, epi, &st->status, FEMK_TIMEOUT, cptr);
   if (!ok && (threadIdx.x & 31) == 0) st->done = 1;
-  double v[1] = {(double)acc}, tot[1];
-  if (!reduce_finish<1, WPB * 32>(v, partials, &st->ticket, tot)) return;
+  double v[3] = {(double)epi.a[0], (double)epi.a[1], (double)epi.a[2]}, tot[3];
+  if (!reduce_finish<3, WPB * 32>(v, partials, &st->ticket, tot)) return;
   if (threadIdx.x) return;
-  finish_alpha(st, tot[0]);
+  step_finish<REFRESH>(st, tot);
 }
 
-// The same step with matrix and p staged per tile in shared memory (femk_tile.cuh).
-template <int WMAX>
-__global__ void __launch_bounds__(kTileW * 32) k_step32_tile(const TileMeta* __restrict__ meta, int64_t ntiles,
-                                                            int xcap, const int64_t* __restrict__ sptr,
-                                                            const int64_t* __restrict__ cptr,
-                                                            const int16_t* __restrict__ slots,
-                                                            const float* __restrict__ vals, int64_t n,
-                                                            int64_t nslices, const float* __restrict__ p,
-                                                            float* __restrict__ q, double* __restrict__ partials,
-                                                            MixedState* st) {
-  extern __shared__ __align__(128) unsigned char tile_smem[];
-  if (blockIdx.x == 0 && threadIdx.x == 0) st->epend = 0;  // the last e update is applied
-  if (st->done || st->hold) return;
-  float acc = 0.f;
-  const bool ok = sell_tile_rows<float, kTileW, WMAX>(
-      tile_smem, xcap, meta, ntiles, sptr, cptr, slots, vals, p, n, nslices,
-      [&](int64_t row, float sv, float prow) {
-        q[row] = sv;
-        acc = fmaf(prow, sv, acc);
-      },
-      &st->status, FEMK_TIMEOUT);
-  if (!ok && threadIdx.x == 0) st->done = 1;
-  double v[1] = {(double)acc}, tot[1];
-  if (!reduce_finish<1, kTileW * 32>(v, partials, &st->ticket, tot)) return;
-  if (threadIdx.x) return;
-  finish_alpha(st, tot[0]);
-}
-
-// the same step on the CSR copy (plans without a sliced-ELL layout)
-template <int L, int U, typename IDX>
+// K_B on the CSR copy (plans without a sliced-ELL layout)
+template <int L, int U, typename IDX, bool REFRESH>
 __global__ void __launch_bounds__(kThreads) k_step32(const int32_t* __restrict__ indptr, const IDX* __restrict__ cols,
-                                                    const float* __restrict__ vals, int64_t n, const float* __restrict__ p,
-                                                    float* __restrict__ q, double* __restrict__ partials, MixedState* st) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) st->epend = 0;  // the last e update is applied
-  if (st->done || st->hold) return;
+                                                    const float* __restrict__ vals, int64_t n,
+                                                    const float* __restrict__ u, const float* __restrict__ r,
+                                                    float* __restrict__ w, double* __restrict__ partials,
+                                                    MixedState* st) {
+  if (step_skip(st, REFRESH)) return;
   const int lane = threadIdx.x & 31, sub = lane % L;
   const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
   constexpr int RPW = 32 / L;
-  float acc = 0.f;
+  StepEpi epi{u, r, w, {0.f, 0.f, 0.f}};
   for (int64_t base = warp * RPW * U; base < n; base += nwarps * RPW * U) {
     float sv[U];
     int64_t rows[U];
-    csr_rows<L, U, float, IDX>(indptr, cols, vals, p, n, base, lane, sv, rows);
+    csr_rows<L, U, float, IDX>(indptr, cols, vals, u, n, base, lane, sv, rows);
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (rows[u] >= n || sub != 0) continue;
-      q[rows[u]] = sv[u];
-      acc = fmaf(__ldg(p + rows[u]), sv[u], acc);
-    }
+    for (int k = 0; k < U; ++k)
+      if (rows[k] < n && sub == 0) epi(rows[k], sv[k]);
   }
-  double v[1] = {(double)acc}, tot[1];
-  if (!reduce_finish<1>(v, partials, &st->ticket, tot)) return;
+  double v[3] = {(double)epi.a[0], (double)epi.a[1], (double)epi.a[2]}, tot[3];
+  if (!reduce_finish<3>(v, partials, &st->ticket, tot)) return;
   if (threadIdx.x) return;
-  finish_alpha(st, tot[0]);
+  step_finish<REFRESH>(st, tot);
 }
 
-// e += alpha p; r -= alpha q; z = D^-1 r; <r, z>, <r, r>; request a reliable update or set beta.
-// All six vectors are plan-owned and 16-byte aligned: four rows per load.
-__global__ void __launch_bounds__(kThreads) k_update32(int64_t n, float* __restrict__ e, float* __restrict__ r,
-                                                      float* __restrict__ z, const float* __restrict__ p,
-                                                      const float* __restrict__ q, const float* __restrict__ dinv,
-                                                      double* __restrict__ partials, MixedState* st) {
+// K_A: p = u + beta p; s = w + beta s; e += alpha p; r -= alpha s; u = D^-1 r (no reduction).
+// All seven vectors are plan-owned and 16-byte aligned: four rows per load.
+__device__ __forceinline__ void cgcg_one(float alpha, float beta, float& u, float w, float& p, float& s, float& e,
+                                         float& r, float d) {
+  p = fmaf(beta, p, u);
+  s = fmaf(beta, s, w);
+  e = fmaf(alpha, p, e);
+  r = fmaf(-alpha, s, r);
+  u = d * r;
+}
+
+__global__ void __launch_bounds__(kThreads) k_cgcg_update(int64_t n, float* __restrict__ u, const float* __restrict__ w,
+                                                         float* __restrict__ p, float* __restrict__ s,
+                                                         float* __restrict__ e, float* __restrict__ r,
+                                                         const float* __restrict__ dinv, const MixedState* st) {
   if (st->done || st->hold) return;
-  const float alpha = (float)st->alpha;
-  float a0 = 0.f, a1 = 0.f;
-  const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
-  const int64_t nt = (int64_t)gridDim.x * kThreads;
-  const int64_t n4 = n >> 2;
-  float4* e4 = reinterpret_cast<float4*>(e);
-  float4* r4 = reinterpret_cast<float4*>(r);
-  float4* z4 = reinterpret_cast<float4*>(z);
-  const float4* p4 = reinterpret_cast<const float4*>(p);
-  const float4* q4 = reinterpret_cast<const float4*>(q);
-  const float4* d4 = reinterpret_cast<const float4*>(dinv);
-  for (int64_t i = tid; i < n4; i += nt) {
-    const float4 pi = p4[i], qi = q4[i], di = d4[i], ri0 = r4[i];
-    float4 ei = e4[i];
-    ei.x = fmaf(alpha, pi.x, ei.x);
-    ei.y = fmaf(alpha, pi.y, ei.y);
-    ei.z = fmaf(alpha, pi.z, ei.z);
-    ei.w = fmaf(alpha, pi.w, ei.w);
-    float4 ri, zi;
-    ri.x = fmaf(-alpha, qi.x, ri0.x);
-    ri.y = fmaf(-alpha, qi.y, ri0.y);
-    ri.z = fmaf(-alpha, qi.z, ri0.z);
-    ri.w = fmaf(-alpha, qi.w, ri0.w);
-    zi.x = di.x * ri.x;
-    zi.y = di.y * ri.y;
-    zi.z = di.z * ri.z;
-    zi.w = di.w * ri.w;
-    e4[i] = ei;
-    r4[i] = ri;
-    z4[i] = zi;
-    a0 = fmaf(ri.x, zi.x, fmaf(ri.y, zi.y, fmaf(ri.z, zi.z, fmaf(ri.w, zi.w, a0))));
-    a1 = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, fmaf(ri.z, ri.z, fmaf(ri.w, ri.w, a1))));
-  }
-  for (int64_t i = 4 * n4 + tid; i < n; i += nt) {
-    e[i] = fmaf(alpha, p[i], e[i]);
-    const float ri = fmaf(-alpha, q[i], r[i]);
-    const float zi = dinv[i] * ri;
-    r[i] = ri;
-    z[i] = zi;
-    a0 = fmaf(ri, zi, a0);
-    a1 = fmaf(ri, ri, a1);
-  }
-  double v[2] = {(double)a0, (double)a1}, tot[2];
-  if (!reduce_finish<2>(v, partials, &st->ticket, tot)) return;
-  if (threadIdx.x) return;
-  st->iter += 1;
-  st->rr = tot[1];
-  if (!isfinite(tot[0]) || !isfinite(tot[1])) {
-    st->status = FEMK_NONFINITE;
-    st->done = 1;
-    return;
-  }
-  const bool conv = !(tot[1] > st->atol2);
-  const bool drop = tot[1] < st->delta2 * st->rr_since;
-  if (conv || drop || st->iter >= st->maxiter) {
-    st->need_update = 1;
-    st->hold = 1;
-  } else {
-    st->beta = tot[0] / st->gamma;
-    st->gamma = tot[0];
-  }
-}
-
-// Split form of k_update32 + k_pupdate32<0> (same floating-point operations, z not stored):
-//   k_update32_r : r -= alpha q; <r, D^-1 r>, <r, r>; update request or beta   (reads r, q, D^-1)
-//   k_pupdate32_x: e += alpha p; p = D^-1 r + beta p (p only while not held)   (reads e, p, r, D^-1)
-// The iteration that requests a reliable update still owes its e update: k_update32_r raises
-// st->epend and the next step kernel clears it.
-template <bool H>
-__global__ void __launch_bounds__(kThreads) k_update32_r(int64_t n, float* __restrict__ r, const float* __restrict__ q,
-                                                        const float* __restrict__ dinv, double* __restrict__ partials,
-                                                        MixedState* st) {
-  pdl_wait();
-  pdl_trigger();
-  if (st->done || st->hold) return;
-  const float alpha = (float)st->alpha;
-  float a0 = 0.f, a1 = 0.f;
-  const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
-  const int64_t nt = (int64_t)gridDim.x * kThreads;
-  const int64_t n4 = n >> 2;
-  float4* r4 = reinterpret_cast<float4*>(r);
-  const float4* q4 = reinterpret_cast<const float4*>(q);
-  const float4* d4 = reinterpret_cast<const float4*>(dinv);
-  uint64_t pol = 0;
-  if (H) pol = l2_evict_last();
-  for (int64_t i = tid; i < n4; i += nt) {
-    const float4 qi = H ? ld_last4(q4 + i, pol) : q4[i];
-    const float4 di = H ? ld_last4(d4 + i, pol) : d4[i];
-    const float4 ri0 = H ? ld_last4(r4 + i, pol) : r4[i];
-    float4 ri, zi;
-    ri.x = fmaf(-alpha, qi.x, ri0.x);
-    ri.y = fmaf(-alpha, qi.y, ri0.y);
-    ri.z = fmaf(-alpha, qi.z, ri0.z);
-    ri.w = fmaf(-alpha, qi.w, ri0.w);
-    zi.x = di.x * ri.x;
-    zi.y = di.y * ri.y;
-    zi.z = di.z * ri.z;
-    zi.w = di.w * ri.w;
-    if (H)
-      st_last4(r4 + i, ri, pol);
-    else
-      r4[i] = ri;
-    a0 = fmaf(ri.x, zi.x, fmaf(ri.y, zi.y, fmaf(ri.z, zi.z, fmaf(ri.w, zi.w, a0))));
-    a1 = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, fmaf(ri.z, ri.z, fmaf(ri.w, ri.w, a1))));
-  }
-  for (int64_t i = 4 * n4 + tid; i < n; i += nt) {
-    const float ri = fmaf(-alpha, q[i], r[i]);
-    const float zi = dinv[i] * ri;
-    r[i] = ri;
-    a0 = fmaf(ri, zi, a0);
-    a1 = fmaf(ri, ri, a1);
-  }
-  double v[2] = {(double)a0, (double)a1}, tot[2];
-  if (!reduce_finish<2>(v, partials, &st->ticket, tot)) return;
-  if (threadIdx.x) return;
-  st->iter += 1;
-  st->rr = tot[1];
-  st->epend = 1;
-  if (!isfinite(tot[0]) || !isfinite(tot[1])) {
-    st->status = FEMK_NONFINITE;
-    st->done = 1;
-    return;
-  }
-  const bool conv = !(tot[1] > st->atol2);
-  const bool drop = tot[1] < st->delta2 * st->rr_since;
-  if (conv || drop || st->iter >= st->maxiter) {
-    st->need_update = 1;
-    st->hold = 1;
-  } else {
-    st->beta = tot[0] / st->gamma;
-    st->gamma = tot[0];
-  }
-}
-
-template <bool H>
-__global__ void __launch_bounds__(kThreads) k_pupdate32_x(int64_t n, float* __restrict__ e, float* __restrict__ p,
-                                                         const float* __restrict__ r, const float* __restrict__ dinv,
-                                                         const MixedState* st) {
-  pdl_wait();
-  pdl_trigger();
-  if (st->done || !st->epend) return;
-  const bool dir = !st->hold;
   const float alpha = (float)st->alpha, beta = (float)st->beta;
   const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
   const int64_t nt = (int64_t)gridDim.x * kThreads;
   const int64_t n4 = n >> 2;
-  float4* e4 = reinterpret_cast<float4*>(e);
+  float4* u4 = reinterpret_cast<float4*>(u);
+  const float4* w4 = reinterpret_cast<const float4*>(w);
   float4* p4 = reinterpret_cast<float4*>(p);
-  const float4* r4 = reinterpret_cast<const float4*>(r);
+  float4* s4 = reinterpret_cast<float4*>(s);
+  float4* e4 = reinterpret_cast<float4*>(e);
+  float4* r4 = reinterpret_cast<float4*>(r);
   const float4* d4 = reinterpret_cast<const float4*>(dinv);
-  uint64_t pol = 0;
-  if (H) pol = l2_evict_last();
-  auto ld = [&](const float4* a) { return H ? ld_last4(a, pol) : *a; };
-  auto st4 = [&](float4* a, float4 v) {
-    if (H)
-      st_last4(a, v, pol);
-    else
-      *a = v;
-  };
   for (int64_t i = tid; i < n4; i += nt) {
-    const float4 pi = ld(p4 + i);
-    float4 ei = ld(e4 + i);
-    ei.x = fmaf(alpha, pi.x, ei.x);
-    ei.y = fmaf(alpha, pi.y, ei.y);
-    ei.z = fmaf(alpha, pi.z, ei.z);
-    ei.w = fmaf(alpha, pi.w, ei.w);
-    st4(e4 + i, ei);
-    if (dir) {
-      const float4 ri = ld(r4 + i), di = ld(d4 + i);
-      st4(p4 + i, make_float4(fmaf(beta, pi.x, di.x * ri.x), fmaf(beta, pi.y, di.y * ri.y),
-                              fmaf(beta, pi.z, di.z * ri.z), fmaf(beta, pi.w, di.w * ri.w)));
-    }
+    float4 uu = u4[i], pp = p4[i], ss = s4[i], ee = e4[i], rr = r4[i];
+    const float4 ww = w4[i], dd = d4[i];
+    cgcg_one(alpha, beta, uu.x, ww.x, pp.x, ss.x, ee.x, rr.x, dd.x);
+    cgcg_one(alpha, beta, uu.y, ww.y, pp.y, ss.y, ee.y, rr.y, dd.y);
+    cgcg_one(alpha, beta, uu.z, ww.z, pp.z, ss.z, ee.z, rr.z, dd.z);
+    cgcg_one(alpha, beta, uu.w, ww.w, pp.w, ss.w, ee.w, rr.w, dd.w);
+    u4[i] = uu;
+    p4[i] = pp;
+    s4[i] = ss;
+    e4[i] = ee;
+    r4[i] = rr;
   }
-  for (int64_t i = 4 * n4 + tid; i < n; i += nt) {
-    const float pi = p[i];
-    e[i] = fmaf(alpha, pi, e[i]);
-    if (dir) p[i] = fmaf(beta, pi, dinv[i] * r[i]);
-  }
+  for (int64_t i = 4 * n4 + tid; i < n; i += nt) cgcg_one(alpha, beta, u[i], w[i], p[i], s[i], e[i], r[i], dinv[i]);
 }
 
 // x += e; e = 0 (only at a requested update)
-// Fused form, after the step: zn = the pair buffer the step wrote p into. e += alpha p;
-// r -= alpha q; z = D^-1 r into zn; <r, z>, <r, r>; request a reliable update or set beta; flip par.
-__global__ void __launch_bounds__(kThreads) k_update32_fz(int64_t n, float* __restrict__ r, const float* __restrict__ q,
-                                                         const float* __restrict__ dinv, float* __restrict__ e,
-                                                         float2* __restrict__ zp, int64_t zs,
-                                                         double* __restrict__ partials, MixedState* st) {
-  if (st->done || st->hold) return;
-  const float alpha = (float)st->alpha;
-  float2* zn = zp + (int64_t)(st->par ^ 1) * zs;
-  float a0 = 0.f, a1 = 0.f;
-  const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
-  const int64_t nt = (int64_t)gridDim.x * kThreads;
-  const int64_t n4 = n >> 2;
-  float4* r4 = reinterpret_cast<float4*>(r);
-  float4* e4 = reinterpret_cast<float4*>(e);
-  const float4* q4 = reinterpret_cast<const float4*>(q);
-  const float4* d4 = reinterpret_cast<const float4*>(dinv);
-  float4* zn4 = reinterpret_cast<float4*>(zn);  // two (z, p) pairs per float4
-  for (int64_t i = tid; i < n4; i += nt) {
-    const float4 qi = q4[i], di = d4[i], ri0 = r4[i];
-    float4 ei = e4[i];
-    float4 za = zn4[2 * i], zb = zn4[2 * i + 1];  // (z0, p0, z1, p1), (z2, p2, z3, p3)
-    ei.x = fmaf(alpha, za.y, ei.x);
-    ei.y = fmaf(alpha, za.w, ei.y);
-    ei.z = fmaf(alpha, zb.y, ei.z);
-    ei.w = fmaf(alpha, zb.w, ei.w);
-    float4 ri, zi;
-    ri.x = fmaf(-alpha, qi.x, ri0.x);
-    ri.y = fmaf(-alpha, qi.y, ri0.y);
-    ri.z = fmaf(-alpha, qi.z, ri0.z);
-    ri.w = fmaf(-alpha, qi.w, ri0.w);
-    zi.x = di.x * ri.x;
-    zi.y = di.y * ri.y;
-    zi.z = di.z * ri.z;
-    zi.w = di.w * ri.w;
-    za.x = zi.x;
-    za.z = zi.y;
-    zb.x = zi.z;
-    zb.z = zi.w;
-    e4[i] = ei;
-    r4[i] = ri;
-    zn4[2 * i] = za;
-    zn4[2 * i + 1] = zb;
-    a0 = fmaf(ri.x, zi.x, fmaf(ri.y, zi.y, fmaf(ri.z, zi.z, fmaf(ri.w, zi.w, a0))));
-    a1 = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, fmaf(ri.z, ri.z, fmaf(ri.w, ri.w, a1))));
-  }
-  for (int64_t i = 4 * n4 + tid; i < n; i += nt) {
-    float2 v = zn[i];
-    e[i] = fmaf(alpha, v.y, e[i]);
-    const float ri = fmaf(-alpha, q[i], r[i]);
-    const float zi = dinv[i] * ri;
-    r[i] = ri;
-    v.x = zi;
-    zn[i] = v;
-    a0 = fmaf(ri, zi, a0);
-    a1 = fmaf(ri, ri, a1);
-  }
-  double v[2] = {(double)a0, (double)a1}, tot[2];
-  if (!reduce_finish<2>(v, partials, &st->ticket, tot)) return;
-  if (threadIdx.x) return;
-  st->iter += 1;
-  st->rr = tot[1];
-  st->par ^= 1;  // the next step reads the pairs written here
-  if (!isfinite(tot[0]) || !isfinite(tot[1])) {
-    st->status = FEMK_NONFINITE;
-    st->done = 1;
-    return;
-  }
-  const bool conv = !(tot[1] > st->atol2);
-  const bool drop = tot[1] < st->delta2 * st->rr_since;
-  if (conv || drop || st->iter >= st->maxiter) {
-    st->need_update = 1;
-    st->hold = 1;
-  } else {
-    st->beta = tot[0] / st->gamma;
-    st->gamma = tot[0];
-  }
-}
-
 __global__ void k_fold(int64_t n, double* __restrict__ x, float* __restrict__ e, const MixedState* st) {
   if (st->done || st->need_update != 1) return;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -566,18 +316,16 @@ __global__ void k_fold(int64_t n, double* __restrict__ x, float* __restrict__ e,
   }
 }
 
-// r64 = b - A64 x; r = fp32(r64); z = D^-1 r; <r, z>, <r64, r64> (+ <b, b> and p = z at init)
+// r64 = b - A64 x; r = fp32(r64); u = D^-1 r; <r, u>, <r64, r64> (+ <b, b> at init)
 template <int L, int U, bool INIT>
 __global__ void __launch_bounds__(kThreads) k_true_resid(const int32_t* __restrict__ indptr,
                                                         const int32_t* __restrict__ indices,
                                                         const double* __restrict__ vals, int64_t n,
                                                         const double* __restrict__ x, const double* __restrict__ b,
                                                         const float* __restrict__ dinv, float* __restrict__ r,
-                                                        float* __restrict__ z, float* __restrict__ p,
-                                                        double* __restrict__ partials, MixedState* st, double tol2,
-                                                        double atol2, float2* __restrict__ zp, int64_t zs) {
+                                                        float* __restrict__ u, double* __restrict__ partials,
+                                                        MixedState* st, double tol2, double atol2) {
   if (!INIT && (st->done || st->need_update != 1)) return;
-  float2* zc = zp ? zp + (int64_t)st->par * zs : nullptr;  // fused form: z into the pairs the next step reads
   const int lane = threadIdx.x & 31, sub = lane % L;
   const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
@@ -588,23 +336,16 @@ __global__ void __launch_bounds__(kThreads) k_true_resid(const int32_t* __restri
     int64_t rows[U];
     csr_rows<L, U, double, int32_t>(indptr, indices, vals, x, n, base, lane, sv, rows);
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int64_t row = rows[u];
+    for (int k = 0; k < U; ++k) {
+      const int64_t row = rows[k];
       if (row >= n || sub != 0) continue;
       const double bi = b[row];
-      const double r64 = bi - sv[u];
+      const double r64 = bi - sv[k];
       const float rf = (float)r64;
-      const float zf = dinv[row] * rf;
+      const float uf = dinv[row] * rf;
       r[row] = rf;
-      z[row] = zf;
-      if (INIT) p[row] = zf;
-      if (zc) {
-        if (INIT)
-          zc[row] = make_float2(zf, 0.f);  // beta = 0 at the start: the first step's p is z
-        else
-          zc[row].x = zf;
-      }
-      a0 += (double)rf * (double)zf;
+      u[row] = uf;
+      a0 += (double)rf * (double)uf;
       a1 += r64 * r64;
       if (INIT) a2 += bi * bi;
     }
@@ -618,226 +359,38 @@ __global__ void __launch_bounds__(kThreads) k_true_resid(const int32_t* __restri
   if (INIT) {
     st->bb = tot[2];
     st->atol2 = fmax(tol2 * tot[2], atol2);
-    st->gamma = tot[0];
     st->iter = 0;
-    st->need_update = 0;
-    st->hold = 0;
-    st->epend = 0;
+    st->fresh = 1;
     st->status = isfinite(tot[0]) && isfinite(tot[1]) ? FEMK_OK : FEMK_NONFINITE;
     st->done = (!(tot[1] > st->atol2) || st->maxiter <= 0 || st->status != FEMK_OK) ? 1 : 0;
-    return;
-  }
-  if (!isfinite(tot[0]) || !isfinite(tot[1])) {
+  } else if (!isfinite(tot[0]) || !isfinite(tot[1])) {
     st->status = FEMK_NONFINITE;
     st->done = 1;
     return;
-  }
-  if (!(tot[1] > st->atol2) || st->iter >= st->maxiter) {
+  } else if (!(tot[1] > st->atol2) || st->iter >= st->maxiter) {
     st->done = 1;
     return;
   }
-  st->beta = st->restart ? 0.0 : tot[0] / st->gamma;
-  st->gamma = tot[0];
-  st->need_update = 2;
-  st->hold = 0;
-}
-
-// p = z + beta p: every iteration (MODE 0, skipped while held) or after a chunk-end update (MODE 1)
-template <int MODE>
-__global__ void k_pupdate32(int64_t n, float* __restrict__ p, const float* __restrict__ z, const MixedState* st) {
-  if (st->done) return;
-  if (MODE == 0 && st->hold) return;
-  if (MODE == 1 && st->need_update != 2) return;
-  const float beta = (float)st->beta;
-  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t nt = (int64_t)gridDim.x * blockDim.x;
-  const int64_t n4 = n >> 2;
-  float4* p4 = reinterpret_cast<float4*>(p);
-  const float4* z4 = reinterpret_cast<const float4*>(z);
-  for (int64_t i = tid; i < n4; i += nt) {
-    const float4 a = p4[i], c = z4[i];
-    p4[i] = make_float4(fmaf(beta, a.x, c.x), fmaf(beta, a.y, c.y), fmaf(beta, a.z, c.z), fmaf(beta, a.w, c.w));
-  }
-  for (int64_t i = 4 * n4 + tid; i < n; i += nt) p[i] = fmaf(beta, p[i], z[i]);
-}
-
-// ---------------------------------------------------------------------------------------------
-// Persistent form: the whole mixed solve in one cooperative launch. Phases per inner iteration:
-// A (q = A32 p, <p, q>), B (e, r, z updates, <r, z>, <r, r>, update decision), C (p = z + beta p);
-// on a reliable update two more phases run between B and C: U1 (x += e) and U2 (the FP64 true
-// residual on the FP64 sliced-ELL values). Vectors written by other blocks earlier in the launch
-// are read through L2 (__ldcg).
-// ---------------------------------------------------------------------------------------------
-constexpr int kPersistThreads = 512;
-
-template <typename IDX>
-__global__ void __launch_bounds__(kPersistThreads, 2)
-    k_mixed_persist(const int64_t* __restrict__ sptr, const IDX* __restrict__ scols, const float* __restrict__ sv32,
-                    const double* __restrict__ sv64, int64_t n, int64_t nslices, const double* __restrict__ b,
-                    double* __restrict__ x, const float* __restrict__ dinv, float* __restrict__ r,
-                    float* __restrict__ z, float* __restrict__ pv, float* __restrict__ q, float* __restrict__ e,
-                    double* __restrict__ partials, MixedState* st, GridBar* bar) {
-  if (st->done) return;
-  double gamma = st->gamma, rr_since = st->rr_since, rr64 = st->rr64, rr = st->rr;
-  const double atol2 = st->atol2, delta2 = st->delta2;
-  const int maxiter = st->maxiter, restart = st->restart;
-  int iter = st->iter, outer = st->outer, status = FEMK_OK;
-  unsigned int gen = 0;
-  const int G = gridDim.x;
-  double* P1 = partials;
-  double* P2 = partials + G;
-  double* P3 = partials + 3 * G;
-  const int lane = threadIdx.x & 31;
-  const int64_t gwarp = (blockIdx.x * (int64_t)kPersistThreads + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)G * kPersistThreads) >> 5;
-  const int64_t gtid = blockIdx.x * (int64_t)kPersistThreads + threadIdx.x;
-  const int64_t nthr = (int64_t)G * kPersistThreads;
-  while (true) {
-    // A: q = A32 p, <p, q>
-    float acc = 0.f;
-    for (int64_t sl = gwarp; sl < nslices; sl += nwarps) {
-      const int64_t row = sl * 32 + lane;
-      if (row >= n) continue;
-      const int64_t b0 = __ldg(sptr + sl);
-      const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
-      const float s32 = sell_row(sv32 + b0 + lane, scols + b0 + lane, w, (int32_t)row, GatherXcg<float>{pv});
-      q[row] = s32;
-      acc = fmaf(__ldcg(pv + row), s32, acc);
-    }
-    double a1[1] = {(double)acc};
-    block_partials<1, kPersistThreads>(a1, P1);
-    if (!grid_sync(bar, gen)) {
-      status = FEMK_TIMEOUT;
-      break;
-    }
-    double pq[1];
-    grid_totals<1>(P1, pq);
-    if (!isfinite(pq[0])) {
-      status = FEMK_NONFINITE;
-      break;
-    }
-    if (!(pq[0] > 0.0)) {
-      status = FEMK_BREAKDOWN;
-      break;
-    }
-    const float falpha = (float)(gamma / pq[0]);
-    // B: e += alpha p; r -= alpha q; z = D^-1 r; <r, z>, <r, r>
-    float f0 = 0.f, f1 = 0.f;
-    for (int64_t i = gtid; i < n; i += nthr) {
-      e[i] = fmaf(falpha, __ldcg(pv + i), e[i]);
-      const float ri = fmaf(-falpha, __ldcg(q + i), __ldcg(r + i));
-      const float zi = dinv[i] * ri;
-      r[i] = ri;
-      z[i] = zi;
-      f0 = fmaf(ri, zi, f0);
-      f1 = fmaf(ri, ri, f1);
-    }
-    double a2[2] = {(double)f0, (double)f1};
-    block_partials<2, kPersistThreads>(a2, P2);
-    if (!grid_sync(bar, gen)) {
-      status = FEMK_TIMEOUT;
-      break;
-    }
-    double t2[2];
-    grid_totals<2>(P2, t2);
-    ++iter;
-    rr = t2[1];
-    if (!isfinite(t2[0]) || !isfinite(t2[1])) {
-      status = FEMK_NONFINITE;
-      break;
-    }
-    const bool cap = iter >= maxiter;
-    double beta;
-    if (!(t2[1] > atol2) || t2[1] < delta2 * rr_since || cap) {
-      // U1: x += e; e = 0
-      for (int64_t i = gtid; i < n; i += nthr) {
-        x[i] += (double)e[i];
-        e[i] = 0.f;
-      }
-      if (!grid_sync(bar, gen)) {
-        status = FEMK_TIMEOUT;
-        break;
-      }
-      // U2: r64 = b - A64 x; r = fp32(r64); z = D^-1 r; <r, z>, <r64, r64>
-      double d[2] = {0.0, 0.0};
-      for (int64_t sl = gwarp; sl < nslices; sl += nwarps) {
-        const int64_t row = sl * 32 + lane;
-        if (row >= n) continue;
-        const int64_t b0 = __ldg(sptr + sl);
-        const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
-        const double s64 = sell_row(sv64 + b0 + lane, scols + b0 + lane, w, (int32_t)row, GatherXcg<double>{x});
-        const double r64 = b[row] - s64;
-        const float rf = (float)r64;
-        const float zf = dinv[row] * rf;
-        r[row] = rf;
-        z[row] = zf;
-        d[0] += (double)rf * (double)zf;
-        d[1] += r64 * r64;
-      }
-      block_partials<2, kPersistThreads>(d, P3);
-      if (!grid_sync(bar, gen)) {
-        status = FEMK_TIMEOUT;
-        break;
-      }
-      double t3[2];
-      grid_totals<2>(P3, t3);
-      ++outer;
-      rr64 = t3[1];
-      rr_since = t3[1];
-      if (!isfinite(t3[0]) || !isfinite(t3[1])) {
-        status = FEMK_NONFINITE;
-        break;
-      }
-      if (!(t3[1] > atol2) || cap) break;
-      beta = restart ? 0.0 : t3[0] / gamma;
-      gamma = t3[0];
-    } else {
-      beta = t2[0] / gamma;
-      gamma = t2[0];
-    }
-    // C: p = z + beta p
-    const float fbeta = (float)beta;
-    for (int64_t i = gtid; i < n; i += nthr) pv[i] = fmaf(fbeta, __ldcg(pv + i), __ldcg(z + i));
-    if (!grid_sync(bar, gen)) {
-      status = FEMK_TIMEOUT;
-      break;
-    }
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    st->iter = iter;
-    st->outer = outer;
-    st->gamma = gamma;
-    st->rr = rr;
-    st->rr64 = rr64;
-    st->status = status;
-    st->done = 1;
-  }
-}
-
-__global__ void k_gather64(const int32_t* __restrict__ src, int64_t m, const double* __restrict__ vals,
-                           double* __restrict__ out) {
-  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t k = __ldcs(src + j);
-    out[j] = k >= 0 ? __ldcs(vals + k) : 0.0;
-  }
+  st->gnew = tot[0];
+  st->need_update = 2;  // the refresh step forms w = A u, beta and alpha
+  st->hold = 1;
 }
 
 template <bool INIT>
 void launch_true_resid(const femk_plan* p, const double* vals, const double* x, const double* b, const float* dinv,
-                       float* r, float* z, float* pv, MixedState* st, double tol2, double atol2, cudaStream_t s,
-                       float2* zp = nullptr) {
+                       float* r, float* u, MixedState* st, double tol2, double atol2, cudaStream_t s) {
   with_spmv_cfg(p->spmv_L, p->spmv_U, [&](auto Lc, auto Uc) {
     constexpr int L = decltype(Lc)::value, U = decltype(Uc)::value;
     const int grid = wave_grid(k_true_resid<L, U, INIT>, kThreads, p);
     k_true_resid<L, U, INIT><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
-        p->indptr, p->indices, vals, p->n, x, b, dinv, r, z, pv, p->partials, st, tol2, atol2, zp, p->vstride);
+        p->indptr, p->indices, vals, p->n, x, b, dinv, r, u, p->partials, st, tol2, atol2);
   });
 }
 
-template <int S, int WPB, int WMAX, int K>
-bool launch_step32_bulk_h(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
-                          bool prime) {
-  auto kern = k_step32_bulk<WMAX, S, WPB, K>;
+template <int S, int WPB, int WMAX, bool REFRESH>
+bool launch_step32_bulk_cfg(const femk_plan* p, const float* u, const float* r, float* w, MixedState* st,
+                            cudaStream_t s, bool prime) {
+  auto kern = k_step32_bulk<WMAX, S, WPB, REFRESH>;
   constexpr int kSmem = WPB * BulkRing<float, int16_t, WMAX, S>::kWarpBytes;
   static int per_sm = -1;  // per instantiation: opt-in shared memory size + occupancy, queried once
   if (per_sm < 0) {
@@ -851,44 +404,32 @@ bool launch_step32_bulk_h(const femk_plan* p, const float* pv, float* q, MixedSt
   if (prime) return true;
   const int grid = p->n_sm * std::min(per_sm, 16);
   const bool tab = p->sell_cu != nullptr;  // per-slice column tables (shared-offset slices stored once)
-  (void)launch_ex(p->pdl != 0, kern, grid, WPB * 32, kSmem, s, (const int64_t*)p->sell_ptr,
-                  (const int16_t*)(tab ? p->sell_cu : p->sell_c16), (const float*)p->sell_vals32, p->n, p->n_slices,
-                  pv, q, p->partials, st, (const int64_t*)(tab ? p->sell_cuptr : nullptr), (float2*)p->mx_zp,
-                  p->vstride);
+  kern<<<::femk::counted_launch() + grid, WPB * 32, kSmem, s>>>(
+      (const int64_t*)p->sell_ptr, (const int16_t*)(tab ? p->sell_cu : p->sell_c16), (const float*)p->sell_vals32,
+      p->n, p->n_slices, u, r, w, p->partials, st, (const int64_t*)(tab ? p->sell_cuptr : nullptr));
   return true;
 }
 
-template <int S, int WPB, int WMAX>
-bool launch_step32_bulk_cfg(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
-                            bool prime) {
-  if (p->mx_fz_on) return launch_step32_bulk_h<S, WPB, WMAX, 2>(p, pv, q, st, s, prime);
-  return p->l2_mode32 != 0 ? launch_step32_bulk_h<S, WPB, WMAX, 1>(p, pv, q, st, s, prime)
-                           : launch_step32_bulk_h<S, WPB, WMAX, 0>(p, pv, q, st, s, prime);
-}
-
-// bulk-copy FP32 step in the plan's configuration (bulk32_cfg: 10 * stages + warps per block)
+// bulk-copy K_B in the plan's configuration (bulk32_cfg: 10 * stages + warps per block)
 // prime = true only sets the kernel attribute and reads the occupancy (before a graph capture)
-bool launch_step32_bulk(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
+template <bool REFRESH>
+bool launch_step32_bulk(const femk_plan* p, const float* u, const float* r, float* w, MixedState* st, cudaStream_t s,
                         bool prime = false) {
   if (!p->bulk32_cfg || !p->sell_vals32 || !p->sell_c16 || p->max_row > 32) return false;
   if (((uintptr_t)p->sell_vals32 & 15u) || ((uintptr_t)p->sell_c16 & 15u)) return false;
   if (p->sell_cu && ((uintptr_t)p->sell_cu & 15u)) return false;
   // ring stages sized for the widest row: 8 (2-D P1 triangles), 16 (P1 tetrahedra), 32
   const int wsel = p->max_row <= 8 ? 8 : (p->max_row <= 16 ? 16 : 32);
-#define FEMK_BULK_CFG(code, S, WPB)                                                          \
-  case code:                                                                                 \
-    return wsel == 8    ? launch_step32_bulk_cfg<S, WPB, 8>(p, pv, q, st, s, prime)  \
-           : wsel == 16 ? launch_step32_bulk_cfg<S, WPB, 16>(p, pv, q, st, s, prime) \
-                        : launch_step32_bulk_cfg<S, WPB, 32>(p, pv, q, st, s, prime);
+#define FEMK_BULK_CFG(code, S, WPB)                                                                     \
+  case code:                                                                                            \
+    return wsel == 8    ? launch_step32_bulk_cfg<S, WPB, 8, REFRESH>(p, u, r, w, st, s, prime)  \
+           : wsel == 16 ? launch_step32_bulk_cfg<S, WPB, 16, REFRESH>(p, u, r, w, st, s, prime) \
+                        : launch_step32_bulk_cfg<S, WPB, 32, REFRESH>(p, u, r, w, st, s, prime);
   switch (p->bulk32_cfg) {
-    FEMK_BULK_CFG(11, 1, 1)
-    FEMK_BULK_CFG(12, 1, 2)
     FEMK_BULK_CFG(14, 1, 4)
     FEMK_BULK_CFG(18, 1, 8)
-    FEMK_BULK_CFG(22, 2, 2)
     FEMK_BULK_CFG(24, 2, 4)
     FEMK_BULK_CFG(28, 2, 8)
-    FEMK_BULK_CFG(34, 3, 4)
     FEMK_BULK_CFG(38, 3, 8)
     default:
       return false;
@@ -896,73 +437,57 @@ bool launch_step32_bulk(const femk_plan* p, const float* pv, float* q, MixedStat
 #undef FEMK_BULK_CFG
 }
 
-template <int WMAX>
-bool launch_step32_tile_w(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
-                          bool prime) {
-  auto kern = k_step32_tile<WMAX>;
-  static int attr_ok = -1;  // per instantiation: opt in to the largest stage size once
-  if (attr_ok < 0) {
-    const int most = 2 * TileStage<float, kTileW, WMAX>::bytes(4096) + 16;
-    attr_ok = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, most) == cudaSuccess;
-    if (!attr_ok) cudaGetLastError();
-  }
-  if (!attr_ok) return false;
-  const int smem = 2 * TileStage<float, kTileW, WMAX>::bytes(p->tile_xcap) + 16;
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileW * 32, smem) != cudaSuccess || per_sm <= 0) {
-    cudaGetLastError();
-    return false;
-  }
-  if (prime) return true;
-  const int grid = (int)std::min<int64_t>(p->ntiles, (int64_t)p->n_sm * std::min(per_sm, 16));
-  kern<<<::femk::counted_launch() + grid, kTileW * 32, smem, s>>>(
-      (const TileMeta*)p->tile_meta, p->ntiles, p->tile_xcap, p->sell_ptr, p->sell_cuptr, p->tile_slots,
-      p->sell_vals32, p->n, p->n_slices, pv, q, p->partials, st);
-  return true;
-}
-
-// staged-x FP32 step when the plan built its tiles; false: nothing launched
-bool launch_step32_tile(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s,
-                        bool prime = false) {
-  if (!p->tile_ok || !p->tile32 || !p->sell_vals32 || ((uintptr_t)p->sell_vals32 & 15u) || ((uintptr_t)pv & 15u))
-    return false;
-  return p->max_row <= 16 ? launch_step32_tile_w<16>(p, pv, q, st, s, prime)
-                          : launch_step32_tile_w<32>(p, pv, q, st, s, prime);
-}
-
-void launch_step32(const femk_plan* p, const float* pv, float* q, MixedState* st, cudaStream_t s) {
-  if (launch_step32_tile(p, pv, q, st, s)) return;
-  if (launch_step32_bulk(p, pv, q, st, s)) return;
+template <bool REFRESH>
+void launch_step32(const femk_plan* p, const float* u, const float* r, float* w, MixedState* st, cudaStream_t s) {
+  if (launch_step32_bulk<REFRESH>(p, u, r, w, st, s)) return;
   if (p->sell_vals32) {
-    auto go = [&](auto Bc) {
-      constexpr int B = decltype(Bc)::value;
-      if (p->sell_c16) {
-        k_step32_sell<int16_t, B><<<::femk::counted_launch() + wave_grid(k_step32_sell<int16_t, B>, kThreads, p),
-                                    kThreads, 0, s>>>(p->sell_ptr, p->sell_c16, p->sell_vals32, p->n, p->n_slices, pv,
-                                                      q, p->partials, st);
-      } else {
-        k_step32_sell<int32_t, B><<<::femk::counted_launch() + wave_grid(k_step32_sell<int32_t, B>, kThreads, p),
-                                    kThreads, 0, s>>>(p->sell_ptr, p->sell_cols, p->sell_vals32, p->n, p->n_slices,
-                                                      pv, q, p->partials, st);
-      }
-    };
-    go(std::integral_constant<int, 8>{});
+    if (p->sell_c16) {
+      auto k = k_step32_sell<int16_t, REFRESH>;
+      k<<<::femk::counted_launch() + wave_grid(k, kThreads, p), kThreads, 0, s>>>(
+          p->sell_ptr, p->sell_c16, p->sell_vals32, p->n, p->n_slices, u, r, w, p->partials, st);
+    } else {
+      auto k = k_step32_sell<int32_t, REFRESH>;
+      k<<<::femk::counted_launch() + wave_grid(k, kThreads, p), kThreads, 0, s>>>(
+          p->sell_ptr, p->sell_cols, p->sell_vals32, p->n, p->n_slices, u, r, w, p->partials, st);
+    }
     return;
   }
   with_spmv_cfg(p->spmv_L, p->spmv_U, [&](auto Lc, auto Uc) {
     constexpr int L = decltype(Lc)::value, U = decltype(Uc)::value;
     if (p->cols16) {
-      k_step32<L, U, int16_t><<<::femk::counted_launch() + wave_grid(k_step32<L, U, int16_t>, kThreads, p), kThreads,
-                                0, s>>>(p->indptr, p->cols16, p->vals32, p->n, pv, q, p->partials, st);
+      auto k = k_step32<L, U, int16_t, REFRESH>;
+      k<<<::femk::counted_launch() + wave_grid(k, kThreads, p), kThreads, 0, s>>>(p->indptr, p->cols16, p->vals32,
+                                                                                  p->n, u, r, w, p->partials, st);
     } else {
-      k_step32<L, U, int32_t><<<::femk::counted_launch() + wave_grid(k_step32<L, U, int32_t>, kThreads, p), kThreads,
-                                0, s>>>(p->indptr, p->indices, p->vals32, p->n, pv, q, p->partials, st);
+      auto k = k_step32<L, U, int32_t, REFRESH>;
+      k<<<::femk::counted_launch() + wave_grid(k, kThreads, p), kThreads, 0, s>>>(p->indptr, p->indices, p->vals32,
+                                                                                  p->n, u, r, w, p->partials, st);
     }
   });
 }
 
+// occupancy queries and shared-memory attributes of every kernel a chunk may launch (before capture)
+void prime_mixed(const femk_plan* p) {
+  with_spmv_cfg(p->spmv_L, p->spmv_U, [&](auto Lc, auto Uc) {
+    constexpr int L = decltype(Lc)::value, U = decltype(Uc)::value;
+    (void)wave_grid(k_true_resid<L, U, false>, kThreads, p);
+    (void)wave_grid(k_step32<L, U, int16_t, false>, kThreads, p);
+    (void)wave_grid(k_step32<L, U, int32_t, false>, kThreads, p);
+    (void)wave_grid(k_step32<L, U, int16_t, true>, kThreads, p);
+    (void)wave_grid(k_step32<L, U, int32_t, true>, kThreads, p);
+  });
+  (void)wave_grid(k_step32_sell<int16_t, false>, kThreads, p);
+  (void)wave_grid(k_step32_sell<int32_t, false>, kThreads, p);
+  (void)wave_grid(k_step32_sell<int16_t, true>, kThreads, p);
+  (void)wave_grid(k_step32_sell<int32_t, true>, kThreads, p);
+  (void)launch_step32_bulk<false>(p, nullptr, nullptr, nullptr, nullptr, nullptr, true);
+  (void)launch_step32_bulk<true>(p, nullptr, nullptr, nullptr, nullptr, nullptr, true);
+  (void)vec_grid(k_cgcg_update, kThreads, p);
+  (void)wave_grid(k_fold, 256, p);
+}
+
 struct MixedPtrs {
-  float *r, *z, *pv, *q, *e, *d32;
+  float *r, *u, *w, *pv, *s, *e, *d32;
   MixedState* st;
 };
 
@@ -970,61 +495,37 @@ MixedPtrs mixed_ptrs(const femk_plan* p) {
   const int64_t vs = p->vstride;
   MixedPtrs m;
   m.r = p->work32;
-  m.z = m.r + vs;
-  m.pv = m.z + vs;
-  m.q = m.pv + vs;
-  m.e = m.q + vs;
+  m.u = m.r + vs;
+  m.w = m.u + vs;
+  m.pv = m.w + vs;
+  m.s = m.pv + vs;
+  m.e = m.s + vs;
   m.d32 = m.e + vs;
   m.st = (MixedState*)p->work64b;
   return m;
 }
 
-// one chunk: kChunk inner iterations, then the (conditional) reliable update
+// one chunk: kChunk inner iterations, then the (conditional) reliable update and refresh step
 int enqueue_mixed_chunk(const femk_plan* p, const double* vals, const double* b, double* x, cudaStream_t s) {
   const MixedPtrs m = mixed_ptrs(p);
   const int64_t n = p->n;
-  if (p->mx_fz_on) {  // fused form: step (p formed on the fly) + one update kernel per iteration
-    float2* zp = (float2*)p->mx_zp;
-    for (int it = 0; it < kChunk; ++it) {
-      launch_step32(p, m.pv, m.q, m.st, s);
-      (void)launch_ex(p->pdl != 0, k_update32_fz, vec_grid(k_update32_fz, kThreads, p), kThreads, 0, s, n, m.r,
-                      (const float*)m.q, (const float*)m.d32, m.e, zp, p->vstride, p->partials, m.st);
-    }
-    k_fold<<<::femk::counted_launch() + wave_grid(k_fold, 256, p), 256, 0, s>>>(n, x, m.e, m.st);
-    launch_true_resid<false>(p, vals, x, b, m.d32, m.r, m.z, nullptr, m.st, 0.0, 0.0, s, zp);
-    FEMK_CUDA_TRY(cudaGetLastError());
-    return FEMK_OK;
-  }
   for (int it = 0; it < kChunk; ++it) {
-    launch_step32(p, m.pv, m.q, m.st, s);
-    if (p->cg_split) {
-      auto ku = p->l2_mode32 != 0 ? k_update32_r<true> : k_update32_r<false>;
-      auto kp = p->l2_mode32 != 0 ? k_pupdate32_x<true> : k_pupdate32_x<false>;
-      (void)launch_ex(p->pdl != 0, ku, vec_grid(ku, kThreads, p), kThreads, 0, s, n, m.r, (const float*)m.q,
-                      (const float*)m.d32, p->partials, m.st);
-      (void)launch_ex(p->pdl != 0, kp, vec_grid(kp, kThreads, p), kThreads, 0, s, n, m.e, m.pv, (const float*)m.r,
-                      (const float*)m.d32, (const MixedState*)m.st);
-    } else {
-      k_update32<<<::femk::counted_launch() + wave_grid(k_update32, kThreads, p), kThreads, 0, s>>>(
-          n, m.e, m.r, m.z, m.pv, m.q, m.d32, p->partials, m.st);
-      k_pupdate32<0><<<::femk::counted_launch() + wave_grid(k_pupdate32<0>, 256, p), 256, 0, s>>>(n, m.pv, m.z,
-                                                                                                   m.st);
-    }
+    k_cgcg_update<<<::femk::counted_launch() + vec_grid(k_cgcg_update, kThreads, p), kThreads, 0, s>>>(
+        n, m.u, m.w, m.pv, m.s, m.e, m.r, m.d32, m.st);
+    launch_step32<false>(p, m.u, m.r, m.w, m.st, s);
   }
   k_fold<<<::femk::counted_launch() + wave_grid(k_fold, 256, p), 256, 0, s>>>(n, x, m.e, m.st);
-  launch_true_resid<false>(p, vals, x, b, m.d32, m.r, m.z, nullptr, m.st, 0.0, 0.0, s);
-  k_pupdate32<1><<<::femk::counted_launch() + wave_grid(k_pupdate32<1>, 256, p), 256, 0, s>>>(n, m.pv, m.z, m.st);
+  launch_true_resid<false>(p, vals, x, b, m.d32, m.r, m.u, m.st, 0.0, 0.0, s);
+  launch_step32<true>(p, m.u, m.r, m.w, m.st, s);
   FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;
 }
 
 int ensure_mixed(femk_plan* p) {
   FEMK_TRY(ensure_workspace(p));
-  if (!p->work32) FEMK_CUDA_TRY(cudaMalloc(&p->work32, sizeof(float) * 6 * p->vstride));
+  if (!p->work32) FEMK_CUDA_TRY(cudaMalloc(&p->work32, sizeof(float) * kWork32Vectors * p->vstride));
   if (p->use_sell && p->sell_src) {
     if (!p->sell_vals32) FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals32, sizeof(float) * (p->sell_nnz + 1)));
-    if (p->cg_persist && p->coop && !p->sell_vals)
-      FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals, sizeof(double) * (p->sell_nnz + 1)));
   } else if (!p->vals32) {
     FEMK_CUDA_TRY(cudaMalloc(&p->vals32, sizeof(float) * (p->nnz + 1)));
   }
@@ -1043,33 +544,11 @@ int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double
     set_error("femk_pcg_mixed: workspace missing at graph capture");
     return FEMK_EINVAL;
   }
-  const void* key[5] = {vals, b, x, p->sell_vals32 ? (const void*)p->sell_vals32 : (const void*)p->vals32,
-                        (const void*)(uintptr_t)(p->mx_fz_on ? 1 : 0)};
+  const void* key[5] = {vals, b, x, p->sell_vals32 ? (const void*)p->sell_vals32 : (const void*)p->vals32, nullptr};
   bool same = p->mx_exec != nullptr;
   for (int i = 0; i < 5; ++i) same = same && key[i] == p->mx_key[i];
   if (same) return FEMK_OK;
-  // occupancy queries happen before capture begins
-  with_spmv_cfg(p->spmv_L, p->spmv_U, [&](auto Lc, auto Uc) {
-    constexpr int L = decltype(Lc)::value, U = decltype(Uc)::value;
-    (void)wave_grid(k_true_resid<L, U, false>, kThreads, p);
-    (void)wave_grid(k_step32<L, U, int16_t>, kThreads, p);
-    (void)wave_grid(k_step32<L, U, int32_t>, kThreads, p);
-  });
-  (void)wave_grid(k_step32_sell<int16_t, 8>, kThreads, p);
-  (void)wave_grid(k_step32_sell<int32_t, 8>, kThreads, p);
-  (void)wave_grid(k_step32_sell<int16_t, 16>, kThreads, p);
-  (void)wave_grid(k_step32_sell<int32_t, 16>, kThreads, p);
-  (void)launch_step32_bulk(p, nullptr, nullptr, nullptr, nullptr, true);
-  (void)launch_step32_tile(p, nullptr, nullptr, nullptr, nullptr, true);
-  (void)wave_grid(k_update32, kThreads, p);
-  (void)wave_grid(k_update32_r<true>, kThreads, p);
-  (void)wave_grid(k_update32_r<false>, kThreads, p);
-  (void)wave_grid(k_pupdate32_x<true>, kThreads, p);
-  (void)wave_grid(k_pupdate32_x<false>, kThreads, p);
-  (void)wave_grid(k_pupdate32<0>, 256, p);
-  (void)wave_grid(k_pupdate32<1>, 256, p);
-  (void)wave_grid(k_update32_fz, kThreads, p);
-  (void)wave_grid(k_fold, 256, p);
+  prime_mixed(p);
   cudaGraph_t g = nullptr;
   set_capturing(true);
   cudaError_t e = cudaStreamBeginCapture(p->mx_stream, cudaStreamCaptureModeThreadLocal);
@@ -1102,7 +581,7 @@ int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double
   }
   cudaGraphDestroy(g);
   for (int i = 0; i < 5; ++i) p->mx_key[i] = key[i];
-  p->mx_nodes = 3 * kChunk + 3;
+  p->mx_nodes = 2 * kChunk + 3;
   return FEMK_OK;
 }
 
@@ -1117,6 +596,7 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   clear_error();
   FEMK_CHECK_ARG(pc && vals && b && x && dinv64, "femk_pcg_mixed: NULL argument (a Jacobi inverse is required)");
   FEMK_CHECK_ARG(mode == FEMK_MIXED_RELIABLE || mode == FEMK_MIXED_RESTART, "femk_pcg_mixed: unknown mode");
+  FEMK_CHECK_ARG(tol >= 0.0 && atol >= 0.0, "femk_pcg_mixed: negative tolerance");
   femk_plan* p = const_cast<femk_plan*>(pc);
   cudaStream_t s = (cudaStream_t)stream;
   FEMK_TRY(ensure_mixed(p));
@@ -1125,32 +605,29 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   cudaStream_t ws = p->mx_stream;
   FEMK_CUDA_TRY(cudaEventRecord(p->mx_ev[2], s));
   FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->mx_ev[2], 0));
-  const bool persist = p->cg_persist && p->coop && p->sell_vals32 && p->sell_vals;
-  // the fused form runs on the bulk-copy FP32 step with split updates only
-  p->mx_fz_on = p->mx_fz && !persist && p->cg_split && !(p->tile_ok && p->tile32) &&
-                launch_step32_bulk(p, nullptr, nullptr, nullptr, nullptr, true);
-  if (p->mx_fz_on && !p->mx_zp) FEMK_CUDA_TRY(cudaMalloc(&p->mx_zp, sizeof(float) * 4 * p->vstride));
-  if (p->cg_graph && !persist) FEMK_TRY(ensure_mixed_graph(p, vals, b, x));
-  if (persist)
-    k_gather64<<<::femk::counted_launch() + p->n_sm * 8, 256, 0, ws>>>(p->sell_src, p->sell_nnz, vals, p->sell_vals);
+  if (p->cg_graph) FEMK_TRY(ensure_mixed_graph(p, vals, b, x));
+  else prime_mixed(p);
   const int g1 = p->n_sm * 8;
   if (p->sell_vals32)
     k_gather32<<<::femk::counted_launch() + g1, 256, 0, ws>>>(p->sell_src, p->sell_nnz, vals, p->sell_vals32);
   else
     k_demote<<<::femk::counted_launch() + g1, 256, 0, ws>>>(vals, p->nnz, p->vals32);
   k_demote<<<::femk::counted_launch() + g1, 256, 0, ws>>>(dinv64, n, m.d32);
+  // e, p and s start at zero (beta = 0 multiplies p and s at the first step: 0 * NaN would stick)
   k_fill_f<<<::femk::counted_launch() + g1, 256, 0, ws>>>(m.e, n, 0.f);
+  k_fill_f<<<::femk::counted_launch() + g1, 256, 0, ws>>>(m.pv, n, 0.f);
+  k_fill_f<<<::femk::counted_launch() + g1, 256, 0, ws>>>(m.s, n, 0.f);
   MixedState init{};
   init.maxiter = maxiter;
   // reliable updates when <r, r> has fallen by delta2 since the last one: measured on B200 at P1 128^3,
   // 26.6 ms per mixed step with 1e-4 vs 27.1 ms with 1e-2 (9 FP64 updates), same 1e-8 stop rule
-  init.delta2 = mode == FEMK_MIXED_RESTART ? 1e-8 : 1e-4;
-  if (const char* e = std::getenv("FEMK_MIXED_DELTA2")) init.delta2 = std::atof(e);  // tuning runs
+  init.delta2 = mode == FEMK_MIXED_RESTART ? 1e-8 : (p->mixed_delta2 > 0.0 ? p->mixed_delta2 : 1e-4);
   init.restart = mode == FEMK_MIXED_RESTART ? 1 : 0;
+  init.alpha = 1.0;
   FEMK_CUDA_TRY(cudaMemcpyAsync(m.st, &init, sizeof(MixedState), cudaMemcpyHostToDevice, ws));
   const double tol2 = tol * tol, atol2 = atol * atol;
-  launch_true_resid<true>(p, vals, x, b, m.d32, m.r, m.z, m.pv, m.st, tol2, atol2, ws,
-                          p->mx_fz_on ? (float2*)p->mx_zp : nullptr);
+  launch_true_resid<true>(p, vals, x, b, m.d32, m.r, m.u, m.st, tol2, atol2, ws);
+  launch_step32<true>(p, m.u, m.r, m.w, m.st, ws);  // w = A u, the first alpha
   FEMK_CUDA_TRY(cudaGetLastError());
   MixedState* hs = (MixedState*)p->mx_host;
   int64_t enq = 0;
@@ -1159,27 +636,7 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   // a chunk performs at least one inner iteration unless the solve is done, so maxiter + 1 chunks
   // bound the loop
   const int64_t max_chunks = (int64_t)maxiter + 1;
-  if (persist) {
-    FEMK_CUDA_TRY(cudaMemsetAsync(p->bar, 0, sizeof(GridBar), ws));
-    const bool c16 = p->sell_c16 != nullptr;
-    const void* fn = c16 ? (const void*)k_mixed_persist<int16_t> : (const void*)k_mixed_persist<int32_t>;
-    const int per_sm = std::min(2, resident_blocks(fn, kPersistThreads));
-    const int grid = p->n_sm * per_sm;
-    const void* cols = c16 ? (const void*)p->sell_c16 : (const void*)p->sell_cols;
-    const float* sv32 = p->sell_vals32;
-    const double* sv64 = p->sell_vals;
-    int64_t nn = n, ns = p->n_slices;
-    float *r = m.r, *z = m.z, *pv = m.pv, *q = m.q, *e = m.e;
-    const float* d32 = m.d32;
-    MixedState* stp = m.st;
-    GridBar* bar = (GridBar*)p->bar;
-    void* args[] = {(void*)&p->sell_ptr, (void*)&cols, (void*)&sv32, (void*)&sv64, (void*)&nn, (void*)&ns,
-                    (void*)&b, (void*)&x, (void*)&d32, (void*)&r, (void*)&z, (void*)&pv, (void*)&q, (void*)&e,
-                    (void*)&p->partials, (void*)&stp, (void*)&bar};
-    counted_launch();
-    FEMK_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kPersistThreads), args, 0, ws));
-  }
-  while (!persist) {
+  while (true) {
     if (p->cg_graph) {
       FEMK_CUDA_TRY(cudaGraphLaunch(p->mx_exec, ws));
       count_launches(p->mx_nodes);
@@ -1214,7 +671,7 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
     return FEMK_NONFINITE;
   }
   if (fin.status == FEMK_TIMEOUT) {
-    set_error("femk_pcg_mixed: a grid barrier of the persistent solver gave up waiting");
+    set_error("femk_pcg_mixed: a bulk-copy wait of the FP32 SpMV gave up");
     return FEMK_TIMEOUT;
   }
   if (fin.rr64 > fin.atol2) {

@@ -13,14 +13,12 @@
 #include <algorithm>
 #include <atomic>
 #include <climits>
-#include <cstdlib>
 #include <thread>
 #include <vector>
 
 #include "femk_element.cuh"
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
-#include "femk_tile.cuh"
 
 namespace femk {
 namespace {
@@ -418,7 +416,6 @@ int build_incidence(const int32_t* cells, int64_t ntet, int64_t n, int32_t** ptr
 }
 
 int build_uniform_columns(femk_plan* p, cudaStream_t s);
-int build_tiles(femk_plan* p, cudaStream_t s);
 
 template <int ND>
 int build_pattern(femk_plan* p, int* d_err, int* h_err, cudaStream_t s) {
@@ -442,7 +439,7 @@ int build_pattern(femk_plan* p, int* d_err, int* h_err, cudaStream_t s) {
     return FEMK_EINVAL;
   }
   p->nnz = nnz;
-  choose_spmv_cfg(n > 0 ? (double)nnz / (double)n : 1.0, &p->spmv_L, &p->spmv_U);
+  if (p->spmv_L == 0) choose_spmv_cfg(n > 0 ? (double)nnz / (double)n : 1.0, &p->spmv_L, &p->spmv_U);
   FEMK_TRY(dev_alloc(&p->indptr, n + 1, s));
   FEMK_TRY(dev_alloc(&p->indices, nnz, s));
   k_to_i32<<<::femk::counted_launch() + blocks_for(n + 1, kThreads, 65535 * 4), kThreads, 0, s>>>((const int64_t*)rowptr.p, n + 1, p->indptr);
@@ -552,139 +549,6 @@ int build_uniform_columns(femk_plan* p, cudaStream_t s) {
                                                                         p->sell_cuptr, p->sell_cu);
   FEMK_CUDA_TRY(cudaGetLastError());
   FEMK_CUDA_TRY(cudaStreamSynchronize(s));
-  return build_tiles(p, s);
-}
-
-// Tiles of the staged-x SpMV (femk_tile.cuh): kTileW consecutive slices each. Built on the host
-// from the CSR pattern and the per-slice column tables (a one-off cost of the plan): per tile the
-// x windows covering its columns (column runs closer than kTileGap merged, starts and lengths on
-// 4-element boundaries, clamped to the solver vectors' padded length) and a slot table in the
-// layout of the column tables. A plan whose tiles need more than kTileMaxWin windows or more than
-// kTileXCap staged values, or whose shared-offset slices do not map to consecutive slots, keeps
-// the bulk-copy kernel instead (tile_ok = 0).
-constexpr int kTileGap = 16;
-constexpr int kTileXCap = 4096;
-
-int build_tiles(femk_plan* p, cudaStream_t s) {
-  if (!p->sell_cu || !p->tile_on || p->max_row > 32) return FEMK_OK;
-  const int64_t n = p->n, ns = p->n_slices, W = kTileW;
-  const int64_t vlim = (n + 63) / 64 * 64;  // solver vectors hold n rounded up to 64 elements
-  std::vector<int32_t> indptr(n + 1), indices(p->nnz);
-  std::vector<int64_t> sptr(ns + 1), cptr(ns + 1);
-  FEMK_CUDA_TRY(cudaMemcpyAsync(indptr.data(), p->indptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, s));
-  FEMK_CUDA_TRY(cudaMemcpyAsync(indices.data(), p->indices, sizeof(int32_t) * p->nnz, cudaMemcpyDeviceToHost, s));
-  FEMK_CUDA_TRY(cudaMemcpyAsync(sptr.data(), p->sell_ptr, sizeof(int64_t) * (ns + 1), cudaMemcpyDeviceToHost, s));
-  FEMK_CUDA_TRY(cudaMemcpyAsync(cptr.data(), p->sell_cuptr, sizeof(int64_t) * (ns + 1), cudaMemcpyDeviceToHost, s));
-  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
-  const int64_t ntiles = (ns + W - 1) / W;
-  std::vector<TileMeta> meta(ntiles);
-  std::vector<int16_t> tab(p->sell_cu_len, 0);
-  std::atomic<int> bad{0};
-  std::atomic<int> xcap{4};
-  auto work = [&](int64_t t0, int64_t t1) {
-    std::vector<int32_t> cols;
-    for (int64_t t = t0; t < t1 && !bad.load(std::memory_order_relaxed); ++t) {
-      const int64_t s0 = t * W, s1 = std::min(ns, s0 + W);
-      const int64_t r0 = s0 * 32, r1 = std::min(n, s1 * 32);
-      cols.assign(indices.begin() + indptr[r0], indices.begin() + indptr[r1]);
-      std::sort(cols.begin(), cols.end());
-      cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
-      TileMeta m{};
-      int nwin = 0;
-      int64_t lo = cols[0], hi = cols[0];
-      auto close = [&](int64_t a, int64_t b) -> bool {  // [a, b] inclusive -> aligned window
-        const int64_t st = a / 4 * 4, en = std::min(vlim, (b + 1 + 3) / 4 * 4);
-        if (nwin > 0 && st <= (int64_t)m.wstart[nwin - 1] + m.wlen[nwin - 1]) {  // overlaps after rounding
-          m.wlen[nwin - 1] = (int32_t)(en - m.wstart[nwin - 1]);
-          return true;
-        }
-        if (nwin == kTileMaxWin) return false;
-        m.wstart[nwin] = (int32_t)st;
-        m.wlen[nwin] = (int32_t)(en - st);
-        ++nwin;
-        return true;
-      };
-      bool ok = true;
-      for (size_t j = 1; j < cols.size() && ok; ++j) {
-        if (cols[j] - hi <= kTileGap) {
-          hi = cols[j];
-        } else {
-          ok = close(lo, hi);
-          lo = hi = cols[j];
-        }
-      }
-      ok = ok && close(lo, hi);
-      int64_t xlen = 0;
-      int32_t base[kTileMaxWin];
-      for (int j = 0; j < nwin; ++j) {
-        base[j] = (int32_t)xlen;
-        xlen += m.wlen[j];
-      }
-      if (!ok || xlen > kTileXCap) {
-        bad = 1;
-        return;
-      }
-      m.nwin = nwin;
-      m.xlen = (int32_t)xlen;
-      auto slot = [&](int64_t c) -> int64_t {
-        for (int j = 0; j < nwin; ++j)
-          if (c >= m.wstart[j] && c < (int64_t)m.wstart[j] + m.wlen[j]) return base[j] + (c - m.wstart[j]);
-        return -1;
-      };
-      const int64_t sr = slot(r0);
-      m.self_base = (int32_t)(sr - r0);
-      m.v0 = sptr[s0];
-      m.v1 = sptr[s1];
-      m.c0 = cptr[s0];
-      m.c1 = cptr[s1];
-      for (int64_t sl = s0; sl < s1 && ok; ++sl) {
-        const int64_t w = (sptr[sl + 1] - sptr[sl]) / 32;
-        const bool uni = (cptr[sl + 1] - cptr[sl]) != 32 * w;
-        for (int64_t k = 0; k < w && ok; ++k)
-          for (int l = 0; l < 32 && ok; ++l) {
-            const int64_t row = sl * 32 + l;
-            const int64_t self = row < n ? row : n - 1;
-            const int64_t len = row < n ? indptr[row + 1] - indptr[row] : 0;
-            const int64_t col = k < len ? indices[indptr[row] + k] : self;
-            const int64_t sv = slot(col);
-            if (sv < 0 || sv >= xlen || (row < n && slot(row) != row + m.self_base)) {
-              ok = false;
-            } else if (uni) {
-              if (l == 0) tab[cptr[sl] + k] = (int16_t)sv;
-              else if ((int64_t)tab[cptr[sl] + k] + l != sv) ok = false;
-            } else {
-              tab[cptr[sl] + 32 * k + l] = (int16_t)sv;
-            }
-          }
-      }
-      if (!ok) {
-        bad = 1;
-        return;
-      }
-      meta[t] = m;
-      int cur = xcap.load();
-      while ((int)xlen > cur && !xcap.compare_exchange_weak(cur, (int)xlen)) {
-      }
-    }
-  };
-  const int nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-  std::vector<std::thread> pool;
-  const int64_t per = (ntiles + nth - 1) / nth;
-  for (int i = 0; i < nth; ++i) {
-    const int64_t a = i * per, b = std::min(ntiles, a + per);
-    if (a < b) pool.emplace_back(work, a, b);
-  }
-  for (auto& th : pool) th.join();
-  if (bad) return FEMK_OK;  // the plan keeps the bulk-copy kernel
-  FEMK_TRY(dev_alloc((char**)&p->tile_meta, (int64_t)sizeof(TileMeta) * ntiles, s));
-  FEMK_TRY(dev_alloc(&p->tile_slots, p->sell_cu_len, s));
-  FEMK_CUDA_TRY(cudaMemcpyAsync(p->tile_meta, meta.data(), sizeof(TileMeta) * ntiles, cudaMemcpyHostToDevice, s));
-  FEMK_CUDA_TRY(cudaMemcpyAsync(p->tile_slots, tab.data(), sizeof(int16_t) * p->sell_cu_len, cudaMemcpyHostToDevice,
-                                s));
-  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
-  p->ntiles = ntiles;
-  p->tile_xcap = (xcap.load() + 3) / 4 * 4;
-  p->tile_ok = 1;
   return FEMK_OK;
 }
 
@@ -818,8 +682,7 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
                   p->work,     p->partials,  p->state,     p->work32,    p->vals32,    p->work64b,
                   p->sell_ptr, p->sell_src,  p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32,
                   p->bar,      p->batch_ws,  p->bicg_ws,   p->bicg_state, p->sell_cuptr, p->sell_cu,
-                  p->tile_meta, p->tile_slots, p->coef_tmp, p->theta_ws, p->cl_ptr, p->cl_dof, p->cl_loc,
-                  p->cl_off, p->cl_inv, p->mx_zp, p->cmp_ws, p->gm_ws};
+                  p->coef_tmp, p->theta_ws, p->cmp_ws, p->gm_ws};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->state_host) cudaFreeHost(p->state_host);
@@ -845,9 +708,82 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
   return FEMK_OK;
 }
 
-extern "C" int femk_plan_create_simplex(const double* coords_dev, int dim, int64_t nvert, const int32_t* cells_dev,
-                                        int64_t ncell, int order, const uint8_t* dirichlet_mask_dev, void* stream,
-                                        femk_plan** out) {
+extern "C" void femk_plan_options_default(femk_plan_options* o) {
+  if (!o) return;
+  *o = femk_plan_options{};
+  o->size = (int32_t)sizeof(femk_plan_options);
+  o->solver_layout = 1;
+  o->column_tables = 1;
+  o->cols16 = 1;
+  o->graph_replay = 1;
+  o->l2_hints = -1;
+  o->ring64 = -1;
+  o->ring32 = -1;
+  o->csr_lanes = 0;
+  o->csr_rows = 0;
+  o->sell_batch = 16;
+  o->vec_blocks = 0;
+  o->split_updates = 1;
+  o->test_skip_arrival = -1;
+  o->mixed_delta2 = 0.0;
+  o->barrier_limit_ms = 0.0;
+}
+
+namespace {
+
+bool ring_ok(int v) { return v == -1 || v == 0 || v == 14 || v == 18 || v == 24 || v == 28 || v == 38; }
+
+// validate the options and copy them into the plan (before the build: the layout ones act there)
+int apply_options(femk_plan* p, const femk_plan_options& o) {
+  FEMK_CHECK_ARG(o.size == (int32_t)sizeof(femk_plan_options),
+                 "femk_plan_create_ex: options.size mismatch (fill them with femk_plan_options_default)");
+  FEMK_CHECK_ARG((o.solver_layout | 1) == 1 && (o.column_tables | 1) == 1 && (o.cols16 | 1) == 1 &&
+                     (o.graph_replay | 1) == 1 && (o.split_updates | 1) == 1,
+                 "femk_plan_create_ex: solver_layout, column_tables, cols16, graph_replay and split_updates are 0 or 1");
+  FEMK_CHECK_ARG(o.l2_hints >= -1 && o.l2_hints <= 4, "femk_plan_create_ex: l2_hints must be in [-1, 4]");
+  FEMK_CHECK_ARG(ring_ok(o.ring64) && ring_ok(o.ring32),
+                 "femk_plan_create_ex: ring64 / ring32 must be -1, 0, 14, 18, 24, 28 or 38");
+  const bool csr_auto = o.csr_lanes == 0 && o.csr_rows == 0;
+  FEMK_CHECK_ARG(csr_auto || femk::with_spmv_cfg(o.csr_lanes, o.csr_rows, [](auto, auto) {}),
+                 "femk_plan_create_ex: unsupported (csr_lanes, csr_rows) pair");
+  FEMK_CHECK_ARG(o.sell_batch == 8 || o.sell_batch == 16, "femk_plan_create_ex: sell_batch must be 8 or 16");
+  FEMK_CHECK_ARG(o.vec_blocks >= 0 && o.vec_blocks <= 8, "femk_plan_create_ex: vec_blocks must be in [0, 8]");
+  FEMK_CHECK_ARG(o.test_skip_arrival >= -1, "femk_plan_create_ex: test_skip_arrival must be >= -1");
+  FEMK_CHECK_ARG(o.mixed_delta2 >= 0.0 && o.mixed_delta2 < 1.0, "femk_plan_create_ex: mixed_delta2 must be in [0, 1)");
+  FEMK_CHECK_ARG(o.barrier_limit_ms >= 0.0 && o.barrier_limit_ms <= 60000.0,
+                 "femk_plan_create_ex: barrier_limit_ms must be in [0, 60000]");
+  p->use_sell = o.solver_layout;
+  p->sell_uni = o.column_tables;
+  p->sell64_c16 = o.cols16;
+  p->cg_graph = o.graph_replay;
+  // measured on B200 (FP64 PCG to 1e-8): P1 128^3 48.7 ms with hints (mode 1) vs 52.0 ms without;
+  // P2 64^3 117 ms without vs 168 ms with, so P2 plans stream without them
+  p->l2_mode = o.l2_hints >= 0 ? o.l2_hints : (p->order == 1 ? 1 : 0);
+  // bulk-copy SpMV rings, measured on B200 at P1 128^3 (to 1e-8): FP64 1 stage x 4 warps (38.4 ms per
+  // step; 2 x 4: 43.2, 1 x 2: 40.4, thread-per-row: 45.8), FP32 2 stages x 8 warps (27.1 ms; 1 x 8:
+  // 27.2, 2 x 4: 29.5); rows of at most 8 entries (2-D P1) get 2 x 8 (set after the build)
+  p->bulk_cfg = o.ring64 >= 0 ? o.ring64 : 14;
+  p->bulk32_cfg = o.ring32 >= 0 ? o.ring32 : 28;
+  p->spmv_L = csr_auto ? 0 : o.csr_lanes;
+  p->spmv_U = csr_auto ? 0 : o.csr_rows;
+  p->sell_batch = o.sell_batch;
+  p->vec_blocks = o.vec_blocks;
+  p->cg_split = o.split_updates;
+  p->skip_arrival = o.test_skip_arrival;
+  p->mixed_delta2 = o.mixed_delta2;
+  int khz = 0;
+  cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, p->device);
+  if (khz <= 0) khz = 2000000;
+  const double ms = o.barrier_limit_ms > 0.0 ? o.barrier_limit_ms : 2000.0;
+  p->barrier_spin = (long long)(ms * (double)khz);  // cycles at the maximum SM clock
+  return FEMK_OK;
+}
+
+}  // namespace
+
+extern "C" int femk_plan_create_ex(const double* coords_dev, int dim, int64_t nvert, const int32_t* cells_dev,
+                                   int64_t ncell, int order, const uint8_t* dirichlet_mask_dev,
+                                   const femk_plan_options* opts, void* stream, femk_plan** out) {
   femk::clear_error();
   FEMK_CHECK_ARG(out != nullptr, "femk_plan_create: out is NULL");
   *out = nullptr;
@@ -859,6 +795,9 @@ extern "C" int femk_plan_create_simplex(const double* coords_dev, int dim, int64
   FEMK_CHECK_ARG(nvert >= nv && ncell >= 1, "femk_plan_create: empty mesh");
   FEMK_CHECK_ARG(ncell * nd * nd < INT32_MAX, "femk_plan_create: mesh too large for int32 slot map");
   FEMK_CHECK_ARG(nvert < INT32_MAX, "femk_plan_create: too many vertices");
+  femk_plan_options o;
+  femk_plan_options_default(&o);
+  if (opts) o = *opts;
   cudaStream_t s = (cudaStream_t)stream;
   femk_plan* p = new femk_plan();
   cudaGetDevice(&p->device);
@@ -867,47 +806,32 @@ extern "C" int femk_plan_create_simplex(const double* coords_dev, int dim, int64
   p->dim = dim;
   p->nv = nv;
   p->nd = nd;
-  if (const char* e = std::getenv("FEMK_CG_FUSED")) p->cg_fused = std::atoi(e) != 0;
-  if (const char* e = std::getenv("FEMK_CG_GRAPH")) p->cg_graph = std::atoi(e) != 0;
-  if (const char* e = std::getenv("FEMK_SELL")) p->use_sell = std::atoi(e) != 0;
-  if (const char* e = std::getenv("FEMK_SELL64_C16")) p->sell64_c16 = std::atoi(e) != 0;
-  // measured on B200 (FP64 PCG to 1e-8): P1 128^3 48.7 ms with hints (mode 1) vs 52.0 ms without;
-  // P2 64^3 117 ms without vs 168 ms with, so P2 plans stream without them
-  p->l2_mode = std::getenv("FEMK_L2HINT") ? femk::l2_hints() : (order == 1 ? 1 : 0);
-  if (const char* e = std::getenv("FEMK_CG_PERSIST")) p->cg_persist = std::atoi(e) != 0;
-  if (const char* e = std::getenv("FEMK_CG_SPLIT")) p->cg_split = std::atoi(e) != 0;
-  // bulk-copy SpMV configurations, measured on B200 at P1 128^3 (to 1e-8): FP64 1 stage x 4 warps
-  // (38.4 ms/step; 2 x 4: 43.2, 1 x 2: 40.4, register-streamed: 45.8), FP32 2 stages x 8 warps
-  // (27.1 ms; 1 x 8: 27.2, 2 x 4: 29.5)
-  p->bulk_cfg = 14;
-  p->bulk32_cfg = 28;
-  if (const char* e = std::getenv("FEMK_BULK")) p->bulk_cfg = std::atoi(e);
-  if (const char* e = std::getenv("FEMK_BULK32")) p->bulk32_cfg = std::atoi(e);
-  if (const char* e = std::getenv("FEMK_PDL")) p->pdl = std::atoi(e) != 0;
-  if (const char* e = std::getenv("FEMK_VEC_BLOCKS")) p->vec_blocks = std::atoi(e);
-  if (const char* e = std::getenv("FEMK_MIXED_FUSE")) p->mx_fz = std::atoi(e) != 0;
-  if (const char* e = std::getenv("FEMK_SELL_UNI")) p->sell_uni = std::atoi(e) != 0;
-  if (const char* e = std::getenv("FEMK_TILE")) p->tile_on = std::atoi(e) != 0;
-  if (const char* e = std::getenv("FEMK_TILE64")) p->tile64 = std::atoi(e) != 0;
-  if (const char* e = std::getenv("FEMK_TILE32")) p->tile32 = std::atoi(e) != 0;
-  // FP32 kernels stream without hints: measured on B200 at P1 128^3, mixed solve 31.7 ms without
-  // vs 32.8 ms with evict-last vectors and gathers
-  p->l2_mode32 = 0;
-  if (const char* e = std::getenv("FEMK_L2HINT32")) p->l2_mode32 = std::atoi(e) != 0;
+  int st = apply_options(p, o);
+  if (st != FEMK_OK) {
+    delete p;
+    return st;
+  }
   cudaDeviceGetAttribute(&p->coop, cudaDevAttrCooperativeLaunch, p->device);
   p->nvert = nvert;
   p->ntet = ncell;
-  const int st = dim == 2 ? femk::create_impl<3>(p, coords_dev, cells_dev, dirichlet_mask_dev, s)
-                          : femk::create_impl<4>(p, coords_dev, cells_dev, dirichlet_mask_dev, s);
+  st = dim == 2 ? femk::create_impl<3>(p, coords_dev, cells_dev, dirichlet_mask_dev, s)
+                : femk::create_impl<4>(p, coords_dev, cells_dev, dirichlet_mask_dev, s);
   if (st != FEMK_OK) {
     femk_plan_destroy(p);
     return st;
   }
   // rows of at most 8 entries (2-D P1 triangles) run on the 8-wide ring, where 2 stages x 8 warps
   // measured best on B200: 2-D P1 1024^2 PCG 109.7 ms vs 115.1 ms with 1 x 4
-  if (p->max_row <= 8 && !std::getenv("FEMK_BULK")) p->bulk_cfg = 28;
+  if (p->max_row <= 8 && o.ring64 < 0) p->bulk_cfg = 28;
   *out = p;
   return FEMK_OK;
+}
+
+extern "C" int femk_plan_create_simplex(const double* coords_dev, int dim, int64_t nvert, const int32_t* cells_dev,
+                                        int64_t ncell, int order, const uint8_t* dirichlet_mask_dev, void* stream,
+                                        femk_plan** out) {
+  return femk_plan_create_ex(coords_dev, dim, nvert, cells_dev, ncell, order, dirichlet_mask_dev, nullptr, stream,
+                             out);
 }
 
 extern "C" int femk_plan_create(const double* xyz_dev, int64_t nvert, const int32_t* tets_dev, int64_t ntet,
@@ -928,7 +852,6 @@ extern "C" int femk_plan_get_info(const femk_plan* p, femk_plan_info* out) {
   out->device = p->device;
   out->sell_nnz = p->sell_src ? p->sell_nnz : 0;
   out->batch_graph = p->batch_graph_used;
-  out->tiles = p->tile_ok;
   out->sell_col_units = p->sell_cu ? p->sell_cu_len : (p->sell_src ? p->sell_nnz : 0);
   out->dim = p->dim;
   return FEMK_OK;

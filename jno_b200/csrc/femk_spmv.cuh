@@ -156,16 +156,6 @@ __device__ __forceinline__ V sell_row(const V* __restrict__ vb, const I* __restr
   return acc;
 }
 
-// L2 eviction hints of the FP64 CG kernels, chosen per plan (FEMK_L2HINT overrides, for comparison runs):
-// 0 none; 1 matrix evict_first + x gathers and vector kernels evict_last; 2 matrix evict_first +
-// vector kernels evict_last (plain gathers); 3 vector kernels only; 4 matrix ld.global.cs (already
-// evict-first) + x gathers and vector kernels evict_last
-int l2_hints();
-
-// entries per batch of the FP64 sliced-ELL row loop (FEMK_SELL_BATCH=8|16 overrides for tuning);
-// the FP32 loop always uses 8 (16 doubles its registers and halves its occupancy)
-int sell_batch();
-
 // Call f(integral_constant<L>, integral_constant<U>) for a supported (lanes per row, rows in
 // flight) pair; returns false for an unsupported one.
 template <typename F>
@@ -188,8 +178,8 @@ inline bool with_spmv_cfg(int L, int U, F&& f) {
   return false;
 }
 
-// Default (L, U) from the mean row length; FEMK_SPMV_CFG="L,U" in the environment overrides it
-// (tuning sweeps). Called once per plan.
+// Default (L, U) from the mean row length (a plan's csr_lanes / csr_rows options override it).
+// Called once per plan.
 void choose_spmv_cfg(double mean_row, int* L, int* U);
 
 }  // namespace femk

@@ -2,8 +2,6 @@
 #include <atomic>
 #include <mutex>
 #include <unordered_map>
-#include <cstdio>
-#include <cstdlib>
 
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
@@ -38,24 +36,6 @@ int resident_blocks(const void* fn, int threads) {
   return b;
 }
 
-int l2_hints() {
-  static int h = [] {
-    const char* e = std::getenv("FEMK_L2HINT");
-    const int v = e ? std::atoi(e) : 1;
-    return v >= 0 && v <= 4 ? v : 1;
-  }();
-  return h;
-}
-
-int sell_batch() {
-  static int b = [] {
-    const char* e = std::getenv("FEMK_SELL_BATCH");
-    const int v = e ? std::atoi(e) : 16;  // B200: 63 vs 66 us per FP64 SpMV at P1 128^3
-    return v == 8 ? 8 : 16;
-  }();
-  return b;
-}
-
 void choose_spmv_cfg(double mean_row, int* L, int* U) {
   // measured on B200 at P1 128^3 (mean 14.8) and P2 64^3 (mean 28.4): 8 lanes x 2 rows in flight
   // beats 16x1/16x2/32x1/32x2 and 4x4, 8x4 by 20-60%
@@ -65,12 +45,6 @@ void choose_spmv_cfg(double mean_row, int* L, int* U) {
     *L = 8, *U = 2;
   } else {
     *L = 16, *U = 2;
-  }
-  const char* env = std::getenv("FEMK_SPMV_CFG");
-  int l = 0, u = 0;
-  if (env && std::sscanf(env, "%d,%d", &l, &u) == 2 && with_spmv_cfg(l, u, [](auto, auto) {})) {
-    *L = l;
-    *U = u;
   }
 }
 void clear_error() { g_last_error.clear(); }

@@ -28,10 +28,11 @@ class FemPlan:
     ``points`` f64[nv, 3] with ``tets`` int[T, 4] (tetrahedra), or ``points`` f64[nv, 2] with
     int[T, 3] triangles, describe the P1 mesh; ``order`` 2 adds the edge midpoint DOFs in the
     reference's first-encounter numbering. ``dirichlet_mask`` (bool/uint8 per DOF) overrides the
-    default Dirichlet set (every node on a boundary facet).
+    default Dirichlet set (every node on a boundary facet). ``options`` maps fields of
+    ``femk_plan_options`` (include/femk.h) to values; unnamed fields keep the library defaults.
     """
 
-    def __init__(self, points, tets, order=1, dirichlet_mask=None):
+    def __init__(self, points, tets, order=1, dirichlet_mask=None, options=None):
         if not torch.cuda.is_available():
             raise RuntimeError("jno_b200 needs a CUDA device (B200, sm_100a); there is no CPU path")
         lib = _lib.load()
@@ -52,11 +53,17 @@ class FemPlan:
         xyz = _device_tensor(points, torch.float64)
         cells = _device_tensor(t, torch.int32)
         mask = None if dirichlet_mask is None else _device_tensor(dirichlet_mask, torch.uint8)
+        opts = _lib.PlanOptions()
+        lib.femk_plan_options_default(ctypes.byref(opts))
+        for key, value in (options or {}).items():
+            if key == "size" or key not in dict(_lib.PlanOptions._fields_):
+                raise ValueError(f"unknown plan option {key!r}")
+            setattr(opts, key, value)
         handle = ctypes.c_void_p()
         _lib.check(
-            lib.femk_plan_create_simplex(
+            lib.femk_plan_create_ex(
                 _lib.ptr(xyz), dim, xyz.shape[0], _lib.ptr(cells), cells.shape[0], int(order), _lib.ptr(mask),
-                _lib.stream_handle(), ctypes.byref(handle),
+                ctypes.byref(opts), _lib.stream_handle(), ctypes.byref(handle),
             )
         )
         self._h = handle
@@ -73,7 +80,6 @@ class FemPlan:
         self.cols16 = bool(info.cols16)
         self.sell_nnz = int(info.sell_nnz)
         self.sell_col_units = int(info.sell_col_units)
-        self.tiles = bool(info.tiles)
         self.device = torch.device("cuda", info.device)
         self._pattern = None
 
@@ -342,13 +348,14 @@ class FemPlan:
 
     def gmres(self, vals, b, x=None, inv_diag=None, tol=1e-8, atol=0.0, restart=30, maxiter=None):
         """Restarted Jacobi-GMRES (jax gmres, solve_method="batched"). Returns (x, Arnoldi steps,
-        restart cycles, relres, status); maxiter None is jax's 10 n restart cycles."""
+        restart cycles, relres, status); maxiter None is jax's 10 n restart cycles, 0 runs none.
+        1 <= restart <= 64 (the library's largest Krylov basis)."""
         x = torch.zeros(self.n, dtype=torch.float64, device=self.device) if x is None else x
         it = ctypes.c_int32(0)
         cyc = ctypes.c_int32(0)
         rr = ctypes.c_double(float("nan"))
         st = self._lib.femk_gmres(self._h, _lib.ptr(vals), _lib.ptr(b), _lib.ptr(x), _lib.ptr(inv_diag), float(tol),
-                                  float(atol), int(restart), 0 if maxiter is None else int(maxiter), ctypes.byref(it),
+                                  float(atol), int(restart), -1 if maxiter is None else int(maxiter), ctypes.byref(it),
                                   ctypes.byref(cyc), ctypes.byref(rr), _lib.stream_handle())
         _lib.check(st, allow=(_lib.FEMK_NOT_CONVERGED,))
         return x, it.value, cyc.value, rr.value, st

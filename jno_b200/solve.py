@@ -129,10 +129,18 @@ def cg(*, tol=1e-8, atol=0.0, maxiter=20_000, precision="fp64", refine="reliable
     return LinearSolver(tol, atol, maxiter, precision, refine, mixed_maxiter=mixed_maxiter)
 
 
+GMRES_MAX_RESTART = 64  # restart lengths the library's GMRES accepts (femk_gmres)
+
+
 def gmres(*, tol=1e-8, atol=0.0, maxiter=None, restart=30):
     """Restarted GMRES on the B200 kernels (``jax.scipy.sparse.linalg.gmres`` with
     ``solve_method="batched"``, jno/solve.py:216-221): ``maxiter`` counts restart cycles (None: jax's
     10 n); ``last_info.iterations`` = Arnoldi steps, ``last_info.outer`` = cycles."""
+    if not 1 <= int(restart) <= GMRES_MAX_RESTART:
+        raise ValueError(f"jno.solve.gmres: restart must be in [1, {GMRES_MAX_RESTART}] on the B200 path "
+                         f"(the library keeps at most {GMRES_MAX_RESTART + 1} Krylov vectors), got {restart}")
+    if maxiter is not None and int(maxiter) < 0:
+        raise ValueError("jno.solve.gmres: maxiter must be >= 0 (or None for jax's 10 n restart cycles)")
     s = LinearSolver(tol, atol, 20_000, name="gmres")
     s.restart = int(restart)
     s.gmres_maxiter = None if maxiter is None else int(maxiter)

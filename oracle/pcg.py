@@ -135,8 +135,9 @@ def gmres(A, b, inv_diag=None, x0=None, tol=1e-8, atol=0.0, restart=20, maxiter=
             V[:, 0] = w;  H = eye(m, m + 1)                   # row j of H = column j of the Hessenberg
             for j in 0 .. m-1 (until breakdown):
                 v = M A V[:, j];  v0 = ||v||
-                classical Gram-Schmidt of v against V, twice ("twice is enough"; once if v0 = 0):
-                    h = V^T v;  v -= V h;  accumulate h
+                one classical Gram-Schmidt pass of v against V: h = V^T v;  v -= V h
+                (jax's _iterative_classical_gram_schmidt with max_iterations=2 loops while
+                k < max_iterations - 1, so it stops after its first pass)
                 V[:, j+1], h[j+1] = normalize(v, threshold eps * v0);  H[j, :] = h
                 breakdown = h[j+1] == 0
             y = solve(H H^T, H e1 beta) by Cholesky           # the normal equations of min ||H^T y - beta e1||
@@ -170,11 +171,8 @@ def gmres(A, b, inv_diag=None, x0=None, tol=1e-8, atol=0.0, restart=20, maxiter=
         for j in range(m):
             v = M(A @ V[:, j])
             _, v0 = _safe_normalize(v)
-            h = np.zeros(m + 1)
-            for _ in range(2 if v0 > 0 else 1):
-                hj = V.T @ v
-                v = v - V @ hj
-                h += hj
+            h = V.T @ v
+            v = v - V @ h
             unit, h[j + 1] = _safe_normalize(v, eps * v0)
             V[:, j + 1] = unit
             H[j, :] = h

@@ -18,8 +18,8 @@ are the four vertices of the reference tet followed by the midpoints of the edge
 triangle (``lagrange_interp_points(2, 2)``) the three vertices followed by the midpoints of the
 edges ``(1,2),(0,2),(0,1)`` (``jno/utils/solver/fem_topology.py:36``).
 
-Run from the repository root in a container that has the reference at /root/reference:
-    python tests/golden/make_golden.py
+Run from the repository root with the path of a jNO checkout:
+    python tests/golden/make_golden.py <path to jNO>
 Writes tests/golden/reference_small.npz (tetrahedra) and tests/golden/reference_small_2d.npz
 (triangles). Nothing at test time reads the reference.
 """
@@ -33,7 +33,7 @@ import typing
 
 import numpy as np
 
-REF = "/root/reference"
+REF = None  # the jNO checkout, set from the command line
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
 
@@ -184,4 +184,9 @@ def main():
 
 
 if __name__ == "__main__":
+    import argparse
+
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("reference", help="path of the jNO checkout whose functions are executed")
+    REF = os.path.abspath(ap.parse_args().reference)
     main()

@@ -45,6 +45,30 @@ def test_null_arguments_are_rejected_without_a_gpu():
     assert lib.femk_plan_destroy(None) == _lib.FEMK_OK
 
 
+def test_plan_options_defaults_and_validation_without_a_gpu():
+    """femk_plan_options_default fills the documented defaults; femk_plan_create_ex rejects an unknown
+    value before touching a device (the pointers are never dereferenced on that path)."""
+    from jno_b200 import _lib
+
+    lib = _lib.load()
+    o = _lib.PlanOptions()
+    lib.femk_plan_options_default(ctypes.byref(o))
+    assert o.size == ctypes.sizeof(_lib.PlanOptions)
+    assert (o.solver_layout, o.column_tables, o.cols16, o.graph_replay, o.split_updates) == (1, 1, 1, 1, 1)
+    assert (o.l2_hints, o.ring64, o.ring32, o.sell_batch, o.test_skip_arrival) == (-1, -1, -1, 16, -1)
+    assert o.mixed_delta2 == 0.0 and o.barrier_limit_ms == 0.0
+    fake = ctypes.c_void_p(16)
+    for field, bad in (("ring64", 13), ("sell_batch", 4), ("l2_hints", 7), ("solver_layout", 2),
+                       ("barrier_limit_ms", -1.0), ("mixed_delta2", 1.5), ("csr_lanes", 3), ("size", 8)):
+        b = _lib.PlanOptions()
+        lib.femk_plan_options_default(ctypes.byref(b))
+        setattr(b, field, bad)
+        out = ctypes.c_void_p()
+        st = lib.femk_plan_create_ex(fake, 3, 8, fake, 1, 1, None, ctypes.byref(b), None, ctypes.byref(out))
+        assert st == _lib.FEMK_EINVAL and out.value is None, field
+        assert b"femk_plan_create_ex" in lib.femk_last_error_string()
+
+
 def _recipe():
     import jno_b200 as jno
 

@@ -16,12 +16,12 @@ from oracle import pcg as op  # noqa: E402
 from oracle import transient as ot  # noqa: E402
 
 
-def _system(dim, n, order, seed):
+def _system(dim, n, order, seed, options=None):
     from jno_b200.plan import FemPlan
 
     pf, cf, cells, p1 = om.kuhn_cube(n, order, seed=1) if dim == 3 else om.unit_square(n, order, seed=1)
     logk = om.logk_field(len(cells), seed)
-    plan = FemPlan(p1, cells, order)
+    plan = FemPlan(p1, cells, order, options=options)
     vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
     s = oa.assemble(pf, cf, order, om.boundary_nodes(cf, order, nv=dim + 1), np.exp(logk))
     return plan, vals, b, s
@@ -71,9 +71,52 @@ def test_gmres_unpreconditioned_warm_start_zero_rhs_and_cap():
     assert stc == _lib.FEMK_NOT_CONVERGED and cyclesc == 1 and stepsc == 2 and relc < 1.0
 
 
-def test_gmres_on_the_canonical_csr_path_matches(monkeypatch):
-    monkeypatch.setenv("FEMK_SELL", "0")
+def test_gmres_breakdown_ignores_stale_basis_columns():
+    """An Arnoldi breakdown ends a cycle early; the basis columns past it are never written in that
+    cycle (jax starts every cycle from a zero basis). Here they hold NaN left by an earlier call: a
+    restart-30 solve sizes the plan's Krylov workspace, a restart-5 call on NaN values leaves NaN in
+    the scratch vector that a restart-20 cycle sees as basis column 6, and a right-hand side e_d on a
+    Dirichlet DOF d (A e_d = e_d, diag 1) then breaks down after one step. The update must read only
+    the written column: x = e_d exactly."""
+    import ctypes
+
+    from jno_b200 import _lib
+
     plan, vals, b, s = _system(3, 6, 1, 1022)
+    inv = plan.jacobi(vals)
+    plan.gmres(vals, b, inv_diag=inv, tol=1e-8, restart=30)
+    bad = vals.clone()
+    bad[::7] = float("nan")
+    x = torch.zeros_like(b)
+    it, cyc, rr = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_double(0.0)
+    st = plan._lib.femk_gmres(plan.handle, _lib.ptr(bad), _lib.ptr(b), _lib.ptr(x), _lib.ptr(inv), 1e-8, 0.0, 5, -1,
+                              ctypes.byref(it), ctypes.byref(cyc), ctypes.byref(rr), _lib.stream_handle())
+    assert st == _lib.FEMK_NONFINITE
+    d = int(torch.nonzero(plan.export()["dirichlet_mask"]).flatten()[0])
+    e = torch.zeros_like(b)
+    e[d] = 1.0
+    x, steps, cycles, rel, st = plan.gmres(vals, e, inv_diag=inv, tol=1e-8, restart=20)
+    assert st == 0 and steps == 1 and cycles == 1 and rel == 0.0
+    assert torch.equal(x, e)
+    xo, so, co, beta = op.gmres(s.csr(), e.cpu().numpy(), oa.jacobi_inverse(oa.matrix_diagonal(s)), tol=1e-8,
+                                restart=20)
+    assert (so, co, beta) == (1, 1, 0.0) and np.array_equal(xo, e.cpu().numpy())
+
+
+def test_gmres_maxiter_zero_runs_no_cycle_and_restart_is_validated():
+    import jno_b200 as jno
+
+    plan, vals, b, s = _system(2, 8, 1, 1023)
+    x, steps, cycles, rel, st = plan.gmres(vals, b, tol=1e-8, restart=10, maxiter=0)
+    assert st == 4 and steps == 0 and cycles == 0 and torch.count_nonzero(x) == 0
+    with pytest.raises(ValueError):
+        jno.solve.gmres(restart=65)
+    with pytest.raises(ValueError):
+        jno.solve.gmres(maxiter=-1)
+
+
+def test_gmres_on_the_canonical_csr_path_matches():
+    plan, vals, b, s = _system(3, 6, 1, 1022, options={"solver_layout": 0})
     inv = plan.jacobi(vals)
     x, steps, cycles, rel, st = plan.gmres(vals, b, inv_diag=inv, tol=1e-8, restart=30)
     xo, so, co, _ = op.gmres(s.csr(), s.b, oa.jacobi_inverse(oa.matrix_diagonal(s)), tol=1e-8, restart=30)

@@ -20,10 +20,10 @@ from oracle import pcg as op  # noqa: E402
 VAL_TOL = 1e-12
 
 
-def _plan(points, tets, order):
+def _plan(points, tets, order, options=None):
     from jno_b200.plan import FemPlan
 
-    return FemPlan(points, tets, order)
+    return FemPlan(points, tets, order, options=options)
 
 
 def _mesh(n, order, seed=0):
@@ -393,13 +393,12 @@ def plan_n(fem):
 
 
 @pytest.mark.parametrize("n,order,bulk", [(8, 1, True), (8, 1, False), (24, 1, True), (4, 2, True)])
-def test_bicgstab_matches_oracle(n, order, bulk, monkeypatch):
-    """femk_bicgstab against the oracle's restatement of jax.scipy.sparse.linalg.bicgstab."""
-    if not bulk:
-        monkeypatch.setenv("FEMK_BULK", "0")
+def test_bicgstab_matches_oracle(n, order, bulk):
+    """femk_bicgstab against the oracle's restatement of jax.scipy.sparse.linalg.bicgstab (bulk-copy
+    SpMV ring, and the thread-per-row kernel with ring64 = 0)."""
     pf, cf, tets, p1 = _mesh(n, order)
     logk = om.logk_field(len(tets), 1005)
-    plan = _plan(p1, tets, order)
+    plan = _plan(p1, tets, order, None if bulk else {"ring64": 0})
     vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
     inv = plan.jacobi(vals)
     u, it, rel, st = plan.bicgstab(vals, b, inv_diag=inv, tol=1e-8)
@@ -441,30 +440,24 @@ def test_bicgstab_status_paths():
         jno.solve.bicgstab(maxiter=1)(CsrMatrix(plan, vals), b, M=jno.precond.jacobi())
 
 
-def test_spmv_layouts_agree(monkeypatch):
+def test_spmv_layouts_agree():
     """The CG-step SpMV has three layouts: bulk-copy slices with per-slice column tables (the
-    default), bulk-copy slices with per-entry columns, and staged-x tiles (opt-in). All sum rows in the same order; the two
-    bulk forms (same grid, same reductions) give bit-identical solves, the tile form agrees to
-    rounding of its dot products. 64^3 hexes: z-lines of 65 rows, so about half the 32-row slices
-    share one offset sequence."""
+    default), bulk-copy slices with per-entry columns (column_tables = 0), and the thread-per-row
+    kernel (ring64 = ring32 = 0). All sum each row in the same order; the two bulk forms (same grid,
+    same reductions) give bit-identical solves, the thread-per-row form agrees to rounding of its dot
+    products (another grid). 64^3 hexes: z-lines of 65 rows, so about half the 32-row slices share
+    one offset sequence."""
     pf, cf, tets, p1 = _mesh(64, 1)
     lk = torch.as_tensor(om.logk_field(len(tets), 1006), device="cuda")
     out = {}
     vals = b = inv = None
-    for tag, env in (("tile", {"FEMK_TILE": "1"}), ("table", {}), ("entry", {"FEMK_SELL_UNI": "0"})):
-        for k in ("FEMK_TILE", "FEMK_SELL_UNI"):
-            monkeypatch.delenv(k, raising=False)
-        for k, v in env.items():
-            monkeypatch.setenv(k, v)
-        plan = _plan(p1, tets, 1)
-        assert plan.tiles == (tag == "tile")
+    for tag, opts in (("table", None), ("entry", {"column_tables": 0}), ("thread", {"ring64": 0, "ring32": 0})):
+        plan = _plan(p1, tets, 1, opts)
         if tag == "entry":
             assert plan.sell_col_units == plan.sell_nnz
         else:
             assert plan.sell_col_units < 0.7 * plan.sell_nnz
         if vals is None:
-            # one assembly for every plan (same pattern): two assemblies' FP64 atomics may round
-            # differently in the last bit
             vals, b = plan.assemble(lk)
             inv = plan.jacobi(vals)
         u, it, rel, st = plan.pcg(vals, b, inv_diag=inv, tol=1e-8)
@@ -472,30 +465,27 @@ def test_spmv_layouts_agree(monkeypatch):
         ub, itb, relb, stb = plan.bicgstab(vals, b, inv_diag=inv, tol=1e-8)
         assert st == 0 and stm == 0 and stb == 0 and rel <= 2e-8 and relm <= 1e-8 and relb <= 2e-8
         out[tag] = (u, it, um, inner, ub, itb)
-    a, c, e = out["tile"], out["table"], out["entry"]
+    a, c, e = out["thread"], out["table"], out["entry"]
     assert c[1] == e[1] and torch.equal(c[0], e[0])
     assert c[3] == e[3] and torch.equal(c[2], e[2])
     assert c[5] == e[5] and torch.equal(c[4], e[4])
     assert abs(a[1] - c[1]) <= 1 and (torch.linalg.norm(a[0] - c[0]) / torch.linalg.norm(c[0])).item() <= 1e-9
-    assert abs(a[3] - c[3]) <= 3 and (torch.linalg.norm(a[2] - c[2]) / torch.linalg.norm(c[2])).item() <= 1e-7
+    assert abs(a[3] - c[3]) <= 10 and (torch.linalg.norm(a[2] - c[2]) / torch.linalg.norm(c[2])).item() <= 1e-7
 
 
-def test_canonical_csr_solver_path_matches(monkeypatch):
+def test_canonical_csr_solver_path_matches():
     """A plan without the sliced-ELL operator (the path taken when the sliced-ELL entry count passes
-    2^31; forced here with FEMK_SELL=0) runs FP64 PCG and the mixed solver on the canonical-CSR
-    kernels. Its row sums are lane-split shuffle reductions, so it agrees with the sliced-ELL plan to
-    rounding, and both meet the oracle's solution."""
+    2^31; chosen here with the solver_layout = 0 plan option) runs FP64 PCG and the mixed solver on
+    the canonical-CSR kernels. Its row sums are lane-split shuffle reductions, so it agrees with the
+    sliced-ELL plan to rounding, and both meet the oracle's solution."""
     pf, cf, tets, p1 = _mesh(32, 1)
     lk = torch.as_tensor(om.logk_field(len(tets), 1007), device="cuda")
-    for k in ("FEMK_TILE", "FEMK_SELL_UNI", "FEMK_SELL"):
-        monkeypatch.delenv(k, raising=False)
     sell = _plan(p1, tets, 1)
     vals, b = sell.assemble(lk)
     inv = sell.jacobi(vals)
     u, it, rel, st = sell.pcg(vals, b, inv_diag=inv, tol=1e-8)
     um, inner, _, relm, stm = sell.pcg_mixed(vals, b, inv, tol=1e-8)
-    monkeypatch.setenv("FEMK_SELL", "0")
-    csr = _plan(p1, tets, 1)
+    csr = _plan(p1, tets, 1, {"solver_layout": 0})
     uc, itc, relc, stc = csr.pcg(vals, b, inv_diag=inv, tol=1e-8)
     umc, innerc, _, relmc, stmc = csr.pcg_mixed(vals, b, inv, tol=1e-8)
     assert st == stm == stc == stmc == 0
@@ -647,44 +637,33 @@ def test_p0_linearity_and_support_on_device():
     assert np.abs(a[free] - fl[free]).max() <= 1e-12 * np.abs(fl).max()
 
 
-@pytest.mark.parametrize("n,order", [(8, 1), (4, 2)])
-def test_cluster_staged_matrix_free_matches(n, order, monkeypatch):
-    """The opt-in matrix-free operator on shared-memory-staged element clusters (FEMK_MATFREE_CL=1)
-    agrees with the assembled operator to 1e-12 and solves like it."""
-    monkeypatch.setenv("FEMK_MATFREE_CL", "1")
-    pf, cf, tets, p1 = _mesh(n, order, seed=5)
-    logk = om.logk_field(len(tets), 8)
-    plan = _plan(p1, tets, order)
-    lk = torch.as_tensor(logk, device="cuda")
-    vals, b = plan.assemble(lk)
-    xv = torch.as_tensor(np.random.default_rng(1).standard_normal(plan.n), device="cuda")
-    y = plan.spmv(vals, xv).cpu().numpy()
-    ym = plan.spmv_matfree(lk, xv).cpu().numpy()
-    assert np.abs(ym - y).max() <= 1e-12 * np.abs(y).max()
-    inv = plan.jacobi_matfree(lk)
-    u1, it1, _, _ = plan.pcg(vals, b, inv_diag=plan.jacobi(vals))
-    u2, it2, rel2, _ = plan.pcg_matfree(lk, b, inv_diag=inv)
-    assert abs(it1 - it2) <= 1 and rel2 <= 2e-8
-    assert torch.linalg.norm(u1 - u2) <= 1e-7 * torch.linalg.norm(u1)
 
 
-@pytest.mark.parametrize("mode", [0, 1])
-def test_mixed_fused_form_matches_split(mode, monkeypatch):
-    """The fused mixed iteration (FEMK_MIXED_FUSE=1: p formed from (z, p) pairs inside the step,
-    two kernels per iteration) runs the arithmetic of the three-kernel split: same inner and outer
-    counts and the same solution to rounding of the reductions' grid shapes."""
-    pf, cf, tets, p1 = _mesh(24, 1)
-    logk = om.logk_field(len(tets), 1001)
-    out = {}
-    for fuse in ("0", "1"):
-        monkeypatch.setenv("FEMK_MIXED_FUSE", fuse)
-        plan = _plan(p1, tets, 1)
+@pytest.mark.parametrize("n,order,opts", [(12, 1, {}), (12, 1, {"ring32": 0}), (12, 1, {"solver_layout": 0}),
+                                          (4, 2, {})])
+def test_mixed_single_reduction_loop(n, order, opts):
+    """The FP32 inner loop in single-reduction (Chronopoulos-Gear) form on each of its SpMV kernels
+    (bulk-copy ring, thread-per-row sliced ELL, canonical CSR; P2 rows wider than the ring): the
+    FP64 residual meets the 1e-8 stop rule, the solution agrees with a tight FP64 solve to 1e-7, the
+    FP32 iteration count stays near FP64 CG's, and graph replay and direct launches of the same
+    chunks give bit-identical iterates."""
+    pf, cf, tets, p1 = _mesh(n, order)
+    logk = om.logk_field(len(tets), 1011)
+    sols = []
+    for replay in (1, 0):
+        plan = _plan(p1, tets, order, {**opts, "graph_replay": replay})
         vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
         inv = plan.jacobi(vals)
-        u, inner, outer, rel, st = plan.pcg_mixed(vals, b, inv, tol=1e-8, mode=mode)
-        assert st == 0 and rel <= 1e-8
-        r = b - plan.spmv(vals, u)
-        assert (torch.linalg.norm(r) / torch.linalg.norm(b)).item() <= 1e-8
-        out[fuse] = (u, inner, outer)
-    assert abs(out["0"][1] - out["1"][1]) <= 2 and out["0"][2] == out["1"][2]
-    assert (torch.linalg.norm(out["0"][0] - out["1"][0]) / torch.linalg.norm(out["0"][0])).item() <= 1e-8
+        u64, it64, _, _ = plan.pcg(vals, b, inv_diag=inv, tol=1e-8)
+        ut, _, _, _ = plan.pcg(vals, b, inv_diag=inv, tol=1e-13)
+        for mode in (0, 1):
+            u, inner, outer, rel, st = plan.pcg_mixed(vals, b, inv, tol=1e-8, mode=mode)
+            assert st == 0 and rel <= 1e-8 and outer >= 2
+            r = b - plan.spmv(vals, u)
+            assert (torch.linalg.norm(r) / torch.linalg.norm(b)).item() <= 1e-8
+            assert (torch.linalg.norm(u - ut) / torch.linalg.norm(ut)).item() <= 1e-7
+            if mode == 0:
+                assert inner <= 1.25 * it64 + 16, (inner, it64)
+            sols.append((mode, u, inner, outer))
+    for (m0, u0, i0, o0), (m1, u1, i1, o1) in zip(sols[:2], sols[2:]):
+        assert m0 == m1 and i0 == i1 and o0 == o1 and torch.equal(u0, u1)
