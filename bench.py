@@ -5,11 +5,12 @@ One step = assemble the CSR operator for one of 20 seeded log-conductivity field
 inverse, run PCG from x0 = 0 to the 1e-8 relative stop rule and evaluate the eager residual guard
 (one more SpMV), with the mesh, plan and k fields resident in HBM. ``value`` = DOFs / step time
 (all ranks' DOFs over the max-over-ranks time). Variants (mixed precision, matrix-free), the SpMV
-roofline, the end-to-end number through the public ``jno_b200`` API with host buffers, SM clocks
-and a CPU baseline (the numpy/scipy oracle on a bounded sample) ride on the same JSON line.
+roofline, the end-to-end number through the public ``jno_b200`` API with host buffers, SM clocks,
+a CPU baseline (full steps of the path restated in C on all host threads) and full-size parity
+against that restatement ride on the same JSON line.
 
-``--impl reference`` times the oracle (the CPU restatement of jNO's path; jNO itself cannot be
-imported on this image) on the same workload instead.
+``--impl reference`` times that CPU restatement (jNO itself cannot be imported on this image) on
+the same workload instead, full steps on all host threads.
 """
 
 import argparse
@@ -189,106 +190,105 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-# ------------------------------------------------------------------------------------------ CPU oracle
-class CpuOracle:
-    """The oracle pipeline on the CPU: pattern and boundary set as setup, then timed samples."""
+# ------------------------------------------------------------------------------------------ CPU restatement
+class CpuPath:
+    """The path on the host: oracle/femcpu.c (C, OpenMP, FP64) -- the compress-plan pattern, the
+    row-gather assembly, the Jacobi inverse and jax-cg PCG -- on all host threads. Setup (mesh,
+    boundary set, incidence, pattern) is untimed; a step is a full assembly + Jacobi + PCG to 1e-8
+    from zero, nothing sampled or extrapolated."""
 
-    def __init__(self, n):
-        from oracle import assemble as oa
+    def __init__(self, n, order=1, cells=None, threads=None):
+        from oracle import build_cpu
         from oracle import mesh as om
 
-        self.oa = oa
-        self.n_h = n
-        self.pf, self.cf, self.tets, self.p1 = om.kuhn_cube(n, order=1, seed=0)
-        self.ndof = self.pf.shape[0]
-        self.indptr, self.indices, self.slot = oa.csr_pattern_fast(self.cf, self.ndof)
-        self.bnd = om.boundary_nodes(self.cf, 1)
-        self.fields = logk_fields(len(self.tets), 2)
+        self.n_h, self.order = n, order
+        pf, cf, tets, p1 = om.kuhn_cube(n, order=1, seed=0)
+        if order == 2:
+            cf = np.asarray(cells)  # the P2 numbering exported by the device plan (pinned at small sizes)
+        self.bnd = om.boundary_nodes(cf, order)
+        self.cpu = build_cpu.FemCpu(p1, cf, self.bnd, threads=threads)
+        self.ndof, self.ntet = self.cpu.nv, cf.shape[0]
+        self.threads = self.cpu.threads
 
-    def assemble_full(self, logk):
-        return self.oa.assemble(self.pf, self.cf, 1, self.bnd, np.exp(logk), plan=(self.indptr, self.indices,
-                                                                                   self.slot))
-
-    def sample(self, logk, iters_total, slab_fraction=8, cg_iters=20, system=None):
-        """Time 1/slab_fraction of the element assembly and cg_iters PCG iterations; extrapolate."""
-        from oracle import element as oe
-        from oracle import pcg as op
-
-        T = len(self.tets)
-        m = T // slab_fraction
+    def step(self, logk):
         t0 = time.perf_counter()
-        K, F = oe.element_matrices(self.p1[self.tets[:m]], 1)
-        Ke = np.exp(logk[:m])[:, None, None] * K
-        np.bincount(self.slot[: m * 16], weights=Ke.reshape(-1), minlength=self.indices.size)
-        np.bincount(self.cf[:m].reshape(-1), weights=F.reshape(-1), minlength=self.ndof)
-        t_asm = (time.perf_counter() - t0) * slab_fraction
-        if system is None:
-            system = self.assemble_full(logk)
-        A = system.csr()
-        t0 = time.perf_counter()
-        inv = self.oa.jacobi_inverse(self.oa.matrix_diagonal(system))
-        t_jac = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        op.pcg(A, system.b, inv, tol=1e-8, maxiter=cg_iters)
-        t_cg = time.perf_counter() - t0
-        t_total = t_asm + t_jac + t_cg / cg_iters * iters_total
-        desc = (f"oracle (numpy/scipy, FP64, 1 thread) on P1 {self.n_h}^3: element assembly of 1/{slab_fraction} "
-                f"of the tets x{slab_fraction}, Jacobi, {cg_iters} PCG iterations x {iters_total}/{cg_iters} "
-                f"(iterations of the full solve)")
-        return self.ndof / t_total, t_total, desc
+        it, rel = self.cpu.step(logk)
+        return time.perf_counter() - t0, it, rel
 
-    def torch_spmv(self, system, reps=10):
-        """The same CSR matvec through torch's multi-threaded CPU sparse kernel (ms per matvec)."""
-        import torch
 
-        A = system.csr()
-        At = torch.sparse_csr_tensor(torch.as_tensor(A.indptr.astype(np.int64)),
-                                     torch.as_tensor(A.indices.astype(np.int64)), torch.as_tensor(A.data),
-                                     size=A.shape)
-        xv = torch.ones(A.shape[0], dtype=torch.float64)
-        At @ xv
-        t0 = time.perf_counter()
-        for _ in range(reps):
-            At @ xv
-        ms = (time.perf_counter() - t0) / reps * 1e3
-        return {"ms_per_matvec": ms, "threads": torch.get_num_threads(),
-                "GB/s": (12 * A.nnz + 20 * A.shape[0]) / (ms / 1e3) / 1e9}
+def cpu_steps(cpu, fields, steps, warmup=0):
+    """(mean seconds per full step, iterations) of `steps` timed steps after `warmup` untimed ones."""
+    times, iters = [], []
+    for i in range(warmup + steps):
+        t, it, rel = cpu.step(fields[i % len(fields)])
+        if not rel <= 1e-4:
+            raise RuntimeError(f"CPU PCG did not solve (relres {rel})")
+        if i >= warmup:
+            times.append(t)
+            iters.append(it)
+    return float(np.mean(times)), float(np.mean(iters))
 
 
 def run_reference(args):
+    """The reference arm: jNO's own path cannot run on this image (no jax), so the C/OpenMP
+    restatement of the path (oracle/femcpu.c) times full steps of the same workload on all host
+    threads. Rank 0 alone runs it; other ranks exit without work."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cpu = CpuOracle(args.n)
-    sys_full = cpu.assemble_full(cpu.fields[0])
-    from oracle import pcg as op
-
-    A = sys_full.csr()
-    x, iters, _ = op.pcg(A, sys_full.b, cpu.oa.jacobi_inverse(cpu.oa.matrix_diagonal(sys_full)), tol=1e-8)
-    vals, totals = [], []
-    desc = ""
-    # one step is a bounded sample: about 4 s of host work at (1/8 of the tets, 20 PCG iterations),
-    # shrunk for long runs so that the whole --steps/--warmup run stays within a few minutes
-    n_samples = args.warmup + args.steps
-    slab, cg_iters = (8, 20) if n_samples <= 20 else ((16, 12) if n_samples <= 40 else (32, 8))
-    for i in range(n_samples):
-        v, t, desc = cpu.sample(cpu.fields[0], iters, slab_fraction=slab, cg_iters=cg_iters, system=sys_full)
-        if i >= args.warmup:
-            vals.append(v)
-            totals.append(t)
-    value = cpu.ndof / float(np.mean(totals))
+    cpu = CpuPath(args.n)
+    fields = logk_fields(cpu.ntet, N_FIELDS)
+    sec, iters = cpu_steps(cpu, fields, args.steps, args.warmup)
+    value = cpu.ndof / sec
+    desc = (f"oracle/femcpu.c (C, OpenMP, FP64) on {cpu.threads} host threads: {args.steps} full steps of P1 "
+            f"{args.n}^3 (assembly + Jacobi + PCG to 1e-8 from zero, {iters:.1f} iterations), after {args.warmup} "
+            f"warm-up steps; nothing sampled or extrapolated")
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(totals)) * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded jittered Kuhn cube, lognormal P0 k)",
-        "config": {"workload": workload_desc(args.n, 1, len(cpu.tets), cpu.ndof, cpu.indices.size),
-                   "iterations": iters, "parallelism": "cpu, 1 thread"},
-        "cpu_baseline": {"value": value, "unit": "DOF/s", "cores": 1, "kind": "port", "sample": desc},
+        "config": {"workload": workload_desc(args.n, 1, cpu.ntet, cpu.ndof, cpu.cpu.indices.size),
+                   "iterations": iters, "parallelism": f"cpu, {cpu.threads} threads (OpenMP)"},
+        "cpu_baseline": {"value": value, "unit": "DOF/s", "cores": cpu.threads, "kind": "port", "sample": desc},
         "e2e": {"value": value, "unit": "DOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "jNO (JAX) cannot be imported on this image; the oracle port stands in for its CPU path",
+        "note": "jNO (JAX) cannot be imported on this image; its path restated in C stands in for its CPU path",
     }
     print(json.dumps(out), flush=True)
+
+
+def parity_full_size(plan, fields_h, dev, cpu=None):
+    """The device path against the CPU restatement at the benchmark size, field 0: CSR pattern
+    bit-exact, values and load within 1e-12 of the largest entry, PCG iterations and solution."""
+    import torch
+
+    cpu = cpu or CpuPath(round(plan.ntet ** (1 / 3) / 6 ** (1 / 3)), plan.order,
+                         cells=plan.export()["cells"].cpu().numpy() if plan.order == 2 else None)
+    ip, ind = plan.pattern()
+    same_pattern = bool(np.array_equal(ip.cpu().numpy(), cpu.cpu.indptr) and
+                        np.array_equal(ind.cpu().numpy(), cpu.cpu.indices))
+    same_dirichlet = bool(np.array_equal(np.flatnonzero(plan.export()["dirichlet_mask"].cpu().numpy()), cpu.bnd))
+    lk = fields_h[0]
+    vals, b = plan.assemble(torch.as_tensor(lk, device=dev))
+    vc, bc = cpu.cpu.assemble(lk)
+    v_err = float(np.abs(vals.cpu().numpy() - vc).max() / np.abs(vc).max())
+    b_err = float(np.abs(b.cpu().numpy() - bc).max() / np.abs(bc).max())
+    out = {"workload": f"P{plan.order} ({plan.ntet:,} tets, {plan.n:,} DOF, {plan.nnz:,} nnz), k field 0",
+           "pattern_bit_exact": same_pattern, "dirichlet_bit_exact": same_dirichlet,
+           "max_val_err_rel": v_err, "max_b_err_rel": b_err}
+    if plan.order == 1:
+        inv = plan.jacobi(vals)
+        x, it, rel, st = plan.pcg(vals, b, inv_diag=inv, tol=1e-8)
+        cpu.cpu.jacobi()
+        xc, itc, relc = cpu.cpu.pcg(1e-8)
+        out.update({"iterations": it, "iterations_cpu": itc, "relres": rel,
+                    "x_err_rel": float(np.linalg.norm(x.cpu().numpy() - xc) / np.linalg.norm(xc))})
+    out["bars"] = ("pattern and Dirichlet set bit-exact; values and b <= 1e-12 of max; iterations within 1; "
+                   "x within 1e-7")
+    out["met"] = bool(same_pattern and same_dirichlet and v_err <= 1e-12 and b_err <= 1e-12 and
+                      (plan.order == 2 or (abs(out["iterations"] - out["iterations_cpu"]) <= 1 and
+                                           out["x_err_rel"] <= 1e-7)))
+    return out
 
 
 # ------------------------------------------------------------------------------------------ replicas
@@ -325,8 +325,9 @@ def roofline_traffic():
 
 
 
-def p2_variants(args, world, dev, timed):
-    """P2 tets at 64^3 hexes (2.15M DOF): FP64 and mixed assemble + solve, 3 steps each."""
+def p2_variants(args, world, dev, timed, parity=False):
+    """P2 tets at 64^3 hexes (2.15M DOF): FP64 and mixed assemble + solve, 3 steps each (and, with
+    ``parity``, the values against the CPU restatement: returned under "parity")."""
     import torch
 
     from jno_b200.plan import FemPlan
@@ -362,7 +363,8 @@ def p2_variants(args, world, dev, timed):
     plan.pcg_mixed(vals, b, inv, x, tol=1e-8)
     err = (torch.linalg.norm(x - x_ref) / torch.linalg.norm(x_ref)).item()
     base = {"workload": f"P2 64^3 Kuhn tets ({plan.ntet:,} tets, {plan.n:,} DOF, {plan.nnz:,} nnz)"}
-    return {
+    out_parity = parity_full_size(plan, [f.cpu().numpy() for f in fields], dev) if parity else None
+    return out_parity, {
         "p2_64_fp64": {**base, "value": world * plan.n / (ms64 / 1e3), "unit": "DOF/s", "ms_per_step": ms64,
                        "iters": float(np.mean(info["it"]))},
         "p2_64_mixed": {**base, "value": world * plan.n / (ms32 / 1e3), "unit": "DOF/s", "ms_per_step": ms32,
@@ -484,61 +486,106 @@ def batched_variant(dev, count=256, reps=3):
                       "status_ok": bool(stm == 0), "max_err_vs_fp64_batched": err}}
 
 
-def adjoint_variant(dev, n=64, n_fd=32):
+def adjoint_variant(dev, n=64, n_fd=32, check=True):
     """Adjoint config: J = 1/2 sum_i M_ii (u_i - u*_i)^2 at P1 64^3, dJ/dlogk by the adjoint (forward
-    solve + transposed solve + element contraction), checked by FP64 central differences on n_fd
-    random elements."""
+    solve + transposed solve + element contraction). Checked (``check``) against the adjoint computed
+    on the host by the C restatement (every element) and against central differences on n_fd random
+    elements, evaluated without cancellation (jno_b200.autograd.central_difference)."""
     import torch
 
-    from jno_b200.autograd import solve_p0
+    from jno_b200.autograd import central_difference, solve_p0
     from jno_b200.plan import FemPlan
 
     pts, tets = make_mesh(n)
     plan = FemPlan(pts, tets, 1)
-    logk = torch.as_tensor(np.random.default_rng(FIELD_SEED0).normal(0, 0.5, plan.ntet), device=dev)
-    lk_star = torch.as_tensor(np.random.default_rng(2000).normal(0, 0.5, plan.ntet), device=dev)
+    logk_h = np.random.default_rng(FIELD_SEED0).normal(0, 0.5, plan.ntet)
+    lk_star_h = np.random.default_rng(2000).normal(0, 0.5, plan.ntet)
+    logk = torch.as_tensor(logk_h, device=dev)
     m = plan.lumped_mass()
     with torch.no_grad():
-        ustar = solve_p0(plan, lk_star, tol=1e-12)
-
-    def J_of(v, tol):
-        with torch.no_grad():
-            u = solve_p0(plan, v, tol=tol)
-            return (0.5 * torch.sum(m * (u - ustar) ** 2)).item()
+        ustar = solve_p0(plan, torch.as_tensor(lk_star_h, device=dev), tol=1e-13)
 
     def grad_once(tol=1e-10):
         lk = logk.clone().requires_grad_(True)
         u = solve_p0(plan, lk, tol=tol)
         J = 0.5 * torch.sum(m * (u - ustar) ** 2)
-        J.backward()
-        return lk.grad
+        (g,) = torch.autograd.grad(J, lk)
+        return g
 
     grad_once()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = 3
+    e0.record()
     for _ in range(reps):
-        g = grad_once()
+        grad_once()
+    e1.record()
     torch.cuda.synchronize()
-    ms = (time.perf_counter() - t0) / reps * 1e3
+    out = {"workload": f"P1 {n}^3 ({plan.ntet:,} tets), gradient of a lumped-mass misfit w.r.t. per-element log k",
+           "ms_per_gradient": e0.elapsed_time(e1) / reps, "timing_tol": 1e-10}
+    if not check:
+        return out
     g = grad_once(tol=1e-13).cpu().numpy()
-    rng = np.random.default_rng(7)
-    idx = rng.choice(plan.ntet, n_fd, replace=False)
-    base = logk.cpu().numpy()
-    eps = 1e-6
-    errs, errs_g = [], []
     gmax = float(np.abs(g).max())
-    for c in idx:
-        e = np.zeros(plan.ntet)
-        e[c] = eps
-        fd = (J_of(torch.as_tensor(base + e, device=dev), 1e-14) - J_of(torch.as_tensor(base - e, device=dev), 1e-14)) / (2 * eps)
-        errs.append(abs(fd - g[c]) / max(abs(fd), 1e-300))
-        errs_g.append(abs(fd - g[c]) / gmax)
-    return {"workload": f"P1 {n}^3 ({plan.ntet:,} tets), gradient of a lumped-mass misfit w.r.t. per-element log k",
-            "ms_per_gradient": ms, "fd_checked_elements": n_fd, "fd_step": eps,
-            "max_rel_err_vs_fd": float(np.max(errs)), "median_rel_err_vs_fd": float(np.median(errs)),
-            "max_err_vs_fd_rel_to_max_grad": float(np.max(errs_g)),
-            "note": "forward + adjoint PCG at tol 1e-10 for the timing; 1e-13/1e-14 for the FD check"}
+    # the adjoint on the host (C restatement: assembly + PCG to 1e-13 for u and lambda; numpy contraction)
+    from oracle import element as oe
+
+    cpu = CpuPath(n)
+    us_h = ustar.cpu().numpy()
+    mass_h = m.cpu().numpy()
+    cpu.cpu.assemble(logk_h)
+    cpu.cpu.jacobi()
+    u_h = cpu.cpu.pcg(1e-13)[0].copy()
+    cpu.cpu.b[:] = mass_h * (u_h - us_h)
+    lam_h = cpu.cpu.pcg(1e-13)[0].copy()
+    free = 1.0 - cpu.cpu.dmask.astype(np.float64)
+    K, _ = oe.element_matrices(oe.vertices(cpu.cpu.xyz, cpu.cpu.tets.astype(np.int64)), 1)
+    cells = cpu.cpu.tets.astype(np.int64)
+    g_h = -np.exp(logk_h) * np.einsum("ta,tab,tb->t", (free * lam_h)[cells], K, (free * u_h)[cells])
+    idx = np.random.default_rng(7).choice(plan.ntet, n_fd, replace=False)
+    eps = 1e-6
+    fd = central_difference(plan, logk_h, us_h, mass_h, idx, eps=eps)
+    big = np.abs(g[idx]) > 1e-3 * gmax
+    out.update({
+        "max_err_vs_host_adjoint_rel_max_grad": float(np.abs(g - g_h).max() / gmax),
+        "fd_checked_elements": n_fd, "fd_step": eps,
+        "max_err_vs_fd_rel_max_grad": float(np.abs(fd - g[idx]).max() / gmax),
+        "max_rel_err_vs_fd_where_g_gt_1e-3_max": float(np.max(np.abs(fd - g[idx])[big] / np.abs(g[idx])[big]))
+        if big.any() else None,
+        "fd_method": ("(J(+eps) - J(-eps)) / 2 eps with J(+) - J(-) = sum M d (u- + d/2 - u*), d solving "
+                      "A(+) d = (A(-) - A(+)) u-: no subtractive cancellation; truncation O(eps^2), solves to 1e-13"),
+        "target": "1e-6 relative (north star); jax.grad cannot run here, the host adjoint stands in",
+    })
+    return out
+
+
+def summary_of(out):
+    """The key figures of a bench line in one small object (variants, parity, baselines)."""
+    v = out.get("variants") or {}
+
+    def pick(key, *fields):
+        d = v.get(key) or {}
+        return {f: d.get(f) for f in fields if f in d} or None
+
+    par = out.get("parity") or {}
+    return {
+        "fp64_DOF_per_s": out["value"], "ms_per_step": out["ms_per_step"],
+        "spmv_frac_of_hbm": (out.get("roofline") or {}).get("frac"),
+        "mixed_vs_fp64": pick("mixed_fp32_fp64_reliable", "speedup_vs_fp64", "ms_per_step", "inner_iters",
+                              "err_vs_fp64_tight"),
+        "mixed_1e-10": pick("mixed_1e-10_vs_fp64_1e-10", "speedup_vs_fp64", "err_vs_fp64_tight"),
+        "p2_64": {"fp64_ms": (v.get("p2_64_fp64") or {}).get("ms_per_step"),
+                  "mixed_ms": (v.get("p2_64_mixed") or {}).get("ms_per_step"),
+                  "mixed_speedup": (v.get("p2_64_mixed") or {}).get("speedup_vs_fp64")} if "p2_64_fp64" in v else None,
+        "adjoint_p1_64": pick("adjoint_p1_64", "ms_per_gradient", "max_err_vs_host_adjoint_rel_max_grad",
+                              "max_err_vs_fd_rel_max_grad", "max_rel_err_vs_fd_where_g_gt_1e-3_max"),
+        "matrix_free_ms": (v.get("matrix_free_fp64") or {}).get("ms_per_step"),
+        "batched_ms": (v.get("batched_256") or {}).get("ms_per_batch"),
+        "parity_met": {k: p.get("met") for k, p in par.items()} or None,
+        "e2e_DOF_per_s": (out.get("e2e") or {}).get("value"),
+        "cpu_baseline_DOF_per_s": (out.get("cpu_baseline") or {}).get("value"),
+        "cpu_threads": (out.get("cpu_baseline") or {}).get("cores"),
+    }
 
 
 def run_ours(args):
@@ -719,6 +766,7 @@ def run_ours(args):
                                          "bytes_per_launch": csr_bytes}}
 
     variants = {}
+    p2_parity = None
     if not args.no_variants:
         # FP64 tight reference solution for error reporting
         plan.assemble(fields[0], vals=vals, b=b)
@@ -802,7 +850,7 @@ def run_ours(args):
 
         def fstep(i):
             lk = fields[i % N_FIELDS]
-            plan.assemble(lk, vals=None, b=b)
+            plan.load(lk, b=b)
             plan.jacobi_matfree(lk, out=inv)
             x.zero_()
             _, it, rel, st = plan.pcg_matfree(lk, b, x, inv, tol=1e-8)
@@ -842,10 +890,11 @@ def run_ours(args):
                                       "note": "bytes: values read twice + columns + kept entries + row arrays"}
         variants["spmv_sell_fp64"] = {"GB/s": achieved, "frac_of_peak": achieved / peak, "ms_in_loop": sell_ms,
                                       "ms_standalone": sell_standalone_ms}
-        variants.update(p2_variants(args, world, dev, timed))
+        p2_parity, p2 = p2_variants(args, world, dev, timed, parity=rank == 0 and world == 1 and not args.no_cpu_baseline)
+        variants.update(p2)
         variants.update(tri_variants(world, dev, timed))
         variants["theta_p1_128"] = theta_variant(plan, fields, dev, timed)
-        variants["adjoint_p1_64"] = adjoint_variant(dev)
+        variants["adjoint_p1_64"] = adjoint_variant(dev, check=rank == 0 and world == 1 and not args.no_cpu_baseline)
         variants["batched_256"] = batched_variant(dev)
 
     # ---- end to end through the public API with host buffers
@@ -928,12 +977,19 @@ def run_ours(args):
            "path": "jno_b200.fem(...).operator.evaluate({'logk'}) + jno_b200.solve.cg(tol=1e-8)(A, b, M=jacobi())"}
 
     cpu_baseline = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = CpuOracle(args.n)
-        system = cpu.assemble_full(fields_h[0])
-        v_cpu, t_cpu, desc = cpu.sample(fields_h[0], int(round(iters_mean)), system=system)
-        cpu_baseline = {"value": v_cpu, "unit": "DOF/s", "cores": 1, "kind": "port", "sample": desc,
-                        "host_cpus": os.cpu_count(), "torch_cpu_csr_spmv": cpu.torch_spmv(system)}
+        cpu = CpuPath(args.n, args.order, cells=plan.export()["cells"].cpu().numpy() if args.order == 2 else None)
+        parity = {f"p{args.order}_{args.n}": parity_full_size(plan, fields_h, dev, cpu)}
+        if p2_parity is not None:
+            parity["p2_64"] = p2_parity
+        k_cpu = 3
+        sec, it_cpu = cpu_steps(cpu, fields_h, k_cpu)
+        cpu_baseline = {"value": cpu.ndof / sec, "unit": "DOF/s", "cores": cpu.threads, "kind": "port",
+                        "sample": (f"oracle/femcpu.c (C, OpenMP, FP64) on {cpu.threads} host threads: {k_cpu} full "
+                                   f"steps of the same workload (assembly + Jacobi + PCG to 1e-8 from zero, "
+                                   f"{it_cpu:.1f} iterations, fields 0-{k_cpu - 1}), {sec * 1e3:.0f} ms per step"),
+                        "host_cpus": os.cpu_count()}
 
     if world > 1:
         dist.barrier()
@@ -950,9 +1006,10 @@ def run_ours(args):
                        "plan_setup_s": setup_s,
                        "l2": "inputs larger than L2 (381 MB CSR stream per SpMV vs 126 MB L2)",
                        "parallelism": f"replicas x{world} (independent problems per GPU, no collective)"},
-            "variants": variants, "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e,
+            "variants": variants, "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e, "parity": parity,
             "gpu_launches": int(launches), "clocks": clk,
         }
+        out["summary"] = summary_of(out)  # last key: the end of the line carries the key figures
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -178,6 +178,20 @@ int femk_assemble(const femk_plan* plan, const double* param_dev, int coef_mode,
                   double f, const double* g_dev, double* vals_dev, double* b_dev, void* stream);
 
 /*
+ * Vector-Jacobian product of femk_assemble with respect to its parameter (the reverse pass jax.grad
+ * takes through the parametric assembly: segment_sum and the per-cell jacfwd, fem_native.py:2318-2334,
+ * and the Dirichlet lift b -= A e g). Given cotangents grad_vals_dev f64[nnz] of the values and
+ * grad_b_dev f64[n] of the load (either may be NULL = zero), grad_param_dev receives
+ *   P0 modes: f64[ntet], grad[e] = dk_e/dparam_e * S_e,
+ *   nodal modes: f64[nvert], grad[i] = sum over elements e holding vertex i of S_e * dk_e/dparam_i,
+ *   S_e = sum_{a,b free} grad_vals[slot(e,a,b)] K_hat_e[a,b] - sum_{a free, b Dirichlet} grad_b[a] K_hat_e[a,b] g[b].
+ * param, mode, scale and g are those of the femk_assemble call (CONST has no parameter: FEMK_EINVAL).
+ */
+int femk_assemble_vjp(const femk_plan* plan, const double* param_dev, int coef_mode, double coef_scale,
+                      const double* g_dev, const double* grad_vals_dev, const double* grad_b_dev,
+                      double* grad_param_dev, void* stream);
+
+/*
  * Compact export of assembled values: the canonical CSR entries with |v| > 0, in CSR order (rows
  * ascending, columns ascending). Exact zeros (the zeroed Dirichlet rows and columns, values that
  * summed to 0) and NaNs are dropped.

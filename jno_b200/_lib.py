@@ -104,6 +104,7 @@ SIGNATURES = {
     "femk_plan_get_info": [_P, ctypes.POINTER(PlanInfo)],
     "femk_plan_export": [_P, _P, _P, _P, _P, _P, _P, _P, _P],
     "femk_assemble": [_P, _P, _I, _D, _D, _P, _P, _P, _P],
+    "femk_assemble_vjp": [_P, _P, _I, _D, _P, _P, _P, _P, _P],
     "femk_compact": [_P, _P, _P, _P, _P, _I64, ctypes.POINTER(_I64), _P],
     "femk_element_matrices": [_P, _P, _P, _P],
     "femk_jacobi": [_P, _P, _P, _P],

@@ -33,7 +33,7 @@ def batched_workload(count=256, seed=42, lo=8, hi=48, amp=0.1):
 class BatchedPoisson:
     """``k_e grad u . grad v - f v`` with u = 0 on each problem's boundary, for a list of P1 meshes."""
 
-    def __init__(self, meshes):
+    def __init__(self, meshes, options=None):
         pts, tets, row_off, tet_off = [], [], [0], [0]
         for p, t in meshes:
             tets.append(np.asarray(t, dtype=np.int64) + row_off[-1])
@@ -42,7 +42,7 @@ class BatchedPoisson:
             tet_off.append(tet_off[-1] + len(t))
         self.row_off = np.asarray(row_off, dtype=np.int64)
         self.tet_off = np.asarray(tet_off, dtype=np.int64)
-        self.plan = FemPlan(np.concatenate(pts), np.concatenate(tets), 1)
+        self.plan = FemPlan(np.concatenate(pts), np.concatenate(tets), 1, options=options)
         self.nprob = len(meshes)
 
     def assemble(self, logk):

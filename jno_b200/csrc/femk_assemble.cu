@@ -1,5 +1,5 @@
-// Fused parametric assembly: element geometry -> local stiffness -> scatter-add through the
-// element -> CSR slot map -> symmetric Dirichlet elimination -> RHS, in one pass over elements.
+// Parametric assembly: element geometry -> local stiffness -> CSR values -> symmetric Dirichlet
+// elimination -> RHS.
 //
 // Replaces FemLinearSystem.evaluate (jno/trace/__init__.py:3612-3615) -> _assemble_at
 // (jno/utils/solver/fem_native.py:3311-3316): per-cell jacfwd (fem_native.py:2333-2334) +
@@ -9,6 +9,15 @@
 // Dirichlet semantics of the parametric route: entries in a Dirichlet row or column are stored as
 // explicit zeros (they are never added), the diagonal slot of a Dirichlet row holds exactly 1
 // (masked 0 + the appended unit triplet), b[d] = g[d], and free rows receive b -= A e.
+//
+// femk_assemble gathers instead of scattering: each CSR row is owned by one thread, which walks the
+// row's DOF -> element incidence list (ascending element ids) and adds the row's entries of each
+// element matrix, in that fixed order, into the row's values staged in shared memory; a block's
+// rows are consecutive, so their values form one contiguous span that the block zeroes, accumulates
+// and writes back with coalesced stores. Columns are found by binary search in the block's staged
+// column indices. No atomics: the values and the load are the same bits on every run (the
+// segment_sum of the reference has no defined order either). Each element's geometry is evaluated
+// once per incident row (4 times for P1, 10 for P2), which the FP64 units absorb.
 #include <cmath>
 
 #include "femk_element.cuh"
@@ -19,40 +28,111 @@ namespace {
 
 constexpr int kThreads = 128;
 
-template <int ND>
-__global__ void __launch_bounds__(kThreads) k_assemble(const double* __restrict__ xyz, const int32_t* __restrict__ cells,
-                                                       int64_t ntet, const int32_t* __restrict__ slot,
-                                                       const uint8_t* __restrict__ dmask, const double* __restrict__ param,
-                                                       int mode, double scale, double f, const double* __restrict__ g,
-                                                       double* __restrict__ vals, double* __restrict__ b) {
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
-    int32_t dof[ND];
+__device__ __forceinline__ int32_t search_col(const int32_t* cols, int32_t len, int32_t col) {
+  int32_t lo = 0, hi = len;
+  while (lo < hi) {
+    const int32_t mid = (lo + hi) >> 1;
+    if (cols[mid] < col)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Row A of one element matrix (A compile-time: the element matrices stay in registers) added into
+// the row's staged values; returns the row's load contribution f fhat_A - sum over Dirichlet
+// columns of k K_hat[A][c] g[c].
+template <int ND, int A, bool VALS>
+__device__ __forceinline__ double add_row(const double (&VG)[Cell<ND>::NV][Cell<ND>::NV], double vol, double k,
+                                          const int32_t (&dof)[ND], const uint8_t* __restrict__ dmask,
+                                          const double* __restrict__ g, double f, const int32_t* scl, int32_t len,
+                                          double* svl, int* __restrict__ err) {
+  double bi = f * fhat<ND>(vol, A);
 #pragma unroll
-    for (int a = 0; a < ND; ++a) dof[a] = __ldg(cells + c * ND + a);
-    Geom<Cell<ND>::NV> T;
-    cell_geometry(xyz, dof, T);
-    double VG[Cell<ND>::NV][Cell<ND>::NV];
-    gram(T, VG);
-    const double k = coef_of(param, mode, scale, c);
-    bool dir[ND];
-#pragma unroll
-    for (int a = 0; a < ND; ++a) dir[a] = __ldg(dmask + dof[a]) != 0;
-    const int32_t* srow = slot + c * ND * ND;
-#pragma unroll
-    for (int a = 0; a < ND; ++a) {
-      if (dir[a]) continue;
-      double rhs = f * fhat<ND>(T.vol, a);
-#pragma unroll
-      for (int bb = 0; bb < ND; ++bb) {
-        const double kab = k * khat<ND>(VG, a, bb);
-        if (dir[bb]) {
-          if (g) rhs -= kab * __ldg(g + dof[bb]);
-        } else if (vals) {
-          atomicAdd(vals + __ldg(srow + a * ND + bb), kab);
-        }
-      }
-      atomicAdd(b + dof[a], rhs);
+  for (int c = 0; c < ND; ++c) {
+    const double kac = k * khat<ND>(VG, A, c);
+    if (__ldg(dmask + dof[c])) {
+      if (g) bi -= kac * __ldg(g + dof[c]);
+    } else if (VALS) {
+      const int32_t pos = search_col(scl, len, dof[c]);
+      if (pos < len && scl[pos] == dof[c])
+        svl[pos] += kac;
+      else
+        atomicOr(err, 1);  // the pattern was built from these cells: unreachable
     }
+  }
+  return bi;
+}
+
+template <int ND, int A, bool VALS>
+__device__ __forceinline__ double add_row_at(int a, const double (&VG)[Cell<ND>::NV][Cell<ND>::NV], double vol,
+                                             double k, const int32_t (&dof)[ND], const uint8_t* __restrict__ dmask,
+                                             const double* __restrict__ g, double f, const int32_t* scl, int32_t len,
+                                             double* svl, int* __restrict__ err) {
+  if constexpr (A + 1 < ND) {
+    if (a != A) return add_row_at<ND, A + 1, VALS>(a, VG, vol, k, dof, dmask, g, f, scl, len, svl, err);
+  }
+  return add_row<ND, A, VALS>(VG, vol, k, dof, dmask, g, f, scl, len, svl, err);
+}
+
+// One thread per row (blockDim.x consecutive rows per block); VALS: the CSR values are assembled
+// (else the load alone, for matrix-free use). Shared memory: span_cap doubles of values + span_cap
+// int32 columns, span_cap = the plan's largest block span.
+template <int ND, bool VALS>
+__global__ void __launch_bounds__(kThreads) k_assemble_rows(
+    const double* __restrict__ xyz, const int32_t* __restrict__ cells, const int32_t* __restrict__ inc_ptr,
+    const int32_t* __restrict__ inc_elem, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+    const uint8_t* __restrict__ dmask, const int32_t* __restrict__ diag, int64_t n, int span_cap,
+    const double* __restrict__ param, int mode, double scale, double f, const double* __restrict__ g,
+    double* __restrict__ vals, double* __restrict__ b, int* __restrict__ err) {
+  constexpr int NV = Cell<ND>::NV;
+  extern __shared__ __align__(16) unsigned char asm_smem[];
+  double* sv = reinterpret_cast<double*>(asm_smem);
+  int32_t* sc = reinterpret_cast<int32_t*>(sv + span_cap);
+  const int64_t r0 = (int64_t)blockIdx.x * blockDim.x;
+  const int64_t r1 = r0 + blockDim.x < n ? r0 + blockDim.x : n;
+  const int32_t base = VALS ? __ldg(indptr + r0) : 0;
+  const int32_t span = VALS ? __ldg(indptr + r1) - base : 0;
+  if (VALS) {
+    for (int32_t k = threadIdx.x; k < span; k += blockDim.x) {
+      sv[k] = 0.0;
+      sc[k] = __ldg(indices + base + k);
+    }
+    __syncthreads();
+  }
+  const int64_t row = r0 + threadIdx.x;
+  if (row < r1) {
+    const int32_t lo = VALS ? __ldg(indptr + row) - base : 0;
+    const int32_t len = VALS ? __ldg(indptr + row + 1) - base - lo : 0;
+    if (__ldg(dmask + row)) {
+      if (VALS) sv[__ldg(diag + row) - base] = 1.0;
+      b[row] = g ? __ldg(g + row) : 0.0;
+    } else {
+      double bi = 0.0;
+      const int32_t j1 = __ldg(inc_ptr + row + 1);
+      for (int32_t j = __ldg(inc_ptr + row); j < j1; ++j) {
+        const int64_t e = __ldg(inc_elem + j);
+        int32_t dof[ND];
+#pragma unroll
+        for (int q = 0; q < ND; ++q) dof[q] = __ldg(cells + e * ND + q);
+        int a = 0;
+#pragma unroll
+        for (int q = 1; q < ND; ++q)
+          if (dof[q] == (int32_t)row) a = q;
+        Geom<NV> T;
+        cell_geometry(xyz, dof, T);
+        double VG[NV][NV];
+        gram(T, VG);
+        const double k = coef_of(param, mode, scale, e);
+        bi += add_row_at<ND, 0, VALS>(a, VG, T.vol, k, dof, dmask, g, f, sc + lo, len, sv + lo, err);
+      }
+      b[row] = bi;
+    }
+  }
+  if (VALS) {
+    __syncthreads();
+    for (int32_t k = threadIdx.x; k < span; k += blockDim.x) vals[base + k] = sv[k];
   }
 }
 
@@ -66,15 +146,6 @@ __global__ void k_nodal_coef(const int32_t* __restrict__ cells, int64_t ntet, co
 #pragma unroll
     for (int i = 0; i < NV; ++i) v[i] = __ldg(cells + c * NV + i);
     ke[c] = coef_nodal<NV>(param, mode, 1.0, v);
-  }
-}
-
-__global__ void k_dirichlet_rows(const int32_t* __restrict__ dlist, int64_t nd, const int32_t* __restrict__ diag,
-                                 const double* __restrict__ g, double* __restrict__ vals, double* __restrict__ b) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nd; t += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t d = dlist[t];
-    if (vals) vals[diag[d]] = 1.0;
-    b[d] = g ? g[d] : 0.0;
   }
 }
 
@@ -294,6 +365,105 @@ __global__ void k_adjoint_nodal(const double* __restrict__ xyz, const int32_t* _
   }
 }
 
+// Vector-Jacobian product of femk_assemble with respect to its parameter: given the cotangents
+// gv of the values and gb of the load, S_e = sum_{a,b free} gv[slot(e,a,b)] K_hat_ab
+// - sum_{a free, b Dirichlet} gb[a] K_hat_ab g[b] (the lift b -= A e g), and d(vals, b)/dparam_e
+// = dk_e/dparam_e times that pattern. P0 modes: grad[e] = dk_e S_e (one write per element).
+template <int ND>
+__device__ __forceinline__ double vjp_sum(const double (&VG)[Cell<ND>::NV][Cell<ND>::NV], const int32_t (&dof)[ND],
+                                          const bool (&dir)[ND], const int32_t* __restrict__ srow,
+                                          const double* __restrict__ gv, const double* __restrict__ gb,
+                                          const double* __restrict__ g) {
+  double acc = 0.0;
+#pragma unroll
+  for (int a = 0; a < ND; ++a) {
+    if (dir[a]) continue;
+    const double gba = (gb && g) ? __ldg(gb + dof[a]) : 0.0;
+#pragma unroll
+    for (int bb = 0; bb < ND; ++bb) {
+      const double kab = khat<ND>(VG, a, bb);
+      if (!dir[bb]) {
+        if (gv) acc += __ldg(gv + __ldg(srow + a * ND + bb)) * kab;
+      } else if (gb && g) {
+        acc -= gba * kab * __ldg(g + dof[bb]);
+      }
+    }
+  }
+  return acc;
+}
+
+template <int ND>
+__global__ void __launch_bounds__(kThreads) k_assemble_vjp(const double* __restrict__ xyz,
+                                                           const int32_t* __restrict__ cells, int64_t ntet,
+                                                           const int32_t* __restrict__ slot,
+                                                           const uint8_t* __restrict__ dmask,
+                                                           const double* __restrict__ param, int mode, double scale,
+                                                           const double* __restrict__ g, const double* __restrict__ gv,
+                                                           const double* __restrict__ gb, double* __restrict__ grad) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t dof[ND];
+    bool dir[ND];
+#pragma unroll
+    for (int a = 0; a < ND; ++a) {
+      dof[a] = __ldg(cells + c * ND + a);
+      dir[a] = __ldg(dmask + dof[a]) != 0;
+    }
+    Geom<Cell<ND>::NV> T;
+    cell_geometry(xyz, dof, T);
+    double VG[Cell<ND>::NV][Cell<ND>::NV];
+    gram(T, VG);
+    const double S = vjp_sum<ND>(VG, dof, dir, slot + c * ND * ND, gv, gb, g);
+    const double dk = mode == FEMK_COEF_EXP ? scale * exp(__ldg(param + c)) : scale;
+    grad[c] = dk * S;
+  }
+}
+
+// Nodal P1 parameter: the element's S_e spread onto its NV vertex values by dk_e/dp_i (as in
+// k_adjoint_nodal). grad f64[nvert] must start at zero.
+template <int NV>
+__global__ void __launch_bounds__(kThreads) k_assemble_vjp_nodal(
+    const double* __restrict__ xyz, const int32_t* __restrict__ cells, int64_t ntet, const int32_t* __restrict__ slot,
+    const uint8_t* __restrict__ dmask, const double* __restrict__ param, int mode, double scale,
+    const double* __restrict__ g, const double* __restrict__ gv, const double* __restrict__ gb,
+    double* __restrict__ grad) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t dof[NV];
+    bool dir[NV];
+    double pv[NV];
+#pragma unroll
+    for (int a = 0; a < NV; ++a) {
+      dof[a] = __ldg(cells + c * NV + a);
+      dir[a] = __ldg(dmask + dof[a]) != 0;
+      pv[a] = __ldg(param + dof[a]);
+    }
+    Geom<NV> T;
+    cell_geometry(xyz, dof, T);
+    double VG[NV][NV];
+    gram(T, VG);
+    const double S = vjp_sum<NV>(VG, dof, dir, slot + c * NV * NV, gv, gb, g);
+    double dk[NV];
+    if (mode == FEMK_COEF_NODAL_LINEAR) {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) dk[i] = NodalRule<NV>::w * scale;
+    } else {
+      constexpr double qa = NodalRule<NV>::a, qb = NodalRule<NV>::b;
+      double Ssum = 0.0;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) Ssum += pv[i];
+      double e[NV], es = 0.0;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        e[i] = exp(qa * Ssum + (qb - qa) * pv[i]);
+        es += e[i];
+      }
+#pragma unroll
+      for (int i = 0; i < NV; ++i) dk[i] = NodalRule<NV>::w * scale * (qa * es + (qb - qa) * e[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < NV; ++i) atomicAdd(grad + dof[i], S * dk[i]);
+  }
+}
+
 }  // namespace
 }  // namespace femk
 
@@ -329,15 +499,51 @@ extern "C" int femk_assemble(const femk_plan* p, const double* param, int mode, 
                  "femk_assemble: unknown coef_mode, NULL param, or a nodal mode on a P2 plan");
   cudaStream_t s = (cudaStream_t)stream;
   FEMK_TRY(resolve_coef(p, param, mode, s, &param, &mode));
-  if (vals) FEMK_CUDA_TRY(cudaMemsetAsync(vals, 0, sizeof(double) * p->nnz, s));
-  FEMK_CUDA_TRY(cudaMemsetAsync(b, 0, sizeof(double) * p->n, s));
-  const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);
-  FEMK_BY_ND(p->nd, k_assemble<ND><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->xyz, p->cells, p->ntet, p->slot, p->dmask, param, mode, scale, f, g, vals, b));
+  const int rows = p->asm_rows;
+  const int grid = (int)((p->n + rows - 1) / rows);
+  const size_t smem = vals ? (size_t)p->asm_span * (sizeof(double) + sizeof(int32_t)) : 0;
+  int* err = p->dev_err;
+  FEMK_BY_ND(p->nd, {
+    if (vals) {
+      auto kern = k_assemble_rows<ND, true>;
+      FEMK_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      kern<<<::femk::counted_launch() + grid, rows, smem, s>>>(p->xyz, p->cells, p->inc_ptr, p->inc_elem, p->indptr,
+                                                               p->indices, p->dmask, p->diag, p->n, p->asm_span,
+                                                               param, mode, scale, f, g, vals, b, err);
+    } else {
+      k_assemble_rows<ND, false><<<::femk::counted_launch() + grid, rows, 0, s>>>(
+          p->xyz, p->cells, p->inc_ptr, p->inc_elem, p->indptr, p->indices, p->dmask, p->diag, p->n, 0, param, mode,
+          scale, f, g, nullptr, b, err);
+    }
+  });
   FEMK_CUDA_TRY(cudaGetLastError());
-  if (p->n_dir > 0) {
-    k_dirichlet_rows<<<::femk::counted_launch() + blocks_for(p->n_dir, 256, 65535), 256, 0, s>>>(p->dlist, p->n_dir, p->diag, g, vals, b);
-    FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}
+
+extern "C" int femk_assemble_vjp(const femk_plan* p, const double* param, int mode, double scale, const double* g,
+                                 const double* grad_vals, const double* grad_b, double* grad_param, void* stream) {
+  clear_error();
+  FEMK_CHECK_ARG(p && grad_param, "femk_assemble_vjp: NULL plan or grad_param");
+  FEMK_CHECK_ARG(mode == FEMK_COEF_EXP || mode == FEMK_COEF_LINEAR || mode == FEMK_COEF_NODAL_EXP ||
+                     mode == FEMK_COEF_NODAL_LINEAR,
+                 "femk_assemble_vjp: coef_mode must be a P0 or nodal EXP/LINEAR mode (CONST has no parameter)");
+  FEMK_CHECK_ARG(coef_mode_ok(p, mode, param), "femk_assemble_vjp: param is NULL or a nodal mode on a P2 plan");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int grid = blocks_for(p->ntet, kThreads, p->n_sm * 16);
+  if (mode == FEMK_COEF_NODAL_EXP || mode == FEMK_COEF_NODAL_LINEAR) {
+    FEMK_CUDA_TRY(cudaMemsetAsync(grad_param, 0, sizeof(double) * p->nvert, s));
+    if (p->nd == 3)
+      k_assemble_vjp_nodal<3><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
+          p->xyz, p->cells, p->ntet, p->slot, p->dmask, param, mode, scale, g, grad_vals, grad_b, grad_param);
+    else
+      k_assemble_vjp_nodal<4><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
+          p->xyz, p->cells, p->ntet, p->slot, p->dmask, param, mode, scale, g, grad_vals, grad_b, grad_param);
+  } else {
+    FEMK_BY_ND(p->nd, k_assemble_vjp<ND><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
+                          p->xyz, p->cells, p->ntet, p->slot, p->dmask, param, mode, scale, g, grad_vals, grad_b,
+                          grad_param));
   }
+  FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;
 }
 

@@ -120,6 +120,9 @@ struct femk_plan {
   int32_t* inc_elem = nullptr;  // i32[ntet*nd]
   int16_t* cols16 = nullptr;    // i16[nnz] col - row, when every entry fits
   int max_row = 0;              // longest CSR row
+  int asm_rows = 128;           // rows per block of the row-gather assembly
+  int64_t asm_span = 0;         // largest CSR span (entries) of asm_rows consecutive rows
+  int* dev_err = nullptr;       // device error word of kernels whose index checks can only fail on a corrupt plan
   int spmv_L = 16, spmv_U = 2;  // SpMV lanes per row / rows in flight per lane group
   // sliced-ELL solver layout (SELL-32), built with the pattern
   int64_t n_slices = 0, sell_nnz = 0;

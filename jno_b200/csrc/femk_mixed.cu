@@ -1,25 +1,36 @@
 // Mixed-precision Jacobi-PCG: FP32 values, vectors and SpMV accumulation in the inner CG; FP64
 // solution and FP64 true residual r = b - A x (FP64 values) at every reliable update.
 //
-// The inner iteration is preconditioned CG in the single-reduction form of Chronopoulos and Gear
-// (J. Comput. Appl. Math. 25, 1989): with u = D^-1 r, w = A u, s = A p,
+// The FP32 inner loop runs CG on the symmetrically scaled operator A^ = S A S, S = D^-1/2 (D the
+// Jacobi diagonal), which is the Jacobi-PCG iteration in split form: with x = S x^, r^ = S r, the
+// iterates map one to one, and the preconditioned residual z = D^-1 r never has to be stored
+// (z^ = r^). A^ is formed in FP64 and rounded to FP32 when the values are gathered. Each iteration
+// is two kernels with one grid reduction, after the single-reduction arrangement of Chronopoulos and
+// Gear (J. Comput. Appl. Math. 25, 1989): w = A^ r and s = A^ p kept by recurrence,
 //
-//   K_A  p = u + beta p;  s = w + beta s;  e += alpha p;  r -= alpha s;  u = D^-1 r
-//   K_B  w = A32 u;  gamma' = <r, u>,  delta = <w, u>,  rho = <r, r>       (one grid reduction)
-//        beta = gamma' / gamma;  alpha = gamma' / (delta - beta gamma' / alpha)
+//   K_A  p = r + beta p;  s = w + beta s;  e += alpha p;  r -= alpha s          (elementwise)
+//        block partials of <p, s>, <r, s>, <r, r>, <r, D r>                     (no grid wait)
+//   K_B  w = A^ r;  <r, w>;  the last block adds K_A's partials in block order and forms
+//        gamma' = <r, r>;  beta' = gamma' / gamma;
+//        <p', A^ p'> = <r, w> + 2 beta' <r, s> + beta'^2 <p, s>   (p' = r + beta' p);
+//        alpha' = gamma' / <p', A^ p'>;  <r, D r> = ||r_unscaled||^2 for the stop test
 //
-// Both inner products of an iteration come out of the SpMV's epilogue, so an iteration is two
-// kernels and one reduction (the textbook form needs three kernels and two reductions; the
-// denominator delta - beta gamma' / alpha equals <p, A p> in exact arithmetic).
+// <p', A^ p'> is the expanded product of the next direction with itself (A^ symmetric, s = A^ p), not
+// Chronopoulos and Gear's delta - beta gamma' / alpha: that identity assumes the new residual is
+// orthogonal to the old direction, which a reliable update (residual replacement) breaks -- in a
+// numpy model of this loop on 2-D P1 128^2 the FP32 residual then grew 4.6e3x within 68 steps. With
+// the expanded form the model takes the textbook FP32 loop's iteration counts (517 vs 517 there,
+// 194 vs 193 on 3-D P1 48^3), and so does oracle.pcg.mixed_pcg.
 //
-// A reliable update is requested when rho fell below delta2 of its value at the previous update,
-// when the FP32 recurrence meets the stop test, or at the iteration cap. The iterations left in the
-// chunk then return at entry, and the chunk ends with
-//     x += e;  e = 0;  r64 = b - A64 x;  r = fp32(r64);  u = D^-1 r       (k_fold, k_true_resid)
-//     w = A32 u and the three products; beta = gamma'/gamma (0 to restart)  (K_B refresh)
-// which keeps the search direction (FEMK_MIXED_RELIABLE, residual replacement: p and s = A p are
-// unchanged) or restarts it (FEMK_MIXED_RESTART, classic iterative refinement). The solve stops
-// only on the FP64 true residual: <r64, r64> <= max(tol^2 <b, b>, atol^2), femk_pcg's stop rule.
+// A reliable update is requested when <r, D r> fell below delta2 of the FP64 <r, r> at the previous
+// update, when the FP32 recurrence meets the stop test, or at the iteration cap. The iterations left
+// in the chunk then return at entry, and the chunk ends with
+//     x += S e;  e = 0;  r64 = b - A64 x;  r^ = fp32(S r64);  <r^, r^>, <p, s>, <r^, s>   (k_fold, k_true_resid)
+//     K_B again on the replaced r^ (refresh): beta' = <r^, r^> / gamma (0 to restart)
+// which keeps the search direction (FEMK_MIXED_RELIABLE, residual replacement: p and s = A^ p are
+// unchanged) or restarts it with beta' = 0 (FEMK_MIXED_RESTART, classic iterative refinement). The
+// solve stops only on the FP64 true residual: <r64, r64> <= max(tol^2 <b, b>, atol^2), femk_pcg's
+// stop rule.
 //
 // The FP32 operator is the plan's sliced-ELL copy: 4 B value + 2 B column offset (int16, col - row)
 // per entry when the bandwidth allows it, else 4 B + 4 B. Each chunk (16 iterations of 2 kernels,
@@ -39,12 +50,14 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kChunk = 16;
+// K_A's block partials live past K_B's in the plan's partials buffer
+constexpr int64_t kPartialsA = 16384;
 
 struct MixedState {
-  double gamma;    // <r, u> of the current direction's residual
-  double gnew;     // <r, u> after a reliable update, waiting for the refresh step
-  double delta;    // <w, u>
-  double rr;       // FP32 recurrence <r, r>
+  double gamma;    // <r^, r^> of the current direction's residual
+  double gnew;     // <r^, r^> after a reliable update, waiting for the refresh step
+  double ps, rs;   // <p, s> and <r^, s> after a reliable update (the refresh step's products)
+  double rr;       // FP32 recurrence <r, r> (unscaled: <r^, D r^>)
   double rr64, bb, atol2, alpha, beta, rr_since, delta2;
   int32_t iter, maxiter, done, status;
   int32_t need_update;  // 1: update requested this chunk; 2: update done, refresh step pending
@@ -54,24 +67,33 @@ struct MixedState {
   uint32_t ticket;
 };
 
-template <int NV, int THREADS = kThreads>
-__device__ __forceinline__ bool reduce_finish(double (&v)[NV], double* partials, uint32_t* ticket, double (&out)[NV]) {
+// Block sum of NV values per thread, in a fixed order; the result is valid in every thread.
+template <int NV, int THREADS>
+__device__ __forceinline__ void block_sum(double (&v)[NV]) {
   __shared__ double red[NV][THREADS / 32];
-  __shared__ bool last;
 #pragma unroll
   for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
+  __syncthreads();
   if ((threadIdx.x & 31) == 0) {
 #pragma unroll
     for (int j = 0; j < NV; ++j) red[j][threadIdx.x >> 5] = v[j];
   }
   __syncthreads();
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double t = 0.0;
+    for (int w = 0; w < THREADS / 32; ++w) t += red[j][w];
+    v[j] = t;
+  }
+}
+
+template <int NV, int THREADS = kThreads>
+__device__ __forceinline__ bool reduce_finish(double (&v)[NV], double* partials, uint32_t* ticket, double (&out)[NV]) {
+  __shared__ bool last;
+  block_sum<NV, THREADS>(v);
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int j = 0; j < NV; ++j) {
-      double t = 0.0;
-      for (int w = 0; w < THREADS / 32; ++w) t += red[j][w];
-      partials[(int64_t)blockIdx.x * NV + j] = t;
-    }
+    for (int j = 0; j < NV; ++j) partials[(int64_t)blockIdx.x * NV + j] = v[j];
     __threadfence();
     last = atomicAdd(ticket, 1u) == gridDim.x - 1;
   }
@@ -81,40 +103,25 @@ __device__ __forceinline__ bool reduce_finish(double (&v)[NV], double* partials,
   double s[NV];
 #pragma unroll
   for (int j = 0; j < NV; ++j) s[j] = 0.0;
-  for (int b0 = threadIdx.x; b0 < (int)gridDim.x; b0 += 4 * THREADS) {
-    double t[4][NV];
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += THREADS)
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int b = b0 + u * THREADS;
+    for (int j = 0; j < NV; ++j) s[j] += __ldcg(partials + (int64_t)b * NV + j);
+  block_sum<NV, THREADS>(s);
 #pragma unroll
-      for (int j = 0; j < NV; ++j) t[u][j] = b < (int)gridDim.x ? __ldcg(partials + (int64_t)b * NV + j) : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int j = 0; j < NV; ++j) s[j] += t[u][j];
-  }
-#pragma unroll
-  for (int j = 0; j < NV; ++j) s[j] = warp_sum(s[j]);
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-    for (int j = 0; j < NV; ++j) red[j][threadIdx.x >> 5] = s[j];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int j = 0; j < NV; ++j) {
-    double t = 0.0;
-    for (int w = 0; w < THREADS / 32; ++w) t += red[j][w];
-    out[j] = t;
-  }
+  for (int j = 0; j < NV; ++j) out[j] = s[j];
   if (threadIdx.x == 0) *ticket = 0u;
   return true;
 }
 
-__global__ void k_demote(const double* __restrict__ in, int64_t n, float* __restrict__ out) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = (float)in[i];
+// the NV partials of nblk blocks of an earlier kernel, summed in block order by one block
+template <int NV, int THREADS>
+__device__ __forceinline__ void sum_block_partials(const double* partials, int nblk, double (&out)[NV]) {
+#pragma unroll
+  for (int j = 0; j < NV; ++j) out[j] = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += THREADS)
+#pragma unroll
+    for (int j = 0; j < NV; ++j) out[j] += __ldcg(partials + (int64_t)b * NV + j);
+  block_sum<NV, THREADS>(out);
 }
 
 __global__ void k_fill_f(float* __restrict__ v, int64_t n, float val) {
@@ -122,42 +129,96 @@ __global__ void k_fill_f(float* __restrict__ v, int64_t n, float val) {
     v[i] = val;
 }
 
-__global__ void k_gather32(const int32_t* __restrict__ src, int64_t m, const double* __restrict__ vals,
-                           float* __restrict__ out) {
-  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t k = __ldcs(src + j);
-    out[j] = k >= 0 ? (float)__ldcs(vals + k) : 0.f;
+// S = D^-1/2 from the Jacobi inverse (FP32) and D itself (FP32, for <r, D r>)
+__global__ void k_scaling(const double* __restrict__ dinv, int64_t n, float* __restrict__ sc, float* __restrict__ dd) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double di = dinv[i];
+    sc[i] = (float)sqrt(di);
+    dd[i] = (float)(1.0 / di);
   }
 }
 
-// K_B epilogue state: w[row] = (A u)[row] and the three products of the row
+// A^ = S A S into the FP32 sliced-ELL copy: thread per (slice, lane) row, entries in k order
+template <typename IDX>
+__global__ void k_gather_scaled(const int64_t* __restrict__ sptr, const int32_t* __restrict__ src,
+                                const IDX* __restrict__ cols, int64_t n, int64_t nslices, const double* __restrict__ vals,
+                                const double* __restrict__ dinv, float* __restrict__ out) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nslices * 32; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t sl = t >> 5, row = t;
+    const int lane = (int)(t & 31);
+    const int64_t b0 = sptr[sl];
+    const int64_t w = (sptr[sl + 1] - b0) >> 5;
+    const double si = row < n ? sqrt(dinv[row]) : 0.0;
+    for (int64_t k = 0; k < w; ++k) {
+      const int64_t j = b0 + 32 * k + lane;
+      const int32_t at = __ldcs(src + j);
+      float v = 0.f;
+      if (at >= 0) {
+        const int64_t col = sizeof(IDX) == 2 ? row + (int64_t)cols[j] : (int64_t)cols[j];
+        v = (float)(__ldcs(vals + at) * si * sqrt(dinv[col]));
+      }
+      out[j] = v;
+    }
+  }
+}
+
+// the same on the canonical CSR (plans without a sliced-ELL layout): thread per row
+__global__ void k_scale_csr(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices, int64_t n,
+                            const double* __restrict__ vals, const double* __restrict__ dinv, float* __restrict__ out) {
+  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n; row += (int64_t)gridDim.x * blockDim.x) {
+    const double si = sqrt(dinv[row]);
+    for (int32_t k = indptr[row]; k < indptr[row + 1]; ++k) out[k] = (float)(vals[k] * si * sqrt(dinv[indices[k]]));
+  }
+}
+
+// beta of the refresh step: 0 for the first direction and in restart mode, else <r^, r^> of the
+// replaced residual over the old gamma
+__device__ __forceinline__ double refresh_beta(const MixedState* st) {
+  return (st->restart || st->fresh) ? 0.0 : st->gnew / st->gamma;
+}
+
+// K_B epilogue: w[row] = (A^ r)[row] and the row's share of <r, w>
 struct StepEpi {
-  const float* __restrict__ u;
   const float* __restrict__ r;
   float* __restrict__ w;
-  float a[3];  // <w, u>, <r, u>, <r, r>
+  float a;
   __device__ __forceinline__ void operator()(int64_t row, float wv) {
     w[row] = wv;
-    const float ui = __ldg(u + row), ri = __ldg(r + row);
-    a[0] = fmaf(wv, ui, a[0]);
-    a[1] = fmaf(ri, ui, a[1]);
-    a[2] = fmaf(ri, ri, a[2]);
+    a = fmaf(__ldg(r + row), wv, a);
   }
 };
 
-// Last block of K_B: the new scalars. REFRESH = the step after a reliable update (or the first one).
-template <bool REFRESH>
-__device__ __forceinline__ void step_finish(MixedState* st, const double (&t)[3]) {
-  const double delta = t[0], gnew = REFRESH ? st->gnew : t[1], rho = t[2];
-  st->delta = delta;
-  st->rr = rho;
-  if (!isfinite(delta) || !isfinite(gnew) || !isfinite(rho)) {
+__device__ __forceinline__ bool step_skip(const MixedState* st, bool refresh) {
+  return st->done || (refresh ? st->need_update != 2 : st->hold != 0);
+}
+
+// Last block of K_B (all its threads): the new scalars from <r, w> and, for a normal step, K_A's
+// partials (<p, s>, <r, s>, <r, r>, <r, D r>); a refresh step takes them from the update.
+// (not inlined: it runs once per launch in one block, and inlined it adds registers to the row loop)
+template <bool REFRESH, int THREADS>
+__device__ __noinline__ void step_finish(MixedState* st, double rw, const double* pa, int ga) {
+  double t[4];
+  if (!REFRESH) sum_block_partials<4, THREADS>(pa, ga, t);
+  if (threadIdx.x) return;
+  double ps, rs, gnew;
+  if (REFRESH) {
+    ps = st->ps;
+    rs = st->rs;
+    gnew = st->gnew;
+  } else {
+    ps = t[0];
+    rs = t[1];
+    gnew = t[2];
+    st->rr = t[3];
+    st->iter += 1;
+  }
+  if (!isfinite(rw) || !isfinite(ps) || !isfinite(rs) || !isfinite(gnew) || !isfinite(st->rr)) {
     st->status = FEMK_NONFINITE;
     st->done = 1;
     return;
   }
   if (!REFRESH) {
-    st->iter += 1;
+    const double rho = t[3];
     const bool conv = !(rho > st->atol2);
     const bool drop = rho < st->delta2 * st->rr_since;
     if (conv || drop || st->iter >= st->maxiter) {  // fold e into x and replace r at the chunk end
@@ -166,10 +227,10 @@ __device__ __forceinline__ void step_finish(MixedState* st, const double (&t)[3]
       return;
     }
   }
-  const double beta = (REFRESH && (st->restart || st->fresh)) ? 0.0 : gnew / st->gamma;
-  const double den = beta == 0.0 ? delta : delta - beta * gnew / st->alpha;  // <p, A p> of the new direction
+  const double beta = REFRESH ? refresh_beta(st) : gnew / st->gamma;
+  const double den = rw + 2.0 * beta * rs + beta * beta * ps;  // <p', A^ p'>, p' = r + beta p
   if (!(den > 0.0)) {
-    st->status = isfinite(den) ? FEMK_BREAKDOWN : FEMK_NONFINITE;
+    st->status = FEMK_BREAKDOWN;
     st->done = 1;
     return;
   }
@@ -183,34 +244,28 @@ __device__ __forceinline__ void step_finish(MixedState* st, const double (&t)[3]
   }
 }
 
-__device__ __forceinline__ bool step_skip(const MixedState* st, bool refresh) {
-  return st->done || (refresh ? st->need_update != 2 : st->hold != 0);
-}
-
 // K_B on the register-streamed sliced-ELL operator (one thread per row)
 template <typename IDX, bool REFRESH>
 __global__ void __launch_bounds__(kThreads, 8) k_step32_sell(const int64_t* __restrict__ sptr, const IDX* __restrict__ cols,
                                                          const float* __restrict__ vals, int64_t n, int64_t nslices,
-                                                         const float* __restrict__ u, const float* __restrict__ r,
-                                                         float* __restrict__ w, double* __restrict__ partials,
-                                                         MixedState* st) {
+                                                         const float* __restrict__ r, float* __restrict__ w,
+                                                         double* __restrict__ partials, int ga, MixedState* st) {
   if (step_skip(st, REFRESH)) return;
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
-  StepEpi epi{u, r, w, {0.f, 0.f, 0.f}};
+  StepEpi epi{r, w, 0.f};
   for (int64_t sl = warp; sl < nslices; sl += nwarps) {
     const int64_t row = sl * 32 + lane;
     if (row >= n) continue;
     const int64_t b0 = __ldg(sptr + sl);
     const int32_t wd = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
     epi(row, sell_row<float, IDX, GatherX<float>, 8>(vals + b0 + lane, cols + b0 + lane, wd, (int32_t)row,
-                                                     GatherX<float>{u}));
+                                                     GatherX<float>{r}));
   }
-  double v[3] = {(double)epi.a[0], (double)epi.a[1], (double)epi.a[2]}, tot[3];
-  if (!reduce_finish<3>(v, partials, &st->ticket, tot)) return;
-  if (threadIdx.x) return;
-  step_finish<REFRESH>(st, tot);
+  double v[1] = {(double)epi.a}, tot[1];
+  if (!reduce_finish<1>(v, partials, &st->ticket, tot)) return;
+  step_finish<REFRESH, kThreads>(st, tot[0], partials + kPartialsA, ga);
 }
 
 // K_B with the FP32 sliced-ELL stream moved into shared memory by bulk copies (femk_bulk.cuh):
@@ -219,118 +274,126 @@ template <int WMAX, int S, int WPB, bool REFRESH>
 __global__ void __launch_bounds__(WPB * 32) k_step32_bulk(const int64_t* __restrict__ sptr,
                                                          const int16_t* __restrict__ cols,
                                                          const float* __restrict__ vals, int64_t n, int64_t nslices,
-                                                         const float* __restrict__ u, const float* __restrict__ r,
-                                                         float* __restrict__ w, double* __restrict__ partials,
-                                                         MixedState* st, const int64_t* __restrict__ cptr) {
+                                                         const float* __restrict__ r, float* __restrict__ w,
+                                                         double* __restrict__ partials, int ga, MixedState* st,
+                                                         const int64_t* __restrict__ cptr) {
   extern __shared__ __align__(128) unsigned char bulk_smem[];
   constexpr int kWarpBytes = BulkRing<float, int16_t, WMAX, S>::kWarpBytes;
   if (step_skip(st, REFRESH)) return;
   const int wib = threadIdx.x >> 5;
-  StepEpi epi{u, r, w, {0.f, 0.f, 0.f}};
+  StepEpi epi{r, w, 0.f};
   const bool ok = sell_bulk_rows<float, int16_t, WMAX, S>(
       bulk_smem + wib * kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * WPB + wib,
-      (int64_t)gridDim.x * WPB, GatherX<float>{u}, epi, &st->status, FEMK_TIMEOUT, cptr);
+      (int64_t)gridDim.x * WPB, GatherX<float>{r}, epi, &st->status, FEMK_TIMEOUT, cptr);
   if (!ok && (threadIdx.x & 31) == 0) st->done = 1;
-  double v[3] = {(double)epi.a[0], (double)epi.a[1], (double)epi.a[2]}, tot[3];
-  if (!reduce_finish<3, WPB * 32>(v, partials, &st->ticket, tot)) return;
-  if (threadIdx.x) return;
-  step_finish<REFRESH>(st, tot);
+  double v[1] = {(double)epi.a}, tot[1];
+  if (!reduce_finish<1, WPB * 32>(v, partials, &st->ticket, tot)) return;
+  step_finish<REFRESH, WPB * 32>(st, tot[0], partials + kPartialsA, ga);
 }
 
 // K_B on the CSR copy (plans without a sliced-ELL layout)
 template <int L, int U, typename IDX, bool REFRESH>
 __global__ void __launch_bounds__(kThreads) k_step32(const int32_t* __restrict__ indptr, const IDX* __restrict__ cols,
                                                     const float* __restrict__ vals, int64_t n,
-                                                    const float* __restrict__ u, const float* __restrict__ r,
-                                                    float* __restrict__ w, double* __restrict__ partials,
-                                                    MixedState* st) {
+                                                    const float* __restrict__ r, float* __restrict__ w,
+                                                    double* __restrict__ partials, int ga, MixedState* st) {
   if (step_skip(st, REFRESH)) return;
   const int lane = threadIdx.x & 31, sub = lane % L;
   const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
   constexpr int RPW = 32 / L;
-  StepEpi epi{u, r, w, {0.f, 0.f, 0.f}};
+  StepEpi epi{r, w, 0.f};
   for (int64_t base = warp * RPW * U; base < n; base += nwarps * RPW * U) {
     float sv[U];
     int64_t rows[U];
-    csr_rows<L, U, float, IDX>(indptr, cols, vals, u, n, base, lane, sv, rows);
+    csr_rows<L, U, float, IDX>(indptr, cols, vals, r, n, base, lane, sv, rows);
 #pragma unroll
     for (int k = 0; k < U; ++k)
       if (rows[k] < n && sub == 0) epi(rows[k], sv[k]);
   }
-  double v[3] = {(double)epi.a[0], (double)epi.a[1], (double)epi.a[2]}, tot[3];
-  if (!reduce_finish<3>(v, partials, &st->ticket, tot)) return;
-  if (threadIdx.x) return;
-  step_finish<REFRESH>(st, tot);
+  double v[1] = {(double)epi.a}, tot[1];
+  if (!reduce_finish<1>(v, partials, &st->ticket, tot)) return;
+  step_finish<REFRESH, kThreads>(st, tot[0], partials + kPartialsA, ga);
 }
 
-// K_A: p = u + beta p; s = w + beta s; e += alpha p; r -= alpha s; u = D^-1 r (no reduction).
-// All seven vectors are plan-owned and 16-byte aligned: four rows per load.
-__device__ __forceinline__ void cgcg_one(float alpha, float beta, float& u, float w, float& p, float& s, float& e,
-                                         float& r, float d) {
-  p = fmaf(beta, p, u);
+// K_A: p = r + beta p; s = w + beta s; e += alpha p; r -= alpha s; block partials of <p, s>,
+// <r, s>, <r, r>, <r, D r> for the next K_B (no grid-wide wait here). All vectors are plan-owned
+// and 16-byte aligned: four rows per load.
+__device__ __forceinline__ void mx_one(float alpha, float beta, float w, float d, float& p, float& s, float& e,
+                                       float& r, float (&a)[4]) {
+  p = fmaf(beta, p, r);
   s = fmaf(beta, s, w);
   e = fmaf(alpha, p, e);
   r = fmaf(-alpha, s, r);
-  u = d * r;
+  a[0] = fmaf(p, s, a[0]);
+  a[1] = fmaf(r, s, a[1]);
+  a[2] = fmaf(r, r, a[2]);
+  a[3] = fmaf(r * r, d, a[3]);
 }
 
-__global__ void __launch_bounds__(kThreads) k_cgcg_update(int64_t n, float* __restrict__ u, const float* __restrict__ w,
-                                                         float* __restrict__ p, float* __restrict__ s,
-                                                         float* __restrict__ e, float* __restrict__ r,
-                                                         const float* __restrict__ dinv, const MixedState* st) {
+__global__ void __launch_bounds__(kThreads) k_mixed_update(int64_t n, const float* __restrict__ w, float* __restrict__ p,
+                                                          float* __restrict__ s, float* __restrict__ e,
+                                                          float* __restrict__ r, const float* __restrict__ dd,
+                                                          double* __restrict__ pa, const MixedState* st) {
   if (st->done || st->hold) return;
   const float alpha = (float)st->alpha, beta = (float)st->beta;
   const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
   const int64_t nt = (int64_t)gridDim.x * kThreads;
   const int64_t n4 = n >> 2;
-  float4* u4 = reinterpret_cast<float4*>(u);
   const float4* w4 = reinterpret_cast<const float4*>(w);
   float4* p4 = reinterpret_cast<float4*>(p);
   float4* s4 = reinterpret_cast<float4*>(s);
   float4* e4 = reinterpret_cast<float4*>(e);
   float4* r4 = reinterpret_cast<float4*>(r);
-  const float4* d4 = reinterpret_cast<const float4*>(dinv);
+  const float4* d4 = reinterpret_cast<const float4*>(dd);
+  float a[4] = {0.f, 0.f, 0.f, 0.f};
   for (int64_t i = tid; i < n4; i += nt) {
-    float4 uu = u4[i], pp = p4[i], ss = s4[i], ee = e4[i], rr = r4[i];
-    const float4 ww = w4[i], dd = d4[i];
-    cgcg_one(alpha, beta, uu.x, ww.x, pp.x, ss.x, ee.x, rr.x, dd.x);
-    cgcg_one(alpha, beta, uu.y, ww.y, pp.y, ss.y, ee.y, rr.y, dd.y);
-    cgcg_one(alpha, beta, uu.z, ww.z, pp.z, ss.z, ee.z, rr.z, dd.z);
-    cgcg_one(alpha, beta, uu.w, ww.w, pp.w, ss.w, ee.w, rr.w, dd.w);
-    u4[i] = uu;
+    float4 pp = p4[i], ss = s4[i], ee = e4[i], rr = r4[i];
+    const float4 ww = w4[i], d = d4[i];
+    mx_one(alpha, beta, ww.x, d.x, pp.x, ss.x, ee.x, rr.x, a);
+    mx_one(alpha, beta, ww.y, d.y, pp.y, ss.y, ee.y, rr.y, a);
+    mx_one(alpha, beta, ww.z, d.z, pp.z, ss.z, ee.z, rr.z, a);
+    mx_one(alpha, beta, ww.w, d.w, pp.w, ss.w, ee.w, rr.w, a);
     p4[i] = pp;
     s4[i] = ss;
     e4[i] = ee;
     r4[i] = rr;
   }
-  for (int64_t i = 4 * n4 + tid; i < n; i += nt) cgcg_one(alpha, beta, u[i], w[i], p[i], s[i], e[i], r[i], dinv[i]);
+  for (int64_t i = 4 * n4 + tid; i < n; i += nt) mx_one(alpha, beta, w[i], dd[i], p[i], s[i], e[i], r[i], a);
+  double v[4] = {(double)a[0], (double)a[1], (double)a[2], (double)a[3]};
+  block_sum<4, kThreads>(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) pa[(int64_t)blockIdx.x * 4 + j] = v[j];
+  }
 }
 
-// x += e; e = 0 (only at a requested update)
-__global__ void k_fold(int64_t n, double* __restrict__ x, float* __restrict__ e, const MixedState* st) {
+// x += S e; e = 0 (only at a requested update)
+__global__ void k_fold(int64_t n, double* __restrict__ x, float* __restrict__ e, const float* __restrict__ sc,
+                       const MixedState* st) {
   if (st->done || st->need_update != 1) return;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    x[i] += (double)e[i];
+    x[i] += (double)sc[i] * (double)e[i];
     e[i] = 0.f;
   }
 }
 
-// r64 = b - A64 x; r = fp32(r64); u = D^-1 r; <r, u>, <r64, r64> (+ <b, b> at init)
+// r64 = b - A64 x; r^ = fp32(S r64); <r^, r^>, <r64, r64> (+ <b, b> at init, + <p, s>, <r^, s> after)
 template <int L, int U, bool INIT>
 __global__ void __launch_bounds__(kThreads) k_true_resid(const int32_t* __restrict__ indptr,
                                                         const int32_t* __restrict__ indices,
                                                         const double* __restrict__ vals, int64_t n,
                                                         const double* __restrict__ x, const double* __restrict__ b,
-                                                        const float* __restrict__ dinv, float* __restrict__ r,
-                                                        float* __restrict__ u, double* __restrict__ partials,
-                                                        MixedState* st, double tol2, double atol2) {
+                                                        const double* __restrict__ dinv, float* __restrict__ r,
+                                                        const float* __restrict__ p, const float* __restrict__ s,
+                                                        double* __restrict__ partials, MixedState* st, double tol2,
+                                                        double atol2) {
   if (!INIT && (st->done || st->need_update != 1)) return;
   const int lane = threadIdx.x & 31, sub = lane % L;
   const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
   constexpr int RPW = 32 / L;
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  double a[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   for (int64_t base = warp * RPW * U; base < n; base += nwarps * RPW * U) {
     double sv[U];
     int64_t rows[U];
@@ -341,21 +404,28 @@ __global__ void __launch_bounds__(kThreads) k_true_resid(const int32_t* __restri
       if (row >= n || sub != 0) continue;
       const double bi = b[row];
       const double r64 = bi - sv[k];
-      const float rf = (float)r64;
-      const float uf = dinv[row] * rf;
+      const float rf = (float)(sqrt(dinv[row]) * r64);
       r[row] = rf;
-      u[row] = uf;
-      a0 += (double)rf * (double)uf;
-      a1 += r64 * r64;
-      if (INIT) a2 += bi * bi;
+      a[0] += (double)rf * (double)rf;
+      a[1] += r64 * r64;
+      if (INIT) {
+        a[2] += bi * bi;
+      } else {
+        const float si = s[row];
+        a[3] += (double)p[row] * (double)si;
+        a[4] += (double)rf * (double)si;
+      }
     }
   }
-  double v[3] = {a0, a1, a2}, tot[3];
-  if (!reduce_finish<3>(v, partials, &st->ticket, tot)) return;
+  double tot[5];
+  if (!reduce_finish<5>(a, partials, &st->ticket, tot)) return;
   if (threadIdx.x) return;
   st->outer += 1;
   st->rr64 = tot[1];
   st->rr_since = tot[1];
+  st->rr = tot[1];
+  st->ps = tot[3];
+  st->rs = tot[4];
   if (INIT) {
     st->bb = tot[2];
     st->atol2 = fmax(tol2 * tot[2], atol2);
@@ -372,24 +442,27 @@ __global__ void __launch_bounds__(kThreads) k_true_resid(const int32_t* __restri
     return;
   }
   st->gnew = tot[0];
-  st->need_update = 2;  // the refresh step forms w = A u, beta and alpha
+  st->need_update = 2;  // the refresh step forms w = A^ r^, beta and alpha
   st->hold = 1;
 }
 
 template <bool INIT>
-void launch_true_resid(const femk_plan* p, const double* vals, const double* x, const double* b, const float* dinv,
-                       float* r, float* u, MixedState* st, double tol2, double atol2, cudaStream_t s) {
+void launch_true_resid(const femk_plan* p, const double* vals, const double* x, const double* b, const double* dinv,
+                       float* r, const float* pv, const float* sv, MixedState* st, double tol2, double atol2,
+                       cudaStream_t s) {
   with_spmv_cfg(p->spmv_L, p->spmv_U, [&](auto Lc, auto Uc) {
     constexpr int L = decltype(Lc)::value, U = decltype(Uc)::value;
     const int grid = wave_grid(k_true_resid<L, U, INIT>, kThreads, p);
     k_true_resid<L, U, INIT><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
-        p->indptr, p->indices, vals, p->n, x, b, dinv, r, u, p->partials, st, tol2, atol2);
+        p->indptr, p->indices, vals, p->n, x, b, dinv, r, pv, sv, p->partials, st, tol2, atol2);
   });
 }
 
+// grid of K_A (fixed per plan: K_B's last block reads this many block partials)
+int update_grid(const femk_plan* p) { return vec_grid(k_mixed_update, kThreads, p); }
+
 template <int S, int WPB, int WMAX, bool REFRESH>
-bool launch_step32_bulk_cfg(const femk_plan* p, const float* u, const float* r, float* w, MixedState* st,
-                            cudaStream_t s, bool prime) {
+bool launch_step32_bulk_cfg(const femk_plan* p, const float* r, float* w, MixedState* st, cudaStream_t s, bool prime) {
   auto kern = k_step32_bulk<WMAX, S, WPB, REFRESH>;
   constexpr int kSmem = WPB * BulkRing<float, int16_t, WMAX, S>::kWarpBytes;
   static int per_sm = -1;  // per instantiation: opt-in shared memory size + occupancy, queried once
@@ -406,25 +479,25 @@ bool launch_step32_bulk_cfg(const femk_plan* p, const float* u, const float* r, 
   const bool tab = p->sell_cu != nullptr;  // per-slice column tables (shared-offset slices stored once)
   kern<<<::femk::counted_launch() + grid, WPB * 32, kSmem, s>>>(
       (const int64_t*)p->sell_ptr, (const int16_t*)(tab ? p->sell_cu : p->sell_c16), (const float*)p->sell_vals32,
-      p->n, p->n_slices, u, r, w, p->partials, st, (const int64_t*)(tab ? p->sell_cuptr : nullptr));
+      p->n, p->n_slices, r, w, p->partials, update_grid(p), st, (const int64_t*)(tab ? p->sell_cuptr : nullptr));
   return true;
 }
 
 // bulk-copy K_B in the plan's configuration (bulk32_cfg: 10 * stages + warps per block)
 // prime = true only sets the kernel attribute and reads the occupancy (before a graph capture)
 template <bool REFRESH>
-bool launch_step32_bulk(const femk_plan* p, const float* u, const float* r, float* w, MixedState* st, cudaStream_t s,
+bool launch_step32_bulk(const femk_plan* p, const float* r, float* w, MixedState* st, cudaStream_t s,
                         bool prime = false) {
   if (!p->bulk32_cfg || !p->sell_vals32 || !p->sell_c16 || p->max_row > 32) return false;
   if (((uintptr_t)p->sell_vals32 & 15u) || ((uintptr_t)p->sell_c16 & 15u)) return false;
   if (p->sell_cu && ((uintptr_t)p->sell_cu & 15u)) return false;
   // ring stages sized for the widest row: 8 (2-D P1 triangles), 16 (P1 tetrahedra), 32
   const int wsel = p->max_row <= 8 ? 8 : (p->max_row <= 16 ? 16 : 32);
-#define FEMK_BULK_CFG(code, S, WPB)                                                                     \
-  case code:                                                                                            \
-    return wsel == 8    ? launch_step32_bulk_cfg<S, WPB, 8, REFRESH>(p, u, r, w, st, s, prime)  \
-           : wsel == 16 ? launch_step32_bulk_cfg<S, WPB, 16, REFRESH>(p, u, r, w, st, s, prime) \
-                        : launch_step32_bulk_cfg<S, WPB, 32, REFRESH>(p, u, r, w, st, s, prime);
+#define FEMK_BULK_CFG(code, S, WPB)                                                             \
+  case code:                                                                                    \
+    return wsel == 8    ? launch_step32_bulk_cfg<S, WPB, 8, REFRESH>(p, r, w, st, s, prime)  \
+           : wsel == 16 ? launch_step32_bulk_cfg<S, WPB, 16, REFRESH>(p, r, w, st, s, prime) \
+                        : launch_step32_bulk_cfg<S, WPB, 32, REFRESH>(p, r, w, st, s, prime);
   switch (p->bulk32_cfg) {
     FEMK_BULK_CFG(14, 1, 4)
     FEMK_BULK_CFG(18, 1, 8)
@@ -438,17 +511,18 @@ bool launch_step32_bulk(const femk_plan* p, const float* u, const float* r, floa
 }
 
 template <bool REFRESH>
-void launch_step32(const femk_plan* p, const float* u, const float* r, float* w, MixedState* st, cudaStream_t s) {
-  if (launch_step32_bulk<REFRESH>(p, u, r, w, st, s)) return;
+void launch_step32(const femk_plan* p, const float* r, float* w, MixedState* st, cudaStream_t s) {
+  if (launch_step32_bulk<REFRESH>(p, r, w, st, s)) return;
+  const int ga = update_grid(p);
   if (p->sell_vals32) {
     if (p->sell_c16) {
       auto k = k_step32_sell<int16_t, REFRESH>;
       k<<<::femk::counted_launch() + wave_grid(k, kThreads, p), kThreads, 0, s>>>(
-          p->sell_ptr, p->sell_c16, p->sell_vals32, p->n, p->n_slices, u, r, w, p->partials, st);
+          p->sell_ptr, p->sell_c16, p->sell_vals32, p->n, p->n_slices, r, w, p->partials, ga, st);
     } else {
       auto k = k_step32_sell<int32_t, REFRESH>;
       k<<<::femk::counted_launch() + wave_grid(k, kThreads, p), kThreads, 0, s>>>(
-          p->sell_ptr, p->sell_cols, p->sell_vals32, p->n, p->n_slices, u, r, w, p->partials, st);
+          p->sell_ptr, p->sell_cols, p->sell_vals32, p->n, p->n_slices, r, w, p->partials, ga, st);
     }
     return;
   }
@@ -457,11 +531,11 @@ void launch_step32(const femk_plan* p, const float* u, const float* r, float* w,
     if (p->cols16) {
       auto k = k_step32<L, U, int16_t, REFRESH>;
       k<<<::femk::counted_launch() + wave_grid(k, kThreads, p), kThreads, 0, s>>>(p->indptr, p->cols16, p->vals32,
-                                                                                  p->n, u, r, w, p->partials, st);
+                                                                                  p->n, r, w, p->partials, ga, st);
     } else {
       auto k = k_step32<L, U, int32_t, REFRESH>;
       k<<<::femk::counted_launch() + wave_grid(k, kThreads, p), kThreads, 0, s>>>(p->indptr, p->indices, p->vals32,
-                                                                                  p->n, u, r, w, p->partials, st);
+                                                                                  p->n, r, w, p->partials, ga, st);
     }
   });
 }
@@ -480,14 +554,14 @@ void prime_mixed(const femk_plan* p) {
   (void)wave_grid(k_step32_sell<int32_t, false>, kThreads, p);
   (void)wave_grid(k_step32_sell<int16_t, true>, kThreads, p);
   (void)wave_grid(k_step32_sell<int32_t, true>, kThreads, p);
-  (void)launch_step32_bulk<false>(p, nullptr, nullptr, nullptr, nullptr, nullptr, true);
-  (void)launch_step32_bulk<true>(p, nullptr, nullptr, nullptr, nullptr, nullptr, true);
-  (void)vec_grid(k_cgcg_update, kThreads, p);
+  (void)launch_step32_bulk<false>(p, nullptr, nullptr, nullptr, nullptr, true);
+  (void)launch_step32_bulk<true>(p, nullptr, nullptr, nullptr, nullptr, true);
+  (void)update_grid(p);
   (void)wave_grid(k_fold, 256, p);
 }
 
 struct MixedPtrs {
-  float *r, *u, *w, *pv, *s, *e, *d32;
+  float *r, *w, *pv, *s, *e, *sc, *dd;
   MixedState* st;
 };
 
@@ -495,28 +569,30 @@ MixedPtrs mixed_ptrs(const femk_plan* p) {
   const int64_t vs = p->vstride;
   MixedPtrs m;
   m.r = p->work32;
-  m.u = m.r + vs;
-  m.w = m.u + vs;
+  m.w = m.r + vs;
   m.pv = m.w + vs;
   m.s = m.pv + vs;
   m.e = m.s + vs;
-  m.d32 = m.e + vs;
+  m.sc = m.e + vs;
+  m.dd = m.sc + vs;
   m.st = (MixedState*)p->work64b;
   return m;
 }
 
 // one chunk: kChunk inner iterations, then the (conditional) reliable update and refresh step
-int enqueue_mixed_chunk(const femk_plan* p, const double* vals, const double* b, double* x, cudaStream_t s) {
+int enqueue_mixed_chunk(const femk_plan* p, const double* vals, const double* b, double* x, const double* dinv,
+                        cudaStream_t s) {
   const MixedPtrs m = mixed_ptrs(p);
   const int64_t n = p->n;
+  const int ga = update_grid(p);
   for (int it = 0; it < kChunk; ++it) {
-    k_cgcg_update<<<::femk::counted_launch() + vec_grid(k_cgcg_update, kThreads, p), kThreads, 0, s>>>(
-        n, m.u, m.w, m.pv, m.s, m.e, m.r, m.d32, m.st);
-    launch_step32<false>(p, m.u, m.r, m.w, m.st, s);
+    k_mixed_update<<<::femk::counted_launch() + ga, kThreads, 0, s>>>(n, m.w, m.pv, m.s, m.e, m.r, m.dd,
+                                                                     p->partials + kPartialsA, m.st);
+    launch_step32<false>(p, m.r, m.w, m.st, s);
   }
-  k_fold<<<::femk::counted_launch() + wave_grid(k_fold, 256, p), 256, 0, s>>>(n, x, m.e, m.st);
-  launch_true_resid<false>(p, vals, x, b, m.d32, m.r, m.u, m.st, 0.0, 0.0, s);
-  launch_step32<true>(p, m.u, m.r, m.w, m.st, s);
+  k_fold<<<::femk::counted_launch() + wave_grid(k_fold, 256, p), 256, 0, s>>>(n, x, m.e, m.sc, m.st);
+  launch_true_resid<false>(p, vals, x, b, dinv, m.r, m.pv, m.s, m.st, 0.0, 0.0, s);
+  launch_step32<true>(p, m.r, m.w, m.st, s);
   FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;
 }
@@ -538,13 +614,13 @@ int ensure_mixed(femk_plan* p) {
   return FEMK_OK;
 }
 
-int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double* x) {
+int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double* x, const double* dinv) {
   // every buffer the captured kernels read is allocated by ensure_mixed before this point
   if (!p->work32 || !p->work64b || !(p->sell_vals32 || p->vals32)) {
     set_error("femk_pcg_mixed: workspace missing at graph capture");
     return FEMK_EINVAL;
   }
-  const void* key[5] = {vals, b, x, p->sell_vals32 ? (const void*)p->sell_vals32 : (const void*)p->vals32, nullptr};
+  const void* key[5] = {vals, b, x, p->sell_vals32 ? (const void*)p->sell_vals32 : (const void*)p->vals32, dinv};
   bool same = p->mx_exec != nullptr;
   for (int i = 0; i < 5; ++i) same = same && key[i] == p->mx_key[i];
   if (same) return FEMK_OK;
@@ -552,7 +628,7 @@ int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double
   cudaGraph_t g = nullptr;
   set_capturing(true);
   cudaError_t e = cudaStreamBeginCapture(p->mx_stream, cudaStreamCaptureModeThreadLocal);
-  int st = e == cudaSuccess ? enqueue_mixed_chunk(p, vals, b, x, p->mx_stream) : FEMK_ECUDA;
+  int st = e == cudaSuccess ? enqueue_mixed_chunk(p, vals, b, x, dinv, p->mx_stream) : FEMK_ECUDA;
   const cudaError_t e2 = cudaStreamEndCapture(p->mx_stream, &g);
   set_capturing(false);
   if (e != cudaSuccess || e2 != cudaSuccess || st != FEMK_OK) {
@@ -600,19 +676,28 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   femk_plan* p = const_cast<femk_plan*>(pc);
   cudaStream_t s = (cudaStream_t)stream;
   FEMK_TRY(ensure_mixed(p));
+  FEMK_CHECK_ARG(kPartialsA + 4 * (int64_t)update_grid(p) <= 4 * (int64_t)p->n_sm * 64 &&
+                     (int64_t)p->n_sm * 16 * 5 <= kPartialsA,
+                 "femk_pcg_mixed: reduction partials do not fit the plan's buffer");
   const int64_t n = p->n;
   const MixedPtrs m = mixed_ptrs(p);
   cudaStream_t ws = p->mx_stream;
   FEMK_CUDA_TRY(cudaEventRecord(p->mx_ev[2], s));
   FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->mx_ev[2], 0));
-  if (p->cg_graph) FEMK_TRY(ensure_mixed_graph(p, vals, b, x));
+  if (p->cg_graph) FEMK_TRY(ensure_mixed_graph(p, vals, b, x, dinv64));
   else prime_mixed(p);
   const int g1 = p->n_sm * 8;
-  if (p->sell_vals32)
-    k_gather32<<<::femk::counted_launch() + g1, 256, 0, ws>>>(p->sell_src, p->sell_nnz, vals, p->sell_vals32);
-  else
-    k_demote<<<::femk::counted_launch() + g1, 256, 0, ws>>>(vals, p->nnz, p->vals32);
-  k_demote<<<::femk::counted_launch() + g1, 256, 0, ws>>>(dinv64, n, m.d32);
+  k_scaling<<<::femk::counted_launch() + g1, 256, 0, ws>>>(dinv64, n, m.sc, m.dd);
+  if (p->sell_vals32) {
+    if (p->sell_c16)
+      k_gather_scaled<int16_t><<<::femk::counted_launch() + g1, 256, 0, ws>>>(
+          p->sell_ptr, p->sell_src, p->sell_c16, n, p->n_slices, vals, dinv64, p->sell_vals32);
+    else
+      k_gather_scaled<int32_t><<<::femk::counted_launch() + g1, 256, 0, ws>>>(
+          p->sell_ptr, p->sell_src, p->sell_cols, n, p->n_slices, vals, dinv64, p->sell_vals32);
+  } else {
+    k_scale_csr<<<::femk::counted_launch() + g1, 256, 0, ws>>>(p->indptr, p->indices, n, vals, dinv64, p->vals32);
+  }
   // e, p and s start at zero (beta = 0 multiplies p and s at the first step: 0 * NaN would stick)
   k_fill_f<<<::femk::counted_launch() + g1, 256, 0, ws>>>(m.e, n, 0.f);
   k_fill_f<<<::femk::counted_launch() + g1, 256, 0, ws>>>(m.pv, n, 0.f);
@@ -626,8 +711,8 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   init.alpha = 1.0;
   FEMK_CUDA_TRY(cudaMemcpyAsync(m.st, &init, sizeof(MixedState), cudaMemcpyHostToDevice, ws));
   const double tol2 = tol * tol, atol2 = atol * atol;
-  launch_true_resid<true>(p, vals, x, b, m.d32, m.r, m.u, m.st, tol2, atol2, ws);
-  launch_step32<true>(p, m.u, m.r, m.w, m.st, ws);  // w = A u, the first alpha
+  launch_true_resid<true>(p, vals, x, b, dinv64, m.r, m.pv, m.s, m.st, tol2, atol2, ws);
+  launch_step32<true>(p, m.r, m.w, m.st, ws);  // w = A^ r^, the first alpha
   FEMK_CUDA_TRY(cudaGetLastError());
   MixedState* hs = (MixedState*)p->mx_host;
   int64_t enq = 0;
@@ -641,7 +726,7 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
       FEMK_CUDA_TRY(cudaGraphLaunch(p->mx_exec, ws));
       count_launches(p->mx_nodes);
     } else {
-      FEMK_TRY(enqueue_mixed_chunk(p, vals, b, x, ws));
+      FEMK_TRY(enqueue_mixed_chunk(p, vals, b, x, dinv64, ws));
     }
     ++enq;
     FEMK_CUDA_TRY(cudaMemcpyAsync(hs + (chunk & 1), m.st, sizeof(MixedState), cudaMemcpyDeviceToHost, ws));

@@ -299,6 +299,15 @@ __global__ void k_compact(const uint8_t* __restrict__ mask, const int64_t* __res
     if (mask[i]) list[pos[i]] = (int32_t)i;
 }
 
+// Largest CSR span of R consecutive rows (one value per block of the row-gather assembly).
+__global__ void k_block_span(const int32_t* __restrict__ indptr, int64_t n, int R, int64_t nblk,
+                             unsigned long long* __restrict__ out) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nblk; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r0 = t * R, r1 = r0 + R < n ? r0 + R : n;
+    atomicMax(out, (unsigned long long)(indptr[r1] - indptr[r0]));
+  }
+}
+
 // Width of each 32-row slice (its longest row) and its entry count.
 __global__ void k_sell_width(const int32_t* __restrict__ indptr, int64_t n, int64_t nslices, int64_t* __restrict__ len) {
   const int lane = threadIdx.x & 31;
@@ -448,6 +457,32 @@ int build_pattern(femk_plan* p, int* d_err, int* h_err, cudaStream_t s) {
   FEMK_TRY(dev_alloc(&p->slot, p->ntet * ND * ND, s));
   k_slot_map<ND><<<::femk::counted_launch() + blocks_for(p->ntet * ND, kThreads, 65535 * 4), kThreads, 0, s>>>(p->cells, p->ntet, p->indptr,
                                                                                     p->indices, p->slot, d_err);
+  // rows per block of the row-gather assembly: as many as keep the block's staged span (8 B value +
+  // 4 B column per entry) within 64 KB of shared memory
+  {
+    Temp span;
+    FEMK_CUDA_TRY(cudaMalloc(&span.p, sizeof(unsigned long long)));
+    int R = ND <= 4 ? 128 : 64;
+    while (true) {
+      FEMK_CUDA_TRY(cudaMemsetAsync(span.p, 0, sizeof(unsigned long long), s));
+      const int64_t nblk = (n + R - 1) / R;
+      k_block_span<<<::femk::counted_launch() + blocks_for(nblk, kThreads, 65535 * 4), kThreads, 0, s>>>(
+          p->indptr, n, R, nblk, (unsigned long long*)span.p);
+      unsigned long long h = 0;
+      FEMK_CUDA_TRY(cudaMemcpyAsync(&h, span.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+      FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+      if (h * 12 <= 65536 || R == 32) {
+        p->asm_rows = R;
+        p->asm_span = (int64_t)h;
+        break;
+      }
+      R /= 2;
+    }
+    if (p->asm_span * 12 > 200 * 1024) {
+      set_error("femk_plan_create: rows too long for the shared-memory assembly");
+      return FEMK_EINVAL;
+    }
+  }
   FEMK_TRY(dev_alloc(&p->diag, n, s));
   k_diag_slot<<<::femk::counted_launch() + blocks_for(n, kThreads, 65535 * 4), kThreads, 0, s>>>(p->indptr, p->indices, n, p->diag, d_err);
   FEMK_CUDA_TRY(cudaGetLastError());
@@ -682,7 +717,7 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
                   p->work,     p->partials,  p->state,     p->work32,    p->vals32,    p->work64b,
                   p->sell_ptr, p->sell_src,  p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32,
                   p->bar,      p->batch_ws,  p->bicg_ws,   p->bicg_state, p->sell_cuptr, p->sell_cu,
-                  p->coef_tmp, p->theta_ws, p->cmp_ws, p->gm_ws};
+                  p->coef_tmp, p->theta_ws, p->cmp_ws, p->gm_ws, p->dev_err};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->state_host) cudaFreeHost(p->state_host);
@@ -812,6 +847,11 @@ extern "C" int femk_plan_create_ex(const double* coords_dev, int dim, int64_t nv
     return st;
   }
   cudaDeviceGetAttribute(&p->coop, cudaDevAttrCooperativeLaunch, p->device);
+  if (cudaMalloc(&p->dev_err, sizeof(int)) != cudaSuccess || cudaMemset(p->dev_err, 0, sizeof(int)) != cudaSuccess) {
+    femk_plan_destroy(p);
+    femk::set_error("femk_plan_create: device allocation failed");
+    return FEMK_ENOMEM;
+  }
   p->nvert = nvert;
   p->ntet = ncell;
   st = dim == 2 ? femk::create_impl<3>(p, coords_dev, cells_dev, dirichlet_mask_dev, s)

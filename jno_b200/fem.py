@@ -29,7 +29,13 @@ from .trace import classify_condition, classify_volume, evaluate_on
 
 
 class FemLinearSystem:
-    """Parametric linear system: ``evaluate(args) -> (A, b)`` re-assembles on the device."""
+    """Parametric linear system: ``evaluate(args) -> (A, b)`` re-assembles on the device.
+
+    ``evaluate`` is differentiable (torch autograd) in the parameter tensor: ``A.data`` and ``b`` carry
+    the graph of the assembly (``femk_assemble_vjp`` in the backward pass), so a loss built from them
+    -- a dense solve of ``A.todense()``, or ``jno.solve.cg(...)(A, b)`` -- has a gradient with respect
+    to the parameter, as ``jax.grad`` gives in the reference (tests/test_fem_native_lagrange.py:688-711).
+    """
 
     def __init__(self, fem_obj):
         self._fem = fem_obj
@@ -46,7 +52,25 @@ class FemLinearSystem:
     def rhs(self, args=None):
         return self.evaluate(args)[1]
 
-    def solve(self, args=None, linear=None, precond=None, x0=None):
+    def solve(self, solve_fn=None, *, periodic=None):
+        """Differentiable forward solve ``u = solve_fn(A(theta), b(theta))`` as a callable
+        (jno/trace/__init__.py:3617-3669 returns the same as a lazy trace node): ``call(value)`` or
+        ``call({name: value})`` evaluates it at the parameter value, and gradients flow back to the
+        value through the assembly and ``solve_fn``. ``solve_fn`` is any ``(A, b) -> u``; the
+        reference's default is its sparse direct solve, which this path does not have, so the
+        default here is Jacobi-PCG at tol 1e-10 (``jno.solve.cg``, differentiable by its adjoint).
+        Periodic reduction is outside this path."""
+        if periodic is not None:
+            raise NotImplementedError("periodic reduction is outside the B200 path")
+        if solve_fn is None:
+            cg10 = cg(tol=1e-10)
+
+            def solve_fn(A, b):
+                return cg10(A, b, M=jacobi())
+
+        return FemSolveCall(self, solve_fn)
+
+    def _solve_eager(self, args=None, linear=None, precond=None, x0=None):
         A, b = self.evaluate(args)
         return _solve(A, b, linear, precond, x0)
 
@@ -57,6 +81,26 @@ class FemLinearSystem:
     @property
     def b(self):
         return self.evaluate({self._fem.form.param: 0.0})[1]
+
+
+class FemSolveCall:
+    """The value of ``FemLinearSystem.solve(solve_fn)``: ``call(value)``, ``call(*values)`` in the order
+    of ``params``, or ``call({name: value})`` -> ``u`` (differentiable in the values)."""
+
+    def __init__(self, system, solve_fn):
+        self.system, self.solve_fn = system, solve_fn
+        self.params = list(system.runtime_parameter_exprs)
+        self.name = "fem_solve"
+
+    def __call__(self, *values):
+        if len(values) == 1 and isinstance(values[0], dict):
+            args = values[0]
+        else:
+            if len(values) != len(self.params):
+                raise TypeError(f"fem_solve takes {len(self.params)} parameter value(s) {self.params}")
+            args = dict(zip(self.params, values))
+        A, b = self.system.evaluate(args)
+        return self.solve_fn(A, b.reshape(-1))
 
 
 def _solve(A, b, linear, precond, x0, default=cg):
@@ -98,27 +142,34 @@ class FEM:
         return self.plan.export()["points"]
 
     def _param_tensor(self, args):
+        """The parameter as an f64 CUDA tensor of one value per element (P0, or a scalar broadcast to
+        every element) or per P1 vertex (nodal), keeping the caller's autograd graph."""
         name = self.form.param
         if name is None:
             return None
         if name not in args:
             raise KeyError(f"missing runtime parameter {name!r}")
         v = args[name]
+        nodal = self.form.mode in (_lib.COEF_NODAL_EXP, _lib.COEF_NODAL_LINEAR)
+        size = self.plan.nvert if nodal else self.plan.ntet
         if isinstance(v, (int, float)):
-            nodal = self.form.mode in (_lib.COEF_NODAL_EXP, _lib.COEF_NODAL_LINEAR)
-            size = self.plan.nvert if nodal else self.plan.ntet
             return torch.full((size,), float(v), dtype=torch.float64, device=self.plan.device)
         t = v if isinstance(v, torch.Tensor) else torch.as_tensor(np.asarray(v))
-        t = t.to(device=self.plan.device, dtype=torch.float64).reshape(-1).contiguous()
-        nodal = self.form.mode in (_lib.COEF_NODAL_EXP, _lib.COEF_NODAL_LINEAR)
-        want, kind = (self.plan.nvert, "nodal P1") if nodal else (self.plan.ntet, "P0")
-        if t.numel() != want:
-            raise ValueError(f"parameter {name!r} is {kind}: it needs {want} values, got {t.numel()}")
-        return t
+        t = t.to(device=self.plan.device, dtype=torch.float64).reshape(-1)
+        if self.form.scalar:
+            if t.numel() != 1:
+                raise ValueError(f"parameter {name!r} is a scalar: it needs 1 value, got {t.numel()}")
+            return t.expand(size).contiguous()
+        kind = "nodal P1" if nodal else "P0"
+        if t.numel() != size:
+            raise ValueError(f"parameter {name!r} is {kind}: it needs {size} values, got {t.numel()}")
+        return t.contiguous()
 
     def _assemble(self, args):
+        from . import autograd
+
         param = self._param_tensor(args)
-        vals, b = self.plan.assemble(param, self.form.mode, self.form.scale, self.form.f, self._g)
+        vals, b = autograd.assemble(self.plan, param, self.form.mode, self.form.scale, self.form.f, self._g)
         return CsrMatrix(self.plan, vals, (param, self.form.mode, self.form.scale)), b
 
     @property
@@ -147,7 +198,8 @@ class FEM:
     def matrix_free(self, args=None):
         """Matrix-free operator and RHS for the same form (``b`` from one assembly of the load)."""
         param = self._param_tensor(args or {})
-        _, b = self._assemble(args or {})
+        b = self.plan.load(param.detach() if param is not None else None, self.form.mode, self.form.scale,
+                           self.form.f, self._g)
         return MatrixFreeOperator(self.plan, param, self.form.mode, self.form.scale), b
 
     @property
@@ -222,7 +274,7 @@ class FEM:
         if time is not None:
             raise ValueError("fem.solve: time= needs a transient form (a ui.t * vi term)")
         if self.form.param is not None:
-            return self.operator.solve(args, linear, precond, x0)
+            return self.operator._solve_eager(args, linear, precond, x0)
         A, b = self.operator
         # steady linear default of the reference: Jacobi-preconditioned BiCGStab (jno/_fem.py:110-116)
         return _solve(A, b, linear, precond, x0, default=bicgstab)

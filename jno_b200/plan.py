@@ -143,6 +143,28 @@ class FemPlan:
                                            _lib.ptr(vals), _lib.ptr(b), _lib.stream_handle()))
         return vals, b
 
+    def load(self, param=None, mode=_lib.COEF_EXP, scale=1.0, f=1.0, g=None, b=None):
+        """The load ``b`` of :meth:`assemble` alone (no values): what a matrix-free solve needs."""
+        if mode != _lib.COEF_CONST:
+            param = _device_tensor(param, torch.float64)
+        g = None if g is None else _device_tensor(g, torch.float64)
+        b = torch.empty(self.n, dtype=torch.float64, device=self.device) if b is None else b
+        _lib.check(self._lib.femk_assemble(self._h, _lib.ptr(param), int(mode), float(scale), float(f), _lib.ptr(g),
+                                           None, _lib.ptr(b), _lib.stream_handle()))
+        return b
+
+    def assemble_vjp(self, param, grad_vals=None, grad_b=None, mode=_lib.COEF_EXP, scale=1.0, g=None):
+        """d(vals, b)/dparam applied to the cotangents (grad_vals f64[nnz], grad_b f64[n], either
+        may be None): f64[ntet] for P0 modes, f64[nvert] for nodal modes (``femk_assemble_vjp``)."""
+        param = _device_tensor(param, torch.float64)
+        g = None if g is None else _device_tensor(g, torch.float64)
+        nodal = mode in (_lib.COEF_NODAL_EXP, _lib.COEF_NODAL_LINEAR)
+        out = torch.empty(self.nvert if nodal else self.ntet, dtype=torch.float64, device=self.device)
+        _lib.check(self._lib.femk_assemble_vjp(self._h, _lib.ptr(param), int(mode), float(scale), _lib.ptr(g),
+                                               _lib.ptr(grad_vals), _lib.ptr(grad_b), _lib.ptr(out),
+                                               _lib.stream_handle()))
+        return out
+
     def compact(self, vals):
         """(indptr i32[n+1], indices i32[m], data f64[m]): the entries of ``vals`` with ``|v| > 0``
         in CSR order (``compress_eager``, jno/utils/solver/fem_utils.py:4063-4091)."""

@@ -75,45 +75,77 @@ class LinearSolver:
         return hash(self.key)
 
     def __call__(self, A, b, *, M=None, x0=None):
+        """``x = solve(A, b)``. Differentiable (torch autograd) in ``b`` and in ``A``: through the
+        assembly parameter when ``A`` is the unmodified output of ``FemLinearSystem.evaluate`` (or a
+        matrix-free operator of a parameter that requires grad), else through ``A.data``; the
+        backward pass is one more solve with the same solver on the transposed (= the same) system,
+        as ``custom_linear_solve`` does in the reference (jno/solve.py:202-206)."""
+        from . import autograd
+        from .sparse import CompactCsrMatrix
+
         op = A.A if isinstance(A, LinearOperator) else A
         if not isinstance(op, (CsrMatrix, MatrixFreeOperator)):
             raise TypeError("the B200 CG takes an assembled CsrMatrix or a MatrixFreeOperator")
         plan = op.plan
-        b = _as_cuda(b, plan.device).reshape(-1)
+        b = b if isinstance(b, torch.Tensor) and b.is_cuda and b.dtype == torch.float64 else _as_cuda(b, plan.device)
+        b = b.reshape(-1)
         if M is not None and hasattr(M, "materialize"):
             M = M.materialize(PrecondContext(op))
         if M is not None and not isinstance(M, JacobiApplier):
             raise TypeError("the fused CG kernels apply the Jacobi preconditioner only (jno_b200.precond.jacobi())")
-        inv = None if M is None else M.inv_diag
-        x = torch.zeros_like(b) if x0 is None else _as_cuda(x0, plan.device).reshape(-1).clone()
+        inv = None if M is None else M.inv_diag.detach()
+        x0 = None if x0 is None else _as_cuda(x0, plan.device).reshape(-1).detach()
+        grad_a = False
+        if torch.is_grad_enabled():
+            if isinstance(op, MatrixFreeOperator):
+                grad_a = isinstance(op.param, torch.Tensor) and op.param.requires_grad
+            else:
+                grad_a = op.data.requires_grad
+                if grad_a and isinstance(op, CompactCsrMatrix):
+                    raise NotImplementedError("gradients through a compacted (non-parametric) operator")
+        if not (grad_a or (torch.is_grad_enabled() and b.requires_grad)):
+            return self._run(op, None, b.detach(), inv, x0)
+        first = [True]
+
+        def solve(vals, rhs):
+            x = self._run(op, vals, rhs, inv, x0 if first[0] else None)  # the adjoint solve starts at 0
+            first[0] = False
+            return x
+
+        return autograd.linear_solve(op, b, solve)
+
+    def _run(self, op, vals, b, inv, x0):
+        """One solve on the device (no autograd): the forward, or the adjoint of a backward pass."""
+        plan = op.plan
+        if vals is None and isinstance(op, CsrMatrix):
+            vals = op.solver_values
+        x = torch.zeros_like(b) if x0 is None else x0.clone()
         if self.precision == "mixed":
             if not isinstance(op, CsrMatrix) or inv is None:
                 raise ValueError("precision='mixed' needs an assembled CsrMatrix and M=jacobi()")
             mode = _lib.MIXED_RELIABLE if self.refine == "reliable" else _lib.MIXED_RESTART
-            x, inner, outer, rel, st = plan.pcg_mixed(op.solver_values, b, inv, x, self.tol, self.atol,
-                                                      self.mixed_maxiter, mode)
+            x, inner, outer, rel, st = plan.pcg_mixed(vals, b, inv, x, self.tol, self.atol, self.mixed_maxiter, mode)
             fb = 0
             if st == _lib.FEMK_NOT_CONVERGED:
                 # FP32 rounding stalled the inner loop: finish in FP64 from the mixed iterate
-                x, fb, rel, st = plan.pcg(op.solver_values, b, x, inv, self.tol, self.atol, self.maxiter)
+                x, fb, rel, st = plan.pcg(vals, b, x, inv, self.tol, self.atol, self.maxiter)
             self.last_info = SolveInfo(inner, rel, st, outer, fb)
         elif self.name == "bicgstab":
             if not isinstance(op, CsrMatrix):
                 raise TypeError("the B200 BiCGStab takes an assembled CsrMatrix")
-            x, it, rel, st = plan.bicgstab(op.solver_values, b, x, inv, self.tol, self.atol, self.maxiter)
+            x, it, rel, st = plan.bicgstab(vals, b, x, inv, self.tol, self.atol, self.maxiter)
             self.last_info = SolveInfo(it, rel, st)
         elif self.name == "gmres":
             if not isinstance(op, CsrMatrix):
                 raise TypeError("the B200 GMRES takes an assembled CsrMatrix")
-            x, it, cyc, rel, st = plan.gmres(op.solver_values, b, x, inv, self.tol, self.atol, self.restart,
-                                             self.gmres_maxiter)
+            x, it, cyc, rel, st = plan.gmres(vals, b, x, inv, self.tol, self.atol, self.restart, self.gmres_maxiter)
             self.last_info = SolveInfo(it, rel, st, outer=cyc)
         elif isinstance(op, MatrixFreeOperator):
-            x, it, rel, st = plan.pcg_matfree(op.param, b, x, inv, op.mode, op.scale, self.tol, self.atol,
+            x, it, rel, st = plan.pcg_matfree(op.param.detach(), b, x, inv, op.mode, op.scale, self.tol, self.atol,
                                               self.maxiter)
             self.last_info = SolveInfo(it, rel, st)
         else:
-            x, it, rel, st = plan.pcg(op.solver_values, b, x, inv, self.tol, self.atol, self.maxiter)
+            x, it, rel, st = plan.pcg(vals, b, x, inv, self.tol, self.atol, self.maxiter)
             self.last_info = SolveInfo(it, rel, st)
         rel = self.last_info.relres
         if not math.isfinite(rel) or rel > 1e-4:

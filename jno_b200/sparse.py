@@ -22,7 +22,10 @@ class CsrMatrix:
         self.data = data
         self.indptr, self.indices = plan.pattern()
         self.shape = (plan.n, plan.n)
-        self.assembly = assembly  # (param, mode, scale) of the values, for matrix-free use
+        # (param, mode, scale) of the values: matrix-free use, and the solves' gradient through the
+        # parameter while `data` is still the assembly's own output
+        self.assembly = assembly
+        self._assembled_data = data if assembly is not None else None
         self._inv_diag = None
 
     @property
@@ -31,8 +34,8 @@ class CsrMatrix:
 
     @property
     def solver_values(self):
-        """Values on the plan's canonical pattern: what the SpMV and CG kernels stream."""
-        return self.data
+        """Values on the plan's canonical pattern: what the SpMV and CG kernels stream (no autograd)."""
+        return self.data.detach()
 
     def compact(self):
         """:class:`CompactCsrMatrix` of the entries with ``|v| > 0`` (``compress_eager``)."""
@@ -54,18 +57,18 @@ class CsrMatrix:
         return self._inv_diag
 
     def todense(self):
+        """Dense copy (differentiable in ``data``)."""
         rows = torch.repeat_interleave(
             torch.arange(self.plan.n, device=self.data.device), (self.indptr[1:] - self.indptr[:-1]).long()
         )
         out = torch.zeros(self.shape, dtype=self.data.dtype, device=self.data.device)
-        out[rows, self.indices.long()] = self.data
-        return out
+        return out.index_put((rows, self.indices.long()), self.data)
 
     def to_scipy(self):
         import scipy.sparse as sp
 
         return sp.csr_matrix(
-            (self.data.cpu().numpy(), self.indices.cpu().numpy(), self.indptr.cpu().numpy()), shape=self.shape
+            (self.data.detach().cpu().numpy(), self.indices.cpu().numpy(), self.indptr.cpu().numpy()), shape=self.shape
         )
 
     def to_bcoo(self, appended=False):
@@ -75,7 +78,7 @@ class CsrMatrix:
             (self.indptr[1:] - self.indptr[:-1]).long(),
         )
         idx = torch.stack([rows, self.indices], dim=1)
-        data = self.data.clone()
+        data = self.data.detach().clone()
         if not appended:
             return idx, data
         ex = self.plan.export()
@@ -99,7 +102,8 @@ class CompactCsrMatrix(CsrMatrix):
     def __init__(self, full):
         self.plan = full.plan
         self.shape = full.shape
-        self.assembly = full.assembly
+        self.assembly = None  # the compact form comes from the non-parametric route
+        self._assembled_data = None
         self._full = full.solver_values
         self.indptr, self.indices, self.data = full.plan.compact(self._full)
         self._inv_diag = None

@@ -145,15 +145,18 @@ class TraceOn(Expr):
 
 class Param(Expr):
     """``jno.np.parameter(<symbol>, name=...)`` (jno/architectures/models.py:85-117): one value per
-    element for a P0 symbol, one value per P1 vertex (``nodal``) for a P1 symbol."""
+    element for a P0 symbol, one value per P1 vertex (``nodal``) for a P1 symbol; or
+    ``jno.np.parameter((1,), name=...)``, one value for the whole mesh (``scalar``)."""
 
-    def __init__(self, sym, name, nodal=False):
-        self.sym, self.name, self.nodal = sym, name, nodal
+    def __init__(self, sym, name, nodal=False, scalar=False):
+        self.sym, self.name, self.nodal, self.scalar = sym, name, nodal, scalar
 
 
 def parameter(sym, name="param", **_):
+    if isinstance(sym, tuple) and tuple(sym) in ((), (1,)):
+        return Param(None, name, scalar=True)  # a global scalar (tests/test_fem_native_lagrange.py:666)
     if not isinstance(sym, FieldSymbol):
-        raise NotImplementedError("jno.np.parameter takes a field symbol on the B200 path")
+        raise NotImplementedError("jno.np.parameter takes a field symbol or the shape (1,) on the B200 path")
     if sym.space == "P0":
         return Param(sym, name)
     if sym.order != 1:
@@ -207,19 +210,22 @@ def _coef_key(factors):
     if not params and not exps:
         return ("const",)
     if len(params) == 1 and not exps:
-        return ("nodal_linear" if params[0].nodal else "linear", params[0].name)
+        kind = "nodal_linear" if params[0].nodal else ("scalar_linear" if params[0].scalar else "linear")
+        return (kind, params[0].name)
     if len(exps) == 1 and not params and isinstance(exps[0].a, Param):
-        return ("nodal_exp" if exps[0].a.nodal else "exp", exps[0].a.name)
+        kind = "nodal_exp" if exps[0].a.nodal else ("scalar_exp" if exps[0].a.scalar else "exp")
+        return (kind, exps[0].a.name)
     raise NotImplementedError("only c, c*p and c*exp(p) coefficients are on the B200 path")
 
 
 class WeakForm:
     """Classified volume form: k_e = scale * g(param_e), source f, field order; ``mass`` is the
-    constant coefficient of the ``ui.t * vi`` term of a transient form (None when steady)."""
+    constant coefficient of the ``ui.t * vi`` term of a transient form (None when steady);
+    ``scalar`` when the parameter is one value for the whole mesh (broadcast to every element)."""
 
-    def __init__(self, order, mode, scale, param, f, domain, mass=None):
+    def __init__(self, order, mode, scale, param, f, domain, mass=None, scalar=False):
         self.order, self.mode, self.scale, self.param, self.f, self.domain = order, mode, scale, param, f, domain
-        self.mass = mass
+        self.mass, self.scalar = mass, scalar
 
 
 def classify_volume(expr):
@@ -269,12 +275,14 @@ def classify_volume(expr):
     from . import _lib
 
     mode = {"const": _lib.COEF_CONST, "linear": _lib.COEF_LINEAR, "exp": _lib.COEF_EXP,
+            "scalar_linear": _lib.COEF_LINEAR, "scalar_exp": _lib.COEF_EXP,
             "nodal_linear": _lib.COEF_NODAL_LINEAR, "nodal_exp": _lib.COEF_NODAL_EXP}[key[0]]
     if key[0].startswith("nodal") and order != 1:
         raise NotImplementedError("a nodal P1 parameter in a P2 form is outside the B200 path")
     if mass is not None and not mass > 0.0:
         raise NotImplementedError("the ui.t * vi coefficient must be a positive constant")
-    return WeakForm(order, mode, scale, key[1] if len(key) > 1 else None, source, domain, mass)
+    return WeakForm(order, mode, scale, key[1] if len(key) > 1 else None, source, domain, mass,
+                    scalar=key[0].startswith("scalar"))
 
 
 def evaluate_on(expr, pts):

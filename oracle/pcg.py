@@ -194,3 +194,108 @@ def residual_check(A, b, x, rtol=1e-4):
     if not np.isfinite(rel) or rel > rtol:
         raise RuntimeError(f"jno.solve.cg did not solve the system (relative residual {rel:.1e})")
     return rel
+
+
+def mixed_pcg(A, b, inv_diag, tol=1e-8, atol=0.0, maxiter=20_000, delta2=1e-4, restart=False,
+              single_reduction=True):
+    """The mixed-precision Jacobi-PCG of ``femk_pcg_mixed`` (no reference counterpart): FP32 values
+    and inner vectors, FP64 solution, FP64 true residual at reliable updates (when the FP32 <r, r>
+    fell by ``delta2`` since the last update, met the stop test, or at the cap), stopping on the FP64
+    residual with the stop rule of :func:`pcg`. ``restart`` starts a new direction at every update.
+
+    ``single_reduction`` selects the device's arrangement: CG on A^ = S A S (S = D^-1/2, formed in
+    FP64, rounded to FP32) -- Jacobi-PCG in split form, so z^ = r^ -- with w = A^ r and s = A^ p by
+    recurrence, the products <p, s>, <r, s>, <r, r>, <r, D r> taken after the vector update and
+    <r, w> after the SpMV, and <p', A^ p'> = <r, w> + 2 beta <r, s> + beta^2 <p, s>. Otherwise the
+    textbook FP32 loop (q = A p, <p, q> and <r, z> in two reductions, z = D^-1 r). FP32 products are
+    summed in FP64 here (the device sums FP32 per thread, then FP64), so iteration counts agree to a
+    few. Returns (x, FP32 iterations, FP64 residual evaluations)."""
+    import scipy.sparse as sp
+
+    A64 = A.tocsr()
+    f32 = np.float32
+    b = np.asarray(b, dtype=np.float64)
+    dinv = np.asarray(inv_diag, dtype=np.float64)
+    n = b.size
+
+    def dot(a, c):
+        return float(np.dot(a.astype(np.float64), c.astype(np.float64)))
+
+    x = np.zeros(n)
+    e = np.zeros(n, f32)
+    atol2 = max(tol * tol * float(b @ b), atol * atol)
+    it, outer = 0, 1
+    if not single_reduction:
+        A32, d32 = A64.astype(f32), dinv.astype(f32)
+        r64 = b - A64 @ x
+        rr_since = float(r64 @ r64)
+        if not rr_since > atol2 or maxiter <= 0:
+            return x, 0, outer
+        r = r64.astype(f32)
+        u = d32 * r
+        p = u.copy()
+        gamma = dot(r, u)
+        while True:
+            q = A32 @ p
+            alpha = gamma / dot(p, q)
+            e = f32(alpha) * p + e
+            r = -f32(alpha) * q + r
+            u = d32 * r
+            g2, rho = dot(r, u), dot(r, r)
+            it += 1
+            if rho <= atol2 or rho < delta2 * rr_since or it >= maxiter:
+                x = x + e
+                e[:] = 0
+                r64 = b - A64 @ x
+                rr_since = float(r64 @ r64)
+                outer += 1
+                if rr_since <= atol2 or it >= maxiter:
+                    return x, it, outer
+                r = r64.astype(f32)
+                u = d32 * r
+                g2 = dot(r, u)
+                beta = 0.0 if restart else g2 / gamma
+            else:
+                beta = g2 / gamma
+            gamma = g2
+            p = f32(beta) * p + u
+    sc64 = np.sqrt(dinv)
+    Ah = (sp.diags(sc64) @ A64 @ sp.diags(sc64)).tocsr().astype(f32)
+    dd = (1.0 / dinv).astype(f32)
+    p = np.zeros(n, f32)
+    s = np.zeros(n, f32)
+
+    def replace():
+        r64 = b - A64 @ x
+        return (sc64 * r64).astype(f32), float(r64 @ r64)
+
+    r, rr_since = replace()
+    if not rr_since > atol2 or maxiter <= 0:
+        return x, 0, outer
+    gamma, alpha, beta = None, 1.0, 0.0
+    w = Ah @ r  # the first direction: beta = 0
+    g2, ps, rs = dot(r, r), 0.0, 0.0
+    while True:
+        den = dot(r, w) + 2.0 * beta * rs + beta * beta * ps
+        if not den > 0:
+            raise ArithmeticError("mixed_pcg: <p, A p> <= 0 in FP32")
+        alpha, gamma = g2 / den, g2
+        p = f32(beta) * p + r  # K_A
+        s = f32(beta) * s + w
+        e = f32(alpha) * p + e
+        r = -f32(alpha) * s + r
+        ps, rs, g2, rho = dot(p, s), dot(r, s), dot(r, r), dot(r * r, dd)
+        w = Ah @ r  # K_B
+        it += 1
+        if rho <= atol2 or rho < delta2 * rr_since or it >= maxiter:
+            x = x + sc64 * e.astype(np.float64)
+            e[:] = 0
+            r, rr_since = replace()
+            outer += 1
+            if rr_since <= atol2 or it >= maxiter:
+                return x, it, outer
+            g2, ps, rs = dot(r, r), dot(p, s), dot(r, s)  # the refresh step's products
+            w = Ah @ r
+            beta = 0.0 if restart else g2 / gamma
+        else:
+            beta = g2 / gamma

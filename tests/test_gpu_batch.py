@@ -101,3 +101,34 @@ def test_batched_mixed_reaches_the_fp64_stop_rule(tile_rows, bps):
     assert outer[-1] >= 2  # the 16^3 problem needs FP64 reliable updates to reach 1e-8
     x2, it2, rel2 = batch.solve(vals, b, tol=1e-8, schedule=sched, precision="mixed")
     assert torch.equal(x, x2) and np.array_equal(it, it2)
+
+
+def test_grid_barrier_wait_runs_out_and_the_context_survives():
+    """Failure detection without a GPU fault: with the plan option test_skip_arrival = 0, block 0 of
+    the persistent batched launch does not arrive at its first grid barrier, so every other block
+    waits out barrier_limit_ms (5 ms here), raises the barrier's timeout word and returns; the call
+    reports FEMK_TIMEOUT within a bounded time. The same plan then solves with femk_pcg, and a plan of
+    the same batch without the option solves the batch: the context is intact."""
+    import time
+
+    from jno_b200 import _lib
+    from jno_b200.batch import BatchedPoisson
+
+    probs = _problems([4, 4])
+    meshes = [(p, t) for p, t, _ in probs]
+    logk = [lk for _, _, lk in probs]
+    bad = BatchedPoisson(meshes, options={"test_skip_arrival": 0, "barrier_limit_ms": 5.0})
+    vals, b = bad.assemble(logk)
+    inv = bad.plan.jacobi(vals)
+    t0 = time.perf_counter()
+    with pytest.raises(_lib.FemkError) as err:
+        bad.plan.pcg_batched(bad.row_off, vals, b, None, inv, 1e-8, 0.0, 1000, 32, 1)
+    assert err.value.status == _lib.FEMK_TIMEOUT
+    assert time.perf_counter() - t0 < 10.0
+    x, it, rel, st = bad.plan.pcg(vals, b, inv_diag=inv, tol=1e-8)
+    assert st == 0 and rel <= 2e-8
+    good = BatchedPoisson(meshes)
+    vg, bg = good.assemble(logk)
+    xg, itg, relg = good.solve(vg, bg, tol=1e-8, schedule={"tile_rows": 32, "blocks_per_sm": 1})
+    assert np.all(relg <= 2e-8)
+    assert torch.linalg.norm(xg - x) <= 1e-7 * torch.linalg.norm(x)

@@ -639,31 +639,61 @@ def test_p0_linearity_and_support_on_device():
 
 
 
-@pytest.mark.parametrize("n,order,opts", [(12, 1, {}), (12, 1, {"ring32": 0}), (12, 1, {"solver_layout": 0}),
-                                          (4, 2, {})])
-def test_mixed_single_reduction_loop(n, order, opts):
-    """The FP32 inner loop in single-reduction (Chronopoulos-Gear) form on each of its SpMV kernels
-    (bulk-copy ring, thread-per-row sliced ELL, canonical CSR; P2 rows wider than the ring): the
-    FP64 residual meets the 1e-8 stop rule, the solution agrees with a tight FP64 solve to 1e-7, the
-    FP32 iteration count stays near FP64 CG's, and graph replay and direct launches of the same
-    chunks give bit-identical iterates."""
-    pf, cf, tets, p1 = _mesh(n, order)
+@pytest.mark.parametrize("dim,n,order,opts", [(3, 12, 1, {}), (3, 12, 1, {"ring32": 0}),
+                                              (3, 12, 1, {"solver_layout": 0}), (3, 4, 2, {}), (2, 64, 1, {})])
+def test_mixed_single_reduction_loop(dim, n, order, opts):
+    """The FP32 inner loop in single-reduction form on each of its SpMV kernels (bulk-copy ring,
+    thread-per-row sliced ELL, canonical CSR; P2 rows wider than the ring; 2-D rows of 7): the FP64
+    residual meets the 1e-8 stop rule, the solution agrees with a tight FP64 solve to 1e-7, the FP32
+    iteration count is the oracle restatement's (oracle.pcg.mixed_pcg) within 10 % + 3, in both modes,
+    and graph replay and direct launches of the same chunks give bit-identical iterates."""
+    pf, cf, tets, p1 = _mesh(n, order) if dim == 3 else om.unit_square(n, order, seed=0)
     logk = om.logk_field(len(tets), 1011)
+    s, _ = (_oracle_system(pf, cf, order, logk) if dim == 3 else
+            (oa.assemble(pf, cf, order, om.boundary_nodes(cf, order, nv=3), np.exp(logk)), None))
+    inv_o = oa.jacobi_inverse(oa.matrix_diagonal(s))
     sols = []
+    vals = None
     for replay in (1, 0):
         plan = _plan(p1, tets, order, {**opts, "graph_replay": replay})
-        vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
-        inv = plan.jacobi(vals)
-        u64, it64, _, _ = plan.pcg(vals, b, inv_diag=inv, tol=1e-8)
-        ut, _, _, _ = plan.pcg(vals, b, inv_diag=inv, tol=1e-13)
+        if vals is None:  # one assembly for both plans (same pattern): FP64 atomics may round differently
+            vals, b = plan.assemble(torch.as_tensor(logk, device="cuda"))
+            inv = plan.jacobi(vals)
+            ut, _, _, _ = plan.pcg(vals, b, inv_diag=inv, tol=1e-13)
         for mode in (0, 1):
             u, inner, outer, rel, st = plan.pcg_mixed(vals, b, inv, tol=1e-8, mode=mode)
             assert st == 0 and rel <= 1e-8 and outer >= 2
             r = b - plan.spmv(vals, u)
             assert (torch.linalg.norm(r) / torch.linalg.norm(b)).item() <= 1e-8
             assert (torch.linalg.norm(u - ut) / torch.linalg.norm(ut)).item() <= 1e-7
-            if mode == 0:
-                assert inner <= 1.25 * it64 + 16, (inner, it64)
+            # the device's reliable-update thresholds: 1e-4 (reliable), 1e-8 (restart); FP32 rounding
+            # order alone moves the counts by several percent (the oracle's two arrangements differ so)
+            _, ito, outo = op.mixed_pcg(s.csr(), s.b, inv_o, tol=1e-8, restart=mode == 1,
+                                        delta2=1e-8 if mode == 1 else 1e-4)
+            assert abs(inner - ito) <= 0.1 * ito + 3, (inner, ito)
             sols.append((mode, u, inner, outer))
     for (m0, u0, i0, o0), (m1, u1, i1, o1) in zip(sols[:2], sols[2:]):
         assert m0 == m1 and i0 == i1 and o0 == o1 and torch.equal(u0, u1)
+
+
+@pytest.mark.parametrize("dim,n,order", [(3, 16, 1), (3, 6, 2), (2, 32, 1), (2, 12, 2)])
+def test_assembly_is_bitwise_reproducible(dim, n, order):
+    """The row-gather assembly adds each row's entries in one fixed order (its incidence list): two
+    assemblies, and two plans of the same mesh, give the same bits for the values and the load; the
+    load-only form (matrix-free use) gives the same load."""
+    pf, cf, cells, p1 = om.kuhn_cube(n, order=order, seed=4) if dim == 3 else om.unit_square(n, order, seed=4)
+    lk = torch.as_tensor(om.logk_field(len(cells), 1012), device="cuda")
+    g = torch.as_tensor(np.cos(pf[:, 0]) + pf[:, 1], device="cuda")
+    out = []
+    for _ in range(2):
+        plan = _plan(p1, cells, order)
+        for _ in range(2):
+            vals, b = plan.assemble(lk, g=g)
+            out.append((vals, b))
+        assert torch.equal(plan.load(lk, g=g), out[0][1])
+    for vals, b in out[1:]:
+        assert torch.equal(vals, out[0][0]) and torch.equal(b, out[0][1])
+    s = oa.assemble(pf, cf, order, om.boundary_nodes(cf, order, nv=dim + 1), np.exp(lk.cpu().numpy()),
+                    g=g.cpu().numpy())
+    assert np.abs(out[0][0].cpu().numpy() - s.data).max() <= VAL_TOL * np.abs(s.data).max()
+    assert np.abs(out[0][1].cpu().numpy() - s.b).max() <= VAL_TOL * np.abs(s.b).max()

@@ -267,3 +267,23 @@ def test_oracle_nodal_gradient_matches_fd(mode):
         e[i] = 1e-6
         fd = (Jof(vals + e) - Jof(vals - e)) / 2e-6
         assert abs(fd - g[i]) <= 1e-6 * np.abs(g).max() + 1e-6 * abs(g[i])
+
+
+@pytest.mark.parametrize("dim,n", [(2, 32), (3, 12)])
+def test_mixed_single_reduction_matches_textbook_loop(dim, n):
+    """The mixed solver's FP32 iteration in single-reduction form (all products of an iteration in
+    one reduction, <p', A p'> expanded) runs the same iteration as the textbook FP32 loop: FP32
+    iteration counts within a few, FP64 updates equal, both meet the FP64 stop rule, and the solutions
+    agree with a tight FP64 solve to 1e-7. Restart mode (beta = 0 at each update) also converges."""
+    pf, cf, cells, p1 = om.unit_square(n, 1, seed=0) if dim == 2 else om.kuhn_cube(n, 1, seed=0)
+    s = oa.assemble(pf, cf, 1, om.boundary_nodes(cf, 1, nv=dim + 1), np.exp(om.logk_field(len(cells), 1000)))
+    A = s.csr()
+    inv = oa.jacobi_inverse(oa.matrix_diagonal(s))
+    xt, _, _ = op.pcg(A, s.b, inv, tol=1e-13)
+    out = {}
+    for tag, kw in (("single", {}), ("textbook", {"single_reduction": False}), ("restart", {"restart": True})):
+        x, it, outer = op.mixed_pcg(A, s.b, inv, tol=1e-8, **kw)
+        assert np.linalg.norm(s.b - A @ x) <= 1e-8 * np.linalg.norm(s.b)
+        assert np.linalg.norm(x - xt) <= 1e-7 * np.linalg.norm(xt)
+        out[tag] = (it, outer)
+    assert abs(out["single"][0] - out["textbook"][0]) <= 3 and out["single"][1] == out["textbook"][1]
