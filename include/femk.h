@@ -69,6 +69,10 @@ typedef struct femk_plan_info {
 /* Library version (major*10000 + minor*100 + patch). */
 int femk_version(void);
 
+/* 1 in the bounds-checked build (-DFEMK_BOUNDS_CHECK: kernels check their indexed accesses and the
+ * entry points return FEMK_EBOUNDS when a check failed), 0 in the normal build. */
+int femk_bounds_checked(void);
+
 /* Number of CUDA kernels this library has launched in this process (all devices, all threads). */
 int64_t femk_kernel_launches(void);
 
@@ -134,6 +138,10 @@ typedef struct femk_plan_options {
   int32_t test_skip_arrival; /* testing the bounded waits: the block with this index skips its first
                                 grid-barrier arrival in femk_pcg_batched*, so every other block waits out
                                 barrier_limit_ms and the call returns FEMK_TIMEOUT; -1 (default): none */
+  int32_t l2_persist;     /* 1: the CG and mixed loops keep their workspace vectors resident in L2 (an
+                             access-policy window with persisting hits over the solver workspace; the
+                             context's persisting-L2 limit is raised to what the window needs, never lowered,
+                             and the persisting lines are reset when the solve returns); 0 (default): off */
   double mixed_delta2;    /* reliable update of the mixed solvers once <r, r> fell by this factor; 0 (default): 1e-4 */
   double barrier_limit_ms; /* limit of each grid-barrier wait of femk_pcg_batched*, in milliseconds at the
                               maximum SM clock; 0 (default): 2000 */

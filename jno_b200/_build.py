@@ -2,7 +2,7 @@
 
 ``python -m jno_b200._build`` (or ``__graft_entry__.build()``) compiles every ``csrc/*.cu`` with
 nvcc for ``-gencode arch=compute_100a,code=sm_100a`` and links one shared library next to this
-file. The CUDA runtime is linked statically, so the library loads without a CUDA toolkit on the
+file; ``--bounds`` builds ``libfemk_bounds.so`` from the same sources with ``-DFEMK_BOUNDS_CHECK``. The CUDA runtime is linked statically, so the library loads without a CUDA toolkit on the
 library path; streams created by PyTorch are plain driver streams and are accepted as ``void*``.
 """
 
@@ -15,6 +15,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libfemk.so")
+# the same sources with -DFEMK_BOUNDS_CHECK: every checked index returns FEMK_EBOUNDS instead of faulting
+LIB_BOUNDS = os.path.join(HERE, "libfemk_bounds.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr"]
 
@@ -30,9 +32,12 @@ def sources():
     return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
 
 
-def build(verbose=False, extra=()):
+def build(verbose=False, extra=(), bounds=False):
+    """Compile every source into LIB (or, with ``bounds``, the bounds-checked LIB_BOUNDS)."""
     nvcc = _nvcc()
-    objdir = os.path.join(ROOT, "_build")
+    objdir = os.path.join(ROOT, "_build", "bounds") if bounds else os.path.join(ROOT, "_build")
+    extra = tuple(extra) + (("-DFEMK_BOUNDS_CHECK",) if bounds else ())
+    lib = LIB_BOUNDS if bounds else LIB
     os.makedirs(objdir, exist_ok=True)
     objs = []
     inc = ["-I", os.path.join(ROOT, "include")]
@@ -45,14 +50,14 @@ def build(verbose=False, extra=()):
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
         objs.append(obj)
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-cudart", "static"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv))
+    print(build(verbose="-v" in sys.argv, bounds="--bounds" in sys.argv))

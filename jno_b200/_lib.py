@@ -80,6 +80,7 @@ class PlanOptions(ctypes.Structure):
         ("vec_blocks", ctypes.c_int32),
         ("split_updates", ctypes.c_int32),
         ("test_skip_arrival", ctypes.c_int32),
+        ("l2_persist", ctypes.c_int32),
         ("mixed_delta2", ctypes.c_double),
         ("barrier_limit_ms", ctypes.c_double),
     ]
@@ -94,6 +95,7 @@ _D = ctypes.c_double
 #: name -> argtypes of every entry point declared in include/femk.h
 SIGNATURES = {
     "femk_version": [],
+    "femk_bounds_checked": [],
     "femk_kernel_launches": [],
     "femk_last_error_string": [],
     "femk_plan_create": [_P, _I64, _P, _I64, _I, _P, _P, ctypes.POINTER(_P)],

@@ -11,13 +11,15 @@
 // (masked 0 + the appended unit triplet), b[d] = g[d], and free rows receive b -= A e.
 //
 // femk_assemble gathers instead of scattering: each CSR row is owned by one thread, which walks the
-// row's DOF -> element incidence list (ascending element ids) and adds the row's entries of each
-// element matrix, in that fixed order, into the row's values staged in shared memory; a block's
-// rows are consecutive, so their values form one contiguous span that the block zeroes, accumulates
-// and writes back with coalesced stores. Columns are found by binary search in the block's staged
-// column indices. No atomics: the values and the load are the same bits on every run (the
-// segment_sum of the reference has no defined order either). Each element's geometry is evaluated
-// once per incident row (4 times for P1, 10 for P2), which the FP64 units absorb.
+// row's incident elements (ascending element ids) in the plan's assembly stream -- per (row,
+// element) pair the row of the element's unit-coefficient stiffness matrix and the positions of its
+// columns in the CSR row, precomputed when the plan is built, since the geometry does not change
+// between assemblies -- and adds k_e times that row, in that fixed order, into the row's values
+// staged in shared memory; a block's rows are consecutive, so their values form one contiguous span
+// that the block zeroes, accumulates and writes back with coalesced stores. The stream is laid out in
+// 32-row slices (entry k of a row beside entry k of its 31 neighbours), so a warp's loads are
+// coalesced; the only gather is the coefficient of each element. No atomics: the values and the load
+// are the same bits on every run (the segment_sum of the reference has no defined order either).
 #include <cmath>
 
 #include "femk_element.cuh"
@@ -28,111 +30,70 @@ namespace {
 
 constexpr int kThreads = 128;
 
-__device__ __forceinline__ int32_t search_col(const int32_t* cols, int32_t len, int32_t col) {
-  int32_t lo = 0, hi = len;
-  while (lo < hi) {
-    const int32_t mid = (lo + hi) >> 1;
-    if (cols[mid] < col)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  return lo;
-}
-
-// Row A of one element matrix (A compile-time: the element matrices stay in registers) added into
-// the row's staged values; returns the row's load contribution f fhat_A - sum over Dirichlet
-// columns of k K_hat[A][c] g[c].
-template <int ND, int A, bool VALS>
-__device__ __forceinline__ double add_row(const double (&VG)[Cell<ND>::NV][Cell<ND>::NV], double vol, double k,
-                                          const int32_t (&dof)[ND], const uint8_t* __restrict__ dmask,
-                                          const double* __restrict__ g, double f, const int32_t* scl, int32_t len,
-                                          double* svl, int* __restrict__ err) {
-  double bi = f * fhat<ND>(vol, A);
-#pragma unroll
-  for (int c = 0; c < ND; ++c) {
-    const double kac = k * khat<ND>(VG, A, c);
-    if (__ldg(dmask + dof[c])) {
-      if (g) bi -= kac * __ldg(g + dof[c]);
-    } else if (VALS) {
-      const int32_t pos = search_col(scl, len, dof[c]);
-      if (pos < len && scl[pos] == dof[c])
-        svl[pos] += kac;
-      else
-        atomicOr(err, 1);  // the pattern was built from these cells: unreachable
-    }
-  }
-  return bi;
-}
-
-template <int ND, int A, bool VALS>
-__device__ __forceinline__ double add_row_at(int a, const double (&VG)[Cell<ND>::NV][Cell<ND>::NV], double vol,
-                                             double k, const int32_t (&dof)[ND], const uint8_t* __restrict__ dmask,
-                                             const double* __restrict__ g, double f, const int32_t* scl, int32_t len,
-                                             double* svl, int* __restrict__ err) {
-  if constexpr (A + 1 < ND) {
-    if (a != A) return add_row_at<ND, A + 1, VALS>(a, VG, vol, k, dof, dmask, g, f, scl, len, svl, err);
-  }
-  return add_row<ND, A, VALS>(VG, vol, k, dof, dmask, g, f, scl, len, svl, err);
-}
-
-// One thread per row (blockDim.x consecutive rows per block); VALS: the CSR values are assembled
-// (else the load alone, for matrix-free use). Shared memory: span_cap doubles of values + span_cap
-// int32 columns, span_cap = the plan's largest block span.
+// One thread per row (blockDim.x consecutive rows per block, a multiple of 32 so that a warp walks
+// one slice of the assembly stream); VALS: the CSR values are assembled (else the load alone, for
+// matrix-free use). Shared memory: span_cap doubles, span_cap = the plan's largest block span.
 template <int ND, bool VALS>
-__global__ void __launch_bounds__(kThreads) k_assemble_rows(
-    const double* __restrict__ xyz, const int32_t* __restrict__ cells, const int32_t* __restrict__ inc_ptr,
-    const int32_t* __restrict__ inc_elem, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
-    const uint8_t* __restrict__ dmask, const int32_t* __restrict__ diag, int64_t n, int span_cap,
-    const double* __restrict__ param, int mode, double scale, double f, const double* __restrict__ g,
-    double* __restrict__ vals, double* __restrict__ b, int* __restrict__ err) {
-  constexpr int NV = Cell<ND>::NV;
-  extern __shared__ __align__(16) unsigned char asm_smem[];
-  double* sv = reinterpret_cast<double*>(asm_smem);
-  int32_t* sc = reinterpret_cast<int32_t*>(sv + span_cap);
+__global__ void __launch_bounds__(kThreads) k_assemble_stream(
+    const int64_t* __restrict__ aptr, const int32_t* __restrict__ ae, const double* __restrict__ ak,
+    const uint8_t* __restrict__ apos, int64_t alen, const double* __restrict__ aload,
+    const int32_t* __restrict__ cells, const int32_t* __restrict__ indptr, const uint8_t* __restrict__ dmask,
+    const int32_t* __restrict__ diag, int64_t n, int64_t ntet, int64_t nnz, const double* __restrict__ param,
+    int mode, double scale, double f, const double* __restrict__ g, double* __restrict__ vals,
+    double* __restrict__ b, int* __restrict__ err) {
+  constexpr int PB = (ND + 3) / 4 * 4;
+  extern __shared__ __align__(16) double asm_sv[];
   const int64_t r0 = (int64_t)blockIdx.x * blockDim.x;
   const int64_t r1 = r0 + blockDim.x < n ? r0 + blockDim.x : n;
   const int32_t base = VALS ? __ldg(indptr + r0) : 0;
   const int32_t span = VALS ? __ldg(indptr + r1) - base : 0;
   if (VALS) {
-    for (int32_t k = threadIdx.x; k < span; k += blockDim.x) {
-      sv[k] = 0.0;
-      sc[k] = __ldg(indices + base + k);
-    }
+    for (int32_t k = threadIdx.x; k < span; k += blockDim.x) asm_sv[k] = 0.0;
     __syncthreads();
   }
   const int64_t row = r0 + threadIdx.x;
   if (row < r1) {
-    const int32_t lo = VALS ? __ldg(indptr + row) - base : 0;
-    const int32_t len = VALS ? __ldg(indptr + row + 1) - base - lo : 0;
     if (__ldg(dmask + row)) {
-      if (VALS) sv[__ldg(diag + row) - base] = 1.0;
+      if (VALS) {
+        const int32_t d = __ldg(diag + row) - base;
+        if (FEMK_IN_BOUNDS(d, span, err)) asm_sv[d] = 1.0;
+      }
       b[row] = g ? __ldg(g + row) : 0.0;
     } else {
-      double bi = 0.0;
-      const int32_t j1 = __ldg(inc_ptr + row + 1);
-      for (int32_t j = __ldg(inc_ptr + row); j < j1; ++j) {
-        const int64_t e = __ldg(inc_elem + j);
-        int32_t dof[ND];
+      const int32_t lo = VALS ? __ldg(indptr + row) - base : 0;
+      double bi = f * __ldg(aload + row);
+      const int64_t sl = row >> 5;
+      const int64_t a0 = __ldg(aptr + sl) + (row & 31);
+      const int64_t w = (__ldg(aptr + sl + 1) - __ldg(aptr + sl)) >> 5;
+      for (int64_t k = 0; k < w; ++k) {
+        const int64_t at = a0 + 32 * k;
+        const int32_t e = __ldcs(ae + at);
+        if (e < 0 || !FEMK_IN_BOUNDS(e, ntet, err)) continue;  // padding past this row's elements
+        const double kk = coef_of(param, mode, scale, e);
+        uint8_t pos[PB];
 #pragma unroll
-        for (int q = 0; q < ND; ++q) dof[q] = __ldg(cells + e * ND + q);
-        int a = 0;
+        for (int q = 0; q < PB / 4; ++q) {
+          const uint32_t word = __ldcs(reinterpret_cast<const uint32_t*>(apos + at * PB) + q);
 #pragma unroll
-        for (int q = 1; q < ND; ++q)
-          if (dof[q] == (int32_t)row) a = q;
-        Geom<NV> T;
-        cell_geometry(xyz, dof, T);
-        double VG[NV][NV];
-        gram(T, VG);
-        const double k = coef_of(param, mode, scale, e);
-        bi += add_row_at<ND, 0, VALS>(a, VG, T.vol, k, dof, dmask, g, f, sc + lo, len, sv + lo, err);
+          for (int c = 0; c < 4; ++c) pos[4 * q + c] = (uint8_t)(word >> (8 * c));
+        }
+#pragma unroll
+        for (int c = 0; c < ND; ++c) {
+          const double kac = kk * __ldcs(ak + c * alen + at);
+          if (pos[c] != 0xff) {
+            if (VALS && FEMK_IN_BOUNDS(lo + pos[c], span, err)) asm_sv[lo + pos[c]] += kac;
+          } else if (g) {
+            bi -= kac * __ldg(g + __ldg(cells + (int64_t)e * ND + c));
+          }
+        }
       }
       b[row] = bi;
     }
   }
   if (VALS) {
     __syncthreads();
-    for (int32_t k = threadIdx.x; k < span; k += blockDim.x) vals[base + k] = sv[k];
+    for (int32_t k = threadIdx.x; k < span; k += blockDim.x)
+      if (FEMK_IN_BOUNDS(base + k, nnz, err)) vals[base + k] = asm_sv[k];
   }
 }
 
@@ -501,23 +462,23 @@ extern "C" int femk_assemble(const femk_plan* p, const double* param, int mode, 
   FEMK_TRY(resolve_coef(p, param, mode, s, &param, &mode));
   const int rows = p->asm_rows;
   const int grid = (int)((p->n + rows - 1) / rows);
-  const size_t smem = vals ? (size_t)p->asm_span * (sizeof(double) + sizeof(int32_t)) : 0;
-  int* err = p->dev_err;
+  const size_t smem = vals ? (size_t)p->asm_span * sizeof(double) : 0;
+  const int64_t alen = p->astr_len > 0 ? p->astr_len : 1;
   FEMK_BY_ND(p->nd, {
     if (vals) {
-      auto kern = k_assemble_rows<ND, true>;
+      auto kern = k_assemble_stream<ND, true>;
       FEMK_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      kern<<<::femk::counted_launch() + grid, rows, smem, s>>>(p->xyz, p->cells, p->inc_ptr, p->inc_elem, p->indptr,
-                                                               p->indices, p->dmask, p->diag, p->n, p->asm_span,
-                                                               param, mode, scale, f, g, vals, b, err);
+      kern<<<::femk::counted_launch() + grid, rows, smem, s>>>(
+          p->astr_ptr, p->astr_elem, p->astr_k, p->astr_pos, alen, p->astr_load, p->cells, p->indptr, p->dmask,
+          p->diag, p->n, p->ntet, p->nnz, param, mode, scale, f, g, vals, b, p->dev_err);
     } else {
-      k_assemble_rows<ND, false><<<::femk::counted_launch() + grid, rows, 0, s>>>(
-          p->xyz, p->cells, p->inc_ptr, p->inc_elem, p->indptr, p->indices, p->dmask, p->diag, p->n, 0, param, mode,
-          scale, f, g, nullptr, b, err);
+      k_assemble_stream<ND, false><<<::femk::counted_launch() + grid, rows, 0, s>>>(
+          p->astr_ptr, p->astr_elem, p->astr_k, p->astr_pos, alen, p->astr_load, p->cells, p->indptr, p->dmask,
+          p->diag, p->n, p->ntet, p->nnz, param, mode, scale, f, g, nullptr, b, p->dev_err);
     }
   });
   FEMK_CUDA_TRY(cudaGetLastError());
-  return FEMK_OK;
+  return check_bounds(p, s, "femk_assemble");
 }
 
 extern "C" int femk_assemble_vjp(const femk_plan* p, const double* param, int mode, double scale, const double* g,

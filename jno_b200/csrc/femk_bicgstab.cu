@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_sell(const int64_t* __restric
     if (row >= n) continue;
     const int64_t b0 = __ldg(sptr + sl);
     const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
-    epi(row, sell_row<double, IDX, GatherX<double>, 16>(vals + b0 + lane, cols + b0 + lane, w, (int32_t)row,
+    epi(row, sell_row<double, IDX, 16>(vals + b0 + lane, cols + b0 + lane, w, (int32_t)row,
                                                         GatherX<double>{x}));
   }
   finish<KIND, kThreads>(st, acc, partials);

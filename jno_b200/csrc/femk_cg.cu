@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(kThreads) k_csr(const int32_t* __restrict__ in
                                                  double* __restrict__ y, const double* __restrict__ b,
                                                  const double* __restrict__ dinv, double* __restrict__ z,
                                                  double* __restrict__ pout, double* __restrict__ partials, CgState* st,
-                                                 double tol2, double atol2) {
+                                                 double tol2, double atol2, int* __restrict__ err) {
   constexpr int NV = MODE == kPlain ? 1 : (MODE == kCgStep ? 1 : (MODE == kInit ? 3 : 2));
   if (MODE == kCgStep && blockIdx.x == 0 && threadIdx.x == 0) st->xpend = 0;  // the last x update is applied
   if (MODE == kCgStep && st->done) return;
@@ -58,7 +58,8 @@ __global__ void __launch_bounds__(kThreads) k_csr(const int32_t* __restrict__ in
   for (int64_t base = warp * RPW * U; base < n; base += nwarps * RPW * U) {
     double s[U];
     int64_t rows[U];
-    csr_rows<L, U, double, int32_t>(indptr, indices, vals, x, n, base, lane, s, rows);
+    csr_rows_g<L, U, double, int32_t>(indptr, indices, vals, checked(GatherX<double>{x}, n, err), n, base, lane, s,
+                                      rows);
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int64_t row = rows[u];
@@ -127,7 +128,7 @@ __global__ void __launch_bounds__(kThreads) k_sell(const int64_t* __restrict__ s
                                                   const double* __restrict__ b, const double* __restrict__ dinv,
                                                   double* __restrict__ z, double* __restrict__ pout,
                                                   double* __restrict__ partials, CgState* st, double tol2,
-                                                  double atol2) {
+                                                  double atol2, int* __restrict__ err) {
   constexpr int NV = MODE == kPlain ? 1 : (MODE == kCgStep ? 1 : (MODE == kInit ? 3 : 2));
   if (MODE == kCgStep && blockIdx.x == 0 && threadIdx.x == 0) st->xpend = 0;  // the last x update is applied
   if (MODE == kCgStep && st->done) return;
@@ -144,17 +145,17 @@ __global__ void __launch_bounds__(kThreads) k_sell(const int64_t* __restrict__ s
     const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
     double sv;
     if (H == 1)
-      sv = sell_row<double, IDX, GatherXL<double>, B, true>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row,
-                                                           GatherXL<double>{x, l2_evict_last()});
+      sv = sell_row<double, IDX, B, true>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row,
+                                          checked(GatherXL<double>{x, l2_evict_last()}, n, err));
     else if (H == 2)
-      sv = sell_row<double, IDX, GatherX<double>, B, true>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row,
-                                                          GatherX<double>{x});
+      sv = sell_row<double, IDX, B, true>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row,
+                                          checked(GatherX<double>{x}, n, err));
     else if (H == 4)
-      sv = sell_row<double, IDX, GatherXL<double>, B, false>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row,
-                                                            GatherXL<double>{x, l2_evict_last()});
+      sv = sell_row<double, IDX, B, false>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row,
+                                           checked(GatherXL<double>{x, l2_evict_last()}, n, err));
     else
-      sv = sell_row<double, IDX, GatherX<double>, B>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row,
-                                                    GatherX<double>{x});
+      sv = sell_row<double, IDX, B>(svals + b0 + lane, scols + b0 + lane, w, (int32_t)row,
+                                    checked(GatherX<double>{x}, n, err));
     if (MODE == kPlain) {
       y[row] = sv;
     } else if (MODE == kCgStep) {
@@ -231,7 +232,8 @@ __global__ void __launch_bounds__(WPB * 32) k_sell_bulk(const int64_t* __restric
   double acc[1] = {0.0};
   int* errp = MODE == kCgStep ? &st->status : err;
   const bool ok = sell_bulk_rows<double, IDX, WMAX, S>(
-      bulk_smem + wib * kWarpBytes, sptr, scols, svals, n, nslices, g, NW, GatherXL<double>{x, l2_evict_last()},
+      bulk_smem + wib * kWarpBytes, sptr, scols, svals, n, nslices, g, NW,
+      checked(GatherXL<double>{x, l2_evict_last()}, n, errp),
       [&](int64_t row, double sv) {
         y[row] = sv;
         if (MODE == kCgStep) acc[0] += __ldg(x + row) * sv;
@@ -255,11 +257,11 @@ __global__ void __launch_bounds__(WPB * 32) k_sell_bulk(const int64_t* __restric
 }
 
 template <typename T>
-__global__ void k_sell_gather(const int32_t* __restrict__ src, int64_t m, const double* __restrict__ vals,
-                              T* __restrict__ out) {
+__global__ void k_sell_gather(const int32_t* __restrict__ src, int64_t m, const double* __restrict__ vals, int64_t nnz,
+                              T* __restrict__ out, int* __restrict__ err) {
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
     const int32_t k = __ldcs(src + j);
-    out[j] = k >= 0 ? (T)__ldcs(vals + k) : T(0);
+    out[j] = (k >= 0 && FEMK_IN_BOUNDS(k, nnz, err)) ? (T)__ldcs(vals + k) : T(0);
   }
 }
 
@@ -643,10 +645,11 @@ __global__ void __launch_bounds__(kThreads) k_resid_from_ax(int64_t n, const dou
   st->bb = tot[1];
 }
 
-__global__ void k_jacobi(const int32_t* __restrict__ diag, const double* __restrict__ vals, int64_t n,
-                         double* __restrict__ inv) {
+__global__ void k_jacobi(const int32_t* __restrict__ diag, const double* __restrict__ vals, int64_t n, int64_t nnz,
+                         double* __restrict__ inv, int* __restrict__ err) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double d = vals[diag[i]];
+    const int32_t k = diag[i];
+    const double d = FEMK_IN_BOUNDS(k, nnz, err) ? vals[k] : 0.0;
     inv[i] = 1.0 / (fabs(d) > 1e-30 ? d : 1.0);
   }
 }
@@ -716,7 +719,8 @@ int launch_csr_p(const femk_plan* p, const double* vals, const double* x, double
     constexpr int L = decltype(Lc)::value, U = decltype(Uc)::value;
     const int grid = wave_grid(k_csr<L, U, MODE>, kThreads, p);
     k_csr<L, U, MODE><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(p->indptr, p->indices, vals, p->n, x, y, b,
-                                                                           dinv, z, pout, partials, st, tol2, atol2);
+                                                                           dinv, z, pout, partials, st, tol2, atol2,
+                                                                           st ? &st->status : p->dev_err);
   });
   if (!ok) {
     set_error("unsupported SpMV configuration");
@@ -797,6 +801,7 @@ int launch_op(const femk_plan* p, bool sell, const double* vals, const double* x
     return FEMK_OK;
   }
   // column offsets in 16 bits when the plan's bandwidth allows it (same values, 2 B less per entry)
+  int* err = st ? &st->status : p->dev_err;
   auto go = [&](auto Bc, auto cols) {
     constexpr int B = decltype(Bc)::value;
     using I = std::remove_const_t<std::remove_pointer_t<decltype(cols)>>;
@@ -804,19 +809,23 @@ int launch_op(const femk_plan* p, bool sell, const double* vals, const double* x
     if (hm == 1) {
       const int grid = wave_grid(k_sell<MODE, I, B, 1>, kThreads, p);
       k_sell<MODE, I, B, 1><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
-          p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+          p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2,
+          err);
     } else if (hm == 2) {
       const int grid = wave_grid(k_sell<MODE, I, B, 2>, kThreads, p);
       k_sell<MODE, I, B, 2><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
-          p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+          p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2,
+          err);
     } else if (hm == 4) {
       const int grid = wave_grid(k_sell<MODE, I, B, 4>, kThreads, p);
       k_sell<MODE, I, B, 4><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
-          p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+          p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2,
+          err);
     } else {
       const int grid = wave_grid(k_sell<MODE, I, B>, kThreads, p);
       k_sell<MODE, I, B><<<::femk::counted_launch() + grid, kThreads, 0, s>>>(
-          p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2);
+          p->sell_ptr, cols, p->sell_vals, p->n, p->n_slices, x, y, b, dinv, z, pout, p->partials, st, tol2, atol2,
+          err);
     }
   };
   const bool c16 = p->sell_c16 && p->sell64_c16;
@@ -838,7 +847,7 @@ int launch_op(const femk_plan* p, bool sell, const double* vals, const double* x
 int prepare_sell(femk_plan* p, const double* vals, cudaStream_t s) {
   if (!p->sell_vals) FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals, sizeof(double) * (p->sell_nnz + 1)));
   k_sell_gather<double><<<::femk::counted_launch() + p->n_sm * 8, 256, 0, s>>>(p->sell_src, p->sell_nnz, vals,
-                                                                              p->sell_vals);
+                                                                              p->nnz, p->sell_vals, p->dev_err);
   FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;
 }
@@ -954,6 +963,7 @@ int ensure_chunk_graph(femk_plan* p, const double* vals, double* x, const double
   int st = e == cudaSuccess ? enqueue_chunk(p, vals, x, dinv, sell, kChunk, p->cg_stream) : FEMK_ECUDA;
   const cudaError_t e2 = cudaStreamEndCapture(p->cg_stream, &g);
   set_capturing(false);
+  if (e == cudaSuccess && e2 == cudaSuccess && st == FEMK_OK) st = l2_persist_graph(p, g, p->work, work_bytes(p));
   if (e != cudaSuccess || e2 != cudaSuccess || st != FEMK_OK) {
     if (g) cudaGraphDestroy(g);
     set_error(std::string("femk_pcg: graph capture failed: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
@@ -1011,6 +1021,7 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
   cudaStream_t ws = p->cg_stream;
   FEMK_CUDA_TRY(cudaEventRecord(p->cg_ev[2], s));
   FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->cg_ev[2], 0));
+  FEMK_TRY(l2_persist_begin(p, ws, p->work, work_bytes(p)));
   // the sliced-ELL values buffer must exist before a graph that reads it is captured
   if (sell) FEMK_TRY(prepare_sell(p, vals, ws));
   if (graph) FEMK_TRY(ensure_chunk_graph(p, vals, x, dinv, sell));
@@ -1078,6 +1089,7 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
     ++chunk_id;
   }
   FEMK_CUDA_TRY(cudaStreamSynchronize(ws));
+  FEMK_TRY(l2_persist_end(p, ws));
   CgState fin{};
   FEMK_CUDA_TRY(cudaMemcpy(&fin, st, sizeof(CgState), cudaMemcpyDeviceToHost));
   if (iters_out) *iters_out = fin.iter;
@@ -1109,6 +1121,12 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
     set_error("femk_pcg: non-finite value in a CG reduction");
   } else if (status == FEMK_TIMEOUT) {
     set_error("femk_pcg: a bulk-copy wait of the CG-step SpMV gave up");
+  } else if (status == FEMK_EBOUNDS) {
+    set_error("femk_pcg: an index check inside a kernel failed (bounds-checked build)");
+  }
+  if (status == FEMK_OK || status == FEMK_NOT_CONVERGED) {
+    const int bc = check_bounds(p, s, "femk_pcg");  // the value gather and plain products of the solve
+    if (bc != FEMK_OK) return bc;
   }
   return status;
 }
@@ -1137,15 +1155,17 @@ using namespace femk;
 extern "C" int femk_jacobi(const femk_plan* p, const double* vals, double* inv, void* stream) {
   clear_error();
   FEMK_CHECK_ARG(p && vals && inv, "femk_jacobi: NULL argument");
-  k_jacobi<<<::femk::counted_launch() + blocks_for(p->n, 256, p->n_sm * 8), 256, 0, (cudaStream_t)stream>>>(p->diag, vals, p->n, inv);
+  k_jacobi<<<::femk::counted_launch() + blocks_for(p->n, 256, p->n_sm * 8), 256, 0, (cudaStream_t)stream>>>(
+      p->diag, vals, p->n, p->nnz, inv, p->dev_err);
   FEMK_CUDA_TRY(cudaGetLastError());
-  return FEMK_OK;
+  return check_bounds(p, (cudaStream_t)stream, "femk_jacobi");
 }
 
 extern "C" int femk_spmv(const femk_plan* p, const double* vals, const double* x, double* y, void* stream) {
   clear_error();
   FEMK_CHECK_ARG(p && vals && x && y, "femk_spmv: NULL argument");
-  return spmv_csr(p, vals, x, y, (cudaStream_t)stream);
+  FEMK_TRY(spmv_csr(p, vals, x, y, (cudaStream_t)stream));
+  return check_bounds(p, (cudaStream_t)stream, "femk_spmv");
 }
 
 extern "C" int femk_set_profiling(femk_plan* p, int on) {
@@ -1184,15 +1204,17 @@ extern "C" int femk_prepare_operator(const femk_plan* p, const double* vals, voi
   clear_error();
   FEMK_CHECK_ARG(p && vals, "femk_prepare_operator: NULL argument");
   FEMK_CHECK_ARG(p->sell_src, "femk_prepare_operator: the plan has no sliced-ELL layout");
-  return prepare_sell(const_cast<femk_plan*>(p), vals, (cudaStream_t)stream);
+  FEMK_TRY(prepare_sell(const_cast<femk_plan*>(p), vals, (cudaStream_t)stream));
+  return check_bounds(p, (cudaStream_t)stream, "femk_prepare_operator");
 }
 
 extern "C" int femk_spmv_prepared(const femk_plan* p, const double* x, double* y, void* stream) {
   clear_error();
   FEMK_CHECK_ARG(p && x && y, "femk_spmv_prepared: NULL argument");
   FEMK_CHECK_ARG(p->sell_vals, "femk_spmv_prepared: call femk_prepare_operator first");
-  return launch_op<kPlain>(p, true, nullptr, x, y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.0, 0.0,
-                           (cudaStream_t)stream);
+  FEMK_TRY(launch_op<kPlain>(p, true, nullptr, x, y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.0, 0.0,
+                             (cudaStream_t)stream));
+  return check_bounds(p, (cudaStream_t)stream, "femk_spmv_prepared");
 }
 
 extern "C" int femk_spmv_matfree(const femk_plan* p, const double* param, int mode, double scale, const double* x,

@@ -15,6 +15,43 @@ namespace femk {
 
 constexpr int kWork32Vectors = 7;  // FP32 vectors of the mixed solvers (plan->work32 holds this many)
 
+// Bounds-checked build (-DFEMK_BOUNDS_CHECK, jno_b200/libfemk_bounds.so): FEMK_IN_BOUNDS(i, n, err)
+// is false when i lies outside [0, n), after recording FEMK_EBOUNDS in *err; the caller then skips
+// the access, so a bad index becomes a returned status instead of a fault. In the normal build it is
+// the constant true and generates no code.
+#ifdef FEMK_BOUNDS_CHECK
+constexpr bool kBoundsCheck = true;
+__device__ __forceinline__ bool in_bounds(int64_t i, int64_t n, int* err) {
+  if (i >= 0 && i < n) return true;
+  if (err) atomicExch(err, FEMK_EBOUNDS);
+  return false;
+}
+#define FEMK_IN_BOUNDS(i, n, err) ::femk::in_bounds((int64_t)(i), (int64_t)(n), (err))
+#else
+constexpr bool kBoundsCheck = false;
+#define FEMK_IN_BOUNDS(i, n, err) true
+#endif
+
+// A gather functor with an index check in the bounds-checked build (the functor itself otherwise).
+template <typename G>
+struct Checked {
+  G g;
+  int64_t n;
+  int* err;
+  template <typename I>
+  __device__ __forceinline__ auto operator()(I j) const -> decltype(g(j)) {
+    if (!FEMK_IN_BOUNDS(j, n, err)) return decltype(g(j))(0);
+    return g(j);
+  }
+};
+template <typename G>
+__device__ __forceinline__ auto checked(G g, int64_t n, int* err) {
+  if constexpr (kBoundsCheck)
+    return Checked<G>{g, n, err};
+  else
+    return g;
+}
+
 void set_error(const std::string& msg);
 void clear_error();
 
@@ -123,6 +160,14 @@ struct femk_plan {
   int asm_rows = 128;           // rows per block of the row-gather assembly
   int64_t asm_span = 0;         // largest CSR span (entries) of asm_rows consecutive rows
   int* dev_err = nullptr;       // device error word of kernels whose index checks can only fail on a corrupt plan
+  // assembly stream (femk_plan.cu, build_assembly_stream): per (free row, incident element) pair in
+  // 32-row slices, the element, its unit-coefficient stiffness row (nd planes) and column positions
+  int64_t* astr_ptr = nullptr;  // i64[n_slices+1] first entry of each slice
+  int64_t astr_len = 0;         // entries (padding included)
+  int32_t* astr_elem = nullptr; // i32[astr_len] element, -1 = padding
+  double* astr_k = nullptr;     // f64[nd * astr_len] K_hat[a][c], plane c
+  uint8_t* astr_pos = nullptr;  // u8[astr_len * pb] column positions in the row (0xff: Dirichlet column), pb = nd rounded up to 4
+  double* astr_load = nullptr;  // f64[n] integral of the row's basis function (0 on Dirichlet rows)
   int spmv_L = 16, spmv_U = 2;  // SpMV lanes per row / rows in flight per lane group
   // sliced-ELL solver layout (SELL-32), built with the pattern
   int64_t n_slices = 0, sell_nnz = 0;
@@ -145,6 +190,9 @@ struct femk_plan {
   double mixed_delta2 = 0.0;     // reliable-update threshold of the mixed solvers (0: 1e-4)
   long long barrier_spin = 0;    // clock64 budget of each grid-barrier wait of the batched solvers
   int skip_arrival = -1;         // testing: block that skips its first grid-barrier arrival (-1: none)
+  int l2_persist = 0;            // solver workspace vectors kept resident in L2 (access-policy window)
+  size_t l2_persist_max = 0;     // cudaDevAttrMaxPersistingL2CacheSize of the plan's device
+  size_t l2_window_max = 0;      // cudaDevAttrMaxAccessPolicyWindowSize
   // solver workspace (allocated on first use)
   int64_t vstride = 0;          // solver vector stride: n rounded up to 64 (keeps every slot 512-byte aligned)
   double* work = nullptr;       // 5 slots of vstride doubles: r, z, p, q, p' (double-buffered direction)
@@ -216,11 +264,30 @@ inline int blocks_for(int64_t n, int threads, int cap = 1 << 30) {
   return (int)b;
 }
 
+// In the bounds-checked build: wait for `s`, read and clear the plan's device error word, and
+// return FEMK_EBOUNDS (message naming `what`) if a kernel recorded a failed index check. In the
+// normal build: FEMK_OK without touching the device.
+int check_bounds(const femk_plan* p, cudaStream_t s, const char* what);
+
+// L2 residency of a solver's hot vectors (plan option l2_persist). l2_window fills an access-policy
+// window over [base, base + bytes) with persisting hits (hit ratio = persisting capacity / window, at
+// most 1) and streaming misses; num_bytes == 0 when the option is off or the device has no
+// persisting L2. l2_persist_begin raises the context's persisting-L2 limit to what the window needs
+// (never lowers it) and sets the window on stream s; l2_persist_graph sets it on every kernel node of
+// a captured graph (before instantiation); l2_persist_end clears the stream's window and returns the
+// persisting lines to normal, so kernels after the solve see the whole L2 again.
+cudaAccessPolicyWindow l2_window(const femk_plan* p, const void* base, size_t bytes);
+int l2_persist_begin(const femk_plan* p, cudaStream_t s, const void* base, size_t bytes);
+int l2_persist_graph(const femk_plan* p, cudaGraph_t g, const void* base, size_t bytes);
+int l2_persist_end(const femk_plan* p, cudaStream_t s);
+
 // Exclusive scan of int64 values: out[0..n] with out[n] = total. Works in place only when
 // in != out is false-safe (it is not: pass distinct buffers).
 int scan_exclusive_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
 
 int ensure_workspace(femk_plan* p);
+// bytes of the FP64 CG workspace (5 vectors of vstride doubles)
+inline size_t work_bytes(const femk_plan* p) { return sizeof(double) * 5 * (size_t)p->vstride; }
 
 // Nodal P1 coefficient modes become a per-element coefficient (plan-owned f64[ntet], computed on
 // stream s) read as FEMK_COEF_LINEAR; other modes pass through unchanged.

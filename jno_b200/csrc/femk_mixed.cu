@@ -260,8 +260,8 @@ __global__ void __launch_bounds__(kThreads, 8) k_step32_sell(const int64_t* __re
     if (row >= n) continue;
     const int64_t b0 = __ldg(sptr + sl);
     const int32_t wd = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
-    epi(row, sell_row<float, IDX, GatherX<float>, 8>(vals + b0 + lane, cols + b0 + lane, wd, (int32_t)row,
-                                                     GatherX<float>{r}));
+    epi(row, sell_row<float, IDX, 8>(vals + b0 + lane, cols + b0 + lane, wd, (int32_t)row,
+                                     checked(GatherX<float>{r}, n, &st->status)));
   }
   double v[1] = {(double)epi.a}, tot[1];
   if (!reduce_finish<1>(v, partials, &st->ticket, tot)) return;
@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(WPB * 32) k_step32_bulk(const int64_t* __restr
   StepEpi epi{r, w, 0.f};
   const bool ok = sell_bulk_rows<float, int16_t, WMAX, S>(
       bulk_smem + wib * kWarpBytes, sptr, cols, vals, n, nslices, (int64_t)blockIdx.x * WPB + wib,
-      (int64_t)gridDim.x * WPB, GatherX<float>{r}, epi, &st->status, FEMK_TIMEOUT, cptr);
+      (int64_t)gridDim.x * WPB, checked(GatherX<float>{r}, n, &st->status), epi, &st->status, FEMK_TIMEOUT, cptr);
   if (!ok && (threadIdx.x & 31) == 0) st->done = 1;
   double v[1] = {(double)epi.a}, tot[1];
   if (!reduce_finish<1, WPB * 32>(v, partials, &st->ticket, tot)) return;
@@ -306,7 +306,8 @@ __global__ void __launch_bounds__(kThreads) k_step32(const int32_t* __restrict__
   for (int64_t base = warp * RPW * U; base < n; base += nwarps * RPW * U) {
     float sv[U];
     int64_t rows[U];
-    csr_rows<L, U, float, IDX>(indptr, cols, vals, r, n, base, lane, sv, rows);
+    csr_rows_g<L, U, float, IDX>(indptr, cols, vals, checked(GatherX<float>{r}, n, &st->status), n, base, lane, sv,
+                                 rows);
 #pragma unroll
     for (int k = 0; k < U; ++k)
       if (rows[k] < n && sub == 0) epi(rows[k], sv[k]);
@@ -597,6 +598,9 @@ int enqueue_mixed_chunk(const femk_plan* p, const double* vals, const double* b,
   return FEMK_OK;
 }
 
+// the FP32 workspace (r, w, p, s, e, S, D): the vectors every inner iteration reads and writes
+size_t work32_bytes(const femk_plan* p) { return sizeof(float) * kWork32Vectors * (size_t)p->vstride; }
+
 int ensure_mixed(femk_plan* p) {
   FEMK_TRY(ensure_workspace(p));
   if (!p->work32) FEMK_CUDA_TRY(cudaMalloc(&p->work32, sizeof(float) * kWork32Vectors * p->vstride));
@@ -631,6 +635,7 @@ int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double
   int st = e == cudaSuccess ? enqueue_mixed_chunk(p, vals, b, x, dinv, p->mx_stream) : FEMK_ECUDA;
   const cudaError_t e2 = cudaStreamEndCapture(p->mx_stream, &g);
   set_capturing(false);
+  if (e == cudaSuccess && e2 == cudaSuccess && st == FEMK_OK) st = l2_persist_graph(p, g, p->work32, work32_bytes(p));
   if (e != cudaSuccess || e2 != cudaSuccess || st != FEMK_OK) {
     if (g) cudaGraphDestroy(g);
     set_error(std::string("femk_pcg_mixed: graph capture failed: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
@@ -684,6 +689,7 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   cudaStream_t ws = p->mx_stream;
   FEMK_CUDA_TRY(cudaEventRecord(p->mx_ev[2], s));
   FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->mx_ev[2], 0));
+  FEMK_TRY(l2_persist_begin(p, ws, p->work32, work32_bytes(p)));
   if (p->cg_graph) FEMK_TRY(ensure_mixed_graph(p, vals, b, x, dinv64));
   else prime_mixed(p);
   const int g1 = p->n_sm * 8;
@@ -740,6 +746,7 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
     ++chunk;
   }
   FEMK_CUDA_TRY(cudaStreamSynchronize(ws));
+  FEMK_TRY(l2_persist_end(p, ws));
   MixedState fin{};
   FEMK_CUDA_TRY(cudaMemcpy(&fin, m.st, sizeof(MixedState), cudaMemcpyDeviceToHost));
   FEMK_CUDA_TRY(cudaEventRecord(p->mx_ev[2], ws));

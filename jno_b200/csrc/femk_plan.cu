@@ -587,6 +587,128 @@ int build_uniform_columns(femk_plan* p, cudaStream_t s) {
   return FEMK_OK;
 }
 
+// Assembly stream of the parametric assembly (femk_assemble): the geometry of a mesh does not change
+// between assemblies, only the coefficient does, so for every (row, incident element) pair the plan
+// keeps the row of the element's unit-coefficient stiffness matrix and the positions of the
+// element's columns in the CSR row, in a sliced layout: slice s holds rows 32s..32s+31, entry k of
+// row 32s + l at astr_ptr[s] + 32 k + l (width = the slice's largest incidence count; Dirichlet rows
+// count 0). Per entry: the element (-1 = padding), ND FP64 stiffness values in ND planes of
+// astr_len entries, and ND column positions (one byte each, 0xff for a Dirichlet column) padded to
+// a multiple of 4 bytes. The load of every free row (the integral of its basis function) is kept too.
+__global__ void k_astream_width(const int32_t* __restrict__ inc_ptr, const uint8_t* __restrict__ dmask, int64_t n,
+                                int64_t nslices, int64_t* __restrict__ len) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t sl = warp; sl < nslices; sl += nwarps) {
+    const int64_t row = sl * 32 + lane;
+    int w = (row < n && !dmask[row]) ? inc_ptr[row + 1] - inc_ptr[row] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) w = max(w, __shfl_xor_sync(0xffffffffu, w, o));
+    if (lane == 0) len[sl] = (int64_t)w * 32;
+  }
+}
+
+template <int ND>
+__global__ void k_astream_fill(const double* __restrict__ xyz, const int32_t* __restrict__ cells,
+                               const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc_elem,
+                               const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                               const uint8_t* __restrict__ dmask, int64_t n, int64_t nslices,
+                               const int64_t* __restrict__ aptr, int64_t alen, int32_t* __restrict__ ae,
+                               double* __restrict__ ak, uint8_t* __restrict__ apos, double* __restrict__ aload,
+                               int* __restrict__ err) {
+  constexpr int NV = Cell<ND>::NV, PB = (ND + 3) / 4 * 4;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nslices * 32;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t sl = t >> 5, row = t;
+    const int lane = (int)(t & 31);
+    const int64_t a0 = aptr[sl], w = (aptr[sl + 1] - a0) >> 5;
+    const bool free_row = row < n && !dmask[row];
+    const int32_t j0 = free_row ? inc_ptr[row] : 0;
+    const int32_t cnt = free_row ? inc_ptr[row + 1] - j0 : 0;
+    const int32_t lo = free_row ? indptr[row] : 0, len = free_row ? indptr[row + 1] - lo : 0;
+    double load = 0.0;
+    for (int64_t k = 0; k < w; ++k) {
+      const int64_t at = a0 + 32 * k + lane;
+      if (k >= cnt) {
+        ae[at] = -1;
+#pragma unroll
+        for (int c = 0; c < ND; ++c) ak[c * alen + at] = 0.0;
+#pragma unroll
+        for (int c = 0; c < PB; ++c) apos[at * PB + c] = 0xff;
+        continue;
+      }
+      const int32_t e = inc_elem[j0 + k];
+      int32_t dof[ND];
+#pragma unroll
+      for (int q = 0; q < ND; ++q) dof[q] = cells[(int64_t)e * ND + q];
+      int a = 0;
+#pragma unroll
+      for (int q = 1; q < ND; ++q)
+        if (dof[q] == (int32_t)row) a = q;
+      Geom<NV> T;
+      cell_geometry(xyz, dof, T);
+      double VG[NV][NV];
+      gram(T, VG);
+      ae[at] = e;
+#pragma unroll
+      for (int c = 0; c < ND; ++c) {
+        ak[c * alen + at] = khat<ND>(VG, a, c);
+        uint8_t pos = 0xff;
+        if (!dmask[dof[c]]) {
+          const int32_t q = find_col(indices, lo, lo + len, dof[c]) - lo;
+          if (q < len && indices[lo + q] == dof[c] && q < 0xff)
+            pos = (uint8_t)q;
+          else
+            atomicOr(err, 32);
+        }
+        apos[at * PB + c] = pos;
+      }
+#pragma unroll
+      for (int c = ND; c < PB; ++c) apos[at * PB + c] = 0xff;
+      load += fhat<ND>(T.vol, a);
+    }
+    if (row < n) aload[row] = load;
+  }
+}
+
+template <int ND>
+int build_assembly_stream(femk_plan* p, cudaStream_t s) {
+  constexpr int PB = (ND + 3) / 4 * 4;
+  const int64_t n = p->n, ns = (n + 31) / 32;
+  FEMK_CHECK_ARG(p->max_row < 0xff, "femk_plan_create: a CSR row has 255 or more entries");
+  Temp len;
+  FEMK_CUDA_TRY(cudaMalloc(&len.p, sizeof(int64_t) * (ns + 1)));
+  FEMK_TRY(dev_alloc(&p->astr_ptr, ns + 1, s));
+  const int sgrid = blocks_for(ns * 32, kThreads, p->n_sm * 64);
+  k_astream_width<<<::femk::counted_launch() + sgrid, kThreads, 0, s>>>(p->inc_ptr, p->dmask, n, ns,
+                                                                        (int64_t*)len.p);
+  FEMK_TRY(scan_exclusive_i64((const int64_t*)len.p, p->astr_ptr, ns, s));
+  FEMK_CUDA_TRY(cudaMemcpyAsync(&p->astr_len, p->astr_ptr + ns, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  FEMK_CUDA_TRY(cudaStreamSynchronize(s));
+  const int64_t m = p->astr_len > 0 ? p->astr_len : 1;
+  FEMK_TRY(dev_alloc(&p->astr_elem, m, s));
+  FEMK_TRY(dev_alloc(&p->astr_k, ND * m, s));
+  FEMK_TRY(dev_alloc(&p->astr_pos, PB * m, s));
+  FEMK_TRY(dev_alloc(&p->astr_load, n, s));
+  int* d_err = nullptr;
+  FEMK_CUDA_TRY(cudaMalloc(&d_err, sizeof(int)));
+  Temp eg;
+  eg.p = d_err;
+  FEMK_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), s));
+  k_astream_fill<ND><<<::femk::counted_launch() + sgrid, kThreads, 0, s>>>(
+      p->xyz, p->cells, p->inc_ptr, p->inc_elem, p->indptr, p->indices, p->dmask, n, ns, p->astr_ptr, m,
+      p->astr_elem, p->astr_k, p->astr_pos, p->astr_load, d_err);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  int h = 0;
+  FEMK_TRY(read_err(d_err, s, &h));
+  if (h) {
+    set_error("femk_plan_create: assembly stream: a column is missing from its CSR row (corrupt connectivity?)");
+    return FEMK_EBOUNDS;
+  }
+  return FEMK_OK;
+}
+
 int build_dirichlet(femk_plan* p, const uint8_t* user_mask, const int32_t* vptr, const int32_t* vinc, cudaStream_t s) {
   const int64_t n = p->n;
   FEMK_TRY(dev_alloc(&p->dmask, n, s));
@@ -696,6 +818,7 @@ int create_impl(femk_plan* p, const double* coords, const int32_t* tets, const u
   int st = FEMK_OK;
   FEMK_BY_ND(p->nd, st = build_pattern<ND>(p, d_err, &h_err, s));
   if (st == FEMK_OK) st = build_dirichlet(p, mask, vptr, vinc, s);
+  if (st == FEMK_OK) FEMK_BY_ND(p->nd, st = build_assembly_stream<ND>(p, s));
   if (vptr != p->inc_ptr) {
     cudaFree(vptr);
     cudaFree(vinc);
@@ -717,7 +840,8 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
                   p->work,     p->partials,  p->state,     p->work32,    p->vals32,    p->work64b,
                   p->sell_ptr, p->sell_src,  p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32,
                   p->bar,      p->batch_ws,  p->bicg_ws,   p->bicg_state, p->sell_cuptr, p->sell_cu,
-                  p->coef_tmp, p->theta_ws, p->cmp_ws, p->gm_ws, p->dev_err};
+                  p->coef_tmp, p->theta_ws, p->cmp_ws, p->gm_ws, p->dev_err, p->astr_ptr, p->astr_elem,
+                  p->astr_k, p->astr_pos, p->astr_load};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->state_host) cudaFreeHost(p->state_host);
@@ -760,6 +884,7 @@ extern "C" void femk_plan_options_default(femk_plan_options* o) {
   o->vec_blocks = 0;
   o->split_updates = 1;
   o->test_skip_arrival = -1;
+  o->l2_persist = 0;
   o->mixed_delta2 = 0.0;
   o->barrier_limit_ms = 0.0;
 }
@@ -784,6 +909,7 @@ int apply_options(femk_plan* p, const femk_plan_options& o) {
   FEMK_CHECK_ARG(o.sell_batch == 8 || o.sell_batch == 16, "femk_plan_create_ex: sell_batch must be 8 or 16");
   FEMK_CHECK_ARG(o.vec_blocks >= 0 && o.vec_blocks <= 8, "femk_plan_create_ex: vec_blocks must be in [0, 8]");
   FEMK_CHECK_ARG(o.test_skip_arrival >= -1, "femk_plan_create_ex: test_skip_arrival must be >= -1");
+  FEMK_CHECK_ARG((o.l2_persist | 1) == 1, "femk_plan_create_ex: l2_persist is 0 or 1");
   FEMK_CHECK_ARG(o.mixed_delta2 >= 0.0 && o.mixed_delta2 < 1.0, "femk_plan_create_ex: mixed_delta2 must be in [0, 1)");
   FEMK_CHECK_ARG(o.barrier_limit_ms >= 0.0 && o.barrier_limit_ms <= 60000.0,
                  "femk_plan_create_ex: barrier_limit_ms must be in [0, 60000]");
@@ -806,6 +932,12 @@ int apply_options(femk_plan* p, const femk_plan_options& o) {
   p->cg_split = o.split_updates;
   p->skip_arrival = o.test_skip_arrival;
   p->mixed_delta2 = o.mixed_delta2;
+  p->l2_persist = o.l2_persist;
+  int pmax = 0, wmax = 0;
+  cudaDeviceGetAttribute(&pmax, cudaDevAttrMaxPersistingL2CacheSize, p->device);
+  cudaDeviceGetAttribute(&wmax, cudaDevAttrMaxAccessPolicyWindowSize, p->device);
+  p->l2_persist_max = pmax > 0 ? (size_t)pmax : 0;
+  p->l2_window_max = wmax > 0 ? (size_t)wmax : 0;
   int khz = 0;
   cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, p->device);
   if (khz <= 0) khz = 2000000;

@@ -128,7 +128,7 @@ __device__ __forceinline__ int32_t sell_col(const int16_t* __restrict__ cb, int3
 
 // Row sum of one thread's row. vals/cols point at the row's first entry (slice base + lane);
 // entry k sits at offset 32k. Index arithmetic is 32-bit (n < 2^31 is checked at plan build).
-template <typename V, typename I, typename G, int B = 8, bool HINT = false>
+template <typename V, typename I, int B = 8, bool HINT = false, typename G>
 __device__ __forceinline__ V sell_row(const V* __restrict__ vb, const I* __restrict__ cb, int32_t w, int32_t row,
                                       const G& gx) {
   V acc = V(0);

@@ -30,6 +30,19 @@ def test_library_exports_every_declared_symbol():
     assert isinstance(lib.femk_last_error_string(), bytes)
 
 
+def test_bounds_checked_library_exports_the_same_symbols():
+    """libfemk_bounds.so (the -DFEMK_BOUNDS_CHECK build of the same sources) exports every declared
+    entry point and reports itself as bounds-checked; the product library reports 0."""
+    from jno_b200 import _build, _lib
+
+    assert os.path.exists(_build.LIB_BOUNDS), "build it with python -m jno_b200._build --bounds"
+    lib = ctypes.CDLL(_build.LIB_BOUNDS)
+    for name in _declared():
+        assert hasattr(lib, name), name
+    assert lib.femk_bounds_checked() == 1
+    assert _lib.load().femk_bounds_checked() == 0
+
+
 def test_null_arguments_are_rejected_without_a_gpu():
     from jno_b200 import _lib
 
