@@ -129,7 +129,7 @@ typedef struct femk_plan_options {
                              vectors evict-last; 3 vectors evict-last only; 4 as 1 with streaming matrix loads */
   int32_t ring64;         /* bulk-copy ring of the FP64 CG-step SpMV, 10 * stages + warps per block (14, 18,
                              24, 28, 38); -1 (default): 14, 28 for rows of at most 8 entries; 0: thread-per-row kernel */
-  int32_t ring32;         /* the same for the FP32 step of femk_pcg_mixed; -1 (default): 28 */
+  int32_t ring32;         /* the same for the FP32 step of femk_pcg_mixed; -1 (default): 14 */
   int32_t csr_lanes;      /* CSR SpMV lanes per row (4, 8, 16, 32); 0 (default): from the mean row length */
   int32_t csr_rows;       /* CSR rows in flight per lane group (1, 2, 4); 0 (default): with csr_lanes */
   int32_t sell_batch;     /* entries in flight per thread of the thread-per-row FP64 kernel: 8 or 16 (default) */
@@ -138,10 +138,6 @@ typedef struct femk_plan_options {
   int32_t test_skip_arrival; /* testing the bounded waits: the block with this index skips its first
                                 grid-barrier arrival in femk_pcg_batched*, so every other block waits out
                                 barrier_limit_ms and the call returns FEMK_TIMEOUT; -1 (default): none */
-  int32_t l2_persist;     /* 1: the CG and mixed loops keep their workspace vectors resident in L2 (an
-                             access-policy window with persisting hits over the solver workspace; the
-                             context's persisting-L2 limit is raised to what the window needs, never lowered,
-                             and the persisting lines are reset when the solve returns); 0 (default): off */
   double mixed_delta2;    /* reliable update of the mixed solvers once <r, r> fell by this factor; 0 (default): 1e-4 */
   double barrier_limit_ms; /* limit of each grid-barrier wait of femk_pcg_batched*, in milliseconds at the
                               maximum SM clock; 0 (default): 2000 */

@@ -6,11 +6,13 @@ file; ``--bounds`` builds ``libfemk_bounds.so`` from the same sources with ``-DF
 library path; streams created by PyTorch are plain driver streams and are accepted as ``void*``.
 """
 
+import fcntl
 import glob
 import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -33,29 +35,37 @@ def sources():
 
 
 def build(verbose=False, extra=(), bounds=False):
-    """Compile every source into LIB (or, with ``bounds``, the bounds-checked LIB_BOUNDS)."""
+    """Compile every source into LIB (or, with ``bounds``, the bounds-checked LIB_BOUNDS).
+
+    Sources compile in parallel; an object is rebuilt when it is older than its source, any
+    ``csrc/*.cuh`` or ``include/femk.h``. A lock on the object directory keeps two builds from
+    interleaving (an object written by an older build after a newer one would look up to date)."""
     nvcc = _nvcc()
     objdir = os.path.join(ROOT, "_build", "bounds") if bounds else os.path.join(ROOT, "_build")
     extra = tuple(extra) + (("-DFEMK_BOUNDS_CHECK",) if bounds else ())
     lib = LIB_BOUNDS if bounds else LIB
     os.makedirs(objdir, exist_ok=True)
-    objs = []
     inc = ["-I", os.path.join(ROOT, "include")]
-    for src in sources():
-        obj = os.path.join(objdir, os.path.basename(src).replace(".cu", ".o"))
-        deps = [src] + glob.glob(os.path.join(HERE, "csrc", "*.cuh")) + [os.path.join(ROOT, "include", "femk.h")]
-        if not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(d) for d in deps):
-            cmd = [nvcc, *ARCH, *FLAGS, *inc, *extra, "-c", src, "-o", obj]
+    with open(os.path.join(objdir, ".lock"), "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        jobs, objs = [], []
+        headers = glob.glob(os.path.join(HERE, "csrc", "*.cuh")) + [os.path.join(ROOT, "include", "femk.h")]
+        for src in sources():
+            obj = os.path.join(objdir, os.path.basename(src).replace(".cu", ".o"))
+            if not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(d) for d in [src] + headers):
+                jobs.append([nvcc, *ARCH, *FLAGS, *inc, *extra, "-c", src, "-o", obj])
+            objs.append(obj)
+
+        def run(cmd):
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
-        objs.append(obj)
-    tmp = lib + ".tmp"
-    cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-cudart", "static"]
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
-    os.replace(tmp, lib)
+
+        with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+            list(pool.map(run, jobs))
+        tmp = lib + ".tmp"
+        run([nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-cudart", "static"])
+        os.replace(tmp, lib)
     return lib
 
 

@@ -80,7 +80,6 @@ class PlanOptions(ctypes.Structure):
         ("vec_blocks", ctypes.c_int32),
         ("split_updates", ctypes.c_int32),
         ("test_skip_arrival", ctypes.c_int32),
-        ("l2_persist", ctypes.c_int32),
         ("mixed_delta2", ctypes.c_double),
         ("barrier_limit_ms", ctypes.c_double),
     ]

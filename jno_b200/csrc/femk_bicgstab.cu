@@ -469,7 +469,7 @@ extern "C" int femk_bicgstab(const femk_plan* pc, const double* vals, const doub
   FEMK_CHECK_ARG(pc && vals && b && x, "femk_bicgstab: plan, vals, b and x are required");
   FEMK_CHECK_ARG(tol >= 0.0 && atol >= 0.0, "femk_bicgstab: tol and atol must be >= 0");
   femk_plan* p = const_cast<femk_plan*>(pc);
-  FEMK_CHECK_ARG(p->use_sell && p->sell_src, "femk_bicgstab: the plan has no sliced-ELL operator");
+  FEMK_CHECK_ARG(p->use_sell && p->sell_cols, "femk_bicgstab: the plan has no sliced-ELL operator");
   FEMK_TRY(ensure_bicg(p));
   cudaStream_t cs = (cudaStream_t)stream;
   cudaStream_t ws = p->bicg_stream;
@@ -497,7 +497,7 @@ extern "C" int femk_theta_march(const femk_plan* pc, const double* step_vals, co
   FEMK_CHECK_ARG(pc && step_vals && rhs_vals && q && u, "femk_theta_march: plan, operators, q and u are required");
   FEMK_CHECK_ARG(nsteps >= 0 && tol >= 0.0 && maxiter >= 0, "femk_theta_march: nsteps, tol and maxiter must be >= 0");
   femk_plan* p = const_cast<femk_plan*>(pc);
-  FEMK_CHECK_ARG(p->use_sell && p->sell_src, "femk_theta_march: the plan has no sliced-ELL operator");
+  FEMK_CHECK_ARG(p->use_sell && p->sell_cols, "femk_theta_march: the plan has no sliced-ELL operator");
   FEMK_TRY(ensure_bicg(p));
   if (!p->theta_ws) FEMK_CUDA_TRY(cudaMalloc(&p->theta_ws, sizeof(double) * 3 * p->vstride));
   double* dinv = (double*)p->theta_ws;

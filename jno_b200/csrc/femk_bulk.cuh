@@ -82,16 +82,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return true;
 }
 
-// Warp-wide wait: lane 0 waits (bounded), then every lane observes the completed phase once (its
-// own acquire of the bulk-copy writes). Returns the same outcome in every lane.
-__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity) {
-  bool ok = true;
-  if ((threadIdx.x & 31) == 0) ok = mbar_wait(bar, parity);
-  ok = __shfl_sync(0xffffffffu, ok, 0);
-  if (ok) ok = mbar_try_wait(bar, parity);
-  return __all_sync(0xffffffffu, ok);
-}
-
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar, uint64_t pol) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
@@ -105,20 +95,44 @@ __device__ __forceinline__ void bulk_g2s_plain(void* dst, const void* src, uint3
                : "memory");
 }
 
-// Shared memory one warp needs: S stages of [32*WMAX values][32*WMAX columns] + S mbarriers + S widths.
+// Where the copies of one slice come from: values at vals + b0 (32 w entries), columns at cols + c0
+// (cn entries; cn < 32 w marks a shared-offset table).
+struct SliceDir {
+  int64_t b0, c0;
+  int32_t w, cn;
+};
+
+// Shared memory one warp needs: S mbarriers + S widths (128 B), a directory of the
+// warp's next kDir slices, then S stages of [32*WMAX values][32*WMAX columns].
 template <typename V, typename IDX, int WMAX, int S>
 struct BulkRing {
   static constexpr int kVal = 32 * WMAX * (int)sizeof(V);
   static constexpr int kCol = ((32 * WMAX * (int)sizeof(IDX)) + 127) / 128 * 128;
   static constexpr int kStage = kVal + kCol;
-  static constexpr int kHead = 128;  // S mbarriers (8 B) + S widths (4 B), padded
+  static constexpr int kDir = 16;
+  static constexpr int kHead = 128 + (kDir * (int)sizeof(SliceDir) + 127) / 128 * 128;
   static constexpr int kWarpBytes = kHead + S * kStage;
-  static_assert(S * 12 <= kHead, "ring header too small");
-  static_assert(kVal % 128 == 0, "stage alignment");
+  static_assert(S * 16 <= 128, "ring header too small");
+  static_assert(S < kDir, "the directory must cover the slices issued ahead");
+  static_assert(kVal % 128 == 0 && kHead % 128 == 0, "stage alignment");
 };
 
+// Bounded warp-wide wait for the phase with the given parity: every lane polls (one warp
+// instruction whether one lane or all poll) and so observes the completed phase itself, which is
+// what makes the bulk-copy writes visible to it. Returns the same outcome in every lane.
+__device__ __forceinline__ bool mbar_wait_all(uint64_t* bar, uint32_t parity) {
+  bool ok = mbar_try_wait(bar, parity);
+  if (!__all_sync(0xffffffffu, ok)) {
+    const long long t0 = clock64();
+    while (!(ok = mbar_try_wait_suspend(bar, parity)))
+      if (clock64() - t0 > kBulkSpinCycles) break;
+  }
+  return __all_sync(0xffffffffu, ok);
+}
+
 // Every slice of this warp (global warp g takes slices g, g + NW, ...): for each row,
-// epi(row, row_sum). Returns false if a wait timed out (and sets *err to errval).
+// epi(row, row_sum). Returns false if a wait timed out (and sets *err to errval). Rows and slices
+// fit in 32 bits (the plan's column indices are int32), so the loop runs on 32-bit indices.
 //
 // cptr == NULL: cols holds one column (or offset) per stored entry, like vals. cptr != NULL: cols is
 // the per-slice column table (int16 offsets): slice s's table starts at cptr[s] and holds either w
@@ -126,12 +140,14 @@ struct BulkRing {
 template <typename V, typename IDX, int WMAX, int S, typename G, typename Epi>
 __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64_t* __restrict__ sptr,
                                                const IDX* __restrict__ cols, const V* __restrict__ vals, int64_t n,
-                                               int64_t nslices, int64_t g, int64_t NW, const G& gx, Epi&& epi,
+                                               int64_t nslices64, int64_t g64, int64_t NW64, const G& gx, Epi&& epi,
                                                int* err, int errval, const int64_t* __restrict__ cptr = nullptr) {
   using R = BulkRing<V, IDX, WMAX, S>;
   const int lane = threadIdx.x & 31;
+  const int32_t nslices = (int32_t)nslices64, g = (int32_t)g64, NW = (int32_t)NW64;
   uint64_t* bar = reinterpret_cast<uint64_t*>(wsmem);
-  int32_t* wid = reinterpret_cast<int32_t*>(wsmem + 8 * S);  // slice width; negative: shared offsets
+  int32_t* wid = reinterpret_cast<int32_t*>(wsmem + 8 * S);  // slice width per stage; negative: shared offsets
+  SliceDir* dir = reinterpret_cast<SliceDir*>(wsmem + 128);
   unsigned char* stages = wsmem + R::kHead;
   uint64_t pol = 0;
   if (lane == 0) {
@@ -139,43 +155,57 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
     for (int s = 0; s < S; ++s) mbar_init(bar + s, 1);
     mbar_fence_init();
   }
-  __syncwarp();
-  // lane 0: stream slice `sl` into stage `s`
-  auto issue = [&](int64_t sl, int s) {
-    const int64_t b0 = __ldg(sptr + sl);
-    const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
-    int64_t c0 = b0, cn = 32 * (int64_t)w;
-    if (cptr) {
-      c0 = __ldg(cptr + sl);
-      cn = __ldg(cptr + sl + 1) - c0;
+  // All lanes: the directory entries of this warp's slices with ordinals [base, base + kDir) (the
+  // slice of ordinal j is g + j NW), one slice per lane, so the offsets of kDir slices cost one round
+  // trip instead of one dependent load per slice on lane 0's refill path.
+  int32_t dbase = 0;
+  auto fill_dir = [&](int32_t base) {
+    if (lane < R::kDir) {
+      const int32_t sl = g + (base + lane) * NW;
+      if (sl < nslices) {
+        const int64_t b0 = __ldg(sptr + sl);
+        const int32_t w = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
+        int64_t c0 = b0;
+        int32_t cn = 32 * w;
+        if (cptr) {
+          c0 = __ldg(cptr + sl);
+          cn = (int32_t)(__ldg(cptr + sl + 1) - c0);
+        }
+        dir[lane] = SliceDir{b0, c0, w, cn};
+      }
     }
-    wid[s] = cn == 32 * (int64_t)w ? w : -w;
-    const uint32_t vb = (uint32_t)(32 * w * (int)sizeof(V));
-    const uint32_t cb = (uint32_t)(cn * (int64_t)sizeof(IDX));
+    __syncwarp();
+  };
+  fill_dir(0);
+  // lane 0: stream the slice of ordinal j (in the directory) into stage `s`
+  auto issue = [&](int32_t j, int s) {
+    const SliceDir d = dir[j - dbase];
+    wid[s] = d.cn == 32 * d.w ? d.w : -d.w;
+    const uint32_t vb = (uint32_t)(32 * d.w * (int)sizeof(V));
+    const uint32_t cb = (uint32_t)(d.cn * (int)sizeof(IDX));
     unsigned char* st = stages + s * R::kStage;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(bar + s, vb + cb);  // with w == 0 this arrival alone completes the phase
-    if (w > 0) {
-      bulk_g2s(st, vals + b0, vb, bar + s, pol);
-      bulk_g2s(st + R::kVal, cols + c0, cb, bar + s, pol);
+    if (d.w > 0) {
+      bulk_g2s(st, vals + d.b0, vb, bar + s, pol);
+      bulk_g2s(st + R::kVal, cols + d.c0, cb, bar + s, pol);
     }
   };
-  int64_t issued = 0;  // slices issued so far (lane 0's count; slice i lives in stage i % S)
+  int32_t issued = 0;  // slices issued so far (lane 0's count; ordinal j lives in stage j % S)
   if (lane == 0)
     for (int s = 0; s < S; ++s) {
-      const int64_t sl = g + (int64_t)s * NW;
-      if (sl >= nslices) break;
-      issue(sl, s);
+      if (g + s * NW >= nslices) break;
+      issue(s, s);
       ++issued;
     }
   __syncwarp();
   bool ok = true;
-  int64_t i = 0;
-  for (int64_t sl = g; sl < nslices; sl += NW, ++i) {
-    const int s = (int)(i % S);
-    const uint32_t parity = (uint32_t)((i / S) & 1);
+  int32_t j = 0;
+  for (int32_t sl = g; sl < nslices; sl += NW, ++j) {
+    const int s = j % S;
+    const uint32_t parity = (uint32_t)((j / S) & 1);
     // warp-uniform outcome: a timed-out wait takes the whole warp out of the loop
-    if (!mbar_wait_warp(bar + s, parity)) {
+    if (!mbar_wait_all(bar + s, parity)) {
       ok = false;
       break;
     }
@@ -183,7 +213,7 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
     const int32_t w = ws < 0 ? -ws : ws;
     const V* sv = reinterpret_cast<const V*>(stages + s * R::kStage) + lane;
     const IDX* sc = reinterpret_cast<const IDX*>(stages + s * R::kStage + R::kVal);
-    const int64_t row = sl * 32 + lane;
+    const int32_t row = sl * 32 + lane;
     const bool live = row < n;  // rows past n in the last slice gather nothing
     V acc = V(0);
     // Row sum in k order. The common widths (WMAX, WMAX - 1) run without per-entry predicates, and
@@ -202,20 +232,20 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
         constexpr int NQ = (K + 7) / 8;
         int4 cq[NQ];
 #pragma unroll
-        for (int j = 0; j < NQ; ++j) cq[j] = reinterpret_cast<const int4*>(sc)[j];
+        for (int q = 0; q < NQ; ++q) cq[q] = reinterpret_cast<const int4*>(sc)[q];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
           const int4 q4 = cq[k / 8];
           const int w2 = (k % 8) / 2;
           const int32_t word = w2 == 0 ? q4.x : (w2 == 1 ? q4.y : (w2 == 2 ? q4.z : q4.w));
           const int32_t c = (k & 1) ? (word >> 16) : (int32_t)(int16_t)(word & 0xffff);
-          xg[k] = gx((int32_t)row + c);
+          xg[k] = gx(row + c);
         }
       } else {
 #pragma unroll
         for (int k = 0; k < K; ++k) {
           const IDX c = cb[U ? k : k * 32];
-          xg[k] = gx(sizeof(IDX) == 2 ? (int32_t)row + (int32_t)c : (int32_t)c);
+          xg[k] = gx(sizeof(IDX) == 2 ? row + (int32_t)c : (int32_t)c);
         }
       }
 #pragma unroll
@@ -237,7 +267,7 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
         for (int k = 0; k < WMAX; ++k) {
           if (k < w) {
             const IDX c = sc[k * cstride + clane];
-            xg[k] = gx(sizeof(IDX) == 2 ? (int32_t)row + (int32_t)c : (int32_t)c);
+            xg[k] = gx(sizeof(IDX) == 2 ? row + (int32_t)c : (int32_t)c);
           }
         }
 #pragma unroll
@@ -246,21 +276,25 @@ __device__ __forceinline__ bool sell_bulk_rows(unsigned char* wsmem, const int64
       }
     }
     __syncwarp();  // every lane is done with stage s before it is refilled
-    if (lane == 0) {
-      const int64_t nsl = g + (i + S) * NW;
-      if (nsl < nslices) {
-        issue(nsl, s);
+    const int32_t nj = j + S;  // next ordinal to issue (every smaller one is issued)
+    if (g + nj * NW < nslices) {
+      if (nj >= dbase + R::kDir) {  // warp-uniform: the directory moves on to [nj, nj + kDir)
+        dbase = nj;
+        fill_dir(dbase);
+      }
+      if (lane == 0) {
+        issue(nj, s);
         ++issued;
       }
     }
     __syncwarp();
-    if (live) epi(row, acc);
+    if (live) epi((int64_t)row, acc);
   }
   if (!ok) {
     if (lane == 0) {
       atomicExch(err, errval);
       // drain: wait (bounded) for every copy this warp still has in flight
-      for (int64_t j = i; j < issued; ++j) mbar_wait(bar + (int)(j % S), (uint32_t)((j / S) & 1));
+      for (int32_t q = j; q < issued; ++q) mbar_wait(bar + (q % S), (uint32_t)((q / S) & 1));
     }
     __syncwarp();
   }

@@ -257,11 +257,18 @@ __global__ void __launch_bounds__(WPB * 32) k_sell_bulk(const int64_t* __restric
 }
 
 template <typename T>
-__global__ void k_sell_gather(const int32_t* __restrict__ src, int64_t m, const double* __restrict__ vals, int64_t nnz,
-                              T* __restrict__ out, int* __restrict__ err) {
-  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t k = __ldcs(src + j);
-    out[j] = (k >= 0 && FEMK_IN_BOUNDS(k, nnz, err)) ? (T)__ldcs(vals + k) : T(0);
+__global__ void k_sell_gather(const int64_t* __restrict__ sptr, const int32_t* __restrict__ indptr, int64_t n,
+                              int64_t nslices, const double* __restrict__ vals, int64_t nnz, T* __restrict__ out,
+                              int* __restrict__ err) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nslices * 32; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t sl = t >> 5, row = t;
+    const int64_t b0 = sptr[sl] + (t & 31);
+    const int32_t w = (int32_t)((sptr[sl + 1] - sptr[sl]) >> 5);
+    const int32_t beg = row < n ? indptr[row] : 0;
+    const int32_t len = row < n ? indptr[row + 1] - beg : 0;
+#pragma unroll 4
+    for (int32_t k = 0; k < w; ++k)
+      out[b0 + 32 * k] = (k < len && FEMK_IN_BOUNDS(beg + k, nnz, err)) ? (T)__ldcs(vals + beg + k) : T(0);
   }
 }
 
@@ -510,39 +517,57 @@ __global__ void __launch_bounds__(kThreads) k_pupdate_x(int64_t n, double* __res
 }
 
 // ---------------------------------------------------------------------------------------------
-// matrix-free operator: y = A x, A the Dirichlet-eliminated stiffness, recomputed per element
+// matrix-free operator: y = A x, A the Dirichlet-eliminated stiffness, recomputed per element from
+// the vertex coordinates (thread per element, FP64 atomics into y). mcells is the connectivity with
+// each Dirichlet DOF d stored as -1 - d, so one load gives the DOF and its mask: a Dirichlet DOF
+// contributes x = 0 and receives nothing (its row is the identity, k_dirichlet_identity).
 // ---------------------------------------------------------------------------------------------
+// (P2 tetrahedra: 6 resident blocks per SM fit the product in 80 registers without spills)
 template <int ND>
-__global__ void __launch_bounds__(128) k_matfree(const double* __restrict__ xyz, const int32_t* __restrict__ cells,
-                                                 int64_t ntet, const uint8_t* __restrict__ dmask,
-                                                 const double* __restrict__ param, int mode, double scale,
+__global__ void __launch_bounds__(128, ND == 10 ? 6 : 8) k_matfree(const double* __restrict__ xyz,
+                                                                   const int32_t* __restrict__ mcells,
+                                                 int64_t ntet, const double* __restrict__ param, int mode, double scale,
                                                  const double* __restrict__ x, double* __restrict__ y,
                                                  const CgState* st) {
+  constexpr int NV = Cell<ND>::NV;
   if (st && st->done) return;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
     int32_t dof[ND];
     double xe[ND];
-    bool dir[ND];
 #pragma unroll
     for (int a = 0; a < ND; ++a) {
-      dof[a] = __ldg(cells + c * ND + a);
-      dir[a] = __ldg(dmask + dof[a]) != 0;
-      xe[a] = dir[a] ? 0.0 : __ldg(x + dof[a]);
+      dof[a] = __ldg(mcells + c * ND + a);
+      xe[a] = dof[a] >= 0 ? __ldg(x + dof[a]) : 0.0;
     }
-    Geom<Cell<ND>::NV> T;
-    cell_geometry(xyz, dof, T);
-    double VG[Cell<ND>::NV][Cell<ND>::NV];
+    int32_t v[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i] = dof[i] >= 0 ? dof[i] : -1 - dof[i];
+    Geom<NV> T;
+    cell_geometry(xyz, v, T);
+    double VG[NV][NV];
     gram(T, VG);
     const double k = coef_of(param, mode, scale, c);
+    double ye[ND];
+    khat_apply<ND>(VG, xe, ye);
 #pragma unroll
-    for (int a = 0; a < ND; ++a) {
-      if (dir[a]) continue;
-      double s = 0.0;
-#pragma unroll
-      for (int b = 0; b < ND; ++b) s += khat<ND>(VG, a, b) * xe[b];
-      atomicAdd(y + dof[a], k * s);
-    }
+    for (int a = 0; a < ND; ++a)
+      if (dof[a] >= 0) atomicAdd(y + dof[a], k * ye[a]);
   }
+}
+
+// the masked connectivity of the matrix-free operator
+__global__ void k_mask_cells(const int32_t* __restrict__ cells, int64_t len, const uint8_t* __restrict__ dmask,
+                             int32_t* __restrict__ mcells) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < len; t += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t d = cells[t];
+    mcells[t] = dmask[d] ? -1 - d : d;
+  }
+}
+
+// k_e = exp(param_e), once per matrix-free solve instead of once per element and product
+__global__ void k_exp_coef(const double* __restrict__ param, int64_t ntet, double* __restrict__ ke) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x)
+    ke[c] = exp(param[c]);
 }
 
 __global__ void k_dirichlet_identity(const int32_t* __restrict__ dlist, int64_t nd, const double* __restrict__ x,
@@ -846,8 +871,8 @@ int launch_op(const femk_plan* p, bool sell, const double* vals, const double* x
 
 int prepare_sell(femk_plan* p, const double* vals, cudaStream_t s) {
   if (!p->sell_vals) FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals, sizeof(double) * (p->sell_nnz + 1)));
-  k_sell_gather<double><<<::femk::counted_launch() + p->n_sm * 8, 256, 0, s>>>(p->sell_src, p->sell_nnz, vals,
-                                                                              p->nnz, p->sell_vals, p->dev_err);
+  k_sell_gather<double><<<::femk::counted_launch() + blocks_for(p->n_slices * 32, 256, p->n_sm * 16), 256, 0, s>>>(
+      p->sell_ptr, p->indptr, p->n, p->n_slices, vals, p->nnz, p->sell_vals, p->dev_err);
   FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;
 }
@@ -865,11 +890,24 @@ __global__ void k_zero(double* __restrict__ y, int64_t n, const CgState* st) {
 }
 
 // y = A x for the matrix-free operator; with st != NULL every launch is a no-op once st->done.
+// the masked connectivity, built on first use (the Dirichlet set of a plan is fixed)
+int ensure_mcells(const femk_plan* pc, cudaStream_t s) {
+  femk_plan* p = const_cast<femk_plan*>(pc);
+  if (p->mcells) return FEMK_OK;
+  const int64_t len = p->ntet * p->nd;
+  FEMK_CUDA_TRY(cudaMalloc(&p->mcells, sizeof(int32_t) * (len > 0 ? len : 1)));
+  k_mask_cells<<<::femk::counted_launch() + blocks_for(len, 256, p->n_sm * 16), 256, 0, s>>>(p->cells, len, p->dmask,
+                                                                                             p->mcells);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}
+
 int launch_matfree(const femk_plan* p, const MatFree& m, const double* x, double* y, cudaStream_t s,
                    const CgState* st = nullptr) {
+  FEMK_TRY(ensure_mcells(p, s));
   k_zero<<<::femk::counted_launch() + p->n_sm * 8, 256, 0, s>>>(y, p->n, st);
   const int grid = blocks_for(p->ntet, 128, p->n_sm * 16);
-  FEMK_BY_ND(p->nd, k_matfree<ND><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->cells, p->ntet, p->dmask, m.param, m.mode, m.scale, x, y, st));
+  FEMK_BY_ND(p->nd, k_matfree<ND><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->mcells, p->ntet, m.param, m.mode, m.scale, x, y, st));
   FEMK_CUDA_TRY(cudaGetLastError());
   if (p->n_dir > 0) {
     k_dirichlet_identity<<<::femk::counted_launch() + blocks_for(p->n_dir, 256, 65535), 256, 0, s>>>(p->dlist, p->n_dir, x, y, st);
@@ -963,7 +1001,6 @@ int ensure_chunk_graph(femk_plan* p, const double* vals, double* x, const double
   int st = e == cudaSuccess ? enqueue_chunk(p, vals, x, dinv, sell, kChunk, p->cg_stream) : FEMK_ECUDA;
   const cudaError_t e2 = cudaStreamEndCapture(p->cg_stream, &g);
   set_capturing(false);
-  if (e == cudaSuccess && e2 == cudaSuccess && st == FEMK_OK) st = l2_persist_graph(p, g, p->work, work_bytes(p));
   if (e != cudaSuccess || e2 != cudaSuccess || st != FEMK_OK) {
     if (g) cudaGraphDestroy(g);
     set_error(std::string("femk_pcg: graph capture failed: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
@@ -1015,13 +1052,12 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
   CgState* st = p->state;
   ProfData* pd = !mf ? (ProfData*)p->prof : nullptr;
   const bool graph = !mf && p->cg_graph && !pd;
-  const bool sell = !mf && p->use_sell && p->sell_src;
+  const bool sell = !mf && p->use_sell && p->sell_cols;
   // all solver work runs on the plan's stream, ordered after the caller's stream and before
   // whatever the caller enqueues next
   cudaStream_t ws = p->cg_stream;
   FEMK_CUDA_TRY(cudaEventRecord(p->cg_ev[2], s));
   FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->cg_ev[2], 0));
-  FEMK_TRY(l2_persist_begin(p, ws, p->work, work_bytes(p)));
   // the sliced-ELL values buffer must exist before a graph that reads it is captured
   if (sell) FEMK_TRY(prepare_sell(p, vals, ws));
   if (graph) FEMK_TRY(ensure_chunk_graph(p, vals, x, dinv, sell));
@@ -1089,7 +1125,6 @@ int pcg_run(const femk_plan* pc, const double* vals, const MatFree* mf, const do
     ++chunk_id;
   }
   FEMK_CUDA_TRY(cudaStreamSynchronize(ws));
-  FEMK_TRY(l2_persist_end(p, ws));
   CgState fin{};
   FEMK_CUDA_TRY(cudaMemcpy(&fin, st, sizeof(CgState), cudaMemcpyDeviceToHost));
   if (iters_out) *iters_out = fin.iter;
@@ -1203,7 +1238,7 @@ extern "C" int femk_get_profile(const femk_plan* p, double* step_ms, double* upd
 extern "C" int femk_prepare_operator(const femk_plan* p, const double* vals, void* stream) {
   clear_error();
   FEMK_CHECK_ARG(p && vals, "femk_prepare_operator: NULL argument");
-  FEMK_CHECK_ARG(p->sell_src, "femk_prepare_operator: the plan has no sliced-ELL layout");
+  FEMK_CHECK_ARG(p->sell_cols, "femk_prepare_operator: the plan has no sliced-ELL layout");
   FEMK_TRY(prepare_sell(const_cast<femk_plan*>(p), vals, (cudaStream_t)stream));
   return check_bounds(p, (cudaStream_t)stream, "femk_prepare_operator");
 }
@@ -1257,9 +1292,19 @@ extern "C" int femk_pcg_matfree(const femk_plan* p, const double* param, int mod
   clear_error();
   FEMK_CHECK_ARG(p && b && x, "femk_pcg_matfree: NULL argument");
   FEMK_CHECK_ARG(coef_mode_ok(p, mode, param), "femk_pcg_matfree: bad coefficient");
-  FEMK_TRY(resolve_coef(p, param, mode, (cudaStream_t)stream, &param, &mode));
+  cudaStream_t s = (cudaStream_t)stream;
+  FEMK_TRY(resolve_coef(p, param, mode, s, &param, &mode));
+  if (mode == FEMK_COEF_EXP) {  // every CG step applies the operator: exponentiate once
+    femk_plan* pm = const_cast<femk_plan*>(p);
+    if (!pm->mf_coef) FEMK_CUDA_TRY(cudaMalloc(&pm->mf_coef, sizeof(double) * (p->ntet > 0 ? p->ntet : 1)));
+    k_exp_coef<<<::femk::counted_launch() + blocks_for(p->ntet, 256, p->n_sm * 16), 256, 0, s>>>(param, p->ntet,
+                                                                                               pm->mf_coef);
+    FEMK_CUDA_TRY(cudaGetLastError());
+    param = pm->mf_coef;
+    mode = FEMK_COEF_LINEAR;
+  }
   MatFree m{param, mode, scale};
-  return pcg_run(p, nullptr, &m, b, x, dinv, tol, atol, maxiter, iters_out, relres_out, (cudaStream_t)stream);
+  return pcg_run(p, nullptr, &m, b, x, dinv, tol, atol, maxiter, iters_out, relres_out, s);
 }
 
 // ---------------------------------------------------------------------------------------------

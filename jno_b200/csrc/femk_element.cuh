@@ -41,6 +41,15 @@ __host__ __device__ constexpr int cell_edge_b(int e) {
   return NV == 3 ? tri_edge_b(e) : edge_b(e);
 }
 
+// local index of the edge between vertices j != m (compile-time when j and m are)
+template <int NV>
+__host__ __device__ constexpr int cell_edge_of(int j, int m) {
+  for (int e = 0; e < (NV == 4 ? 6 : 3); ++e)
+    if ((cell_edge_a<NV>(e) == j && cell_edge_b<NV>(e) == m) || (cell_edge_a<NV>(e) == m && cell_edge_b<NV>(e) == j))
+      return e;
+  return -1;
+}
+
 template <int NV>
 struct Geom {
   double g[NV][NV - 1];  // barycentric gradients
@@ -182,6 +191,64 @@ __device__ __forceinline__ double khat(const double VG[Cell<ND>::NV][Cell<ND>::N
   const double cil = i == l ? ve_d : ve_o;
   const double cij = i == j ? ve_d : ve_o;
   return 4.0 * (VG[i][j] * cil + VG[i][l] * cij);
+}
+
+// ye = K_hat xe for one element (unit coefficient) without forming the ND x ND matrix.
+// P1: ye_a = sum_b VG[a][b] xe_b.
+// P2: u = sum_a xe_a phi_a has grad u = sum_j G_j g_j with G_j = du/dlambda_j affine in the
+// barycentric coordinates; using sum_l lambda_l = 1, G_j = sum_l H_jl lambda_l with H_jj = 3 x_j and
+// H_jl = 4 x_(jl) - x_j (x_j the vertex values, x_(jl) the value at the midpoint of edge (j, l)).
+// With int lambda_k lambda_l = V (1 + delta_kl) c, c = 1 / (NV (NV + 1)), and
+// dphi_a/dlambda_j = sum_k A^a_jk lambda_k:
+//   ye_a = c sum_jk A^a_jk Q_jk,  Q_jk = sum_m VG[j][m] (S_m + H_mk),  S_m = sum_l H_ml;
+//   vertex i (A^i_jk = delta_ij (4 delta_ik - 1)):        ye_i    = c (4 Q_ii - sum_k Q_ik);
+//   edge (i, m) (A_ik = 4 delta_mk, A_mk = 4 delta_ik):    ye_(im) = 4 c (Q_im + Q_mi).
+// About NV^3 + 4 NV^2 FP64 operations against ~ND^2 (the matrix) plus forming K_hat; the same
+// values as K_hat xe up to rounding.
+template <int ND>
+__device__ __forceinline__ void khat_apply(const double (&VG)[Cell<ND>::NV][Cell<ND>::NV], const double (&xe)[ND],
+                                           double (&ye)[ND]) {
+  constexpr int NV = Cell<ND>::NV;
+  if constexpr (!Cell<ND>::P2) {
+#pragma unroll
+    for (int a = 0; a < ND; ++a) {
+      double s = VG[a][0] * xe[0];
+#pragma unroll
+      for (int b = 1; b < ND; ++b) s = fma(VG[a][b], xe[b], s);
+      ye[a] = s;
+    }
+  } else {
+    constexpr double c = 1.0 / (NV * (NV + 1));
+    auto H = [&](int m, int k) { return m == k ? 3.0 * xe[m] : 4.0 * xe[NV + cell_edge_of<NV>(m, k)] - xe[m]; };
+    double S[NV];
+#pragma unroll
+    for (int m = 0; m < NV; ++m) {
+      double t = 0.0;
+#pragma unroll
+      for (int l = 0; l < NV; ++l) t += H(m, l);
+      S[m] = t;
+    }
+#pragma unroll
+    for (int a = 0; a < ND; ++a) ye[a] = 0.0;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      double Q[NV], qs = 0.0;
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        double q = 0.0;
+#pragma unroll
+        for (int m = 0; m < NV; ++m) q = fma(VG[j][m], S[m] + H(m, k), q);
+        Q[k] = q;
+        qs += q;
+      }
+      ye[j] = c * (4.0 * Q[j] - qs);
+#pragma unroll
+      for (int m = 0; m < NV; ++m)
+        if (m != j) ye[NV + cell_edge_of<NV>(j, m)] += Q[m];
+    }
+#pragma unroll
+    for (int e = 0; e < ND - NV; ++e) ye[NV + e] *= 4.0 * c;
+  }
 }
 
 // Unit-source load integral(phi_a): P1 V / (d+1); P2 vertex V (2 - d) / ((d+1)(d+2)), edge

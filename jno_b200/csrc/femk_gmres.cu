@@ -361,7 +361,7 @@ extern "C" int femk_gmres(const femk_plan* pc, const double* vals, const double*
   FEMK_CHECK_ARG(restart >= 1 && restart <= kGmMaxM, "femk_gmres: restart must be in [1, 64]");
   femk_plan* p = const_cast<femk_plan*>(pc);
   cudaStream_t s = (cudaStream_t)stream;
-  const bool sell = p->use_sell && p->sell_src;
+  const bool sell = p->use_sell && p->sell_cols;
   if (sell) FEMK_TRY(femk_prepare_operator(p, vals, s));
   GmresInfo info;
   const int64_t cap = maxiter >= 0 ? maxiter : 10 * p->n;  // negative: jax's default of 10 n restart cycles

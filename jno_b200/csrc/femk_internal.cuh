@@ -172,7 +172,6 @@ struct femk_plan {
   // sliced-ELL solver layout (SELL-32), built with the pattern
   int64_t n_slices = 0, sell_nnz = 0;
   int64_t* sell_ptr = nullptr;   // i64[n_slices+1] first entry of each slice
-  int32_t* sell_src = nullptr;   // i32[sell_nnz] CSR position of each entry, -1 = padding
   int32_t* sell_cols = nullptr;  // i32[sell_nnz]
   int16_t* sell_c16 = nullptr;   // i16[sell_nnz] col - row, when the bandwidth fits
   double* sell_vals = nullptr;   // f64[sell_nnz] values gathered for the current solve
@@ -190,9 +189,6 @@ struct femk_plan {
   double mixed_delta2 = 0.0;     // reliable-update threshold of the mixed solvers (0: 1e-4)
   long long barrier_spin = 0;    // clock64 budget of each grid-barrier wait of the batched solvers
   int skip_arrival = -1;         // testing: block that skips its first grid-barrier arrival (-1: none)
-  int l2_persist = 0;            // solver workspace vectors kept resident in L2 (access-policy window)
-  size_t l2_persist_max = 0;     // cudaDevAttrMaxPersistingL2CacheSize of the plan's device
-  size_t l2_window_max = 0;      // cudaDevAttrMaxAccessPolicyWindowSize
   // solver workspace (allocated on first use)
   int64_t vstride = 0;          // solver vector stride: n rounded up to 64 (keeps every slot 512-byte aligned)
   double* work = nullptr;       // 5 slots of vstride doubles: r, z, p, q, p' (double-buffered direction)
@@ -233,6 +229,8 @@ struct femk_plan {
   int batch_graph_ok = 1;
   void* prof = nullptr;         // per-kernel CG timing (femk_set_profiling)
   double* coef_tmp = nullptr;   // f64[ntet] element coefficients of a nodal parameter
+  double* mf_coef = nullptr;    // f64[ntet] exp(param) of a matrix-free solve
+  int32_t* mcells = nullptr;    // i32[ntet*nd] cells with each Dirichlet DOF d as -1 - d (matrix-free operator)
   double* theta_ws = nullptr;   // f64[3 vstride] theta march: step Jacobi inverse, step right-hand side, previous state
   double* gm_ws = nullptr;      // GMRES: Krylov basis (restart + 1 vectors), w, q, partials, small arrays
   int64_t gm_size = 0;          // doubles in gm_ws
@@ -269,25 +267,11 @@ inline int blocks_for(int64_t n, int threads, int cap = 1 << 30) {
 // normal build: FEMK_OK without touching the device.
 int check_bounds(const femk_plan* p, cudaStream_t s, const char* what);
 
-// L2 residency of a solver's hot vectors (plan option l2_persist). l2_window fills an access-policy
-// window over [base, base + bytes) with persisting hits (hit ratio = persisting capacity / window, at
-// most 1) and streaming misses; num_bytes == 0 when the option is off or the device has no
-// persisting L2. l2_persist_begin raises the context's persisting-L2 limit to what the window needs
-// (never lowers it) and sets the window on stream s; l2_persist_graph sets it on every kernel node of
-// a captured graph (before instantiation); l2_persist_end clears the stream's window and returns the
-// persisting lines to normal, so kernels after the solve see the whole L2 again.
-cudaAccessPolicyWindow l2_window(const femk_plan* p, const void* base, size_t bytes);
-int l2_persist_begin(const femk_plan* p, cudaStream_t s, const void* base, size_t bytes);
-int l2_persist_graph(const femk_plan* p, cudaGraph_t g, const void* base, size_t bytes);
-int l2_persist_end(const femk_plan* p, cudaStream_t s);
-
 // Exclusive scan of int64 values: out[0..n] with out[n] = total. Works in place only when
 // in != out is false-safe (it is not: pass distinct buffers).
 int scan_exclusive_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
 
 int ensure_workspace(femk_plan* p);
-// bytes of the FP64 CG workspace (5 vectors of vstride doubles)
-inline size_t work_bytes(const femk_plan* p) { return sizeof(double) * 5 * (size_t)p->vstride; }
 
 // Nodal P1 coefficient modes become a per-element coefficient (plan-owned f64[ntet], computed on
 // stream s) read as FEMK_COEF_LINEAR; other modes pass through unchanged.

@@ -129,33 +129,40 @@ __global__ void k_fill_f(float* __restrict__ v, int64_t n, float val) {
     v[i] = val;
 }
 
-// S = D^-1/2 from the Jacobi inverse (FP32) and D itself (FP32, for <r, D r>)
-__global__ void k_scaling(const double* __restrict__ dinv, int64_t n, float* __restrict__ sc, float* __restrict__ dd) {
+// S = D^-1/2 from the Jacobi inverse: FP32 (the fold x += S e) and FP64 (s64, forming A^); D itself
+// (FP32, for <r, D r>)
+__global__ void k_scaling(const double* __restrict__ dinv, int64_t n, float* __restrict__ sc, float* __restrict__ dd,
+                          double* __restrict__ s64) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double di = dinv[i];
-    sc[i] = (float)sqrt(di);
+    const double si = sqrt(di);
+    sc[i] = (float)si;
     dd[i] = (float)(1.0 / di);
+    s64[i] = si;
   }
 }
 
-// A^ = S A S into the FP32 sliced-ELL copy: thread per (slice, lane) row, entries in k order
+// A^ = S A S into the FP32 sliced-ELL copy: thread per (slice, lane) row, entry k of the row being
+// CSR position indptr[row] + k (padding past the row's length holds 0); each value is
+// (a_ij s_i) s_j in FP64, rounded once to FP32
 template <typename IDX>
-__global__ void k_gather_scaled(const int64_t* __restrict__ sptr, const int32_t* __restrict__ src,
+__global__ void k_gather_scaled(const int64_t* __restrict__ sptr, const int32_t* __restrict__ indptr,
                                 const IDX* __restrict__ cols, int64_t n, int64_t nslices, const double* __restrict__ vals,
-                                const double* __restrict__ dinv, float* __restrict__ out) {
+                                const double* __restrict__ s64, float* __restrict__ out) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nslices * 32; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t sl = t >> 5, row = t;
-    const int lane = (int)(t & 31);
-    const int64_t b0 = sptr[sl];
-    const int64_t w = (sptr[sl + 1] - b0) >> 5;
-    const double si = row < n ? sqrt(dinv[row]) : 0.0;
-    for (int64_t k = 0; k < w; ++k) {
-      const int64_t j = b0 + 32 * k + lane;
-      const int32_t at = __ldcs(src + j);
+    const int64_t b0 = sptr[sl] + (t & 31);
+    const int32_t w = (int32_t)((sptr[sl + 1] - sptr[sl]) >> 5);
+    const int32_t beg = row < n ? indptr[row] : 0;
+    const int32_t len = row < n ? indptr[row + 1] - beg : 0;
+    const double si = row < n ? s64[row] : 0.0;
+#pragma unroll 4
+    for (int32_t k = 0; k < w; ++k) {
+      const int64_t j = b0 + 32 * k;
       float v = 0.f;
-      if (at >= 0) {
-        const int64_t col = sizeof(IDX) == 2 ? row + (int64_t)cols[j] : (int64_t)cols[j];
-        v = (float)(__ldcs(vals + at) * si * sqrt(dinv[col]));
+      if (k < len) {
+        const int64_t col = sizeof(IDX) == 2 ? row + (int64_t)__ldcs(cols + j) : (int64_t)__ldcs(cols + j);
+        v = (float)(__ldcs(vals + beg + k) * si * s64[col]);
       }
       out[j] = v;
     }
@@ -164,10 +171,10 @@ __global__ void k_gather_scaled(const int64_t* __restrict__ sptr, const int32_t*
 
 // the same on the canonical CSR (plans without a sliced-ELL layout): thread per row
 __global__ void k_scale_csr(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices, int64_t n,
-                            const double* __restrict__ vals, const double* __restrict__ dinv, float* __restrict__ out) {
+                            const double* __restrict__ vals, const double* __restrict__ s64, float* __restrict__ out) {
   for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n; row += (int64_t)gridDim.x * blockDim.x) {
-    const double si = sqrt(dinv[row]);
-    for (int32_t k = indptr[row]; k < indptr[row + 1]; ++k) out[k] = (float)(vals[k] * si * sqrt(dinv[indices[k]]));
+    const double si = s64[row];
+    for (int32_t k = indptr[row]; k < indptr[row + 1]; ++k) out[k] = (float)(vals[k] * si * s64[indices[k]]);
   }
 }
 
@@ -598,13 +605,10 @@ int enqueue_mixed_chunk(const femk_plan* p, const double* vals, const double* b,
   return FEMK_OK;
 }
 
-// the FP32 workspace (r, w, p, s, e, S, D): the vectors every inner iteration reads and writes
-size_t work32_bytes(const femk_plan* p) { return sizeof(float) * kWork32Vectors * (size_t)p->vstride; }
-
 int ensure_mixed(femk_plan* p) {
   FEMK_TRY(ensure_workspace(p));
   if (!p->work32) FEMK_CUDA_TRY(cudaMalloc(&p->work32, sizeof(float) * kWork32Vectors * p->vstride));
-  if (p->use_sell && p->sell_src) {
+  if (p->use_sell && p->sell_cols) {
     if (!p->sell_vals32) FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals32, sizeof(float) * (p->sell_nnz + 1)));
   } else if (!p->vals32) {
     FEMK_CUDA_TRY(cudaMalloc(&p->vals32, sizeof(float) * (p->nnz + 1)));
@@ -635,7 +639,6 @@ int ensure_mixed_graph(femk_plan* p, const double* vals, const double* b, double
   int st = e == cudaSuccess ? enqueue_mixed_chunk(p, vals, b, x, dinv, p->mx_stream) : FEMK_ECUDA;
   const cudaError_t e2 = cudaStreamEndCapture(p->mx_stream, &g);
   set_capturing(false);
-  if (e == cudaSuccess && e2 == cudaSuccess && st == FEMK_OK) st = l2_persist_graph(p, g, p->work32, work32_bytes(p));
   if (e != cudaSuccess || e2 != cudaSuccess || st != FEMK_OK) {
     if (g) cudaGraphDestroy(g);
     set_error(std::string("femk_pcg_mixed: graph capture failed: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
@@ -689,20 +692,21 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   cudaStream_t ws = p->mx_stream;
   FEMK_CUDA_TRY(cudaEventRecord(p->mx_ev[2], s));
   FEMK_CUDA_TRY(cudaStreamWaitEvent(ws, p->mx_ev[2], 0));
-  FEMK_TRY(l2_persist_begin(p, ws, p->work32, work32_bytes(p)));
   if (p->cg_graph) FEMK_TRY(ensure_mixed_graph(p, vals, b, x, dinv64));
   else prime_mixed(p);
   const int g1 = p->n_sm * 8;
-  k_scaling<<<::femk::counted_launch() + g1, 256, 0, ws>>>(dinv64, n, m.sc, m.dd);
+  double* s64 = p->work;  // the FP64 CG workspace is free during a mixed solve
+  k_scaling<<<::femk::counted_launch() + g1, 256, 0, ws>>>(dinv64, n, m.sc, m.dd, s64);
   if (p->sell_vals32) {
+    const int gg = blocks_for(p->n_slices * 32, 256, p->n_sm * 16);
     if (p->sell_c16)
-      k_gather_scaled<int16_t><<<::femk::counted_launch() + g1, 256, 0, ws>>>(
-          p->sell_ptr, p->sell_src, p->sell_c16, n, p->n_slices, vals, dinv64, p->sell_vals32);
+      k_gather_scaled<int16_t><<<::femk::counted_launch() + gg, 256, 0, ws>>>(
+          p->sell_ptr, p->indptr, p->sell_c16, n, p->n_slices, vals, s64, p->sell_vals32);
     else
-      k_gather_scaled<int32_t><<<::femk::counted_launch() + g1, 256, 0, ws>>>(
-          p->sell_ptr, p->sell_src, p->sell_cols, n, p->n_slices, vals, dinv64, p->sell_vals32);
+      k_gather_scaled<int32_t><<<::femk::counted_launch() + gg, 256, 0, ws>>>(
+          p->sell_ptr, p->indptr, p->sell_cols, n, p->n_slices, vals, s64, p->sell_vals32);
   } else {
-    k_scale_csr<<<::femk::counted_launch() + g1, 256, 0, ws>>>(p->indptr, p->indices, n, vals, dinv64, p->vals32);
+    k_scale_csr<<<::femk::counted_launch() + g1, 256, 0, ws>>>(p->indptr, p->indices, n, vals, s64, p->vals32);
   }
   // e, p and s start at zero (beta = 0 multiplies p and s at the first step: 0 * NaN would stick)
   k_fill_f<<<::femk::counted_launch() + g1, 256, 0, ws>>>(m.e, n, 0.f);
@@ -746,7 +750,6 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
     ++chunk;
   }
   FEMK_CUDA_TRY(cudaStreamSynchronize(ws));
-  FEMK_TRY(l2_persist_end(p, ws));
   MixedState fin{};
   FEMK_CUDA_TRY(cudaMemcpy(&fin, m.st, sizeof(MixedState), cudaMemcpyDeviceToHost));
   FEMK_CUDA_TRY(cudaEventRecord(p->mx_ev[2], ws));

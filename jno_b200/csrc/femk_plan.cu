@@ -323,8 +323,8 @@ __global__ void k_sell_width(const int32_t* __restrict__ indptr, int64_t n, int6
 }
 
 __global__ void k_sell_fill(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices, int64_t n,
-                            int64_t nslices, const int64_t* __restrict__ sptr, int32_t* __restrict__ src,
-                            int32_t* __restrict__ cols, int16_t* __restrict__ c16) {
+                            int64_t nslices, const int64_t* __restrict__ sptr, int32_t* __restrict__ cols,
+                            int16_t* __restrict__ c16) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -338,7 +338,6 @@ __global__ void k_sell_fill(const int32_t* __restrict__ indptr, const int32_t* _
       const int64_t j = sptr[sl] + k * 32 + lane;
       const bool real = k < len;
       const int32_t col = real ? indices[beg + k] : (int32_t)self;
-      src[j] = real ? beg + (int32_t)k : -1;
       cols[j] = col;
       if (c16) c16[j] = (int16_t)(col - self);
     }
@@ -519,11 +518,10 @@ int build_pattern(femk_plan* p, int* d_err, int* h_err, cudaStream_t s) {
     p->use_sell = 0;
     return FEMK_OK;
   }
-  FEMK_TRY(dev_alloc(&p->sell_src, p->sell_nnz, s));
   FEMK_TRY(dev_alloc(&p->sell_cols, p->sell_nnz, s));
   if (p->cols16) FEMK_TRY(dev_alloc(&p->sell_c16, p->sell_nnz, s));
   k_sell_fill<<<::femk::counted_launch() + sgrid, kThreads, 0, s>>>(p->indptr, p->indices, n, p->n_slices, p->sell_ptr,
-                                                                    p->sell_src, p->sell_cols, p->sell_c16);
+                                                                    p->sell_cols, p->sell_c16);
   FEMK_CUDA_TRY(cudaGetLastError());
   FEMK_CUDA_TRY(cudaStreamSynchronize(s));
   return build_uniform_columns(p, s);
@@ -838,10 +836,10 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
   void* ptrs[] = {p->xyz,      p->points,    p->cells,     p->indptr,    p->indices,   p->slot,
                   p->diag,     p->dmask,     p->dlist,     p->inc_ptr,   p->inc_elem,  p->cols16,
                   p->work,     p->partials,  p->state,     p->work32,    p->vals32,    p->work64b,
-                  p->sell_ptr, p->sell_src,  p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32,
+                  p->sell_ptr, p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32,
                   p->bar,      p->batch_ws,  p->bicg_ws,   p->bicg_state, p->sell_cuptr, p->sell_cu,
                   p->coef_tmp, p->theta_ws, p->cmp_ws, p->gm_ws, p->dev_err, p->astr_ptr, p->astr_elem,
-                  p->astr_k, p->astr_pos, p->astr_load};
+                  p->astr_k, p->astr_pos, p->astr_load, p->mf_coef, p->mcells};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->state_host) cudaFreeHost(p->state_host);
@@ -884,7 +882,6 @@ extern "C" void femk_plan_options_default(femk_plan_options* o) {
   o->vec_blocks = 0;
   o->split_updates = 1;
   o->test_skip_arrival = -1;
-  o->l2_persist = 0;
   o->mixed_delta2 = 0.0;
   o->barrier_limit_ms = 0.0;
 }
@@ -909,7 +906,6 @@ int apply_options(femk_plan* p, const femk_plan_options& o) {
   FEMK_CHECK_ARG(o.sell_batch == 8 || o.sell_batch == 16, "femk_plan_create_ex: sell_batch must be 8 or 16");
   FEMK_CHECK_ARG(o.vec_blocks >= 0 && o.vec_blocks <= 8, "femk_plan_create_ex: vec_blocks must be in [0, 8]");
   FEMK_CHECK_ARG(o.test_skip_arrival >= -1, "femk_plan_create_ex: test_skip_arrival must be >= -1");
-  FEMK_CHECK_ARG((o.l2_persist | 1) == 1, "femk_plan_create_ex: l2_persist is 0 or 1");
   FEMK_CHECK_ARG(o.mixed_delta2 >= 0.0 && o.mixed_delta2 < 1.0, "femk_plan_create_ex: mixed_delta2 must be in [0, 1)");
   FEMK_CHECK_ARG(o.barrier_limit_ms >= 0.0 && o.barrier_limit_ms <= 60000.0,
                  "femk_plan_create_ex: barrier_limit_ms must be in [0, 60000]");
@@ -920,11 +916,12 @@ int apply_options(femk_plan* p, const femk_plan_options& o) {
   // measured on B200 (FP64 PCG to 1e-8): P1 128^3 48.7 ms with hints (mode 1) vs 52.0 ms without;
   // P2 64^3 117 ms without vs 168 ms with, so P2 plans stream without them
   p->l2_mode = o.l2_hints >= 0 ? o.l2_hints : (p->order == 1 ? 1 : 0);
-  // bulk-copy SpMV rings, measured on B200 at P1 128^3 (to 1e-8): FP64 1 stage x 4 warps (38.4 ms per
-  // step; 2 x 4: 43.2, 1 x 2: 40.4, thread-per-row: 45.8), FP32 2 stages x 8 warps (27.1 ms; 1 x 8:
-  // 27.2, 2 x 4: 29.5); rows of at most 8 entries (2-D P1) get 2 x 8 (set after the build)
+  // bulk-copy SpMV rings, measured on B200 at P1 128^3 (solves to 1e-8): FP64 1 stage x 4 warps
+  // (35.5 ms; 1 x 8: 35.0, 2 x 4: 43.4, 2 x 8: 38.2, thread-per-row: 44.0), FP32 1 stage x 4 warps
+  // (23.6 ms; 1 x 8: 23.6, 2 x 4: 24.4, 2 x 8: 24.7); rows of at most 8 entries (2-D P1) get 2 x 8
+  // (set after the build)
   p->bulk_cfg = o.ring64 >= 0 ? o.ring64 : 14;
-  p->bulk32_cfg = o.ring32 >= 0 ? o.ring32 : 28;
+  p->bulk32_cfg = o.ring32 >= 0 ? o.ring32 : 14;
   p->spmv_L = csr_auto ? 0 : o.csr_lanes;
   p->spmv_U = csr_auto ? 0 : o.csr_rows;
   p->sell_batch = o.sell_batch;
@@ -932,12 +929,6 @@ int apply_options(femk_plan* p, const femk_plan_options& o) {
   p->cg_split = o.split_updates;
   p->skip_arrival = o.test_skip_arrival;
   p->mixed_delta2 = o.mixed_delta2;
-  p->l2_persist = o.l2_persist;
-  int pmax = 0, wmax = 0;
-  cudaDeviceGetAttribute(&pmax, cudaDevAttrMaxPersistingL2CacheSize, p->device);
-  cudaDeviceGetAttribute(&wmax, cudaDevAttrMaxAccessPolicyWindowSize, p->device);
-  p->l2_persist_max = pmax > 0 ? (size_t)pmax : 0;
-  p->l2_window_max = wmax > 0 ? (size_t)wmax : 0;
   int khz = 0;
   cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, p->device);
   if (khz <= 0) khz = 2000000;
@@ -1022,9 +1013,9 @@ extern "C" int femk_plan_get_info(const femk_plan* p, femk_plan_info* out) {
   out->n_dirichlet = p->n_dir;
   out->cols16 = p->cols16 ? 1 : 0;
   out->device = p->device;
-  out->sell_nnz = p->sell_src ? p->sell_nnz : 0;
+  out->sell_nnz = p->sell_cols ? p->sell_nnz : 0;
   out->batch_graph = p->batch_graph_used;
-  out->sell_col_units = p->sell_cu ? p->sell_cu_len : (p->sell_src ? p->sell_nnz : 0);
+  out->sell_col_units = p->sell_cu ? p->sell_cu_len : (p->sell_cols ? p->sell_nnz : 0);
   out->dim = p->dim;
   return FEMK_OK;
 }

@@ -3,7 +3,6 @@
 #include <atomic>
 #include <mutex>
 #include <unordered_map>
-#include <vector>
 
 #include "femk_internal.cuh"
 #include "femk_spmv.cuh"
@@ -66,56 +65,6 @@ int check_bounds(const femk_plan* p, cudaStream_t s, const char* what) {
   FEMK_CUDA_TRY(cudaMemsetAsync(p->dev_err, 0, sizeof(int), s));
   set_error(std::string(what) + ": an index check inside a kernel failed (bounds-checked build)");
   return FEMK_EBOUNDS;
-}
-
-cudaAccessPolicyWindow l2_window(const femk_plan* p, const void* base, size_t bytes) {
-  cudaAccessPolicyWindow w{};
-  if (!p->l2_persist || p->l2_persist_max == 0 || p->l2_window_max == 0 || !base || bytes == 0) return w;
-  w.base_ptr = const_cast<void*>(base);
-  w.num_bytes = std::min(bytes, p->l2_window_max);
-  w.hitRatio = (float)std::min(1.0, (double)p->l2_persist_max / (double)w.num_bytes);
-  w.hitProp = cudaAccessPropertyPersisting;
-  w.missProp = cudaAccessPropertyStreaming;
-  return w;
-}
-
-int l2_persist_begin(const femk_plan* p, cudaStream_t s, const void* base, size_t bytes) {
-  const cudaAccessPolicyWindow w = l2_window(p, base, bytes);
-  if (w.num_bytes == 0) return FEMK_OK;
-  size_t cur = 0;
-  FEMK_CUDA_TRY(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
-  const size_t want = std::min(w.num_bytes, p->l2_persist_max);
-  if (cur < want) FEMK_CUDA_TRY(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want));
-  cudaStreamAttrValue a{};
-  a.accessPolicyWindow = w;
-  FEMK_CUDA_TRY(cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &a));
-  return FEMK_OK;
-}
-
-int l2_persist_graph(const femk_plan* p, cudaGraph_t g, const void* base, size_t bytes) {
-  const cudaAccessPolicyWindow w = l2_window(p, base, bytes);
-  if (w.num_bytes == 0) return FEMK_OK;
-  size_t nn = 0;
-  FEMK_CUDA_TRY(cudaGraphGetNodes(g, nullptr, &nn));
-  std::vector<cudaGraphNode_t> nodes(nn);
-  if (nn) FEMK_CUDA_TRY(cudaGraphGetNodes(g, nodes.data(), &nn));
-  cudaKernelNodeAttrValue a{};
-  a.accessPolicyWindow = w;
-  for (cudaGraphNode_t nd : nodes) {
-    cudaGraphNodeType t;
-    FEMK_CUDA_TRY(cudaGraphNodeGetType(nd, &t));
-    if (t == cudaGraphNodeTypeKernel)
-      FEMK_CUDA_TRY(cudaGraphKernelNodeSetAttribute(nd, cudaKernelNodeAttributeAccessPolicyWindow, &a));
-  }
-  return FEMK_OK;
-}
-
-int l2_persist_end(const femk_plan* p, cudaStream_t s) {
-  if (!p->l2_persist || p->l2_persist_max == 0 || p->l2_window_max == 0) return FEMK_OK;
-  cudaStreamAttrValue a{};
-  FEMK_CUDA_TRY(cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &a));
-  FEMK_CUDA_TRY(cudaCtxResetPersistingL2Cache());
-  return FEMK_OK;
 }
 
 namespace {
