@@ -258,18 +258,13 @@ __global__ void __launch_bounds__(WPB * 32) k_sell_bulk(const int64_t* __restric
 
 template <typename T>
 __global__ void k_sell_gather(const int64_t* __restrict__ sptr, const int32_t* __restrict__ indptr, int64_t n,
-                              int64_t nslices, const double* __restrict__ vals, int64_t nnz, T* __restrict__ out,
-                              int* __restrict__ err) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nslices * 32; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t sl = t >> 5, row = t;
-    const int64_t b0 = sptr[sl] + (t & 31);
-    const int32_t w = (int32_t)((sptr[sl + 1] - sptr[sl]) >> 5);
-    const int32_t beg = row < n ? indptr[row] : 0;
-    const int32_t len = row < n ? indptr[row + 1] - beg : 0;
-#pragma unroll 4
-    for (int32_t k = 0; k < w; ++k)
-      out[b0 + 32 * k] = (k < len && FEMK_IN_BOUNDS(beg + k, nnz, err)) ? (T)__ldcs(vals + beg + k) : T(0);
-  }
+                              int64_t nslices, const double* __restrict__ vals, int64_t nnz, int32_t cap,
+                              T* __restrict__ out, int* __restrict__ err) {
+  extern __shared__ double sg_buf[];
+  const int wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  sell_transpose_warp<T>(sg_buf + (int64_t)wib * cap, cap, sptr, indptr, n, nslices, vals, nnz, out,
+                         (int64_t)blockIdx.x * wpb + wib, (int64_t)gridDim.x * wpb,
+                         [](double v, int64_t, int64_t) { return (T)v; }, err);
 }
 
 // x += alpha p; r -= alpha q; z = D^-1 r; <r, z>, <r, r>; stop test; beta.
@@ -871,8 +866,11 @@ int launch_op(const femk_plan* p, bool sell, const double* vals, const double* x
 
 int prepare_sell(femk_plan* p, const double* vals, cudaStream_t s) {
   if (!p->sell_vals) FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals, sizeof(double) * (p->sell_nnz + 1)));
-  k_sell_gather<double><<<::femk::counted_launch() + blocks_for(p->n_slices * 32, 256, p->n_sm * 16), 256, 0, s>>>(
-      p->sell_ptr, p->indptr, p->n, p->n_slices, vals, p->nnz, p->sell_vals, p->dev_err);
+  const int32_t cap = 32 * (p->max_row > 0 ? p->max_row : 1);
+  const size_t smem = sizeof(double) * 4 * (size_t)cap;
+  FEMK_CUDA_TRY(cudaFuncSetAttribute(k_sell_gather<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_sell_gather<double><<<::femk::counted_launch() + blocks_for(p->n_slices, 4, p->n_sm * 16), 128, smem, s>>>(
+      p->sell_ptr, p->indptr, p->n, p->n_slices, vals, p->nnz, cap, p->sell_vals, p->dev_err);
   FEMK_CUDA_TRY(cudaGetLastError());
   return FEMK_OK;
 }

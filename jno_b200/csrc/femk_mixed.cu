@@ -23,8 +23,9 @@
 // 194 vs 193 on 3-D P1 48^3), and so does oracle.pcg.mixed_pcg.
 //
 // A reliable update is requested when <r, D r> fell below delta2 of the FP64 <r, r> at the previous
-// update, when the FP32 recurrence meets the stop test, or at the iteration cap. The iterations left
-// in the chunk then return at entry, and the chunk ends with
+// update, when the FP32 recurrence meets the stop test (both tested on odd steps, the ones that read
+// D), or at the iteration cap. The iterations left in the chunk then return at entry, and the chunk
+// ends with
 //     x += S e;  e = 0;  r64 = b - A64 x;  r^ = fp32(S r64);  <r^, r^>, <p, s>, <r^, s>   (k_fold, k_true_resid)
 //     K_B again on the replaced r^ (refresh): beta' = <r^, r^> / gamma (0 to restart)
 // which keeps the search direction (FEMK_MIXED_RELIABLE, residual replacement: p and s = A^ p are
@@ -50,6 +51,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kChunk = 16;
+static_assert(kChunk % 2 == 0, "steps alternate even / odd within a chunk");
 // K_A's block partials live past K_B's in the plan's partials buffer
 constexpr int64_t kPartialsA = 16384;
 
@@ -59,6 +61,7 @@ struct MixedState {
   double ps, rs;   // <p, s> and <r^, s> after a reliable update (the refresh step's products)
   double rr;       // FP32 recurrence <r, r> (unscaled: <r^, D r^>)
   double rr64, bb, atol2, alpha, beta, rr_since, delta2;
+  double alpha_pend;  // alpha of an even step whose e += alpha p is still owed (the next odd step or the fold pays it)
   int32_t iter, maxiter, done, status;
   int32_t need_update;  // 1: update requested this chunk; 2: update done, refresh step pending
   int32_t hold;         // inner iterations return at entry until the refresh step
@@ -148,25 +151,18 @@ __global__ void k_scaling(const double* __restrict__ dinv, int64_t n, float* __r
 template <typename IDX>
 __global__ void k_gather_scaled(const int64_t* __restrict__ sptr, const int32_t* __restrict__ indptr,
                                 const IDX* __restrict__ cols, int64_t n, int64_t nslices, const double* __restrict__ vals,
-                                const double* __restrict__ s64, float* __restrict__ out) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nslices * 32; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t sl = t >> 5, row = t;
-    const int64_t b0 = sptr[sl] + (t & 31);
-    const int32_t w = (int32_t)((sptr[sl + 1] - sptr[sl]) >> 5);
-    const int32_t beg = row < n ? indptr[row] : 0;
-    const int32_t len = row < n ? indptr[row + 1] - beg : 0;
-    const double si = row < n ? s64[row] : 0.0;
-#pragma unroll 4
-    for (int32_t k = 0; k < w; ++k) {
-      const int64_t j = b0 + 32 * k;
-      float v = 0.f;
-      if (k < len) {
+                                int64_t nnz, int32_t cap, const double* __restrict__ s64, float* __restrict__ out,
+                                int* __restrict__ err) {
+  extern __shared__ double sg_buf[];
+  const int wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  sell_transpose_warp<float>(
+      sg_buf + (int64_t)wib * cap, cap, sptr, indptr, n, nslices, vals, nnz, out, (int64_t)blockIdx.x * wpb + wib,
+      (int64_t)gridDim.x * wpb,
+      [&](double v, int64_t row, int64_t j) {
         const int64_t col = sizeof(IDX) == 2 ? row + (int64_t)__ldcs(cols + j) : (int64_t)__ldcs(cols + j);
-        v = (float)(__ldcs(vals + beg + k) * si * s64[col]);
-      }
-      out[j] = v;
-    }
-  }
+        return (float)(v * __ldg(s64 + row) * __ldg(s64 + col));
+      },
+      err);
 }
 
 // the same on the canonical CSR (plans without a sliced-ELL layout): thread per row
@@ -200,10 +196,12 @@ __device__ __forceinline__ bool step_skip(const MixedState* st, bool refresh) {
 }
 
 // Last block of K_B (all its threads): the new scalars from <r, w> and, for a normal step, K_A's
-// partials (<p, s>, <r, s>, <r, r>, <r, D r>); a refresh step takes them from the update.
+// partials (<p, s>, <r, s>, <r, r>, and on odd steps <r, D r>, which the stop and drop tests need:
+// they run on odd steps only); a refresh step takes them from the update. An even step leaves its
+// e += alpha p owed (alpha_pend), paid by the next odd K_A or by the fold.
 // (not inlined: it runs once per launch in one block, and inlined it adds registers to the row loop)
 template <bool REFRESH, int THREADS>
-__device__ __noinline__ void step_finish(MixedState* st, double rw, const double* pa, int ga) {
+__device__ __noinline__ void step_finish(MixedState* st, double rw, const double* pa, int ga, int odd) {
   double t[4];
   if (!REFRESH) sum_block_partials<4, THREADS>(pa, ga, t);
   if (threadIdx.x) return;
@@ -216,8 +214,9 @@ __device__ __noinline__ void step_finish(MixedState* st, double rw, const double
     ps = t[0];
     rs = t[1];
     gnew = t[2];
-    st->rr = t[3];
+    if (odd) st->rr = t[3];
     st->iter += 1;
+    st->alpha_pend = odd ? 0.0 : st->alpha;
   }
   if (!isfinite(rw) || !isfinite(ps) || !isfinite(rs) || !isfinite(gnew) || !isfinite(st->rr)) {
     st->status = FEMK_NONFINITE;
@@ -226,8 +225,8 @@ __device__ __noinline__ void step_finish(MixedState* st, double rw, const double
   }
   if (!REFRESH) {
     const double rho = t[3];
-    const bool conv = !(rho > st->atol2);
-    const bool drop = rho < st->delta2 * st->rr_since;
+    const bool conv = odd && !(rho > st->atol2);
+    const bool drop = odd && rho < st->delta2 * st->rr_since;
     if (conv || drop || st->iter >= st->maxiter) {  // fold e into x and replace r at the chunk end
       st->need_update = 1;
       st->hold = 1;
@@ -237,7 +236,12 @@ __device__ __noinline__ void step_finish(MixedState* st, double rw, const double
   const double beta = REFRESH ? refresh_beta(st) : gnew / st->gamma;
   const double den = rw + 2.0 * beta * rs + beta * beta * ps;  // <p', A^ p'>, p' = r + beta p
   if (!(den > 0.0)) {
-    st->status = FEMK_BREAKDOWN;
+    if (!REFRESH) {  // in exact arithmetic only r = 0 gets here (an untested even step): the FP64 residual decides
+      st->need_update = 1;
+      st->hold = 1;
+      return;
+    }
+    st->status = FEMK_BREAKDOWN;  // <p', A^ p'> <= 0 right after a residual replacement
     st->done = 1;
     return;
   }
@@ -256,7 +260,8 @@ template <typename IDX, bool REFRESH>
 __global__ void __launch_bounds__(kThreads, 8) k_step32_sell(const int64_t* __restrict__ sptr, const IDX* __restrict__ cols,
                                                          const float* __restrict__ vals, int64_t n, int64_t nslices,
                                                          const float* __restrict__ r, float* __restrict__ w,
-                                                         double* __restrict__ partials, int ga, MixedState* st) {
+                                                         double* __restrict__ partials, int ga, MixedState* st,
+                                                         int odd) {
   if (step_skip(st, REFRESH)) return;
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
@@ -272,7 +277,7 @@ __global__ void __launch_bounds__(kThreads, 8) k_step32_sell(const int64_t* __re
   }
   double v[1] = {(double)epi.a}, tot[1];
   if (!reduce_finish<1>(v, partials, &st->ticket, tot)) return;
-  step_finish<REFRESH, kThreads>(st, tot[0], partials + kPartialsA, ga);
+  step_finish<REFRESH, kThreads>(st, tot[0], partials + kPartialsA, ga, odd);
 }
 
 // K_B with the FP32 sliced-ELL stream moved into shared memory by bulk copies (femk_bulk.cuh):
@@ -283,7 +288,7 @@ __global__ void __launch_bounds__(WPB * 32) k_step32_bulk(const int64_t* __restr
                                                          const float* __restrict__ vals, int64_t n, int64_t nslices,
                                                          const float* __restrict__ r, float* __restrict__ w,
                                                          double* __restrict__ partials, int ga, MixedState* st,
-                                                         const int64_t* __restrict__ cptr) {
+                                                         const int64_t* __restrict__ cptr, int odd) {
   extern __shared__ __align__(128) unsigned char bulk_smem[];
   constexpr int kWarpBytes = BulkRing<float, int16_t, WMAX, S>::kWarpBytes;
   if (step_skip(st, REFRESH)) return;
@@ -295,7 +300,7 @@ __global__ void __launch_bounds__(WPB * 32) k_step32_bulk(const int64_t* __restr
   if (!ok && (threadIdx.x & 31) == 0) st->done = 1;
   double v[1] = {(double)epi.a}, tot[1];
   if (!reduce_finish<1, WPB * 32>(v, partials, &st->ticket, tot)) return;
-  step_finish<REFRESH, WPB * 32>(st, tot[0], partials + kPartialsA, ga);
+  step_finish<REFRESH, WPB * 32>(st, tot[0], partials + kPartialsA, ga, odd);
 }
 
 // K_B on the CSR copy (plans without a sliced-ELL layout)
@@ -303,7 +308,8 @@ template <int L, int U, typename IDX, bool REFRESH>
 __global__ void __launch_bounds__(kThreads) k_step32(const int32_t* __restrict__ indptr, const IDX* __restrict__ cols,
                                                     const float* __restrict__ vals, int64_t n,
                                                     const float* __restrict__ r, float* __restrict__ w,
-                                                    double* __restrict__ partials, int ga, MixedState* st) {
+                                                    double* __restrict__ partials, int ga, MixedState* st,
+                                                    int odd) {
   if (step_skip(st, REFRESH)) return;
   const int lane = threadIdx.x & 31, sub = lane % L;
   const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
@@ -321,30 +327,37 @@ __global__ void __launch_bounds__(kThreads) k_step32(const int32_t* __restrict__
   }
   double v[1] = {(double)epi.a}, tot[1];
   if (!reduce_finish<1>(v, partials, &st->ticket, tot)) return;
-  step_finish<REFRESH, kThreads>(st, tot[0], partials + kPartialsA, ga);
+  step_finish<REFRESH, kThreads>(st, tot[0], partials + kPartialsA, ga, odd);
 }
 
-// K_A: p = r + beta p; s = w + beta s; e += alpha p; r -= alpha s; block partials of <p, s>,
-// <r, s>, <r, r>, <r, D r> for the next K_B (no grid-wide wait here). All vectors are plan-owned
-// and 16-byte aligned: four rows per load.
-__device__ __forceinline__ void mx_one(float alpha, float beta, float w, float d, float& p, float& s, float& e,
-                                       float& r, float (&a)[4]) {
+// K_A: p = r + beta p; s = w + beta s; r -= alpha s; block partials of <p, s>, <r, s>, <r, r>
+// (+ <r, D r> on odd steps) for the next K_B (no grid-wide wait here). Steps alternate within a chunk
+// (16 steps, so a chunk starts on an even step): an even step owes its e += alpha p, and the next
+// odd step pays both at once from values it reads anyway,
+//     e += alpha' p' + alpha p = (alpha' + alpha beta) p' + alpha r    (p = r + beta p', r before the update),
+// so e moves every other step, and D (for the stop test's <r, D r>) only on odd steps. All vectors
+// are plan-owned and 16-byte aligned: four rows per load.
+template <bool ODD>
+__device__ __forceinline__ void mx_one(float alpha, float beta, float c1, float w, float d, float& p, float& s,
+                                       float& e, float& r, float (&a)[4]) {
+  if (ODD) e = fmaf(c1, p, fmaf(alpha, r, e));
   p = fmaf(beta, p, r);
   s = fmaf(beta, s, w);
-  e = fmaf(alpha, p, e);
   r = fmaf(-alpha, s, r);
   a[0] = fmaf(p, s, a[0]);
   a[1] = fmaf(r, s, a[1]);
   a[2] = fmaf(r, r, a[2]);
-  a[3] = fmaf(r * r, d, a[3]);
+  if (ODD) a[3] = fmaf(r * r, d, a[3]);
 }
 
+template <bool ODD>
 __global__ void __launch_bounds__(kThreads) k_mixed_update(int64_t n, const float* __restrict__ w, float* __restrict__ p,
                                                           float* __restrict__ s, float* __restrict__ e,
                                                           float* __restrict__ r, const float* __restrict__ dd,
                                                           double* __restrict__ pa, const MixedState* st) {
   if (st->done || st->hold) return;
   const float alpha = (float)st->alpha, beta = (float)st->beta;
+  const float c1 = (float)(st->alpha_pend + st->alpha * st->beta);
   const int64_t tid = blockIdx.x * (int64_t)kThreads + threadIdx.x;
   const int64_t nt = (int64_t)gridDim.x * kThreads;
   const int64_t n4 = n >> 2;
@@ -356,18 +369,27 @@ __global__ void __launch_bounds__(kThreads) k_mixed_update(int64_t n, const floa
   const float4* d4 = reinterpret_cast<const float4*>(dd);
   float a[4] = {0.f, 0.f, 0.f, 0.f};
   for (int64_t i = tid; i < n4; i += nt) {
-    float4 pp = p4[i], ss = s4[i], ee = e4[i], rr = r4[i];
-    const float4 ww = w4[i], d = d4[i];
-    mx_one(alpha, beta, ww.x, d.x, pp.x, ss.x, ee.x, rr.x, a);
-    mx_one(alpha, beta, ww.y, d.y, pp.y, ss.y, ee.y, rr.y, a);
-    mx_one(alpha, beta, ww.z, d.z, pp.z, ss.z, ee.z, rr.z, a);
-    mx_one(alpha, beta, ww.w, d.w, pp.w, ss.w, ee.w, rr.w, a);
+    float4 pp = p4[i], ss = s4[i], rr = r4[i];
+    const float4 ww = w4[i];
+    float4 ee = make_float4(0.f, 0.f, 0.f, 0.f), d = ee;
+    if (ODD) {
+      ee = e4[i];
+      d = d4[i];
+    }
+    mx_one<ODD>(alpha, beta, c1, ww.x, d.x, pp.x, ss.x, ee.x, rr.x, a);
+    mx_one<ODD>(alpha, beta, c1, ww.y, d.y, pp.y, ss.y, ee.y, rr.y, a);
+    mx_one<ODD>(alpha, beta, c1, ww.z, d.z, pp.z, ss.z, ee.z, rr.z, a);
+    mx_one<ODD>(alpha, beta, c1, ww.w, d.w, pp.w, ss.w, ee.w, rr.w, a);
     p4[i] = pp;
     s4[i] = ss;
-    e4[i] = ee;
     r4[i] = rr;
+    if (ODD) e4[i] = ee;
   }
-  for (int64_t i = 4 * n4 + tid; i < n; i += nt) mx_one(alpha, beta, w[i], dd[i], p[i], s[i], e[i], r[i], a);
+  for (int64_t i = 4 * n4 + tid; i < n; i += nt) {
+    float ei = ODD ? e[i] : 0.f;
+    mx_one<ODD>(alpha, beta, c1, w[i], ODD ? dd[i] : 0.f, p[i], s[i], ei, r[i], a);
+    if (ODD) e[i] = ei;
+  }
   double v[4] = {(double)a[0], (double)a[1], (double)a[2], (double)a[3]};
   block_sum<4, kThreads>(v);
   if (threadIdx.x == 0) {
@@ -376,12 +398,14 @@ __global__ void __launch_bounds__(kThreads) k_mixed_update(int64_t n, const floa
   }
 }
 
-// x += S e; e = 0 (only at a requested update)
-__global__ void k_fold(int64_t n, double* __restrict__ x, float* __restrict__ e, const float* __restrict__ sc,
-                       const MixedState* st) {
+// x += S (e + alpha_pend p); e = 0 (only at a requested update; the owed term of an even last step
+// is paid here)
+__global__ void k_fold(int64_t n, double* __restrict__ x, float* __restrict__ e, const float* __restrict__ p,
+                       const float* __restrict__ sc, const MixedState* st) {
   if (st->done || st->need_update != 1) return;
+  const float ap = (float)st->alpha_pend;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    x[i] += (double)sc[i] * (double)e[i];
+    x[i] += (double)sc[i] * (double)fmaf(ap, p[i], e[i]);
     e[i] = 0.f;
   }
 }
@@ -429,6 +453,7 @@ __global__ void __launch_bounds__(kThreads) k_true_resid(const int32_t* __restri
   if (!reduce_finish<5>(a, partials, &st->ticket, tot)) return;
   if (threadIdx.x) return;
   st->outer += 1;
+  st->alpha_pend = 0.0;  // k_fold paid it
   st->rr64 = tot[1];
   st->rr_since = tot[1];
   st->rr = tot[1];
@@ -467,10 +492,11 @@ void launch_true_resid(const femk_plan* p, const double* vals, const double* x, 
 }
 
 // grid of K_A (fixed per plan: K_B's last block reads this many block partials)
-int update_grid(const femk_plan* p) { return vec_grid(k_mixed_update, kThreads, p); }
+int update_grid(const femk_plan* p) { return vec_grid(k_mixed_update<true>, kThreads, p); }
 
 template <int S, int WPB, int WMAX, bool REFRESH>
-bool launch_step32_bulk_cfg(const femk_plan* p, const float* r, float* w, MixedState* st, cudaStream_t s, bool prime) {
+bool launch_step32_bulk_cfg(const femk_plan* p, const float* r, float* w, MixedState* st, cudaStream_t s, bool prime,
+                            int odd) {
   auto kern = k_step32_bulk<WMAX, S, WPB, REFRESH>;
   constexpr int kSmem = WPB * BulkRing<float, int16_t, WMAX, S>::kWarpBytes;
   static int per_sm = -1;  // per instantiation: opt-in shared memory size + occupancy, queried once
@@ -487,7 +513,7 @@ bool launch_step32_bulk_cfg(const femk_plan* p, const float* r, float* w, MixedS
   const bool tab = p->sell_cu != nullptr;  // per-slice column tables (shared-offset slices stored once)
   kern<<<::femk::counted_launch() + grid, WPB * 32, kSmem, s>>>(
       (const int64_t*)p->sell_ptr, (const int16_t*)(tab ? p->sell_cu : p->sell_c16), (const float*)p->sell_vals32,
-      p->n, p->n_slices, r, w, p->partials, update_grid(p), st, (const int64_t*)(tab ? p->sell_cuptr : nullptr));
+      p->n, p->n_slices, r, w, p->partials, update_grid(p), st, (const int64_t*)(tab ? p->sell_cuptr : nullptr), odd);
   return true;
 }
 
@@ -495,7 +521,7 @@ bool launch_step32_bulk_cfg(const femk_plan* p, const float* r, float* w, MixedS
 // prime = true only sets the kernel attribute and reads the occupancy (before a graph capture)
 template <bool REFRESH>
 bool launch_step32_bulk(const femk_plan* p, const float* r, float* w, MixedState* st, cudaStream_t s,
-                        bool prime = false) {
+                        bool prime = false, int odd = 0) {
   if (!p->bulk32_cfg || !p->sell_vals32 || !p->sell_c16 || p->max_row > 32) return false;
   if (((uintptr_t)p->sell_vals32 & 15u) || ((uintptr_t)p->sell_c16 & 15u)) return false;
   if (p->sell_cu && ((uintptr_t)p->sell_cu & 15u)) return false;
@@ -503,9 +529,9 @@ bool launch_step32_bulk(const femk_plan* p, const float* r, float* w, MixedState
   const int wsel = p->max_row <= 8 ? 8 : (p->max_row <= 16 ? 16 : 32);
 #define FEMK_BULK_CFG(code, S, WPB)                                                             \
   case code:                                                                                    \
-    return wsel == 8    ? launch_step32_bulk_cfg<S, WPB, 8, REFRESH>(p, r, w, st, s, prime)  \
-           : wsel == 16 ? launch_step32_bulk_cfg<S, WPB, 16, REFRESH>(p, r, w, st, s, prime) \
-                        : launch_step32_bulk_cfg<S, WPB, 32, REFRESH>(p, r, w, st, s, prime);
+    return wsel == 8    ? launch_step32_bulk_cfg<S, WPB, 8, REFRESH>(p, r, w, st, s, prime, odd)  \
+           : wsel == 16 ? launch_step32_bulk_cfg<S, WPB, 16, REFRESH>(p, r, w, st, s, prime, odd) \
+                        : launch_step32_bulk_cfg<S, WPB, 32, REFRESH>(p, r, w, st, s, prime, odd);
   switch (p->bulk32_cfg) {
     FEMK_BULK_CFG(14, 1, 4)
     FEMK_BULK_CFG(18, 1, 8)
@@ -518,19 +544,20 @@ bool launch_step32_bulk(const femk_plan* p, const float* r, float* w, MixedState
 #undef FEMK_BULK_CFG
 }
 
+// K_B in the plan's layout; odd: the parity of the step (normal steps; 0 for a refresh)
 template <bool REFRESH>
-void launch_step32(const femk_plan* p, const float* r, float* w, MixedState* st, cudaStream_t s) {
-  if (launch_step32_bulk<REFRESH>(p, r, w, st, s)) return;
+void launch_step32(const femk_plan* p, const float* r, float* w, MixedState* st, cudaStream_t s, int odd = 0) {
+  if (launch_step32_bulk<REFRESH>(p, r, w, st, s, false, odd)) return;
   const int ga = update_grid(p);
   if (p->sell_vals32) {
     if (p->sell_c16) {
       auto k = k_step32_sell<int16_t, REFRESH>;
       k<<<::femk::counted_launch() + wave_grid(k, kThreads, p), kThreads, 0, s>>>(
-          p->sell_ptr, p->sell_c16, p->sell_vals32, p->n, p->n_slices, r, w, p->partials, ga, st);
+          p->sell_ptr, p->sell_c16, p->sell_vals32, p->n, p->n_slices, r, w, p->partials, ga, st, odd);
     } else {
       auto k = k_step32_sell<int32_t, REFRESH>;
       k<<<::femk::counted_launch() + wave_grid(k, kThreads, p), kThreads, 0, s>>>(
-          p->sell_ptr, p->sell_cols, p->sell_vals32, p->n, p->n_slices, r, w, p->partials, ga, st);
+          p->sell_ptr, p->sell_cols, p->sell_vals32, p->n, p->n_slices, r, w, p->partials, ga, st, odd);
     }
     return;
   }
@@ -539,11 +566,11 @@ void launch_step32(const femk_plan* p, const float* r, float* w, MixedState* st,
     if (p->cols16) {
       auto k = k_step32<L, U, int16_t, REFRESH>;
       k<<<::femk::counted_launch() + wave_grid(k, kThreads, p), kThreads, 0, s>>>(p->indptr, p->cols16, p->vals32,
-                                                                                  p->n, r, w, p->partials, ga, st);
+                                                                                  p->n, r, w, p->partials, ga, st, odd);
     } else {
       auto k = k_step32<L, U, int32_t, REFRESH>;
       k<<<::femk::counted_launch() + wave_grid(k, kThreads, p), kThreads, 0, s>>>(p->indptr, p->indices, p->vals32,
-                                                                                  p->n, r, w, p->partials, ga, st);
+                                                                                  p->n, r, w, p->partials, ga, st, odd);
     }
   });
 }
@@ -594,11 +621,13 @@ int enqueue_mixed_chunk(const femk_plan* p, const double* vals, const double* b,
   const int64_t n = p->n;
   const int ga = update_grid(p);
   for (int it = 0; it < kChunk; ++it) {
-    k_mixed_update<<<::femk::counted_launch() + ga, kThreads, 0, s>>>(n, m.w, m.pv, m.s, m.e, m.r, m.dd,
-                                                                     p->partials + kPartialsA, m.st);
-    launch_step32<false>(p, m.r, m.w, m.st, s);
+    const int odd = it & 1;  // a chunk has an even number of steps, so it starts on an even one
+    auto ka = odd ? k_mixed_update<true> : k_mixed_update<false>;
+    ka<<<::femk::counted_launch() + ga, kThreads, 0, s>>>(n, m.w, m.pv, m.s, m.e, m.r, m.dd, p->partials + kPartialsA,
+                                                         m.st);
+    launch_step32<false>(p, m.r, m.w, m.st, s, odd);
   }
-  k_fold<<<::femk::counted_launch() + wave_grid(k_fold, 256, p), 256, 0, s>>>(n, x, m.e, m.sc, m.st);
+  k_fold<<<::femk::counted_launch() + wave_grid(k_fold, 256, p), 256, 0, s>>>(n, x, m.e, m.pv, m.sc, m.st);
   launch_true_resid<false>(p, vals, x, b, dinv, m.r, m.pv, m.s, m.st, 0.0, 0.0, s);
   launch_step32<true>(p, m.r, m.w, m.st, s);
   FEMK_CUDA_TRY(cudaGetLastError());
@@ -698,13 +727,18 @@ extern "C" int femk_pcg_mixed(const femk_plan* pc, const double* vals, const dou
   double* s64 = p->work;  // the FP64 CG workspace is free during a mixed solve
   k_scaling<<<::femk::counted_launch() + g1, 256, 0, ws>>>(dinv64, n, m.sc, m.dd, s64);
   if (p->sell_vals32) {
-    const int gg = blocks_for(p->n_slices * 32, 256, p->n_sm * 16);
-    if (p->sell_c16)
-      k_gather_scaled<int16_t><<<::femk::counted_launch() + gg, 256, 0, ws>>>(
-          p->sell_ptr, p->indptr, p->sell_c16, n, p->n_slices, vals, s64, p->sell_vals32);
-    else
-      k_gather_scaled<int32_t><<<::femk::counted_launch() + gg, 256, 0, ws>>>(
-          p->sell_ptr, p->indptr, p->sell_cols, n, p->n_slices, vals, s64, p->sell_vals32);
+    const int gg = blocks_for(p->n_slices, 4, p->n_sm * 16);
+    const int32_t cap = 32 * (p->max_row > 0 ? p->max_row : 1);
+    const size_t smem = sizeof(double) * 4 * (size_t)cap;
+    if (p->sell_c16) {
+      FEMK_CUDA_TRY(cudaFuncSetAttribute(k_gather_scaled<int16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_gather_scaled<int16_t><<<::femk::counted_launch() + gg, 128, smem, ws>>>(
+          p->sell_ptr, p->indptr, p->sell_c16, n, p->n_slices, vals, p->nnz, cap, s64, p->sell_vals32, p->dev_err);
+    } else {
+      FEMK_CUDA_TRY(cudaFuncSetAttribute(k_gather_scaled<int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_gather_scaled<int32_t><<<::femk::counted_launch() + gg, 128, smem, ws>>>(
+          p->sell_ptr, p->indptr, p->sell_cols, n, p->n_slices, vals, p->nnz, cap, s64, p->sell_vals32, p->dev_err);
+    }
   } else {
     k_scale_csr<<<::femk::counted_launch() + g1, 256, 0, ws>>>(p->indptr, p->indices, n, vals, s64, p->vals32);
   }

@@ -13,6 +13,7 @@
 
 #include <type_traits>
 
+#include "femk_internal.cuh"
 #include "femk_l2.cuh"
 
 namespace femk {
@@ -23,6 +24,37 @@ __device__ __forceinline__ int64_t col_at(const int32_t* __restrict__ cols, int3
 }
 __device__ __forceinline__ int64_t col_at(const int16_t* __restrict__ cols, int32_t k, int64_t row) {
   return row + (int64_t)__ldcs(cols + k);
+}
+
+// Sliced-ELL copy of CSR values, one warp per 32-row slice (global warp g takes slices g, g + NW,
+// ...): rows 32s ... 32s+31 are one contiguous CSR range, read coalesced into the warp's shared
+// buffer wbuf (room for 32 rows of the plan's longest row), then entry k of row 32s + l is written
+// to out[sptr[s] + 32 k + l] as f(value, row, out index), and padding past the row's length as 0.
+// Both the reads and the writes are coalesced; only the shared-memory reads are strided.
+template <typename T, typename F>
+__device__ __forceinline__ void sell_transpose_warp(double* wbuf, int32_t cap, const int64_t* __restrict__ sptr,
+                                                    const int32_t* __restrict__ indptr, int64_t n, int64_t nslices,
+                                                    const double* __restrict__ vals, int64_t nnz, T* __restrict__ out,
+                                                    int64_t g, int64_t NW, F f, int* err) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t sl = g; sl < nslices; sl += NW) {
+    const int64_t r0 = sl * 32, row = r0 + lane;
+    const int64_t rl = r0 + 32 < n ? r0 + 32 : n;
+    const int32_t base = __ldg(indptr + r0);
+    const int32_t end = __ldg(indptr + rl);
+    for (int32_t e = base + lane; e < end; e += 32)
+      if (FEMK_IN_BOUNDS(e - base, cap, err) && FEMK_IN_BOUNDS(e, nnz, err)) wbuf[e - base] = __ldcs(vals + e);
+    __syncwarp();
+    const int32_t beg = row < n ? __ldg(indptr + row) - base : 0;
+    const int32_t len = row < n ? __ldg(indptr + row + 1) - base - beg : 0;
+    const int64_t b0 = sptr[sl] + lane;
+    const int32_t w = (int32_t)((sptr[sl + 1] - sptr[sl]) >> 5);
+    for (int32_t k = 0; k < w; ++k) {
+      const int64_t j = b0 + 32 * k;
+      out[j] = (k < len && FEMK_IN_BOUNDS(beg + k, cap, err)) ? f(wbuf[beg + k], row, j) : T(0);
+    }
+    __syncwarp();  // the buffer is refilled for the next slice
+  }
 }
 
 // gather functors: x[j], or the CG direction z[j] + beta p[j] formed on the fly

@@ -205,8 +205,10 @@ def mixed_pcg(A, b, inv_diag, tol=1e-8, atol=0.0, maxiter=20_000, delta2=1e-4, r
 
     ``single_reduction`` selects the device's arrangement: CG on A^ = S A S (S = D^-1/2, formed in
     FP64, rounded to FP32) -- Jacobi-PCG in split form, so z^ = r^ -- with w = A^ r and s = A^ p by
-    recurrence, the products <p, s>, <r, s>, <r, r>, <r, D r> taken after the vector update and
-    <r, w> after the SpMV, and <p', A^ p'> = <r, w> + 2 beta <r, s> + beta^2 <p, s>. Otherwise the
+    recurrence, the products <p, s>, <r, s>, <r, r> taken after the vector update and <r, w> after
+    the SpMV, and <p', A^ p'> = <r, w> + 2 beta <r, s> + beta^2 <p, s>. Steps alternate: the odd ones
+    (counted from 0 after each refresh) form <r, D r> for the stop and drop tests and add two steps'
+    worth of e, (alpha' + alpha beta) p' + alpha r; an owed term is paid at the update. Otherwise the
     textbook FP32 loop (q = A p, <p, q> and <r, z> in two reductions, z = D^-1 r). FP32 products are
     summed in FP64 here (the device sums FP32 per thread, then FP64), so iteration counts agree to a
     few. Returns (x, FP32 iterations, FP64 residual evaluations)."""
@@ -275,21 +277,45 @@ def mixed_pcg(A, b, inv_diag, tol=1e-8, atol=0.0, maxiter=20_000, delta2=1e-4, r
     gamma, alpha, beta = None, 1.0, 0.0
     w = Ah @ r  # the first direction: beta = 0
     g2, ps, rs = dot(r, r), 0.0, 0.0
+    j, pend = 0, 0.0  # steps since the last refresh; alpha whose e += alpha p an even step owes
+    refreshed = True
     while True:
         den = dot(r, w) + 2.0 * beta * rs + beta * beta * ps
         if not den > 0:
-            raise ArithmeticError("mixed_pcg: <p, A p> <= 0 in FP32")
+            if refreshed:
+                raise ArithmeticError("mixed_pcg: <p, A p> <= 0 in FP32")
+            # an untested even step left r = 0 (exact arithmetic): the FP64 residual decides
+            x = x + sc64 * (f32(pend) * p + e).astype(np.float64)
+            e[:] = 0
+            pend, j = 0.0, 0
+            r, rr_since = replace()
+            outer += 1
+            if rr_since <= atol2 or it >= maxiter:
+                return x, it, outer
+            g2, ps, rs = dot(r, r), dot(p, s), dot(r, s)
+            w = Ah @ r
+            beta = 0.0 if restart else g2 / gamma
+            refreshed = True
+            continue
+        refreshed = False
         alpha, gamma = g2 / den, g2
+        odd = j % 2 == 1  # odd steps pay e for two steps and read D for the tests
+        p_prev, r_prev = p, r
         p = f32(beta) * p + r  # K_A
         s = f32(beta) * s + w
-        e = f32(alpha) * p + e
+        if odd:  # alpha' p' + alpha p = (alpha' + alpha beta) p' + alpha r
+            e = f32(pend + alpha * beta) * p_prev + (f32(alpha) * r_prev + e)
         r = -f32(alpha) * s + r
-        ps, rs, g2, rho = dot(p, s), dot(r, s), dot(r, r), dot(r * r, dd)
+        ps, rs, g2 = dot(p, s), dot(r, s), dot(r, r)
+        rho = dot(r * r, dd) if odd else None
+        pend = 0.0 if odd else alpha
         w = Ah @ r  # K_B
         it += 1
-        if rho <= atol2 or rho < delta2 * rr_since or it >= maxiter:
-            x = x + sc64 * e.astype(np.float64)
+        j += 1
+        if (odd and (rho <= atol2 or rho < delta2 * rr_since)) or it >= maxiter:
+            x = x + sc64 * (f32(pend) * p + e).astype(np.float64)
             e[:] = 0
+            pend, j = 0.0, 0
             r, rr_since = replace()
             outer += 1
             if rr_since <= atol2 or it >= maxiter:
@@ -297,5 +323,6 @@ def mixed_pcg(A, b, inv_diag, tol=1e-8, atol=0.0, maxiter=20_000, delta2=1e-4, r
             g2, ps, rs = dot(r, r), dot(p, s), dot(r, s)  # the refresh step's products
             w = Ah @ r
             beta = 0.0 if restart else g2 / gamma
+            refreshed = True
         else:
             beta = g2 / gamma
