@@ -44,6 +44,9 @@ def parse_args():
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--solver", choices=["fp64", "mixed", "matfree"], default="fp64",
                     help="solver of the timed step (fp64 is the headline; the others serve profiling runs)")
+    ap.add_argument("--profile-step", action="store_true",
+                    help="kernel profiling: after the warm-up run ONE step of --solver between cudaProfilerStart "
+                         "and cudaProfilerStop (for ncu --profile-from-start off), print a short line and exit")
     ap.add_argument("--path", choices=["tri", "theta"], default=None,
                     help="time a secondary workload instead of the headline (kernel profiling): 'tri' = 2-D P1 "
                          "triangles, n^2 rectangles (--n, default 1024), FP64 assemble + PCG; 'theta' = the P1 "
@@ -683,6 +686,16 @@ def run_ours(args):
     # ---- headline: FP64 CSR
     for i in range(args.warmup):
         step(i)
+    if args.profile_step:
+        barrier()
+        torch.cuda.profiler.start()
+        step(args.warmup)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        if rank == 0:
+            print(json.dumps({"profile_step": args.solver, "workload": workload_desc(args.n, args.order, T, ndof, nnz),
+                              "iters": iters_seen[-1], "relres": rel_seen[-1]}))
+        return
     iters_seen.clear()
     rel_seen.clear()
     clocks = ClockSampler(dev.index)

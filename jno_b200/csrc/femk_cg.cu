@@ -559,12 +559,6 @@ __global__ void k_mask_cells(const int32_t* __restrict__ cells, int64_t len, con
   }
 }
 
-// k_e = exp(param_e), once per matrix-free solve instead of once per element and product
-__global__ void k_exp_coef(const double* __restrict__ param, int64_t ntet, double* __restrict__ ke) {
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x)
-    ke[c] = exp(param[c]);
-}
-
 __global__ void k_dirichlet_identity(const int32_t* __restrict__ dlist, int64_t nd, const double* __restrict__ x,
                                      double* __restrict__ y, const CgState* st) {
   if (st && st->done) return;
@@ -1291,16 +1285,7 @@ extern "C" int femk_pcg_matfree(const femk_plan* p, const double* param, int mod
   FEMK_CHECK_ARG(p && b && x, "femk_pcg_matfree: NULL argument");
   FEMK_CHECK_ARG(coef_mode_ok(p, mode, param), "femk_pcg_matfree: bad coefficient");
   cudaStream_t s = (cudaStream_t)stream;
-  FEMK_TRY(resolve_coef(p, param, mode, s, &param, &mode));
-  if (mode == FEMK_COEF_EXP) {  // every CG step applies the operator: exponentiate once
-    femk_plan* pm = const_cast<femk_plan*>(p);
-    if (!pm->mf_coef) FEMK_CUDA_TRY(cudaMalloc(&pm->mf_coef, sizeof(double) * (p->ntet > 0 ? p->ntet : 1)));
-    k_exp_coef<<<::femk::counted_launch() + blocks_for(p->ntet, 256, p->n_sm * 16), 256, 0, s>>>(param, p->ntet,
-                                                                                               pm->mf_coef);
-    FEMK_CUDA_TRY(cudaGetLastError());
-    param = pm->mf_coef;
-    mode = FEMK_COEF_LINEAR;
-  }
+  FEMK_TRY(resolve_coef_exp(p, param, mode, s, &param, &mode));  // every CG step applies the operator
   MatFree m{param, mode, scale};
   return pcg_run(p, nullptr, &m, b, x, dinv, tol, atol, maxiter, iters_out, relres_out, s);
 }

@@ -229,7 +229,7 @@ struct femk_plan {
   int batch_graph_ok = 1;
   void* prof = nullptr;         // per-kernel CG timing (femk_set_profiling)
   double* coef_tmp = nullptr;   // f64[ntet] element coefficients of a nodal parameter
-  double* mf_coef = nullptr;    // f64[ntet] exp(param) of a matrix-free solve
+  double* kcoef = nullptr;      // f64[ntet] exp(param) of the current assembly or matrix-free solve
   int32_t* mcells = nullptr;    // i32[ntet*nd] cells with each Dirichlet DOF d as -1 - d (matrix-free operator)
   double* theta_ws = nullptr;   // f64[3 vstride] theta march: step Jacobi inverse, step right-hand side, previous state
   double* gm_ws = nullptr;      // GMRES: Krylov basis (restart + 1 vectors), w, q, partials, small arrays
@@ -277,6 +277,10 @@ int ensure_workspace(femk_plan* p);
 // stream s) read as FEMK_COEF_LINEAR; other modes pass through unchanged.
 int resolve_coef(const femk_plan* p, const double* param, int mode, cudaStream_t s, const double** param_out,
                  int* mode_out);
+// resolve_coef, then FEMK_COEF_EXP as well: exp(param) once per element into the plan's kcoef
+// buffer, read as FEMK_COEF_LINEAR (callers that visit an element more than once per call)
+int resolve_coef_exp(const femk_plan* p, const double* param, int mode, cudaStream_t s, const double** param_out,
+                     int* mode_out);
 
 // Restarted GMRES (femk_gmres.cu) on the plan's prepared sliced-ELL operator (sell) or the canonical
 // CSR values; x holds x0 on entry and the solution on return.
