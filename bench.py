@@ -47,10 +47,11 @@ def parse_args():
     ap.add_argument("--profile-step", action="store_true",
                     help="kernel profiling: after the warm-up run ONE step of --solver between cudaProfilerStart "
                          "and cudaProfilerStop (for ncu --profile-from-start off), print a short line and exit")
-    ap.add_argument("--path", choices=["tri", "theta"], default=None,
+    ap.add_argument("--path", choices=["tri", "theta", "batched"], default=None,
                     help="time a secondary workload instead of the headline (kernel profiling): 'tri' = 2-D P1 "
                          "triangles, n^2 rectangles (--n, default 1024), FP64 assemble + PCG; 'theta' = the P1 "
-                         "n^3 transient march (--n, default 128), step-operator assembly + 10 backward-Euler steps")
+                         "n^3 transient march (--n, default 128), step-operator assembly + 10 backward-Euler steps; "
+                         "'batched' = the 256-problem batch, assemble + one batched FP64 PCG launch")
     return ap.parse_args()
 
 
@@ -66,7 +67,30 @@ def run_path(args):
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
     info = {}
-    if args.path == "tri":
+    if args.path == "batched":
+        from jno_b200.batch import BatchedPoisson, batched_workload
+        from jno_b200.tuner import batched_schedule
+
+        sides, probs = batched_workload(256)
+        batch = BatchedPoisson([(p, t) for p, t, _ in probs])
+        plan = batch.plan
+        logk = torch.as_tensor(np.concatenate([lk for _, _, lk in probs]), device=dev)
+        vals, b = plan.assemble(logk)
+        inv = plan.jacobi(vals)
+        sched = batched_schedule(batch, vals, b, inv, 1e-8)
+
+        def step(i):
+            plan.assemble(logk, vals=vals, b=b)
+            plan.jacobi(vals, out=inv)
+            x, it, rel, stv, st = plan.pcg_batched(batch.row_off, vals, b, None, inv, 1e-8, 0.0, 20_000,
+                                                   sched["tile_rows"], sched["blocks_per_sm"])
+            info.setdefault("iters", []).append(float(it.max()))
+
+        workload = (f"256 P1 problems, sides {int(sides.min())}..{int(sides.max())} hexes ({plan.n:,} DOF), "
+                    f"assemble + batched Jacobi-PCG to 1e-8, schedule {sched['tile_rows']} rows x "
+                    f"{sched['blocks_per_sm']} blocks/SM")
+        metric, units = "DOF/s", plan.n
+    elif args.path == "tri":
         n = 1024 if args.n == 128 else args.n
         pts, tris = rect_points_tris(n, n)
         plan = FemPlan(jitter_interior_2d(pts, n, n, seed=0)[:, :2], tris, 1)
@@ -318,6 +342,18 @@ def whole_job_value(ndof, world, ms_step):
 
 
 # ------------------------------------------------------------------------------------------ ours
+def peak_hbm_gbs():
+    """(HBM copy bandwidth in GB/s, its source): MEASURED_PEAKS.json's hbm_gbs when the file exists,
+    else the earlier copy-bandwidth measurement on this pool (6650 GB/s)."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        try:
+            return float(json.load(open(path))["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+        except Exception:
+            pass
+    return 6650.0, "fallback (no MEASURED_PEAKS.json): 6.65 TB/s"
+
+
 def roofline_traffic():
     """DRAM bytes per SpMV launch from the committed ncu summary, if one exists."""
     path = os.path.join(ROOT, "profiles", "sell_spmv_fp64_p1_128.md")
@@ -489,10 +525,19 @@ def batched_variant(dev, count=256, reps=3):
     ms_m = e0.elapsed_time(e1) / reps
     err = max(float(torch.linalg.norm(xm[r0:r1] - x64[r0:r1]) / max(torch.linalg.norm(x64[r0:r1]).item(), 1e-300))
               for r0, r1 in zip(batch.row_off[:-1], batch.row_off[1:]) if r1 > r0)
+    # algorithmic bytes of the FP64 batch: per problem and iteration the CSR product (12 nnz + 20 n)
+    # and the vector phases (x, r read + written, p, q, D^-1 read, z written: 64 n; p = z + beta p: 24 n)
+    ip = batch.plan.pattern()[0].cpu().numpy().astype(np.int64)
+    ro = np.asarray(batch.row_off, dtype=np.int64)
+    nk, nnzk = np.diff(ro), ip[ro[1:]] - ip[ro[:-1]]
+    it_np = np.asarray(it.cpu() if hasattr(it, "cpu") else it, dtype=np.float64)
+    sum_bytes = float(np.sum(it_np * (12.0 * nnzk + 108.0 * nk)))
     return {"workload": f"{count} P1 problems, sides {int(sides.min())}..{int(sides.max())} hexes "
                         f"({batch.plan.ntet:,} tets, {batch.plan.n:,} DOF in total)",
             "value": batch.plan.n / (ms / 1e3), "unit": "DOF/s", "ms_per_batch": ms,
             "iters_min": int(it.min()), "iters_max": int(it.max()), "max_relres": float(rel.max()),
+            "sum_iteration_bytes": sum_bytes, "GB/s": sum_bytes / (ms / 1e3) / 1e9,
+            "frac_of_hbm": sum_bytes / (ms / 1e3) / 1e9 / peak_hbm_gbs()[0],
             "status_ok": bool(st == 0), "schedule": {k: sched[k] for k in ("tile_rows", "blocks_per_sm")},
             "one_graph_launch": bool(getattr(batch.plan, "batch_graph", False)), "precision": "fp64",
             "mixed": {"value": batch.plan.n / (ms_m / 1e3), "unit": "DOF/s", "ms_per_batch": ms_m,
@@ -766,15 +811,7 @@ def run_ours(args):
     sell_bytes = (plan.sell_nnz * 8 + plan.sell_col_units * col_bytes + 8 * (nsl + 1) * (2 if tables else 1)
                   + 16 * ndof)
     csr_bytes = 12 * nnz + 20 * ndof + 4
-    peak = 6650.0  # the earlier copy-bandwidth measurement on this pool, used only without the file below
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    peak_src = "fallback (no MEASURED_PEAKS.json): 6.65 TB/s"
-    if os.path.exists(peaks_path):
-        try:
-            peak = float(json.load(open(peaks_path))["hbm_gbs"])
-            peak_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
-        except Exception:
-            pass
+    peak, peak_src = peak_hbm_gbs()
     achieved = sell_bytes / (sell_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": roofline_traffic(),

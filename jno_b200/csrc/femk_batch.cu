@@ -5,7 +5,9 @@
 // the plan build and one femk_assemble call serve all of them; problem k owns the contiguous rows
 // [row_off[k], row_off[k+1]). Rows are cut into tiles that never cross a problem; a tile is one
 // warp's work item, and every grid phase walks the tiles of the still-active problems (tile t on
-// warp t mod W, W = warps in the grid, no block-wide synchronisation inside a phase):
+// warp t mod W, W = warps in the grid, no block-wide synchronisation inside a phase). The products
+// run on the plan's sliced-ELL copy (lane per row; copied from the CSR values in the same graph),
+// with the vectors gathered through L1 (the barriers' acquire makes other blocks' writes visible):
 //   phase 0 (once): r = b - A x0, z = D^-1 r, p = z, per-tile <r,z>, <r,r>, <b,b>
 //   phase 1: q = A p, per-tile <p, q>          | owner pass: alpha_k
 //   phase 2: x, r, z updates, <r,z>, <r,r>     | owner pass: beta_k, stop test of problem k
@@ -43,6 +45,12 @@ struct BatchArgs {
   const int32_t* indptr;
   const int32_t* indices;
   const double* vals;
+  // the plan's sliced-ELL copy (sptr == NULL: the products run on the CSR)
+  const int64_t* sptr;
+  const double* svals;
+  const float* svals32;
+  const int16_t* sc16;  // int16 column offsets, or NULL: absolute columns in scols
+  const int32_t* scols;
   // mixed precision: FP32 values and inner vectors, per-problem update bookkeeping
   const float* vals32;
   float *r32, *z32, *p32, *q32, *d32;
@@ -76,12 +84,41 @@ struct BatchArgs {
   int32_t skip;    // testing: block that skips its first barrier arrival (-1: none)
 };
 
+// x[j] with a plain (L1-cached) load. The vectors a phase gathers were written in an earlier phase,
+// and the grid barrier between the two (fence, then a GPU-scope acquire by every block) makes those
+// writes visible to plain loads; the read-only path (__ldg) could return stale lines inside the launch.
+template <typename V>
+struct GatherPlain {
+  const V* x;
+  __device__ __forceinline__ V operator()(int64_t j) const { return x[j]; }
+  __device__ __forceinline__ V operator()(int32_t j) const { return x[j]; }
+};
+
 // One warp computes (A v)[row] for the rows of its tile; the epilogue functor sees (row, Av).
-// V = double: the FP64 values a.vals; V = float: the FP32 values a.vals32 (FP32 accumulation).
+// V = double: the FP64 values; V = float: the FP32 values (FP32 accumulation). On the sliced-ELL
+// copy a lane owns a row of each 32-row slice the tile covers (tiles start and end on slice
+// boundaries except at the ends of a problem), with every value and column load independent of the
+// others; on the CSR kL lanes share a row.
 template <typename V = double, typename F>
-__device__ __forceinline__ void tile_spmv(const BatchArgs& a, int32_t r0, int32_t r1, const V* __restrict__ v,
-                                          F&& epi) {
+__device__ __forceinline__ void tile_spmv(const BatchArgs& a, int32_t r0, int32_t r1, const V* v, F&& epi) {
   const int lane = threadIdx.x & 31;
+  if (a.sptr) {
+    const V* vals;
+    if constexpr (sizeof(V) == 8)
+      vals = a.svals;
+    else
+      vals = a.svals32;
+    for (int32_t s = r0 >> 5; s <= (r1 - 1) >> 5; ++s) {
+      const int32_t row = s * 32 + lane;
+      if (row < r0 || row >= r1) continue;
+      const int64_t b0 = __ldg(a.sptr + s);
+      const int32_t w = (int32_t)((__ldg(a.sptr + s + 1) - b0) >> 5);
+      const V acc = a.sc16 ? sell_row<V, int16_t, 8>(vals + b0 + lane, a.sc16 + b0 + lane, w, row, GatherPlain<V>{v})
+                           : sell_row<V, int32_t, 8>(vals + b0 + lane, a.scols + b0 + lane, w, row, GatherPlain<V>{v});
+      epi((int64_t)row, acc);
+    }
+    return;
+  }
   const int sub = lane % kL;
   constexpr int RPW = 32 / kL;
   const V* vals;
@@ -92,7 +129,7 @@ __device__ __forceinline__ void tile_spmv(const BatchArgs& a, int32_t r0, int32_
   for (int64_t base = r0; base < r1; base += RPW * kU) {
     V sv[kU];
     int64_t rows[kU];
-    csr_rows_g<kL, kU, V, int32_t>(a.indptr, a.indices, vals, GatherXcg<V>{v}, r1, base, lane, sv, rows);
+    csr_rows_g<kL, kU, V, int32_t>(a.indptr, a.indices, vals, GatherPlain<V>{v}, r1, base, lane, sv, rows);
 #pragma unroll
     for (int u = 0; u < kU; ++u)
       if (rows[u] < r1 && sub == 0) epi(rows[u], sv[u]);
@@ -502,15 +539,20 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
   FEMK_CHECK_ARG(pc->coop, "femk_pcg_batched: the device does not support cooperative launch");
   femk_plan* p = const_cast<femk_plan*>(pc);
   FEMK_CHECK_ARG(row_off[0] == 0 && row_off[nprob] == p->n, "femk_pcg_batched: row_off must span [0, n)");
-  // tiles
+  // tiles: on the sliced-ELL copy they end on global multiples of tile_rows (rounded up to a whole
+  // slice), so only the first and last tile of a problem cover part of a slice
+  const bool sell = p->use_sell && p->sell_cols;
+  const int64_t tr = sell ? (tile_rows + 31) / 32 * 32 : tile_rows;
   std::vector<int32_t> r0, r1, tp, t0(nprob), t1(nprob);
   for (int32_t k = 0; k < nprob; ++k) {
     FEMK_CHECK_ARG(row_off[k + 1] > row_off[k], "femk_pcg_batched: empty problem");
     t0[k] = (int32_t)r0.size();
-    for (int64_t s0 = row_off[k]; s0 < row_off[k + 1]; s0 += tile_rows) {
+    for (int64_t s0 = row_off[k]; s0 < row_off[k + 1];) {
+      const int64_t e = std::min<int64_t>(sell ? (s0 / tr + 1) * tr : s0 + tr, row_off[k + 1]);
       r0.push_back((int32_t)s0);
-      r1.push_back((int32_t)std::min<int64_t>(s0 + tile_rows, row_off[k + 1]));
+      r1.push_back((int32_t)e);
       tp.push_back(k);
+      s0 = e;
     }
     t1[k] = (int32_t)r0.size();
   }
@@ -534,6 +576,19 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
   a.indptr = p->indptr;
   a.indices = p->indices;
   a.vals = vals;
+  a.sptr = nullptr;
+  a.svals = nullptr;
+  a.svals32 = nullptr;
+  a.sc16 = nullptr;
+  a.scols = nullptr;
+  if (sell) {
+    FEMK_TRY(ensure_sell_values(p, mixed));
+    a.sptr = p->sell_ptr;
+    a.svals = p->sell_vals;
+    a.svals32 = mixed ? p->sell_vals32 : nullptr;
+    a.sc16 = p->sell_c16;
+    a.scols = p->sell_cols;
+  }
   a.tile_r0 = ib;
   a.tile_r1 = ib + ntiles;
   a.tile_prob = ib + 2 * ntiles;
@@ -569,7 +624,7 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
   a.vals32 = nullptr;
   a.r32 = a.z32 = a.p32 = a.q32 = a.d32 = nullptr;
   if (mixed) {
-    if (!p->vals32) FEMK_CUDA_TRY(cudaMalloc(&p->vals32, sizeof(float) * (p->nnz + 1)));
+    if (!sell && !p->vals32) FEMK_CUDA_TRY(cudaMalloc(&p->vals32, sizeof(float) * (p->nnz + 1)));
     if (!p->work32) FEMK_CUDA_TRY(cudaMalloc(&p->work32, sizeof(float) * kWork32Vectors * p->vstride));
     a.vals32 = p->vals32;
     a.r32 = p->work32;
@@ -614,7 +669,10 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
     cudaError_t e = cudaStreamBeginCapture(p->batch_stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       k_batch_reset<<<8, 256, 0, p->batch_stream>>>(a.done, a.status, a.active, nprob, a.bar);
-      if (mixed) k_to_f32<<<cgrid, 256, 0, p->batch_stream>>>(vals, p->nnz, p->vals32);
+      if (sell)
+        (void)launch_sell_values(p, vals, mixed, p->batch_stream);
+      else if (mixed)
+        k_to_f32<<<cgrid, 256, 0, p->batch_stream>>>(vals, p->nnz, p->vals32);
       void* cargs[] = {(void*)&a};
       cudaError_t el = cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), cargs, 0, p->batch_stream);
       cudaError_t ee = cudaStreamEndCapture(p->batch_stream, &g);
@@ -637,13 +695,16 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
     FEMK_CUDA_TRY(cudaEventRecord(p->batch_ev, s));
     FEMK_CUDA_TRY(cudaStreamWaitEvent(p->batch_stream, p->batch_ev, 0));
     FEMK_CUDA_TRY(cudaGraphLaunch(p->batch_exec, p->batch_stream));
-    count_launches(mixed ? 3 : 2);
+    count_launches(2 + (sell ? (mixed ? 2 : 1) : (mixed ? 1 : 0)));
     p->batch_graph_used = 1;
     FEMK_CUDA_TRY(cudaEventRecord(p->batch_ev, p->batch_stream));
     FEMK_CUDA_TRY(cudaStreamWaitEvent(s, p->batch_ev, 0));
   } else {
     k_batch_reset<<<::femk::counted_launch() + 8, 256, 0, s>>>(a.done, a.status, a.active, nprob, a.bar);
-    if (mixed) k_to_f32<<<::femk::counted_launch() + cgrid, 256, 0, s>>>(vals, p->nnz, p->vals32);
+    if (sell)
+      FEMK_TRY(launch_sell_values(p, vals, mixed, s));
+    else if (mixed)
+      k_to_f32<<<::femk::counted_launch() + cgrid, 256, 0, s>>>(vals, p->nnz, p->vals32);
     FEMK_CUDA_TRY(cudaGetLastError());
     void* args[] = {(void*)&a};
     counted_launch();

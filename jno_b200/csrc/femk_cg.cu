@@ -1175,6 +1175,29 @@ int spmv_csr(const femk_plan* p, const double* vals, const double* x, double* y,
   return launch_csr<kPlain>(p, vals, x, y, nullptr, nullptr, nullptr, nullptr, nullptr, 0.0, 0.0, s);
 }
 
+int ensure_sell_values(femk_plan* p, bool fp32) {
+  if (!p->sell_vals) FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals, sizeof(double) * (p->sell_nnz + 1)));
+  if (fp32 && !p->sell_vals32) FEMK_CUDA_TRY(cudaMalloc(&p->sell_vals32, sizeof(float) * (p->sell_nnz + 1)));
+  const int32_t cap = 32 * (p->max_row > 0 ? p->max_row : 1);
+  const int smem = (int)(sizeof(double) * 4 * (size_t)cap);
+  FEMK_CUDA_TRY(cudaFuncSetAttribute(k_sell_gather<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  FEMK_CUDA_TRY(cudaFuncSetAttribute(k_sell_gather<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  return FEMK_OK;
+}
+
+int launch_sell_values(const femk_plan* p, const double* vals, bool fp32, cudaStream_t s) {
+  const int32_t cap = 32 * (p->max_row > 0 ? p->max_row : 1);
+  const size_t smem = sizeof(double) * 4 * (size_t)cap;
+  const int grid = blocks_for(p->n_slices, 4, p->n_sm * 16);
+  k_sell_gather<double><<<::femk::counted_launch() + grid, 128, smem, s>>>(p->sell_ptr, p->indptr, p->n, p->n_slices,
+                                                                           vals, p->nnz, cap, p->sell_vals, p->dev_err);
+  if (fp32)
+    k_sell_gather<float><<<::femk::counted_launch() + grid, 128, smem, s>>>(p->sell_ptr, p->indptr, p->n, p->n_slices,
+                                                                            vals, p->nnz, cap, p->sell_vals32, p->dev_err);
+  FEMK_CUDA_TRY(cudaGetLastError());
+  return FEMK_OK;
+}
+
 }  // namespace femk
 
 using namespace femk;

@@ -9,7 +9,7 @@
 
 #include "../../include/femk.h"
 
-#define FEMK_VERSION 10000
+#define FEMK_VERSION 10100
 
 namespace femk {
 
@@ -272,6 +272,12 @@ int check_bounds(const femk_plan* p, cudaStream_t s, const char* what);
 int scan_exclusive_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
 
 int ensure_workspace(femk_plan* p);
+
+// The sliced-ELL value copies of a caller's CSR values (femk_cg.cu): ensure_sell_values allocates
+// sell_vals (and, fp32, sell_vals32) and sets the copy kernels' shared-memory size (not during a
+// graph capture); launch_sell_values enqueues the copies (FP64, and the unscaled FP32 values).
+int ensure_sell_values(femk_plan* p, bool fp32);
+int launch_sell_values(const femk_plan* p, const double* vals, bool fp32, cudaStream_t s);
 
 // Nodal P1 coefficient modes become a per-element coefficient (plan-owned f64[ntet], computed on
 // stream s) read as FEMK_COEF_LINEAR; other modes pass through unchanged.

@@ -1,14 +1,18 @@
 """Autotuner for the batched persistent PCG schedule (tile size x blocks per SM).
 
-Each candidate runs the real batched solve once after a warm-up run; the fastest (CUDA events) is
-kept and cached in a JSON file (``$JNO_B200_TUNE_CACHE``, default ``~/.cache/jno_b200/tune.json``)
-keyed by the device name and the batch's size signature, so later runs skip the search.
+Each candidate runs the real batched solve once as a warm-up and then ``reps`` (default 3) timed
+times (CUDA events); the candidate with the smallest median is kept and cached in a JSON file
+(``$JNO_B200_TUNE_CACHE``, default ``~/.cache/jno_b200/tune.json``) keyed by the device name, the
+library version and the batch's size signature, so later runs skip the search.
 """
 
 import json
 import os
+import statistics
 
 import torch
+
+from . import _lib
 
 CANDIDATES = [(t, b) for t in (32, 64, 128, 256, 512) for b in (1, 2)]
 
@@ -40,23 +44,28 @@ def _store(cache):
 
 def signature(batch):
     name = torch.cuda.get_device_name(batch.plan.device)
-    return f"{name}|nprob={batch.nprob}|n={batch.plan.n}|nnz={batch.plan.nnz}"
+    version = _lib.load().femk_version()
+    return f"{name}|femk {version}|nprob={batch.nprob}|n={batch.plan.n}|nnz={batch.plan.nnz}"
 
 
-def tune(batch, vals, b, inv, tol, candidates=None):
-    """Time every candidate schedule; returns (best, {candidate: ms})."""
+def tune(batch, vals, b, inv, tol, candidates=None, reps=3):
+    """Time every candidate schedule (median of ``reps`` runs after a warm-up); returns
+    (best, {candidate: median ms})."""
     candidates = CANDIDATES if candidates is None else candidates
     plan = batch.plan
     times = {}
     for tile_rows, bps in candidates:
         plan.pcg_batched(batch.row_off, vals, b, None, inv, tol, 0.0, 20_000, tile_rows, bps)  # warm-up
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record()
-        plan.pcg_batched(batch.row_off, vals, b, None, inv, tol, 0.0, 20_000, tile_rows, bps)
-        e1.record()
-        torch.cuda.synchronize()
-        times[(tile_rows, bps)] = e0.elapsed_time(e1)
+        runs = []
+        for _ in range(max(1, reps)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            plan.pcg_batched(batch.row_off, vals, b, None, inv, tol, 0.0, 20_000, tile_rows, bps)
+            e1.record()
+            torch.cuda.synchronize()
+            runs.append(e0.elapsed_time(e1))
+        times[(tile_rows, bps)] = statistics.median(runs)
     best = min(times, key=times.get)
     return {"tile_rows": best[0], "blocks_per_sm": best[1], "ms": times[best]}, times
 
