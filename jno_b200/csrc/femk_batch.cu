@@ -22,10 +22,10 @@
 // The mixed-precision form (k_batch_mixed) runs the same phases on FP32 values and vectors (FP32
 // SpMV accumulation, dot products summed in FP64) with x kept in FP64, and gives every problem
 // FP64 reliable updates, as femk_pcg_mixed does for one problem: when its FP32 <r, r> fell by
-// delta2 since the last update, met the stop test or hit the cap, an update phase replaces r by
-// fp32(b - A x) with the FP64 values, keeps the direction, and retires the problem once the FP64
-// residual meets the stop rule. The update phase (two more grid barriers) runs only in the
-// iterations where some problem asked for one.
+// delta2 since the last update, met the stop test or hit the cap, the problem's next phase 1
+// replaces r by fp32(b - A x) with the FP64 values in place of its FP32 product, keeps the
+// direction, and retires the problem once the FP64 residual meets the stop rule. A replacement thus
+// costs the problem one step slot and no extra phase or grid barrier.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -55,9 +55,8 @@ struct BatchArgs {
   const float* vals32;
   float *r32, *z32, *p32, *q32, *d32;
   double* rr_since;  // [nprob] FP64 <r, r> at the last reliable update
-  int32_t* upd;      // [nprob] 1 while a reliable update is pending
+  int32_t* upd;      // [nprob] per-problem step mode of the mixed form (0 normal, 1 update requested, 2 replaced)
   int32_t* outer;    // [nprob] FP64 residual evaluations
-  int32_t* any_upd;  // [1] some problem requested an update this iteration
   double delta2;
   const int32_t* tile_r0;
   const int32_t* tile_r1;
@@ -113,8 +112,10 @@ __device__ __forceinline__ void tile_spmv(const BatchArgs& a, int32_t r0, int32_
       if (row < r0 || row >= r1) continue;
       const int64_t b0 = __ldg(a.sptr + s);
       const int32_t w = (int32_t)((__ldg(a.sptr + s + 1) - b0) >> 5);
-      const V acc = a.sc16 ? sell_row<V, int16_t, 8>(vals + b0 + lane, a.sc16 + b0 + lane, w, row, GatherPlain<V>{v})
-                           : sell_row<V, int32_t, 8>(vals + b0 + lane, a.scols + b0 + lane, w, row, GatherPlain<V>{v});
+      // entries in flight per lane: 16 FP32 (half the bytes each) or 8 FP64
+      constexpr int EB = sizeof(V) == 4 ? 16 : 8;
+      const V acc = a.sc16 ? sell_row<V, int16_t, EB>(vals + b0 + lane, a.sc16 + b0 + lane, w, row, GatherPlain<V>{v})
+                           : sell_row<V, int32_t, EB>(vals + b0 + lane, a.scols + b0 + lane, w, row, GatherPlain<V>{v});
       epi((int64_t)row, acc);
     }
     return;
@@ -361,38 +362,83 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
         retire(a, k, FEMK_OK);
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) *a.any_upd = 0;
   if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   double* alpha = a.gam + a.nprob;
   double* beta = alpha;
+  // Per-problem mode (a.upd): 0 a normal step; 1 a reliable update was requested, so this
+  // iteration's phase 3 leaves p alone and the next phase 1 computes the FP64 residual in place of
+  // the FP32 product; 2 the residual was replaced in phase 1, so phase 2 skips the problem and
+  // phase 3 forms the kept direction with beta = <r, z>_new / gamma. Only the owner passes change a
+  // mode, so every phase sees one value per iteration, and no iteration needs an extra phase.
   while (ld_acquire_u32((const unsigned int*)a.active) != 0u) {
-    // ---- phase 1: q = A32 p (FP32), <p, q>
+    // ---- phase 1: q = A32 p (FP32), <p, q>; or (mode 1) r = fp32(b - A64 x), z = D^-1 r, <r, z>, <r64, r64>
     for (int32_t t = gw; t < a.ntiles; t += NW) {
       const int32_t k = a.tile_prob[t];
       if (warp_done(a.done, k)) continue;
-      double acc[1] = {0.0};
-      tile_spmv<float>(a, a.tile_r0[t], a.tile_r1[t], a.p32, [&](int64_t row, float s) {
-        a.q32[row] = s;
-        acc[0] += (double)__ldcg(a.p32 + row) * (double)s;
-      });
-      tile_partial<1>(acc, a.P, a.ntiles, t, 3);
+      int m = lane == 0 ? __ldcg(a.upd + k) : 0;
+      m = __shfl_sync(0xffffffffu, m, 0);
+      if (m == 1) {
+        double acc[2] = {0.0, 0.0};
+        tile_spmv<double>(a, a.tile_r0[t], a.tile_r1[t], a.x, [&](int64_t row, double sv) {
+          const double r64 = a.b[row] - sv;
+          const float rf = (float)r64;
+          const float zf = a.d32[row] * rf;
+          a.r32[row] = rf;
+          a.z32[row] = zf;
+          acc[0] += (double)rf * (double)zf;
+          acc[1] += r64 * r64;
+        });
+        tile_partial<2>(acc, a.P, a.ntiles, t, 4);
+      } else {
+        double acc[1] = {0.0};
+        tile_spmv<float>(a, a.tile_r0[t], a.tile_r1[t], a.p32, [&](int64_t row, float sv) {
+          a.q32[row] = sv;
+          acc[0] += (double)__ldcg(a.p32 + row) * (double)sv;
+        });
+        tile_partial<1>(acc, a.P, a.ntiles, t, 3);
+      }
     }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
       if (block_done(a.done, k)) continue;
-      const double pq = prob_sum(a, 3, k);
-      if (threadIdx.x == 0) {
-        if (!(pq > 0.0) || !isfinite(pq))
-          retire(a, k, isfinite(pq) ? FEMK_BREAKDOWN : FEMK_NONFINITE);
-        else
-          alpha[k] = a.gam[k] / pq;
+      __shared__ int32_t mode_s;
+      if (threadIdx.x == 0) mode_s = __ldcg(a.upd + k);
+      __syncthreads();
+      const int32_t mode = mode_s;
+      __syncthreads();
+      if (mode == 1) {
+        const double rz = prob_sum(a, 4, k), rr = prob_sum(a, 5, k);
+        if (threadIdx.x == 0) {
+          a.outer[k] += 1;
+          a.rr[k] = rr;
+          if (!isfinite(rz) || !isfinite(rr)) {
+            retire(a, k, FEMK_NONFINITE);
+          } else if (!(rr > a.atol2[k]) || a.iter[k] >= a.maxiter) {
+            retire(a, k, FEMK_OK);
+          } else {
+            beta[k] = rz / a.gam[k];  // residual replacement keeps the search direction
+            a.gam[k] = rz;
+            a.rr_since[k] = rr;
+            a.upd[k] = 2;
+          }
+        }
+      } else {
+        const double pq = prob_sum(a, 3, k);
+        if (threadIdx.x == 0) {
+          if (!(pq > 0.0) || !isfinite(pq))
+            retire(a, k, isfinite(pq) ? FEMK_BREAKDOWN : FEMK_NONFINITE);
+          else
+            alpha[k] = a.gam[k] / pq;
+        }
       }
     }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
-    // ---- phase 2: x += alpha p (FP64), r -= alpha q, z = D^-1 r (FP32); <r, z>, <r, r>
+    // ---- phase 2 (mode 0): x += alpha p (FP64), r -= alpha q, z = D^-1 r (FP32); <r, z>, <r, r>
     for (int32_t t = gw; t < a.ntiles; t += NW) {
       const int32_t k = a.tile_prob[t];
       if (warp_done(a.done, k)) continue;
+      int m = lane == 0 ? __ldcg(a.upd + k) : 0;
+      if (__shfl_sync(0xffffffffu, m, 0) != 0) continue;
       const double al = __ldcg(alpha + k);
       const float alf = (float)al;
       double acc[2] = {0.0, 0.0};
@@ -411,6 +457,15 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
       if (block_done(a.done, k)) continue;
+      __shared__ int32_t mode2_s;
+      if (threadIdx.x == 0) mode2_s = __ldcg(a.upd + k);
+      __syncthreads();
+      const int32_t mode = mode2_s;
+      __syncthreads();
+      if (mode == 2) {  // the direction step of the replaced residual runs in phase 3
+        if (threadIdx.x == 0) a.upd[k] = 0;
+        continue;
+      }
       const double rz = prob_sum(a, 4, k), rr = prob_sum(a, 5, k);
       if (threadIdx.x == 0) {
         const int32_t itk = a.iter[k] + 1;
@@ -418,8 +473,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
         if (!isfinite(rz) || !isfinite(rr)) {
           retire(a, k, FEMK_NONFINITE);
         } else if (!(rr > a.atol2[k]) || rr < a.delta2 * a.rr_since[k] || itk >= a.maxiter) {
-          a.upd[k] = 1;  // FP64 residual replacement before the next direction
-          atomicExch(a.any_upd, 1);
+          a.upd[k] = 1;  // FP64 residual replacement in the next phase 1; p stays as it is
         } else {
           beta[k] = rz / a.gam[k];
           a.gam[k] = rz;
@@ -428,57 +482,12 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
       }
     }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
-    if (__ldcg(a.any_upd)) {
-      // ---- phase U: r = fp32(b - A64 x), z = D^-1 r for the problems that asked; <r, z>, <r64, r64>
-      for (int32_t t = gw; t < a.ntiles; t += NW) {
-        const int32_t k = a.tile_prob[t];
-        if (warp_done(a.done, k)) continue;
-        int u = lane == 0 ? __ldcg(a.upd + k) : 0;
-        if (!__shfl_sync(0xffffffffu, u, 0)) continue;
-        double acc[2] = {0.0, 0.0};
-        tile_spmv<double>(a, a.tile_r0[t], a.tile_r1[t], a.x, [&](int64_t row, double s) {
-          const double r64 = a.b[row] - s;
-          const float rf = (float)r64;
-          const float zf = a.d32[row] * rf;
-          a.r32[row] = rf;
-          a.z32[row] = zf;
-          acc[0] += (double)rf * (double)zf;
-          acc[1] += r64 * r64;
-        });
-        tile_partial<2>(acc, a.P, a.ntiles, t, 4);
-      }
-      if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
-      FEMK_OWNER_LOOP {
-        if (block_done(a.done, k)) continue;
-        __shared__ int32_t uk;
-        if (threadIdx.x == 0) uk = __ldcg(a.upd + k);
-        __syncthreads();
-        const bool pending = uk != 0;
-        __syncthreads();
-        if (!pending) continue;
-        const double rz = prob_sum(a, 4, k), rr = prob_sum(a, 5, k);
-        if (threadIdx.x == 0) {
-          a.upd[k] = 0;
-          a.outer[k] += 1;
-          a.rr[k] = rr;
-          if (!isfinite(rz) || !isfinite(rr))
-            retire(a, k, FEMK_NONFINITE);
-          else if (!(rr > a.atol2[k]) || a.iter[k] >= a.maxiter)
-            retire(a, k, FEMK_OK);
-          else {
-            beta[k] = rz / a.gam[k];  // residual replacement keeps the search direction
-            a.gam[k] = rz;
-            a.rr_since[k] = rr;
-          }
-        }
-      }
-      if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.any_upd, 0);
-      if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
-    }
-    // ---- phase 3: p = z + beta p
+    // ---- phase 3 (modes 0 and the one after a replacement): p = z + beta p
     for (int32_t t = gw; t < a.ntiles; t += NW) {
       const int32_t k = a.tile_prob[t];
       if (warp_done(a.done, k)) continue;
+      int m = lane == 0 ? __ldcg(a.upd + k) : 0;
+      if (__shfl_sync(0xffffffffu, m, 0) == 1) continue;
       const float be = (float)__ldcg(beta + k);
       for (int32_t i = a.tile_r0[t] + lane; i < a.tile_r1[t]; i += 32)
         a.p32[i] = fmaf(be, __ldcg(a.p32 + i), __ldcg(a.z32 + i));
@@ -619,7 +628,6 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
   a.rr_since = a.relres + nprob;
   a.upd = a.active + 1;
   a.outer = a.upd + nprob;
-  a.any_upd = a.outer + nprob;
   a.delta2 = delta2;
   a.vals32 = nullptr;
   a.r32 = a.z32 = a.p32 = a.q32 = a.d32 = nullptr;
