@@ -167,13 +167,6 @@ __device__ __forceinline__ void tile_partial(double (&v)[NV], double* P, int nti
   }
 }
 
-// done[k] read once per warp (lane 0, broadcast), so the whole warp takes the same branch
-__device__ __forceinline__ bool warp_done(const int32_t* done, int32_t k) {
-  int d = (threadIdx.x & 31) == 0 ? __ldcg(done + k) : 0;
-  d = __shfl_sync(0xffffffffu, d, 0);
-  return d != 0;
-}
-
 // done[k] read once per block (a problem's owner may retire it while other blocks run its tiles;
 // every thread of a block must take the same branch around the barriers inside the tile loop)
 __device__ __forceinline__ bool block_done(const int32_t* done, int32_t k) {
@@ -191,6 +184,41 @@ __device__ __forceinline__ void retire(const BatchArgs& a, int32_t k, int32_t st
   atomicSub(a.active, 1);
 }
 
+// The tiles of one warp (tiles gw, gw + NW, ..., at most 32 of them): lane j holds tile gw + j NW's
+// rows and problem, loaded once per launch. A phase then evaluates its filter for all of the warp's
+// tiles in one load per lane, where a per-tile loop would wait on a chain of dependent loads
+// (tile -> problem -> done flag -> rows) before each tile's work.
+struct WarpTiles {
+  int32_t r0, r1, k, count;
+};
+
+__device__ __forceinline__ WarpTiles warp_tiles(const BatchArgs& a, int32_t gw, int32_t NW) {
+  const int lane = threadIdx.x & 31;
+  const int64_t t = gw + (int64_t)lane * NW;
+  const bool have = t < a.ntiles;
+  WarpTiles w;
+  w.r0 = have ? a.tile_r0[t] : 0;
+  w.r1 = have ? a.tile_r1[t] : 0;
+  w.k = have ? a.tile_prob[t] : -1;
+  w.count = gw < a.ntiles ? min(32, (a.ntiles - 1 - gw) / NW + 1) : 0;
+  return w;
+}
+
+// body(t, r0, r1, k) for every tile of the warp whose problem passes keep(k), in tile order; keep is
+// evaluated by lane j for the warp's tile j, all lanes at once
+template <typename Keep, typename Body>
+__device__ __forceinline__ void for_warp_tiles(const WarpTiles& w, int32_t gw, int32_t NW, Keep&& keep, Body&& body) {
+  const int lane = threadIdx.x & 31;
+  const bool mine = lane < w.count && keep(w.k);
+  unsigned int mask = __ballot_sync(0xffffffffu, mine);
+  while (mask) {
+    const int j = __ffs(mask) - 1;
+    mask &= mask - 1;
+    body(gw + j * NW, __shfl_sync(0xffffffffu, w.r0, j), __shfl_sync(0xffffffffu, w.r1, j),
+         __shfl_sync(0xffffffffu, w.k, j));
+  }
+}
+
 // Owner pass: block b finishes problems k = b, b + G, ... from their tile partials.
 #define FEMK_OWNER_LOOP for (int32_t k = blockIdx.x; k < a.nprob; k += gridDim.x)
 
@@ -199,9 +227,12 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
   const int32_t gw = (int32_t)((blockIdx.x * (int64_t)kBT + threadIdx.x) >> 5);  // global warp
   const int32_t NW = (int32_t)(((int64_t)gridDim.x * kBT) >> 5);
   const int lane = threadIdx.x & 31;
+  const WarpTiles wt = warp_tiles(a, gw, NW);
+  auto every = [](int32_t) { return true; };
+  auto live = [&](int32_t k) { return __ldcg(a.done + k) == 0; };
   // ---- phase 0: residual of x0
-  for (int32_t t = gw; t < a.ntiles; t += NW) {
-    const int32_t r0 = a.tile_r0[t], r1 = a.tile_r1[t];
+  for_warp_tiles(wt, gw, NW, every, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t) {
+    const int32_t r0 = tr0, r1 = tr1;
     double acc[3] = {0.0, 0.0, 0.0};
     tile_spmv(a, r0, r1, a.x, [&](int64_t row, double s) {
       const double bi = a.b[row];
@@ -215,7 +246,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
       acc[2] += bi * bi;
     });
     tile_partial<3>(acc, a.P, a.ntiles, t, 0);
-  }
+  });
   if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   FEMK_OWNER_LOOP {
     const double rz = prob_sum(a, 0, k), rr = prob_sum(a, 1, k), bb = prob_sum(a, 2, k);
@@ -237,16 +268,14 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
   double* beta = alpha;             // (alpha is dead once phase 2 is done; beta reuses the slot)
   while (ld_acquire_u32((const unsigned int*)a.active) != 0u) {
     // ---- phase 1: q = A p, <p, q>
-    for (int32_t t = gw; t < a.ntiles; t += NW) {
-      const int32_t k = a.tile_prob[t];
-      if (warp_done(a.done, k)) continue;
+    for_warp_tiles(wt, gw, NW, live, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t k) {
       double acc[1] = {0.0};
-      tile_spmv(a, a.tile_r0[t], a.tile_r1[t], a.p, [&](int64_t row, double s) {
+      tile_spmv(a, tr0, tr1, a.p, [&](int64_t row, double s) {
         a.q[row] = s;
         acc[0] += __ldcg(a.p + row) * s;
       });
       tile_partial<1>(acc, a.P, a.ntiles, t, 3);
-    }
+    });
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
       if (block_done(a.done, k)) continue;
@@ -260,12 +289,10 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
     }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     // ---- phase 2: x, r, z updates; <r, z>, <r, r>
-    for (int32_t t = gw; t < a.ntiles; t += NW) {
-      const int32_t k = a.tile_prob[t];
-      if (warp_done(a.done, k)) continue;
+    for_warp_tiles(wt, gw, NW, live, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t k) {
       const double al = __ldcg(alpha + k);
       double acc[2] = {0.0, 0.0};
-      for (int32_t i = a.tile_r0[t] + lane; i < a.tile_r1[t]; i += 32) {
+      for (int32_t i = tr0 + lane; i < tr1; i += 32) {
         a.x[i] = a.x[i] + al * __ldcg(a.p + i);
         const double ri = __ldcg(a.r + i) - al * __ldcg(a.q + i);
         const double zi = a.dinv ? a.dinv[i] * ri : ri;
@@ -275,7 +302,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
         acc[1] += ri * ri;
       }
       tile_partial<2>(acc, a.P, a.ntiles, t, 4);
-    }
+    });
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
       if (block_done(a.done, k)) continue;
@@ -293,26 +320,24 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
     }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     // ---- phase 3: p = z + beta p
-    for (int32_t t = gw; t < a.ntiles; t += NW) {
-      const int32_t k = a.tile_prob[t];
-      if (warp_done(a.done, k)) continue;
+    for_warp_tiles(wt, gw, NW, live, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t k) {
       const double be = __ldcg(beta + k);
-      for (int32_t i = a.tile_r0[t] + lane; i < a.tile_r1[t]; i += 32)
+      for (int32_t i = tr0 + lane; i < tr1; i += 32)
         a.p[i] = __ldcg(a.z + i) + be * __ldcg(a.p + i);
-    }
+    });
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   }
   // ---- phase R: per-problem ||b - A x||, ||b||
-  for (int32_t t = gw; t < a.ntiles; t += NW) {
+  for_warp_tiles(wt, gw, NW, every, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t) {
     double acc[2] = {0.0, 0.0};
-    tile_spmv(a, a.tile_r0[t], a.tile_r1[t], a.x, [&](int64_t row, double s) {
+    tile_spmv(a, tr0, tr1, a.x, [&](int64_t row, double s) {
       const double bi = a.b[row];
       const double w = bi - s;
       acc[0] += w * w;
       acc[1] += bi * bi;
     });
     tile_partial<2>(acc, a.P, a.ntiles, t, 5);
-  }
+  });
   if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   FEMK_OWNER_LOOP {
     const double ww = prob_sum(a, 5, k), bb = prob_sum(a, 6, k);
@@ -325,10 +350,13 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
   const int32_t gw = (int32_t)((blockIdx.x * (int64_t)kBT + threadIdx.x) >> 5);  // global warp
   const int32_t NW = (int32_t)(((int64_t)gridDim.x * kBT) >> 5);
   const int lane = threadIdx.x & 31;
+  const WarpTiles wt = warp_tiles(a, gw, NW);
+  auto every = [](int32_t) { return true; };
+  auto live = [&](int32_t k) { return __ldcg(a.done + k) == 0; };
   // ---- phase 0: FP64 residual of x0, FP32 copies; <r, z> (FP32 data), <r64, r64>, <b, b>
-  for (int32_t t = gw; t < a.ntiles; t += NW) {
+  for_warp_tiles(wt, gw, NW, every, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t) {
     double acc[3] = {0.0, 0.0, 0.0};
-    tile_spmv<double>(a, a.tile_r0[t], a.tile_r1[t], a.x, [&](int64_t row, double s) {
+    tile_spmv<double>(a, tr0, tr1, a.x, [&](int64_t row, double s) {
       const double bi = a.b[row];
       const double r64 = bi - s;
       const float d = a.dinv ? (float)a.dinv[row] : 1.0f;
@@ -343,7 +371,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
       acc[2] += bi * bi;
     });
     tile_partial<3>(acc, a.P, a.ntiles, t, 0);
-  }
+  });
   if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   FEMK_OWNER_LOOP {
     const double rz = prob_sum(a, 0, k), rr = prob_sum(a, 1, k), bb = prob_sum(a, 2, k);
@@ -372,14 +400,12 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
   // mode, so every phase sees one value per iteration, and no iteration needs an extra phase.
   while (ld_acquire_u32((const unsigned int*)a.active) != 0u) {
     // ---- phase 1: q = A32 p (FP32), <p, q>; or (mode 1) r = fp32(b - A64 x), z = D^-1 r, <r, z>, <r64, r64>
-    for (int32_t t = gw; t < a.ntiles; t += NW) {
-      const int32_t k = a.tile_prob[t];
-      if (warp_done(a.done, k)) continue;
+    for_warp_tiles(wt, gw, NW, live, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t k) {
       int m = lane == 0 ? __ldcg(a.upd + k) : 0;
       m = __shfl_sync(0xffffffffu, m, 0);
       if (m == 1) {
         double acc[2] = {0.0, 0.0};
-        tile_spmv<double>(a, a.tile_r0[t], a.tile_r1[t], a.x, [&](int64_t row, double sv) {
+        tile_spmv<double>(a, tr0, tr1, a.x, [&](int64_t row, double sv) {
           const double r64 = a.b[row] - sv;
           const float rf = (float)r64;
           const float zf = a.d32[row] * rf;
@@ -391,13 +417,13 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
         tile_partial<2>(acc, a.P, a.ntiles, t, 4);
       } else {
         double acc[1] = {0.0};
-        tile_spmv<float>(a, a.tile_r0[t], a.tile_r1[t], a.p32, [&](int64_t row, float sv) {
+        tile_spmv<float>(a, tr0, tr1, a.p32, [&](int64_t row, float sv) {
           a.q32[row] = sv;
           acc[0] += (double)__ldcg(a.p32 + row) * (double)sv;
         });
         tile_partial<1>(acc, a.P, a.ntiles, t, 3);
       }
-    }
+    });
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
       if (block_done(a.done, k)) continue;
@@ -434,15 +460,12 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
     }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     // ---- phase 2 (mode 0): x += alpha p (FP64), r -= alpha q, z = D^-1 r (FP32); <r, z>, <r, r>
-    for (int32_t t = gw; t < a.ntiles; t += NW) {
-      const int32_t k = a.tile_prob[t];
-      if (warp_done(a.done, k)) continue;
-      int m = lane == 0 ? __ldcg(a.upd + k) : 0;
-      if (__shfl_sync(0xffffffffu, m, 0) != 0) continue;
+    auto normal = [&](int32_t k) { return live(k) && __ldcg(a.upd + k) == 0; };
+    for_warp_tiles(wt, gw, NW, normal, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t k) {
       const double al = __ldcg(alpha + k);
       const float alf = (float)al;
       double acc[2] = {0.0, 0.0};
-      for (int32_t i = a.tile_r0[t] + lane; i < a.tile_r1[t]; i += 32) {
+      for (int32_t i = tr0 + lane; i < tr1; i += 32) {
         const float pi = __ldcg(a.p32 + i);
         a.x[i] = a.x[i] + al * (double)pi;
         const float ri = fmaf(-alf, __ldcg(a.q32 + i), __ldcg(a.r32 + i));
@@ -453,7 +476,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
         acc[1] += (double)ri * (double)ri;
       }
       tile_partial<2>(acc, a.P, a.ntiles, t, 4);
-    }
+    });
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
       if (block_done(a.done, k)) continue;
@@ -483,28 +506,25 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
     }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     // ---- phase 3 (modes 0 and the one after a replacement): p = z + beta p
-    for (int32_t t = gw; t < a.ntiles; t += NW) {
-      const int32_t k = a.tile_prob[t];
-      if (warp_done(a.done, k)) continue;
-      int m = lane == 0 ? __ldcg(a.upd + k) : 0;
-      if (__shfl_sync(0xffffffffu, m, 0) == 1) continue;
+    auto stepping = [&](int32_t k) { return live(k) && __ldcg(a.upd + k) != 1; };
+    for_warp_tiles(wt, gw, NW, stepping, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t k) {
       const float be = (float)__ldcg(beta + k);
-      for (int32_t i = a.tile_r0[t] + lane; i < a.tile_r1[t]; i += 32)
+      for (int32_t i = tr0 + lane; i < tr1; i += 32)
         a.p32[i] = fmaf(be, __ldcg(a.p32 + i), __ldcg(a.z32 + i));
-    }
+    });
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   }
   // ---- phase R: per-problem ||b - A x||, ||b|| (FP64)
-  for (int32_t t = gw; t < a.ntiles; t += NW) {
+  for_warp_tiles(wt, gw, NW, every, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t) {
     double acc[2] = {0.0, 0.0};
-    tile_spmv<double>(a, a.tile_r0[t], a.tile_r1[t], a.x, [&](int64_t row, double s) {
+    tile_spmv<double>(a, tr0, tr1, a.x, [&](int64_t row, double s) {
       const double bi = a.b[row];
       const double w = bi - s;
       acc[0] += w * w;
       acc[1] += bi * bi;
     });
     tile_partial<2>(acc, a.P, a.ntiles, t, 5);
-  }
+  });
   if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   FEMK_OWNER_LOOP {
     const double ww = prob_sum(a, 5, k), bb = prob_sum(a, 6, k);
@@ -548,22 +568,34 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
   FEMK_CHECK_ARG(pc->coop, "femk_pcg_batched: the device does not support cooperative launch");
   femk_plan* p = const_cast<femk_plan*>(pc);
   FEMK_CHECK_ARG(row_off[0] == 0 && row_off[nprob] == p->n, "femk_pcg_batched: row_off must span [0, n)");
+  for (int32_t k = 0; k < nprob; ++k) FEMK_CHECK_ARG(row_off[k + 1] > row_off[k], "femk_pcg_batched: empty problem");
+  const void* kern = mixed ? (const void*)k_batch_mixed : (const void*)k_batch_pcg;
+  const int per_sm = std::min(blocks_per_sm, resident_blocks(kern, kBT));
+  const int grid = p->n_sm * std::max(1, per_sm);
+  const int64_t nwarps = (int64_t)grid * (kBT / 32);
   // tiles: on the sliced-ELL copy they end on global multiples of tile_rows (rounded up to a whole
-  // slice), so only the first and last tile of a problem cover part of a slice
+  // slice), so only the first and last tile of a problem cover part of a slice. A warp holds at
+  // most 32 tiles (one per lane), so tile_rows doubles until the tiles fit.
   const bool sell = p->use_sell && p->sell_cols;
-  const int64_t tr = sell ? (tile_rows + 31) / 32 * 32 : tile_rows;
+  int64_t tr = sell ? (tile_rows + 31) / 32 * 32 : tile_rows;
   std::vector<int32_t> r0, r1, tp, t0(nprob), t1(nprob);
-  for (int32_t k = 0; k < nprob; ++k) {
-    FEMK_CHECK_ARG(row_off[k + 1] > row_off[k], "femk_pcg_batched: empty problem");
-    t0[k] = (int32_t)r0.size();
-    for (int64_t s0 = row_off[k]; s0 < row_off[k + 1];) {
-      const int64_t e = std::min<int64_t>(sell ? (s0 / tr + 1) * tr : s0 + tr, row_off[k + 1]);
-      r0.push_back((int32_t)s0);
-      r1.push_back((int32_t)e);
-      tp.push_back(k);
-      s0 = e;
+  while (true) {
+    r0.clear();
+    r1.clear();
+    tp.clear();
+    for (int32_t k = 0; k < nprob; ++k) {
+      t0[k] = (int32_t)r0.size();
+      for (int64_t s0 = row_off[k]; s0 < row_off[k + 1];) {
+        const int64_t e = std::min<int64_t>(sell ? (s0 / tr + 1) * tr : s0 + tr, row_off[k + 1]);
+        r0.push_back((int32_t)s0);
+        r1.push_back((int32_t)e);
+        tp.push_back(k);
+        s0 = e;
+      }
+      t1[k] = (int32_t)r0.size();
     }
-    t1[k] = (int32_t)r0.size();
+    if ((int64_t)r0.size() <= 32 * nwarps) break;
+    tr *= 2;
   }
   const int32_t ntiles = (int32_t)r0.size();
   cudaStream_t s = (cudaStream_t)stream;
@@ -647,7 +679,8 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
   // tile tables: uploaded only when the schedule changes (pageable copies stay outside the graph)
   uint64_t h = 1469598103934665603ull;
   for (int32_t k = 0; k <= nprob; ++k) h = (h ^ (uint64_t)row_off[k]) * 1099511628211ull;
-  h = (h ^ (uint64_t)tile_rows) * 1099511628211ull;
+  h = (h ^ (uint64_t)tr) * 1099511628211ull;
+  h = (h ^ (uint64_t)grid) * 1099511628211ull;
   const bool same_tiles = p->batch_key[0] == (const void*)(uintptr_t)h && p->batch_key[1] == p->batch_ws;
   if (!same_tiles) {
     FEMK_CUDA_TRY(cudaMemcpyAsync(ib, r0.data(), 4 * ntiles, cudaMemcpyHostToDevice, s));
@@ -656,9 +689,6 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
     FEMK_CUDA_TRY(cudaMemcpyAsync(ib + 3 * ntiles, t0.data(), 4 * nprob, cudaMemcpyHostToDevice, s));
     FEMK_CUDA_TRY(cudaMemcpyAsync(ib + 3 * ntiles + nprob, t1.data(), 4 * nprob, cudaMemcpyHostToDevice, s));
   }
-  const void* kern = mixed ? (const void*)k_batch_mixed : (const void*)k_batch_pcg;
-  const int per_sm = std::min(blocks_per_sm, resident_blocks(kern, kBT));
-  const int grid = p->n_sm * std::max(1, per_sm);
   const int cgrid = blocks_for(p->nnz, 256, p->n_sm * 8);
   // the solve itself (reset + one cooperative launch) is one CUDA graph, replayed while the
   // operands and the schedule stay the same; a device that refuses to capture the cooperative

