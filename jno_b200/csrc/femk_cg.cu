@@ -529,21 +529,37 @@ __global__ void __launch_bounds__(128, ND == 10 ? 6 : 8) k_matfree(const double*
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ntet; c += (int64_t)gridDim.x * blockDim.x) {
     int32_t dof[ND];
     double xe[ND];
+    if constexpr (ND == 4) {  // one 16-byte load (mcells is 256-byte aligned, c * 16 bytes in)
+      const int4 d4 = __ldg(reinterpret_cast<const int4*>(mcells) + c);
+      dof[0] = d4.x;
+      dof[1] = d4.y;
+      dof[2] = d4.z;
+      dof[3] = d4.w;
+    } else {
 #pragma unroll
-    for (int a = 0; a < ND; ++a) {
-      dof[a] = __ldg(mcells + c * ND + a);
-      xe[a] = dof[a] >= 0 ? __ldg(x + dof[a]) : 0.0;
+      for (int a = 0; a < ND; ++a) dof[a] = __ldg(mcells + c * ND + a);
     }
+#pragma unroll
+    for (int a = 0; a < ND; ++a) xe[a] = dof[a] >= 0 ? __ldg(x + dof[a]) : 0.0;
     int32_t v[NV];
 #pragma unroll
     for (int i = 0; i < NV; ++i) v[i] = dof[i] >= 0 ? dof[i] : -1 - dof[i];
-    Geom<NV> T;
-    cell_geometry(xyz, v, T);
-    double VG[NV][NV];
-    gram(T, VG);
     const double k = coef_of(param, mode, scale, c);
     double ye[ND];
-    khat_apply<ND>(VG, xe, ye);
+    if constexpr (!Cell<ND>::P2) {
+      double P[NV][3];
+#pragma unroll
+      for (int i = 0; i < NV; ++i)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) P[i][q] = (q < NV - 1) ? __ldg(xyz + (int64_t)v[i] * 3 + q) : 0.0;
+      p1_apply(P, xe, ye);
+    } else {
+      Geom<NV> T;
+      cell_geometry(xyz, v, T);
+      double VG[NV][NV];
+      gram(T, VG);
+      khat_apply<ND>(VG, xe, ye);
+    }
 #pragma unroll
     for (int a = 0; a < ND; ++a)
       if (dof[a] >= 0) atomicAdd(y + dof[a], k * ye[a]);

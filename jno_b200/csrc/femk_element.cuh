@@ -193,6 +193,50 @@ __device__ __forceinline__ double khat(const double VG[Cell<ND>::NV][Cell<ND>::N
   return 4.0 * (VG[i][j] * cil + VG[i][l] * cij);
 }
 
+// P1 element product ye = K_hat xe (unit coefficient) straight from the vertex coordinates P, without
+// the barycentric gradients or the Gram matrix. Tetrahedron: edges e_b = P_b - P_0, c_1 = e_2 x e_3,
+// c_2 = e_3 x e_1, c_3 = e_1 x e_2 (det = e_1 . c_1, g_b = c_b / det) and w = sum_{b>=1} (x_b - x_0) c_b;
+// then ye_a = V g_a . grad u = (c_a . w) / (6 |det|) for a >= 1, and ye_0 = -(ye_1 + ye_2 + ye_3)
+// (the rows of K_hat sum to zero). Triangle: r_1 = (e_2y, -e_2x), r_2 = (-e_1y, e_1x),
+// det = e_1x e_2y - e_1y e_2x, ye_a = (r_a . w) / (2 |det|). About 60 FP64 operations for a
+// tetrahedron against ~140 through g and the Gram matrix; the same values up to rounding.
+__device__ __forceinline__ void p1_apply(const double (&P)[4][3], const double (&xe)[4], double (&ye)[4]) {
+  double e[3][3];
+#pragma unroll
+  for (int b = 0; b < 3; ++b)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) e[b][k] = P[b + 1][k] - P[0][k];
+  double c[3][3];
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    const double* u = e[(b + 1) % 3];
+    const double* v = e[(b + 2) % 3];
+    c[b][0] = u[1] * v[2] - u[2] * v[1];
+    c[b][1] = u[2] * v[0] - u[0] * v[2];
+    c[b][2] = u[0] * v[1] - u[1] * v[0];
+  }
+  const double det = e[0][0] * c[0][0] + e[0][1] * c[0][1] + e[0][2] * c[0][2];
+  double w[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    w[k] = (xe[1] - xe[0]) * c[0][k] + (xe[2] - xe[0]) * c[1][k] + (xe[3] - xe[0]) * c[2][k];
+  const double s = 1.0 / (6.0 * fabs(det));
+#pragma unroll
+  for (int b = 0; b < 3; ++b) ye[b + 1] = (c[b][0] * w[0] + c[b][1] * w[1] + c[b][2] * w[2]) * s;
+  ye[0] = -(ye[1] + ye[2] + ye[3]);
+}
+__device__ __forceinline__ void p1_apply(const double (&P)[3][3], const double (&xe)[3], double (&ye)[3]) {
+  const double e1x = P[1][0] - P[0][0], e1y = P[1][1] - P[0][1];
+  const double e2x = P[2][0] - P[0][0], e2y = P[2][1] - P[0][1];
+  const double det = e1x * e2y - e1y * e2x;
+  const double d1 = xe[1] - xe[0], d2 = xe[2] - xe[0];
+  const double wx = d1 * e2y - d2 * e1y, wy = -d1 * e2x + d2 * e1x;  // w = d1 r_1 + d2 r_2
+  const double s = 1.0 / (2.0 * fabs(det));
+  ye[1] = (e2y * wx - e2x * wy) * s;
+  ye[2] = (-e1y * wx + e1x * wy) * s;
+  ye[0] = -(ye[1] + ye[2]);
+}
+
 // ye = K_hat xe for one element (unit coefficient) without forming the ND x ND matrix.
 // P1: ye_a = sum_b VG[a][b] xe_b.
 // P2: u = sum_a xe_a phi_a has grad u = sum_j G_j g_j with G_j = du/dlambda_j affine in the
