@@ -8,11 +8,12 @@
 // warp t mod W, W = warps in the grid, no block-wide synchronisation inside a phase). The products
 // run on the plan's sliced-ELL copy (lane per row; copied from the CSR values in the same graph),
 // with the vectors gathered through L1 (the barriers' acquire makes other blocks' writes visible):
-//   phase 0 (once): r = b - A x0, z = D^-1 r, p = z, per-tile <r,z>, <r,r>, <b,b>
-//   phase 1: q = A p, per-tile <p, q>          | owner pass: alpha_k
-//   phase 2: x, r, z updates, <r,z>, <r,r>     | owner pass: beta_k, stop test of problem k
-//   phase 3: p = z + beta_k p
+//   phase 0 (once): r = b - A x0, z = D^-1 r, per-tile <r,z>, <r,r>, <b,b> | owner pass: beta_k = 0
+//   phase 1: w = A z, p = z + beta_k p, q = w + beta_k q, per-tile <p, q>   | owner pass: alpha_k
+//   phase 2: x, r, z updates, <r,z>, <r,r>   | owner pass: beta_k, stop test of problem k
 //   phase R (once): per-problem ||b - A x|| for the residual guard
+// q = A p is carried by the recurrence A (z + beta p) = A z + beta A p, so the direction update
+// rides in the product phase: an iteration is two row phases, two owner passes, four grid barriers.
 // After every reduction phase an owner pass (block b finishes problems b, b + G, ...) sums the
 // problem's tile partials in a fixed order and writes its scalars, so tiles can be small (the
 // largest problems keep every SM busy after the small ones have converged) without each tile
@@ -24,7 +25,7 @@
 // FP64 reliable updates, as femk_pcg_mixed does for one problem: when its FP32 <r, r> fell by
 // delta2 since the last update, met the stop test or hit the cap, the problem's next phase 1
 // replaces r by fp32(b - A x) with the FP64 values in place of its FP32 product, keeps the
-// direction, and retires the problem once the FP64 residual meets the stop rule. A replacement thus
+// direction (p and q = A p), and retires the problem once the FP64 residual meets the stop rule. A replacement thus
 // costs the problem one step slot and no extra phase or grid barrier.
 #include <algorithm>
 #include <cmath>
@@ -93,13 +94,16 @@ struct GatherPlain {
   __device__ __forceinline__ V operator()(int32_t j) const { return x[j]; }
 };
 
-// One warp computes (A v)[row] for the rows of its tile; the epilogue functor sees (row, Av).
-// V = double: the FP64 values; V = float: the FP32 values (FP32 accumulation). On the sliced-ELL
-// copy a lane owns a row of each 32-row slice the tile covers (tiles start and end on slice
-// boundaries except at the ends of a problem), with every value and column load independent of the
-// others; on the CSR kL lanes share a row.
-template <typename V = double, typename F>
-__device__ __forceinline__ void tile_spmv(const BatchArgs& a, int32_t r0, int32_t r1, const V* v, F&& epi) {
+// One warp computes (A v)[row] for the rows of its tile. pre(row, ok) issues the row's own epilogue
+// loads ahead of the product's (ok false: the lane has no row in this slice, load nothing) and
+// returns them; post(row, Av, pre's values) finishes the row. V = double: the FP64 values; V = float:
+// the FP32 values (FP32 accumulation). On the sliced-ELL copy a lane owns a row of each 32-row slice
+// the tile covers (tiles start and end on slice boundaries except at the ends of a problem), every
+// value and column load is independent of the others, and the next slice's offset is read while the
+// current slice runs; on the CSR kL lanes share a row.
+template <typename V = double, typename Pre, typename Post>
+__device__ __forceinline__ void tile_product(const BatchArgs& a, int32_t r0, int32_t r1, const V* v, Pre&& pre,
+                                             Post&& post) {
   const int lane = threadIdx.x & 31;
   if (a.sptr) {
     const V* vals;
@@ -107,16 +111,21 @@ __device__ __forceinline__ void tile_spmv(const BatchArgs& a, int32_t r0, int32_
       vals = a.svals;
     else
       vals = a.svals32;
-    for (int32_t s = r0 >> 5; s <= (r1 - 1) >> 5; ++s) {
+    const int32_t s0 = r0 >> 5, s1 = (r1 - 1) >> 5;
+    int64_t b0 = __ldg(a.sptr + s0), b1 = __ldg(a.sptr + s0 + 1);
+    for (int32_t s = s0; s <= s1; ++s) {
+      const int64_t b2 = s < s1 ? __ldg(a.sptr + s + 2) : b1;
       const int32_t row = s * 32 + lane;
-      if (row < r0 || row >= r1) continue;
-      const int64_t b0 = __ldg(a.sptr + s);
-      const int32_t w = (int32_t)((__ldg(a.sptr + s + 1) - b0) >> 5);
+      const bool ok = row >= r0 && row < r1;
+      const auto ld = pre(row, ok);
       // entries in flight per lane: 16 FP32 (half the bytes each) or 8 FP64
       constexpr int EB = sizeof(V) == 4 ? 16 : 8;
+      const int32_t w = ok ? (int32_t)((b1 - b0) >> 5) : 0;
       const V acc = a.sc16 ? sell_row<V, int16_t, EB>(vals + b0 + lane, a.sc16 + b0 + lane, w, row, GatherPlain<V>{v})
                            : sell_row<V, int32_t, EB>(vals + b0 + lane, a.scols + b0 + lane, w, row, GatherPlain<V>{v});
-      epi((int64_t)row, acc);
+      if (ok) post((int64_t)row, acc, ld);
+      b0 = b1;
+      b1 = b2;
     }
     return;
   }
@@ -133,25 +142,71 @@ __device__ __forceinline__ void tile_spmv(const BatchArgs& a, int32_t r0, int32_
     csr_rows_g<kL, kU, V, int32_t>(a.indptr, a.indices, vals, GatherPlain<V>{v}, r1, base, lane, sv, rows);
 #pragma unroll
     for (int u = 0; u < kU; ++u)
-      if (rows[u] < r1 && sub == 0) epi(rows[u], sv[u]);
+      if (rows[u] < r1 && sub == 0) post(rows[u], sv[u], pre(rows[u], true));
   }
 }
 
-// sum of problem k's tile partials P[j][t], t in [t0, t1): whole block, fixed order, broadcast
-__device__ __forceinline__ double prob_sum(const BatchArgs& a, int j, int32_t k) {
-  __shared__ double part[kBT / 32];
-  const int32_t t0 = a.prob_t0[k], t1 = a.prob_t1[k];
-  double t = 0.0;
-  for (int32_t i = t0 + threadIdx.x; i < t1; i += kBT) t += __ldcg(a.P + (int64_t)j * a.ntiles + i);
+// The rows [r0, r1) of a tile, S trips of 32 at a time: load(i) for all S rows of a round first
+// (every load of a round in flight together; the stores of a trip may alias the next trip's loads),
+// then step(i, loaded values). The kernels use S = 1: at 2 blocks of 512 threads per SM (64
+// registers a thread) S = 2 or 4 spilled and the FP64 batch took 50.7 ms against 44.7 ms, and one
+// block per SM with S = 4 (104-118 registers) took 66 ms.
+template <int S, typename Load, typename Step>
+__device__ __forceinline__ void tile_rows(int32_t r0, int32_t r1, Load&& load, Step&& step) {
+  const int lane = threadIdx.x & 31;
+  for (int32_t i0 = r0 + lane; i0 < r1; i0 += 32 * S) {
+    decltype(load(i0)) v[S];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = t;
-  __syncthreads();
-  double out = 0.0;
+    for (int u = 0; u < S; ++u)
+      if (i0 + 32 * u < r1) v[u] = load(i0 + 32 * u);
 #pragma unroll
-  for (int w = 0; w < kBT / 32; ++w) out += part[w];
+    for (int u = 0; u < S; ++u)
+      if (i0 + 32 * u < r1) step(i0 + 32 * u, v[u]);
+  }
+}
+
+// Problem k's sums of the tile partials P[slot[j]][t], t in [t0, t1), for NV slots at once (whole
+// block, fixed order, broadcast), with done[k] and the mixed form's mode read in the same round: one
+// pair of block barriers per owner pass instead of one per sum and flag.
+struct ProbFlags {
+  int32_t done, mode;
+};
+template <int NV>
+__device__ __forceinline__ ProbFlags prob_sums(const BatchArgs& a, const int (&slot)[NV], int32_t k, bool mode,
+                                               double (&out)[NV]) {
+  __shared__ double part[NV][kBT / 32];
+  __shared__ ProbFlags fl;
+  const int32_t t0 = __ldg(a.prob_t0 + k), t1 = __ldg(a.prob_t1 + k);
+  if (threadIdx.x == 0) {
+    fl.done = __ldcg(a.done + k);
+    fl.mode = mode ? __ldcg(a.upd + k) : 0;
+  }
+  double t[NV];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) t[j] = 0.0;
+  for (int32_t i = t0 + threadIdx.x; i < t1; i += kBT)
+#pragma unroll
+    for (int j = 0; j < NV; ++j) t[j] += __ldcg(a.P + (int64_t)slot[j] * a.ntiles + i);
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t[j] += __shfl_xor_sync(0xffffffffu, t[j], o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) part[j][threadIdx.x >> 5] = t[j];
+  }
   __syncthreads();
-  return out;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double v = 0.0;
+#pragma unroll
+    for (int w = 0; w < kBT / 32; ++w) v += part[j][w];
+    out[j] = v;
+  }
+  const ProbFlags f = fl;
+  __syncthreads();
+  return f;
 }
 
 // warp sum of NV values, stored by lane 0 as tile t's partials P[slot0 + j][t]
@@ -165,17 +220,6 @@ __device__ __forceinline__ void tile_partial(double (&v)[NV], double* P, int nti
 #pragma unroll
     for (int j = 0; j < NV; ++j) P[(int64_t)(slot0 + j) * ntiles + t] = v[j];
   }
-}
-
-// done[k] read once per block (a problem's owner may retire it while other blocks run its tiles;
-// every thread of a block must take the same branch around the barriers inside the tile loop)
-__device__ __forceinline__ bool block_done(const int32_t* done, int32_t k) {
-  __shared__ int32_t d;
-  if (threadIdx.x == 0) d = __ldcg(done + k);
-  __syncthreads();
-  const bool out = d != 0;
-  __syncthreads();
-  return out;
 }
 
 __device__ __forceinline__ void retire(const BatchArgs& a, int32_t k, int32_t status) {
@@ -219,43 +263,83 @@ __device__ __forceinline__ void for_warp_tiles(const WarpTiles& w, int32_t gw, i
   }
 }
 
+// As for_warp_tiles, and lane j also fetches scalar(k) and tag(k) for the warp's tile j, so a
+// phase that needs a per-problem scalar (alpha_k, beta_k) or mode bit reads them for all of the
+// warp's tiles in one load per lane: body(t, r0, r1, k, scalar, tag).
+template <typename Keep, typename Scalar, typename Tag, typename Body>
+__device__ __forceinline__ void for_warp_tiles_s(const WarpTiles& w, int32_t gw, int32_t NW, Keep&& keep,
+                                                 Scalar&& scalar, Tag&& tag, Body&& body) {
+  const int lane = threadIdx.x & 31;
+  double sc = 0.0;
+  bool mine = false, tg = false;
+  if (lane < w.count) {  // independent loads, all in flight together
+    sc = scalar(w.k);
+    mine = keep(w.k);
+    tg = tag(w.k);
+  }
+  const unsigned int tags = __ballot_sync(0xffffffffu, mine && tg);
+  unsigned int mask = __ballot_sync(0xffffffffu, mine);
+  while (mask) {
+    const int j = __ffs(mask) - 1;
+    mask &= mask - 1;
+    body(gw + j * NW, __shfl_sync(0xffffffffu, w.r0, j), __shfl_sync(0xffffffffu, w.r1, j),
+         __shfl_sync(0xffffffffu, w.k, j), __shfl_sync(0xffffffffu, sc, j), ((tags >> j) & 1u) != 0u);
+  }
+}
+
 // Owner pass: block b finishes problems k = b, b + G, ... from their tile partials.
 #define FEMK_OWNER_LOOP for (int32_t k = blockIdx.x; k < a.nprob; k += gridDim.x)
+
+// the vector operands of one row in the update phases
+struct RowF64 {
+  double x, p, r, q, d;
+};
+struct RowMixed {
+  double x;
+  float p, q, r, d;
+};
 
 __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
   unsigned int gen = 0;
   const int32_t gw = (int32_t)((blockIdx.x * (int64_t)kBT + threadIdx.x) >> 5);  // global warp
   const int32_t NW = (int32_t)(((int64_t)gridDim.x * kBT) >> 5);
-  const int lane = threadIdx.x & 31;
   const WarpTiles wt = warp_tiles(a, gw, NW);
   auto every = [](int32_t) { return true; };
   auto live = [&](int32_t k) { return __ldcg(a.done + k) == 0; };
+  auto no_tag = [](int32_t) { return false; };
+  // per-problem step scalars: beta (read by phase 1, written by the second owner pass) and alpha
+  // (written by the first owner pass, read by phase 2) are never live together and share a slot
+  double* alpha = a.gam + a.nprob;
+  double* beta = alpha;
   // ---- phase 0: residual of x0
   for_warp_tiles(wt, gw, NW, every, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t) {
-    const int32_t r0 = tr0, r1 = tr1;
     double acc[3] = {0.0, 0.0, 0.0};
-    tile_spmv(a, r0, r1, a.x, [&](int64_t row, double s) {
-      const double bi = a.b[row];
-      const double ri = bi - s;
-      const double zi = a.dinv ? a.dinv[row] * ri : ri;
-      a.r[row] = ri;
-      a.z[row] = zi;
-      a.p[row] = zi;
-      acc[0] += ri * zi;
-      acc[1] += ri * ri;
-      acc[2] += bi * bi;
-    });
+    tile_product(
+        a, tr0, tr1, a.x,
+        [&](int64_t row, bool ok) { return make_double2(ok ? a.b[row] : 0.0, ok && a.dinv ? a.dinv[row] : 1.0); },
+        [&](int64_t row, double s, double2 bd) {
+          const double ri = bd.x - s;
+          const double zi = a.dinv ? bd.y * ri : ri;
+          a.r[row] = ri;
+          a.z[row] = zi;
+          acc[0] += ri * zi;
+          acc[1] += ri * ri;
+          acc[2] += bd.x * bd.x;
+        });
     tile_partial<3>(acc, a.P, a.ntiles, t, 0);
   });
   if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   FEMK_OWNER_LOOP {
-    const double rz = prob_sum(a, 0, k), rr = prob_sum(a, 1, k), bb = prob_sum(a, 2, k);
+    double v[3];
+    prob_sums<3>(a, {0, 1, 2}, k, false, v);
+    const double rz = v[0], rr = v[1], bb = v[2];
     if (threadIdx.x == 0) {
       const double at2 = fmax(a.tol2 * bb, a.atol2_abs);
       a.gam[k] = rz;
       a.rr[k] = rr;
       a.atol2[k] = at2;
       a.iter[k] = 0;
+      beta[k] = 0.0;  // the first direction is z itself
       const double rs = a.dinv ? rr : rz;
       if (!isfinite(rz) || !isfinite(rr))
         retire(a, k, FEMK_NONFINITE);
@@ -264,22 +348,40 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
     }
   }
   if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
-  double* alpha = a.gam + a.nprob;  // per-problem step scalars of the current iteration
-  double* beta = alpha;             // (alpha is dead once phase 2 is done; beta reuses the slot)
   while (ld_acquire_u32((const unsigned int*)a.active) != 0u) {
-    // ---- phase 1: q = A p, <p, q>
-    for_warp_tiles(wt, gw, NW, live, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t k) {
-      double acc[1] = {0.0};
-      tile_spmv(a, tr0, tr1, a.p, [&](int64_t row, double s) {
-        a.q[row] = s;
-        acc[0] += __ldcg(a.p + row) * s;
-      });
-      tile_partial<1>(acc, a.P, a.ntiles, t, 3);
-    });
+    // ---- phase 1: w = A z; p = z + beta p; q = w + beta q (= A p); <p, q>
+    for_warp_tiles_s(
+        wt, gw, NW, live, [&](int32_t k) { return __ldcg(beta + k); }, no_tag,
+        [&](int32_t t, int32_t tr0, int32_t tr1, int32_t, double be, bool) {
+          const bool step = be != 0.0;
+          double acc[1] = {0.0};
+          tile_product(
+              a, tr0, tr1, a.z,
+              [&](int64_t row, bool ok) {
+                double3 v = make_double3(0.0, 0.0, 0.0);
+                if (ok) {
+                  v.x = __ldcg(a.z + row);
+                  if (step) {
+                    v.y = __ldcg(a.p + row);
+                    v.z = __ldcg(a.q + row);
+                  }
+                }
+                return v;
+              },
+              [&](int64_t row, double w, double3 v) {
+                const double pi = step ? fma(be, v.y, v.x) : v.x;
+                const double qi = step ? fma(be, v.z, w) : w;
+                a.p[row] = pi;
+                a.q[row] = qi;
+                acc[0] += pi * qi;
+              });
+          tile_partial<1>(acc, a.P, a.ntiles, t, 3);
+        });
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
-      if (block_done(a.done, k)) continue;
-      const double pq = prob_sum(a, 3, k);
+      double v[1];
+      if (prob_sums<1>(a, {3}, k, false, v).done) continue;
+      const double pq = v[0];
       if (threadIdx.x == 0) {
         if (!(pq > 0.0) || !isfinite(pq))
           retire(a, k, isfinite(pq) ? FEMK_BREAKDOWN : FEMK_NONFINITE);
@@ -289,24 +391,37 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
     }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     // ---- phase 2: x, r, z updates; <r, z>, <r, r>
-    for_warp_tiles(wt, gw, NW, live, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t k) {
-      const double al = __ldcg(alpha + k);
-      double acc[2] = {0.0, 0.0};
-      for (int32_t i = tr0 + lane; i < tr1; i += 32) {
-        a.x[i] = a.x[i] + al * __ldcg(a.p + i);
-        const double ri = __ldcg(a.r + i) - al * __ldcg(a.q + i);
-        const double zi = a.dinv ? a.dinv[i] * ri : ri;
-        a.r[i] = ri;
-        a.z[i] = zi;
-        acc[0] += ri * zi;
-        acc[1] += ri * ri;
-      }
-      tile_partial<2>(acc, a.P, a.ntiles, t, 4);
-    });
+    for_warp_tiles_s(
+        wt, gw, NW, live, [&](int32_t k) { return __ldcg(alpha + k); }, no_tag,
+        [&](int32_t t, int32_t tr0, int32_t tr1, int32_t, double al, bool) {
+          double acc[2] = {0.0, 0.0};
+          tile_rows<1>(
+              tr0, tr1,
+              [&](int32_t i) {
+                RowF64 v;
+                v.x = a.x[i];
+                v.p = __ldcg(a.p + i);
+                v.r = __ldcg(a.r + i);
+                v.q = __ldcg(a.q + i);
+                v.d = a.dinv ? a.dinv[i] : 1.0;
+                return v;
+              },
+              [&](int32_t i, const RowF64& v) {
+                a.x[i] = v.x + al * v.p;
+                const double ri = v.r - al * v.q;
+                const double zi = a.dinv ? v.d * ri : ri;
+                a.r[i] = ri;
+                a.z[i] = zi;
+                acc[0] += ri * zi;
+                acc[1] += ri * ri;
+              });
+          tile_partial<2>(acc, a.P, a.ntiles, t, 4);
+        });
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
-      if (block_done(a.done, k)) continue;
-      const double rz = prob_sum(a, 4, k), rr = prob_sum(a, 5, k);
+      double v[2];
+      if (prob_sums<2>(a, {4, 5}, k, false, v).done) continue;
+      const double rz = v[0], rr = v[1];
       if (threadIdx.x == 0) {
         const int32_t itk = a.iter[k] + 1;
         const double rs = a.dinv ? rr : rz;
@@ -319,28 +434,24 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
       }
     }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
-    // ---- phase 3: p = z + beta p
-    for_warp_tiles(wt, gw, NW, live, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t k) {
-      const double be = __ldcg(beta + k);
-      for (int32_t i = tr0 + lane; i < tr1; i += 32)
-        a.p[i] = __ldcg(a.z + i) + be * __ldcg(a.p + i);
-    });
-    if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   }
   // ---- phase R: per-problem ||b - A x||, ||b||
   for_warp_tiles(wt, gw, NW, every, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t) {
     double acc[2] = {0.0, 0.0};
-    tile_spmv(a, tr0, tr1, a.x, [&](int64_t row, double s) {
-      const double bi = a.b[row];
-      const double w = bi - s;
-      acc[0] += w * w;
-      acc[1] += bi * bi;
-    });
+    tile_product(
+        a, tr0, tr1, a.x, [&](int64_t row, bool ok) { return ok ? a.b[row] : 0.0; },
+        [&](int64_t, double s, double bi) {
+          const double w = bi - s;
+          acc[0] += w * w;
+          acc[1] += bi * bi;
+        });
     tile_partial<2>(acc, a.P, a.ntiles, t, 5);
   });
   if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   FEMK_OWNER_LOOP {
-    const double ww = prob_sum(a, 5, k), bb = prob_sum(a, 6, k);
+    double v[2];
+    prob_sums<2>(a, {5, 6}, k, false, v);
+    const double ww = v[0], bb = v[1];
     if (threadIdx.x == 0) a.relres[k] = sqrt(ww) / (sqrt(bb) + 1e-30);
   }
 }
@@ -349,32 +460,37 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
   unsigned int gen = 0;
   const int32_t gw = (int32_t)((blockIdx.x * (int64_t)kBT + threadIdx.x) >> 5);  // global warp
   const int32_t NW = (int32_t)(((int64_t)gridDim.x * kBT) >> 5);
-  const int lane = threadIdx.x & 31;
   const WarpTiles wt = warp_tiles(a, gw, NW);
   auto every = [](int32_t) { return true; };
   auto live = [&](int32_t k) { return __ldcg(a.done + k) == 0; };
+  auto no_tag = [](int32_t) { return false; };
+  double* alpha = a.gam + a.nprob;
+  double* beta = alpha;
   // ---- phase 0: FP64 residual of x0, FP32 copies; <r, z> (FP32 data), <r64, r64>, <b, b>
   for_warp_tiles(wt, gw, NW, every, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t) {
     double acc[3] = {0.0, 0.0, 0.0};
-    tile_spmv<double>(a, tr0, tr1, a.x, [&](int64_t row, double s) {
-      const double bi = a.b[row];
-      const double r64 = bi - s;
-      const float d = a.dinv ? (float)a.dinv[row] : 1.0f;
-      const float rf = (float)r64;
-      const float zf = d * rf;
-      a.d32[row] = d;
-      a.r32[row] = rf;
-      a.z32[row] = zf;
-      a.p32[row] = zf;
-      acc[0] += (double)rf * (double)zf;
-      acc[1] += r64 * r64;
-      acc[2] += bi * bi;
-    });
+    tile_product<double>(
+        a, tr0, tr1, a.x,
+        [&](int64_t row, bool ok) { return make_double2(ok ? a.b[row] : 0.0, ok && a.dinv ? a.dinv[row] : 1.0); },
+        [&](int64_t row, double s, double2 bd) {
+          const double r64 = bd.x - s;
+          const float d = a.dinv ? (float)bd.y : 1.0f;
+          const float rf = (float)r64;
+          const float zf = d * rf;
+          a.d32[row] = d;
+          a.r32[row] = rf;
+          a.z32[row] = zf;
+          acc[0] += (double)rf * (double)zf;
+          acc[1] += r64 * r64;
+          acc[2] += bd.x * bd.x;
+        });
     tile_partial<3>(acc, a.P, a.ntiles, t, 0);
   });
   if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   FEMK_OWNER_LOOP {
-    const double rz = prob_sum(a, 0, k), rr = prob_sum(a, 1, k), bb = prob_sum(a, 2, k);
+    double v[3];
+    prob_sums<3>(a, {0, 1, 2}, k, false, v);
+    const double rz = v[0], rr = v[1], bb = v[2];
     if (threadIdx.x == 0) {
       const double at2 = fmax(a.tol2 * bb, a.atol2_abs);
       a.gam[k] = rz;
@@ -384,6 +500,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
       a.iter[k] = 0;
       a.outer[k] = 1;
       a.upd[k] = 0;
+      beta[k] = 0.0;
       if (!isfinite(rz) || !isfinite(rr))
         retire(a, k, FEMK_NONFINITE);
       else if (!(rr > at2) || a.maxiter <= 0)
@@ -391,49 +508,67 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
     }
   }
   if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
-  double* alpha = a.gam + a.nprob;
-  double* beta = alpha;
-  // Per-problem mode (a.upd): 0 a normal step; 1 a reliable update was requested, so this
-  // iteration's phase 3 leaves p alone and the next phase 1 computes the FP64 residual in place of
-  // the FP32 product; 2 the residual was replaced in phase 1, so phase 2 skips the problem and
-  // phase 3 forms the kept direction with beta = <r, z>_new / gamma. Only the owner passes change a
-  // mode, so every phase sees one value per iteration, and no iteration needs an extra phase.
+  // Per-problem mode (a.upd): 0 a normal step; 1 a reliable update was requested, so the next
+  // phase 1 computes the FP64 residual in place of the FP32 product and leaves p and q alone; 2 the
+  // residual was replaced in phase 1, so phase 2 skips the problem and the next phase 1 forms the
+  // kept direction with beta = <r, z>_new / gamma. Only the owner passes change a mode, so every
+  // phase sees one value per iteration, and no iteration needs an extra phase.
   while (ld_acquire_u32((const unsigned int*)a.active) != 0u) {
-    // ---- phase 1: q = A32 p (FP32), <p, q>; or (mode 1) r = fp32(b - A64 x), z = D^-1 r, <r, z>, <r64, r64>
-    for_warp_tiles(wt, gw, NW, live, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t k) {
-      int m = lane == 0 ? __ldcg(a.upd + k) : 0;
-      m = __shfl_sync(0xffffffffu, m, 0);
-      if (m == 1) {
-        double acc[2] = {0.0, 0.0};
-        tile_spmv<double>(a, tr0, tr1, a.x, [&](int64_t row, double sv) {
-          const double r64 = a.b[row] - sv;
-          const float rf = (float)r64;
-          const float zf = a.d32[row] * rf;
-          a.r32[row] = rf;
-          a.z32[row] = zf;
-          acc[0] += (double)rf * (double)zf;
-          acc[1] += r64 * r64;
+    // ---- phase 1: w = A32 z, p = z + beta p, q = w + beta q (= A32 p) (FP32), <p, q>;
+    //      or (mode 1) r = fp32(b - A64 x), z = D^-1 r, <r, z>, <r64, r64>
+    for_warp_tiles_s(
+        wt, gw, NW, live, [&](int32_t k) { return __ldcg(beta + k); },
+        [&](int32_t k) { return __ldcg(a.upd + k) == 1; },
+        [&](int32_t t, int32_t tr0, int32_t tr1, int32_t, double be, bool replace) {
+          if (replace) {
+            double acc[2] = {0.0, 0.0};
+            tile_product<double>(
+                a, tr0, tr1, a.x,
+                [&](int64_t row, bool ok) { return make_double2(ok ? a.b[row] : 0.0, ok ? (double)a.d32[row] : 0.0); },
+                [&](int64_t row, double sv, double2 bd) {
+                  const double r64 = bd.x - sv;
+                  const float rf = (float)r64;
+                  const float zf = (float)bd.y * rf;
+                  a.r32[row] = rf;
+                  a.z32[row] = zf;
+                  acc[0] += (double)rf * (double)zf;
+                  acc[1] += r64 * r64;
+                });
+            tile_partial<2>(acc, a.P, a.ntiles, t, 4);
+          } else {
+            const bool step = be != 0.0;
+            const float bf = (float)be;
+            double acc[1] = {0.0};
+            tile_product<float>(
+                a, tr0, tr1, a.z32,
+                [&](int64_t row, bool ok) {
+                  float3 v = make_float3(0.0f, 0.0f, 0.0f);
+                  if (ok) {
+                    v.x = __ldcg(a.z32 + row);
+                    if (step) {
+                      v.y = __ldcg(a.p32 + row);
+                      v.z = __ldcg(a.q32 + row);
+                    }
+                  }
+                  return v;
+                },
+                [&](int64_t row, float w, float3 v) {
+                  const float pi = step ? fmaf(bf, v.y, v.x) : v.x;
+                  const float qi = step ? fmaf(bf, v.z, w) : w;
+                  a.p32[row] = pi;
+                  a.q32[row] = qi;
+                  acc[0] += (double)pi * (double)qi;
+                });
+            tile_partial<1>(acc, a.P, a.ntiles, t, 3);
+          }
         });
-        tile_partial<2>(acc, a.P, a.ntiles, t, 4);
-      } else {
-        double acc[1] = {0.0};
-        tile_spmv<float>(a, tr0, tr1, a.p32, [&](int64_t row, float sv) {
-          a.q32[row] = sv;
-          acc[0] += (double)__ldcg(a.p32 + row) * (double)sv;
-        });
-        tile_partial<1>(acc, a.P, a.ntiles, t, 3);
-      }
-    });
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
-      if (block_done(a.done, k)) continue;
-      __shared__ int32_t mode_s;
-      if (threadIdx.x == 0) mode_s = __ldcg(a.upd + k);
-      __syncthreads();
-      const int32_t mode = mode_s;
-      __syncthreads();
-      if (mode == 1) {
-        const double rz = prob_sum(a, 4, k), rr = prob_sum(a, 5, k);
+      double v[3];  // slot 3 (<p, q>) of a step, slots 4, 5 (<r, z>, <r64, r64>) of a replacement
+      const ProbFlags f = prob_sums<3>(a, {3, 4, 5}, k, true, v);
+      if (f.done) continue;
+      if (f.mode == 1) {
+        const double rz = v[1], rr = v[2];
         if (threadIdx.x == 0) {
           a.outer[k] += 1;
           a.rr[k] = rr;
@@ -449,7 +584,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
           }
         }
       } else {
-        const double pq = prob_sum(a, 3, k);
+        const double pq = v[0];
         if (threadIdx.x == 0) {
           if (!(pq > 0.0) || !isfinite(pq))
             retire(a, k, isfinite(pq) ? FEMK_BREAKDOWN : FEMK_NONFINITE);
@@ -461,42 +596,50 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     // ---- phase 2 (mode 0): x += alpha p (FP64), r -= alpha q, z = D^-1 r (FP32); <r, z>, <r, r>
     auto normal = [&](int32_t k) { return live(k) && __ldcg(a.upd + k) == 0; };
-    for_warp_tiles(wt, gw, NW, normal, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t k) {
-      const double al = __ldcg(alpha + k);
-      const float alf = (float)al;
-      double acc[2] = {0.0, 0.0};
-      for (int32_t i = tr0 + lane; i < tr1; i += 32) {
-        const float pi = __ldcg(a.p32 + i);
-        a.x[i] = a.x[i] + al * (double)pi;
-        const float ri = fmaf(-alf, __ldcg(a.q32 + i), __ldcg(a.r32 + i));
-        const float zi = a.d32[i] * ri;
-        a.r32[i] = ri;
-        a.z32[i] = zi;
-        acc[0] += (double)ri * (double)zi;
-        acc[1] += (double)ri * (double)ri;
-      }
-      tile_partial<2>(acc, a.P, a.ntiles, t, 4);
-    });
+    for_warp_tiles_s(
+        wt, gw, NW, normal, [&](int32_t k) { return __ldcg(alpha + k); }, no_tag,
+        [&](int32_t t, int32_t tr0, int32_t tr1, int32_t, double al, bool) {
+          const float alf = (float)al;
+          double acc[2] = {0.0, 0.0};
+          tile_rows<1>(
+              tr0, tr1,
+              [&](int32_t i) {
+                RowMixed v;
+                v.x = a.x[i];
+                v.p = __ldcg(a.p32 + i);
+                v.q = __ldcg(a.q32 + i);
+                v.r = __ldcg(a.r32 + i);
+                v.d = a.d32[i];
+                return v;
+              },
+              [&](int32_t i, const RowMixed& v) {
+                a.x[i] = v.x + al * (double)v.p;
+                const float ri = fmaf(-alf, v.q, v.r);
+                const float zi = v.d * ri;
+                a.r32[i] = ri;
+                a.z32[i] = zi;
+                acc[0] += (double)ri * (double)zi;
+                acc[1] += (double)ri * (double)ri;
+              });
+          tile_partial<2>(acc, a.P, a.ntiles, t, 4);
+        });
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
-      if (block_done(a.done, k)) continue;
-      __shared__ int32_t mode2_s;
-      if (threadIdx.x == 0) mode2_s = __ldcg(a.upd + k);
-      __syncthreads();
-      const int32_t mode = mode2_s;
-      __syncthreads();
-      if (mode == 2) {  // the direction step of the replaced residual runs in phase 3
+      double v[2];
+      const ProbFlags f = prob_sums<2>(a, {4, 5}, k, true, v);
+      if (f.done) continue;
+      if (f.mode == 2) {  // the direction step of the replaced residual runs in the next phase 1
         if (threadIdx.x == 0) a.upd[k] = 0;
         continue;
       }
-      const double rz = prob_sum(a, 4, k), rr = prob_sum(a, 5, k);
+      const double rz = v[0], rr = v[1];
       if (threadIdx.x == 0) {
         const int32_t itk = a.iter[k] + 1;
         a.iter[k] = itk;
         if (!isfinite(rz) || !isfinite(rr)) {
           retire(a, k, FEMK_NONFINITE);
         } else if (!(rr > a.atol2[k]) || rr < a.delta2 * a.rr_since[k] || itk >= a.maxiter) {
-          a.upd[k] = 1;  // FP64 residual replacement in the next phase 1; p stays as it is
+          a.upd[k] = 1;  // FP64 residual replacement in the next phase 1; p and q stay as they are
         } else {
           beta[k] = rz / a.gam[k];
           a.gam[k] = rz;
@@ -505,29 +648,24 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
       }
     }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
-    // ---- phase 3 (modes 0 and the one after a replacement): p = z + beta p
-    auto stepping = [&](int32_t k) { return live(k) && __ldcg(a.upd + k) != 1; };
-    for_warp_tiles(wt, gw, NW, stepping, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t k) {
-      const float be = (float)__ldcg(beta + k);
-      for (int32_t i = tr0 + lane; i < tr1; i += 32)
-        a.p32[i] = fmaf(be, __ldcg(a.p32 + i), __ldcg(a.z32 + i));
-    });
-    if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   }
   // ---- phase R: per-problem ||b - A x||, ||b|| (FP64)
   for_warp_tiles(wt, gw, NW, every, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t) {
     double acc[2] = {0.0, 0.0};
-    tile_spmv<double>(a, tr0, tr1, a.x, [&](int64_t row, double s) {
-      const double bi = a.b[row];
-      const double w = bi - s;
-      acc[0] += w * w;
-      acc[1] += bi * bi;
-    });
+    tile_product<double>(
+        a, tr0, tr1, a.x, [&](int64_t row, bool ok) { return ok ? a.b[row] : 0.0; },
+        [&](int64_t, double s, double bi) {
+          const double w = bi - s;
+          acc[0] += w * w;
+          acc[1] += bi * bi;
+        });
     tile_partial<2>(acc, a.P, a.ntiles, t, 5);
   });
   if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   FEMK_OWNER_LOOP {
-    const double ww = prob_sum(a, 5, k), bb = prob_sum(a, 6, k);
+    double v[2];
+    prob_sums<2>(a, {5, 6}, k, false, v);
+    const double ww = v[0], bb = v[1];
     if (threadIdx.x == 0) a.relres[k] = sqrt(ww) / (sqrt(bb) + 1e-30);
   }
 }
