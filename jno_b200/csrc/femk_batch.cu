@@ -17,16 +17,19 @@
 // After every reduction phase an owner pass (block b finishes problems b, b + G, ...) sums the
 // problem's tile partials in a fixed order and writes its scalars, so tiles can be small (the
 // largest problems keep every SM busy after the small ones have converged) without each tile
-// re-reducing its problem. Barriers are the bounded-spin grid barriers of femk_grid.cuh. No reference counterpart (jNO batches only by vmap over
-// right-hand sides, tests/test_fem_solver_slots.py:123-132).
+// re-reducing its problem. Barriers are the bounded-spin grid barriers of femk_grid.cuh. No
+// reference counterpart (jNO batches only by vmap over right-hand sides,
+// tests/test_fem_solver_slots.py:123-132).
 //
 // The mixed-precision form (k_batch_mixed) runs the same phases on FP32 values and vectors (FP32
-// SpMV accumulation, dot products summed in FP64) with x kept in FP64, and gives every problem
-// FP64 reliable updates, as femk_pcg_mixed does for one problem: when its FP32 <r, r> fell by
-// delta2 since the last update, met the stop test or hit the cap, the problem's next phase 1
-// replaces r by fp32(b - A x) with the FP64 values in place of its FP32 product, keeps the
-// direction (p and q = A p), and retires the problem once the FP64 residual meets the stop rule. A replacement thus
-// costs the problem one step slot and no extra phase or grid barrier.
+// SpMV accumulation, dot products summed in FP64). x stays in FP64; the steps alpha p of a segment
+// accumulate in an FP32 vector e that is folded into x (x += e, FP64) after each reliable update.
+// Every problem gets FP64 reliable updates, as femk_pcg_mixed does for one problem: when its FP32
+// <r, r> fell by delta2 since the last update, met the stop test or hit the cap, the problem's next
+// phase 1 replaces r by fp32(b - A (x + e)) with the FP64 values in place of its FP32 product and
+// keeps the direction (p and q = A p); its next phase 2 folds e into x in place of a step. The
+// problem retires once the FP64 residual meets the stop rule. A replacement thus costs the problem
+// two step slots and no extra phase or grid barrier.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -55,6 +58,7 @@ struct BatchArgs {
   // mixed precision: FP32 values and inner vectors, per-problem update bookkeeping
   const float* vals32;
   float *r32, *z32, *p32, *q32, *d32;
+  float* e32;        // FP32 increments of x not yet folded into it
   double* rr_since;  // [nprob] FP64 <r, r> at the last reliable update
   int32_t* upd;      // [nprob] per-problem step mode of the mixed form (0 normal, 1 update requested, 2 replaced)
   int32_t* outer;    // [nprob] FP64 residual evaluations
@@ -94,6 +98,15 @@ struct GatherPlain {
   __device__ __forceinline__ V operator()(int32_t j) const { return x[j]; }
 };
 
+// x[j] + e[j]: the FP64 iterate plus the FP32 increments not yet folded into it (plain loads, as
+// GatherPlain)
+struct GatherSum {
+  const double* x;
+  const float* e;
+  __device__ __forceinline__ double operator()(int64_t j) const { return x[j] + (double)e[j]; }
+  __device__ __forceinline__ double operator()(int32_t j) const { return x[j] + (double)e[j]; }
+};
+
 // One warp computes (A v)[row] for the rows of its tile. pre(row, ok) issues the row's own epilogue
 // loads ahead of the product's (ok false: the lane has no row in this slice, load nothing) and
 // returns them; post(row, Av, pre's values) finishes the row. V = double: the FP64 values; V = float:
@@ -101,9 +114,9 @@ struct GatherPlain {
 // the tile covers (tiles start and end on slice boundaries except at the ends of a problem), every
 // value and column load is independent of the others, and the next slice's offset is read while the
 // current slice runs; on the CSR kL lanes share a row.
-template <typename V = double, typename Pre, typename Post>
-__device__ __forceinline__ void tile_product(const BatchArgs& a, int32_t r0, int32_t r1, const V* v, Pre&& pre,
-                                             Post&& post) {
+template <typename V, int EB, typename G, typename Pre, typename Post>
+__device__ __forceinline__ void tile_product_g(const BatchArgs& a, int32_t r0, int32_t r1, const G& gx, Pre&& pre,
+                                               Post&& post) {
   const int lane = threadIdx.x & 31;
   if (a.sptr) {
     const V* vals;
@@ -118,11 +131,9 @@ __device__ __forceinline__ void tile_product(const BatchArgs& a, int32_t r0, int
       const int32_t row = s * 32 + lane;
       const bool ok = row >= r0 && row < r1;
       const auto ld = pre(row, ok);
-      // entries in flight per lane: 16 FP32 (half the bytes each) or 8 FP64
-      constexpr int EB = sizeof(V) == 4 ? 16 : 8;
       const int32_t w = ok ? (int32_t)((b1 - b0) >> 5) : 0;
-      const V acc = a.sc16 ? sell_row<V, int16_t, EB>(vals + b0 + lane, a.sc16 + b0 + lane, w, row, GatherPlain<V>{v})
-                           : sell_row<V, int32_t, EB>(vals + b0 + lane, a.scols + b0 + lane, w, row, GatherPlain<V>{v});
+      const V acc = a.sc16 ? sell_row<V, int16_t, EB>(vals + b0 + lane, a.sc16 + b0 + lane, w, row, gx)
+                           : sell_row<V, int32_t, EB>(vals + b0 + lane, a.scols + b0 + lane, w, row, gx);
       if (ok) post((int64_t)row, acc, ld);
       b0 = b1;
       b1 = b2;
@@ -139,11 +150,19 @@ __device__ __forceinline__ void tile_product(const BatchArgs& a, int32_t r0, int
   for (int64_t base = r0; base < r1; base += RPW * kU) {
     V sv[kU];
     int64_t rows[kU];
-    csr_rows_g<kL, kU, V, int32_t>(a.indptr, a.indices, vals, GatherPlain<V>{v}, r1, base, lane, sv, rows);
+    csr_rows_g<kL, kU, V, int32_t>(a.indptr, a.indices, vals, gx, r1, base, lane, sv, rows);
 #pragma unroll
     for (int u = 0; u < kU; ++u)
       if (rows[u] < r1 && sub == 0) post(rows[u], sv[u], pre(rows[u], true));
   }
+}
+
+template <typename V = double, typename Pre, typename Post>
+__device__ __forceinline__ void tile_product(const BatchArgs& a, int32_t r0, int32_t r1, const V* v, Pre&& pre,
+                                             Post&& post) {
+  // entries in flight per lane: 16 FP32 (half the bytes each) or 8 FP64
+  tile_product_g<V, sizeof(V) == 4 ? 16 : 8>(a, r0, r1, GatherPlain<V>{v}, static_cast<Pre&&>(pre),
+                                             static_cast<Post&&>(post));
 }
 
 // The rows [r0, r1) of a tile, S trips of 32 at a time: load(i) for all S rows of a round first
@@ -295,8 +314,7 @@ struct RowF64 {
   double x, p, r, q, d;
 };
 struct RowMixed {
-  double x;
-  float p, q, r, d;
+  float e, p, q, r, d;
 };
 
 __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
@@ -463,7 +481,6 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
   const WarpTiles wt = warp_tiles(a, gw, NW);
   auto every = [](int32_t) { return true; };
   auto live = [&](int32_t k) { return __ldcg(a.done + k) == 0; };
-  auto no_tag = [](int32_t) { return false; };
   double* alpha = a.gam + a.nprob;
   double* beta = alpha;
   // ---- phase 0: FP64 residual of x0, FP32 copies; <r, z> (FP32 data), <r64, r64>, <b, b>
@@ -480,6 +497,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
           a.d32[row] = d;
           a.r32[row] = rf;
           a.z32[row] = zf;
+          a.e32[row] = 0.0f;
           acc[0] += (double)rf * (double)zf;
           acc[1] += r64 * r64;
           acc[2] += bd.x * bd.x;
@@ -522,8 +540,8 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
         [&](int32_t t, int32_t tr0, int32_t tr1, int32_t, double be, bool replace) {
           if (replace) {
             double acc[2] = {0.0, 0.0};
-            tile_product<double>(
-                a, tr0, tr1, a.x,
+            tile_product_g<double, 4>(  // two gathers an entry: 4 entries in flight keep it unspilled
+                a, tr0, tr1, GatherSum{a.x, a.e32},
                 [&](int64_t row, bool ok) { return make_double2(ok ? a.b[row] : 0.0, ok ? (double)a.d32[row] : 0.0); },
                 [&](int64_t row, double sv, double2 bd) {
                   const double r64 = bd.x - sv;
@@ -594,18 +612,26 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
       }
     }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
-    // ---- phase 2 (mode 0): x += alpha p (FP64), r -= alpha q, z = D^-1 r (FP32); <r, z>, <r, r>
-    auto normal = [&](int32_t k) { return live(k) && __ldcg(a.upd + k) == 0; };
+    // ---- phase 2: (mode 0) e += alpha p, r -= alpha q, z = D^-1 r (FP32); <r, z>, <r, r>;
+    //      (mode 2, the residual was just replaced) x += e (FP64), e = 0
     for_warp_tiles_s(
-        wt, gw, NW, normal, [&](int32_t k) { return __ldcg(alpha + k); }, no_tag,
-        [&](int32_t t, int32_t tr0, int32_t tr1, int32_t, double al, bool) {
+        wt, gw, NW, [&](int32_t k) { return live(k) && __ldcg(a.upd + k) != 1; },
+        [&](int32_t k) { return __ldcg(alpha + k); }, [&](int32_t k) { return __ldcg(a.upd + k) == 2; },
+        [&](int32_t t, int32_t tr0, int32_t tr1, int32_t, double al, bool fold) {
+          if (fold) {
+            for (int32_t i = tr0 + (threadIdx.x & 31); i < tr1; i += 32) {
+              a.x[i] = a.x[i] + (double)__ldcg(a.e32 + i);
+              a.e32[i] = 0.0f;
+            }
+            return;
+          }
           const float alf = (float)al;
           double acc[2] = {0.0, 0.0};
           tile_rows<1>(
               tr0, tr1,
               [&](int32_t i) {
                 RowMixed v;
-                v.x = a.x[i];
+                v.e = __ldcg(a.e32 + i);
                 v.p = __ldcg(a.p32 + i);
                 v.q = __ldcg(a.q32 + i);
                 v.r = __ldcg(a.r32 + i);
@@ -613,7 +639,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
                 return v;
               },
               [&](int32_t i, const RowMixed& v) {
-                a.x[i] = v.x + al * (double)v.p;
+                a.e32[i] = fmaf(alf, v.p, v.e);
                 const float ri = fmaf(-alf, v.q, v.r);
                 const float zi = v.d * ri;
                 a.r32[i] = ri;
@@ -649,6 +675,12 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
     }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   }
+  // ---- fold: x += e for every problem (a problem that retired on a replaced residual still holds
+  // the increments of its last segment)
+  for_warp_tiles(wt, gw, NW, every, [&](int32_t, int32_t tr0, int32_t tr1, int32_t) {
+    for (int32_t i = tr0 + (threadIdx.x & 31); i < tr1; i += 32) a.x[i] = a.x[i] + (double)__ldcg(a.e32 + i);
+  });
+  if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
   // ---- phase R: per-problem ||b - A x||, ||b|| (FP64)
   for_warp_tiles(wt, gw, NW, every, [&](int32_t t, int32_t tr0, int32_t tr1, int32_t) {
     double acc[2] = {0.0, 0.0};
@@ -800,7 +832,7 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
   a.outer = a.upd + nprob;
   a.delta2 = delta2;
   a.vals32 = nullptr;
-  a.r32 = a.z32 = a.p32 = a.q32 = a.d32 = nullptr;
+  a.r32 = a.z32 = a.p32 = a.q32 = a.d32 = a.e32 = nullptr;
   if (mixed) {
     if (!sell && !p->vals32) FEMK_CUDA_TRY(cudaMalloc(&p->vals32, sizeof(float) * (p->nnz + 1)));
     if (!p->work32) FEMK_CUDA_TRY(cudaMalloc(&p->work32, sizeof(float) * kWork32Vectors * p->vstride));
@@ -810,6 +842,7 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
     a.p32 = a.z32 + vs;
     a.q32 = a.p32 + vs;
     a.d32 = a.q32 + vs;
+    a.e32 = a.d32 + vs;
   }
   a.bar = (GridBar*)p->bar;
   a.spin = p->barrier_spin;
