@@ -63,6 +63,9 @@ struct BatchArgs {
   int32_t* upd;      // [nprob] per-problem step mode of the mixed form (0 normal, 1 update requested, 2 replaced)
   int32_t* outer;    // [nprob] FP64 residual evaluations
   double delta2;
+  // the mixed form's FP32 product ring (shared memory, 2 stages a warp); ring_stage == 0: off
+  int32_t ring_w;      // widest slice (entries a row) a stage holds
+  int32_t ring_stage;  // bytes a stage: 32 ring_w FP32 values, then 32 ring_w columns
   const int32_t* tile_r0;
   const int32_t* tile_r1;
   const int32_t* tile_prob;
@@ -97,6 +100,17 @@ struct GatherPlain {
   __device__ __forceinline__ V operator()(int64_t j) const { return x[j]; }
   __device__ __forceinline__ V operator()(int32_t j) const { return x[j]; }
 };
+
+// 16-byte asynchronous copy global -> shared through L2 (cp.async.cg), and its group bookkeeping
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned int d = (unsigned int)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 // x[j] + e[j]: the FP64 iterate plus the FP32 increments not yet folded into it (plain loads, as
 // GatherPlain)
@@ -309,6 +323,135 @@ __device__ __forceinline__ void for_warp_tiles_s(const WarpTiles& w, int32_t gw,
 // Owner pass: block b finishes problems k = b, b + G, ... from their tile partials.
 #define FEMK_OWNER_LOOP for (int32_t k = blockIdx.x; k < a.nprob; k += gridDim.x)
 
+// The FP32 product phase of the mixed form (w = A32 z, p = z + beta p, q = w + beta q, <p, q>) over
+// the warp's tiles in `mask`, with each slice's values and columns staged in the warp's two-stage
+// shared-memory ring by 16-byte cp.async copies: slice i + 1 is in flight while slice i gathers, so
+// a slice waits on its gathers only. A tile's slice offsets sptr[s0 .. s1 + 1] are read one tile
+// ahead (lane i holds sptr[s0 + i]). Every cursor below is warp-uniform. The FP32 sums run in the
+// order of sell_row, so the products are the bits of the direct path.
+__device__ __forceinline__ void product32_ring(const BatchArgs& a, const WarpTiles& wt, int32_t gw, int32_t NW,
+                                               unsigned int mask, double beta_lane, char* ring) {
+  constexpr unsigned int kFull = 0xffffffffu;
+  constexpr int EB = 16;
+  if (!mask) return;
+  const int lane = threadIdx.x & 31;
+  using I = int16_t;  // int16 column offsets (an int32-column instance spilled at the 64-register cap)
+  const I* cols = a.sc16;
+  const int32_t stage = a.ring_stage;
+  const int32_t coff = 128 * a.ring_w;  // the columns follow the values in a stage
+  auto first = [&](int j) { return __shfl_sync(kFull, wt.r0, j) >> 5; };
+  auto last = [&](int j) { return (__shfl_sync(kFull, wt.r1, j) - 1) >> 5; };
+  auto after = [&](int j) {  // the next tile of the mask after tile j, or -1
+    const unsigned int rest = j < 31 ? mask & (~0u << (j + 1)) : 0u;
+    return rest ? __ffs(rest) - 1 : -1;
+  };
+  auto offsets = [&](int j) -> int32_t {  // the ring is on only for fewer than 2^31 stored entries
+    if (j < 0) return 0;
+    const int32_t s0 = first(j), s1 = last(j);
+    return lane <= s1 - s0 + 1 ? (int32_t)__ldg(a.sptr + s0 + lane) : 0;
+  };
+  // prefetch cursor: tile pj, slice ps of [ps0, pe]; pdir its offsets, ndir those of tile pn
+  int pj = __ffs(mask) - 1;
+  int pn = after(pj);
+  int32_t pdir = offsets(pj);
+  int32_t ndir = offsets(pn);
+  int32_t ps0 = first(pj), ps = ps0, pe = last(pj);
+  int32_t w0 = 0, w1 = 0;  // entries a row of the slice in stage 0 / 1
+  auto issue = [&](int st) {
+    if (pj >= 0) {
+      const int32_t b0 = __shfl_sync(kFull, pdir, ps - ps0), b1 = __shfl_sync(kFull, pdir, ps - ps0 + 1);
+      const int32_t wd = (int32_t)((b1 - b0) >> 5);
+      char* dst = ring + st * stage;
+      const char* gv = (const char*)(a.svals32 + b0);
+      const char* gc = (const char*)(cols + b0);
+      const int32_t nv = 8 * wd;                      // 16-byte chunks of the values (128 wd bytes)
+      const int32_t nc = 4 * wd;                      // ... of the columns (64 wd bytes)
+      for (int32_t c = lane; c < nv; c += 32) cp_async16(dst + 16 * c, gv + 16 * c);
+      for (int32_t c = lane; c < nc; c += 32) cp_async16(dst + coff + 16 * c, gc + 16 * c);
+      if (st)
+        w1 = wd;
+      else
+        w0 = wd;
+      if (ps < pe) {
+        ++ps;
+      } else {
+        pj = pn;
+        if (pj >= 0) {
+          pdir = ndir;
+          ps0 = ps = first(pj);
+          pe = last(pj);
+          pn = after(pj);
+          ndir = offsets(pn);
+        }
+      }
+    }
+    cp_async_commit();  // an empty group once the sequence is exhausted keeps the counts aligned
+  };
+  issue(0);
+  // compute cursor: tile cj, slice cs of [.., ce], rows [r0, r1), its beta
+  int cj = __ffs(mask) - 1;
+  int32_t cs = first(cj), ce = last(cj);
+  int32_t r0 = __shfl_sync(kFull, wt.r0, cj), r1 = __shfl_sync(kFull, wt.r1, cj);
+  double be = __shfl_sync(kFull, beta_lane, cj);
+  double acc[1] = {0.0};
+  for (int it = 0;; ++it) {
+    const int st = it & 1;
+    __syncwarp();  // every lane is done with the other stage (slice it - 1)
+    issue(st ^ 1);
+    const int32_t row = cs * 32 + lane;
+    const bool ok = row >= r0 && row < r1;
+    const bool step = be != 0.0;
+    float zr = 0.0f, pr = 0.0f, qr = 0.0f;  // the row's own operands, loaded under the wait
+    if (ok) {
+      zr = __ldcg(a.z32 + row);
+      if (step) {
+        pr = __ldcg(a.p32 + row);
+        qr = __ldcg(a.q32 + row);
+      }
+    }
+    cp_async_wait<1>();  // this lane's copies of slice it have landed
+    __syncwarp();        // ... and every other lane's
+    const int32_t wd = ok ? (st ? w1 : w0) : 0;
+    const float* sv = (const float*)(ring + st * stage) + lane;
+    const I* sc = (const I*)(ring + st * stage + coff) + lane;
+    float w = 0.0f;
+    for (int32_t k0 = 0; k0 < wd; k0 += EB) {
+      float g[EB];  // the gathers first (all in flight), the values re-read from the stage after
+#pragma unroll
+      for (int u = 0; u < EB; ++u) {
+        const int32_t k = (k0 + u) * 32;
+        g[u] = k0 + u < wd ? a.z32[row + (int32_t)sc[k]] : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < EB; ++u)
+        if (k0 + u < wd) w += sv[(k0 + u) * 32] * g[u];
+    }
+    if (ok) {
+      const float bf = (float)be;
+      const float pi = step ? fmaf(bf, pr, zr) : zr;
+      const float qi = step ? fmaf(bf, qr, w) : w;
+      a.p32[row] = pi;
+      a.q32[row] = qi;
+      acc[0] += (double)pi * (double)qi;
+    }
+    if (cs < ce) {
+      ++cs;
+    } else {
+      tile_partial<1>(acc, a.P, a.ntiles, gw + cj * NW, 3);
+      acc[0] = 0.0;
+      cj = after(cj);
+      if (cj < 0) break;
+      cs = first(cj);
+      ce = last(cj);
+      r0 = __shfl_sync(kFull, wt.r0, cj);
+      r1 = __shfl_sync(kFull, wt.r1, cj);
+      be = __shfl_sync(kFull, beta_lane, cj);
+    }
+  }
+  cp_async_wait<0>();
+  __syncwarp();
+}
+
 // the vector operands of one row in the update phases
 struct RowF64 {
   double x, p, r, q, d;
@@ -475,6 +618,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_pcg(BatchArgs a) {
 }
 
 __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
+  extern __shared__ __align__(16) char batch_ring[];  // 2 a.ring_stage bytes a warp when the ring is on
   unsigned int gen = 0;
   const int32_t gw = (int32_t)((blockIdx.x * (int64_t)kBT + threadIdx.x) >> 5);  // global warp
   const int32_t NW = (int32_t)(((int64_t)gridDim.x * kBT) >> 5);
@@ -533,53 +677,69 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
   // phase sees one value per iteration, and no iteration needs an extra phase.
   while (ld_acquire_u32((const unsigned int*)a.active) != 0u) {
     // ---- phase 1: w = A32 z, p = z + beta p, q = w + beta q (= A32 p) (FP32), <p, q>;
-    //      or (mode 1) r = fp32(b - A64 x), z = D^-1 r, <r, z>, <r64, r64>
-    for_warp_tiles_s(
-        wt, gw, NW, live, [&](int32_t k) { return __ldcg(beta + k); },
-        [&](int32_t k) { return __ldcg(a.upd + k) == 1; },
-        [&](int32_t t, int32_t tr0, int32_t tr1, int32_t, double be, bool replace) {
-          if (replace) {
-            double acc[2] = {0.0, 0.0};
-            tile_product_g<double, 4>(  // two gathers an entry: 4 entries in flight keep it unspilled
-                a, tr0, tr1, GatherSum{a.x, a.e32},
-                [&](int64_t row, bool ok) { return make_double2(ok ? a.b[row] : 0.0, ok ? (double)a.d32[row] : 0.0); },
-                [&](int64_t row, double sv, double2 bd) {
-                  const double r64 = bd.x - sv;
-                  const float rf = (float)r64;
-                  const float zf = (float)bd.y * rf;
-                  a.r32[row] = rf;
-                  a.z32[row] = zf;
-                  acc[0] += (double)rf * (double)zf;
-                  acc[1] += r64 * r64;
-                });
-            tile_partial<2>(acc, a.P, a.ntiles, t, 4);
-          } else {
-            const bool step = be != 0.0;
-            const float bf = (float)be;
-            double acc[1] = {0.0};
-            tile_product<float>(
-                a, tr0, tr1, a.z32,
-                [&](int64_t row, bool ok) {
-                  float3 v = make_float3(0.0f, 0.0f, 0.0f);
-                  if (ok) {
-                    v.x = __ldcg(a.z32 + row);
-                    if (step) {
-                      v.y = __ldcg(a.p32 + row);
-                      v.z = __ldcg(a.q32 + row);
-                    }
+    //      or (mode 1) r = fp32(b - A64 (x + e)), z = D^-1 r, <r, z>, <r64, r64>
+    {
+      const int lane = threadIdx.x & 31;
+      double be_l = 0.0;
+      bool lv = false, rp = false;
+      if (lane < wt.count) {  // independent loads, all in flight together
+        be_l = __ldcg(beta + wt.k);
+        lv = __ldcg(a.done + wt.k) == 0;
+        rp = __ldcg(a.upd + wt.k) == 1;
+      }
+      const unsigned int m_rep = __ballot_sync(0xffffffffu, lv && rp);
+      const unsigned int m_step = __ballot_sync(0xffffffffu, lv && !rp);
+      for (unsigned int m = m_rep; m; m &= m - 1) {
+        const int j = __ffs(m) - 1;
+        double acc[2] = {0.0, 0.0};
+        tile_product_g<double, 4>(  // two gathers an entry: 4 entries in flight keep it unspilled
+            a, __shfl_sync(0xffffffffu, wt.r0, j), __shfl_sync(0xffffffffu, wt.r1, j), GatherSum{a.x, a.e32},
+            [&](int64_t row, bool ok) { return make_double2(ok ? a.b[row] : 0.0, ok ? (double)a.d32[row] : 0.0); },
+            [&](int64_t row, double sv, double2 bd) {
+              const double r64 = bd.x - sv;
+              const float rf = (float)r64;
+              const float zf = (float)bd.y * rf;
+              a.r32[row] = rf;
+              a.z32[row] = zf;
+              acc[0] += (double)rf * (double)zf;
+              acc[1] += r64 * r64;
+            });
+        tile_partial<2>(acc, a.P, a.ntiles, gw + j * NW, 4);
+      }
+      if (a.ring_stage) {
+        char* ring = batch_ring + (threadIdx.x >> 5) * 2 * a.ring_stage;
+        product32_ring(a, wt, gw, NW, m_step, be_l, ring);  // the host turns it on with int16 columns only
+      } else {
+        for (unsigned int m = m_step; m; m &= m - 1) {
+          const int j = __ffs(m) - 1;
+          const double be = __shfl_sync(0xffffffffu, be_l, j);
+          const bool step = be != 0.0;
+          const float bf = (float)be;
+          double acc[1] = {0.0};
+          tile_product<float>(
+              a, __shfl_sync(0xffffffffu, wt.r0, j), __shfl_sync(0xffffffffu, wt.r1, j), a.z32,
+              [&](int64_t row, bool ok) {
+                float3 v = make_float3(0.0f, 0.0f, 0.0f);
+                if (ok) {
+                  v.x = __ldcg(a.z32 + row);
+                  if (step) {
+                    v.y = __ldcg(a.p32 + row);
+                    v.z = __ldcg(a.q32 + row);
                   }
-                  return v;
-                },
-                [&](int64_t row, float w, float3 v) {
-                  const float pi = step ? fmaf(bf, v.y, v.x) : v.x;
-                  const float qi = step ? fmaf(bf, v.z, w) : w;
-                  a.p32[row] = pi;
-                  a.q32[row] = qi;
-                  acc[0] += (double)pi * (double)qi;
-                });
-            tile_partial<1>(acc, a.P, a.ntiles, t, 3);
-          }
-        });
+                }
+                return v;
+              },
+              [&](int64_t row, float w, float3 v) {
+                const float pi = step ? fmaf(bf, v.y, v.x) : v.x;
+                const float qi = step ? fmaf(bf, v.z, w) : w;
+                a.p32[row] = pi;
+                a.q32[row] = qi;
+                acc[0] += (double)pi * (double)qi;
+              });
+          tile_partial<1>(acc, a.P, a.ntiles, gw + j * NW, 3);
+        }
+      }
+    }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
       double v[3];  // slot 3 (<p, q>) of a step, slots 4, 5 (<r, z>, <r64, r64>) of a replacement
@@ -740,7 +900,23 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
   FEMK_CHECK_ARG(row_off[0] == 0 && row_off[nprob] == p->n, "femk_pcg_batched: row_off must span [0, n)");
   for (int32_t k = 0; k < nprob; ++k) FEMK_CHECK_ARG(row_off[k + 1] > row_off[k], "femk_pcg_batched: empty problem");
   const void* kern = mixed ? (const void*)k_batch_mixed : (const void*)k_batch_pcg;
-  const int per_sm = std::min(blocks_per_sm, resident_blocks(kern, kBT));
+  // The mixed form's FP32 products stream each slice through a two-stage shared-memory ring a warp
+  // (int16 columns, rows of at most 16 entries: 96 KB a block, so 2 blocks of 512 fit an SM)
+  const int32_t ring_w = std::max(1, p->max_row);
+  const int32_t ring_stage = 32 * ring_w * (4 + 2);
+  const int ring_smem = (kBT / 32) * 2 * ring_stage;
+  bool ring = mixed && p->use_sell && p->sell_cols && p->sell_c16 && ((uintptr_t)p->sell_c16 & 15u) == 0 &&
+              p->sell_nnz < ((int64_t)1 << 31) && ring_smem <= 100 * 1024;
+  int per_sm = 0;
+  if (ring) {
+    if (cudaFuncSetAttribute(k_batch_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, ring_smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_mixed, kBT, ring_smem) != cudaSuccess ||
+        per_sm < 1) {
+      cudaGetLastError();
+      ring = false;
+    }
+  }
+  per_sm = std::min(blocks_per_sm, ring ? per_sm : resident_blocks(kern, kBT));
   const int grid = p->n_sm * std::max(1, per_sm);
   const int64_t nwarps = (int64_t)grid * (kBT / 32);
   // tiles: on the sliced-ELL copy they end on global multiples of tile_rows (rounded up to a whole
@@ -768,6 +944,8 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
     tr *= 2;
   }
   const int32_t ntiles = (int32_t)r0.size();
+  ring = ring && tr <= 512;  // a tile's slice offsets (at most tr / 32 + 2) sit one a lane
+  const int launch_smem = ring ? ring_smem : 0;
   cudaStream_t s = (cudaStream_t)stream;
   FEMK_TRY(ensure_workspace(p));
   // batch workspace: ints (tiles + per-problem), doubles (partials + per-problem)
@@ -831,6 +1009,8 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
   a.upd = a.active + 1;
   a.outer = a.upd + nprob;
   a.delta2 = delta2;
+  a.ring_w = ring_w;
+  a.ring_stage = ring ? ring_stage : 0;
   a.vals32 = nullptr;
   a.r32 = a.z32 = a.p32 = a.q32 = a.d32 = a.e32 = nullptr;
   if (mixed) {
@@ -852,6 +1032,7 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
   for (int32_t k = 0; k <= nprob; ++k) h = (h ^ (uint64_t)row_off[k]) * 1099511628211ull;
   h = (h ^ (uint64_t)tr) * 1099511628211ull;
   h = (h ^ (uint64_t)grid) * 1099511628211ull;
+  h = (h ^ (uint64_t)launch_smem) * 1099511628211ull;
   const bool same_tiles = p->batch_key[0] == (const void*)(uintptr_t)h && p->batch_key[1] == p->batch_ws;
   if (!same_tiles) {
     FEMK_CUDA_TRY(cudaMemcpyAsync(ib, r0.data(), 4 * ntiles, cudaMemcpyHostToDevice, s));
@@ -883,7 +1064,7 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
       else if (mixed)
         k_to_f32<<<cgrid, 256, 0, p->batch_stream>>>(vals, p->nnz, p->vals32);
       void* cargs[] = {(void*)&a};
-      cudaError_t el = cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), cargs, 0, p->batch_stream);
+      cudaError_t el = cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), cargs, launch_smem, p->batch_stream);
       cudaError_t ee = cudaStreamEndCapture(p->batch_stream, &g);
       if (el == cudaSuccess && ee == cudaSuccess && g) e = cudaGraphInstantiate(&p->batch_exec, g, 0);
       else e = el != cudaSuccess ? el : ee;
@@ -917,7 +1098,7 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
     FEMK_CUDA_TRY(cudaGetLastError());
     void* args[] = {(void*)&a};
     counted_launch();
-    FEMK_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), args, 0, s));
+    FEMK_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), args, launch_smem, s));
     p->batch_key[0] = (const void*)(uintptr_t)h;
     p->batch_key[1] = p->batch_ws;
     p->batch_graph_used = 0;
