@@ -66,6 +66,7 @@ struct BatchArgs {
   // the mixed form's FP32 product ring (shared memory, 2 stages a warp); ring_stage == 0: off
   int32_t ring_w;      // widest slice (entries a row) a stage holds
   int32_t ring_stage;  // bytes a stage: 32 ring_w FP32 values, then 32 ring_w columns
+  int32_t urows;       // rows a vector in the update phase's three ring stages; 0: direct loads
   const int32_t* tile_r0;
   const int32_t* tile_r1;
   const int32_t* tile_prob;
@@ -452,6 +453,68 @@ __device__ __forceinline__ void product32_ring(const BatchArgs& a, const WarpTil
   __syncwarp();
 }
 
+// The update phase of the mixed form (e += alpha p, r -= alpha q, z = D^-1 r, <r, z>, <r, r>) over
+// the warp's tiles in `mask`, with each tile's e, p, q, r and D staged in the warp's shared-memory
+// ring: three stages of a.urows rows a vector, so the next two tiles' operands are in flight while a
+// tile computes. A stage holds whole slices (rows 32 s0 to 32 (s1 + 1)), so every copy starts on 16
+// bytes and stays inside the vectors' vstride slots. The arithmetic is the direct path's.
+__device__ __forceinline__ void update32_ring(const BatchArgs& a, const WarpTiles& wt, int32_t gw, int32_t NW,
+                                              unsigned int mask, double al_lane, char* ring) {
+  constexpr unsigned int kFull = 0xffffffffu;
+  if (!mask) return;
+  const int lane = threadIdx.x & 31;
+  const int32_t vrow = a.urows;        // rows of one vector in a stage (a multiple of 32)
+  const int32_t sbytes = 5 * 4 * vrow;  // a stage: e, p, q, r, D
+  const float* src[5] = {a.e32, a.p32, a.q32, a.r32, a.d32};
+  auto after = [&](int j) {
+    const unsigned int rest = j < 31 ? mask & (~0u << (j + 1)) : 0u;
+    return rest ? __ffs(rest) - 1 : -1;
+  };
+  int pj = __ffs(mask) - 1;
+  auto issue = [&](int st) {
+    if (pj >= 0) {
+      const int32_t a0 = __shfl_sync(kFull, wt.r0, pj) & ~31;
+      const int32_t a1 = (__shfl_sync(kFull, wt.r1, pj) + 31) & ~31;
+      const int32_t nch = (a1 - a0) >> 2;  // 16-byte chunks of one vector
+      char* dst = ring + st * sbytes;
+#pragma unroll
+      for (int v = 0; v < 5; ++v)
+        for (int32_t c = lane; c < nch; c += 32) cp_async16(dst + v * 4 * vrow + 16 * c, src[v] + a0 + 4 * c);
+      pj = after(pj);
+    }
+    cp_async_commit();
+  };
+  issue(0);
+  issue(1);
+  int cj = __ffs(mask) - 1;
+  for (int it = 0; cj >= 0; ++it) {
+    const int st = it % 3;
+    __syncwarp();  // every lane is done with stage (it + 2) % 3 (tile it - 1)
+    issue((it + 2) % 3);
+    cp_async_wait<2>();  // this lane's copies of tile it have landed
+    __syncwarp();        // ... and every other lane's
+    const int32_t r0 = __shfl_sync(kFull, wt.r0, cj), r1 = __shfl_sync(kFull, wt.r1, cj);
+    const int32_t a0 = r0 & ~31;
+    const float alf = (float)__shfl_sync(kFull, al_lane, cj);
+    const float* sb = (const float*)(ring + st * sbytes);
+    double acc[2] = {0.0, 0.0};
+    for (int32_t i = r0 + lane; i < r1; i += 32) {
+      const int32_t li = i - a0;
+      a.e32[i] = fmaf(alf, sb[vrow + li], sb[li]);
+      const float ri = fmaf(-alf, sb[2 * vrow + li], sb[3 * vrow + li]);
+      const float zi = sb[4 * vrow + li] * ri;
+      a.r32[i] = ri;
+      a.z32[i] = zi;
+      acc[0] += (double)ri * (double)zi;
+      acc[1] += (double)ri * (double)ri;
+    }
+    tile_partial<2>(acc, a.P, a.ntiles, gw + cj * NW, 4);
+    cj = after(cj);
+  }
+  cp_async_wait<0>();
+  __syncwarp();
+}
+
 // the vector operands of one row in the update phases
 struct RowF64 {
   double x, p, r, q, d;
@@ -624,7 +687,6 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
   const int32_t NW = (int32_t)(((int64_t)gridDim.x * kBT) >> 5);
   const WarpTiles wt = warp_tiles(a, gw, NW);
   auto every = [](int32_t) { return true; };
-  auto live = [&](int32_t k) { return __ldcg(a.done + k) == 0; };
   double* alpha = a.gam + a.nprob;
   double* beta = alpha;
   // ---- phase 0: FP64 residual of x0, FP32 copies; <r, z> (FP32 data), <r64, r64>, <b, b>
@@ -774,21 +836,35 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     // ---- phase 2: (mode 0) e += alpha p, r -= alpha q, z = D^-1 r (FP32); <r, z>, <r, r>;
     //      (mode 2, the residual was just replaced) x += e (FP64), e = 0
-    for_warp_tiles_s(
-        wt, gw, NW, [&](int32_t k) { return live(k) && __ldcg(a.upd + k) != 1; },
-        [&](int32_t k) { return __ldcg(alpha + k); }, [&](int32_t k) { return __ldcg(a.upd + k) == 2; },
-        [&](int32_t t, int32_t tr0, int32_t tr1, int32_t, double al, bool fold) {
-          if (fold) {
-            for (int32_t i = tr0 + (threadIdx.x & 31); i < tr1; i += 32) {
-              a.x[i] = a.x[i] + (double)__ldcg(a.e32 + i);
-              a.e32[i] = 0.0f;
-            }
-            return;
-          }
-          const float alf = (float)al;
+    {
+      const int lane = threadIdx.x & 31;
+      double al_l = 0.0;
+      bool lv = false;
+      int32_t md = 1;
+      if (lane < wt.count) {  // independent loads, all in flight together
+        al_l = __ldcg(alpha + wt.k);
+        lv = __ldcg(a.done + wt.k) == 0;
+        md = __ldcg(a.upd + wt.k);
+      }
+      const unsigned int m_fold = __ballot_sync(0xffffffffu, lv && md == 2);
+      const unsigned int m_step = __ballot_sync(0xffffffffu, lv && md == 0);
+      for (unsigned int m = m_fold; m; m &= m - 1) {
+        const int j = __ffs(m) - 1;
+        const int32_t tr1 = __shfl_sync(0xffffffffu, wt.r1, j);
+        for (int32_t i = __shfl_sync(0xffffffffu, wt.r0, j) + lane; i < tr1; i += 32) {
+          a.x[i] = a.x[i] + (double)__ldcg(a.e32 + i);
+          a.e32[i] = 0.0f;
+        }
+      }
+      if (a.urows) {
+        update32_ring(a, wt, gw, NW, m_step, al_l, batch_ring + (threadIdx.x >> 5) * 2 * a.ring_stage);
+      } else {
+        for (unsigned int m = m_step; m; m &= m - 1) {
+          const int j = __ffs(m) - 1;
+          const float alf = (float)__shfl_sync(0xffffffffu, al_l, j);
           double acc[2] = {0.0, 0.0};
           tile_rows<1>(
-              tr0, tr1,
+              __shfl_sync(0xffffffffu, wt.r0, j), __shfl_sync(0xffffffffu, wt.r1, j),
               [&](int32_t i) {
                 RowMixed v;
                 v.e = __ldcg(a.e32 + i);
@@ -807,8 +883,10 @@ __global__ void __launch_bounds__(kBT, 2) k_batch_mixed(BatchArgs a) {
                 acc[0] += (double)ri * (double)zi;
                 acc[1] += (double)ri * (double)ri;
               });
-          tile_partial<2>(acc, a.P, a.ntiles, t, 4);
-        });
+          tile_partial<2>(acc, a.P, a.ntiles, gw + j * NW, 4);
+        }
+      }
+    }
     if (!grid_sync(a.bar, gen, a.spin, a.skip)) return;
     FEMK_OWNER_LOOP {
       double v[2];
@@ -1011,6 +1089,8 @@ int batched_impl(const femk_plan* pc, int32_t nprob, const int64_t* row_off, con
   a.delta2 = delta2;
   a.ring_w = ring_w;
   a.ring_stage = ring ? ring_stage : 0;
+  // the update phase's ring: three stages of e, p, q, r, D for a tile's whole slices (tr + 32 rows)
+  a.urows = ring && 3 * 5 * 4 * (int32_t)(tr + 32) <= 2 * ring_stage ? (int32_t)(tr + 32) : 0;
   a.vals32 = nullptr;
   a.r32 = a.z32 = a.p32 = a.q32 = a.d32 = a.e32 = nullptr;
   if (mixed) {
