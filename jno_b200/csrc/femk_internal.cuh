@@ -9,7 +9,7 @@
 
 #include "../../include/femk.h"
 
-#define FEMK_VERSION 10200
+#define FEMK_VERSION 10300
 
 namespace femk {
 
