@@ -79,16 +79,22 @@ def run_path(args):
         inv = plan.jacobi(vals)
         sched = batched_schedule(batch, vals, b, inv, 1e-8)
 
+        mixed = args.solver == "mixed"
+
         def step(i):
             plan.assemble(logk, vals=vals, b=b)
             plan.jacobi(vals, out=inv)
-            x, it, rel, stv, st = plan.pcg_batched(batch.row_off, vals, b, None, inv, 1e-8, 0.0, 20_000,
-                                                   sched["tile_rows"], sched["blocks_per_sm"])
-            info.setdefault("iters", []).append(float(it.max()))
+            if mixed:
+                out = plan.pcg_batched_mixed(batch.row_off, vals, b, inv, None, 1e-8, 0.0, 20_000,
+                                             sched["tile_rows"], sched["blocks_per_sm"])
+            else:
+                out = plan.pcg_batched(batch.row_off, vals, b, None, inv, 1e-8, 0.0, 20_000, sched["tile_rows"],
+                                       sched["blocks_per_sm"])
+            info.setdefault("iters", []).append(float(out[1].max()))
 
         workload = (f"256 P1 problems, sides {int(sides.min())}..{int(sides.max())} hexes ({plan.n:,} DOF), "
-                    f"assemble + batched Jacobi-PCG to 1e-8, schedule {sched['tile_rows']} rows x "
-                    f"{sched['blocks_per_sm']} blocks/SM")
+                    f"assemble + batched {'mixed-precision ' if mixed else ''}Jacobi-PCG to 1e-8, schedule "
+                    f"{sched['tile_rows']} rows x {sched['blocks_per_sm']} blocks/SM")
         metric, units = "DOF/s", plan.n
     elif args.path == "tri":
         n = 1024 if args.n == 128 else args.n
