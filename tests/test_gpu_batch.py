@@ -73,11 +73,12 @@ def test_batched_replay_is_bitwise_reproducible():
     assert torch.equal(x1, x2) and np.array_equal(it1, it2) and np.array_equal(rel1, rel2)
 
 
-@pytest.mark.parametrize("tile_rows,bps", [(32, 2), (2048, 1)])
+@pytest.mark.parametrize("tile_rows,bps", [(32, 2), (64, 2), (2048, 1)])
 def test_batched_mixed_reaches_the_fp64_stop_rule(tile_rows, bps):
     """The mixed-precision batched solve: every problem's FP64 residual meets the 1e-8 stop rule,
     each solution is within 1e-6 of the per-problem FP64 oracle, the large problems take FP64
-    reliable updates, and the graph replay is bit-identical."""
+    reliable updates, and the graph replay is bit-identical. Tiles of 32 and 64 rows run the FP32
+    products and the update phase through the shared-memory rings; 2048-row tiles run direct loads."""
     from jno_b200.batch import BatchedPoisson
 
     sides = [3, 5, 1, 8, 4, 6, 2, 12, 16]
