@@ -823,11 +823,16 @@ def run_ours(args):
     csr_bytes = 12 * nnz + 20 * ndof + 4
     peak, peak_src = peak_hbm_gbs()
     achieved = sell_bytes / (sell_ms / 1e3) / 1e9
+    # the bulk-copy ring runs on int16 column offsets and rows of at most 32 entries (3-D P2 rows are
+    # wider); the committed ncu traffic figure is for the P1 128^3 workload only
+    bulk = plan.cols16 and not (plan.dim == 3 and plan.order == 2)
+    profiled = plan.dim == 3 and plan.order == 1 and ndof == 129 ** 3
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": roofline_traffic(),
-                "kernel": (f"k_sell_bulk (FP64 sliced-ELL CG-step SpMV, bulk-copy ring, "
-                           f"{'int16' if plan.cols16 else 'int32'} column offsets"
-                           f"{', per-slice column tables' if tables else ''})"),
+                "traffic": roofline_traffic() if profiled else None,
+                "kernel": ((f"k_sell_bulk (FP64 sliced-ELL CG-step SpMV, bulk-copy ring, " if bulk else
+                            "k_sell (FP64 sliced-ELL CG-step SpMV, thread per row, ")
+                           + f"{'int16' if plan.cols16 else 'int32'} column offsets"
+                           + f"{', per-slice column tables' if tables else ''})"),
                 "bytes_per_launch": sell_bytes, "ms_per_launch": sell_ms, "peak_source": peak_src,
                 "column_entries": plan.sell_col_units, "stored_entries": plan.sell_nnz,
                 "timing": f"CUDA events around each CG-step SpMV inside {prof_iters} profiled iterations",
