@@ -132,7 +132,8 @@ typedef struct femk_plan_options {
   int32_t ring32;         /* the same for the FP32 step of femk_pcg_mixed; -1 (default): 14 */
   int32_t csr_lanes;      /* CSR SpMV lanes per row (4, 8, 16, 32); 0 (default): from the mean row length */
   int32_t csr_rows;       /* CSR rows in flight per lane group (1, 2, 4); 0 (default): with csr_lanes */
-  int32_t sell_batch;     /* entries in flight per thread of the thread-per-row FP64 kernel: 8 or 16 (default) */
+  int32_t sell_batch;     /* entries in flight per thread of the thread-per-row FP64 kernel: 8, or 16 (default;
+                             32 on plans with int32 columns, such as 3-D P2) */
   int32_t vec_blocks;     /* blocks per SM of the FP64 CG vector kernels; 0 (default): one full wave */
   int32_t split_updates;  /* 1 (default): FP64 CG vector updates as r-update + direction/x-update kernels */
   int32_t test_skip_arrival; /* testing the bounded waits: the block with this index skips its first

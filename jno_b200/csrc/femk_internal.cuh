@@ -186,6 +186,7 @@ struct femk_plan {
   int l2_mode = 0;               // L2 eviction hints of the FP64 CG kernels (the l2_hints plan option)
   int sell64_c16 = 1;            // FP64 sliced-ELL streams int16 column offsets when available
   int sell_batch = 16;           // entries in flight per thread of the thread-per-row FP64 sliced-ELL kernel
+                                 // (16: 16 with int16 columns, 32 with int32 columns)
   double mixed_delta2 = 0.0;     // reliable-update threshold of the mixed solvers (0: 1e-4)
   long long barrier_spin = 0;    // clock64 budget of each grid-barrier wait of the batched solvers
   int skip_arrival = -1;         // testing: block that skips its first grid-barrier arrival (-1: none)

@@ -255,9 +255,12 @@ __device__ __noinline__ void step_finish(MixedState* st, double rw, const double
   }
 }
 
-// K_B on the register-streamed sliced-ELL operator (one thread per row)
+// K_B on the register-streamed sliced-ELL operator (one thread per row; the plans that reach it are
+// the ones the bulk-copy ring does not take, chiefly 3-D P2 with rows of up to 65 entries and int32
+// columns). 16 entries in flight a thread (48 registers, 5 blocks of 256 per SM): at P2 64^3 the
+// mixed solve took 77.1 ms against 81.7 ms with 8 entries at 32 registers and 87.8 ms with 32.
 template <typename IDX, bool REFRESH>
-__global__ void __launch_bounds__(kThreads, 8) k_step32_sell(const int64_t* __restrict__ sptr, const IDX* __restrict__ cols,
+__global__ void __launch_bounds__(kThreads) k_step32_sell(const int64_t* __restrict__ sptr, const IDX* __restrict__ cols,
                                                          const float* __restrict__ vals, int64_t n, int64_t nslices,
                                                          const float* __restrict__ r, float* __restrict__ w,
                                                          double* __restrict__ partials, int ga, MixedState* st,
@@ -272,8 +275,8 @@ __global__ void __launch_bounds__(kThreads, 8) k_step32_sell(const int64_t* __re
     if (row >= n) continue;
     const int64_t b0 = __ldg(sptr + sl);
     const int32_t wd = (int32_t)((__ldg(sptr + sl + 1) - b0) >> 5);
-    epi(row, sell_row<float, IDX, 8>(vals + b0 + lane, cols + b0 + lane, wd, (int32_t)row,
-                                     checked(GatherX<float>{r}, n, &st->status)));
+    epi(row, sell_row<float, IDX, 16>(vals + b0 + lane, cols + b0 + lane, wd, (int32_t)row,
+                                      checked(GatherX<float>{r}, n, &st->status)));
   }
   double v[1] = {(double)epi.a}, tot[1];
   if (!reduce_finish<1>(v, partials, &st->ticket, tot)) return;
