@@ -175,9 +175,9 @@ __device__ __forceinline__ void tile_product_g(const BatchArgs& a, int32_t r0, i
 template <typename V = double, typename Pre, typename Post>
 __device__ __forceinline__ void tile_product(const BatchArgs& a, int32_t r0, int32_t r1, const V* v, Pre&& pre,
                                              Post&& post) {
-  // entries in flight per lane: 16 FP32 (half the bytes each) or 8 FP64
-  tile_product_g<V, sizeof(V) == 4 ? 16 : 8>(a, r0, r1, GatherPlain<V>{v}, static_cast<Pre&&>(pre),
-                                             static_cast<Post&&>(post));
+  // 16 entries in flight a lane: a P1 row in one round (FP64 batch 42.4-42.6 ms against 44.7 ms with
+  // 8, no spills at the 64-register cap)
+  tile_product_g<V, 16>(a, r0, r1, GatherPlain<V>{v}, static_cast<Pre&&>(pre), static_cast<Post&&>(post));
 }
 
 // The rows [r0, r1) of a tile, S trips of 32 at a time: load(i) for all S rows of a round first
