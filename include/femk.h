@@ -392,7 +392,9 @@ int femk_pcg_batched(const femk_plan* plan, int32_t nprob, const int64_t* row_of
  * problem. Problem k retires when its FP64 <r, r> <= max(tol^2 <b, b>, atol^2) or at maxiter FP32
  * iterations. iters_out_host = FP32 iterations, outer_out_host = FP64 residual evaluations (may be
  * NULL); the other arguments as femk_pcg_batched (inv_diag_dev may be NULL: no preconditioner).
- * No reference counterpart.
+ * On plans with int16 column offsets and rows of at most 16 entries (P1 tetrahedra) and with
+ * tile_rows <= 512 the launch uses 92-96 KB of dynamic shared memory a block (a two-stage ring a
+ * warp that streams the FP32 slices and the update-phase operands). No reference counterpart.
  */
 int femk_pcg_batched_mixed(const femk_plan* plan, int32_t nprob, const int64_t* row_off_host, const double* vals_dev,
                            const double* b_dev, double* x_dev, const double* inv_diag_dev, double tol, double atol,
