@@ -624,7 +624,7 @@ def adjoint_variant(dev, n=64, n_fd=32, check=True):
         if big.any() else None,
         "fd_method": ("(J(+eps) - J(-eps)) / 2 eps with J(+) - J(-) = sum M d (u- + d/2 - u*), d solving "
                       "A(+) d = (A(-) - A(+)) u-: no subtractive cancellation; truncation O(eps^2), solves to 1e-13"),
-        "target": "1e-6 relative (north star); jax.grad cannot run here, the host adjoint stands in",
+        "target": "1e-6 relative to FD and to jax.grad; jax.grad cannot run here, the host adjoint stands in",
     })
     return out
 
