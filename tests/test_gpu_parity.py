@@ -443,19 +443,21 @@ def test_bicgstab_status_paths():
 def test_spmv_layouts_agree():
     """The CG-step SpMV has three layouts: bulk-copy slices with per-slice column tables (the
     default), bulk-copy slices with per-entry columns (column_tables = 0), and the thread-per-row
-    kernel (ring64 = ring32 = 0). All sum each row in the same order; the two bulk forms (same grid,
-    same reductions) give bit-identical solves, the thread-per-row form agrees to rounding of its dot
-    products (another grid). 64^3 hexes: z-lines of 65 rows, so about half the 32-row slices share
-    one offset sequence."""
+    kernel (ring64 = ring32 = 0), here also on int32 columns (cols16 = 0: the FP64 form keeps 32
+    entries in flight, as on P2 plans). All sum each row in the same order; the two bulk forms (same
+    grid, same reductions) give bit-identical solves, the thread-per-row forms agree to rounding of
+    their dot products (other grids). 64^3 hexes: z-lines of 65 rows, so about half the 32-row
+    slices share one offset sequence."""
     pf, cf, tets, p1 = _mesh(64, 1)
     lk = torch.as_tensor(om.logk_field(len(tets), 1006), device="cuda")
     out = {}
     vals = b = inv = None
-    for tag, opts in (("table", None), ("entry", {"column_tables": 0}), ("thread", {"ring64": 0, "ring32": 0})):
+    for tag, opts in (("table", None), ("entry", {"column_tables": 0}), ("thread", {"ring64": 0, "ring32": 0}),
+                      ("int32", {"cols16": 0, "ring64": 0, "ring32": 0})):
         plan = _plan(p1, tets, 1, opts)
         if tag == "entry":
             assert plan.sell_col_units == plan.sell_nnz
-        else:
+        elif tag != "int32":  # (info.cols16 is the mesh's property; the option switches the FP64 stream)
             assert plan.sell_col_units < 0.7 * plan.sell_nnz
         if vals is None:
             vals, b = plan.assemble(lk)
@@ -465,12 +467,14 @@ def test_spmv_layouts_agree():
         ub, itb, relb, stb = plan.bicgstab(vals, b, inv_diag=inv, tol=1e-8)
         assert st == 0 and stm == 0 and stb == 0 and rel <= 2e-8 and relm <= 1e-8 and relb <= 2e-8
         out[tag] = (u, it, um, inner, ub, itb)
-    a, c, e = out["thread"], out["table"], out["entry"]
+    a, c, e, w = out["thread"], out["table"], out["entry"], out["int32"]
     assert c[1] == e[1] and torch.equal(c[0], e[0])
     assert c[3] == e[3] and torch.equal(c[2], e[2])
     assert c[5] == e[5] and torch.equal(c[4], e[4])
     assert abs(a[1] - c[1]) <= 1 and (torch.linalg.norm(a[0] - c[0]) / torch.linalg.norm(c[0])).item() <= 1e-9
     assert abs(a[3] - c[3]) <= 10 and (torch.linalg.norm(a[2] - c[2]) / torch.linalg.norm(c[2])).item() <= 1e-7
+    assert abs(w[1] - a[1]) <= 1 and (torch.linalg.norm(w[0] - a[0]) / torch.linalg.norm(a[0])).item() <= 1e-9
+    assert abs(w[3] - a[3]) <= 10 and (torch.linalg.norm(w[2] - a[2]) / torch.linalg.norm(a[2])).item() <= 1e-7
 
 
 def test_canonical_csr_solver_path_matches():
