@@ -507,6 +507,10 @@ def batched_variant(dev, count=256, reps=3):
     vals, b = batch.plan.assemble(logk)
     inv = batch.plan.jacobi(vals)
     sched = batched_schedule(batch, vals, b, inv, 1e-8)
+    # one untimed call with the chosen schedule first: the tuner's last trial leaves another
+    # schedule's graph and tile tables in place, and their rebuild is not part of a solve
+    batch.plan.pcg_batched(batch.row_off, vals, b, None, inv, 1e-8, 0.0, 20_000, sched["tile_rows"],
+                           sched["blocks_per_sm"])
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
