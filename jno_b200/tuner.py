@@ -67,6 +67,9 @@ def tune(batch, vals, b, inv, tol, candidates=None, reps=3):
             runs.append(e0.elapsed_time(e1))
         times[(tile_rows, bps)] = statistics.median(runs)
     best = min(times, key=times.get)
+    # leave the plan holding the chosen schedule's graph and tile tables (the last trial's otherwise),
+    # so the caller's first solve does not rebuild them
+    plan.pcg_batched(batch.row_off, vals, b, None, inv, tol, 0.0, 20_000, best[0], best[1])
     return {"tile_rows": best[0], "blocks_per_sm": best[1], "ms": times[best]}, times
 
 
