@@ -570,6 +570,87 @@ __global__ void __launch_bounds__(128, ND == 10 ? 6 : 8) k_matfree(const double*
   }
 }
 
+// Kuhn blocks: six consecutive tetrahedra that split one hexahedron, tet e of a block being the
+// corners kuhn_corner(e, 0..3) (corner bit 2 = x, bit 1 = y, bit 0 = z), the layout the structured box
+// constructor emits (domain.py KUHN). k_kuhn_corners checks a plan's masked connectivity against it
+// block by block and keeps each block's 8 corners; when every block fits, the P1 matrix-free operator
+// works a hexahedron at a time (k_matfree_kuhn).
+// Tet e is the corners {0, a_e, b_e, 7} with a = (4, 4, 2, 2, 1, 1) and b = (6, 5, 6, 3, 5, 3), packed a
+// nibble per tet; in unrolled loops every call folds to a constant.
+__host__ __device__ constexpr int kuhn_corner(int e, int j) {
+  return j == 0 ? 0 : (j == 3 ? 7 : (((j == 1 ? 0x112244 : 0x353656) >> (4 * e)) & 15));
+}
+
+__global__ void k_kuhn_corners(const int32_t* __restrict__ mcells, int64_t nhex, int32_t* __restrict__ corners,
+                               int* __restrict__ bad) {
+  for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < nhex; h += (int64_t)gridDim.x * blockDim.x) {
+    constexpr int32_t kUnset = INT32_MIN;  // a masked id is d >= 0 or -1 - d, never this
+    int32_t c[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) c[u] = kUnset;
+    bool ok = true;
+#pragma unroll
+    for (int e = 0; e < 6; ++e) {
+      const int4 d4 = __ldg(reinterpret_cast<const int4*>(mcells) + 6 * h + e);
+      const int32_t d[4] = {d4.x, d4.y, d4.z, d4.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int u = kuhn_corner(e, j);
+        if (c[u] == kUnset)
+          c[u] = d[j];
+        else
+          ok = ok && c[u] == d[j];
+      }
+    }
+    if (!ok) atomicExch(bad, 1);
+    int4* o = reinterpret_cast<int4*>(corners) + 2 * h;
+    o[0] = make_int4(c[0], c[1], c[2], c[3]);
+    o[1] = make_int4(c[4], c[5], c[6], c[7]);
+  }
+}
+
+// y += A x over whole Kuhn blocks: one thread loads a hexahedron's 8 corners, their coordinates and
+// x once (six separate elements load 24 of each), applies the six element operators (p1_apply, the
+// local indices compile-time constants) and adds into the 8 corners with 8 atomics in place of 24.
+__global__ void __launch_bounds__(128) k_matfree_kuhn(const double* __restrict__ xyz,
+                                                      const int32_t* __restrict__ corners, int64_t nhex,
+                                                      const double* __restrict__ param, int mode, double scale,
+                                                      const double* __restrict__ x, double* __restrict__ y,
+                                                      const CgState* st) {
+  if (st && st->done) return;
+  for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < nhex; h += (int64_t)gridDim.x * blockDim.x) {
+    const int4 c0 = __ldg(reinterpret_cast<const int4*>(corners) + 2 * h);
+    const int4 c1 = __ldg(reinterpret_cast<const int4*>(corners) + 2 * h + 1);
+    const int32_t c[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+    double X[8][3], xv[8], ys[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int64_t v = c[u] >= 0 ? c[u] : -1 - c[u];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) X[u][q] = __ldg(xyz + v * 3 + q);
+      xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : 0.0;
+      ys[u] = 0.0;
+    }
+#pragma unroll
+    for (int e = 0; e < 6; ++e) {
+      double P[4][3], xe[4], ye[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) P[i][q] = X[kuhn_corner(e, i)][q];
+        xe[i] = xv[kuhn_corner(e, i)];
+      }
+      p1_apply(P, xe, ye);
+      const double k = coef_of(param, mode, scale, 6 * h + e);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) ys[kuhn_corner(e, i)] += k * ye[i];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (c[u] >= 0) atomicAdd(y + c[u], ys[u]);
+  }
+}
+
 // the masked connectivity of the matrix-free operator
 __global__ void k_mask_cells(const int32_t* __restrict__ cells, int64_t len, const uint8_t* __restrict__ dmask,
                              int32_t* __restrict__ mcells) {
@@ -904,15 +985,43 @@ __global__ void k_zero(double* __restrict__ y, int64_t n, const CgState* st) {
 }
 
 // y = A x for the matrix-free operator; with st != NULL every launch is a no-op once st->done.
-// the masked connectivity, built on first use (the Dirichlet set of a plan is fixed)
+// the masked connectivity, built on first use (the Dirichlet set of a plan is fixed), and on a P1
+// tetrahedral plan the Kuhn-block check (once, with a synchronous read of its flag)
 int ensure_mcells(const femk_plan* pc, cudaStream_t s) {
   femk_plan* p = const_cast<femk_plan*>(pc);
-  if (p->mcells) return FEMK_OK;
-  const int64_t len = p->ntet * p->nd;
-  FEMK_CUDA_TRY(cudaMalloc(&p->mcells, sizeof(int32_t) * (len > 0 ? len : 1)));
-  k_mask_cells<<<::femk::counted_launch() + blocks_for(len, 256, p->n_sm * 16), 256, 0, s>>>(p->cells, len, p->dmask,
-                                                                                             p->mcells);
-  FEMK_CUDA_TRY(cudaGetLastError());
+  if (!p->mcells) {
+    const int64_t len = p->ntet * p->nd;
+    FEMK_CUDA_TRY(cudaMalloc(&p->mcells, sizeof(int32_t) * (len > 0 ? len : 1)));
+    k_mask_cells<<<::femk::counted_launch() + blocks_for(len, 256, p->n_sm * 16), 256, 0, s>>>(p->cells, len, p->dmask,
+                                                                                               p->mcells);
+    FEMK_CUDA_TRY(cudaGetLastError());
+  }
+  if (p->kuhn_state == 0) {
+    p->kuhn_state = -1;
+    if (p->nd == 4 && p->dim == 3 && p->ntet > 0 && p->ntet % 6 == 0) {
+      const int64_t nhex = p->ntet / 6;
+      int* flag = nullptr;
+      FEMK_CUDA_TRY(cudaMalloc(&p->kuhn, sizeof(int32_t) * 8 * nhex));
+      FEMK_CUDA_TRY(cudaMalloc(&flag, sizeof(int)));
+      int bad = 1;
+      cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), s);
+      if (e == cudaSuccess) {
+        k_kuhn_corners<<<::femk::counted_launch() + blocks_for(nhex, 256, p->n_sm * 16), 256, 0, s>>>(p->mcells, nhex,
+                                                                                                   p->kuhn, flag);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, flag, sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      cudaFree(flag);
+      FEMK_CUDA_TRY(e);
+      if (bad) {
+        cudaFree(p->kuhn);
+        p->kuhn = nullptr;
+      } else {
+        p->kuhn_state = 1;
+      }
+    }
+  }
   return FEMK_OK;
 }
 
@@ -921,7 +1030,11 @@ int launch_matfree(const femk_plan* p, const MatFree& m, const double* x, double
   FEMK_TRY(ensure_mcells(p, s));
   k_zero<<<::femk::counted_launch() + p->n_sm * 8, 256, 0, s>>>(y, p->n, st);
   const int grid = blocks_for(p->ntet, 128, p->n_sm * 16);
-  FEMK_BY_ND(p->nd, k_matfree<ND><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->mcells, p->ntet, m.param, m.mode, m.scale, x, y, st));
+  if (p->kuhn)
+    k_matfree_kuhn<<<::femk::counted_launch() + blocks_for(p->ntet / 6, 128, p->n_sm * 16), 128, 0, s>>>(
+        p->xyz, p->kuhn, p->ntet / 6, m.param, m.mode, m.scale, x, y, st);
+  else
+    FEMK_BY_ND(p->nd, k_matfree<ND><<<::femk::counted_launch() + grid, 128, 0, s>>>(p->xyz, p->mcells, p->ntet, m.param, m.mode, m.scale, x, y, st));
   FEMK_CUDA_TRY(cudaGetLastError());
   if (p->n_dir > 0) {
     k_dirichlet_identity<<<::femk::counted_launch() + blocks_for(p->n_dir, 256, 65535), 256, 0, s>>>(p->dlist, p->n_dir, x, y, st);

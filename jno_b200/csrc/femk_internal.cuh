@@ -232,6 +232,8 @@ struct femk_plan {
   double* coef_tmp = nullptr;   // f64[ntet] element coefficients of a nodal parameter
   double* kcoef = nullptr;      // f64[ntet] exp(param) of the current assembly or matrix-free solve
   int32_t* mcells = nullptr;    // i32[ntet*nd] cells with each Dirichlet DOF d as -1 - d (matrix-free operator)
+  int32_t* kuhn = nullptr;      // i32[ntet/6*8] masked corners of each Kuhn block (P1 matrix-free, hex at a time)
+  int kuhn_state = 0;           // 0 not checked, 1 every block of six tets is a Kuhn block, -1 not
   double* theta_ws = nullptr;   // f64[3 vstride] theta march: step Jacobi inverse, step right-hand side, previous state
   double* gm_ws = nullptr;      // GMRES: Krylov basis (restart + 1 vectors), w, q, partials, small arrays
   int64_t gm_size = 0;          // doubles in gm_ws

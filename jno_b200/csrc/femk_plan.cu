@@ -839,7 +839,7 @@ extern "C" int femk_plan_destroy(femk_plan* p) {
                   p->sell_ptr, p->sell_cols, p->sell_c16,  p->sell_vals, p->sell_vals32,
                   p->bar,      p->batch_ws,  p->bicg_ws,   p->bicg_state, p->sell_cuptr, p->sell_cu,
                   p->coef_tmp, p->theta_ws, p->cmp_ws, p->gm_ws, p->dev_err, p->astr_ptr, p->astr_elem,
-                  p->astr_k, p->astr_pos, p->astr_load, p->kcoef, p->mcells};
+                  p->astr_k, p->astr_pos, p->astr_load, p->kcoef, p->mcells, p->kuhn};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->state_host) cudaFreeHost(p->state_host);

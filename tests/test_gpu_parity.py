@@ -154,6 +154,31 @@ def test_spmv_and_matrix_free_match():
         assert torch.linalg.norm(u1 - u2) <= 1e-7 * torch.linalg.norm(u1)
 
 
+def test_matrix_free_p1_kuhn_blocks_and_per_element():
+    """The P1 matrix-free operator works a hexahedron a thread when the elements come in Kuhn blocks
+    (the box constructor's order) and an element a thread otherwise (here the first two tetrahedra of
+    every block swapped, so the plan's block check fails). Both products match the assembled
+    operator, and so do the solves."""
+    pf, cf, tets, p1 = _mesh(8, 1, seed=2)
+    logk = om.logk_field(len(tets), 7)
+    perm = np.arange(len(tets)).reshape(-1, 6)
+    perm[:, [0, 1]] = perm[:, [1, 0]]
+    perm = perm.ravel()
+    xv = torch.as_tensor(np.random.default_rng(3).standard_normal(len(p1)), device="cuda")
+    sols = []
+    for t, lk in ((tets, logk), (tets[perm], logk[perm])):
+        plan = _plan(p1, t, 1)
+        lkd = torch.as_tensor(lk, device="cuda")
+        vals, b = plan.assemble(lkd)
+        y_asm = plan.spmv(vals, xv)
+        y_mf = plan.spmv_matfree(lkd, xv)
+        assert (y_mf - y_asm).abs().max().item() <= 1e-12 * y_asm.abs().max().item()
+        u, it, rel, st = plan.pcg_matfree(lkd, b, inv_diag=plan.jacobi_matfree(lkd))
+        assert st == 0 and rel <= 2e-8
+        sols.append(u)
+    assert torch.linalg.norm(sols[0] - sols[1]) <= 1e-7 * torch.linalg.norm(sols[0])
+
+
 @pytest.mark.parametrize("mode", [0, 1])
 def test_mixed_precision_reaches_fp64_accuracy(mode):
     pf, cf, tets, p1 = _mesh(16, 1)
